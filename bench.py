@@ -1,0 +1,333 @@
+"""Benchmark of the pressure-Poisson hot path on B200.
+
+Workload (one "step"): one complete solve of the 2-D 1024 x 1024 variable-coefficient
+pressure Poisson -- beta = 1/rho with rho = 1000 inside 64 seeded bubbles (radii 8-48
+cells) and 1 outside, a seeded Gaussian right-hand side with zero mean -- from a zero
+initial guess to ||f - A p||_2 <= 1e-10 ||f||_2 by PCG with a 6-level V(2,2) red-black
+multigrid preconditioner, FP64 throughout, set-up (beta coarsening) included.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank solves its own replica (the 2-D multigrid does not shard
+here); value = solves of all ranks / the slowest rank's time.  Rank 0 prints one JSON
+line.  --impl reference times the CPU restatement of the same solve (the reference has
+no GPU path and cannot be compiled here) on all host cores, rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RK3 steps/s & MG solves/s at 1e-10 residual: plain FP64 vs mixed+learned"
+UNIT = "MG solves/s"
+N = 1024
+NLEVELS = 6
+RTOL = 1e-10
+WORKLOAD = ("2-D 1024x1024 variable-coefficient pressure Poisson, beta=1/rho with rho 1000:1 in 64 seeded "
+            "bubbles (radii 8-48 cells), Gaussian RHS; PCG with 6-level V(2,2) red-black multigrid "
+            "preconditioner to 1e-10 relative residual from p=0, set-up included")
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ clocks sampler
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu=uuid,{self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            if self.uuid and parts[0] != self.uuid:
+                continue
+            self.samples.append(parts[1:])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        smax = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for name, v in zip(names, s[4:8]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------------ CPU legs (oracle)
+def cpu_solves(case, max_seconds, max_solves):
+    """Time the CPU restatement of the same solve (OpenMP on all host cores)."""
+    from oracle import oracle
+    oracle.lib(native=True)
+    times, its = [], []
+    t_all = time.perf_counter()
+    while len(times) < max_solves:
+        t0 = time.perf_counter()
+        _, it, rel, _, st = oracle.mg_solve(case.f, case.bx, case.by, case.hx, case.hy, nlevels=NLEVELS, ncoarse=2,
+                                           sym=5, method="pcg", rtol=RTOL, max_cycles=200, native=True)
+        times.append(time.perf_counter() - t0)
+        its.append(it)
+        if time.perf_counter() - t_all > max_seconds:
+            break
+    return times, its
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from lica_boiling1d_b200.inputs import bubble_poisson_case
+    threads = os.cpu_count()
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    case = bubble_poisson_case(N)
+    cpu_solves(case, 1e9, max(1, args.warmup))  # warm-up (also builds the native oracle)
+    times, its = cpu_solves(case, 1e9, args.steps)
+    total = sum(times)
+    value = len(times) / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": len(times), "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "nx": N, "ny": N, "nlevels": NLEVELS, "rtol": RTOL, "solver": "MG-PCG",
+                   "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
+                         "sample": f"{len(times)} complete solves (one per step), FP64 C++/OpenMP restatement"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "iterations": its[-1],
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU leg
+ALG_BYTES_PER_CELL = {  # FP64, level 0: each distinct array read or written once per cell
+    "down0": 8 * (3 + 1 + 0.25),       # read f, bx, by; write u, f_coarse
+    "up0": 8 * (5 + 0.25),             # read u, u_coarse(1/4), f, bx, by; write u
+    "pupdate": 8 * 5,                  # read z, p, bx, by; write p
+    "xupdate": 8 * 7,                  # read x, p, f, bx, by; write x, r
+}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from lica_boiling1d_b200 import native, poisson
+    from lica_boiling1d_b200.inputs import bubble_poisson_case
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    case = bubble_poisson_case(N)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    f, bx, by = t(case.f), t(case.bx), t(case.by)
+    p = torch.zeros((N, N), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    solver = poisson.MultigridPoisson(N, N, case.hx, case.hy, nlevels=NLEVELS, ncoarse=2, precision=args.precision,
+                                      use_graph=True)
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def slowest(x):
+        if world == 1:
+            return x
+        v = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(v, op=dist.ReduceOp.MAX)
+        return float(v.item())
+
+    # warm-up (builds and caches the graph)
+    for _ in range(args.warmup):
+        p.zero_()
+        solver.solve(p, f, bx, by, rtol=RTOL)
+    torch.cuda.synchronize(dev)
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    props = torch.cuda.get_device_properties(dev)
+    uuid = "GPU-" + str(props.uuid) if hasattr(props, "uuid") else None
+    clocks = ClockSampler(uuid)
+    clocks.start()
+    time.sleep(0.4)
+    barrier()
+    torch.cuda.synchronize(dev)
+    l0 = native.launch_count()
+    its = []
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)            # > L2 between timed solves
+        p.zero_()
+        ev[k][0].record(stream)
+        it, rel, st = solver.solve(p, f, bx, by, rtol=RTOL)
+        ev[k][1].record(stream)
+        its.append(it)
+        if st != 0:
+            raise RuntimeError(f"solve did not converge: status {st} rel {rel}")
+    torch.cuda.synchronize(dev)
+    barrier()
+    launches = native.launch_count() - l0
+    clk = clocks.stop()
+    total_ms = sum(a.elapsed_time(b) for a, b in ev)
+    total_ms = slowest(total_ms)
+    value = world * args.steps / (total_ms / 1e3)
+
+    # end-to-end through the host C-ABI entry: H2D of p0, f, bx, by; solve; D2H of p
+    hf = torch.from_numpy(case.f.copy()).pin_memory().numpy()
+    hbx = torch.from_numpy(case.bx.copy()).pin_memory().numpy()
+    hby = torch.from_numpy(case.by.copy()).pin_memory().numpy()
+    hp = torch.zeros((N, N), dtype=torch.float64).pin_memory().numpy()
+    for _ in range(2):
+        hp[...] = 0.0
+        solver.solve(hp, hf, hbx, hby, rtol=RTOL, stream=stream)
+    ke = max(3, min(args.steps, 10))
+    eve = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(ke)]
+    barrier()
+    torch.cuda.synchronize(dev)
+    for k in range(ke):
+        flush.fill_(k & 0xFF)
+        hp[...] = 0.0
+        eve[k][0].record(stream)
+        solver.solve(hp, hf, hbx, hby, rtol=RTOL, stream=stream)
+        eve[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    e2e_ms = slowest(sum(a.elapsed_time(b) for a, b in eve))
+    e2e = {"value": world * ke / (e2e_ms / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": int(hp.nbytes + hf.nbytes + hbx.nbytes + hby.nbytes),
+           "d2h_bytes_per_step": int(hp.nbytes), "steps": ke, "path": "lica_mg_solve_host (C ABI), pinned host buffers"}
+
+    # kernel-class timing: one profiled solve (separate launches bracketed by CUDA events)
+    solver.profile(True)
+    for _ in range(3):
+        flush.fill_(1)
+        p.zero_()
+        solver.solve(p, f, bx, by, rtol=RTOL)
+    prof = solver.profile_read()
+    solver.profile(False)
+    level0 = {k: prof[k] for k in ALG_BYTES_PER_CELL}
+    dom = max(level0, key=lambda k: level0[k][0])
+    ms, nl = level0[dom]
+    avg_s = ms / 1e3 / max(nl, 1)
+    alg = ALG_BYTES_PER_CELL[dom] * N * N
+    peak, peak_kind = peaks()
+    achieved = alg / avg_s / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                "alg_bytes_per_launch": alg, "avg_launch_us": avg_s * 1e6,
+                "kernel_classes_ms_per_solve": {k: v[0] / 3 for k, v in prof.items()},
+                "note": "one profiled solve as separate launches after the timed region; working set is L2-resident"}
+
+    # secondary: the mixed-precision preconditioner on the same workload
+    variants = {}
+    if args.precision == "fp64" and not args.skip_variants:
+        sm = poisson.MultigridPoisson(N, N, case.hx, case.hy, nlevels=NLEVELS, ncoarse=2, precision="mixed")
+        for _ in range(3):
+            p.zero_()
+            sm.solve(p, f, bx, by, rtol=RTOL)
+        evm = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(ke)]
+        itm = []
+        for k in range(ke):
+            flush.fill_(k & 0xFF)
+            p.zero_()
+            evm[k][0].record(stream)
+            itm.append(sm.solve(p, f, bx, by, rtol=RTOL)[0])
+            evm[k][1].record(stream)
+        torch.cuda.synchronize(dev)
+        mms = sum(a.elapsed_time(b) for a, b in evm)
+        variants["mixed"] = {"value": ke / (mms / 1e3), "unit": UNIT, "iterations": itm[-1],
+                             "note": "FP32 smoothing/restriction/prolongation, FP64 residual, CG and coarsest solve"}
+        sm.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        threads = os.cpu_count()
+        times, cits = cpu_solves(case, 15.0, 30)
+        cpu = {"value": len(times) / sum(times), "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{len(times)} complete solves of the same workload (~15 s), FP64 C++/OpenMP restatement"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "nx": N, "ny": N, "nlevels": NLEVELS, "nu1": 2, "nu2": 2, "rtol": RTOL,
+                       "solver": "MG-PCG", "precision": args.precision, "l2_flush": "256 MiB write between steps",
+                       "parallelism": f"replicas x{world}"},
+            "iterations": its[-1], "rel_residual": rel,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clk, "variants": variants,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-variants", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

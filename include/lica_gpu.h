@@ -1,0 +1,158 @@
+/*
+ * lica_gpu.h -- C ABI of the B200 (sm_100a) hot path of the lica two-phase boiling
+ * solver.  Plain pointers and sizes only; every entry point returns a lica_status.
+ *
+ * Two kinds of entry points:
+ *   1. Drop-ins for the reference's Fortran subroutines (1d.f), taking the same arrays
+ *      in the same Fortran layout (column-major, the Fortran lower bound of each array
+ *      noted per argument).  Arrays are HOST arrays; the call copies them to the GPU,
+ *      runs the CUDA kernels and copies the results back, like the subroutine it
+ *      replaces.  A Fortran host binds them with ISO_C_BINDING.
+ *   2. Device-resident entry points (suffix _device) taking device pointers and a
+ *      cudaStream_t passed as void*, for callers that keep state in HBM.
+ *
+ * Threading: call a given context from one host thread at a time.  Contexts are
+ * independent.  Errors never abort the process: the return value says what happened
+ * and lica_last_error() gives a message for LICA_ERR_CUDA / LICA_BAD_ARG.
+ */
+#ifndef LICA_GPU_H
+#define LICA_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (the reference has none: it STOPs or prints and continues). */
+enum lica_status {
+    LICA_OK = 0,
+    LICA_NOT_CONVERGED = 1, /* iteration cap reached before the tolerance */
+    LICA_BAND_OVERFLOW = 2, /* analogue of the band-size STOP, two_phase.f:1989-1994 */
+    LICA_NAN = 3,           /* non-finite value met */
+    LICA_BAD_ARG = 4,       /* argument outside what the entry point supports */
+    LICA_ERR_CUDA = 5,      /* a CUDA runtime call failed (see lica_last_error) */
+    LICA_ERR_NOMEM = 6
+};
+
+/* Message for the last LICA_ERR_CUDA / LICA_BAD_ARG on the calling thread. */
+const char* lica_last_error(void);
+
+/* Number of kernel launches this library has issued since load (a counter the
+ * benchmark reads; graph replays count each kernel node). */
+int64_t lica_kernel_launch_count(void);
+
+/* ------------------------------------------------------------------------------------
+ * Tridiagonal solvers
+ * ---------------------------------------------------------------------------------- */
+
+/* TRDIAG3 (1d.f:3783-3811): for every line I in [ll1,ll2] solve the tridiagonal
+ * system along J in [l1,l2]:  A(I,J) x(J-1) + B(I,J) x(J) + C(I,J) x(J+1) = R(I,J).
+ * A,B,C,R,UU are Fortran (ld, *) arrays, 1-based: X(I,J) = x[(I-1) + (J-1)*ld].
+ * UU receives the solution, R(I,J) is overwritten with it for J < l2 (as the
+ * reference's loop 30 does); R and UU may be the same array (LHSW, 1d.f:1790).
+ * Host arrays; one GPU thread per line, Thomas algorithm in the reference's order. */
+int lica_gpu_trdiag3(const double* A, const double* B, const double* C, double* R, double* UU,
+                     int64_t l1, int64_t l2, int64_t ll1, int64_t ll2, int64_t ld);
+
+/* TRDIAG3P (1d.f:3929-3983): periodic (cyclic) tridiagonal systems; lines K in
+ * [l1,l2] (first index), unknowns J in [j1,j2] (second index); the solution
+ * overwrites F.  Host arrays, Fortran (ld, *) layout as above. */
+int lica_gpu_trdiag3p(const double* A, const double* B, const double* C, double* F,
+                      int64_t j1, int64_t j2, int64_t l1, int64_t l2, int64_t ld);
+
+/* Device-resident batched variants: same layout, device pointers. */
+int lica_gpu_trdiag3_device(const double* A, const double* B, const double* C, double* R, double* UU,
+                            int64_t l1, int64_t l2, int64_t ll1, int64_t ll2, int64_t ld, void* stream);
+int lica_gpu_trdiag3p_device(const double* A, const double* B, const double* C, double* F,
+                             int64_t j1, int64_t j2, int64_t l1, int64_t l2, int64_t ld, void* stream);
+
+/* POISSON (1d.f:3492-3578), the 1-D column the reference solves (N1M = N2M = 1):
+ * AK = VVDZ(K)*SSDZ(K)*DENF_ZI(1,1,K)*(1-FIXKL(K)), CK = VVDZ(KP1)*SSDZ(K)*DENF_ZI(1,1,KP1),
+ * BK = -(AK+CK), Thomas solve, P(1,1,K) = x(K), then P(I,J,0)=P(I,J,1) and
+ * P(I,J,N3)=P(I,J,N3M).  Array bounds (Fortran):
+ *   P, DENF_ZI: (0:m1, 0:m2, 0:m3)     DIVGSUM: (m1-1, m2-1, m3-1), 1-based
+ *   vvdz: VVDZ(1:m3)   ssdz: SSDZ(0:m3)   fixkl: FIXKL(1:m3-1)   kpv: KPV(0:m3+1)
+ * Host arrays.  Returns LICA_BAD_ARG unless n1m = n2m = 1 (2-D and 3-D fields use the
+ * multigrid entry points below). */
+int lica_gpu_poisson(int64_t m1, int64_t m2, int64_t m3, int64_t n1m, int64_t n2m, int64_t n3m,
+                     const double* vvdz, const double* ssdz, const double* fixkl, const int64_t* kpv,
+                     double* p, const double* divgsum, const double* denf_zi);
+
+/* ------------------------------------------------------------------------------------
+ * Multigrid-preconditioned CG pressure Poisson, 2-D (new build; the reference's POISSON
+ * is 1-D Thomas).  Operator: the 2-D generalisation of 1d.f:3535-3541 on a uniform
+ * nx x ny cell grid, x periodic, y a wall with Neumann bottom (FIXKL) and p = 0 on the
+ * top face (VVDZ(N3) = 2/h, FIXKU commented out at 1d.f:3538):
+ *   (A u)_ij = sum over the 4 faces of beta_face/h^2 * (u_nb - u_ij),
+ *   bx[j*nx+i] = beta on the face left of cell i (periodic), j in [0,ny)
+ *   by[j*nx+i] = beta on the face below cell row j, j in [0,ny]  (row 0 unused, row ny
+ *                the top wall, weighted 2/h^2).
+ * Solves A p = f to ||f - A p||_2 <= rtol ||f||_2 with PCG whose preconditioner is one
+ * symmetric V(nu1,nu2) red-black Gauss-Seidel cycle (piecewise-constant prolongation,
+ * 2x2 restriction, face-averaged beta), the coarsest outer level solved by ncoarse inner
+ * V-cycles ending in a dense elimination.
+ * ---------------------------------------------------------------------------------- */
+typedef struct lica_mg lica_mg;
+
+typedef struct {
+    int32_t nlevels;   /* outer levels, e.g. 6 for 1024^2 (coarsest 32^2) */
+    int32_t nu1, nu2;  /* pre/post red-black sweeps, e.g. 2,2 */
+    int32_t ncoarse;   /* inner V-cycles at the coarsest outer level */
+    int32_t precision; /* 0: FP64 throughout; 1: mixed -- FP32 smoothing, restriction and
+                          prolongation; FP64 residual, CG vectors and coarsest solve */
+    int32_t use_graph; /* 1: the whole solve is one CUDA graph with a device-side loop */
+} lica_mg_options;
+
+typedef struct {
+    int32_t iterations;  /* PCG iterations taken */
+    int32_t status;      /* lica_status of the solve */
+    double rel_residual; /* ||f - A p||_2 / ||f||_2 (FP64 true residual) */
+} lica_mg_result;
+
+/* Create a solver for an nx x ny grid with spacings hx, hy.  nx and ny must be
+ * multiples of 32 and halve evenly nlevels-1 times. */
+int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, const lica_mg_options* opt);
+int lica_mg_destroy(lica_mg* mg);
+
+/* Device-resident solve: p (initial guess in, solution out), f, bx, by are device
+ * arrays of nx*ny, nx*ny, nx*ny, nx*(ny+1) doubles.  Enqueued on stream; the call
+ * returns after the solve finished (it reads back the result). */
+int lica_mg_solve_device(lica_mg* mg, double* p, const double* f, const double* bx, const double* by,
+                         double rtol, int32_t max_iters, lica_mg_result* res, void* stream);
+
+/* Same solve on HOST arrays: copies f, bx, by, p to the GPU, solves, copies p back.
+ * stream may be NULL (the context's own stream); the call returns when p is on the host. */
+int lica_mg_solve_host(lica_mg* mg, double* p, const double* f, const double* bx, const double* by,
+                       double rtol, int32_t max_iters, lica_mg_result* res, void* stream);
+
+/* One application of the preconditioner, z = M r (device arrays). */
+int lica_mg_precond_device(lica_mg* mg, double* z, const double* r, const double* bx, const double* by,
+                           void* stream);
+
+/* out = A u (device arrays). */
+int lica_mg_apply_device(lica_mg* mg, double* out, const double* u, const double* bx, const double* by,
+                         void* stream);
+
+/* Kernel-class timing with CUDA events around each launch.  While enabled, solves run
+ * as individual launches (not as a graph) so each kernel can be bracketed; the kernel
+ * sequence is the same as the graph's.  lica_mg_profile resets the totals. */
+enum lica_mg_kernel_class {
+    LICA_MG_DOWN0 = 0,   /* k_down on level 0 */
+    LICA_MG_DOWN = 1,    /* k_down on coarser grid levels */
+    LICA_MG_UP0 = 2,     /* k_up on level 0 (with the r.z partial) */
+    LICA_MG_UP = 3,
+    LICA_MG_CTA = 4,     /* single-CTA coarse levels */
+    LICA_MG_PUPDATE = 5, /* p = z + beta p, p.Ap */
+    LICA_MG_XUPDATE = 6, /* x += alpha p, r = f - A x, ||r|| */
+    LICA_MG_SETUP = 7,   /* beta coarsening */
+    LICA_MG_NCLASS = 8
+};
+int lica_mg_profile(lica_mg* mg, int32_t enable);
+int lica_mg_profile_read(lica_mg* mg, int32_t kernel_class, double* total_ms, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LICA_GPU_H */

@@ -1,0 +1,51 @@
+"""Build the CUDA library (sm_100a) in-tree: lica_boiling1d_b200/_build/liblica_gpu.so.
+
+nvcc cross-compiles without a GPU.  -fmad=false keeps every kernel's floating-point
+operation order exactly as written (no FMA contraction), which is what makes the
+kernels bit-comparable with the CPU oracle; the stencils are memory-bound, so the
+separate multiply and add cost nothing measurable.
+"""
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB = os.path.join(HERE, "_build", "liblica_gpu.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+FLAGS = [
+    "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-fmad=false",
+    "-Xcompiler", "-fPIC", "-shared", "-I" + os.path.join(ROOT, "include"), "-I" + os.path.join(HERE, "csrc"),
+]
+
+
+def sources():
+    return sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")))
+
+
+def deps():
+    return sources() + sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh"))) + [
+        os.path.join(ROOT, "include", "lica_gpu.h"), __file__]
+
+
+def up_to_date() -> bool:
+    if not os.path.exists(LIB):
+        return False
+    mt = os.path.getmtime(LIB)
+    return all(os.path.getmtime(d) <= mt for d in deps())
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and up_to_date():
+        return LIB
+    os.makedirs(os.path.dirname(LIB), exist_ok=True)
+    cmd = [NVCC] + FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-o", LIB + ".tmp"] + sources()
+    subprocess.run(cmd, check=True)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force=True, verbose="-v" in sys.argv))

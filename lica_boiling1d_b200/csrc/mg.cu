@@ -1,0 +1,1409 @@
+// Multigrid-preconditioned CG for the variable-coefficient pressure Poisson equation on
+// one B200 (sm_100a).  The reference's POISSON (1d.f:3492-3578) is a 1-D Thomas solve of
+// AK p(k-1) + BK p(k) + CK p(k+1) = DIVGSUM with AK/CK built from the face values of
+// 1/rho (DENF_ZI); this file solves the 2-D generalisation of that operator (x periodic
+// as IPX=1, y the wall-normal direction with the reference's bottom Neumann / top
+// p=0-on-the-face boundary) for the 2-D workloads.
+//
+// Design (HBM/L2-bound stencil work; no tensor cores):
+//   * Grid kernels own a TX x TY tile plus a halo staged in shared memory and run every
+//     red-black half-sweep of one visit to a level inside the tile (temporal blocking:
+//     the halo shrinks by one ring per half-sweep), so a visit reads u, f, beta once.
+//       k_down : nu1 sweeps from a zero iterate + residual + 2x2 restriction
+//       k_up   : piecewise-constant prolongation + nu2 sweeps (black first), and at
+//                level 0 the r.z partial of the CG update
+//   * The levels below 64x64 run in one CTA with everything in shared memory
+//     (k_cta): remaining outer levels, the coarsest outer level solved in FP64 by inner
+//     V-cycles that end in a dense elimination; levels <= 16x16 run in warp 0 alone.
+//   * CG vector updates are fused with the stencil they need (k_pupdate: p = z + beta p
+//     and p.Ap; k_xupdate: x += alpha p and the true residual f - A x with its norm).
+//     Grid-wide sums use a deterministic last-block reduction, which also computes the
+//     CG scalars on the device, so the host never reads a scalar inside an iteration.
+//   * With use_graph the whole solve is one CUDA graph: set-up kernels followed by a
+//     conditional WHILE node whose body is one PCG iteration; the last block of
+//     k_xupdate sets the loop condition.
+//   * Every kernel follows the operation order of the oracle and the library is built
+//     with -fmad=false, so a preconditioner application is bit-identical to the CPU
+//     restatement in FP64 and in FP32; only the dot products differ (summation order).
+#include "common.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+extern "C" void lica_count_launches(int64_t n);
+
+namespace lica {
+namespace mg {
+
+constexpr int TX = 32;
+constexpr int TY = 32;
+constexpr int NT = 256;          // threads of a grid-kernel CTA
+constexpr int NT_CTA = 1024;     // threads of the single-CTA coarse kernel
+constexpr int kMaxLevels = 16;
+constexpr int kSmallCells = 256; // levels with <= this many cells run in warp 0 alone
+constexpr int kMaxDense = 64;    // bottom-level unknowns solved by dense elimination
+
+struct State {
+    double fscale;  // ||f||_2 (1 if f = 0)
+    double rel;     // ||f - A x||_2 / fscale
+    double rz;      // r.z of the latest preconditioner application
+    double alpha, beta;
+    double tol;
+    double sums[2];
+    int it, max_it;
+    int status;     // lica_status
+    int cont;       // 1 while the loop should continue
+    unsigned cnt[4];
+};
+
+// ------------------------------------------------------------------------------------
+// shared-memory staging
+// ------------------------------------------------------------------------------------
+template <typename TS, typename TG>
+__device__ __forceinline__ void load_region(TS* __restrict__ s, int w, int h, const TG* __restrict__ g, int nx,
+                                            int nrows, int gi0, int gj0) {
+    for (int k = threadIdx.x; k < w * h; k += blockDim.x) {
+        const int sy = k / w, sx = k - sy * w;
+        const int j = gj0 + sy;
+        int i = gi0 + sx;
+        if (i < 0) i += nx; else if (i >= nx) i -= nx;
+        s[k] = (j >= 0 && j < nrows) ? TS(g[(size_t)j * nx + i]) : TS(0);
+    }
+}
+
+// Stencil sums of cell (sx,sy) of a staged region with row pitch RXp (u, f) and the face
+// arrays sbx (pitch RXp+1) and sby (pitch RXp).  j is the global row of the cell.
+template <typename T>
+struct Stencil {
+    T s, d;
+};
+
+template <typename T>
+__device__ __forceinline__ Stencil<T> stencil(const T* su, const T* sbx, const T* sby, int RXp, int sx, int sy,
+                                              int j, int ny, T cx, T cy) {
+    const int c = sy * RXp + sx;
+    const T aw = cx * sbx[sy * (RXp + 1) + sx];
+    const T ae = cx * sbx[sy * (RXp + 1) + sx + 1];
+    const T as = (j > 0) ? cy * sby[c] : T(0);
+    const T byn = sby[c + RXp];
+    const T an = (j < ny - 1) ? cy * byn : (T(2) * cy) * byn;
+    const T uw = su[c - 1], ue = su[c + 1];
+    const T us = (j > 0) ? su[c - RXp] : T(0);
+    const T un = (j < ny - 1) ? su[c + RXp] : T(0);
+    Stencil<T> r;
+    T s = aw * uw;
+    s += ae * ue;
+    s += as * us;
+    s += an * un;
+    T d = aw;
+    d += ae;
+    d += as;
+    d += an;
+    r.s = s;
+    r.d = d;
+    return r;
+}
+
+// One red-black half-sweep of colour `colour` over the region [lo, hi) x [lo, hiy).
+template <typename T>
+__device__ __forceinline__ void half_sweep(T* su, const T* sf, const T* sbx, const T* sby, int RXp, int lo, int hix,
+                                           int hiy, int colour, int gj0, int ny, T cx, T cy) {
+    const int wc = (hix - lo + 1) >> 1;
+    const int rows = hiy - lo;
+    for (int k = threadIdx.x; k < wc * rows; k += blockDim.x) {
+        const int r = k / wc, m = k - r * wc;
+        const int sy = lo + r;
+        const int sx = lo + ((lo + sy + colour) & 1) + 2 * m;
+        const int j = gj0 + sy;
+        if (sx >= hix || j < 0 || j >= ny) continue;
+        const Stencil<T> st = stencil(su, sbx, sby, RXp, sx, sy, j, ny, cx, cy);
+        su[sy * RXp + sx] = (st.s - sf[sy * RXp + sx]) / st.d;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// k_down: nu1 red-black sweeps from a zero iterate, residual, 2x2 restriction.
+// ------------------------------------------------------------------------------------
+template <typename T, int NSW>
+__global__ void __launch_bounds__(NT) k_down(const T* __restrict__ f, const T* __restrict__ bx,
+                                             const T* __restrict__ by, T* __restrict__ u_out,
+                                             T* __restrict__ fc_out, int nx, int ny, T cx, T cy) {
+    constexpr int H = 2 * NSW + 1;
+    constexpr int RX = TX + 2 * H, RY = TY + 2 * H;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* su = reinterpret_cast<T*>(smem_raw);
+    T* sf = su + RX * RY;
+    T* sbx = sf + RX * RY;
+    T* sby = sbx + (RX + 1) * RY;
+    const int gi0 = blockIdx.x * TX - H, gj0 = blockIdx.y * TY - H;
+    for (int k = threadIdx.x; k < RX * RY; k += blockDim.x) su[k] = T(0);
+    load_region(sf, RX, RY, f, nx, ny, gi0, gj0);
+    load_region(sbx, RX + 1, RY, bx, nx, ny, gi0, gj0);
+    load_region(sby, RX, RY + 1, by, nx, ny + 1, gi0, gj0);
+    __syncthreads();
+#pragma unroll 1
+    for (int q = 0; q < 2 * NSW; ++q) {
+        half_sweep(su, sf, sbx, sby, RX, q + 1, RX - 1 - q, RY - 1 - q, q & 1, gj0, ny, cx, cy);
+        __syncthreads();
+    }
+    // write the tile's iterate
+    for (int k = threadIdx.x; k < TX * TY; k += blockDim.x) {
+        const int ty = k / TX, tx = k - ty * TX;
+        u_out[(size_t)(blockIdx.y * TY + ty) * nx + blockIdx.x * TX + tx] = su[(ty + H) * RX + tx + H];
+    }
+    // residual of the 4 children of each coarse cell and their average
+    const int ncx = nx >> 1;
+    for (int k = threadIdx.x; k < (TX / 2) * (TY / 2); k += blockDim.x) {
+        const int cj = k / (TX / 2), ci = k - cj * (TX / 2);
+        T r[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int sx = H + 2 * ci + (q & 1), sy = H + 2 * cj + (q >> 1);
+            const int j = gj0 + sy;
+            const Stencil<T> st = stencil(su, sbx, sby, RX, sx, sy, j, ny, cx, cy);
+            r[q] = sf[sy * RX + sx] - (st.s - st.d * su[sy * RX + sx]);
+        }
+        const T fc = T(0.25) * ((r[0] + r[1]) + (r[2] + r[3]));
+        fc_out[(size_t)(blockIdx.y * (TY / 2) + cj) * ncx + blockIdx.x * (TX / 2) + ci] = fc;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// k_up: u += P uc (piecewise constant), nu2 sweeps black-then-red; at level 0 also the
+// partial of r.z (r = f of level 0, z = u) and, in the last block, beta = rz/rz_prev.
+// ------------------------------------------------------------------------------------
+template <typename T, int NSW, bool LEVEL0>
+__global__ void __launch_bounds__(NT) k_up(T* __restrict__ u, const T* __restrict__ uc, const T* __restrict__ f,
+                                           const T* __restrict__ bx, const T* __restrict__ by, int nx, int ny, T cx,
+                                           T cy, State* __restrict__ st, double* __restrict__ partials) {
+    constexpr int H = 2 * NSW;
+    constexpr int RX = TX + 2 * H, RY = TY + 2 * H;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* su = reinterpret_cast<T*>(smem_raw);
+    T* sf = su + RX * RY;
+    T* sbx = sf + RX * RY;
+    T* sby = sbx + (RX + 1) * RY;
+    __shared__ double red[32];
+    const int gi0 = blockIdx.x * TX - H, gj0 = blockIdx.y * TY - H;
+    const int ncx = nx >> 1;
+    for (int k = threadIdx.x; k < RX * RY; k += blockDim.x) {
+        const int sy = k / RX, sx = k - sy * RX;
+        const int j = gj0 + sy;
+        int i = gi0 + sx;
+        if (i < 0) i += nx; else if (i >= nx) i -= nx;
+        T v = T(0);
+        if (j >= 0 && j < ny) {
+            v = u[(size_t)j * nx + i];
+            v += uc[(size_t)(j >> 1) * ncx + (i >> 1)];
+        }
+        su[k] = v;
+    }
+    load_region(sf, RX, RY, f, nx, ny, gi0, gj0);
+    load_region(sbx, RX + 1, RY, bx, nx, ny, gi0, gj0);
+    load_region(sby, RX, RY + 1, by, nx, ny + 1, gi0, gj0);
+    __syncthreads();
+#pragma unroll 1
+    for (int q = 0; q < 2 * NSW; ++q) {
+        half_sweep(su, sf, sbx, sby, RX, q + 1, RX - 1 - q, RY - 1 - q, 1 - (q & 1), gj0, ny, cx, cy);
+        __syncthreads();
+    }
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < TX * TY; k += blockDim.x) {
+        const int ty = k / TX, tx = k - ty * TX;
+        const T z = su[(ty + H) * RX + tx + H];
+        u[(size_t)(blockIdx.y * TY + ty) * nx + blockIdx.x * TX + tx] = z;
+        if (LEVEL0) acc += double(sf[(ty + H) * RX + tx + H]) * double(z);
+    }
+    if (LEVEL0) {
+        const double b = block_sum(acc, red);
+        double tot;
+        if (grid_sum_last(b, partials, &st->cnt[0], &tot, red)) {
+            st->beta = (st->it == 0) ? 0.0 : tot / st->rz;
+            st->rz = tot;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// CG kernels (FP64 vectors)
+// ------------------------------------------------------------------------------------
+// p = z + beta*p on the tile and a one-cell ring, then p.(A p) over the tile; the last
+// block sets alpha = rz / p.Ap.
+template <typename TZ>
+__global__ void __launch_bounds__(NT) k_pupdate(double* __restrict__ p, const TZ* __restrict__ z,
+                                                const double* __restrict__ bx, const double* __restrict__ by, int nx,
+                                                int ny, double cx, double cy, State* __restrict__ st,
+                                                double* __restrict__ partials) {
+    constexpr int H = 1, RX = TX + 2, RY = TY + 2;
+    __shared__ double sp[RX * RY];
+    __shared__ double sbx[(RX + 1) * RY];
+    __shared__ double sby[RX * (RY + 1)];
+    __shared__ double red[32];
+    const int gi0 = blockIdx.x * TX - H, gj0 = blockIdx.y * TY - H;
+    const double beta = st->beta;
+    for (int k = threadIdx.x; k < RX * RY; k += blockDim.x) {
+        const int sy = k / RX, sx = k - sy * RX;
+        const int j = gj0 + sy;
+        int i = gi0 + sx;
+        if (i < 0) i += nx; else if (i >= nx) i -= nx;
+        double v = 0.0;
+        if (j >= 0 && j < ny) {
+            const size_t g = (size_t)j * nx + i;
+            v = double(z[g]) + beta * p[g];
+        }
+        sp[k] = v;
+    }
+    load_region(sbx, RX + 1, RY, bx, nx, ny, gi0, gj0);
+    load_region(sby, RX, RY + 1, by, nx, ny + 1, gi0, gj0);
+    __syncthreads();
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < TX * TY; k += blockDim.x) {
+        const int ty = k / TX, tx = k - ty * TX;
+        const int sx = tx + H, sy = ty + H, j = gj0 + sy;
+        const Stencil<double> s = stencil(sp, sbx, sby, RX, sx, sy, j, ny, cx, cy);
+        const double pv = sp[sy * RX + sx];
+        const double q = s.s - s.d * pv;
+        acc += pv * q;
+        p[(size_t)j * nx + blockIdx.x * TX + tx] = pv;
+    }
+    const double b = block_sum(acc, red);
+    double tot;
+    if (grid_sum_last(b, partials, &st->cnt[1], &tot, red)) st->alpha = st->rz / tot;
+}
+
+// x += alpha*p on the tile and a ring, r = f - A x over the tile (FP64), stored as TR;
+// the last block forms rel = ||r||/||f|| and the loop condition.
+template <typename TR>
+__global__ void __launch_bounds__(NT) k_xupdate(double* __restrict__ x, const double* __restrict__ p,
+                                                const double* __restrict__ f, const double* __restrict__ bx,
+                                                const double* __restrict__ by, TR* __restrict__ r_out, int nx, int ny,
+                                                double cx, double cy, State* __restrict__ st,
+                                                double* __restrict__ partials, int first,
+                                                cudaGraphConditionalHandle cond, int use_cond) {
+    constexpr int H = 1, RX = TX + 2, RY = TY + 2;
+    __shared__ double sxv[RX * RY];
+    __shared__ double sbx[(RX + 1) * RY];
+    __shared__ double sby[RX * (RY + 1)];
+    __shared__ double red[32];
+    const int gi0 = blockIdx.x * TX - H, gj0 = blockIdx.y * TY - H;
+    const double alpha = first ? 0.0 : st->alpha;
+    for (int k = threadIdx.x; k < RX * RY; k += blockDim.x) {
+        const int sy = k / RX, sx = k - sy * RX;
+        const int j = gj0 + sy;
+        int i = gi0 + sx;
+        if (i < 0) i += nx; else if (i >= nx) i -= nx;
+        double v = 0.0;
+        if (j >= 0 && j < ny) {
+            const size_t g = (size_t)j * nx + i;
+            v = first ? x[g] : x[g] + alpha * p[g];
+        }
+        sxv[k] = v;
+    }
+    load_region(sbx, RX + 1, RY, bx, nx, ny, gi0, gj0);
+    load_region(sby, RX, RY + 1, by, nx, ny + 1, gi0, gj0);
+    __syncthreads();
+    double acc = 0.0, accf = 0.0;
+    for (int k = threadIdx.x; k < TX * TY; k += blockDim.x) {
+        const int ty = k / TX, tx = k - ty * TX;
+        const int sx = tx + H, sy = ty + H, j = gj0 + sy;
+        const size_t g = (size_t)j * nx + blockIdx.x * TX + tx;
+        const Stencil<double> s = stencil(sxv, sbx, sby, RX, sx, sy, j, ny, cx, cy);
+        const double xv = sxv[sy * RX + sx];
+        const double fv = f[g];
+        const double r = fv - (s.s - s.d * xv);
+        acc += r * r;
+        if (first) accf += fv * fv;
+        if (!first) x[g] = xv;
+        r_out[g] = TR(r);
+    }
+    const double b = block_sum(acc, red);
+    const double bf = first ? block_sum(accf, red) : 0.0;
+    double tot;
+    // first launch: two sums (||r||^2 then ||f||^2) through two passes of the counter
+    if (first) {
+        if (grid_sum_last(bf, partials + gridDim.x * gridDim.y, &st->cnt[3], &tot, red)) st->sums[1] = tot;
+    }
+    if (grid_sum_last(b, partials, &st->cnt[2], &tot, red)) {
+        __threadfence();
+        if (first) {
+            // the ||f|| sum finished in an earlier (or this) block: read it through L2
+            const double ff = *((volatile double*)&st->sums[1]);
+            const double fn = sqrt(ff);
+            st->fscale = (fn > 0.0) ? fn : 1.0;
+            st->it = 0;
+        } else {
+            st->it = st->it + 1;
+        }
+        const double rel = sqrt(tot) / st->fscale;
+        st->rel = rel;
+        int cont = 0;
+        if (!isfinite(rel)) st->status = LICA_NAN;
+        else if (rel <= st->tol) st->status = LICA_OK;
+        else if (st->it >= st->max_it) st->status = LICA_NOT_CONVERGED;
+        else cont = 1;
+        st->cont = cont;
+        if (use_cond) cudaGraphSetConditional(cond, cont ? 1u : 0u);
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Single-CTA coarse part: outer levels [lcta, lc) in T, the coarsest outer level lc and
+// the inner levels in FP64, all in shared memory.
+// ------------------------------------------------------------------------------------
+struct CtaLevel {
+    int nx, ny;
+    double cx, cy;
+    unsigned off_u, off_f, off_bx, off_by;  // byte offsets into dynamic smem
+    const void* gbx;                        // beta of this level in global memory (T or double)
+    const void* gby;
+};
+
+struct CtaParams {
+    int lcta, lc, bottom;
+    int nu1, nu2, ncoarse;
+    unsigned off_dense, off_rhs;
+    const void* f_in;  // f of level lcta (T)
+    void* u_out;       // u of level lcta (T)
+    CtaLevel lv[kMaxLevels];
+};
+
+template <typename E>
+struct SL {
+    E* u;
+    E* f;
+    E* bx;
+    E* by;
+    int nx, ny;
+    E cx, cy;
+};
+
+template <typename E>
+__device__ __forceinline__ SL<E> make_sl(const CtaParams& P, unsigned char* sm, int l) {
+    const CtaLevel& L = P.lv[l];
+    SL<E> s;
+    s.u = reinterpret_cast<E*>(sm + L.off_u);
+    s.f = reinterpret_cast<E*>(sm + L.off_f);
+    s.bx = reinterpret_cast<E*>(sm + L.off_bx);
+    s.by = reinterpret_cast<E*>(sm + L.off_by);
+    s.nx = L.nx;
+    s.ny = L.ny;
+    s.cx = E(L.cx);
+    s.cy = E(L.cy);
+    return s;
+}
+
+template <bool W>
+__device__ __forceinline__ int g_tid() { return W ? (int)(threadIdx.x & 31) : (int)threadIdx.x; }
+template <bool W>
+__device__ __forceinline__ int g_nthr() { return W ? 32 : (int)blockDim.x; }
+template <bool W>
+__device__ __forceinline__ void g_sync() {
+    if (W) __syncwarp(); else __syncthreads();
+}
+
+template <typename E>
+__device__ __forceinline__ void s_sums(const SL<E>& L, int i, int j, E& s, E& d) {
+    const int nx = L.nx, ny = L.ny;
+    const int ip = (i + 1 == nx) ? 0 : i + 1;
+    const int im = (i == 0) ? nx - 1 : i - 1;
+    const E aw = L.cx * L.bx[j * nx + i];
+    const E ae = L.cx * L.bx[j * nx + ip];
+    const E as = (j > 0) ? L.cy * L.by[j * nx + i] : E(0);
+    const E an = (j < ny - 1) ? L.cy * L.by[(j + 1) * nx + i] : (E(2) * L.cy) * L.by[ny * nx + i];
+    const E uw = L.u[j * nx + im], ue = L.u[j * nx + ip];
+    const E us = (j > 0) ? L.u[(j - 1) * nx + i] : E(0);
+    const E un = (j < ny - 1) ? L.u[(j + 1) * nx + i] : E(0);
+    E ss = aw * uw;
+    ss += ae * ue;
+    ss += as * us;
+    ss += an * un;
+    E dd = aw;
+    dd += ae;
+    dd += as;
+    dd += an;
+    s = ss;
+    d = dd;
+}
+
+template <typename E, bool W>
+__device__ void s_sweeps(const SL<E>& L, int nsw, bool reverse) {
+    const int half = L.nx >> 1, total = half * L.ny;
+    for (int q = 0; q < 2 * nsw; ++q) {
+        const int colour = reverse ? 1 - (q & 1) : (q & 1);
+        for (int k = g_tid<W>(); k < total; k += g_nthr<W>()) {
+            const int j = k / half, m = k - j * half;
+            const int i = 2 * m + ((j + colour) & 1);
+            E s, d;
+            s_sums(L, i, j, s, d);
+            L.u[j * L.nx + i] = (s - L.f[j * L.nx + i]) / d;
+        }
+        g_sync<W>();
+    }
+}
+
+template <typename E, typename EC, bool W>
+__device__ void s_restrict(const SL<E>& F, const SL<EC>& C) {
+    const int total = C.nx * C.ny;
+    for (int k = g_tid<W>(); k < total; k += g_nthr<W>()) {
+        const int J = k / C.nx, I = k - J * C.nx;
+        E r[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int i = 2 * I + (q & 1), j = 2 * J + (q >> 1);
+            E s, d;
+            s_sums(F, i, j, s, d);
+            r[q] = F.f[j * F.nx + i] - (s - d * F.u[j * F.nx + i]);
+        }
+        const E fc = E(0.25) * ((r[0] + r[1]) + (r[2] + r[3]));
+        C.f[k] = EC(fc);
+        C.u[k] = EC(0);
+    }
+    g_sync<W>();
+}
+
+template <typename E, typename EC, bool W>
+__device__ void s_prolong(const SL<EC>& C, const SL<E>& F) {
+    const int total = F.nx * F.ny;
+    for (int k = g_tid<W>(); k < total; k += g_nthr<W>()) {
+        const int j = k / F.nx, i = k - j * F.nx;
+        F.u[k] += E(C.u[(j >> 1) * C.nx + (i >> 1)]);
+    }
+    g_sync<W>();
+}
+
+// Dense Gaussian elimination of the bottom level (same order as the oracle).
+template <bool W>
+__device__ void s_dense(const SL<double>& L, double* A, double* b) {
+    const int nx = L.nx, ny = L.ny, n = nx * ny;
+    for (int k = g_tid<W>(); k < n * n; k += g_nthr<W>()) A[k] = 0.0;
+    for (int k = g_tid<W>(); k < n; k += g_nthr<W>()) b[k] = L.f[k];
+    g_sync<W>();
+    for (int row = g_tid<W>(); row < n; row += g_nthr<W>()) {
+        const int j = row / nx, i = row - j * nx;
+        const int ip = (i + 1 == nx) ? 0 : i + 1, im = (i == 0) ? nx - 1 : i - 1;
+        const double aw = L.cx * L.bx[j * nx + i];
+        const double ae = L.cx * L.bx[j * nx + ip];
+        const double as = (j > 0) ? L.cy * L.by[j * nx + i] : 0.0;
+        const double an = (j < ny - 1) ? L.cy * L.by[(j + 1) * nx + i] : (2.0 * L.cy) * L.by[ny * nx + i];
+        double d = aw;
+        d += ae;
+        d += as;
+        d += an;
+        A[row * n + row] -= d;
+        A[row * n + j * nx + im] += aw;
+        A[row * n + j * nx + ip] += ae;
+        if (j > 0) A[row * n + (j - 1) * nx + i] += as;
+        if (j < ny - 1) A[row * n + (j + 1) * nx + i] += an;
+    }
+    g_sync<W>();
+    for (int k = 0; k < n; ++k) {
+        const double piv = A[k * n + k];
+        const int m = n - k - 1;
+        for (int t = g_tid<W>(); t < m * (m + 1); t += g_nthr<W>()) {
+            const int i = k + 1 + t / (m + 1), c = t % (m + 1);
+            const double mult = A[i * n + k] / piv;
+            if (c < m) {
+                const int j = k + 1 + c;
+                A[i * n + j] -= mult * A[k * n + j];
+            } else {
+                b[i] -= mult * b[k];
+            }
+        }
+        g_sync<W>();
+    }
+    if (g_tid<W>() == 0) {
+        for (int i = n - 1; i >= 0; --i) {
+            double s = b[i];
+            for (int j = i + 1; j < n; ++j) s -= A[i * n + j] * L.u[j];
+            L.u[i] = s / A[i * n + i];
+        }
+    }
+    g_sync<W>();
+}
+
+// First level in [l0, bottom] small enough for warp 0 alone.
+__device__ __forceinline__ int first_small(const CtaParams& P, int l0) {
+    int l = l0;
+    while (l < P.bottom && P.lv[l].nx * P.lv[l].ny > kSmallCells) ++l;
+    return l;
+}
+
+// Down-and-up over FP64 levels [la, lb] by group W: sweeps + restriction going down to
+// lb (dense solve there when lb is the bottom) and prolongation + sweeps coming back.
+template <bool W>
+__device__ void s_inner_range_down(const CtaParams& P, unsigned char* sm, int la, int lb) {
+    for (int l = la; l < lb; ++l) {
+        const SL<double> L = make_sl<double>(P, sm, l);
+        const SL<double> C = make_sl<double>(P, sm, l + 1);
+        s_sweeps<double, W>(L, P.nu1, false);
+        s_restrict<double, double, W>(L, C);
+    }
+}
+template <bool W>
+__device__ void s_inner_range_up(const CtaParams& P, unsigned char* sm, int la, int lb) {
+    for (int l = lb - 1; l >= la; --l) {
+        const SL<double> L = make_sl<double>(P, sm, l);
+        const SL<double> C = make_sl<double>(P, sm, l + 1);
+        s_prolong<double, double, W>(C, L);
+        s_sweeps<double, W>(L, P.nu2, true);
+    }
+}
+
+// One inner V-cycle on the FP64 levels [l0, bottom] starting from the iterate in u(l0).
+// Levels above the first small level run block-wide, the rest in warp 0.
+__device__ void s_vcycle_inner(const CtaParams& P, unsigned char* sm, int l0) {
+    double* A = reinterpret_cast<double*>(sm + P.off_dense);
+    double* b = reinterpret_cast<double*>(sm + P.off_rhs);
+    const int ls = first_small(P, l0);
+    s_inner_range_down<false>(P, sm, l0, ls);
+    if (threadIdx.x < 32) {
+        s_inner_range_down<true>(P, sm, ls, P.bottom);
+        s_dense<true>(make_sl<double>(P, sm, P.bottom), A, b);
+        s_inner_range_up<true>(P, sm, ls, P.bottom);
+    }
+    __syncthreads();
+    s_inner_range_up<false>(P, sm, l0, ls);
+}
+
+// Levels [lcta, lc) in T, then the coarsest outer level lc (FP64): ncoarse inner
+// V-cycles from a zero iterate, or the dense solve when lc is the bottom level.
+template <typename T>
+__device__ void s_outer(const CtaParams& P, unsigned char* sm) {
+    for (int l = P.lcta; l < P.lc; ++l) {
+        const SL<T> L = make_sl<T>(P, sm, l);
+        s_sweeps<T, false>(L, P.nu1, false);
+        if (l + 1 == P.lc) s_restrict<T, double, false>(L, make_sl<double>(P, sm, l + 1));
+        else s_restrict<T, T, false>(L, make_sl<T>(P, sm, l + 1));
+    }
+    {
+        const SL<double> L = make_sl<double>(P, sm, P.lc);
+        for (int k = threadIdx.x; k < L.nx * L.ny; k += blockDim.x) L.u[k] = 0.0;
+        __syncthreads();
+        if (P.lc == P.bottom) {
+            if (threadIdx.x < 32)
+                s_dense<true>(L, reinterpret_cast<double*>(sm + P.off_dense), reinterpret_cast<double*>(sm + P.off_rhs));
+            __syncthreads();
+        } else {
+            for (int c = 0; c < P.ncoarse; ++c) s_vcycle_inner(P, sm, P.lc);
+        }
+    }
+    for (int l = P.lc - 1; l >= P.lcta; --l) {
+        const SL<T> L = make_sl<T>(P, sm, l);
+        if (l + 1 == P.lc) s_prolong<T, double, false>(make_sl<double>(P, sm, l + 1), L);
+        else s_prolong<T, T, false>(make_sl<T>(P, sm, l + 1), L);
+        s_sweeps<T, false>(L, P.nu2, true);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(NT_CTA, 1) k_cta(const __grid_constant__ CtaParams P) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    // stage beta of every level handled here, and f of the entry level
+    for (int l = P.lcta; l <= P.bottom; ++l) {
+        const CtaLevel& L = P.lv[l];
+        const int n = L.nx * L.ny, nb = L.nx * (L.ny + 1);
+        if (l < P.lc) {
+            T* bx = reinterpret_cast<T*>(sm + L.off_bx);
+            T* by = reinterpret_cast<T*>(sm + L.off_by);
+            const T* gbx = reinterpret_cast<const T*>(L.gbx);
+            const T* gby = reinterpret_cast<const T*>(L.gby);
+            for (int k = threadIdx.x; k < n; k += blockDim.x) bx[k] = gbx[k];
+            for (int k = threadIdx.x; k < nb; k += blockDim.x) by[k] = gby[k];
+        } else {
+            double* bx = reinterpret_cast<double*>(sm + L.off_bx);
+            double* by = reinterpret_cast<double*>(sm + L.off_by);
+            const double* gbx = reinterpret_cast<const double*>(L.gbx);
+            const double* gby = reinterpret_cast<const double*>(L.gby);
+            for (int k = threadIdx.x; k < n; k += blockDim.x) bx[k] = gbx[k];
+            for (int k = threadIdx.x; k < nb; k += blockDim.x) by[k] = gby[k];
+        }
+    }
+    {
+        const CtaLevel& L = P.lv[P.lcta];
+        const int n = L.nx * L.ny;
+        const T* fin = reinterpret_cast<const T*>(P.f_in);
+        if (P.lcta < P.lc) {
+            T* f = reinterpret_cast<T*>(sm + L.off_f);
+            T* u = reinterpret_cast<T*>(sm + L.off_u);
+            for (int k = threadIdx.x; k < n; k += blockDim.x) { f[k] = fin[k]; u[k] = T(0); }
+        } else {
+            double* f = reinterpret_cast<double*>(sm + L.off_f);
+            for (int k = threadIdx.x; k < n; k += blockDim.x) f[k] = double(fin[k]);
+        }
+    }
+    __syncthreads();
+    s_outer<T>(P, sm);
+    __syncthreads();
+    {
+        const CtaLevel& L = P.lv[P.lcta];
+        const int n = L.nx * L.ny;
+        T* uo = reinterpret_cast<T*>(P.u_out);
+        if (P.lcta < P.lc) {
+            const T* u = reinterpret_cast<const T*>(sm + L.off_u);
+            for (int k = threadIdx.x; k < n; k += blockDim.x) uo[k] = u[k];
+        } else {
+            const double* u = reinterpret_cast<const double*>(sm + L.off_u);
+            for (int k = threadIdx.x; k < n; k += blockDim.x) uo[k] = T(u[k]);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// set-up kernels
+// ------------------------------------------------------------------------------------
+template <typename T>
+__global__ void k_coarsen_beta(const T* __restrict__ bxf, const T* __restrict__ byf, T* __restrict__ bxc,
+                               T* __restrict__ byc, int nxc, int nyc) {
+    const int nxf = 2 * nxc;
+    const int n = nxc * nyc, nb = nxc * (nyc + 1);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n + nb; k += gridDim.x * blockDim.x) {
+        if (k < n) {
+            const int J = k / nxc, I = k - J * nxc;
+            bxc[k] = T(0.5) * (bxf[(size_t)(2 * J) * nxf + 2 * I] + bxf[(size_t)(2 * J + 1) * nxf + 2 * I]);
+        } else {
+            const int kk = k - n;
+            const int J = kk / nxc, I = kk - J * nxc;
+            byc[kk] = T(0.5) * (byf[(size_t)(2 * J) * nxf + 2 * I] + byf[(size_t)(2 * J) * nxf + 2 * I + 1]);
+        }
+    }
+}
+
+__global__ void k_to_float(const double* __restrict__ a, float* __restrict__ b, size_t n) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        b[k] = float(a[k]);
+}
+
+__global__ void k_widen(const float* __restrict__ a, double* __restrict__ b, size_t n) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        b[k] = double(a[k]);
+}
+
+// out = A u (FP64), the operator of the oracle's apply: out = s - d*u.
+__global__ void __launch_bounds__(NT) k_apply(double* __restrict__ out, const double* __restrict__ u,
+                                              const double* __restrict__ bx, const double* __restrict__ by, int nx,
+                                              int ny, double cx, double cy) {
+    constexpr int H = 1, RX = TX + 2, RY = TY + 2;
+    __shared__ double su[RX * RY];
+    __shared__ double sbx[(RX + 1) * RY];
+    __shared__ double sby[RX * (RY + 1)];
+    const int gi0 = blockIdx.x * TX - H, gj0 = blockIdx.y * TY - H;
+    load_region(su, RX, RY, u, nx, ny, gi0, gj0);
+    load_region(sbx, RX + 1, RY, bx, nx, ny, gi0, gj0);
+    load_region(sby, RX, RY + 1, by, nx, ny + 1, gi0, gj0);
+    __syncthreads();
+    for (int k = threadIdx.x; k < TX * TY; k += blockDim.x) {
+        const int ty = k / TX, tx = k - ty * TX;
+        const int sx = tx + H, sy = ty + H, j = gj0 + sy;
+        const Stencil<double> s = stencil(su, sbx, sby, RX, sx, sy, j, ny, cx, cy);
+        out[(size_t)j * nx + blockIdx.x * TX + tx] = s.s - s.d * su[sy * RX + sx];
+    }
+}
+
+__global__ void k_init_state(State* st, double tol, int max_it) {
+    st->tol = tol;
+    st->max_it = max_it;
+    st->it = 0;
+    st->status = LICA_NOT_CONVERGED;
+    st->cont = 0;
+    st->rz = 0.0;
+    st->alpha = 0.0;
+    st->beta = 0.0;
+    st->rel = 0.0;
+    st->sums[0] = st->sums[1] = 0.0;
+    for (int k = 0; k < 4; ++k) st->cnt[k] = 0u;
+}
+
+__global__ void k_zero(double* __restrict__ a, size_t n) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        a[k] = 0.0;
+}
+
+// The oracle's mixed path takes r.z with the FP32 copy of r (the V-cycle input), so the
+// CG r.z partial of k_up<float,...,true> uses f (FP32) and z (FP32) -- the same values.
+
+}  // namespace mg
+}  // namespace lica
+
+using namespace lica;
+using namespace lica::mg;
+
+// ------------------------------------------------------------------------------------
+// host context
+// ------------------------------------------------------------------------------------
+struct LevelBuf {
+    int nx = 0, ny = 0;
+    double cx = 0, cy = 0;
+    void* u = nullptr;      // T
+    void* f = nullptr;      // T
+    double* bx64 = nullptr;  // FP64 beta chain (level 0: the caller's arrays)
+    double* by64 = nullptr;
+    float* bx32 = nullptr;   // FP32 beta chain (mixed)
+    float* by32 = nullptr;
+};
+
+struct lica_mg {
+    int nx, ny;
+    double hx, hy;
+    lica_mg_options o;
+    int nouter = 0, lcta = 0, bottom = 0;
+    std::vector<LevelBuf> lv;  // outer levels then inner levels
+    size_t cta_smem = 0;
+    CtaParams cp{};
+    // level-0 CG vectors
+    double* pcg = nullptr;   // p
+    void* r = nullptr;       // r (T): the V-cycle's level-0 f
+    void* z = nullptr;       // z (T): the V-cycle's level-0 u
+    double* partials = nullptr;
+    State* st = nullptr;
+    State* st_host = nullptr;  // pinned
+    // host staging for lica_mg_solve_host
+    double *d_p = nullptr, *d_f = nullptr, *d_bx = nullptr, *d_by = nullptr;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t cap_stream = nullptr;  // graphs are captured here, launched on the caller's stream
+    // graph cache
+    cudaGraphExec_t gexec = nullptr;
+    const void* gkey[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaStream_t gstream = nullptr;
+    double gtol = -1.0;
+    int gmax = -1;
+    int body_nodes = 0, setup_nodes = 0;
+    // optional per-kernel-class timing (non-graph solves only)
+    bool profile = false;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pending;
+    double prof_ms[LICA_MG_NCLASS] = {0};
+    int64_t prof_n[LICA_MG_NCLASS] = {0};
+    std::vector<cudaEvent_t> event_pool;
+};
+
+namespace {
+
+bool is_mixed(const lica_mg* m) { return m->o.precision == 1; }
+
+// Profiling: bracket one kernel launch with events when profiling is on.
+cudaEvent_t pool_event(lica_mg* m) {
+    if (!m->event_pool.empty()) {
+        cudaEvent_t e = m->event_pool.back();
+        m->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+struct ProfScope {
+    lica_mg* m;
+    int cls;
+    cudaStream_t s;
+    cudaEvent_t a = nullptr, b = nullptr;
+    ProfScope(lica_mg* m_, int cls_, cudaStream_t s_) : m(m_), cls(cls_), s(s_) {
+        if (m->profile) {
+            a = pool_event(m);
+            b = pool_event(m);
+            cudaEventRecord(a, s);
+        }
+    }
+    ~ProfScope() {
+        if (m->profile) {
+            cudaEventRecord(b, s);
+            m->prof_pending.push_back({cls, {a, b}});
+        }
+    }
+};
+void prof_collect(lica_mg* m) {
+    for (auto& pe : m->prof_pending) {
+        float ms = 0.f;
+        cudaEventSynchronize(pe.second.second);
+        cudaEventElapsedTime(&ms, pe.second.first, pe.second.second);
+        m->prof_ms[pe.first] += ms;
+        m->prof_n[pe.first] += 1;
+        m->event_pool.push_back(pe.second.first);
+        m->event_pool.push_back(pe.second.second);
+    }
+    m->prof_pending.clear();
+}
+
+template <typename T, int NSW>
+size_t grid_smem(bool down) {
+    const int H = down ? 2 * NSW + 1 : 2 * NSW;
+    const int RX = TX + 2 * H, RY = TY + 2 * H;
+    return sizeof(T) * (size_t)(2 * RX * RY + (RX + 1) * RY + RX * (RY + 1));
+}
+
+template <typename T>
+int set_smem_attrs(int nsw) {
+    // the kernels are instantiated for NSW = 1, 2, 3
+#define LICA_SET(NS)                                                                                            \
+    LICA_CUDA_TRY(cudaFuncSetAttribute(k_down<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,              \
+                                       (int)grid_smem<T, NS>(true)));                                          \
+    LICA_CUDA_TRY(cudaFuncSetAttribute(k_up<T, NS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
+                                       (int)grid_smem<T, NS>(false)));                                         \
+    LICA_CUDA_TRY(cudaFuncSetAttribute(k_up<T, NS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,          \
+                                       (int)grid_smem<T, NS>(false)));
+    if (nsw == 1) { LICA_SET(1) }
+    else if (nsw == 2) { LICA_SET(2) }
+    else { LICA_SET(3) }
+#undef LICA_SET
+    return LICA_OK;
+}
+
+template <typename T>
+int launch_down(lica_mg* m, int l, cudaStream_t s) {
+    LevelBuf& L = m->lv[l];
+    LevelBuf& C = m->lv[l + 1];
+    const T* bx = std::is_same<T, float>::value ? (const T*)L.bx32 : (const T*)L.bx64;
+    const T* by = std::is_same<T, float>::value ? (const T*)L.by32 : (const T*)L.by64;
+    dim3 grid(L.nx / TX, L.ny / TY);
+    const T* f = (const T*)L.f;
+    T* u = (T*)L.u;
+    T* fc = (T*)C.f;
+    const T cx = T(L.cx), cy = T(L.cy);
+    ProfScope ps(m, l == 0 ? LICA_MG_DOWN0 : LICA_MG_DOWN, s);
+    switch (m->o.nu1) {
+        case 1: k_down<T, 1><<<grid, NT, grid_smem<T, 1>(true), s>>>(f, bx, by, u, fc, L.nx, L.ny, cx, cy); break;
+        case 2: k_down<T, 2><<<grid, NT, grid_smem<T, 2>(true), s>>>(f, bx, by, u, fc, L.nx, L.ny, cx, cy); break;
+        default: k_down<T, 3><<<grid, NT, grid_smem<T, 3>(true), s>>>(f, bx, by, u, fc, L.nx, L.ny, cx, cy); break;
+    }
+    LICA_CUDA_TRY(cudaGetLastError());
+    lica_count_launches(1);
+    return LICA_OK;
+}
+
+template <typename T>
+int launch_up(lica_mg* m, int l, cudaStream_t s) {
+    LevelBuf& L = m->lv[l];
+    LevelBuf& C = m->lv[l + 1];
+    const T* bx = std::is_same<T, float>::value ? (const T*)L.bx32 : (const T*)L.bx64;
+    const T* by = std::is_same<T, float>::value ? (const T*)L.by32 : (const T*)L.by64;
+    dim3 grid(L.nx / TX, L.ny / TY);
+    T* u = (T*)L.u;
+    const T* uc = (const T*)C.u;
+    const T* f = (const T*)L.f;
+    const T cx = T(L.cx), cy = T(L.cy);
+    ProfScope ps(m, l == 0 ? LICA_MG_UP0 : LICA_MG_UP, s);
+#define LICA_UP(NS)                                                                                               \
+    if (l == 0)                                                                                                   \
+        k_up<T, NS, true><<<grid, NT, grid_smem<T, NS>(false), s>>>(u, uc, f, bx, by, L.nx, L.ny, cx, cy, m->st,  \
+                                                                    m->partials);                                 \
+    else                                                                                                          \
+        k_up<T, NS, false><<<grid, NT, grid_smem<T, NS>(false), s>>>(u, uc, f, bx, by, L.nx, L.ny, cx, cy, m->st, \
+                                                                     m->partials);
+    switch (m->o.nu2) {
+        case 1: LICA_UP(1) break;
+        case 2: LICA_UP(2) break;
+        default: LICA_UP(3) break;
+    }
+#undef LICA_UP
+    LICA_CUDA_TRY(cudaGetLastError());
+    lica_count_launches(1);
+    return LICA_OK;
+}
+
+template <typename T>
+int launch_cta(lica_mg* m, cudaStream_t s) {
+    CtaParams P = m->cp;
+    P.f_in = m->lv[m->lcta].f;
+    P.u_out = m->lv[m->lcta].u;
+    ProfScope ps(m, LICA_MG_CTA, s);
+    k_cta<T><<<1, NT_CTA, m->cta_smem, s>>>(P);
+    LICA_CUDA_TRY(cudaGetLastError());
+    lica_count_launches(1);
+    return LICA_OK;
+}
+
+// z = M r on the level-0 buffers m->r (input) and m->z (output).
+template <typename T>
+int vcycle(lica_mg* m, cudaStream_t s) {
+    int st;
+    for (int l = 0; l < m->lcta; ++l)
+        if ((st = launch_down<T>(m, l, s))) return st;
+    if ((st = launch_cta<T>(m, s))) return st;
+    for (int l = m->lcta - 1; l >= 0; --l)
+        if ((st = launch_up<T>(m, l, s))) return st;
+    return LICA_OK;
+}
+
+int run_vcycle(lica_mg* m, cudaStream_t s) { return is_mixed(m) ? vcycle<float>(m, s) : vcycle<double>(m, s); }
+
+// Set up the beta hierarchy for caller arrays bx, by (level 0).
+int setup_beta(lica_mg* m, const double* bx, const double* by, cudaStream_t s) {
+    ProfScope ps(m, LICA_MG_SETUP, s);
+    m->lv[0].bx64 = const_cast<double*>(bx);
+    m->lv[0].by64 = const_cast<double*>(by);
+    const int nlev = (int)m->lv.size();
+    for (int l = 1; l < nlev; ++l) {
+        LevelBuf& F = m->lv[l - 1];
+        LevelBuf& C = m->lv[l];
+        const int work = C.nx * C.ny + C.nx * (C.ny + 1);
+        const int blocks = std::min(1184, (work + 255) / 256);
+        k_coarsen_beta<double><<<blocks, 256, 0, s>>>(F.bx64, F.by64, C.bx64, C.by64, C.nx, C.ny);
+        LICA_CUDA_TRY(cudaGetLastError());
+        lica_count_launches(1);
+    }
+    if (is_mixed(m)) {
+        LevelBuf& L0 = m->lv[0];
+        const size_t n = (size_t)L0.nx * L0.ny;
+        k_to_float<<<1184, 256, 0, s>>>(bx, L0.bx32, n);
+        k_to_float<<<1184, 256, 0, s>>>(by, L0.by32, n + L0.nx);
+        LICA_CUDA_TRY(cudaGetLastError());
+        lica_count_launches(2);
+        for (int l = 1; l < m->nouter - 1; ++l) {
+            LevelBuf& F = m->lv[l - 1];
+            LevelBuf& C = m->lv[l];
+            const int work = C.nx * C.ny + C.nx * (C.ny + 1);
+            const int blocks = std::min(1184, (work + 255) / 256);
+            k_coarsen_beta<float><<<blocks, 256, 0, s>>>(F.bx32, F.by32, C.bx32, C.by32, C.nx, C.ny);
+            LICA_CUDA_TRY(cudaGetLastError());
+            lica_count_launches(1);
+        }
+    }
+    // beta pointers of the levels staged by the single-CTA kernel
+    for (int l = m->lcta; l <= m->bottom; ++l) {
+        if (l < m->nouter - 1 && is_mixed(m)) {
+            m->cp.lv[l].gbx = m->lv[l].bx32;
+            m->cp.lv[l].gby = m->lv[l].by32;
+        } else {
+            m->cp.lv[l].gbx = m->lv[l].bx64;
+            m->cp.lv[l].gby = m->lv[l].by64;
+        }
+    }
+    return LICA_OK;
+}
+
+template <typename TR>
+int launch_xupdate(lica_mg* m, double* x, const double* f, int first, cudaGraphConditionalHandle h, int use_cond,
+                   cudaStream_t s) {
+    LevelBuf& L = m->lv[0];
+    dim3 grid(L.nx / TX, L.ny / TY);
+    ProfScope ps(m, LICA_MG_XUPDATE, s);
+    k_xupdate<TR><<<grid, NT, 0, s>>>(x, m->pcg, f, L.bx64, L.by64, (TR*)m->r, L.nx, L.ny, L.cx, L.cy, m->st,
+                                      m->partials, first, h, use_cond);
+    LICA_CUDA_TRY(cudaGetLastError());
+    lica_count_launches(1);
+    return LICA_OK;
+}
+
+template <typename TZ>
+int launch_pupdate(lica_mg* m, cudaStream_t s) {
+    LevelBuf& L = m->lv[0];
+    dim3 grid(L.nx / TX, L.ny / TY);
+    ProfScope ps(m, LICA_MG_PUPDATE, s);
+    k_pupdate<TZ><<<grid, NT, 0, s>>>(m->pcg, (const TZ*)m->z, L.bx64, L.by64, L.nx, L.ny, L.cx, L.cy, m->st,
+                                      m->partials);
+    LICA_CUDA_TRY(cudaGetLastError());
+    lica_count_launches(1);
+    return LICA_OK;
+}
+
+// Set-up part of a solve: state, beta hierarchy, p = 0, r = f - A x, ||f||, rel.
+int enqueue_setup(lica_mg* m, double* x, const double* f, const double* bx, const double* by, double rtol,
+                  int max_it, cudaGraphConditionalHandle h, int use_cond, cudaStream_t s) {
+    int st;
+    k_init_state<<<1, 1, 0, s>>>(m->st, rtol, max_it);
+    LICA_CUDA_TRY(cudaGetLastError());
+    const size_t n = (size_t)m->nx * m->ny;
+    k_zero<<<1184, 256, 0, s>>>(m->pcg, n);
+    LICA_CUDA_TRY(cudaGetLastError());
+    lica_count_launches(2);
+    if ((st = setup_beta(m, bx, by, s))) return st;
+    return is_mixed(m) ? launch_xupdate<float>(m, x, f, 1, h, use_cond, s)
+                       : launch_xupdate<double>(m, x, f, 1, h, use_cond, s);
+}
+
+// One PCG iteration: z = M r; beta; p = z + beta p; alpha; x += alpha p; r = f - A x.
+int enqueue_iteration(lica_mg* m, double* x, const double* f, cudaGraphConditionalHandle h, int use_cond,
+                      cudaStream_t s) {
+    int st;
+    m->lv[0].u = m->z;
+    m->lv[0].f = m->r;
+    if ((st = run_vcycle(m, s))) return st;
+    if (is_mixed(m)) {
+        if ((st = launch_pupdate<float>(m, s))) return st;
+        return launch_xupdate<float>(m, x, f, 0, h, use_cond, s);
+    }
+    if ((st = launch_pupdate<double>(m, s))) return st;
+    return launch_xupdate<double>(m, x, f, 0, h, use_cond, s);
+}
+
+int read_state(lica_mg* m, cudaStream_t s) {
+    LICA_CUDA_TRY(cudaMemcpyAsync(m->st_host, m->st, sizeof(State), cudaMemcpyDeviceToHost, s));
+    LICA_CUDA_TRY(cudaStreamSynchronize(s));
+    return LICA_OK;
+}
+
+int build_graph(lica_mg* m, double* x, const double* f, const double* bx, const double* by, double rtol,
+                int max_it, cudaStream_t launch_stream) {
+    (void)launch_stream;
+    if (!m->cap_stream) LICA_CUDA_TRY(cudaStreamCreateWithFlags(&m->cap_stream, cudaStreamNonBlocking));
+    cudaStream_t s = m->cap_stream;
+    const bool prof = m->profile;
+    m->profile = false;
+    struct Restore {
+        lica_mg* m;
+        bool p;
+        ~Restore() { m->profile = p; }
+    } restore{m, prof};
+    if (m->gexec) {
+        cudaGraphExecDestroy(m->gexec);
+        m->gexec = nullptr;
+    }
+    cudaGraph_t g;
+    LICA_CUDA_TRY(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    LICA_CUDA_TRY(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+    // set-up part, captured into g
+    int64_t before = lica_kernel_launch_count();
+    LICA_CUDA_TRY(cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    int st = enqueue_setup(m, x, f, bx, by, rtol, max_it, h, 1, s);
+    cudaGraph_t captured = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &captured);
+    if (st) { cudaGraphDestroy(g); return st; }
+    LICA_CUDA_TRY(e);
+    m->setup_nodes = (int)(lica_kernel_launch_count() - before);
+    // conditional WHILE node after the set-up nodes
+    size_t nleaf = 0;
+    LICA_CUDA_TRY(cudaGraphGetNodes(g, nullptr, &nleaf));
+    std::vector<cudaGraphNode_t> nodes(nleaf);
+    LICA_CUDA_TRY(cudaGraphGetNodes(g, nodes.data(), &nleaf));
+    // the set-up was captured on one stream: its sink is the last node added
+    std::vector<cudaGraphNode_t> sinks;
+    for (auto nd : nodes) {
+        size_t nout = 0;
+        LICA_CUDA_TRY(cudaGraphNodeGetDependentNodes(nd, nullptr, &nout));
+        if (nout == 0) sinks.push_back(nd);
+    }
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    LICA_CUDA_TRY(cudaGraphAddNode(&wnode, g, sinks.data(), sinks.size(), &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    before = lica_kernel_launch_count();
+    LICA_CUDA_TRY(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    st = enqueue_iteration(m, x, f, h, 1, s);
+    e = cudaStreamEndCapture(s, &captured);
+    if (st) { cudaGraphDestroy(g); return st; }
+    LICA_CUDA_TRY(e);
+    m->body_nodes = (int)(lica_kernel_launch_count() - before);
+    // the captures counted as launches; undo that (replays are counted per run)
+    lica_count_launches(-(int64_t)(m->setup_nodes + m->body_nodes));
+    e = cudaGraphInstantiate(&m->gexec, g, 0);
+    cudaGraphDestroy(g);
+    LICA_CUDA_TRY(e);
+    m->gkey[0] = x; m->gkey[1] = f; m->gkey[2] = bx; m->gkey[3] = by;
+    m->gstream = launch_stream;
+    return LICA_OK;
+}
+
+int solve_impl(lica_mg* m, double* x, const double* f, const double* bx, const double* by, double rtol, int max_it,
+               lica_mg_result* res, cudaStream_t s) {
+    if (!m || !x || !f || !bx || !by || !(rtol >= 0.0) || max_it < 0) return LICA_BAD_ARG;
+    int st;
+    if (m->o.use_graph && !m->profile) {
+        const bool same = m->gexec && m->gkey[0] == x && m->gkey[1] == f && m->gkey[2] == bx && m->gkey[3] == by &&
+                          m->gstream == s;
+        // rtol/max_it live in the graph's k_init_state node: rebuild when they change
+        if (!same || m->gtol != rtol || m->gmax != max_it) {
+            if ((st = build_graph(m, x, f, bx, by, rtol, max_it, s))) return st;
+            m->gtol = rtol;
+            m->gmax = max_it;
+        }
+        LICA_CUDA_TRY(cudaGraphLaunch(m->gexec, s));
+        if ((st = read_state(m, s))) return st;
+        lica_count_launches(m->setup_nodes + (int64_t)m->st_host->it * m->body_nodes);
+    } else {
+        cudaGraphConditionalHandle h{};
+        if ((st = enqueue_setup(m, x, f, bx, by, rtol, max_it, h, 0, s))) return st;
+        if ((st = read_state(m, s))) return st;
+        while (m->st_host->cont) {
+            if ((st = enqueue_iteration(m, x, f, h, 0, s))) return st;
+            if ((st = read_state(m, s))) return st;
+        }
+        if (m->profile) prof_collect(m);
+    }
+    if (res) {
+        res->iterations = m->st_host->it;
+        res->status = m->st_host->status;
+        res->rel_residual = m->st_host->rel;
+    }
+    return m->st_host->status;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------
+extern "C" {
+
+int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, const lica_mg_options* opt) {
+    if (!out || !opt) return LICA_BAD_ARG;
+    *out = nullptr;
+    const lica_mg_options o = *opt;
+    if (nx < TX || ny < TY || nx % TX || ny % TY || !(hx > 0) || !(hy > 0) || o.nlevels < 2 ||
+        o.nlevels > 12 || o.nu1 < 1 || o.nu1 > 3 || o.nu2 < 1 || o.nu2 > 3 || o.ncoarse < 1 ||
+        (o.precision != 0 && o.precision != 1)) {
+        lica_set_last_error("lica_mg_create", "unsupported sizes or options", __FILE__, __LINE__);
+        return LICA_BAD_ARG;
+    }
+    lica_mg* m = new lica_mg();
+    m->nx = nx; m->ny = ny; m->hx = hx; m->hy = hy; m->o = o;
+    // outer levels
+    int cx = nx, cy = ny;
+    double chx = hx, chy = hy;
+    for (int l = 0; l < o.nlevels; ++l) {
+        if (l > 0) {
+            if ((cx & 1) || (cy & 1) || cx < 4 || cy < 2) { delete m; return LICA_BAD_ARG; }
+            cx /= 2; cy /= 2; chx *= 2; chy *= 2;
+        }
+        LevelBuf L;
+        L.nx = cx; L.ny = cy; L.cx = 1.0 / (chx * chx); L.cy = 1.0 / (chy * chy);
+        m->lv.push_back(L);
+    }
+    m->nouter = o.nlevels;
+    while (!(cx & 1) && !(cy & 1) && cx / 2 >= 2 && cy / 2 >= 2) {
+        cx /= 2; cy /= 2; chx *= 2; chy *= 2;
+        LevelBuf L;
+        L.nx = cx; L.ny = cy; L.cx = 1.0 / (chx * chx); L.cy = 1.0 / (chy * chy);
+        m->lv.push_back(L);
+    }
+    m->bottom = (int)m->lv.size() - 1;
+    if (m->lv[m->bottom].nx * m->lv[m->bottom].ny > kMaxDense || (int)m->lv.size() > kMaxLevels) {
+        delete m;
+        lica_set_last_error("lica_mg_create", "coarsest level too large for the dense solve", __FILE__, __LINE__);
+        return LICA_BAD_ARG;
+    }
+    const bool mixed = o.precision == 1;
+    const size_t tsz = mixed ? sizeof(float) : sizeof(double);
+    // single-CTA levels: from the first level >= 1 whose remaining hierarchy fits in
+    // shared memory and has <= 64*64 cells, or that cannot be tiled
+    auto cta_bytes = [&](int from) {
+        size_t b = 0;
+        for (int l = from; l <= m->bottom; ++l) {
+            const size_t e = (l < m->nouter - 1) ? tsz : sizeof(double);
+            const size_t n = (size_t)m->lv[l].nx * m->lv[l].ny;
+            b += e * (3 * n + n + m->lv[l].nx);
+            b = (b + 15) & ~(size_t)15;
+        }
+        const size_t nb = (size_t)m->lv[m->bottom].nx * m->lv[m->bottom].ny;
+        b += sizeof(double) * (nb * nb + nb);
+        return b;
+    };
+    int lcta = m->nouter - 1;
+    for (int l = 1; l < m->nouter; ++l) {
+        const bool tileable = m->lv[l].nx % TX == 0 && m->lv[l].ny % TY == 0;
+        const size_t n = (size_t)m->lv[l].nx * m->lv[l].ny;
+        if (!tileable || (n <= 64 * 64 && cta_bytes(l) <= 200 * 1024)) { lcta = l; break; }
+    }
+    if (cta_bytes(lcta) > 220 * 1024) {
+        delete m;
+        lica_set_last_error("lica_mg_create", "coarse levels do not fit in shared memory; use more levels",
+                            __FILE__, __LINE__);
+        return LICA_BAD_ARG;
+    }
+    for (int l = 0; l < lcta; ++l) {
+        if (m->lv[l].nx % TX || m->lv[l].ny % TY) { delete m; return LICA_BAD_ARG; }
+    }
+    m->lcta = lcta;
+    // shared-memory layout of the single-CTA kernel
+    CtaParams& P = m->cp;
+    std::memset(&P, 0, sizeof(P));
+    P.lcta = lcta; P.lc = m->nouter - 1; P.bottom = m->bottom;
+    P.nu1 = o.nu1; P.nu2 = o.nu2; P.ncoarse = o.ncoarse;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t r = off; off = (off + bytes + 15) & ~(size_t)15; return (unsigned)r; };
+    for (int l = lcta; l <= m->bottom; ++l) {
+        const size_t e = (l < m->nouter - 1) ? tsz : sizeof(double);
+        const size_t n = (size_t)m->lv[l].nx * m->lv[l].ny;
+        CtaLevel& C = P.lv[l];
+        C.nx = m->lv[l].nx; C.ny = m->lv[l].ny; C.cx = m->lv[l].cx; C.cy = m->lv[l].cy;
+        C.off_u = take(e * n);
+        C.off_f = take(e * n);
+        C.off_bx = take(e * n);
+        C.off_by = take(e * (n + m->lv[l].nx));
+    }
+    const size_t nb = (size_t)m->lv[m->bottom].nx * m->lv[m->bottom].ny;
+    P.off_dense = take(sizeof(double) * nb * nb);
+    P.off_rhs = take(sizeof(double) * nb);
+    m->cta_smem = off;
+
+    auto fail = [&](int code) { lica_mg_destroy(m); return code; };
+#define TRY_ALLOC(ptr, bytes)                                                        \
+    do {                                                                             \
+        cudaError_t _e = cudaMalloc((void**)&(ptr), (bytes));                        \
+        if (_e != cudaSuccess) {                                                     \
+            lica_set_last_error("cudaMalloc", cudaGetErrorString(_e), __FILE__, __LINE__); \
+            return fail(LICA_ERR_NOMEM);                                             \
+        }                                                                            \
+    } while (0)
+    const size_t n0 = (size_t)nx * ny;
+    TRY_ALLOC(m->pcg, sizeof(double) * n0);
+    TRY_ALLOC(m->r, tsz * n0);
+    TRY_ALLOC(m->z, tsz * n0);
+    for (int l = 1; l <= m->bottom; ++l) {
+        LevelBuf& L = m->lv[l];
+        const size_t n = (size_t)L.nx * L.ny;
+        if (l <= lcta) {
+            TRY_ALLOC(L.u, tsz * n);
+            TRY_ALLOC(L.f, tsz * n);
+        }
+        TRY_ALLOC(L.bx64, sizeof(double) * n);
+        TRY_ALLOC(L.by64, sizeof(double) * (n + L.nx));
+    }
+    if (mixed) {
+        for (int l = 0; l < m->nouter - 1; ++l) {
+            LevelBuf& L = m->lv[l];
+            const size_t n = (size_t)L.nx * L.ny;
+            TRY_ALLOC(L.bx32, sizeof(float) * n);
+            TRY_ALLOC(L.by32, sizeof(float) * (n + L.nx));
+        }
+    }
+    const size_t ntiles = (size_t)(nx / TX) * (ny / TY);
+    TRY_ALLOC(m->partials, sizeof(double) * 2 * ntiles);
+    TRY_ALLOC(m->st, sizeof(State));
+    {
+        cudaError_t e = cudaMallocHost((void**)&m->st_host, sizeof(State));
+        if (e != cudaSuccess) return fail(LICA_ERR_NOMEM);
+    }
+#undef TRY_ALLOC
+    int st = mixed ? set_smem_attrs<float>(o.nu1) : set_smem_attrs<double>(o.nu1);
+    if (!st && o.nu2 != o.nu1) st = mixed ? set_smem_attrs<float>(o.nu2) : set_smem_attrs<double>(o.nu2);
+    if (st) return fail(st);
+    cudaError_t e = mixed ? cudaFuncSetAttribute(k_cta<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)m->cta_smem)
+                          : cudaFuncSetAttribute(k_cta<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)m->cta_smem);
+    if (e != cudaSuccess) {
+        lica_set_last_error("cudaFuncSetAttribute(k_cta)", cudaGetErrorString(e), __FILE__, __LINE__);
+        return fail(LICA_ERR_CUDA);
+    }
+    *out = m;
+    return LICA_OK;
+}
+
+int lica_mg_destroy(lica_mg* m) {
+    if (!m) return LICA_OK;
+    if (m->gexec) cudaGraphExecDestroy(m->gexec);
+    for (auto& pe : m->prof_pending) {
+        cudaEventDestroy(pe.second.first);
+        cudaEventDestroy(pe.second.second);
+    }
+    for (auto e : m->event_pool) cudaEventDestroy(e);
+    for (size_t l = 1; l < m->lv.size(); ++l) {
+        cudaFree(m->lv[l].u);
+        cudaFree(m->lv[l].f);
+        cudaFree(m->lv[l].bx64);
+        cudaFree(m->lv[l].by64);
+    }
+    for (auto& L : m->lv) {
+        cudaFree(L.bx32);
+        cudaFree(L.by32);
+    }
+    cudaFree(m->pcg);
+    cudaFree(m->r);
+    cudaFree(m->z);
+    cudaFree(m->partials);
+    cudaFree(m->st);
+    if (m->st_host) cudaFreeHost(m->st_host);
+    cudaFree(m->d_p);
+    cudaFree(m->d_f);
+    cudaFree(m->d_bx);
+    cudaFree(m->d_by);
+    if (m->own_stream) cudaStreamDestroy(m->own_stream);
+    if (m->cap_stream) cudaStreamDestroy(m->cap_stream);
+    delete m;
+    return LICA_OK;
+}
+
+int lica_mg_solve_device(lica_mg* m, double* p, const double* f, const double* bx, const double* by, double rtol,
+                         int32_t max_iters, lica_mg_result* res, void* stream) {
+    return solve_impl(m, p, f, bx, by, rtol, max_iters, res, (cudaStream_t)stream);
+}
+
+int lica_mg_solve_host(lica_mg* m, double* p, const double* f, const double* bx, const double* by, double rtol,
+                       int32_t max_iters, lica_mg_result* res, void* stream) {
+    if (!m || !p || !f || !bx || !by) return LICA_BAD_ARG;
+    const size_t n = (size_t)m->nx * m->ny, nb = n + m->nx;
+    if (!stream && !m->own_stream) LICA_CUDA_TRY(cudaStreamCreateWithFlags(&m->own_stream, cudaStreamNonBlocking));
+    if (!m->d_p) {
+        LICA_CUDA_TRY(cudaMalloc((void**)&m->d_p, sizeof(double) * n));
+        LICA_CUDA_TRY(cudaMalloc((void**)&m->d_f, sizeof(double) * n));
+        LICA_CUDA_TRY(cudaMalloc((void**)&m->d_bx, sizeof(double) * n));
+        LICA_CUDA_TRY(cudaMalloc((void**)&m->d_by, sizeof(double) * nb));
+    }
+    cudaStream_t s = stream ? (cudaStream_t)stream : m->own_stream;
+    LICA_CUDA_TRY(cudaMemcpyAsync(m->d_p, p, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    LICA_CUDA_TRY(cudaMemcpyAsync(m->d_f, f, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    LICA_CUDA_TRY(cudaMemcpyAsync(m->d_bx, bx, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    LICA_CUDA_TRY(cudaMemcpyAsync(m->d_by, by, sizeof(double) * nb, cudaMemcpyHostToDevice, s));
+    int st = solve_impl(m, m->d_p, m->d_f, m->d_bx, m->d_by, rtol, max_iters, res, s);
+    if (st == LICA_ERR_CUDA || st == LICA_BAD_ARG) return st;
+    LICA_CUDA_TRY(cudaMemcpyAsync(p, m->d_p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    LICA_CUDA_TRY(cudaStreamSynchronize(s));
+    return st;
+}
+
+int lica_mg_precond_device(lica_mg* m, double* z, const double* r, const double* bx, const double* by,
+                           void* stream) {
+    if (!m || !z || !r || !bx || !by) return LICA_BAD_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    int st;
+    if ((st = setup_beta(m, bx, by, s))) return st;
+    const size_t n = (size_t)m->nx * m->ny;
+    m->lv[0].u = m->z;
+    m->lv[0].f = m->r;
+    k_init_state<<<1, 1, 0, s>>>(m->st, 0.0, 0);
+    LICA_CUDA_TRY(cudaGetLastError());
+    lica_count_launches(1);
+    if (is_mixed(m)) {
+        k_to_float<<<1184, 256, 0, s>>>(r, (float*)m->r, n);
+        LICA_CUDA_TRY(cudaGetLastError());
+        lica_count_launches(1);
+        if ((st = vcycle<float>(m, s))) return st;
+        k_widen<<<1184, 256, 0, s>>>((const float*)m->z, z, n);
+        LICA_CUDA_TRY(cudaGetLastError());
+        lica_count_launches(1);
+    } else {
+        LICA_CUDA_TRY(cudaMemcpyAsync(m->r, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        if ((st = vcycle<double>(m, s))) return st;
+        LICA_CUDA_TRY(cudaMemcpyAsync(z, m->z, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    }
+    LICA_CUDA_TRY(cudaStreamSynchronize(s));
+    return LICA_OK;
+}
+
+int lica_mg_profile(lica_mg* m, int32_t enable) {
+    if (!m) return LICA_BAD_ARG;
+    m->profile = enable != 0;
+    for (int k = 0; k < LICA_MG_NCLASS; ++k) {
+        m->prof_ms[k] = 0.0;
+        m->prof_n[k] = 0;
+    }
+    return LICA_OK;
+}
+
+int lica_mg_profile_read(lica_mg* m, int32_t kernel_class, double* total_ms, int64_t* launches) {
+    if (!m || kernel_class < 0 || kernel_class >= LICA_MG_NCLASS || !total_ms || !launches) return LICA_BAD_ARG;
+    *total_ms = m->prof_ms[kernel_class];
+    *launches = m->prof_n[kernel_class];
+    return LICA_OK;
+}
+
+int lica_mg_apply_device(lica_mg* m, double* out, const double* u, const double* bx, const double* by,
+                         void* stream) {
+    if (!m || !out || !u || !bx || !by) return LICA_BAD_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const LevelBuf& L = m->lv[0];
+    k_apply<<<dim3(L.nx / TX, L.ny / TY), NT, 0, s>>>(out, u, bx, by, L.nx, L.ny, L.cx, L.cy);
+    LICA_CUDA_TRY(cudaGetLastError());
+    lica_count_launches(1);
+    LICA_CUDA_TRY(cudaStreamSynchronize(s));
+    return LICA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,86 @@
+"""ctypes binding of the C ABI in include/lica_gpu.h (liblica_gpu.so, built in-tree).
+
+There is no CPU fallback: if the library is missing this module raises at import, and
+every entry point runs CUDA kernels.
+"""
+import ctypes as C
+import os
+
+from . import build as _build
+
+_D = C.POINTER(C.c_double)
+_I64 = C.POINTER(C.c_int64)
+
+
+class MgOptions(C.Structure):
+    _fields_ = [("nlevels", C.c_int32), ("nu1", C.c_int32), ("nu2", C.c_int32), ("ncoarse", C.c_int32),
+                ("precision", C.c_int32), ("use_graph", C.c_int32)]
+
+
+class MgResult(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("status", C.c_int32), ("rel_residual", C.c_double)]
+
+
+# every symbol include/lica_gpu.h declares, with its ctypes signature
+SIGNATURES = {
+    "lica_last_error": (C.c_char_p, []),
+    "lica_kernel_launch_count": (C.c_int64, []),
+    "lica_gpu_trdiag3": (C.c_int, [_D, _D, _D, _D, _D] + [C.c_int64] * 5),
+    "lica_gpu_trdiag3p": (C.c_int, [_D, _D, _D, _D] + [C.c_int64] * 5),
+    "lica_gpu_trdiag3_device": (C.c_int, [C.c_void_p] * 5 + [C.c_int64] * 5 + [C.c_void_p]),
+    "lica_gpu_trdiag3p_device": (C.c_int, [C.c_void_p] * 4 + [C.c_int64] * 5 + [C.c_void_p]),
+    "lica_gpu_poisson": (C.c_int, [C.c_int64] * 6 + [_D, _D, _D, _I64, _D, _D, _D]),
+    "lica_mg_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                 C.POINTER(MgOptions)]),
+    "lica_mg_destroy": (C.c_int, [C.c_void_p]),
+    "lica_mg_solve_device": (C.c_int, [C.c_void_p] * 5 + [C.c_double, C.c_int32, C.POINTER(MgResult),
+                                                           C.c_void_p]),
+    "lica_mg_solve_host": (C.c_int, [C.c_void_p, _D, _D, _D, _D, C.c_double, C.c_int32, C.POINTER(MgResult),
+                                      C.c_void_p]),
+    "lica_mg_profile": (C.c_int, [C.c_void_p, C.c_int32]),
+    "lica_mg_profile_read": (C.c_int, [C.c_void_p, C.c_int32, _D, _I64]),
+    "lica_mg_precond_device": (C.c_int, [C.c_void_p] * 6),
+    "lica_mg_apply_device": (C.c_int, [C.c_void_p] * 6),
+}
+
+STATUS = {0: "LICA_OK", 1: "LICA_NOT_CONVERGED", 2: "LICA_BAND_OVERFLOW", 3: "LICA_NAN", 4: "LICA_BAD_ARG",
+          5: "LICA_ERR_CUDA", 6: "LICA_ERR_NOMEM"}
+
+
+class LicaError(RuntimeError):
+    def __init__(self, code, where):
+        msg = lib().lica_last_error().decode(errors="replace")
+        super().__init__(f"{where}: {STATUS.get(code, code)} {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = lib_path()
+        if not os.path.exists(path):
+            raise ImportError(f"lica CUDA library not built: {path} is missing (run __graft_entry__.build())")
+        L = C.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(code, where, ok=(0,)):
+    if code not in ok:
+        raise LicaError(code, where)
+    return code
+
+
+def launch_count() -> int:
+    return int(lib().lica_kernel_launch_count())

@@ -1,0 +1,116 @@
+"""ctypes bindings to the oracle (test infrastructure only).
+
+The oracle is the CPU restatement that the CUDA path is checked against.  Only
+tests/, __graft_entry__.smoke() and bench.py's CPU legs may import this module; the
+product package never does.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import build as _build
+
+_LIBS = {}
+
+_D = C.POINTER(C.c_double)
+_I64 = C.POINTER(C.c_int64)
+_INT = C.POINTER(C.c_int)
+
+
+def lib(native: bool = False):
+    key = bool(native)
+    if key not in _LIBS:
+        L = C.CDLL(_build.build(native=native))
+        L.orc_mg_solve.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double] + [C.c_int] * 7 + \
+            [_D, _D, _D, _D, C.c_double, C.c_int, _INT, _D, _D]
+        L.orc_mg_precond.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double] + [C.c_int] * 6 + [_D] * 4
+        L.orc_mg_apply.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, _D, _D, _D, _D]
+        L.orc_mg_smooth.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, _D, _D, _D, _D, C.c_int,
+                                    C.c_int]
+        L.orc_trdiag3.argtypes = [_D, _D, _D, _D, _D] + [C.c_int64] * 5
+        L.orc_trdiag3p.argtypes = [_D, _D, _D, _D] + [C.c_int64] * 5
+        L.orc_poisson1d.argtypes = [C.c_int64] * 6 + [_D, _D, _D, _I64, _D, _D, _D]
+        _LIBS[key] = L
+    return _LIBS[key]
+
+
+def _p(a):
+    return a.ctypes.data_as(_D if a.dtype == np.float64 else _I64)
+
+
+METHODS = {"vcycle": 0, "defect": 1, "pcg": 2}
+
+
+def mg_solve(f, bx, by, hx, hy, *, nlevels=6, nu1=2, nu2=2, ncoarse=2, sym=True, method="pcg", rtol=1e-10,
+             max_cycles=100, mixed=False, p0=None, native=False):
+    """Multigrid solve of A p = f (see oracle/mg2d.cpp).  Returns (p, cycles, rel, hist, status)."""
+    ny, nx = f.shape
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    bx = np.ascontiguousarray(bx, dtype=np.float64)
+    by = np.ascontiguousarray(by, dtype=np.float64)
+    assert bx.shape == (ny, nx) and by.shape == (ny + 1, nx)
+    p = np.zeros((ny, nx)) if p0 is None else np.array(p0, dtype=np.float64, copy=True, order="C")
+    cyc = C.c_int(0)
+    rel = C.c_double(0.0)
+    hist = np.full(max_cycles + 1, np.nan)
+    st = lib(native).orc_mg_solve(nx, ny, hx, hy, nlevels, nu1, nu2, ncoarse, int(sym), METHODS[method],
+                                  int(mixed), _p(f), _p(bx), _p(by), _p(p), rtol, max_cycles, C.byref(cyc),
+                                  C.byref(rel), _p(hist))
+    return p, cyc.value, rel.value, hist[: cyc.value + 1], st
+
+
+def mg_apply(u, bx, by, hx, hy):
+    ny, nx = u.shape
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    out = np.empty_like(u)
+    lib().orc_mg_apply(nx, ny, hx, hy, _p(np.ascontiguousarray(bx)), _p(np.ascontiguousarray(by)), _p(u),
+                       _p(out))
+    return out
+
+
+def mg_smooth(u, f, bx, by, hx, hy, nsweeps, reverse=False):
+    ny, nx = u.shape
+    u = np.array(u, dtype=np.float64, copy=True, order="C")
+    lib().orc_mg_smooth(nx, ny, hx, hy, _p(np.ascontiguousarray(bx)), _p(np.ascontiguousarray(by)),
+                        _p(np.ascontiguousarray(f)), _p(u), nsweeps, int(reverse))
+    return u
+
+
+def mg_precond(r, bx, by, hx, hy, *, nlevels=6, nu1=2, nu2=2, ncoarse=2, sym=True, mixed=False):
+    """z = M r, one V-cycle preconditioner application."""
+    ny, nx = r.shape
+    z = np.empty((ny, nx))
+    st = lib().orc_mg_precond(nx, ny, hx, hy, nlevels, nu1, nu2, ncoarse, int(sym), int(mixed),
+                              _p(np.ascontiguousarray(bx)), _p(np.ascontiguousarray(by)),
+                              _p(np.ascontiguousarray(r, dtype=np.float64)), _p(z))
+    assert st == 0, st
+    return z
+
+
+def trdiag3(A, B, C_, R, l1, l2, ll1, ll2):
+    """TRDIAG3 on Fortran-ordered (ld, n) arrays; returns (R_out, UU)."""
+    A, B, C_ = (np.asfortranarray(x, dtype=np.float64) for x in (A, B, C_))
+    R = np.array(R, dtype=np.float64, order="F", copy=True)
+    UU = np.zeros_like(R, order="F")
+    st = lib().orc_trdiag3(_p(A), _p(B), _p(C_), _p(R), _p(UU), l1, l2, ll1, ll2, A.shape[0])
+    assert st == 0
+    return R, UU
+
+
+def trdiag3p(A, B, C_, F, j1, j2, l1, l2):
+    A, B, C_ = (np.asfortranarray(x, dtype=np.float64) for x in (A, B, C_))
+    F = np.array(F, dtype=np.float64, order="F", copy=True)
+    st = lib().orc_trdiag3p(_p(A), _p(B), _p(C_), _p(F), j1, j2, l1, l2, A.shape[0])
+    assert st == 0
+    return F
+
+
+def poisson1d(geom, p, divgsum, denf_zi):
+    """POISSON (1d.f:3492) on Fortran-layout arrays; geom is a dict of GEOM arrays."""
+    m1, m2, m3 = geom["m1"], geom["m2"], geom["m3"]
+    p = np.array(p, dtype=np.float64, order="F", copy=True)
+    st = lib().orc_poisson1d(m1, m2, m3, geom["n1m"], geom["n2m"], geom["n3m"], _p(geom["vvdz"]),
+                             _p(geom["ssdz"]), _p(geom["fixkl"]), _p(geom["kpv"]), _p(p),
+                             _p(np.asfortranarray(divgsum)), _p(np.asfortranarray(denf_zi)))
+    assert st == 0
+    return p

@@ -1,0 +1,33 @@
+"""The C-ABI library loads and exports every symbol include/lica_gpu.h declares (no
+compute calls: this runs without a GPU)."""
+import ctypes
+import os
+import re
+
+from lica_boiling1d_b200 import build, native
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    txt = open(os.path.join(ROOT, "include", "lica_gpu.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(lica_\w+)\s*\(", txt)))
+
+
+def test_header_declares_expected_entry_points():
+    syms = declared_symbols()
+    for s in ("lica_gpu_poisson", "lica_gpu_trdiag3", "lica_gpu_trdiag3p", "lica_mg_create", "lica_mg_solve_device",
+              "lica_mg_solve_host"):
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol():
+    build.build()
+    lib = ctypes.CDLL(build.LIB)
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_header():
+    assert set(declared_symbols()) == set(native.SIGNATURES), set(declared_symbols()) ^ set(native.SIGNATURES)
