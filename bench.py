@@ -72,7 +72,7 @@ class ClockSampler:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
-            if self.uuid and parts[0] != self.uuid:
+            if self.uuid and parts[0].lower().replace("gpu-", "") != self.uuid:
                 continue
             self.samples.append(parts[1:])
 
@@ -193,7 +193,7 @@ def run_ours(args):
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     props = torch.cuda.get_device_properties(dev)
-    uuid = "GPU-" + str(props.uuid) if hasattr(props, "uuid") else None
+    uuid = str(props.uuid).lower().replace("gpu-", "") if hasattr(props, "uuid") else None
     clocks = ClockSampler(uuid)
     clocks.start()
     time.sleep(0.4)

@@ -9,6 +9,8 @@
 //   * Grid kernels own a TX x TY tile plus a halo staged in shared memory and run every
 //     red-black half-sweep of one visit to a level inside the tile (temporal blocking:
 //     the halo shrinks by one ring per half-sweep), so a visit reads u, f, beta once.
+//     No kernel writes an array it reads a halo of: k_up writes a separate post-smoothing
+//     buffer and the CG vectors x, p ping-pong between two buffers by iteration parity.
 //       k_down : nu1 sweeps from a zero iterate + residual + 2x2 restriction
 //       k_up   : piecewise-constant prolongation + nu2 sweeps (black first), and at
 //                level 0 the r.z partial of the CG update
@@ -176,10 +178,13 @@ __global__ void __launch_bounds__(NT) k_down(const T* __restrict__ f, const T* _
 // k_up: u += P uc (piecewise constant), nu2 sweeps black-then-red; at level 0 also the
 // partial of r.z (r = f of level 0, z = u) and, in the last block, beta = rz/rz_prev.
 // ------------------------------------------------------------------------------------
+// Out of place: reads the pre-smoothed iterate u_pre (with halo) and writes u_post, so no
+// block ever reads a neighbour's tile after that neighbour has updated it.
 template <typename T, int NSW, bool LEVEL0>
-__global__ void __launch_bounds__(NT) k_up(T* __restrict__ u, const T* __restrict__ uc, const T* __restrict__ f,
-                                           const T* __restrict__ bx, const T* __restrict__ by, int nx, int ny, T cx,
-                                           T cy, State* __restrict__ st, double* __restrict__ partials) {
+__global__ void __launch_bounds__(NT) k_up(const T* __restrict__ u, T* __restrict__ u_post, const T* __restrict__ uc,
+                                           const T* __restrict__ f, const T* __restrict__ bx,
+                                           const T* __restrict__ by, int nx, int ny, T cx, T cy,
+                                           State* __restrict__ st, double* __restrict__ partials) {
     constexpr int H = 2 * NSW;
     constexpr int RX = TX + 2 * H, RY = TY + 2 * H;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -215,7 +220,7 @@ __global__ void __launch_bounds__(NT) k_up(T* __restrict__ u, const T* __restric
     for (int k = threadIdx.x; k < TX * TY; k += blockDim.x) {
         const int ty = k / TX, tx = k - ty * TX;
         const T z = su[(ty + H) * RX + tx + H];
-        u[(size_t)(blockIdx.y * TY + ty) * nx + blockIdx.x * TX + tx] = z;
+        u_post[(size_t)(blockIdx.y * TY + ty) * nx + blockIdx.x * TX + tx] = z;
         if (LEVEL0) acc += double(sf[(ty + H) * RX + tx + H]) * double(z);
     }
     if (LEVEL0) {
@@ -231,13 +236,15 @@ __global__ void __launch_bounds__(NT) k_up(T* __restrict__ u, const T* __restric
 // ------------------------------------------------------------------------------------
 // CG kernels (FP64 vectors)
 // ------------------------------------------------------------------------------------
-// p = z + beta*p on the tile and a one-cell ring, then p.(A p) over the tile; the last
-// block sets alpha = rz / p.Ap.
+// p_new = z + beta*p_old on the tile and a one-cell ring, then p_new.(A p_new) over the
+// tile; the last block sets alpha = rz / p.Ap.  p ping-pongs between two buffers chosen
+// on the device by the iteration parity (p_old = pp[it&1], p_new = pp[(it+1)&1]), so the
+// halo is always read from a buffer no block of this launch writes.
 template <typename TZ>
-__global__ void __launch_bounds__(NT) k_pupdate(double* __restrict__ p, const TZ* __restrict__ z,
-                                                const double* __restrict__ bx, const double* __restrict__ by, int nx,
-                                                int ny, double cx, double cy, State* __restrict__ st,
-                                                double* __restrict__ partials) {
+__global__ void __launch_bounds__(NT) k_pupdate(double* __restrict__ p0, double* __restrict__ p1,
+                                                const TZ* __restrict__ z, const double* __restrict__ bx,
+                                                const double* __restrict__ by, int nx, int ny, double cx, double cy,
+                                                State* __restrict__ st, double* __restrict__ partials) {
     constexpr int H = 1, RX = TX + 2, RY = TY + 2;
     __shared__ double sp[RX * RY];
     __shared__ double sbx[(RX + 1) * RY];
@@ -245,6 +252,9 @@ __global__ void __launch_bounds__(NT) k_pupdate(double* __restrict__ p, const TZ
     __shared__ double red[32];
     const int gi0 = blockIdx.x * TX - H, gj0 = blockIdx.y * TY - H;
     const double beta = st->beta;
+    const int par = st->it & 1;
+    const double* __restrict__ p = par ? p1 : p0;
+    double* __restrict__ pn = par ? p0 : p1;
     for (int k = threadIdx.x; k < RX * RY; k += blockDim.x) {
         const int sy = k / RX, sx = k - sy * RX;
         const int j = gj0 + sy;
@@ -268,17 +278,21 @@ __global__ void __launch_bounds__(NT) k_pupdate(double* __restrict__ p, const TZ
         const double pv = sp[sy * RX + sx];
         const double q = s.s - s.d * pv;
         acc += pv * q;
-        p[(size_t)j * nx + blockIdx.x * TX + tx] = pv;
+        pn[(size_t)j * nx + blockIdx.x * TX + tx] = pv;
     }
     const double b = block_sum(acc, red);
     double tot;
     if (grid_sum_last(b, partials, &st->cnt[1], &tot, red)) st->alpha = st->rz / tot;
 }
 
-// x += alpha*p on the tile and a ring, r = f - A x over the tile (FP64), stored as TR;
-// the last block forms rel = ||r||/||f|| and the loop condition.
+// x_new = x_old + alpha*p on the tile and a ring, r = f - A x_new over the tile (FP64),
+// stored as TR; the last block forms rel = ||r||/||f||, advances the iteration count and
+// sets the loop condition.  x ping-pongs like p: x_old = xx[it&1], x_new = xx[(it+1)&1]
+// (xx[0] is the caller's array); p is the buffer k_pupdate just wrote, pp[(it+1)&1].
+// first = 1: the set-up pass, r = f - A x0 and ||f||, nothing written to x.
 template <typename TR>
-__global__ void __launch_bounds__(NT) k_xupdate(double* __restrict__ x, const double* __restrict__ p,
+__global__ void __launch_bounds__(NT) k_xupdate(double* __restrict__ x0, double* __restrict__ x1,
+                                                const double* __restrict__ p0, const double* __restrict__ p1,
                                                 const double* __restrict__ f, const double* __restrict__ bx,
                                                 const double* __restrict__ by, TR* __restrict__ r_out, int nx, int ny,
                                                 double cx, double cy, State* __restrict__ st,
@@ -291,6 +305,10 @@ __global__ void __launch_bounds__(NT) k_xupdate(double* __restrict__ x, const do
     __shared__ double red[32];
     const int gi0 = blockIdx.x * TX - H, gj0 = blockIdx.y * TY - H;
     const double alpha = first ? 0.0 : st->alpha;
+    const int par = first ? 0 : (st->it & 1);
+    const double* __restrict__ x = par ? x1 : x0;
+    double* __restrict__ xn = par ? x0 : x1;
+    const double* __restrict__ p = par ? p0 : p1;
     for (int k = threadIdx.x; k < RX * RY; k += blockDim.x) {
         const int sy = k / RX, sx = k - sy * RX;
         const int j = gj0 + sy;
@@ -317,7 +335,7 @@ __global__ void __launch_bounds__(NT) k_xupdate(double* __restrict__ x, const do
         const double r = fv - (s.s - s.d * xv);
         acc += r * r;
         if (first) accf += fv * fv;
-        if (!first) x[g] = xv;
+        if (!first) xn[g] = xv;
         r_out[g] = TR(r);
     }
     const double b = block_sum(acc, red);
@@ -677,6 +695,14 @@ __global__ void k_to_float(const double* __restrict__ a, float* __restrict__ b, 
         b[k] = float(a[k]);
 }
 
+// After the loop: an odd iteration count leaves the solution in the internal buffer x1.
+__global__ void k_finish(double* __restrict__ x0, const double* __restrict__ x1, const State* __restrict__ st,
+                         size_t n) {
+    if ((st->it & 1) == 0) return;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        x0[k] = x1[k];
+}
+
 __global__ void k_widen(const float* __restrict__ a, double* __restrict__ b, size_t n) {
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
         b[k] = double(a[k]);
@@ -737,7 +763,8 @@ using namespace lica::mg;
 struct LevelBuf {
     int nx = 0, ny = 0;
     double cx = 0, cy = 0;
-    void* u = nullptr;      // T
+    void* u = nullptr;      // T: iterate after pre-smoothing (k_down), or the CTA kernel's output
+    void* up = nullptr;     // T: iterate after correction and post-smoothing (k_up)
     void* f = nullptr;      // T
     double* bx64 = nullptr;  // FP64 beta chain (level 0: the caller's arrays)
     double* by64 = nullptr;
@@ -754,9 +781,11 @@ struct lica_mg {
     size_t cta_smem = 0;
     CtaParams cp{};
     // level-0 CG vectors
-    double* pcg = nullptr;   // p
+    double* pcg[2] = {nullptr, nullptr};  // p, ping-pong by iteration parity
+    double* xb = nullptr;    // second x buffer (the first is the caller's)
     void* r = nullptr;       // r (T): the V-cycle's level-0 f
-    void* z = nullptr;       // z (T): the V-cycle's level-0 u
+    void* zpre = nullptr;    // z after pre-smoothing (T)
+    void* z = nullptr;       // z (T): the V-cycle's level-0 output
     double* partials = nullptr;
     State* st = nullptr;
     State* st_host = nullptr;  // pinned
@@ -879,18 +908,19 @@ int launch_up(lica_mg* m, int l, cudaStream_t s) {
     const T* bx = std::is_same<T, float>::value ? (const T*)L.bx32 : (const T*)L.bx64;
     const T* by = std::is_same<T, float>::value ? (const T*)L.by32 : (const T*)L.by64;
     dim3 grid(L.nx / TX, L.ny / TY);
-    T* u = (T*)L.u;
-    const T* uc = (const T*)C.u;
+    const T* u = (const T*)L.u;
+    T* up = (T*)L.up;
+    const T* uc = (const T*)((l + 1 == m->lcta) ? C.u : C.up);
     const T* f = (const T*)L.f;
     const T cx = T(L.cx), cy = T(L.cy);
     ProfScope ps(m, l == 0 ? LICA_MG_UP0 : LICA_MG_UP, s);
-#define LICA_UP(NS)                                                                                               \
-    if (l == 0)                                                                                                   \
-        k_up<T, NS, true><<<grid, NT, grid_smem<T, NS>(false), s>>>(u, uc, f, bx, by, L.nx, L.ny, cx, cy, m->st,  \
-                                                                    m->partials);                                 \
-    else                                                                                                          \
-        k_up<T, NS, false><<<grid, NT, grid_smem<T, NS>(false), s>>>(u, uc, f, bx, by, L.nx, L.ny, cx, cy, m->st, \
-                                                                     m->partials);
+#define LICA_UP(NS)                                                                                                  \
+    if (l == 0)                                                                                                      \
+        k_up<T, NS, true><<<grid, NT, grid_smem<T, NS>(false), s>>>(u, up, uc, f, bx, by, L.nx, L.ny, cx, cy, m->st, \
+                                                                    m->partials);                                    \
+    else                                                                                                             \
+        k_up<T, NS, false><<<grid, NT, grid_smem<T, NS>(false), s>>>(u, up, uc, f, bx, by, L.nx, L.ny, cx, cy,       \
+                                                                     m->st, m->partials);
     switch (m->o.nu2) {
         case 1: LICA_UP(1) break;
         case 2: LICA_UP(2) break;
@@ -979,8 +1009,8 @@ int launch_xupdate(lica_mg* m, double* x, const double* f, int first, cudaGraphC
     LevelBuf& L = m->lv[0];
     dim3 grid(L.nx / TX, L.ny / TY);
     ProfScope ps(m, LICA_MG_XUPDATE, s);
-    k_xupdate<TR><<<grid, NT, 0, s>>>(x, m->pcg, f, L.bx64, L.by64, (TR*)m->r, L.nx, L.ny, L.cx, L.cy, m->st,
-                                      m->partials, first, h, use_cond);
+    k_xupdate<TR><<<grid, NT, 0, s>>>(x, m->xb, m->pcg[0], m->pcg[1], f, L.bx64, L.by64, (TR*)m->r, L.nx, L.ny,
+                                      L.cx, L.cy, m->st, m->partials, first, h, use_cond);
     LICA_CUDA_TRY(cudaGetLastError());
     lica_count_launches(1);
     return LICA_OK;
@@ -991,8 +1021,8 @@ int launch_pupdate(lica_mg* m, cudaStream_t s) {
     LevelBuf& L = m->lv[0];
     dim3 grid(L.nx / TX, L.ny / TY);
     ProfScope ps(m, LICA_MG_PUPDATE, s);
-    k_pupdate<TZ><<<grid, NT, 0, s>>>(m->pcg, (const TZ*)m->z, L.bx64, L.by64, L.nx, L.ny, L.cx, L.cy, m->st,
-                                      m->partials);
+    k_pupdate<TZ><<<grid, NT, 0, s>>>(m->pcg[0], m->pcg[1], (const TZ*)m->z, L.bx64, L.by64, L.nx, L.ny, L.cx,
+                                      L.cy, m->st, m->partials);
     LICA_CUDA_TRY(cudaGetLastError());
     lica_count_launches(1);
     return LICA_OK;
@@ -1005,7 +1035,7 @@ int enqueue_setup(lica_mg* m, double* x, const double* f, const double* bx, cons
     k_init_state<<<1, 1, 0, s>>>(m->st, rtol, max_it);
     LICA_CUDA_TRY(cudaGetLastError());
     const size_t n = (size_t)m->nx * m->ny;
-    k_zero<<<1184, 256, 0, s>>>(m->pcg, n);
+    k_zero<<<1184, 256, 0, s>>>(m->pcg[0], n);
     LICA_CUDA_TRY(cudaGetLastError());
     lica_count_launches(2);
     if ((st = setup_beta(m, bx, by, s))) return st;
@@ -1017,7 +1047,8 @@ int enqueue_setup(lica_mg* m, double* x, const double* f, const double* bx, cons
 int enqueue_iteration(lica_mg* m, double* x, const double* f, cudaGraphConditionalHandle h, int use_cond,
                       cudaStream_t s) {
     int st;
-    m->lv[0].u = m->z;
+    m->lv[0].u = m->zpre;
+    m->lv[0].up = m->z;
     m->lv[0].f = m->r;
     if ((st = run_vcycle(m, s))) return st;
     if (is_mixed(m)) {
@@ -1026,6 +1057,13 @@ int enqueue_iteration(lica_mg* m, double* x, const double* f, cudaGraphCondition
     }
     if ((st = launch_pupdate<double>(m, s))) return st;
     return launch_xupdate<double>(m, x, f, 0, h, use_cond, s);
+}
+
+int enqueue_finish(lica_mg* m, double* x, cudaStream_t s) {
+    k_finish<<<1184, 256, 0, s>>>(x, m->xb, m->st, (size_t)m->nx * m->ny);
+    LICA_CUDA_TRY(cudaGetLastError());
+    lica_count_launches(1);
+    return LICA_OK;
 }
 
 int read_state(lica_mg* m, cudaStream_t s) {
@@ -1090,6 +1128,21 @@ int build_graph(lica_mg* m, double* x, const double* f, const double* bx, const 
     if (st) { cudaGraphDestroy(g); return st; }
     LICA_CUDA_TRY(e);
     m->body_nodes = (int)(lica_kernel_launch_count() - before);
+    // finishing copy after the WHILE node, captured into g
+    {
+        cudaGraph_t fin;
+        LICA_CUDA_TRY(cudaGraphCreate(&fin, 0));
+        LICA_CUDA_TRY(cudaStreamBeginCaptureToGraph(s, fin, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        st = enqueue_finish(m, x, s);
+        e = cudaStreamEndCapture(s, &captured);
+        if (st) { cudaGraphDestroy(fin); cudaGraphDestroy(g); return st; }
+        LICA_CUDA_TRY(e);
+        cudaGraphNode_t child;
+        e = cudaGraphAddChildGraphNode(&child, g, &wnode, 1, fin);
+        cudaGraphDestroy(fin);
+        LICA_CUDA_TRY(e);
+        m->setup_nodes += 1;
+    }
     // the captures counted as launches; undo that (replays are counted per run)
     lica_count_launches(-(int64_t)(m->setup_nodes + m->body_nodes));
     e = cudaGraphInstantiate(&m->gexec, g, 0);
@@ -1124,6 +1177,8 @@ int solve_impl(lica_mg* m, double* x, const double* f, const double* bx, const d
             if ((st = enqueue_iteration(m, x, f, h, 0, s))) return st;
             if ((st = read_state(m, s))) return st;
         }
+        if ((st = enqueue_finish(m, x, s))) return st;
+        if ((st = read_state(m, s))) return st;
         if (m->profile) prof_collect(m);
     }
     if (res) {
@@ -1242,8 +1297,11 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
         }                                                                            \
     } while (0)
     const size_t n0 = (size_t)nx * ny;
-    TRY_ALLOC(m->pcg, sizeof(double) * n0);
+    TRY_ALLOC(m->pcg[0], sizeof(double) * n0);
+    TRY_ALLOC(m->pcg[1], sizeof(double) * n0);
+    TRY_ALLOC(m->xb, sizeof(double) * n0);
     TRY_ALLOC(m->r, tsz * n0);
+    TRY_ALLOC(m->zpre, tsz * n0);
     TRY_ALLOC(m->z, tsz * n0);
     for (int l = 1; l <= m->bottom; ++l) {
         LevelBuf& L = m->lv[l];
@@ -1252,6 +1310,7 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
             TRY_ALLOC(L.u, tsz * n);
             TRY_ALLOC(L.f, tsz * n);
         }
+        if (l < lcta) TRY_ALLOC(L.up, tsz * n);
         TRY_ALLOC(L.bx64, sizeof(double) * n);
         TRY_ALLOC(L.by64, sizeof(double) * (n + L.nx));
     }
@@ -1296,6 +1355,7 @@ int lica_mg_destroy(lica_mg* m) {
     for (auto e : m->event_pool) cudaEventDestroy(e);
     for (size_t l = 1; l < m->lv.size(); ++l) {
         cudaFree(m->lv[l].u);
+        cudaFree(m->lv[l].up);
         cudaFree(m->lv[l].f);
         cudaFree(m->lv[l].bx64);
         cudaFree(m->lv[l].by64);
@@ -1304,8 +1364,11 @@ int lica_mg_destroy(lica_mg* m) {
         cudaFree(L.bx32);
         cudaFree(L.by32);
     }
-    cudaFree(m->pcg);
+    cudaFree(m->pcg[0]);
+    cudaFree(m->pcg[1]);
+    cudaFree(m->xb);
     cudaFree(m->r);
+    cudaFree(m->zpre);
     cudaFree(m->z);
     cudaFree(m->partials);
     cudaFree(m->st);
@@ -1355,7 +1418,8 @@ int lica_mg_precond_device(lica_mg* m, double* z, const double* r, const double*
     int st;
     if ((st = setup_beta(m, bx, by, s))) return st;
     const size_t n = (size_t)m->nx * m->ny;
-    m->lv[0].u = m->z;
+    m->lv[0].u = m->zpre;
+    m->lv[0].up = m->z;
     m->lv[0].f = m->r;
     k_init_state<<<1, 1, 0, s>>>(m->st, 0.0, 0);
     LICA_CUDA_TRY(cudaGetLastError());
@@ -1396,7 +1460,7 @@ int lica_mg_profile_read(lica_mg* m, int32_t kernel_class, double* total_ms, int
 
 int lica_mg_apply_device(lica_mg* m, double* out, const double* u, const double* bx, const double* by,
                          void* stream) {
-    if (!m || !out || !u || !bx || !by) return LICA_BAD_ARG;
+    if (!m || !out || !u || !bx || !by || out == u) return LICA_BAD_ARG;  // out must not alias u (halo reads)
     cudaStream_t s = (cudaStream_t)stream;
     const LevelBuf& L = m->lv[0];
     k_apply<<<dim3(L.nx / TX, L.ny / TY), NT, 0, s>>>(out, u, bx, by, L.nx, L.ny, L.cx, L.cy);

@@ -44,7 +44,8 @@ def test_trdiag3_bitwise(alias):
     Rg = R.copy(order="F")
     if alias:
         poisson.trdiag3(A, B, C, Rg, Rg, l1, l2, ll1, ll2)
-        np.testing.assert_array_equal(Rg[:, l1 - 1:l2], UU_ref[:, l1 - 1:l2])
+        np.testing.assert_array_equal(Rg[ll1 - 1:ll2, l1 - 1:l2], UU_ref[ll1 - 1:ll2, l1 - 1:l2])
+        np.testing.assert_array_equal(Rg[ll2:], R[ll2:])  # lines outside [ll1, ll2] untouched
     else:
         UUg = np.zeros_like(R, order="F")
         poisson.trdiag3(A, B, C, Rg, UUg, l1, l2, ll1, ll2)
