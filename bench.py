@@ -165,13 +165,15 @@ def run_ours(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
-    case = bubble_poisson_case(N)
+    n = args.n
+    nlevels = NLEVELS + int(round(np.log2(n / N)))
+    case = bubble_poisson_case(n)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
     f, bx, by = t(case.f), t(case.bx), t(case.by)
-    p = torch.zeros((N, N), dtype=torch.float64, device=dev)
+    p = torch.zeros((n, n), dtype=torch.float64, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    solver = poisson.MultigridPoisson(N, N, case.hx, case.hy, nlevels=NLEVELS, ncoarse=2, precision=args.precision,
-                                      use_graph=True)
+    solver = poisson.MultigridPoisson(n, n, case.hx, case.hy, nlevels=nlevels, ncoarse=2, precision=args.precision,
+                                      use_graph=not args.no_graph)
     stream = torch.cuda.current_stream(dev)
 
     def barrier():
@@ -218,11 +220,14 @@ def run_ours(args):
     total_ms = slowest(total_ms)
     value = world * args.steps / (total_ms / 1e3)
 
+    e2e, roofline, variants, cpu = None, None, {}, None
+    if args.no_e2e:
+        return finish(args, locals())
     # end-to-end through the host C-ABI entry: H2D of p0, f, bx, by; solve; D2H of p
     hf = torch.from_numpy(case.f.copy()).pin_memory().numpy()
     hbx = torch.from_numpy(case.bx.copy()).pin_memory().numpy()
     hby = torch.from_numpy(case.by.copy()).pin_memory().numpy()
-    hp = torch.zeros((N, N), dtype=torch.float64).pin_memory().numpy()
+    hp = torch.zeros((n, n), dtype=torch.float64).pin_memory().numpy()
     for _ in range(2):
         hp[...] = 0.0
         solver.solve(hp, hf, hbx, hby, rtol=RTOL, stream=stream)
@@ -243,6 +248,8 @@ def run_ours(args):
            "h2d_bytes_per_step": int(hp.nbytes + hf.nbytes + hbx.nbytes + hby.nbytes),
            "d2h_bytes_per_step": int(hp.nbytes), "steps": ke, "path": "lica_mg_solve_host (C ABI), pinned host buffers"}
 
+    if args.no_profile:
+        return finish(args, locals())
     # kernel-class timing: one profiled solve (separate launches bracketed by CUDA events)
     solver.profile(True)
     for _ in range(3):
@@ -255,7 +262,7 @@ def run_ours(args):
     dom = max(level0, key=lambda k: level0[k][0])
     ms, nl = level0[dom]
     avg_s = ms / 1e3 / max(nl, 1)
-    alg = ALG_BYTES_PER_CELL[dom] * N * N
+    alg = ALG_BYTES_PER_CELL[dom] * n * n
     peak, peak_kind = peaks()
     achieved = alg / avg_s / 1e9
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -265,9 +272,8 @@ def run_ours(args):
                 "note": "one profiled solve as separate launches after the timed region; working set is L2-resident"}
 
     # secondary: the mixed-precision preconditioner on the same workload
-    variants = {}
     if args.precision == "fp64" and not args.skip_variants:
-        sm = poisson.MultigridPoisson(N, N, case.hx, case.hy, nlevels=NLEVELS, ncoarse=2, precision="mixed")
+        sm = poisson.MultigridPoisson(n, n, case.hx, case.hy, nlevels=nlevels, ncoarse=2, precision="mixed")
         for _ in range(3):
             p.zero_()
             sm.solve(p, f, bx, by, rtol=RTOL)
@@ -285,29 +291,36 @@ def run_ours(args):
                              "note": "FP32 smoothing/restriction/prolongation, FP64 residual, CG and coarsest solve"}
         sm.close()
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.skip_cpu:
+    if rank == 0 and world == 1 and not args.skip_cpu and n == N:
         threads = os.cpu_count()
         times, cits = cpu_solves(case, 15.0, 30)
         cpu = {"value": len(times) / sum(times), "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{len(times)} complete solves of the same workload (~15 s), FP64 C++/OpenMP restatement"}
 
-    if rank == 0:
+    return finish(args, locals())
+
+
+def finish(args, v):
+    import torch.distributed as dist
+    if v["rank"] == 0:
+        n = v["n"]
+        workload = WORKLOAD if n == N else WORKLOAD.replace("1024x1024", f"{n}x{n}").replace(
+            "6-level", f"{v['nlevels']}-level")
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "metric": METRIC, "value": v["value"], "unit": UNIT, "n_gpus": v["world"], "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": v["total_ms"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "nx": N, "ny": N, "nlevels": NLEVELS, "nu1": 2, "nu2": 2, "rtol": RTOL,
-                       "solver": "MG-PCG", "precision": args.precision, "l2_flush": "256 MiB write between steps",
-                       "parallelism": f"replicas x{world}"},
-            "iterations": its[-1], "rel_residual": rel,
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": clk, "variants": variants,
+            "config": {"workload": workload, "nx": n, "ny": n, "nlevels": v["nlevels"], "nu1": 2, "nu2": 2,
+                       "rtol": RTOL, "solver": "MG-PCG", "precision": args.precision,
+                       "l2_flush": "256 MiB write between steps", "parallelism": f"replicas x{v['world']}"},
+            "iterations": v["its"][-1], "rel_residual": v["rel"],
+            "roofline": v["roofline"], "cpu_baseline": v["cpu"], "e2e": v["e2e"], "gpu_launches": int(v["launches"]),
+            "clocks": v["clk"], "variants": v["variants"],
         }
         print(json.dumps(line), flush=True)
-    solver.close()
-    if world > 1:
+    v["solver"].close()
+    if v["world"] > 1:
         dist.destroy_process_group()
 
 
@@ -320,6 +333,12 @@ def main():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-variants", action="store_true")
+    ap.add_argument("--n", type=int, default=N, help="grid size (default: the 1024x1024 workload)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end and later legs (profiling runs)")
+    ap.add_argument("--no-profile", action="store_true", help="skip the kernel-class timing and later legs")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="launch kernels one by one instead of one CUDA graph per solve (for ncu, which cannot "
+                         "profile kernels of a graph with a conditional node)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
