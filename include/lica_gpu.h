@@ -7,7 +7,7 @@
  *      in the same Fortran layout (column-major, the Fortran lower bound of each array
  *      noted per argument).  Arrays are HOST arrays; the call copies them to the GPU,
  *      runs the CUDA kernels and copies the results back, like the subroutine it
- *      replaces.  A Fortran host binds them with ISO_C_BINDING.
+ *      replaces.  A Fortran host binds them with ISO_C_BINDING interfaces.
  *   2. Device-resident entry points (suffix _device) taking device pointers and a
  *      cudaStream_t passed as void*, for callers that keep state in HBM.
  *
@@ -66,6 +66,19 @@ int lica_gpu_trdiag3_device(const double* A, const double* B, const double* C, d
                             int64_t l1, int64_t l2, int64_t ll1, int64_t ll2, int64_t ld, void* stream);
 int lica_gpu_trdiag3p_device(const double* A, const double* B, const double* C, double* F,
                              int64_t j1, int64_t j2, int64_t l1, int64_t l2, int64_t ld, void* stream);
+
+/* TRDIAG3 on device arrays that allocates no memory.  No counterpart in the reference:
+ * it is for callers that cannot call cudaMalloc -- e.g. a solver loop whose device
+ * memory is owned by a pre-allocated pool, or one that must not hit the device-wide
+ * synchronisation of cudaMalloc/cudaFree or an out-of-memory failure mid-run.  Same
+ * kernel and bit-identical results as lica_gpu_trdiag3_device; its scratch is a fixed
+ * 2 MiB device array inside this library, so ld * l2 must not exceed 262144 (else
+ * LICA_BAD_ARG).  The first call on a device sets up the scratch address and should be
+ * made before any stream capture.  Enqueues on `stream` and returns without waiting.
+ * Calls that overlap on the GPU share the scratch and race: serialise them (one stream
+ * per device). */
+int lica_gpu_trdiag3_noalloc_device(const double* A, const double* B, const double* C, double* R, double* UU,
+                                    int64_t l1, int64_t l2, int64_t ll1, int64_t ll2, int64_t ld, void* stream);
 
 /* POISSON (1d.f:3492-3578), the 1-D column the reference solves (N1M = N2M = 1):
  * AK = VVDZ(K)*SSDZ(K)*DENF_ZI(1,1,K)*(1-FIXKL(K)), CK = VVDZ(KP1)*SSDZ(K)*DENF_ZI(1,1,KP1),

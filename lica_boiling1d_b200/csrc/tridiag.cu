@@ -157,6 +157,18 @@ struct DevBufs {
     }
 };
 
+// Fixed scratch for lica_gpu_trdiag3_noalloc_device: 2 MiB of doubles, enough for
+// ld * l2 <= 262144 (e.g. 512 lines of 512 unknowns).  Every GPU that loads this library
+// holds it until the process exits.  All calls on a device share it.
+constexpr size_t kNoAllocScratchDoubles = 262144;
+static __device__ __align__(256) double g_trdiag3_noalloc_scratch[kNoAllocScratchDoubles];
+
+// Device address of g_trdiag3_noalloc_scratch per device ordinal, looked up once with the
+// device current (host code may not use the symbol itself as a device pointer).
+std::mutex g_noalloc_mu;
+constexpr int kMaxDevices = 128;
+double* g_noalloc_addr[kMaxDevices] = {};
+
 }  // namespace tri
 }  // namespace lica
 
@@ -197,6 +209,44 @@ int lica_gpu_trdiag3p_device(const double* A, const double* B, const double* C, 
     LICA_CUDA_TRY(cudaGetLastError());
     lica_count_launches(1);
     LICA_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    return LICA_OK;
+}
+
+// TRDIAG3 on device arrays without allocating: same kernel and results as
+// lica_gpu_trdiag3_device, with the forward-sweep coefficients kept in the fixed scratch
+// array above instead of cudaMalloc'd memory.  The first call on a device looks up the
+// scratch address (cudaGetSymbolAddress) and should come before any stream capture.
+// Returns after enqueueing the kernel on `stream` (no synchronisation).  Calls that
+// overlap on the GPU (different streams, or different host threads on one device) share
+// the scratch and race.  The scratch needs no clearing: each line writes every
+// coefficient before it reads it.
+int lica_gpu_trdiag3_noalloc_device(const double* A, const double* B, const double* C, double* R, double* UU,
+                                    int64_t l1, int64_t l2, int64_t ll1, int64_t ll2, int64_t ld, void* stream) {
+    if (!A || !B || !C || !R || !UU || l2 < l1 || ll2 < ll1 || ll1 < 1 || ld < ll2 || l1 < 1) return LICA_BAD_ARG;
+    if ((double)ld * (double)l2 > (double)kNoAllocScratchDoubles) {
+        lica_set_last_error("lica_gpu_trdiag3_noalloc_device",
+                            "ld * l2 exceeds the fixed scratch of 262144 doubles (2 MiB)", __FILE__, __LINE__);
+        return LICA_BAD_ARG;
+    }
+    int dev = -1;
+    LICA_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return LICA_BAD_ARG;
+    double* gam = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void* addr = nullptr;
+            LICA_CUDA_TRY(cudaGetSymbolAddress(&addr, g_trdiag3_noalloc_scratch));
+            g_noalloc_addr[dev] = static_cast<double*>(addr);
+        }
+        gam = g_noalloc_addr[dev];
+    }
+    const int64_t nlines = ll2 - ll1 + 1;
+    const int threads = 128;
+    const unsigned blocks = (unsigned)((nlines + threads - 1) / threads);
+    k_trdiag3<<<blocks, threads, 0, (cudaStream_t)stream>>>(A, B, C, R, UU, gam, l1, l2, ll1, ll2, ld);
+    LICA_CUDA_TRY(cudaGetLastError());
+    lica_count_launches(1);
     return LICA_OK;
 }
 

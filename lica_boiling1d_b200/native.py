@@ -29,6 +29,7 @@ SIGNATURES = {
     "lica_gpu_trdiag3p": (C.c_int, [_D, _D, _D, _D] + [C.c_int64] * 5),
     "lica_gpu_trdiag3_device": (C.c_int, [C.c_void_p] * 5 + [C.c_int64] * 5 + [C.c_void_p]),
     "lica_gpu_trdiag3p_device": (C.c_int, [C.c_void_p] * 4 + [C.c_int64] * 5 + [C.c_void_p]),
+    "lica_gpu_trdiag3_noalloc_device": (C.c_int, [C.c_void_p] * 5 + [C.c_int64] * 5 + [C.c_void_p]),
     "lica_gpu_poisson": (C.c_int, [C.c_int64] * 6 + [_D, _D, _D, _I64, _D, _D, _D]),
     "lica_mg_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.c_double, C.c_double,
                                  C.POINTER(MgOptions)]),
