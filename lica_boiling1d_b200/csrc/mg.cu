@@ -43,7 +43,8 @@ namespace mg {
 
 constexpr int TX = 32;
 constexpr int TY = 32;
-constexpr int NT = 256;          // threads of a grid-kernel CTA
+constexpr int NT = 256;          // threads of a CG / set-up grid-kernel CTA
+constexpr int NTG = 512;         // threads of a smoothing grid-kernel CTA (two resident per SM)
 constexpr int NT_CTA = 1024;     // threads of the single-CTA coarse kernel
 constexpr int kMaxLevels = 16;
 constexpr int kSmallCells = 256; // levels with <= this many cells run in warp 0 alone
@@ -63,165 +64,275 @@ struct State {
 };
 
 // ------------------------------------------------------------------------------------
-// shared-memory staging
+// Coefficient arrays.  Every level stores its stencil weights pre-scaled, so no kernel
+// branches on the boundary or multiplies by 1/h^2:
+//   AX[j*nx+i] = cx * bx[j*nx+i]                 (west face of cell i; periodic)
+//   AY[j*nx+i] = 0                      j = 0    (Neumann wall: FIXKL(1) = 1)
+//              = cy * by[j*nx+i]        0 < j < ny
+//              = (2*cy) * by[ny*nx+i]   j = ny   (p = 0 on the top face: VVDZ(N3) = 2/h)
+// These are the same products the oracle forms at each use, so results stay identical.
 // ------------------------------------------------------------------------------------
-template <typename TS, typename TG>
-__device__ __forceinline__ void load_region(TS* __restrict__ s, int w, int h, const TG* __restrict__ g, int nx,
-                                            int nrows, int gi0, int gj0) {
-    for (int k = threadIdx.x; k < w * h; k += blockDim.x) {
-        const int sy = k / w, sx = k - sy * w;
-        const int j = gj0 + sy;
-        int i = gi0 + sx;
-        if (i < 0) i += nx; else if (i >= nx) i -= nx;
-        s[k] = (j >= 0 && j < nrows) ? TS(g[(size_t)j * nx + i]) : TS(0);
-    }
-}
-
-// Stencil sums of cell (sx,sy) of a staged region with row pitch RXp (u, f) and the face
-// arrays sbx (pitch RXp+1) and sby (pitch RXp).  j is the global row of the cell.
 template <typename T>
-struct Stencil {
-    T s, d;
+struct V2;
+template <>
+struct V2<double> {
+    using type = double2;
+};
+template <>
+struct V2<float> {
+    using type = float2;
 };
 
+// Asynchronous global->shared copy of one element (cp.async, 4 or 8 bytes), reading
+// nothing and writing zero when valid is false.
 template <typename T>
-__device__ __forceinline__ Stencil<T> stencil(const T* su, const T* sbx, const T* sby, int RXp, int sx, int sy,
-                                              int j, int ny, T cx, T cy) {
-    const int c = sy * RXp + sx;
-    const T aw = cx * sbx[sy * (RXp + 1) + sx];
-    const T ae = cx * sbx[sy * (RXp + 1) + sx + 1];
-    const T as = (j > 0) ? cy * sby[c] : T(0);
-    const T byn = sby[c + RXp];
-    const T an = (j < ny - 1) ? cy * byn : (T(2) * cy) * byn;
-    const T uw = su[c - 1], ue = su[c + 1];
-    const T us = (j > 0) ? su[c - RXp] : T(0);
-    const T un = (j < ny - 1) ? su[c + RXp] : T(0);
-    Stencil<T> r;
-    T s = aw * uw;
-    s += ae * ue;
-    s += as * us;
-    s += an * un;
-    T d = aw;
-    d += ae;
-    d += as;
-    d += an;
-    r.s = s;
-    r.d = d;
-    return r;
+__device__ __forceinline__ void async_copy(T* dst, const T* src, bool valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    const int n = valid ? (int)sizeof(T) : 0;
+    if (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
 }
 
-// One red-black half-sweep of colour `colour` over the region [lo, hi) x [lo, hiy).
-template <typename T>
-__device__ __forceinline__ void half_sweep(T* su, const T* sf, const T* sbx, const T* sby, int RXp, int lo, int hix,
-                                           int hiy, int colour, int gj0, int ny, T cx, T cy) {
-    const int wc = (hix - lo + 1) >> 1;
-    const int rows = hiy - lo;
-    for (int k = threadIdx.x; k < wc * rows; k += blockDim.x) {
-        const int r = k / wc, m = k - r * wc;
-        const int sy = lo + r;
-        const int sx = lo + ((lo + sy + colour) & 1) + 2 * m;
+__device__ __forceinline__ void async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Issues the copies of rows [gj0, gj0+RY) x columns [gi0, gi0+RX) of a row-major array
+// (nx columns, nrows rows, x periodic) into the colour-split arrays X0 (red) and X1
+// (black), each RY x RX/2: cell (sx, sy) has colour c = (sx + sy + gj0) & 1 and sits in
+// X_c at [sy][sx >> 1].  Rows outside [0, nrows) read as zero.  gi0 and nx are even, so
+// the pair of cells (2m, 2m+1) wraps as a pair.  Completion: async_wait_all + barrier.
+template <typename T, int RX, int RY>
+__device__ __forceinline__ void load_split(T* __restrict__ X0, T* __restrict__ X1, const T* __restrict__ g, int nx,
+                                           int nrows, int gi0, int gj0) {
+    constexpr int RXh = RX / 2;
+    for (int k = threadIdx.x; k < RY * RXh; k += blockDim.x) {
+        const int sy = k / RXh, m = k - sy * RXh;
         const int j = gj0 + sy;
-        if (sx >= hix || j < 0 || j >= ny) continue;
-        const Stencil<T> st = stencil(su, sbx, sby, RXp, sx, sy, j, ny, cx, cy);
-        su[sy * RXp + sx] = (st.s - sf[sy * RXp + sx]) / st.d;
+        int i = gi0 + 2 * m;
+        if (i < 0) i += nx; else if (i >= nx) i -= nx;
+        const bool ok = (j >= 0 && j < nrows);
+        const T* src = ok ? g + (size_t)j * nx + i : g;
+        const int odd = (sy + gj0) & 1;
+        async_copy(odd ? X1 + k : X0 + k, src, ok);
+        async_copy(odd ? X0 + k : X1 + k, src + 1, ok);
     }
 }
+
+// Stencil sums of the colour-c cell at compact position idx = sy*RXh + m, o = (c+sy+gj0)&1:
+// neighbours and the east/north faces live in the other colour's arrays (see load_split).
+template <typename T, int RXh>
+__device__ __forceinline__ void split_sums(const T* __restrict__ uO, const T* __restrict__ axC,
+                                           const T* __restrict__ axO, const T* __restrict__ ayC,
+                                           const T* __restrict__ ayO, int idx, int o, T& s, T& d) {
+    const T aw = axC[idx], ae = axO[idx + o], as = ayC[idx], an = ayO[idx + RXh];
+    const T uw = uO[idx + o - 1], ue = uO[idx + o], us = uO[idx - RXh], un = uO[idx + RXh];
+    T ss = aw * uw;
+    ss += ae * ue;
+    ss += as * us;
+    ss += an * un;
+    T dd = aw;
+    dd += ae;
+    dd += as;
+    dd += an;
+    s = ss;
+    d = dd;
+}
+
+// Colour-c half-sweep over the cells (sx, sy) of the ring-d interior, sx in [d, RX-d),
+// sy in [d, RY-d), whose global row lies in [0, ny): u = (s - f) * dinv.
+template <typename T, int RX, int RY>
+__device__ __forceinline__ void split_half_sweep(T* __restrict__ u0, T* __restrict__ u1, const T* __restrict__ f0,
+                                                 const T* __restrict__ f1, const T* __restrict__ ax0,
+                                                 const T* __restrict__ ax1, const T* __restrict__ ay0,
+                                                 const T* __restrict__ ay1, const T* __restrict__ di0,
+                                                 const T* __restrict__ di1, int c, int dring, int gj0, int ny) {
+    const int lo = dring, hi = RX - dring, hiy = RY - dring;
+    constexpr int RXh = RX / 2;
+    T* uC = c ? u1 : u0;
+    const T* uO = c ? u0 : u1;
+    const T* fC = c ? f1 : f0;
+    const T* dC = c ? di1 : di0;
+    const T* axC = c ? ax1 : ax0;
+    const T* axO = c ? ax0 : ax1;
+    const T* ayC = c ? ay1 : ay0;
+    const T* ayO = c ? ay0 : ay1;
+    const int rows = hiy - lo;
+    for (int k = threadIdx.x; k < rows * RXh; k += blockDim.x) {
+        const int r = k / RXh, m = k - r * RXh;
+        const int sy = lo + r;
+        const int o = (c + sy + gj0) & 1;
+        const int sx = 2 * m + o;
+        const int j = gj0 + sy;
+        if (sx < lo || sx >= hi || j < 0 || j >= ny) continue;
+        const int idx = sy * RXh + m;
+        const T aw = axC[idx], ae = axO[idx + o], as = ayC[idx], an = ayO[idx + RXh];
+        const T uw = uO[idx + o - 1], ue = uO[idx + o], us = uO[idx - RXh], un = uO[idx + RXh];
+        T sm = aw * uw;
+        sm += ae * ue;
+        sm += as * us;
+        sm += an * un;
+        uC[idx] = (sm - fC[idx]) * dC[idx];
+    }
+}
+
+// Residual f - A u of the cell (sx, sy) (inside the region's inner ring).
+template <typename T, int RXh>
+__device__ __forceinline__ T split_residual(const T* u0, const T* u1, const T* f0, const T* f1, const T* ax0,
+                                            const T* ax1, const T* ay0, const T* ay1, int sx, int sy, int gj0) {
+    const int c = (sx + sy + gj0) & 1, o = (c + sy + gj0) & 1;
+    const int idx = sy * RXh + (sx >> 1);
+    T sm, d;
+    split_sums<T, RXh>(c ? u0 : u1, c ? ax1 : ax0, c ? ax0 : ax1, c ? ay1 : ay0, c ? ay0 : ay1, idx, o, sm, d);
+    return (c ? f1 : f0)[idx] - (sm - d * (c ? u1 : u0)[idx]);
+}
+
+template <typename T, int NSW, int TXX, int TYY, bool DOWN>
+struct GridCfg {
+    static constexpr int HMIN = DOWN ? 2 * NSW + 1 : 2 * NSW;
+    static constexpr int H = (HMIN + 1) & ~1;  // even, for aligned vector loads
+    static constexpr int RX = TXX + 2 * H, RY = TYY + 2 * H, RXh = RX / 2;
+    static constexpr int ARR = RY * RXh;        // one colour of one array
+    static constexpr size_t SMEM = sizeof(T) * 10 * ARR;  // u, f, ax, ay, dinv x two colours
+};
 
 // ------------------------------------------------------------------------------------
 // k_down: nu1 red-black sweeps from a zero iterate, residual, 2x2 restriction.
 // ------------------------------------------------------------------------------------
-template <typename T, int NSW>
-__global__ void __launch_bounds__(NT) k_down(const T* __restrict__ f, const T* __restrict__ bx,
-                                             const T* __restrict__ by, T* __restrict__ u_out,
-                                             T* __restrict__ fc_out, int nx, int ny, T cx, T cy) {
-    constexpr int H = 2 * NSW + 1;
-    constexpr int RX = TX + 2 * H, RY = TY + 2 * H;
+template <typename T, int NSW, int TXX, int TYY>
+__global__ void __launch_bounds__(NTG, 2) k_down(const T* __restrict__ f, const T* __restrict__ ax,
+                                                 const T* __restrict__ ay, const T* __restrict__ dinv,
+                                                 T* __restrict__ u_out, T* __restrict__ fc_out, int nx, int ny) {
+    using C = GridCfg<T, NSW, TXX, TYY, true>;
+    constexpr int H = C::H, RX = C::RX, RY = C::RY, RXh = C::RXh, ARR = C::ARR, SKIP = C::H - C::HMIN;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* su = reinterpret_cast<T*>(smem_raw);
-    T* sf = su + RX * RY;
-    T* sbx = sf + RX * RY;
-    T* sby = sbx + (RX + 1) * RY;
-    const int gi0 = blockIdx.x * TX - H, gj0 = blockIdx.y * TY - H;
-    for (int k = threadIdx.x; k < RX * RY; k += blockDim.x) su[k] = T(0);
-    load_region(sf, RX, RY, f, nx, ny, gi0, gj0);
-    load_region(sbx, RX + 1, RY, bx, nx, ny, gi0, gj0);
-    load_region(sby, RX, RY + 1, by, nx, ny + 1, gi0, gj0);
+    T* sm = reinterpret_cast<T*>(smem_raw);
+    T* const u0 = sm;
+    T* const u1 = sm + ARR;
+    T* const f0 = sm + 2 * ARR;
+    T* const f1 = sm + 3 * ARR;
+    T* const ax0 = sm + 4 * ARR;
+    T* const ax1 = sm + 5 * ARR;
+    T* const ay0 = sm + 6 * ARR;
+    T* const ay1 = sm + 7 * ARR;
+    T* const di0 = sm + 8 * ARR;
+    T* const di1 = sm + 9 * ARR;
+    const int gi0 = blockIdx.x * TXX - H, gj0 = blockIdx.y * TYY - H;
+    load_split<T, RX, RY>(f0, f1, f, nx, ny, gi0, gj0);
+    load_split<T, RX, RY>(ax0, ax1, ax, nx, ny, gi0, gj0);
+    load_split<T, RX, RY>(ay0, ay1, ay, nx, ny + 1, gi0, gj0);
+    load_split<T, RX, RY>(di0, di1, dinv, nx, ny, gi0, gj0);
+    for (int k = threadIdx.x; k < 2 * ARR; k += blockDim.x) sm[k] = T(0);
+    async_wait_all();
     __syncthreads();
 #pragma unroll 1
     for (int q = 0; q < 2 * NSW; ++q) {
-        half_sweep(su, sf, sbx, sby, RX, q + 1, RX - 1 - q, RY - 1 - q, q & 1, gj0, ny, cx, cy);
+        split_half_sweep<T, RX, RY>(u0, u1, f0, f1, ax0, ax1, ay0, ay1, di0, di1, q & 1, SKIP + q + 1, gj0, ny);
         __syncthreads();
     }
-    // write the tile's iterate
-    for (int k = threadIdx.x; k < TX * TY; k += blockDim.x) {
-        const int ty = k / TX, tx = k - ty * TX;
-        u_out[(size_t)(blockIdx.y * TY + ty) * nx + blockIdx.x * TX + tx] = su[(ty + H) * RX + tx + H];
+    using V = typename V2<T>::type;
+    // tile iterate, two cells per vector store
+    for (int k = threadIdx.x; k < TYY * (TXX / 2); k += blockDim.x) {
+        const int ty = k / (TXX / 2), t = k - ty * (TXX / 2);
+        const int sy = H + ty, idx = sy * RXh + H / 2 + t;
+        const int c0 = (sy + gj0) & 1;
+        V v;
+        v.x = (c0 ? u1 : u0)[idx];
+        v.y = (c0 ? u0 : u1)[idx];
+        *reinterpret_cast<V*>(u_out + (size_t)(blockIdx.y * TYY + ty) * nx + blockIdx.x * TXX + 2 * t) = v;
     }
     // residual of the 4 children of each coarse cell and their average
     const int ncx = nx >> 1;
-    for (int k = threadIdx.x; k < (TX / 2) * (TY / 2); k += blockDim.x) {
-        const int cj = k / (TX / 2), ci = k - cj * (TX / 2);
-        T r[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int sx = H + 2 * ci + (q & 1), sy = H + 2 * cj + (q >> 1);
-            const int j = gj0 + sy;
-            const Stencil<T> st = stencil(su, sbx, sby, RX, sx, sy, j, ny, cx, cy);
-            r[q] = sf[sy * RX + sx] - (st.s - st.d * su[sy * RX + sx]);
-        }
-        const T fc = T(0.25) * ((r[0] + r[1]) + (r[2] + r[3]));
-        fc_out[(size_t)(blockIdx.y * (TY / 2) + cj) * ncx + blockIdx.x * (TX / 2) + ci] = fc;
+    for (int k = threadIdx.x; k < (TXX / 2) * (TYY / 2); k += blockDim.x) {
+        const int cj = k / (TXX / 2), ci = k - cj * (TXX / 2);
+        const int sx = H + 2 * ci, sy = H + 2 * cj;
+        const T r00 = split_residual<T, RXh>(u0, u1, f0, f1, ax0, ax1, ay0, ay1, sx, sy, gj0);
+        const T r10 = split_residual<T, RXh>(u0, u1, f0, f1, ax0, ax1, ay0, ay1, sx + 1, sy, gj0);
+        const T r01 = split_residual<T, RXh>(u0, u1, f0, f1, ax0, ax1, ay0, ay1, sx, sy + 1, gj0);
+        const T r11 = split_residual<T, RXh>(u0, u1, f0, f1, ax0, ax1, ay0, ay1, sx + 1, sy + 1, gj0);
+        const T fcv = T(0.25) * ((r00 + r10) + (r01 + r11));
+        fc_out[(size_t)(blockIdx.y * (TYY / 2) + cj) * ncx + blockIdx.x * (TXX / 2) + ci] = fcv;
     }
 }
 
 // ------------------------------------------------------------------------------------
-// k_up: u += P uc (piecewise constant), nu2 sweeps black-then-red; at level 0 also the
-// partial of r.z (r = f of level 0, z = u) and, in the last block, beta = rz/rz_prev.
+// k_up: u = u_pre + P uc (piecewise constant), nu2 sweeps black-then-red, written to
+// u_post (out of place: no block reads a tile another block has updated); at level 0
+// also the r.z partial (r = f of level 0, z = u) and, in the last block, beta.
 // ------------------------------------------------------------------------------------
-// Out of place: reads the pre-smoothed iterate u_pre (with halo) and writes u_post, so no
-// block ever reads a neighbour's tile after that neighbour has updated it.
-template <typename T, int NSW, bool LEVEL0>
-__global__ void __launch_bounds__(NT) k_up(const T* __restrict__ u, T* __restrict__ u_post, const T* __restrict__ uc,
-                                           const T* __restrict__ f, const T* __restrict__ bx,
-                                           const T* __restrict__ by, int nx, int ny, T cx, T cy,
-                                           State* __restrict__ st, double* __restrict__ partials) {
-    constexpr int H = 2 * NSW;
-    constexpr int RX = TX + 2 * H, RY = TY + 2 * H;
+template <typename T, int NSW, int TXX, int TYY, bool LEVEL0>
+__global__ void __launch_bounds__(NTG, 2) k_up(const T* __restrict__ u_pre, T* __restrict__ u_post,
+                                               const T* __restrict__ uc, const T* __restrict__ f,
+                                               const T* __restrict__ ax, const T* __restrict__ ay,
+                                               const T* __restrict__ dinv, int nx, int ny, State* __restrict__ st,
+                                               double* __restrict__ partials) {
+    using C = GridCfg<T, NSW, TXX, TYY, false>;
+    constexpr int H = C::H, RX = C::RX, RY = C::RY, RXh = C::RXh, ARR = C::ARR, SKIP = C::H - C::HMIN;
+    using V = typename V2<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* su = reinterpret_cast<T*>(smem_raw);
-    T* sf = su + RX * RY;
-    T* sbx = sf + RX * RY;
-    T* sby = sbx + (RX + 1) * RY;
     __shared__ double red[32];
-    const int gi0 = blockIdx.x * TX - H, gj0 = blockIdx.y * TY - H;
+    T* sm = reinterpret_cast<T*>(smem_raw);
+    T* const u0 = sm;
+    T* const u1 = sm + ARR;
+    T* const f0 = sm + 2 * ARR;
+    T* const f1 = sm + 3 * ARR;
+    T* const ax0 = sm + 4 * ARR;
+    T* const ax1 = sm + 5 * ARR;
+    T* const ay0 = sm + 6 * ARR;
+    T* const ay1 = sm + 7 * ARR;
+    T* const di0 = sm + 8 * ARR;
+    T* const di1 = sm + 9 * ARR;
+    const int gi0 = blockIdx.x * TXX - H, gj0 = blockIdx.y * TYY - H;
     const int ncx = nx >> 1;
-    for (int k = threadIdx.x; k < RX * RY; k += blockDim.x) {
-        const int sy = k / RX, sx = k - sy * RX;
+    load_split<T, RX, RY>(f0, f1, f, nx, ny, gi0, gj0);
+    load_split<T, RX, RY>(ax0, ax1, ax, nx, ny, gi0, gj0);
+    load_split<T, RX, RY>(ay0, ay1, ay, nx, ny + 1, gi0, gj0);
+    load_split<T, RX, RY>(di0, di1, dinv, nx, ny, gi0, gj0);
+    for (int k = threadIdx.x; k < ARR; k += blockDim.x) {
+        const int sy = k / RXh, m = k - sy * RXh;
         const int j = gj0 + sy;
-        int i = gi0 + sx;
+        int i = gi0 + 2 * m;
         if (i < 0) i += nx; else if (i >= nx) i -= nx;
-        T v = T(0);
+        V v;
+        v.x = T(0);
+        v.y = T(0);
         if (j >= 0 && j < ny) {
-            v = u[(size_t)j * nx + i];
-            v += uc[(size_t)(j >> 1) * ncx + (i >> 1)];
+            v = *reinterpret_cast<const V*>(u_pre + (size_t)j * nx + i);
+            const T e = uc[(size_t)(j >> 1) * ncx + (i >> 1)];
+            v.x += e;
+            v.y += e;
         }
-        su[k] = v;
+        if ((sy + gj0) & 1) {
+            u1[k] = v.x;
+            u0[k] = v.y;
+        } else {
+            u0[k] = v.x;
+            u1[k] = v.y;
+        }
     }
-    load_region(sf, RX, RY, f, nx, ny, gi0, gj0);
-    load_region(sbx, RX + 1, RY, bx, nx, ny, gi0, gj0);
-    load_region(sby, RX, RY + 1, by, nx, ny + 1, gi0, gj0);
+    async_wait_all();
     __syncthreads();
 #pragma unroll 1
     for (int q = 0; q < 2 * NSW; ++q) {
-        half_sweep(su, sf, sbx, sby, RX, q + 1, RX - 1 - q, RY - 1 - q, 1 - (q & 1), gj0, ny, cx, cy);
+        split_half_sweep<T, RX, RY>(u0, u1, f0, f1, ax0, ax1, ay0, ay1, di0, di1, 1 - (q & 1), SKIP + q + 1, gj0,
+                                    ny);
         __syncthreads();
     }
     double acc = 0.0;
-    for (int k = threadIdx.x; k < TX * TY; k += blockDim.x) {
-        const int ty = k / TX, tx = k - ty * TX;
-        const T z = su[(ty + H) * RX + tx + H];
-        u_post[(size_t)(blockIdx.y * TY + ty) * nx + blockIdx.x * TX + tx] = z;
-        if (LEVEL0) acc += double(sf[(ty + H) * RX + tx + H]) * double(z);
+    for (int k = threadIdx.x; k < TYY * (TXX / 2); k += blockDim.x) {
+        const int ty = k / (TXX / 2), t = k - ty * (TXX / 2);
+        const int sy = H + ty, idx = sy * RXh + H / 2 + t;
+        const int c0 = (sy + gj0) & 1;
+        V v;
+        v.x = (c0 ? u1 : u0)[idx];
+        v.y = (c0 ? u0 : u1)[idx];
+        *reinterpret_cast<V*>(u_post + (size_t)(blockIdx.y * TYY + ty) * nx + blockIdx.x * TXX + 2 * t) = v;
+        if (LEVEL0) {
+            acc += double((c0 ? f1 : f0)[idx]) * double(v.x);
+            acc += double((c0 ? f0 : f1)[idx]) * double(v.y);
+        }
     }
     if (LEVEL0) {
         const double b = block_sum(acc, red);
@@ -234,51 +345,91 @@ __global__ void __launch_bounds__(NT) k_up(const T* __restrict__ u, T* __restric
 }
 
 // ------------------------------------------------------------------------------------
-// CG kernels (FP64 vectors)
+// CG kernels (FP64 vectors) on TX x TY tiles with a 2-cell halo (one ring is used; the
+// second keeps every row segment an aligned vector load).
 // ------------------------------------------------------------------------------------
-// p_new = z + beta*p_old on the tile and a one-cell ring, then p_new.(A p_new) over the
-// tile; the last block sets alpha = rz / p.Ap.  p ping-pongs between two buffers chosen
-// on the device by the iteration parity (p_old = pp[it&1], p_new = pp[(it+1)&1]), so the
-// halo is always read from a buffer no block of this launch writes.
+constexpr int PH = 2, PRX = TX + 2 * PH, PRY = TY + 2 * PH;
+
+// Issues the copies of a (PRY x PRX) region of a row-major array into s (x periodic,
+// rows outside [0, nrows) zero), one pair of cells (8 or 16 bytes) per copy.
+// Completion: async_wait_all + barrier.
+template <typename TG>
+__device__ __forceinline__ void load_plain(TG* __restrict__ s, const TG* __restrict__ g, int nx, int nrows, int gi0,
+                                           int gj0) {
+    for (int k = threadIdx.x; k < PRY * (PRX / 2); k += blockDim.x) {
+        const int sy = k / (PRX / 2), m = k - sy * (PRX / 2);
+        const int j = gj0 + sy;
+        int i = gi0 + 2 * m;
+        if (i < 0) i += nx; else if (i >= nx) i -= nx;
+        const bool ok = (j >= 0 && j < nrows);
+        const TG* src = ok ? g + (size_t)j * nx + i : g;
+        const unsigned d = (unsigned)__cvta_generic_to_shared(s + sy * PRX + 2 * m);
+        if (sizeof(TG) == 8) {
+            const int n = ok ? 16 : 0;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+        } else {
+            const int n = ok ? 8 : 0;
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+        }
+    }
+}
+
+__device__ __forceinline__ void plain_sums(const double* su, const double* sax, const double* say, int sx, int sy,
+                                           double& s, double& d) {
+    const int c = sy * PRX + sx;
+    const double aw = sax[c], ae = sax[c + 1], as = say[c], an = say[c + PRX];
+    double ss = aw * su[c - 1];
+    ss += ae * su[c + 1];
+    ss += as * su[c - PRX];
+    ss += an * su[c + PRX];
+    double dd = aw;
+    dd += ae;
+    dd += as;
+    dd += an;
+    s = ss;
+    d = dd;
+}
+
+constexpr int PAREA = PRX * PRY;
+
+// p_new = z + beta*p_old on the tile and a ring, then p_new.(A p_new) over the tile; the
+// last block sets alpha = rz / p.Ap.  p ping-pongs between two buffers chosen on the
+// device by the iteration parity (p_old = pp[it&1], p_new = pp[(it+1)&1]), so the halo is
+// always read from a buffer no block of this launch writes.
 template <typename TZ>
 __global__ void __launch_bounds__(NT) k_pupdate(double* __restrict__ p0, double* __restrict__ p1,
-                                                const TZ* __restrict__ z, const double* __restrict__ bx,
-                                                const double* __restrict__ by, int nx, int ny, double cx, double cy,
+                                                const TZ* __restrict__ z, const double* __restrict__ ax,
+                                                const double* __restrict__ ay, int nx, int ny,
                                                 State* __restrict__ st, double* __restrict__ partials) {
-    constexpr int H = 1, RX = TX + 2, RY = TY + 2;
-    __shared__ double sp[RX * RY];
-    __shared__ double sbx[(RX + 1) * RY];
-    __shared__ double sby[RX * (RY + 1)];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* sp = reinterpret_cast<double*>(smem_raw);
+    double* sax = sp + PAREA;
+    double* say = sax + PAREA;
+    TZ* sz = reinterpret_cast<TZ*>(say + PAREA);
     __shared__ double red[32];
-    const int gi0 = blockIdx.x * TX - H, gj0 = blockIdx.y * TY - H;
-    const double beta = st->beta;
+    const int gi0 = blockIdx.x * TX - PH, gj0 = blockIdx.y * TY - PH;
     const int par = st->it & 1;
     const double* __restrict__ p = par ? p1 : p0;
     double* __restrict__ pn = par ? p0 : p1;
-    for (int k = threadIdx.x; k < RX * RY; k += blockDim.x) {
-        const int sy = k / RX, sx = k - sy * RX;
-        const int j = gj0 + sy;
-        int i = gi0 + sx;
-        if (i < 0) i += nx; else if (i >= nx) i -= nx;
-        double v = 0.0;
-        if (j >= 0 && j < ny) {
-            const size_t g = (size_t)j * nx + i;
-            v = double(z[g]) + beta * p[g];
-        }
-        sp[k] = v;
-    }
-    load_region(sbx, RX + 1, RY, bx, nx, ny, gi0, gj0);
-    load_region(sby, RX, RY + 1, by, nx, ny + 1, gi0, gj0);
+    load_plain(sp, p, nx, ny, gi0, gj0);
+    load_plain(sz, z, nx, ny, gi0, gj0);
+    load_plain(sax, ax, nx, ny, gi0, gj0);
+    load_plain(say, ay, nx, ny + 1, gi0, gj0);
+    const double beta = st->beta;
+    async_wait_all();
+    __syncthreads();
+    for (int k = threadIdx.x; k < PAREA; k += blockDim.x) sp[k] = double(sz[k]) + beta * sp[k];
     __syncthreads();
     double acc = 0.0;
     for (int k = threadIdx.x; k < TX * TY; k += blockDim.x) {
         const int ty = k / TX, tx = k - ty * TX;
-        const int sx = tx + H, sy = ty + H, j = gj0 + sy;
-        const Stencil<double> s = stencil(sp, sbx, sby, RX, sx, sy, j, ny, cx, cy);
-        const double pv = sp[sy * RX + sx];
-        const double q = s.s - s.d * pv;
+        const int sx = tx + PH, sy = ty + PH;
+        double s, d;
+        plain_sums(sp, sax, say, sx, sy, s, d);
+        const double pv = sp[sy * PRX + sx];
+        const double q = s - d * pv;
         acc += pv * q;
-        pn[(size_t)j * nx + blockIdx.x * TX + tx] = pv;
+        pn[(size_t)(blockIdx.y * TY + ty) * nx + blockIdx.x * TX + tx] = pv;
     }
     const double b = block_sum(acc, red);
     double tot;
@@ -293,46 +444,44 @@ __global__ void __launch_bounds__(NT) k_pupdate(double* __restrict__ p0, double*
 template <typename TR>
 __global__ void __launch_bounds__(NT) k_xupdate(double* __restrict__ x0, double* __restrict__ x1,
                                                 const double* __restrict__ p0, const double* __restrict__ p1,
-                                                const double* __restrict__ f, const double* __restrict__ bx,
-                                                const double* __restrict__ by, TR* __restrict__ r_out, int nx, int ny,
-                                                double cx, double cy, State* __restrict__ st,
-                                                double* __restrict__ partials, int first,
+                                                const double* __restrict__ f, const double* __restrict__ ax,
+                                                const double* __restrict__ ay, TR* __restrict__ r_out, int nx, int ny,
+                                                State* __restrict__ st, double* __restrict__ partials, int first,
                                                 cudaGraphConditionalHandle cond, int use_cond) {
-    constexpr int H = 1, RX = TX + 2, RY = TY + 2;
-    __shared__ double sxv[RX * RY];
-    __shared__ double sbx[(RX + 1) * RY];
-    __shared__ double sby[RX * (RY + 1)];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* sxv = reinterpret_cast<double*>(smem_raw);
+    double* spv = sxv + PAREA;
+    double* sax = spv + PAREA;
+    double* say = sax + PAREA;
+    double* sf = say + PAREA;
     __shared__ double red[32];
-    const int gi0 = blockIdx.x * TX - H, gj0 = blockIdx.y * TY - H;
-    const double alpha = first ? 0.0 : st->alpha;
+    const int gi0 = blockIdx.x * TX - PH, gj0 = blockIdx.y * TY - PH;
     const int par = first ? 0 : (st->it & 1);
     const double* __restrict__ x = par ? x1 : x0;
     double* __restrict__ xn = par ? x0 : x1;
     const double* __restrict__ p = par ? p0 : p1;
-    for (int k = threadIdx.x; k < RX * RY; k += blockDim.x) {
-        const int sy = k / RX, sx = k - sy * RX;
-        const int j = gj0 + sy;
-        int i = gi0 + sx;
-        if (i < 0) i += nx; else if (i >= nx) i -= nx;
-        double v = 0.0;
-        if (j >= 0 && j < ny) {
-            const size_t g = (size_t)j * nx + i;
-            v = first ? x[g] : x[g] + alpha * p[g];
-        }
-        sxv[k] = v;
-    }
-    load_region(sbx, RX + 1, RY, bx, nx, ny, gi0, gj0);
-    load_region(sby, RX, RY + 1, by, nx, ny + 1, gi0, gj0);
+    load_plain(sxv, x, nx, ny, gi0, gj0);
+    if (!first) load_plain(spv, p, nx, ny, gi0, gj0);
+    load_plain(sax, ax, nx, ny, gi0, gj0);
+    load_plain(say, ay, nx, ny + 1, gi0, gj0);
+    load_plain(sf, f, nx, ny, gi0, gj0);
+    const double alpha = first ? 0.0 : st->alpha;
+    async_wait_all();
     __syncthreads();
+    if (!first) {
+        for (int k = threadIdx.x; k < PAREA; k += blockDim.x) sxv[k] = sxv[k] + alpha * spv[k];
+        __syncthreads();
+    }
     double acc = 0.0, accf = 0.0;
     for (int k = threadIdx.x; k < TX * TY; k += blockDim.x) {
         const int ty = k / TX, tx = k - ty * TX;
-        const int sx = tx + H, sy = ty + H, j = gj0 + sy;
-        const size_t g = (size_t)j * nx + blockIdx.x * TX + tx;
-        const Stencil<double> s = stencil(sxv, sbx, sby, RX, sx, sy, j, ny, cx, cy);
-        const double xv = sxv[sy * RX + sx];
-        const double fv = f[g];
-        const double r = fv - (s.s - s.d * xv);
+        const int sx = tx + PH, sy = ty + PH;
+        const size_t g = (size_t)(blockIdx.y * TY + ty) * nx + blockIdx.x * TX + tx;
+        double s, d;
+        plain_sums(sxv, sax, say, sx, sy, s, d);
+        const double xv = sxv[sy * PRX + sx];
+        const double fv = sf[sy * PRX + sx];
+        const double r = fv - (s - d * xv);
         acc += r * r;
         if (first) accf += fv * fv;
         if (!first) xn[g] = xv;
@@ -341,7 +490,7 @@ __global__ void __launch_bounds__(NT) k_xupdate(double* __restrict__ x0, double*
     const double b = block_sum(acc, red);
     const double bf = first ? block_sum(accf, red) : 0.0;
     double tot;
-    // first launch: two sums (||r||^2 then ||f||^2) through two passes of the counter
+    // first launch: two sums (||f||^2 through counter 3, then ||r||^2 through counter 2)
     if (first) {
         if (grid_sum_last(bf, partials + gridDim.x * gridDim.y, &st->cnt[3], &tot, red)) st->sums[1] = tot;
     }
@@ -368,16 +517,22 @@ __global__ void __launch_bounds__(NT) k_xupdate(double* __restrict__ x0, double*
     }
 }
 
+template <typename TZ>
+constexpr size_t pupdate_smem() {
+    return sizeof(double) * 3 * PAREA + sizeof(TZ) * PAREA;
+}
+constexpr size_t xupdate_smem() { return sizeof(double) * 5 * PAREA; }
+
 // ------------------------------------------------------------------------------------
 // Single-CTA coarse part: outer levels [lcta, lc) in T, the coarsest outer level lc and
 // the inner levels in FP64, all in shared memory.
 // ------------------------------------------------------------------------------------
 struct CtaLevel {
     int nx, ny;
-    double cx, cy;
-    unsigned off_u, off_f, off_bx, off_by;  // byte offsets into dynamic smem
-    const void* gbx;                        // beta of this level in global memory (T or double)
-    const void* gby;
+    unsigned off_u, off_f, off_ax, off_ay, off_di;  // byte offsets into dynamic smem
+    const void* gax;                                // AX, AY, DINV of this level (T or double)
+    const void* gay;
+    const void* gdi;
 };
 
 struct CtaParams {
@@ -393,10 +548,10 @@ template <typename E>
 struct SL {
     E* u;
     E* f;
-    E* bx;
-    E* by;
+    E* ax;
+    E* ay;
+    E* di;
     int nx, ny;
-    E cx, cy;
 };
 
 template <typename E>
@@ -405,12 +560,11 @@ __device__ __forceinline__ SL<E> make_sl(const CtaParams& P, unsigned char* sm, 
     SL<E> s;
     s.u = reinterpret_cast<E*>(sm + L.off_u);
     s.f = reinterpret_cast<E*>(sm + L.off_f);
-    s.bx = reinterpret_cast<E*>(sm + L.off_bx);
-    s.by = reinterpret_cast<E*>(sm + L.off_by);
+    s.ax = reinterpret_cast<E*>(sm + L.off_ax);
+    s.ay = reinterpret_cast<E*>(sm + L.off_ay);
+    s.di = reinterpret_cast<E*>(sm + L.off_di);
     s.nx = L.nx;
     s.ny = L.ny;
-    s.cx = E(L.cx);
-    s.cy = E(L.cy);
     return s;
 }
 
@@ -428,10 +582,10 @@ __device__ __forceinline__ void s_sums(const SL<E>& L, int i, int j, E& s, E& d)
     const int nx = L.nx, ny = L.ny;
     const int ip = (i + 1 == nx) ? 0 : i + 1;
     const int im = (i == 0) ? nx - 1 : i - 1;
-    const E aw = L.cx * L.bx[j * nx + i];
-    const E ae = L.cx * L.bx[j * nx + ip];
-    const E as = (j > 0) ? L.cy * L.by[j * nx + i] : E(0);
-    const E an = (j < ny - 1) ? L.cy * L.by[(j + 1) * nx + i] : (E(2) * L.cy) * L.by[ny * nx + i];
+    const E aw = L.ax[j * nx + i];
+    const E ae = L.ax[j * nx + ip];
+    const E as = L.ay[j * nx + i];
+    const E an = L.ay[(j + 1) * nx + i];
     const E uw = L.u[j * nx + im], ue = L.u[j * nx + ip];
     const E us = (j > 0) ? L.u[(j - 1) * nx + i] : E(0);
     const E un = (j < ny - 1) ? L.u[(j + 1) * nx + i] : E(0);
@@ -457,7 +611,7 @@ __device__ void s_sweeps(const SL<E>& L, int nsw, bool reverse) {
             const int i = 2 * m + ((j + colour) & 1);
             E s, d;
             s_sums(L, i, j, s, d);
-            L.u[j * L.nx + i] = (s - L.f[j * L.nx + i]) / d;
+            L.u[j * L.nx + i] = (s - L.f[j * L.nx + i]) * L.di[j * L.nx + i];
         }
         g_sync<W>();
     }
@@ -503,10 +657,10 @@ __device__ void s_dense(const SL<double>& L, double* A, double* b) {
     for (int row = g_tid<W>(); row < n; row += g_nthr<W>()) {
         const int j = row / nx, i = row - j * nx;
         const int ip = (i + 1 == nx) ? 0 : i + 1, im = (i == 0) ? nx - 1 : i - 1;
-        const double aw = L.cx * L.bx[j * nx + i];
-        const double ae = L.cx * L.bx[j * nx + ip];
-        const double as = (j > 0) ? L.cy * L.by[j * nx + i] : 0.0;
-        const double an = (j < ny - 1) ? L.cy * L.by[(j + 1) * nx + i] : (2.0 * L.cy) * L.by[ny * nx + i];
+        const double aw = L.ax[j * nx + i];
+        const double ae = L.ax[j * nx + ip];
+        const double as = L.ay[j * nx + i];
+        const double an = L.ay[(j + 1) * nx + i];
         double d = aw;
         d += ae;
         d += as;
@@ -625,19 +779,23 @@ __global__ void __launch_bounds__(NT_CTA, 1) k_cta(const __grid_constant__ CtaPa
         const CtaLevel& L = P.lv[l];
         const int n = L.nx * L.ny, nb = L.nx * (L.ny + 1);
         if (l < P.lc) {
-            T* bx = reinterpret_cast<T*>(sm + L.off_bx);
-            T* by = reinterpret_cast<T*>(sm + L.off_by);
-            const T* gbx = reinterpret_cast<const T*>(L.gbx);
-            const T* gby = reinterpret_cast<const T*>(L.gby);
-            for (int k = threadIdx.x; k < n; k += blockDim.x) bx[k] = gbx[k];
-            for (int k = threadIdx.x; k < nb; k += blockDim.x) by[k] = gby[k];
+            T* ax = reinterpret_cast<T*>(sm + L.off_ax);
+            T* ay = reinterpret_cast<T*>(sm + L.off_ay);
+            T* di = reinterpret_cast<T*>(sm + L.off_di);
+            const T* gax = reinterpret_cast<const T*>(L.gax);
+            const T* gay = reinterpret_cast<const T*>(L.gay);
+            const T* gdi = reinterpret_cast<const T*>(L.gdi);
+            for (int k = threadIdx.x; k < n; k += blockDim.x) { ax[k] = gax[k]; di[k] = gdi[k]; }
+            for (int k = threadIdx.x; k < nb; k += blockDim.x) ay[k] = gay[k];
         } else {
-            double* bx = reinterpret_cast<double*>(sm + L.off_bx);
-            double* by = reinterpret_cast<double*>(sm + L.off_by);
-            const double* gbx = reinterpret_cast<const double*>(L.gbx);
-            const double* gby = reinterpret_cast<const double*>(L.gby);
-            for (int k = threadIdx.x; k < n; k += blockDim.x) bx[k] = gbx[k];
-            for (int k = threadIdx.x; k < nb; k += blockDim.x) by[k] = gby[k];
+            double* ax = reinterpret_cast<double*>(sm + L.off_ax);
+            double* ay = reinterpret_cast<double*>(sm + L.off_ay);
+            double* di = reinterpret_cast<double*>(sm + L.off_di);
+            const double* gax = reinterpret_cast<const double*>(L.gax);
+            const double* gay = reinterpret_cast<const double*>(L.gay);
+            const double* gdi = reinterpret_cast<const double*>(L.gdi);
+            for (int k = threadIdx.x; k < n; k += blockDim.x) { ax[k] = gax[k]; di[k] = gdi[k]; }
+            for (int k = threadIdx.x; k < nb; k += blockDim.x) ay[k] = gay[k];
         }
     }
     {
@@ -690,6 +848,35 @@ __global__ void k_coarsen_beta(const T* __restrict__ bxf, const T* __restrict__ 
     }
 }
 
+// AX = cx*bx; AY = cy*by inside, 0 on the bottom wall row, (2*cy)*by on the top wall row;
+// DINV = 1/d with d = ((aw + ae) + as) + an, the diagonal the oracle forms per update.
+template <typename T>
+__global__ void k_scale_beta(const T* __restrict__ bx, const T* __restrict__ by, T* __restrict__ ax,
+                             T* __restrict__ ay, T* __restrict__ dinv, int nx, int ny, T cx, T cy) {
+    const size_t n = (size_t)nx * ny, nb = n + nx;
+    const T cy2 = T(2) * cy;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n + nb; k += (size_t)gridDim.x * blockDim.x) {
+        if (k < n) {
+            const size_t j = k / nx, i = k - j * nx;
+            const size_t ip = (i + 1 == (size_t)nx) ? 0 : i + 1;
+            const T aw = cx * bx[k];
+            const T ae = cx * bx[j * nx + ip];
+            const T as = (j > 0) ? cy * by[k] : T(0);
+            const T an = (j + 1 < (size_t)ny) ? cy * by[k + nx] : cy2 * by[k + nx];
+            T d = aw;
+            d += ae;
+            d += as;
+            d += an;
+            ax[k] = aw;
+            dinv[k] = T(1) / d;
+        } else {
+            const size_t kk = k - n;
+            const size_t j = kk / nx;
+            ay[kk] = (j == 0) ? T(0) : ((j == (size_t)ny) ? cy2 * by[kk] : cy * by[kk]);
+        }
+    }
+}
+
 __global__ void k_to_float(const double* __restrict__ a, float* __restrict__ b, size_t n) {
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
         b[k] = float(a[k]);
@@ -710,22 +897,23 @@ __global__ void k_widen(const float* __restrict__ a, double* __restrict__ b, siz
 
 // out = A u (FP64), the operator of the oracle's apply: out = s - d*u.
 __global__ void __launch_bounds__(NT) k_apply(double* __restrict__ out, const double* __restrict__ u,
-                                              const double* __restrict__ bx, const double* __restrict__ by, int nx,
-                                              int ny, double cx, double cy) {
-    constexpr int H = 1, RX = TX + 2, RY = TY + 2;
-    __shared__ double su[RX * RY];
-    __shared__ double sbx[(RX + 1) * RY];
-    __shared__ double sby[RX * (RY + 1)];
-    const int gi0 = blockIdx.x * TX - H, gj0 = blockIdx.y * TY - H;
-    load_region(su, RX, RY, u, nx, ny, gi0, gj0);
-    load_region(sbx, RX + 1, RY, bx, nx, ny, gi0, gj0);
-    load_region(sby, RX, RY + 1, by, nx, ny + 1, gi0, gj0);
+                                              const double* __restrict__ ax, const double* __restrict__ ay, int nx,
+                                              int ny) {
+    __shared__ __align__(16) double su[PRX * PRY];
+    __shared__ __align__(16) double sax[PRX * PRY];
+    __shared__ __align__(16) double say[PRX * PRY];
+    const int gi0 = blockIdx.x * TX - PH, gj0 = blockIdx.y * TY - PH;
+    load_plain(su, u, nx, ny, gi0, gj0);
+    load_plain(sax, ax, nx, ny, gi0, gj0);
+    load_plain(say, ay, nx, ny + 1, gi0, gj0);
+    async_wait_all();
     __syncthreads();
     for (int k = threadIdx.x; k < TX * TY; k += blockDim.x) {
         const int ty = k / TX, tx = k - ty * TX;
-        const int sx = tx + H, sy = ty + H, j = gj0 + sy;
-        const Stencil<double> s = stencil(su, sbx, sby, RX, sx, sy, j, ny, cx, cy);
-        out[(size_t)j * nx + blockIdx.x * TX + tx] = s.s - s.d * su[sy * RX + sx];
+        const int sx = tx + PH, sy = ty + PH;
+        double s, d;
+        plain_sums(su, sax, say, sx, sy, s, d);
+        out[(size_t)(blockIdx.y * TY + ty) * nx + blockIdx.x * TX + tx] = s - d * su[sy * PRX + sx];
     }
 }
 
@@ -766,10 +954,17 @@ struct LevelBuf {
     void* u = nullptr;      // T: iterate after pre-smoothing (k_down), or the CTA kernel's output
     void* up = nullptr;     // T: iterate after correction and post-smoothing (k_up)
     void* f = nullptr;      // T
-    double* bx64 = nullptr;  // FP64 beta chain (level 0: the caller's arrays)
+    double* bx64 = nullptr;  // FP64 face beta (level 0: the caller's arrays), coarsened level by level
     double* by64 = nullptr;
-    float* bx32 = nullptr;   // FP32 beta chain (mixed)
+    float* bx32 = nullptr;   // FP32 face beta (mixed), coarsened in FP32
     float* by32 = nullptr;
+    double* ax64 = nullptr;  // pre-scaled stencil weights AX, AY and reciprocal diagonal (k_scale_beta)
+    double* ay64 = nullptr;
+    double* di64 = nullptr;
+    float* ax32 = nullptr;
+    float* ay32 = nullptr;
+    float* di32 = nullptr;
+    bool big = false;        // grid kernels on 64x32 tiles (else 32x32)
 };
 
 struct lica_mg {
@@ -855,78 +1050,100 @@ void prof_collect(lica_mg* m) {
     m->prof_pending.clear();
 }
 
-template <typename T, int NSW>
-size_t grid_smem(bool down) {
-    const int H = down ? 2 * NSW + 1 : 2 * NSW;
-    const int RX = TX + 2 * H, RY = TY + 2 * H;
-    return sizeof(T) * (size_t)(2 * RX * RY + (RX + 1) * RY + RX * (RY + 1));
+template <typename T>
+const T* lvl_ax(const LevelBuf& L) {
+    return std::is_same<T, float>::value ? (const T*)L.ax32 : (const T*)L.ax64;
+}
+template <typename T>
+const T* lvl_ay(const LevelBuf& L) {
+    return std::is_same<T, float>::value ? (const T*)L.ay32 : (const T*)L.ay64;
+}
+template <typename T>
+const T* lvl_di(const LevelBuf& L) {
+    return std::is_same<T, float>::value ? (const T*)L.di32 : (const T*)L.di64;
+}
+
+template <typename T, int NS, int TXX, int TYY>
+int set_attrs_tile() {
+    LICA_CUDA_TRY(cudaFuncSetAttribute(k_down<T, NS, TXX, TYY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)GridCfg<T, NS, TXX, TYY, true>::SMEM));
+    LICA_CUDA_TRY(cudaFuncSetAttribute(k_up<T, NS, TXX, TYY, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)GridCfg<T, NS, TXX, TYY, false>::SMEM));
+    LICA_CUDA_TRY(cudaFuncSetAttribute(k_up<T, NS, TXX, TYY, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)GridCfg<T, NS, TXX, TYY, false>::SMEM));
+    return LICA_OK;
 }
 
 template <typename T>
 int set_smem_attrs(int nsw) {
-    // the kernels are instantiated for NSW = 1, 2, 3
-#define LICA_SET(NS)                                                                                            \
-    LICA_CUDA_TRY(cudaFuncSetAttribute(k_down<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,              \
-                                       (int)grid_smem<T, NS>(true)));                                          \
-    LICA_CUDA_TRY(cudaFuncSetAttribute(k_up<T, NS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
-                                       (int)grid_smem<T, NS>(false)));                                         \
-    LICA_CUDA_TRY(cudaFuncSetAttribute(k_up<T, NS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,          \
-                                       (int)grid_smem<T, NS>(false)));
-    if (nsw == 1) { LICA_SET(1) }
-    else if (nsw == 2) { LICA_SET(2) }
-    else { LICA_SET(3) }
-#undef LICA_SET
+    int st;
+    switch (nsw) {
+        case 1: if ((st = set_attrs_tile<T, 1, 32, 32>()) || (st = set_attrs_tile<T, 1, 64, 32>())) return st; break;
+        case 2: if ((st = set_attrs_tile<T, 2, 32, 32>()) || (st = set_attrs_tile<T, 2, 64, 32>())) return st; break;
+        default: if ((st = set_attrs_tile<T, 3, 32, 32>()) || (st = set_attrs_tile<T, 3, 64, 32>())) return st; break;
+    }
     return LICA_OK;
+}
+
+template <typename T, int NS, int TXX, int TYY>
+void down_tile(const LevelBuf& L, const LevelBuf& C, cudaStream_t s) {
+    dim3 grid(L.nx / TXX, L.ny / TYY);
+    k_down<T, NS, TXX, TYY><<<grid, NTG, GridCfg<T, NS, TXX, TYY, true>::SMEM, s>>>(
+        (const T*)L.f, lvl_ax<T>(L), lvl_ay<T>(L), lvl_di<T>(L), (T*)L.u, (T*)C.f, L.nx, L.ny);
+}
+
+template <typename T, int NS>
+void down_ns(const LevelBuf& L, const LevelBuf& C, cudaStream_t s) {
+    if (L.big) down_tile<T, NS, 64, 32>(L, C, s);
+    else down_tile<T, NS, 32, 32>(L, C, s);
 }
 
 template <typename T>
 int launch_down(lica_mg* m, int l, cudaStream_t s) {
     LevelBuf& L = m->lv[l];
     LevelBuf& C = m->lv[l + 1];
-    const T* bx = std::is_same<T, float>::value ? (const T*)L.bx32 : (const T*)L.bx64;
-    const T* by = std::is_same<T, float>::value ? (const T*)L.by32 : (const T*)L.by64;
-    dim3 grid(L.nx / TX, L.ny / TY);
-    const T* f = (const T*)L.f;
-    T* u = (T*)L.u;
-    T* fc = (T*)C.f;
-    const T cx = T(L.cx), cy = T(L.cy);
     ProfScope ps(m, l == 0 ? LICA_MG_DOWN0 : LICA_MG_DOWN, s);
     switch (m->o.nu1) {
-        case 1: k_down<T, 1><<<grid, NT, grid_smem<T, 1>(true), s>>>(f, bx, by, u, fc, L.nx, L.ny, cx, cy); break;
-        case 2: k_down<T, 2><<<grid, NT, grid_smem<T, 2>(true), s>>>(f, bx, by, u, fc, L.nx, L.ny, cx, cy); break;
-        default: k_down<T, 3><<<grid, NT, grid_smem<T, 3>(true), s>>>(f, bx, by, u, fc, L.nx, L.ny, cx, cy); break;
+        case 1: down_ns<T, 1>(L, C, s); break;
+        case 2: down_ns<T, 2>(L, C, s); break;
+        default: down_ns<T, 3>(L, C, s); break;
     }
     LICA_CUDA_TRY(cudaGetLastError());
     lica_count_launches(1);
     return LICA_OK;
 }
 
+template <typename T, int NS, int TXX, int TYY>
+void up_tile(lica_mg* m, const LevelBuf& L, const T* uc, bool level0, cudaStream_t s) {
+    dim3 grid(L.nx / TXX, L.ny / TYY);
+    const size_t sm = GridCfg<T, NS, TXX, TYY, false>::SMEM;
+    if (level0)
+        k_up<T, NS, TXX, TYY, true><<<grid, NTG, sm, s>>>((const T*)L.u, (T*)L.up, uc, (const T*)L.f, lvl_ax<T>(L),
+                                                          lvl_ay<T>(L), lvl_di<T>(L), L.nx, L.ny, m->st,
+                                                          m->partials);
+    else
+        k_up<T, NS, TXX, TYY, false><<<grid, NTG, sm, s>>>((const T*)L.u, (T*)L.up, uc, (const T*)L.f, lvl_ax<T>(L),
+                                                           lvl_ay<T>(L), lvl_di<T>(L), L.nx, L.ny, m->st,
+                                                           m->partials);
+}
+
+template <typename T, int NS>
+void up_ns(lica_mg* m, const LevelBuf& L, const T* uc, bool level0, cudaStream_t s) {
+    if (L.big) up_tile<T, NS, 64, 32>(m, L, uc, level0, s);
+    else up_tile<T, NS, 32, 32>(m, L, uc, level0, s);
+}
+
 template <typename T>
 int launch_up(lica_mg* m, int l, cudaStream_t s) {
     LevelBuf& L = m->lv[l];
     LevelBuf& C = m->lv[l + 1];
-    const T* bx = std::is_same<T, float>::value ? (const T*)L.bx32 : (const T*)L.bx64;
-    const T* by = std::is_same<T, float>::value ? (const T*)L.by32 : (const T*)L.by64;
-    dim3 grid(L.nx / TX, L.ny / TY);
-    const T* u = (const T*)L.u;
-    T* up = (T*)L.up;
     const T* uc = (const T*)((l + 1 == m->lcta) ? C.u : C.up);
-    const T* f = (const T*)L.f;
-    const T cx = T(L.cx), cy = T(L.cy);
     ProfScope ps(m, l == 0 ? LICA_MG_UP0 : LICA_MG_UP, s);
-#define LICA_UP(NS)                                                                                                  \
-    if (l == 0)                                                                                                      \
-        k_up<T, NS, true><<<grid, NT, grid_smem<T, NS>(false), s>>>(u, up, uc, f, bx, by, L.nx, L.ny, cx, cy, m->st, \
-                                                                    m->partials);                                    \
-    else                                                                                                             \
-        k_up<T, NS, false><<<grid, NT, grid_smem<T, NS>(false), s>>>(u, up, uc, f, bx, by, L.nx, L.ny, cx, cy,       \
-                                                                     m->st, m->partials);
     switch (m->o.nu2) {
-        case 1: LICA_UP(1) break;
-        case 2: LICA_UP(2) break;
-        default: LICA_UP(3) break;
+        case 1: up_ns<T, 1>(m, L, uc, l == 0, s); break;
+        case 2: up_ns<T, 2>(m, L, uc, l == 0, s); break;
+        default: up_ns<T, 3>(m, L, uc, l == 0, s); break;
     }
-#undef LICA_UP
     LICA_CUDA_TRY(cudaGetLastError());
     lica_count_launches(1);
     return LICA_OK;
@@ -958,18 +1175,26 @@ int vcycle(lica_mg* m, cudaStream_t s) {
 
 int run_vcycle(lica_mg* m, cudaStream_t s) { return is_mixed(m) ? vcycle<float>(m, s) : vcycle<double>(m, s); }
 
-// Set up the beta hierarchy for caller arrays bx, by (level 0).
+// Beta hierarchy for the caller's level-0 faces bx, by: FP64 faces coarsened level by
+// level, and every level's pre-scaled weights AX, AY; in the mixed path also the FP32
+// faces (FP32 copy of level 0, coarsened in FP32) and their FP32 weights.
 int setup_beta(lica_mg* m, const double* bx, const double* by, cudaStream_t s) {
     ProfScope ps(m, LICA_MG_SETUP, s);
     m->lv[0].bx64 = const_cast<double*>(bx);
     m->lv[0].by64 = const_cast<double*>(by);
     const int nlev = (int)m->lv.size();
-    for (int l = 1; l < nlev; ++l) {
-        LevelBuf& F = m->lv[l - 1];
+    auto blocks_for = [](size_t work) { return (int)std::min<size_t>(1184, (work + 255) / 256); };
+    for (int l = 0; l < nlev; ++l) {
         LevelBuf& C = m->lv[l];
-        const int work = C.nx * C.ny + C.nx * (C.ny + 1);
-        const int blocks = std::min(1184, (work + 255) / 256);
-        k_coarsen_beta<double><<<blocks, 256, 0, s>>>(F.bx64, F.by64, C.bx64, C.by64, C.nx, C.ny);
+        const size_t work = (size_t)C.nx * C.ny * 2 + C.nx;
+        if (l > 0) {
+            LevelBuf& F = m->lv[l - 1];
+            k_coarsen_beta<double><<<blocks_for(work), 256, 0, s>>>(F.bx64, F.by64, C.bx64, C.by64, C.nx, C.ny);
+            LICA_CUDA_TRY(cudaGetLastError());
+            lica_count_launches(1);
+        }
+        k_scale_beta<double><<<blocks_for(work), 256, 0, s>>>(C.bx64, C.by64, C.ax64, C.ay64, C.di64, C.nx, C.ny,
+                                                               C.cx, C.cy);
         LICA_CUDA_TRY(cudaGetLastError());
         lica_count_launches(1);
     }
@@ -980,24 +1205,31 @@ int setup_beta(lica_mg* m, const double* bx, const double* by, cudaStream_t s) {
         k_to_float<<<1184, 256, 0, s>>>(by, L0.by32, n + L0.nx);
         LICA_CUDA_TRY(cudaGetLastError());
         lica_count_launches(2);
-        for (int l = 1; l < m->nouter - 1; ++l) {
-            LevelBuf& F = m->lv[l - 1];
+        for (int l = 0; l < m->nouter - 1; ++l) {
             LevelBuf& C = m->lv[l];
-            const int work = C.nx * C.ny + C.nx * (C.ny + 1);
-            const int blocks = std::min(1184, (work + 255) / 256);
-            k_coarsen_beta<float><<<blocks, 256, 0, s>>>(F.bx32, F.by32, C.bx32, C.by32, C.nx, C.ny);
+            const size_t work = (size_t)C.nx * C.ny * 2 + C.nx;
+            if (l > 0) {
+                LevelBuf& F = m->lv[l - 1];
+                k_coarsen_beta<float><<<blocks_for(work), 256, 0, s>>>(F.bx32, F.by32, C.bx32, C.by32, C.nx, C.ny);
+                LICA_CUDA_TRY(cudaGetLastError());
+                lica_count_launches(1);
+            }
+            k_scale_beta<float><<<blocks_for(work), 256, 0, s>>>(C.bx32, C.by32, C.ax32, C.ay32, C.di32, C.nx, C.ny,
+                                                                  float(C.cx), float(C.cy));
             LICA_CUDA_TRY(cudaGetLastError());
             lica_count_launches(1);
         }
     }
-    // beta pointers of the levels staged by the single-CTA kernel
+    // weights of the levels staged by the single-CTA kernel
     for (int l = m->lcta; l <= m->bottom; ++l) {
         if (l < m->nouter - 1 && is_mixed(m)) {
-            m->cp.lv[l].gbx = m->lv[l].bx32;
-            m->cp.lv[l].gby = m->lv[l].by32;
+            m->cp.lv[l].gax = m->lv[l].ax32;
+            m->cp.lv[l].gay = m->lv[l].ay32;
+            m->cp.lv[l].gdi = m->lv[l].di32;
         } else {
-            m->cp.lv[l].gbx = m->lv[l].bx64;
-            m->cp.lv[l].gby = m->lv[l].by64;
+            m->cp.lv[l].gax = m->lv[l].ax64;
+            m->cp.lv[l].gay = m->lv[l].ay64;
+            m->cp.lv[l].gdi = m->lv[l].di64;
         }
     }
     return LICA_OK;
@@ -1009,8 +1241,8 @@ int launch_xupdate(lica_mg* m, double* x, const double* f, int first, cudaGraphC
     LevelBuf& L = m->lv[0];
     dim3 grid(L.nx / TX, L.ny / TY);
     ProfScope ps(m, LICA_MG_XUPDATE, s);
-    k_xupdate<TR><<<grid, NT, 0, s>>>(x, m->xb, m->pcg[0], m->pcg[1], f, L.bx64, L.by64, (TR*)m->r, L.nx, L.ny,
-                                      L.cx, L.cy, m->st, m->partials, first, h, use_cond);
+    k_xupdate<TR><<<grid, NT, xupdate_smem(), s>>>(x, m->xb, m->pcg[0], m->pcg[1], f, L.ax64, L.ay64, (TR*)m->r, L.nx, L.ny,
+                                      m->st, m->partials, first, h, use_cond);
     LICA_CUDA_TRY(cudaGetLastError());
     lica_count_launches(1);
     return LICA_OK;
@@ -1021,8 +1253,8 @@ int launch_pupdate(lica_mg* m, cudaStream_t s) {
     LevelBuf& L = m->lv[0];
     dim3 grid(L.nx / TX, L.ny / TY);
     ProfScope ps(m, LICA_MG_PUPDATE, s);
-    k_pupdate<TZ><<<grid, NT, 0, s>>>(m->pcg[0], m->pcg[1], (const TZ*)m->z, L.bx64, L.by64, L.nx, L.ny, L.cx,
-                                      L.cy, m->st, m->partials);
+    k_pupdate<TZ><<<grid, NT, pupdate_smem<TZ>(), s>>>(m->pcg[0], m->pcg[1], (const TZ*)m->z, L.ax64, L.ay64, L.nx, L.ny, m->st,
+                                      m->partials);
     LICA_CUDA_TRY(cudaGetLastError());
     lica_count_launches(1);
     return LICA_OK;
@@ -1153,9 +1385,20 @@ int build_graph(lica_mg* m, double* x, const double* f, const double* bx, const 
     return LICA_OK;
 }
 
+// The kernels read two cells per 16-byte vector load: caller arrays must be 16-byte aligned.
+bool aligned16(const void* a, const void* b, const void* c, const void* d) {
+    const uintptr_t u = (uintptr_t)a | (uintptr_t)b | (uintptr_t)c | (uintptr_t)d;
+    if (u & 15u) {
+        lica_set_last_error("lica_mg", "device arrays must be 16-byte aligned", __FILE__, __LINE__);
+        return false;
+    }
+    return true;
+}
+
 int solve_impl(lica_mg* m, double* x, const double* f, const double* bx, const double* by, double rtol, int max_it,
                lica_mg_result* res, cudaStream_t s) {
     if (!m || !x || !f || !bx || !by || !(rtol >= 0.0) || max_it < 0) return LICA_BAD_ARG;
+    if (!aligned16(x, f, bx, by)) return LICA_BAD_ARG;
     int st;
     if (m->o.use_graph && !m->profile) {
         const bool same = m->gexec && m->gkey[0] == x && m->gkey[1] == f && m->gkey[2] == bx && m->gkey[3] == by &&
@@ -1242,7 +1485,7 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
         for (int l = from; l <= m->bottom; ++l) {
             const size_t e = (l < m->nouter - 1) ? tsz : sizeof(double);
             const size_t n = (size_t)m->lv[l].nx * m->lv[l].ny;
-            b += e * (3 * n + n + m->lv[l].nx);
+            b += e * (4 * n + n + m->lv[l].nx);
             b = (b + 15) & ~(size_t)15;
         }
         const size_t nb = (size_t)m->lv[m->bottom].nx * m->lv[m->bottom].ny;
@@ -1253,9 +1496,9 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
     for (int l = 1; l < m->nouter; ++l) {
         const bool tileable = m->lv[l].nx % TX == 0 && m->lv[l].ny % TY == 0;
         const size_t n = (size_t)m->lv[l].nx * m->lv[l].ny;
-        if (!tileable || (n <= 64 * 64 && cta_bytes(l) <= 200 * 1024)) { lcta = l; break; }
+        if (!tileable || (n <= 64 * 64 && cta_bytes(l) <= 226 * 1024)) { lcta = l; break; }
     }
-    if (cta_bytes(lcta) > 220 * 1024) {
+    if (cta_bytes(lcta) > 227 * 1024) {
         delete m;
         lica_set_last_error("lica_mg_create", "coarse levels do not fit in shared memory; use more levels",
                             __FILE__, __LINE__);
@@ -1265,6 +1508,10 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
         if (m->lv[l].nx % TX || m->lv[l].ny % TY) { delete m; return LICA_BAD_ARG; }
     }
     m->lcta = lcta;
+    for (int l = 0; l < lcta; ++l) {
+        LevelBuf& L = m->lv[l];
+        L.big = false;  // 64x32 tiles need one SM each at FP64; 32x32 keeps two resident
+    }
     // shared-memory layout of the single-CTA kernel
     CtaParams& P = m->cp;
     std::memset(&P, 0, sizeof(P));
@@ -1276,11 +1523,12 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
         const size_t e = (l < m->nouter - 1) ? tsz : sizeof(double);
         const size_t n = (size_t)m->lv[l].nx * m->lv[l].ny;
         CtaLevel& C = P.lv[l];
-        C.nx = m->lv[l].nx; C.ny = m->lv[l].ny; C.cx = m->lv[l].cx; C.cy = m->lv[l].cy;
+        C.nx = m->lv[l].nx; C.ny = m->lv[l].ny;
         C.off_u = take(e * n);
         C.off_f = take(e * n);
-        C.off_bx = take(e * n);
-        C.off_by = take(e * (n + m->lv[l].nx));
+        C.off_ax = take(e * n);
+        C.off_ay = take(e * (n + m->lv[l].nx));
+        C.off_di = take(e * n);
     }
     const size_t nb = (size_t)m->lv[m->bottom].nx * m->lv[m->bottom].ny;
     P.off_dense = take(sizeof(double) * nb * nb);
@@ -1314,12 +1562,22 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
         TRY_ALLOC(L.bx64, sizeof(double) * n);
         TRY_ALLOC(L.by64, sizeof(double) * (n + L.nx));
     }
+    for (int l = 0; l <= m->bottom; ++l) {
+        LevelBuf& L = m->lv[l];
+        const size_t n = (size_t)L.nx * L.ny;
+        TRY_ALLOC(L.ax64, sizeof(double) * n);
+        TRY_ALLOC(L.ay64, sizeof(double) * (n + L.nx));
+        TRY_ALLOC(L.di64, sizeof(double) * n);
+    }
     if (mixed) {
         for (int l = 0; l < m->nouter - 1; ++l) {
             LevelBuf& L = m->lv[l];
             const size_t n = (size_t)L.nx * L.ny;
             TRY_ALLOC(L.bx32, sizeof(float) * n);
             TRY_ALLOC(L.by32, sizeof(float) * (n + L.nx));
+            TRY_ALLOC(L.ax32, sizeof(float) * n);
+            TRY_ALLOC(L.ay32, sizeof(float) * (n + L.nx));
+            TRY_ALLOC(L.di32, sizeof(float) * n);
         }
     }
     const size_t ntiles = (size_t)(nx / TX) * (ny / TY);
@@ -1333,6 +1591,20 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
     int st = mixed ? set_smem_attrs<float>(o.nu1) : set_smem_attrs<double>(o.nu1);
     if (!st && o.nu2 != o.nu1) st = mixed ? set_smem_attrs<float>(o.nu2) : set_smem_attrs<double>(o.nu2);
     if (st) return fail(st);
+    {
+        cudaError_t e1 = cudaFuncSetAttribute(k_xupdate<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)xupdate_smem());
+        cudaError_t e2 = cudaFuncSetAttribute(k_xupdate<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)xupdate_smem());
+        cudaError_t e3 = cudaFuncSetAttribute(k_pupdate<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)pupdate_smem<double>());
+        cudaError_t e4 = cudaFuncSetAttribute(k_pupdate<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)pupdate_smem<float>());
+        if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess) {
+            lica_set_last_error("cudaFuncSetAttribute(CG kernels)", "failed", __FILE__, __LINE__);
+            return fail(LICA_ERR_CUDA);
+        }
+    }
     cudaError_t e = mixed ? cudaFuncSetAttribute(k_cta<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)m->cta_smem)
                           : cudaFuncSetAttribute(k_cta<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1363,6 +1635,12 @@ int lica_mg_destroy(lica_mg* m) {
     for (auto& L : m->lv) {
         cudaFree(L.bx32);
         cudaFree(L.by32);
+        cudaFree(L.ax32);
+        cudaFree(L.ay32);
+        cudaFree(L.ax64);
+        cudaFree(L.ay64);
+        cudaFree(L.di64);
+        cudaFree(L.di32);
     }
     cudaFree(m->pcg[0]);
     cudaFree(m->pcg[1]);
@@ -1414,6 +1692,7 @@ int lica_mg_solve_host(lica_mg* m, double* p, const double* f, const double* bx,
 int lica_mg_precond_device(lica_mg* m, double* z, const double* r, const double* bx, const double* by,
                            void* stream) {
     if (!m || !z || !r || !bx || !by) return LICA_BAD_ARG;
+    if (!aligned16(z, r, bx, by)) return LICA_BAD_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     int st;
     if ((st = setup_beta(m, bx, by, s))) return st;
@@ -1461,9 +1740,12 @@ int lica_mg_profile_read(lica_mg* m, int32_t kernel_class, double* total_ms, int
 int lica_mg_apply_device(lica_mg* m, double* out, const double* u, const double* bx, const double* by,
                          void* stream) {
     if (!m || !out || !u || !bx || !by || out == u) return LICA_BAD_ARG;  // out must not alias u (halo reads)
+    if (!aligned16(out, u, bx, by)) return LICA_BAD_ARG;
     cudaStream_t s = (cudaStream_t)stream;
+    int st;
+    if ((st = setup_beta(m, bx, by, s))) return st;
     const LevelBuf& L = m->lv[0];
-    k_apply<<<dim3(L.nx / TX, L.ny / TY), NT, 0, s>>>(out, u, bx, by, L.nx, L.ny, L.cx, L.cy);
+    k_apply<<<dim3(L.nx / TX, L.ny / TY), NT, 0, s>>>(out, u, L.ax64, L.ay64, L.nx, L.ny);
     LICA_CUDA_TRY(cudaGetLastError());
     lica_count_launches(1);
     LICA_CUDA_TRY(cudaStreamSynchronize(s));

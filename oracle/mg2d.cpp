@@ -26,7 +26,7 @@
 // Operation order (the CUDA kernels follow it exactly, compiled without FMA
 // contraction, so FP64 and FP32 iterates agree bit for bit):
 //   s = aw*uw; s += ae*ue; s += as*us; s += an*un;   d = aw; d += ae; d += as; d += an;
-//   Gauss-Seidel update: u = (s - f) / d;  residual: r = f - (s - d*u).
+//   Gauss-Seidel update: u = (s - f) * dinv with dinv = 1 / d;  residual: r = f - (s - d*u).
 //
 // Multigrid (new build; no counterpart in the reference):
 //   restriction      fc(I,J) = 0.25*((r00 + r10) + (r01 + r11))  (2x2 average)
@@ -89,7 +89,8 @@ void rb_sweep(Level<T>& L, int nsweeps, bool reverse) {
                 for (int i = (j + colour) & 1; i < L.nx; i += 2) {
                     T sm, d;
                     stencil_sums(L, L.u.data(), i, j, sm, d);
-                    L.u[(size_t)j * L.nx + i] = (sm - L.f[(size_t)j * L.nx + i]) / d;
+                    const T dinv = T(1) / d;
+                    L.u[(size_t)j * L.nx + i] = (sm - L.f[(size_t)j * L.nx + i]) * dinv;
                 }
         }
 }

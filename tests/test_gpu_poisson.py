@@ -198,3 +198,14 @@ def test_status_not_converged_and_nan():
 def test_bad_sizes_rejected():
     with pytest.raises(native.LicaError):
         poisson.MultigridPoisson(100, 64, 0.01, 0.01, nlevels=3)
+
+
+def test_misaligned_device_arrays_rejected():
+    import torch
+    c = bubble_poisson_case(64)
+    s = _solver(64, 2)
+    buf = torch.zeros(64 * 64 + 1, dtype=torch.float64, device="cuda")
+    p = buf[1:].view(64, 64)   # 8-byte offset: not 16-byte aligned
+    with pytest.raises(native.LicaError) as e:
+        s.solve(p, _t(c.f), _t(c.bx), _t(c.by))
+    assert e.value.code == 4
