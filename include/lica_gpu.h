@@ -164,6 +164,51 @@ enum lica_mg_kernel_class {
 int lica_mg_profile(lica_mg* mg, int32_t enable);
 int lica_mg_profile_read(lica_mg* mg, int32_t kernel_class, double* total_ms, int64_t* launches);
 
+/* ------------------------------------------------------------------------------------
+ * Level-set transport of 1-D columns: TRANSPORT (two_phase.f:701-984, called from MAIN,
+ * 1d.f:242) followed by GRID_COUPLING(0) (two_phase.f:4863-5118, 1d.f:244), for the
+ * 1 x 1 x n flow column with its 2 x 2 x 2n refined level-set grid (the reference's 1-D
+ * case; the refined field is the same on the four (I,J) replicas, so one value per
+ * refined z-level is stored).  A batch of ncol columns of equal n and length is stored
+ * back to back; each column is independent.  Per column (nf = 2n):
+ *   phi    [nf+7]  ALPHI(k), k = -2..nf+4 at [k+2]: band values (outside the band any
+ *                  value; TRANSPORT zeroes it)                                    in/out
+ *   layer  [nf+7]  band layer of refined cell k (0 outside, 1..11), the reference's
+ *                  I_B/J_B/K_B lists as a per-cell number                         in/out
+ *   psif   [nf+2]  PSIF(k) at [k], k = 1..nf                                      in/out
+ *   wo     [n+2]   WO(k), k = 0..n+1: the face velocity of the previous call      in/out
+ *   w      [n+2]   W(k), k = 0..n+1                                               in
+ *   mflvs  [nf+7]  interfacial mass flux of band cell k (MFLVS), read if iphs = 1 in
+ *   vol_tot_ori    VOL_TOT_ORI, the target vapour volume                          in/out
+ *   vol_tot_iphs   VOL_TOT_IPHS from VOL_TOT_MFDOT (used if iphs = 1)             in
+ *   psi_cn, psi_zn [n+2] PSI_CN(k), PSI_ZN(k), k = 0..n+1                         in/out
+ *   status         per-column lica_status (LICA_BAND_OVERFLOW: the band, 11 layers around
+ *                  every interface, spans more than 112 refined cells or left its window;
+ *                  that column is left unchanged)                                 out
+ *   stats  [4]     subcycles (0 if there was nothing to move), |grad phi| max and
+ *                  min over layers 1..8, IMASS                                    out
+ * n >= 8.  Host arrays for lica_gpu_lvs_transport (returns the last non-OK column
+ * status, or LICA_OK); device arrays and a stream for the _device form (enqueues and
+ * returns; read status afterwards). */
+typedef struct {
+    int32_t iphs;    /* IPHS: 1 with phase change (source term, reinit every subcycle) */
+    int32_t first;   /* 1 on the first call of a run: WO = W before averaging */
+    int32_t m_step;  /* time step number M (the MOD(M,50) mass-correction trigger) */
+    int32_t mglobal; /* MGLOBAL: 1 applies GLOBAL_MASS_CORRECTION */
+    double denr;     /* DENR, liquid/vapour density ratio used by the source term */
+    double dtconst;  /* DTCONST, the flow time step */
+} lica_lvs_params;
+
+int lica_gpu_lvs_transport(int32_t ncol, int32_t n, double length, double* phi, int32_t* layer, double* psif,
+                           double* wo, const double* w, const double* mflvs, double* vol_tot_ori,
+                           const double* vol_tot_iphs, double* psi_cn, double* psi_zn, int32_t* status,
+                           double* stats, const lica_lvs_params* prm);
+int lica_gpu_lvs_transport_device(int32_t ncol, int32_t n, double length, double* phi, int32_t* layer,
+                                  double* psif, double* wo, const double* w, const double* mflvs,
+                                  double* vol_tot_ori, const double* vol_tot_iphs, double* psi_cn,
+                                  double* psi_zn, int32_t* status, double* stats, const lica_lvs_params* prm,
+                                  void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -21,6 +21,14 @@ class MgResult(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("status", C.c_int32), ("rel_residual", C.c_double)]
 
 
+class LvsParams(C.Structure):
+    _fields_ = [("iphs", C.c_int32), ("first", C.c_int32), ("m_step", C.c_int32), ("mglobal", C.c_int32),
+                ("denr", C.c_double), ("dtconst", C.c_double)]
+
+
+_I32 = C.POINTER(C.c_int32)
+
+
 # every symbol include/lica_gpu.h declares, with its ctypes signature
 SIGNATURES = {
     "lica_last_error": (C.c_char_p, []),
@@ -42,6 +50,10 @@ SIGNATURES = {
     "lica_mg_profile_read": (C.c_int, [C.c_void_p, C.c_int32, _D, _I64]),
     "lica_mg_precond_device": (C.c_int, [C.c_void_p] * 6),
     "lica_mg_apply_device": (C.c_int, [C.c_void_p] * 6),
+    "lica_gpu_lvs_transport": (C.c_int, [C.c_int32, C.c_int32, C.c_double, _D, _I32, _D, _D, _D, _D, _D, _D, _D,
+                                         _D, _I32, _D, C.POINTER(LvsParams)]),
+    "lica_gpu_lvs_transport_device": (C.c_int, [C.c_int32, C.c_int32, C.c_double] + [C.c_void_p] * 12 +
+                                      [C.POINTER(LvsParams), C.c_void_p]),
 }
 
 STATUS = {0: "LICA_OK", 1: "LICA_NOT_CONVERGED", 2: "LICA_BAND_OVERFLOW", 3: "LICA_NAN", 4: "LICA_BAD_ARG",

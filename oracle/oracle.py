@@ -30,6 +30,12 @@ def lib(native: bool = False):
         L.orc_trdiag3.argtypes = [_D, _D, _D, _D, _D] + [C.c_int64] * 5
         L.orc_trdiag3p.argtypes = [_D, _D, _D, _D] + [C.c_int64] * 5
         L.orc_poisson1d.argtypes = [C.c_int64] * 6 + [_D, _D, _D, _I64, _D, _D, _D]
+        L.orc_lvs_init.argtypes = [C.c_int, C.c_double, C.c_double, _D, _INT, _D, _D, _D]
+        L.orc_lvs_transport.argtypes = [C.c_int, C.c_double, _D, _INT, _D, _D, _D, _D, C.c_int, C.c_double,
+                                        C.c_double, C.c_int, C.c_int, _D, C.c_double, C.c_int, _D, _D, _D]
+        L.orc_lvs_alphi_bc.argtypes = [C.c_int, C.c_double, _D]
+        L.orc_lvs_band.argtypes = [C.c_int, C.c_double, _D, _INT]
+        L.orc_lvs_reinit.argtypes = [C.c_int, C.c_double, _D, _INT, C.c_int]
         _LIBS[key] = L
     return _LIBS[key]
 
@@ -114,3 +120,70 @@ def poisson1d(geom, p, divgsum, denf_zi):
                              _p(np.asfortranarray(divgsum)), _p(np.asfortranarray(denf_zi)))
     assert st == 0
     return p
+
+
+# ---------------------------------------------------------------------------------------
+# Level set of one 1-D column (oracle/lvs1d.cpp).  State dict:
+#   phi (nf+7,) f64 at [k+2], layer (nf+7,) int32, psif (nf+2,), wo (n+2,), vol_tot_ori float
+# ---------------------------------------------------------------------------------------
+
+def _pi(a):
+    assert a.dtype == np.int32
+    return a.ctypes.data_as(_INT)
+
+
+def lvs_init(n, length, z0):
+    """LVSINIT for a planar interface at z0 (vapour below).  Returns the state dict."""
+    nf = 2 * n
+    st = {"n": n, "length": float(length), "phi": np.zeros(nf + 7), "layer": np.zeros(nf + 7, np.int32),
+          "psif": np.zeros(nf + 2), "wo": np.zeros(n + 2)}
+    vol = C.c_double(0.0)
+    rc = lib().orc_lvs_init(n, length, z0, _p(st["phi"]), _pi(st["layer"]), _p(st["psif"]), _p(st["wo"]),
+                            C.byref(vol))
+    assert rc == 0
+    st["vol_tot_ori"] = vol.value
+    return st
+
+
+def lvs_copy(st):
+    return {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in st.items()}
+
+
+def lvs_transport(st, w, mflvs, *, iphs, denr, dtconst, first, m_step, vol_tot_iphs, mglobal, psi_cn, psi_zn):
+    """TRANSPORT + GRID_COUPLING(0) on a copy of st.  Returns (state, psi_cn, psi_zn, stats)."""
+    st = lvs_copy(st)
+    n = st["n"]
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    mf = np.ascontiguousarray(mflvs, dtype=np.float64)
+    assert w.shape == (n + 2,) and mf.shape == (2 * n + 7,)
+    pc = np.array(psi_cn, dtype=np.float64, copy=True)
+    pz = np.array(psi_zn, dtype=np.float64, copy=True)
+    stats = np.zeros(4)
+    vol = C.c_double(st["vol_tot_ori"])
+    rc = lib().orc_lvs_transport(n, st["length"], _p(st["phi"]), _pi(st["layer"]), _p(st["psif"]), _p(st["wo"]),
+                                 _p(w), _p(mf), int(iphs), float(denr), float(dtconst), int(first), int(m_step),
+                                 C.byref(vol), float(vol_tot_iphs), int(mglobal), _p(pc), _p(pz), _p(stats))
+    if rc == 2:
+        raise OverflowError("band left the stored range k = -2..nf+4")
+    assert rc == 0
+    st["vol_tot_ori"] = vol.value
+    return st, pc, pz, stats
+
+
+def lvs_alphi_bc(n, length, phi):
+    phi = np.array(phi, dtype=np.float64, copy=True)
+    lib().orc_lvs_alphi_bc(n, length, _p(phi))
+    return phi
+
+
+def lvs_band(n, length, phi, layer):
+    phi = np.array(phi, dtype=np.float64, copy=True)
+    layer = np.array(layer, dtype=np.int32, copy=True)
+    lib().orc_lvs_band(n, length, _p(phi), _pi(layer))
+    return phi, layer
+
+
+def lvs_reinit(n, length, phi, layer, ilimit):
+    phi = np.array(phi, dtype=np.float64, copy=True)
+    lib().orc_lvs_reinit(n, length, _p(phi), _pi(np.ascontiguousarray(layer, dtype=np.int32)), ilimit)
+    return phi
