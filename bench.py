@@ -149,6 +149,12 @@ ALG_BYTES_PER_CELL = {  # FP64, level 0: each distinct array read or written onc
 }
 
 
+# DRAM bytes per level-0 launch from one ncu capture at 1024x1024 FP64
+# (dram__bytes_read.sum + dram__bytes_write.sum; profiles/mg_k_down_k_up_level0_1024_fp64.md),
+# scaled by cells for other sizes.
+NCU_DRAM_BYTES_1024 = {"down0": 33.587456e6 + 0.027392e6, "up0": 44.082944e6 + 0.560128e6}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -266,7 +272,10 @@ def run_ours(args):
     peak, peak_kind = peaks()
     achieved = alg / avg_s / 1e9
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": (NCU_DRAM_BYTES_1024[dom] * (n * n) / (1024 * 1024)
+                            if dom in NCU_DRAM_BYTES_1024 and args.precision == "fp64" else None),
+                "traffic_source": "ncu capture of the same kernel at 1024x1024 (cold cache), scaled by cells",
                 "alg_bytes_per_launch": alg, "avg_launch_us": avg_s * 1e6,
                 "kernel_classes_ms_per_solve": {k: v[0] / 3 for k, v in prof.items()},
                 "note": "one profiled solve as separate launches after the timed region; working set is L2-resident"}
