@@ -18,6 +18,7 @@
 #ifndef LICA_GPU_H
 #define LICA_GPU_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -203,6 +204,60 @@ int lica_gpu_lvs_transport(int32_t ncol, int32_t n, double length, double* phi, 
                            double* wo, const double* w, const double* mflvs, double* vol_tot_ori,
                            const double* vol_tot_iphs, double* psi_cn, double* psi_zn, int32_t* status,
                            double* stats, const lica_lvs_params* prm);
+/* ------------------------------------------------------------------------------------
+ * Whole RK3 time steps of 1-D boiling columns: MAIN's step (1d.f:190-250) -- DETERMINE_DT,
+ * three substeps of RHSNLHS (CAL_CONTINUITY, CAL_CONT_BC, PASSIVE_SCALAR with TEMP_GRAD /
+ * TEMP_EXTP / TF_GRAD / VOL_TOT_MFDOT / CAL_CONTINUITY2, RHSZ, LHSW, BC, FSM_CHOI,
+ * PRESSURE_CORRECTION), CONVRGE1, TRANSPORT and GRID_COUPLING -- for a batch of independent
+ * columns of n flow cells, one persistent kernel for any number of steps.
+ * The missing LHSPS2 of the reference (called at 1d.f:3665) is the LHSPS solve.
+ * ---------------------------------------------------------------------------------- */
+typedef struct {
+    double re, visr, denr; /* RE_M, VISR, DENR (lica.in) */
+    double weber, fr;      /* WEBER, FR */
+    double prm, scr, tcr;  /* PRM, SCR, TCR */
+    double t_sat, jakob;   /* T_SAT, JAKOB */
+    double cflmax, dt0;    /* CFLFAC, initial DT */
+    int32_t iphs, mglobal; /* IPHS (phase change), MGLOBAL (global mass correction) */
+} lica_col_props;
+
+/* State of ncol columns stored back to back (nf = 2n):
+ *   w, p, t, psi_cn, psi_zn, wo : n+2 doubles per column, index k = 0..n+1
+ *   phi, mflvs : nf+7 doubles (k = -2..nf+4 at k+2);  layer : nf+7 int32
+ *   psif, sfgas, sfgas2 : nf+2 doubles (k = 1..nf at k);  imask : n+2 int32
+ *   scal : 5 doubles  (DT, TIME, M = steps taken, VOL_TOT_ORI, VOL_TOT_IPHS)
+ *   stats: 8 doubles  (flow CFL, max |div u - source|, TEMP_EXTP iterations, level-set
+ *                      subcycles, mass-correction triggers, interface height, vapour
+ *                      volume, DT) of the last step */
+typedef struct {
+    double *w, *p, *t, *psi_cn, *psi_zn;
+    double* phi;
+    int32_t* layer;
+    double *psif, *wo, *mflvs, *sfgas, *sfgas2;
+    int32_t* imask;
+    double *scal, *stats;
+} lica_col_state;
+
+/* Initial state of one column with a vapour film of thickness z0 at the wall (MAKEFLD
+ * 1d.f:821-946 with IPHS = 1, LVSINIT two_phase.f:116-388, GRID_COUPLING(1)); host arrays
+ * of one column. */
+int lica_gpu_column_init(int32_t n, double length, double z0, const lica_col_props* props, lica_col_state* st);
+
+/* Device scratch the step kernel needs for ncol columns of n cells. */
+size_t lica_gpu_column_scratch_bytes(int32_t ncol, int32_t n);
+
+/* nsteps time steps of every column; device arrays.  scratch: NULL (the library keeps
+ * one) or lica_gpu_column_scratch_bytes() of device memory.  status[ncol] (device) gets
+ * LICA_OK, LICA_NOT_CONVERGED (TEMP_EXTP did not converge), LICA_BAND_OVERFLOW or
+ * LICA_BAD_ARG per column; a column stops at its first non-OK step.  Enqueues on stream. */
+int lica_gpu_column_steps_device(int32_t ncol, int32_t n, double length, const lica_col_props* props,
+                                 const lica_col_state* st, int32_t nsteps, void* scratch, int32_t* status,
+                                 void* stream);
+
+/* Same on host arrays (copies in, runs, copies out); returns the last non-OK column status. */
+int lica_gpu_column_steps(int32_t ncol, int32_t n, double length, const lica_col_props* props,
+                          lica_col_state* st, int32_t nsteps, int32_t* status);
+
 int lica_gpu_lvs_transport_device(int32_t ncol, int32_t n, double length, double* phi, int32_t* layer,
                                   double* psif, double* wo, const double* w, const double* mflvs,
                                   double* vol_tot_ori, const double* vol_tot_iphs, double* psi_cn,

@@ -1,0 +1,137 @@
+"""Host-side mirror of the reference's time loop for 1-D boiling columns.
+
+``Columns`` holds the state of a batch of independent columns (the reference's MAIN
+state for its 1-D case: W, P, T, PSI_CN, PSI_ZN, the level-set band, the phase-change
+fields and DT/TIME/M) in the layout of ``lica_col_state`` (include/lica_gpu.h), as numpy
+arrays (host) or torch CUDA tensors (device).  ``Columns.steps`` advances every column by
+whole RK3 time steps of MAIN (1d.f:190-250) in one persistent GPU launch.
+
+Column arrays, nf = 2 n refined cells:
+  w, p, t, psi_cn, psi_zn, wo : (ncol, n+2), index k = 0..n+1
+  phi, mflvs : (ncol, nf+7) at k+2, k = -2..nf+4;  layer : int32, same shape
+  psif, sfgas, sfgas2 : (ncol, nf+2) at k;  imask : int32 (ncol, n+2)
+  scal : (ncol, 5) DT, TIME, M, VOL_TOT_ORI, VOL_TOT_IPHS;  stats : (ncol, 8)
+"""
+import ctypes as C
+from dataclasses import dataclass, fields
+
+import numpy as np
+
+from . import native
+
+STATS = ("cfl", "divergence", "extension_iterations", "levelset_subcycles", "mass_corrections", "interface_height",
+         "vapour_volume", "dt")
+
+
+@dataclass
+class ColumnProps:
+    """lica.in properties of the two-phase / heat block (INPUT_SIMULATION, 1d.f:346-379).
+    Defaults: the shipped case."""
+    re: float = 1.42e-2
+    visr: float = 22.22
+    denr: float = 1605.36
+    weber: float = 7.36e-8
+    fr: float = 9.7
+    prm: float = 1.0231
+    scr: float = 2.077
+    tcr: float = 27.16
+    t_sat: float = 1.0
+    jakob: float = 0.009
+    cflmax: float = 0.5
+    dt0: float = 2.5e-6
+    iphs: int = 1
+    mglobal: int = 1
+
+    def c(self):
+        return native.ColProps(*[getattr(self, f.name) for f in fields(self)])
+
+
+def _shapes(ncol, n):
+    nf = 2 * n
+    sf, sp, sq = n + 2, nf + 7, nf + 2
+    return {"w": (sf, np.float64), "p": (sf, np.float64), "t": (sf, np.float64), "psi_cn": (sf, np.float64),
+            "psi_zn": (sf, np.float64), "phi": (sp, np.float64), "layer": (sp, np.int32), "psif": (sq, np.float64),
+            "wo": (sf, np.float64), "mflvs": (sp, np.float64), "sfgas": (sq, np.float64),
+            "sfgas2": (sq, np.float64), "imask": (sf, np.int32), "scal": (5, np.float64), "stats": (8, np.float64)}
+
+
+class Columns:
+    """State of ncol columns of n flow cells over a column of the given length."""
+
+    def __init__(self, n, length, arrays):
+        self.n, self.length = int(n), float(length)
+        self.arrays = arrays
+        self.ncol = arrays["w"].shape[0]
+
+    def __getattr__(self, k):
+        a = self.__dict__.get("arrays")
+        if a is not None and k in a:
+            return a[k]
+        raise AttributeError(k)
+
+    @property
+    def on_device(self):
+        return not isinstance(self.arrays["w"], np.ndarray)
+
+    @staticmethod
+    def empty(ncol, n, length):
+        return Columns(n, length, {k: np.zeros((ncol, m), dt) for k, (m, dt) in _shapes(ncol, n).items()})
+
+    @staticmethod
+    def film(n, length, z0s, props):
+        """Columns each holding a vapour film of thickness z0 at the wall (MAKEFLD +
+        LVSINIT + GRID_COUPLING(1), lica_gpu_column_init)."""
+        z0s = np.atleast_1d(np.asarray(z0s, dtype=np.float64))
+        cols = Columns.empty(len(z0s), n, length)
+        cp = props.c()
+        for c, z0 in enumerate(z0s):
+            st = native.ColState(*[cols.arrays[k][c].ctypes.data for k in native.COL_FIELDS])
+            native.check(native.lib().lica_gpu_column_init(n, length, float(z0), C.byref(cp), C.byref(st)),
+                         "lica_gpu_column_init")
+        return cols
+
+    def to(self, device):
+        """A copy on a torch device, or on the host (numpy) for device=None."""
+        import torch
+        out = {}
+        for k, v in self.arrays.items():
+            if device is None:
+                out[k] = v.detach().cpu().numpy() if isinstance(v, torch.Tensor) else v.copy()
+            else:
+                out[k] = torch.as_tensor(v if isinstance(v, np.ndarray) else v.cpu().numpy(), device=device).clone()
+        return Columns(self.n, self.length, out)
+
+    def _state(self, ptr):
+        return native.ColState(*[ptr(self.arrays[k]) for k in native.COL_FIELDS])
+
+    def steps(self, nsteps, props, stream=None, scratch=None):
+        """Advance every column by nsteps time steps.  Returns the per-column status
+        (numpy for host state; a CUDA tensor for device state, filled when the stream
+        reaches it)."""
+        L = native.lib()
+        cp = props.c()
+        if not self.on_device:
+            for k, (m, dt) in _shapes(self.ncol, self.n).items():
+                a = self.arrays[k]
+                if a.dtype != dt or not a.flags.c_contiguous or a.shape != (self.ncol, m):
+                    raise TypeError(f"{k}: need a C-contiguous {np.dtype(dt).name} array of shape {(self.ncol, m)}")
+            status = np.zeros(self.ncol, np.int32)
+            rc = L.lica_gpu_column_steps(self.ncol, self.n, self.length, C.byref(cp),
+                                         C.byref(self._state(lambda a: a.ctypes.data)), int(nsteps),
+                                         status.ctypes.data_as(C.POINTER(C.c_int32)))
+            native.check(rc, "column steps", ok=(0, 1, 2, 4))
+            return status
+        import torch
+        dev = self.arrays["w"].device
+        status = torch.zeros(self.ncol, dtype=torch.int32, device=dev)
+        s = stream if stream is not None else torch.cuda.current_stream(dev)
+        rc = L.lica_gpu_column_steps_device(self.ncol, self.n, self.length, C.byref(cp),
+                                            C.byref(self._state(lambda a: a.data_ptr())), int(nsteps),
+                                            C.c_void_p(scratch.data_ptr() if scratch is not None else None),
+                                            C.c_void_p(status.data_ptr()), C.c_void_p(s.cuda_stream))
+        native.check(rc, "column steps")
+        return status
+
+
+def scratch_bytes(ncol, n):
+    return int(native.lib().lica_gpu_column_scratch_bytes(ncol, n))

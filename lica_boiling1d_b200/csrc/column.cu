@@ -1,0 +1,1408 @@
+// One or many time steps of the 1-D boiling column on the GPU: MAIN's RK3 step
+// (1d.f:190-250) -- DETERMINE_DT, three substeps of RHSNLHS (CAL_CONTINUITY, CAL_CONT_BC,
+// PASSIVE_SCALAR with TEMP_GRAD / TEMP_EXTP / TF_GRAD / VOL_TOT_MFDOT / CAL_CONTINUITY2,
+// RHSZ, LHSW, BC, FSM_CHOI, PRESSURE_CORRECTION), CONVRGE1, TRANSPORT and GRID_COUPLING --
+// fused into one persistent kernel.
+//
+// Parallel structure: one CTA per column; the CTA loops over the time steps without
+// returning to the host.  Per-cell work is spread over the CTA's threads with a barrier
+// between phases; the three tridiagonal solves per substep (LHSPS, LHSW, POISSON) run as
+// the Thomas algorithm on one thread, in the reference's order; the band work (TEMP_GRAD's
+// interface pieces, TEMP_EXTP's narrow extension region, TRANSPORT) runs on warp 0 with the
+// band window of lvs_device.cuh in shared memory.  Columns of a batch are independent.
+//
+// CONTI_Z / CONTI_C (1d.f:2071-2346) are serial loops that set a face value only while it
+// is still zero; they are evaluated here per face in closed form: the value seen by cell K
+// for its lower face is the one cell K-1 set (a region-0/1 constant, or the swept-volume
+// value of that face, which cell K would compute identically), and the final face value is
+// cell K+1's constant when that cell is in region 0/1, else cell K's value.
+//
+// Every floating-point expression keeps the reference's operation order; with the
+// library's -fmad=false the results agree bit for bit with the CPU restatement.
+#include "lvs_device.cuh"
+
+#include <algorithm>
+#include <cstdio>
+#include <mutex>
+#include <vector>
+
+extern "C" void lica_count_launches(int64_t n);
+
+namespace lica {
+namespace colk {
+
+// lica.in properties and the derived constants of INPUT_SIMULATION (1d.f:437-489).
+struct Phys {
+    double re, rei, denm, denp, den_diff, vism, visp, denscm, denscp, densc_diff, tcm, tcp, tc_diff, prm, prai,
+        surf, gravity, time_st, time_gv, denr, ja, t_sat, cflmax;
+    int iphs, mglobal;
+};
+
+constexpr int NT = 256;          // threads per column CTA
+constexpr int NFLOW = 30;        // flow-sized scratch arrays per column
+constexpr int XR = 132;          // TEMP_EXTP extension range held in shared memory (+halo)
+
+__constant__ double c_gamma[4] = {0.0, 8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
+__constant__ double c_ro[4] = {0.0, 0.0, -17.0 / 60.0, -5.0 / 12.0};
+
+// scratch array indices (each n+2 doubles)
+enum {
+    S_DFZ, S_VFZ, S_PSIZ, S_DFC, S_PSIC, S_DENFZ, S_DENFZI, S_DENFC, S_RHS1, S_RK3ZO, S_RHSPS, S_DIVG,
+    S_AK, S_BK, S_CK, S_GK, S_GAM, S_VZD, S_VZV, S_VCD, S_TEMP0, S_TEMP1, S_NPHI, S_PSIH, S_PSITMP, S_SPARE0,
+    S_SPARE1, S_SPARE2, S_SPARE3, S_SPARE4
+};
+
+struct Args {
+    int ncol, n, nsteps;
+    double L;
+    Phys ph;
+    double *w, *p, *t, *psi_cn, *psi_zn, *phi, *psif, *wo, *mflvs, *sfgas, *sfgas2, *scal, *stats;
+    int *layer, *imask, *status;
+    double* dscr;
+    int* iscr;
+};
+
+struct Geo {
+    int n, nf;
+    double h, hf;
+    __device__ double sdz(int k) const { return (k >= 1 && k <= n) ? h : 0.0; }
+    __device__ double ssdz(int) const { return 1.0 / h; }
+    __device__ double vdz(int k) const { return (k == 1 || k == n + 1) ? 0.5 * h : h; }
+    __device__ double vvdz(int k) const { return 1.0 / vdz(k); }
+    __device__ double z(int k) const { return col::grid_z(h, k); }
+    __device__ double zp(int k) const { return col::grid_zp(h, n, k); }
+    __device__ double zpf(int k) const { return col::grid_zpf(hf, k); }
+    __device__ double akw(int k) const { return -vvdz(k) * ssdz(k - 1); }
+    __device__ double ckw(int k) const { return -vvdz(k) * ssdz(k); }
+    __device__ double akuv(int k) const { return -vvdz(k) * ssdz(k); }
+    __device__ double ckuv(int k) const { return -vvdz(k + 1) * ssdz(k); }
+};
+
+// One column's arrays.
+struct Col {
+    double *w, *p, *t, *psi_cn, *psi_zn, *phi, *psif, *wo, *mflvs, *sfgas, *sfgas2, *scal, *stats, *psif_mtp;
+    int *layer, *imask, *region;   // region indexed k+1, k = -1..n+2
+    double* a[NFLOW];
+};
+
+struct Shared {
+    lvs::Win win;
+    double red[32];
+    // TEMP_EXTP extension region [xk0, xk0+XR)
+    double x_nphi[XR], x_psih[XR], x_tm[XR], x_dt[XR], x_dtrk[XR], x_to[XR], x_trk[XR], x_new[XR];
+    int ibuf[8];
+    double dbuf[8];
+};
+
+__device__ __forceinline__ double block_max(double v, Shared& sh) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh.red[warp] = v;
+    __syncthreads();
+    double r = sh.red[0];
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q) r = fmax(r, sh.red[q]);
+    return r;
+}
+__device__ __forceinline__ double block_min(double v, Shared& sh) {
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh.red[warp] = v;
+    __syncthreads();
+    double r = sh.red[0];
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q) r = fmin(r, sh.red[q]);
+    return r;
+}
+
+// Thomas algorithm of TRDIAG3 (1d.f:3783-3811) on one line, unknowns l1..l2; r becomes the
+// solution.  One thread.
+__device__ void thomas(const double* a, const double* b, const double* c, double* r, double* gam, int l1, int l2) {
+    double bet = 1.0 / b[l1];
+    double u = r[l1] * bet;
+    r[l1] = u;
+    for (int j = l1 + 1; j <= l2; ++j) {
+        gam[j] = c[j - 1] * bet;
+        bet = 1.0 / (b[j] - a[j] * gam[j]);
+        u = (r[j] - a[j] * u) * bet;
+        r[j] = u;
+    }
+    for (int j = l2 - 1; j >= l1; --j) {
+        u = r[j] - gam[j + 1] * u;
+        r[j] = u;
+    }
+}
+
+#define FOR_K(lo, hi) for (int k = (lo) + (int)threadIdx.x; k <= (hi); k += (int)blockDim.x)
+
+// REGION (1d.f:2038-2056), evaluated per cell: 2 within two cells of a PSI_CN jump, else 1
+// in liquid, else 0 (the serial loop's final state).
+__device__ void make_region(const Geo& g, Col& c) {
+    const int n = g.n;
+    FOR_K(-1, n + 2) {
+        int r = 0;
+        for (int kk = max(1, k - 2); kk <= min(n, k + 2); ++kk)
+            if ((c.psi_cn[kk + 1] - c.psi_cn[kk] != 0.0) || (c.psi_cn[kk] - c.psi_cn[kk - 1] != 0.0)) r = 2;
+        if (r == 0 && k >= 1 && k <= n && c.psi_cn[k] == 1.0) r = 1;
+        c.region[k + 1] = r;
+    }
+    __syncthreads();
+}
+
+// CAL_CONTINUITY (1d.f:1994-2068): CONTI_Z and CONTI_C with PSIFACE_Z / PSIFACE_C and the
+// swept-volume box integrals (1d.f:2349-2958).
+__device__ void cal_continuity(const Geo& g, const Phys& ph, Col& c, double dtconst) {
+    const int n = g.n, nf = g.nf;
+    double *df_z = c.a[S_DFZ], *vf_z = c.a[S_VFZ], *psi_z = c.a[S_PSIZ], *df_c = c.a[S_DFC], *psi_c = c.a[S_PSIC];
+    double *vzd = c.a[S_VZD], *vzv = c.a[S_VZV], *vcd = c.a[S_VCD];
+    const double* w = c.w;
+    const int* reg = c.region + 1;
+    make_region(g, c);
+    // face values as cell K sees them: V(j) (z: j = 1..n; c: j = 0..n)
+    FOR_K(0, n) {
+        if (k >= 1) {
+            const int r = reg[k];
+            if (k >= 2 && r == 0) {
+                vzd[k] = ph.denm;
+                vzv[k] = ph.vism;
+            } else if (k >= 2 && r == 1) {
+                vzd[k] = ph.denp;
+                vzv[k] = ph.visp;
+            } else {
+                const double wt = 0.5 * (w[k + 1] + w[k]);
+                double ps;
+                if (fabs(wt) <= 1e-8) {
+                    ps = 0.5 * (c.psi_zn[k] + c.psi_zn[k + 1]);
+                } else {
+                    double z1, z2;
+                    int k1, k2;
+                    if (wt >= 0.0) {
+                        z1 = g.zp(k) - wt * dtconst;
+                        z2 = g.zp(k);
+                        k1 = 2 * (k - 1);
+                        k2 = 2 * k - 1;
+                    } else {
+                        z1 = g.zp(k);
+                        z2 = g.zp(k) - wt * dtconst;
+                        k1 = 2 * k;
+                        k2 = 2 * k + 1;
+                    }
+                    ps = col::box_mean(c.psif, nf, k1, k2, z1, z2, g.hf);
+                }
+                vzv[k] = ph.vism + (ph.visp - ph.vism) * ps;
+                vzd[k] = ph.denm + ph.den_diff * ps;
+            }
+        }
+        {
+            const int r = reg[k];
+            if (k >= 1 && r == 0) {
+                vcd[k] = ph.denm;
+            } else if (k >= 1 && r == 1) {
+                vcd[k] = ph.denp;
+            } else {
+                const double wt = w[k + 1];
+                double ps;
+                if (fabs(wt) <= 1e-8) {
+                    ps = c.psi_cn[k + 1];
+                } else {
+                    double z1, z2;
+                    int k1, k2;
+                    if (wt >= 0.0) {
+                        z1 = g.z(k + 1) - wt * dtconst;
+                        z2 = g.z(k + 1);
+                        k1 = 2 * k - 1;
+                        k2 = 2 * k;
+                    } else {
+                        z1 = g.z(k + 1);
+                        z2 = g.z(k + 1) - wt * dtconst;
+                        k1 = 2 * k + 1;
+                        k2 = 2 * k + 2;
+                    }
+                    ps = col::box_mean(c.psif, nf, k1, k2, z1, z2, g.hf);
+                }
+                vcd[k] = ph.denm + ph.den_diff * ps;
+            }
+        }
+    }
+    __syncthreads();
+    FOR_K(0, n) {
+        // final face values
+        if (k >= 1) {
+            const int rn = (k + 1 <= n) ? reg[k + 1] : 2;
+            if (rn == 0) {
+                df_z[k] = ph.denm;
+                vf_z[k] = ph.vism;
+            } else if (rn == 1) {
+                df_z[k] = ph.denp;
+                vf_z[k] = ph.visp;
+            } else {
+                df_z[k] = vzd[k];
+                vf_z[k] = vzv[k];
+            }
+        }
+        {
+            const int rn = (k + 1 <= n) ? reg[k + 1] : 2;
+            df_c[k] = (rn == 0) ? ph.denm : (rn == 1 ? ph.denp : vcd[k]);
+        }
+        // cell values
+        if (k >= 2) {
+            if (reg[k] == 2) {
+                const double wt = 0.5 * (w[k + 1] + w[k]);
+                const double wb = 0.5 * (w[k] + w[k - 1]);
+                const double flux_z = (vzd[k] * wt - vzd[k - 1] * wb) * g.vvdz(k);
+                const double den_zn = ph.denm + ph.den_diff * c.psi_zn[k];
+                const double den_z = den_zn - dtconst * flux_z;
+                double v = (den_z - ph.denm) / ph.den_diff;
+                psi_z[k] = (v > 1.0) ? 1.0 : (v < 0.0 ? 0.0 : v);
+            } else {
+                const double v = c.psi_zn[k];
+                psi_z[k] = (v > 1.0) ? 1.0 : (v < 0.0 ? 0.0 : v);
+            }
+        }
+        if (k >= 1) {
+            if (reg[k] == 2) {
+                const double wt = w[k + 1], wb = w[k];
+                const double flux_z = (vcd[k] * wt - vcd[k - 1] * wb) * g.ssdz(k);
+                const double den_cn = ph.denm + ph.den_diff * c.psi_cn[k];
+                const double den_c = den_cn - dtconst * flux_z;
+                const double v = (den_c - ph.denm) / ph.den_diff;
+                psi_c[k] = (v > 1.0) ? 1.0 : (v < 0.0 ? 0.0 : v);
+            } else {
+                const double v = c.psi_cn[k];
+                psi_c[k] = (v > 1.0) ? 1.0 : (v < 0.0 ? 0.0 : v);
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        psi_z[1] = psi_z[2];
+        psi_z[n + 1] = psi_z[n];
+        psi_c[1] = psi_c[2];
+        psi_c[n + 1] = psi_c[n];
+    }
+    __syncthreads();
+}
+
+// CAL_CONT_BC, 1d.f:2961-3003.
+__device__ void cal_cont_bc(const Geo& g, const Phys& ph, Col& c) {
+    const int n = g.n;
+    double *dz = c.a[S_DENFZ], *dzi = c.a[S_DENFZI], *dc = c.a[S_DENFC];
+    const double *psi_z = c.a[S_PSIZ], *psi_c = c.a[S_PSIC];
+    FOR_K(1, n) {
+        const double d = ph.denm + ph.den_diff * psi_z[k];
+        dz[k] = d;
+        dzi[k] = 1.0 / d;
+        dc[k] = ph.denm + ph.den_diff * psi_c[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        dz[n + 1] = dz[n];
+        dzi[n + 1] = dzi[n];
+        dz[0] = dz[1];
+        dzi[0] = dzi[1];
+    }
+    __syncthreads();
+}
+
+// LHSPS, 1d.f:4380-4497.
+__device__ void lhsps(const Geo& g, const Phys& ph, Col& c, double alpha, double dt) {
+    const int n = g.n;
+    const double den_diffi = (ph.den_diff == 0.0) ? 1.0 : 1.0 / ph.den_diff;
+    const double acops = alpha * dt / (ph.re * ph.prm);
+    double *ak = c.a[S_AK], *bk = c.a[S_BK], *ck = c.a[S_CK], *gk = c.a[S_GK];
+    const double *psi_c = c.a[S_PSIC], *df_c = c.a[S_DFC];
+    double* rhsps = c.a[S_RHSPS];
+    FOR_K(1, n) {
+        const double denscf = ph.denscm + ph.densc_diff * psi_c[k];
+        const double coef = acops / denscf;
+        double psi_tmp = (df_c[k - 1] - ph.denm) * den_diffi;
+        const double tcb = ph.tcm + ph.tc_diff * psi_tmp;
+        psi_tmp = (df_c[k] - ph.denm) * den_diffi;
+        const double tct = ph.tcm + ph.tc_diff * psi_tmp;
+        double a = coef * tcb * g.akuv(k);
+        double cc = coef * tct * g.ckuv(k);
+        bk[k] = 1.0 - (a + cc);
+        gk[k] = rhsps[k];
+        const double pc = c.psi_cn[k];
+        if (fabs(pc - 0.5) != 0.5) {
+            if (pc <= 0.5) cc = 0.0;
+            else if (pc > 0.5) a = 0.0;
+        }
+        ak[k] = a;
+        ck[k] = cc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) thomas(ak, bk, ck, gk, c.a[S_GAM], 1, n);
+    __syncthreads();
+    FOR_K(1, n) {
+        rhsps[k] = gk[k];
+        c.t[k] = gk[k] + c.t[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        c.t[0] = 0.0;
+        c.t[n] = 1.0;
+        c.t[n + 1] = c.t[n];
+    }
+    __syncthreads();
+}
+
+// TEMP_EXTP_RK3, chphase.f:806-956 (1-D), on the extension range in shared memory: x[i]
+// holds flow cell xk0 + i.  nd = 0: tempo is the DTEMPN array itself.
+__device__ void extp_sweep(const Geo& g, Shared& sh, int xk0, int lo, int hi, double* tempo, int im, double redtl,
+                           int nd) {
+    const int lane = threadIdx.x & 31;
+    const double sm_grid = fmin(fmin(1.0, 1.0), 2.0 * g.hf);
+    for (int i = lo + lane; i <= hi; i += 32) {
+        const int k = xk0 + i;
+        double nv = tempo[i];
+        const double nph = sh.x_nphi[i];
+        if (nph != 0.0) {
+            double dpz;
+            if (sh.x_nphi[i - 1] == 0.0) dpz = (sh.x_nphi[i + 1] - nph) * g.vvdz(k + 1);
+            else if (sh.x_nphi[i + 1] == 0.0) dpz = (nph - sh.x_nphi[i - 1]) * g.vvdz(k);
+            else dpz = 0.5 * (sh.x_nphi[i + 1] - sh.x_nphi[i - 1]) * g.vvdz(k);
+            const double dalphi = (0.0 + 0.0) + dpz * dpz;
+            if (dalphi != 0.0) {
+                double nz = 1.0;
+                const double apzm = (tempo[i] - tempo[i - 1]) * g.vvdz(k);
+                const double apzp = (tempo[i + 1] - tempo[i]) * g.vvdz(k);
+                if (im == 1) nz = (-1.0) * nz;
+                const double ax = 0.0, ay = 0.0;
+                const double az = fmin(nz, 0.0) * apzp + fmax(nz, 0.0) * apzm;
+                double drhs;
+                if (im == 1) {
+                    drhs = (ax + ay + az) + nd * sh.x_dt[i];
+                    nv = tempo[i] - redtl * drhs * (1 - sh.x_psih[i]);
+                } else {
+                    drhs = (ax + ay + az) - nd * sh.x_dt[i];
+                    nv = tempo[i] - redtl * drhs * sh.x_psih[i];
+                }
+                if (nd == 0 && fabs(nph) <= sm_grid) {
+                    drhs = (ax + ay + az);
+                    nv = tempo[i] - redtl * drhs;
+                }
+            }
+        }
+        sh.x_new[i] = nv;
+    }
+    __syncwarp();
+    for (int i = lo + lane; i <= hi; i += 32) tempo[i] = sh.x_new[i];
+    __syncwarp();
+}
+
+__device__ __forceinline__ double warp_maxd(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+constexpr int kMaxHalvings = 40;
+
+// TEMP_EXTP, chphase.f:467-805 (1-D), warp 0.  Only cells with NPHI != 0 change; they lie
+// in [ka, kb], held with one halo cell on each side in shared memory.  Returns the number
+// of pseudo-time iterations or -1 if a phase does not converge within kMaxHalvings
+// halvings of the step.
+__device__ int temp_extp(const Geo& g, const Phys& ph, Col& c, Shared& sh, int ka, int kb) {
+    const int lane = threadIdx.x & 31;
+    const double sm_grid = fmin(fmin(2.0 * 0.5, 2.0 * 0.5), 2.0 * g.hf);
+    const double eps = 1e-4;
+    const int xk0 = ka - 1, lo = 1, hi = kb - xk0;   // x index of ka .. kb
+    const double *nphi = c.a[S_NPHI], *psih = c.a[S_PSIH];
+    int total = 0;
+    for (int i = lane; i <= hi + 1; i += 32) {
+        sh.x_nphi[i] = nphi[xk0 + i];
+        sh.x_psih[i] = psih[xk0 + i];
+    }
+    __syncwarp();
+    for (int im = 0; im <= 1; ++im) {
+        double* tm_g = c.a[im ? S_TEMP1 : S_TEMP0];
+        for (int i = lane; i <= hi + 1; i += 32) {
+            sh.x_tm[i] = tm_g[xk0 + i];
+            sh.x_dt[i] = 0.0;   // DTEMPN: 0 outside the cells set below (halo included)
+        }
+        __syncwarp();
+        for (int i = lo + lane; i <= hi; i += 32) {
+            const int k = xk0 + i;
+            const double nph = sh.x_nphi[i];
+            double d = 0.0;
+            const bool ca = ((fabs(nph) > 1.5 * sm_grid) && (nph != 0.0)) ||
+                            ((fabs(c.psi_cn[k] - 0.5) == 0.5) && (nph != 0.0));
+            if (ca) {
+                double dpz, dtdz;
+                if (sh.x_nphi[i - 1] == 0.0) {
+                    dpz = (sh.x_nphi[i + 1] - nph) * g.vvdz(k + 1);
+                    dtdz = (sh.x_tm[i + 1] - sh.x_tm[i]) * g.vvdz(k + 1);
+                } else if (sh.x_nphi[i + 1] == 0.0) {
+                    dpz = (nph - sh.x_nphi[i - 1]) * g.vvdz(k);
+                    dtdz = (sh.x_tm[i] - sh.x_tm[i - 1]) * g.vvdz(k);
+                } else {
+                    dpz = 0.5 * (sh.x_nphi[i + 1] - sh.x_nphi[i - 1]) * g.vvdz(k);
+                    dtdz = 0.5 * (sh.x_tm[i + 1] - sh.x_tm[i - 1]) * g.vvdz(k);
+                }
+                const double dalphi = (0.0 + 0.0) + dpz * dpz;
+                if (dalphi != 0.0) {
+                    const double nz = 1.0;
+                    if (im == 1) d = (0.0 + 0.0) + nz * dtdz * sh.x_psih[i];
+                    else d = (0.0 + 0.0) + nz * dtdz * (1 - sh.x_psih[i]);
+                }
+            } else if (((fabs(nph) <= 1.5 * sm_grid) || (fabs(c.psi_cn[k] - 0.5) != 0.5)) &&
+                       ((nph != 1e-7) && (nph != 0.0))) {
+                if (im == 1) d = (sh.x_tm[i] - ph.t_sat) / nph * sh.x_psih[i];
+                else d = (sh.x_tm[i] - ph.t_sat) / nph * (1.0 - sh.x_psih[i]);
+            }
+            sh.x_dt[i] = d;
+        }
+        __syncwarp();
+        // extension of the normal gradient (nd = 0)
+        double redtl = 0.2 * sm_grid;
+        bool conv = false;
+        for (int halving = 0; halving <= kMaxHalvings && !conv; ++halving) {
+            for (int it = 1; it <= 100; ++it) {
+                ++total;
+                for (int i = lo + lane; i <= hi; i += 32) sh.x_dtrk[i] = sh.x_dt[i];
+                __syncwarp();
+                extp_sweep(g, sh, xk0, lo, hi, sh.x_dt, im, redtl, 0);
+                extp_sweep(g, sh, xk0, lo, hi, sh.x_dt, im, redtl, 0);
+                for (int i = lo + lane; i <= hi; i += 32) sh.x_dt[i] = 0.75 * sh.x_dtrk[i] + 0.25 * sh.x_dt[i];
+                __syncwarp();
+                extp_sweep(g, sh, xk0, lo, hi, sh.x_dt, im, redtl, 0);
+                double rat = 0.0;
+                for (int i = lo + lane; i <= hi; i += 32) {
+                    const double v = 1.0 / 3.0 * sh.x_dtrk[i] + 2.0 / 3.0 * sh.x_dt[i];
+                    sh.x_dt[i] = v;
+                    if (sh.x_dtrk[i] != 0.0) rat = fmax(fabs(v / sh.x_dtrk[i] - 1.0), rat);
+                    else if (v != 0.0) rat = fmax(fabs(sh.x_dtrk[i] / v - 1.0), rat);
+                }
+                rat = warp_maxd(rat);
+                __syncwarp();
+                if (fabs(rat) < eps) {
+                    conv = true;
+                    break;
+                }
+            }
+            if (!conv) redtl = 0.5 * redtl;
+        }
+        if (!conv) return -1;
+        // extension of the phase temperature (nd = 1)
+        redtl = 0.2 * sm_grid;
+        conv = false;
+        for (int halving = 0; halving <= kMaxHalvings && !conv; ++halving) {
+            for (int it = 1; it <= 100; ++it) {
+                ++total;
+                for (int i = lane; i <= hi + 1; i += 32) {
+                    sh.x_trk[i] = sh.x_tm[i];
+                    sh.x_to[i] = sh.x_tm[i];
+                }
+                __syncwarp();
+                extp_sweep(g, sh, xk0, lo, hi, sh.x_to, im, redtl, 1);
+                extp_sweep(g, sh, xk0, lo, hi, sh.x_to, im, redtl, 1);
+                for (int i = lo + lane; i <= hi; i += 32) sh.x_to[i] = 0.75 * sh.x_trk[i] + 0.25 * sh.x_to[i];
+                __syncwarp();
+                extp_sweep(g, sh, xk0, lo, hi, sh.x_to, im, redtl, 1);
+                double rat = 0.0;
+                for (int i = lo + lane; i <= hi; i += 32) {
+                    const double v = 1.0 / 3.0 * sh.x_trk[i] + 2.0 / 3.0 * sh.x_to[i];
+                    sh.x_to[i] = v;
+                    sh.x_tm[i] = v;
+                    if (sh.x_trk[i] != 0.0) rat = fmax(fabs(v / sh.x_trk[i] - 1.0), rat);
+                }
+                rat = warp_maxd(rat);
+                __syncwarp();
+                if (fabs(rat) < eps) {
+                    conv = true;
+                    break;
+                }
+            }
+            if (!conv) redtl = 0.5 * redtl;
+        }
+        if (!conv) return -1;
+        for (int i = lo + lane; i <= hi; i += 32) tm_g[xk0 + i] = sh.x_tm[i];
+        __syncwarp();
+    }
+    return total;
+}
+
+// TEMP_GRAD (chphase.f:55-368) with PHINSINTP, TEMP_EXTP, TEMPASSIGN, TF_GRAD,
+// VOL_TOT_MFDOT and CAL_PSI_TMP(1); 1-D.  All threads call it; the band work runs on warp
+// 0.  Returns the TEMP_EXTP iteration count, or a negative lica_status.
+__device__ int temp_grad(const Geo& g, const Phys& ph, Col& c, Shared& sh, double L, double dtconst) {
+    const int n = g.n, nf = g.nf;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double *temp0 = c.a[S_TEMP0], *temp1 = c.a[S_TEMP1], *nphi = c.a[S_NPHI], *psih = c.a[S_PSIH];
+    FOR_K(0, nf + 6) c.mflvs[k] = 0.0;
+    FOR_K(0, nf + 1) {
+        c.sfgas[k] = 0.0;
+        c.sfgas2[k] = 0.0;
+    }
+    FOR_K(0, n + 1) {
+        c.imask[k] = 0;
+        temp0[k] = c.t[k];
+        temp1[k] = c.t[k];
+        nphi[k] = 0.0;
+        psih[k] = 0.0;
+    }
+    __syncthreads();
+    lvs::Win* s = &sh.win;
+    lvs::Ctx cx;
+    cx.s = s;
+    int st = 0;
+    if (warp == 0) {
+        st = lvs::load_band_window(cx, lane, n, L, c.phi, c.layer);
+        if (lane == 0) sh.ibuf[0] = st;
+    }
+    __syncthreads();
+    st = sh.ibuf[0];
+    if (st != LICA_OK) return -st;
+    if (warp == 0) {
+        // (1) NPHI / PSIH of the flow cells of the band (:147-211), in list order
+        if (lane == 0) {
+            int ic = 0;
+            for (int j = s->lstart[1]; j < s->lstart[lvs::NN2 + 1]; ++j) {
+                const int k = cx.w0 + s->lst[j];
+                const int kk = col::kcoump_vel(g.h, g.hf, n, k);
+                if (nphi[kk] == 0.0) {
+                    const int k1 = 2 * kk - 1, k2 = 2 * kk;
+                    const double zd = (g.zp(kk) - g.zpf(k1)) / (g.zpf(k2) - g.zpf(k1));
+                    const double a1 = cx.p(k1), a2 = cx.p(k2);
+                    const double c00 = a1 * (1.0 - 0.5) + a1 * 0.5;
+                    const double c01 = a2 * (1.0 - 0.5) + a2 * 0.5;
+                    const double c0 = c00 * (1.0 - 0.5) + c00 * 0.5;
+                    const double c1 = c01 * (1.0 - 0.5) + c01 * 0.5;
+                    double nsphi = c0 * (1.0 - zd) + c1 * zd;
+                    if (nsphi > 0.0) ic = 1;
+                    if (nsphi < 0.0) ic = 0;
+                    if (a1 == 0.0 || a2 == 0.0) nsphi = 0.0;
+                    nphi[kk] = 1e-7;
+                    nphi[kk] = nsphi;
+                    if (fabs(c.psi_cn[kk] - 0.5) != 0.5) psih[kk] = (double)ic;
+                    else psih[kk] = c.psi_cn[kk];
+                }
+            }
+            for (int j = s->lstart[lvs::N_MAX]; j < s->lstart[lvs::N_MAX + 1]; ++j) {
+                const int k = cx.w0 + s->lst[j];
+                const int kk = col::kcoump_vel(g.h, g.hf, n, k);
+                const double dx = 0.25, dy = 0.25;
+                const double dz = g.zpf(k) - g.zp(kk);
+                const double pre = s->phi[s->lst[j]] + sqrt(dx * dx + dy * dy + dz * dz);
+                nphi[kk] = fmin(nphi[kk], pre);
+                psih[kk] = c.psi_cn[kk];
+            }
+            // extension range: the cells with NPHI != 0
+            int ka = n + 1, kb = 0;
+            for (int j = s->lstart[1]; j < s->lstart[lvs::N_MAX + 1]; ++j) {
+                const int kk = col::kcoump_vel(g.h, g.hf, n, cx.w0 + s->lst[j]);
+                if (nphi[kk] != 0.0) {
+                    ka = min(ka, kk);
+                    kb = max(kb, kk);
+                }
+            }
+            sh.ibuf[1] = ka;
+            sh.ibuf[2] = kb;
+        }
+        __syncwarp();
+        const int ka = sh.ibuf[1], kb = sh.ibuf[2];
+        int iters = 0;
+        if (kb >= ka) {
+            if (kb - ka + 3 > XR) iters = -LICA_BAND_OVERFLOW;
+            else iters = temp_extp(g, ph, c, sh, ka, kb);
+        }
+        if (lane == 0) sh.ibuf[3] = iters;
+        __syncwarp();
+        if (iters >= 0) {
+            // (3) TF on layers 1..NN1 by TEMPASSIGN (chphase.f:372-463); tf0 in win.rk3, tf1
+            // in win.alphio (window-indexed, 0 elsewhere)
+            for (int q = 0; q < lvs::PER; ++q) {
+                const int i = lane + 32 * q, k = cx.w0 + i, m = s->layer[i];
+                double v0 = 0.0, v1 = 0.0;
+                if (m >= 1 && m <= lvs::NN1) {
+                    const int kk = col::kcoump_vel(g.h, g.hf, n, k);
+                    int kk1, kk2;
+                    double zd;
+                    if (g.zp(kk) > g.zpf(k)) {
+                        kk1 = kk - 1;
+                        kk2 = kk;
+                        zd = (kk1 == kk2) ? 0.0 : (g.zpf(k) - (g.zp(kk) - g.vdz(kk))) / (g.zp(kk2) - g.zp(kk1));
+                    } else {
+                        kk1 = kk;
+                        kk2 = kk + 1;
+                        zd = (kk1 == kk2) ? 0.0 : (g.zpf(k) - g.zp(kk1)) / (g.zp(kk2) - g.zp(kk1));
+                    }
+                    v0 = temp0[kk] * (1.0 - zd) + temp0[kk2] * zd;
+                    v1 = temp1[kk] * (1.0 - zd) + temp1[kk2] * zd;
+                }
+                s->rk3[i] = v0;
+                s->alphio[i] = v1;
+            }
+            __syncwarp();
+            // (4)-(6) TF_GRAD: MFDOT on layers 1..NN1-2
+            for (int q = 0; q < lvs::PER; ++q) {
+                const int i = lane + 32 * q, k = cx.w0 + i, m = s->layer[i];
+                if (m >= 1 && m <= lvs::NN1 - 2) {
+                    const double gz = 0.5 * (s->phi[i + 1] - s->phi[i - 1]) * cx.ssdzf;
+                    const double agi = 1.0 / sqrt((0.0 + 0.0) + gz * gz);
+                    const double dtz0 = 0.5 * (s->rk3[i + 1] - s->rk3[i - 1]) * cx.ssdzf;
+                    const double dtdn0 = ((0.0 + 0.0) + dtz0 * gz) * agi;
+                    const double dtz1 = 0.5 * (s->alphio[i + 1] - s->alphio[i - 1]) * cx.ssdzf;
+                    const double dtdn1 = ((0.0 + 0.0) + dtz1 * gz) * agi;
+                    const double mf = ph.ja * ph.prai * ph.rei * (-ph.tcp * dtdn1 + ph.tcm * dtdn0);
+                    c.mflvs[k + 2] = mf;
+                    s->mf[i] = mf;
+                } else {
+                    s->mf[i] = 0.0;
+                }
+            }
+            // PSIF_MTP = CAL_PSIF_MTP(1, NN1) of the band (snapped band values, column fill)
+            for (int q = 0; q < lvs::PER; ++q) {
+                const int i = lane + 32 * q, m = s->layer[i];
+                s->start[i] = (m >= 1 && m <= lvs::NN1) ? lvs::psif_band(s, i) : 0.0;
+            }
+            __syncwarp();
+            if (lane == 0) {
+                int ktop = -1, kbot = -1;
+                for (int k = nf; k >= 1; --k)
+                    if (cx.p(k) * cx.p(k + 1) < 0.0) {
+                        if (ktop < 0) ktop = k;
+                        kbot = k;
+                    }
+                sh.ibuf[4] = ktop;
+                sh.ibuf[5] = kbot;
+            }
+            __syncwarp();
+            {
+                const int ktop = sh.ibuf[4], kbot = sh.ibuf[5];
+                double t1 = 1.0, t2 = 1.0;
+                if (ktop >= 0) {
+                    t1 = (cx.p(ktop) < 0.0) ? 0.0 : 1.0;
+                    t2 = (cx.p(kbot + 1) < 0.0) ? 0.0 : 1.0;
+                }
+                for (int k = 1 + lane; k <= nf; k += 32) {
+                    const int i = k - cx.w0;
+                    double v;
+                    if (cx.in(k) && s->layer[i] >= 1 && s->layer[i] <= lvs::NN1) v = s->start[i];
+                    else if (ktop < 0) v = 1.0;
+                    else v = (k > kbot) ? t2 : t1;
+                    c.psif_mtp[k] = v;
+                }
+            }
+            __syncwarp();
+            // VOL_TOT_MFDOT: trial advance of layers 1..NN1-2 by the mass flux, reinit,
+            // volume of CAL_PSIF_MTP(1) of the trial band, SFGAS / SFGAS2
+            for (int q = 0; q < lvs::PER; ++q) {
+                const int i = lane + 32 * q, m = s->layer[i];
+                s->wf[i] = s->phi[i];   // ALPHI at entry
+                if (m >= 1 && m <= lvs::NN1 - 2) {
+                    const double mfd = (s->phi[i] > 0.0) ? s->mf[i] / ph.denr : s->mf[i];
+                    const double a0 = s->phi[i];
+                    double a = a0 - 2 * dtconst * mfd;
+                    a = 0.75 * a0 + 0.25 * a;
+                    a = a - dtconst * mfd;
+                    a = 1.0 / 3.0 * a0 + 2.0 / 3.0 * a;
+                    s->nv[i] = a;
+                }
+            }
+            __syncwarp();
+            for (int q = 0; q < lvs::PER; ++q) {
+                const int i = lane + 32 * q, m = s->layer[i];
+                if (m >= 1 && m <= lvs::NN1 - 2) s->phi[i] = s->nv[i];
+            }
+            __syncwarp();
+            lvs::reinitialization(cx, lvs::NN2);
+            for (int q = 0; q < lvs::PER; ++q) {
+                const int i = lane + 32 * q, m = s->layer[i];
+                s->nv[i] = (m >= 1 && m <= lvs::NN1) ? lvs::psif_band(s, i) : 0.0;
+            }
+            __syncwarp();
+            if (lane == 0) {
+                int ktop = -1, kbot = -1;
+                for (int k = nf; k >= 1; --k)
+                    if (cx.p(k) * cx.p(k + 1) < 0.0) {
+                        if (ktop < 0) ktop = k;
+                        kbot = k;
+                    }
+                double t1 = 1.0, t2 = 1.0;
+                if (ktop >= 0) {
+                    t1 = (cx.p(ktop) < 0.0) ? 0.0 : 1.0;
+                    t2 = (cx.p(kbot + 1) < 0.0) ? 0.0 : 1.0;
+                }
+                const double dvol = 0.5 * 0.5 * g.hf;
+                double vol = 0.0;
+                for (int k = 1; k <= nf; ++k) {
+                    const int i = k - cx.w0;
+                    double v;
+                    if (cx.in(k) && s->layer[i] >= 1 && s->layer[i] <= lvs::NN1) v = s->nv[i];
+                    else if (ktop < 0) v = 1.0;
+                    else v = (k > kbot) ? t2 : t1;
+                    const double d = (1.0 - v) * dvol;
+                    vol = vol + d;
+                    vol = vol + d;
+                    vol = vol + d;
+                    vol = vol + d;
+                }
+                c.scal[4] = vol;
+            }
+            for (int q = 0; q < lvs::PER; ++q) {
+                const int i = lane + 32 * q, k = cx.w0 + i, m = s->layer[i];
+                if (m >= 1 && m <= lvs::NN1 - 2 && s->mf[i] != 0.0 && fabs(c.psif_mtp[k] - 0.5) != 0.5) {
+                    const double d = -(s->nv[i] - c.psif_mtp[k]);
+                    if (s->wf[i] > 0.0) {
+                        c.sfgas[k] = -(s->nv[i] - c.psif_mtp[k]) * ph.denr;
+                        c.sfgas2[k] = d;
+                    } else {
+                        c.sfgas[k] = d;
+                        c.sfgas2[k] = d;
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    const int iters = sh.ibuf[3];
+    if (iters < 0) return iters == -1 ? -LICA_NOT_CONVERGED : iters;
+    // (7) CAL_PSI_TMP(1) and IMASK_PH on the z faces (chphase.f:297-357)
+    double* psi_tmp = c.a[S_PSITMP];
+    FOR_K(1, n) {
+        const double v = col::box_mean(c.psif_mtp, nf, 2 * k - 1, 2 * k, g.z(k), g.z(k + 1), g.hf);
+        psi_tmp[k] = (v <= 1e-3) ? 0.0 : (v >= 0.999 ? 1.0 : v);
+    }
+    __syncthreads();
+    FOR_K(2, n) c.imask[k] = (fabs(psi_tmp[k] - psi_tmp[k - 1]) != 0.0) ? 1 : 0;
+    __syncthreads();
+    return iters;
+}
+
+// CAL_CONTINUITY2, 1d.f:3006-3169 (the REGION of CAL_CONTINUITY is unchanged: same PSI_CN).
+__device__ void cal_continuity2(const Geo& g, const Phys& ph, Col& c) {
+    const int n = g.n, nf = g.nf;
+    double *psi_z = c.a[S_PSIZ], *psi_c = c.a[S_PSIC];
+    const int* reg = c.region + 1;
+    FOR_K(1, n) {
+        if (k >= 2) {
+            double v = psi_z[k];
+            if (reg[k] == 2) v = v - col::box_mean(c.sfgas2, nf, 2 * k - 1, 2 * k, g.zp(k - 1), g.zp(k), g.hf);
+            psi_z[k] = (v > 1.0) ? 1.0 : (v < 0.0 ? 0.0 : v);
+        }
+        double v = psi_c[k];
+        if (reg[k] == 2) v = v - col::box_mean(c.sfgas2, nf, 2 * k - 1, 2 * k, g.z(k), g.z(k + 1), g.hf);
+        psi_c[k] = (v > 1.0) ? 1.0 : (v < 0.0 ? 0.0 : v);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        psi_z[1] = psi_z[2];
+        psi_z[n + 1] = psi_z[n];
+        psi_c[1] = psi_c[2];
+        psi_c[n + 1] = psi_c[n];
+    }
+    __syncthreads();
+}
+
+// One substep of RHSNLHS (1d.f:1444-1600).  Returns the TEMP_EXTP iterations or a negative
+// lica_status.
+__device__ int rhsnlhs(const Geo& g, const Phys& ph, Col& c, Shared& sh, double L, int msub, int m_step) {
+    const int n = g.n;
+    const double dt = c.scal[0];
+    const double alpha = 0.5 * (c_gamma[msub] + c_ro[msub]);
+    const double acoef = alpha * dt;
+    const double dtconst = 2. * alpha * dt;
+    const double dtconsti = 1. / dtconst;
+    double *rhs1 = c.a[S_RHS1], *rhsps = c.a[S_RHSPS], *rk3zo = c.a[S_RK3ZO];
+    const double *denf_zi = c.a[S_DENFZI], *psi_c = c.a[S_PSIC], *df_c = c.a[S_DFC];
+    cal_continuity(g, ph, c, dtconst);
+    cal_cont_bc(g, ph, c);
+    // PASSIVE_SCALAR (1d.f:3630-3707)
+    int iters = 0;
+    if (ph.iphs == 1 && m_step != 1) {
+        FOR_K(1, n) {
+            const double r = (c_gamma[msub] * c.t[k] * (c.w[k + 1] - c.w[k]) * g.vvdz(k)) * dt;
+            double densc, denscf;
+            if (c.psi_cn[k] > 0.5) {
+                densc = ph.denscm + ph.densc_diff;
+                denscf = densc;
+            } else {
+                densc = ph.denscm;
+                denscf = densc;
+            }
+            rhsps[k] = ((densc - denscf) * c.t[k] + r) / denscf;
+        }
+        __syncthreads();
+        lhsps(g, ph, c, alpha, dt);   // substitute for the undefined LHSPS2
+        iters = temp_grad(g, ph, c, sh, L, dtconst);
+        if (iters < 0) return iters;
+        cal_continuity2(g, ph, c);
+        cal_cont_bc(g, ph, c);
+    } else {
+        FOR_K(1, n) {
+            const double anps = 0.0, alps = 0.0, anpso = 0.0, tgr = 0.0;
+            const double densc = ph.denscm + ph.densc_diff * c.psi_cn[k];
+            const double uu = 0.5 * (c.w[k + 1] + c.w[k]);
+            const double ameant1 = densc * uu * tgr;
+            const double tct = ph.tcm + ph.tc_diff * ((df_c[k] - ph.denm) * (1.0 / ph.den_diff));
+            const double tcb = ph.tcm + ph.tc_diff * ((df_c[k - 1] - ph.denm) * (1.0 / ph.den_diff));
+            const double ameant2 = (1.0 / (ph.re * ph.prm)) * (tct - tcb) * g.ssdz(k) * tgr;
+            const double r = ((c_gamma[msub] * anps + c_ro[msub] * anpso) + 2. * alpha * alps +
+                              2. * alpha * (ameant1 - ameant2)) *
+                             dt;
+            const double denscf = ph.denscm + ph.densc_diff * psi_c[k];
+            rhsps[k] = ((densc - denscf) * c.t[k] + r) / denscf;
+        }
+        __syncthreads();
+        lhsps(g, ph, c, alpha, dt);
+    }
+    // RHSZ (1d.f:1603-1745) and RHS1 = RHS1 / rho - W (1564-1568)
+    {
+        const double *df_z = c.a[S_DFZ], *vf_z = c.a[S_VFZ];
+        const double* w = c.w;
+        FOR_K(2, n) {
+            const double wt = 0.5 * (w[k + 1] + w[k]);
+            const double wb = 0.5 * (w[k] + w[k - 1]);
+            const double anzz = (df_z[k] * (wt * wt) - df_z[k - 1] * (wb * wb)) * g.vvdz(k);
+            const double anz = -0.0 - 0.0 - anzz;
+            const double alz5 = (w[k + 1] - w[k]) * g.ssdz(k);
+            const double alz6 = (w[k] - w[k - 1]) * g.ssdz(k - 1);
+            const double alzz = (vf_z[k] * alz5 - vf_z[k - 1] * alz6) * g.vvdz(k);
+            const double alz_sum1 = 0.0 + 0.0 + alzz + alzz;
+            const double alz_sum2 = 0.0 + 0.0;
+            const double pgr_z = (c.p[k] - c.p[k - 1]) * g.vvdz(k);
+            const double den_zn = ph.denm + ph.den_diff * c.psi_zn[k];
+            const double rk3z = anz + alz_sum2;
+            const double cn2z = alz_sum1;
+            const double sur_z = 0.0, buoy = 0.0, pmi = 0.0;
+            double r = den_zn * w[k] + (c_gamma[msub] * rk3z + c_ro[msub] * rk3zo[k] + 2. * alpha * cn2z +
+                                        2. * alpha * (sur_z - pgr_z) - 2. * alpha * buoy - 2. * alpha * (pmi + 0.0)) *
+                                           dt;
+            if (ph.iphs == 1 && c.imask[k] == 1 && fabs(c.psi_zn[k] - 0.5) != 0.5)
+                r = r + c_gamma[msub] * dt * den_zn * w[k] *
+                            ((0.0 - 0.0) * 1.0 + (0.0 - 0.0) * 1.0 + (wt - wb) * g.vvdz(k));
+            rhs1[k] = r * denf_zi[k] - w[k];
+            rk3zo[k] = rk3z;
+        }
+        __syncthreads();
+    }
+    // LHSW (1d.f:1749-1809)
+    {
+        double *ak = c.a[S_AK], *bk = c.a[S_BK], *ck = c.a[S_CK], *gk = c.a[S_GK];
+        const double* vf_z = c.a[S_VFZ];
+        FOR_K(2, n) {
+            const double dk1 = 2. * acoef * denf_zi[k] * vf_z[k - 1] * g.akw(k);
+            const double dk3 = 2. * acoef * denf_zi[k] * vf_z[k] * g.ckw(k);
+            const double dk2 = -dk1 - dk3;
+            ak[k] = dk1;
+            ck[k] = dk3;
+            bk[k] = 1. + dk2;
+            gk[k] = rhs1[k];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) thomas(ak, bk, ck, gk, c.a[S_GAM], 2, n);
+        __syncthreads();
+        FOR_K(2, n) c.w[k] = gk[k] + c.w[k];
+        __syncthreads();
+    }
+    // BC + BC_FLUX (1d.f:1812-1923)
+    if (threadIdx.x == 0) {
+        c.w[1] = 0.0;
+        c.w[n + 1] = c.w[n];
+        double qq3 = 0.0;
+        qq3 = qq3 + (c.w[n + 1] - c.w[1]) * 1.0 * 1.0;
+        double aa = 0.0;
+        aa = aa + 2. * 1.0 * 1.0;
+        const double ubc_avg = -qq3 / aa;
+        c.w[1] = 0.0;
+        c.w[n + 1] = c.w[n + 1] + ubc_avg;
+    }
+    __syncthreads();
+    // FSM_CHOI (1d.f:3365-3400) and DIVGS (1d.f:3180-3303)
+    {
+        double* divg = c.a[S_DIVG];
+        FOR_K(2, n) c.w[k] = c.w[k] + dtconst * ((c.p[k] - c.p[k - 1]) * g.vvdz(k)) * denf_zi[k];
+        __syncthreads();
+        FOR_K(1, n) {
+            double d = (k <= n - 1) ? (c.w[k + 1] - c.w[k]) * g.ssdz(k) : 0.0;
+            if (ph.iphs == 1) {
+                const double ssum = col::box_mean(c.sfgas, g.nf, 2 * k - 1, 2 * k, g.z(k), g.z(k + 1), g.hf);
+                d = d - ssum * (ph.den_diff / (ph.denp * ph.denm));
+            }
+            if (k >= 2) d = d * dtconsti;
+            divg[k] = d;
+        }
+        __syncthreads();
+        // POISSON (1d.f:3492-3578)
+        double *ak = c.a[S_AK], *bk = c.a[S_BK], *ck = c.a[S_CK], *gk = c.a[S_GK];
+        FOR_K(1, n) {
+            const double fixkl = (k == 1) ? 1.0 : 0.0;
+            const double a = g.vvdz(k) * g.ssdz(k) * denf_zi[k] * (1.0 - fixkl);
+            const double cc = g.vvdz(k + 1) * g.ssdz(k) * denf_zi[k + 1];
+            ak[k] = a;
+            ck[k] = cc;
+            bk[k] = -(a + cc);
+            gk[k] = divg[k];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            thomas(ak, bk, ck, gk, c.a[S_GAM], 1, n);
+            for (int k = 1; k <= n; ++k) c.p[k] = gk[k];
+            c.p[0] = c.p[1];
+            c.p[n + 1] = c.p[n];
+        }
+        __syncthreads();
+        // UCALC (1d.f:3582-3627) and the reference shift P -= P(1) (1d.f:3431-3446)
+        FOR_K(2, n) c.w[k] = c.w[k] - dtconst * (c.p[k] - c.p[k - 1]) * g.vvdz(k) * denf_zi[k];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            c.w[1] = 0.0;
+            c.w[n + 1] = c.w[n];
+            sh.dbuf[0] = c.p[1];
+        }
+        __syncthreads();
+        const double phiref = sh.dbuf[0];
+        FOR_K(1, n) c.p[k] = c.p[k] - phiref;
+        __syncthreads();
+        if (threadIdx.x == 0) c.p[0] = c.p[1];
+        __syncthreads();
+    }
+    return iters;
+}
+
+// One time step (1d.f:190-250).  Returns a lica_status.
+__device__ int column_step(const Geo& g, const Phys& ph, Col& c, Shared& sh, double L) {
+    const int n = g.n;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int m_step = (int)c.scal[2] + 1;
+    __syncthreads();
+    if (tid == 0) c.scal[2] = c.scal[2] + 1.0;
+    if (m_step == 1) FOR_K(0, g.nf + 6) c.mflvs[k] = 0.0;
+    // DETERMINE_DT + CFL (1d.f:683-817, 1325-1373)
+    {
+        const double dt = c.scal[0];
+        double dsrc = 1000.0, cfl = 0.0;
+        FOR_K(1, n) {
+            if (ph.time_st != 0.0 && fabs(c.psi_cn[k] - 0.5) < 0.5) {
+                const double dx1 = fmin(1.0, g.sdz(k));
+                const double t1 = 0.5 * dx1 / sqrt(ph.time_st / dx1 + ph.time_gv * dx1);
+                const double dx2 = fmax(1.0, g.sdz(k));
+                const double t2 = 0.5 * dx2 / sqrt(ph.time_st / dx2 + ph.time_gv * dx2);
+                dsrc = fmin(dsrc, fmin(t1, t2));
+            }
+            const double c3 = fabs(c.w[k] + c.w[k + 1]) * g.ssdz(k);
+            cfl = fmax(0.5 * ((0.0 + 0.0) + c3) * dt, cfl);
+        }
+        dsrc = block_min(dsrc, sh);
+        cfl = block_max(cfl, sh);
+        if (ph.time_st == 0.0) dsrc = 1000000.0;
+        __syncthreads();
+        if (tid == 0) {
+            const double dt_old = dt;
+            const double cfl_surf = dt / dsrc;
+            const double cfl_sum = 0.5 * (cfl + sqrt(cfl * cfl + 4.0 * cfl_surf));
+            double dtn = dt * ph.cflmax / cfl_sum;
+            if (dtn / dt_old > 2.0) dtn = dt_old * 1.2;
+            c.scal[0] = dtn;
+            c.stats[0] = cfl;
+        }
+        __syncthreads();
+    }
+    FOR_K(0, n + 1) c.a[S_RK3ZO][k] = 0.0;
+    __syncthreads();
+    double iters = 0.0, subcycles = 0.0, imass = 0.0, dvmax = 0.0;
+    for (int msub = 1; msub <= 3; ++msub) {
+        const int it = rhsnlhs(g, ph, c, sh, L, msub, m_step);
+        if (it < 0) return -it;
+        iters += it;
+        // CONVRGE1 (1d.f:3306-3362)
+        double dv = 0.0;
+        FOR_K(1, n) {
+            double d = (c.w[k + 1] - c.w[k]) * g.ssdz(k);
+            if (ph.iphs == 1) {
+                const double ssum = col::box_mean(c.sfgas, g.nf, 2 * k - 1, 2 * k, g.z(k), g.z(k + 1), g.hf);
+                d = d - ssum * (ph.den_diff / ph.denp);
+            }
+            dv = fmax(fabs(d), dv);
+        }
+        dvmax = block_max(dv, sh);
+        // TRANSPORT + GRID_COUPLING(0) on warp 0
+        __syncthreads();
+        const double dtconst = 2. * (0.5 * (c_gamma[msub] + c_ro[msub])) * c.scal[0];
+        if (warp == 0) {
+            lvs::Params P{ph.iphs, (m_step == 1 && msub == 1) ? 1 : 0, m_step, ph.mglobal, ph.denr, dtconst};
+            double lst[4] = {0, 0, 0, 0};
+            double* st4 = c.stats + 4;   // scratch for the transport statistics
+            const int st = lvs::transport_column(&sh.win, lane, n, L, c.phi, c.layer, c.psif, c.wo, c.w, c.mflvs,
+                                                 &c.scal[3], c.scal[4], c.psi_cn, c.psi_zn, st4, P);
+            __syncwarp();
+            if (lane == 0) {
+                for (int q = 0; q < 4; ++q) lst[q] = st4[q];
+                sh.ibuf[6] = st;
+                sh.dbuf[1] = lst[0];
+                sh.dbuf[2] = (lst[0] > 0) ? lst[3] : 0.0;
+            }
+        }
+        __syncthreads();
+        if (sh.ibuf[6] != LICA_OK) return sh.ibuf[6];
+        subcycles += sh.dbuf[1];
+        imass += sh.dbuf[2];
+    }
+    __syncthreads();
+    if (tid == 0) {
+        c.scal[1] = c.scal[1] + c.scal[0];
+        double zi = 0.0;
+        for (int k = 1; k < g.nf; ++k)
+            if (c.layer[k + 2] > 0 && c.layer[k + 3] > 0 && c.phi[k + 2] < 0.0 && c.phi[k + 3] >= 0.0) {
+                zi = g.zpf(k) - c.phi[k + 2] * (g.zpf(k + 1) - g.zpf(k)) / (c.phi[k + 3] - c.phi[k + 2]);
+                break;
+            }
+        c.stats[1] = dvmax;
+        c.stats[2] = iters;
+        c.stats[3] = subcycles;
+        c.stats[4] = imass;
+        c.stats[5] = zi;
+        c.stats[6] = c.scal[4];
+        c.stats[7] = c.scal[0];
+    }
+    __syncthreads();
+    return LICA_OK;
+}
+
+__global__ void __launch_bounds__(NT) k_column_steps(const __grid_constant__ Args A) {
+    __shared__ Shared sh;
+    const int col = blockIdx.x;
+    if (col >= A.ncol) return;
+    const int n = A.n, nf = 2 * n;
+    const size_t sf = (size_t)n + 2, sp = (size_t)nf + 7, sq = (size_t)nf + 2;
+    Col c;
+    c.w = A.w + col * sf;
+    c.p = A.p + col * sf;
+    c.t = A.t + col * sf;
+    c.psi_cn = A.psi_cn + col * sf;
+    c.psi_zn = A.psi_zn + col * sf;
+    c.wo = A.wo + col * sf;
+    c.imask = A.imask + col * sf;
+    c.phi = A.phi + col * sp;
+    c.layer = A.layer + col * sp;
+    c.mflvs = A.mflvs + col * sp;
+    c.psif = A.psif + col * sq;
+    c.sfgas = A.sfgas + col * sq;
+    c.sfgas2 = A.sfgas2 + col * sq;
+    c.scal = A.scal + col * 5;
+    c.stats = A.stats + col * 8;
+    double* d = A.dscr + col * (NFLOW * sf + sq);
+    for (int q = 0; q < NFLOW; ++q) c.a[q] = d + q * sf;
+    c.psif_mtp = d + NFLOW * sf;
+    c.region = A.iscr + col * (sf + 2);
+    Geo g{n, nf, A.L / n, A.L / nf};
+    int st = LICA_OK;
+    for (int s = 0; s < A.nsteps && st == LICA_OK; ++s) st = column_step(g, A.ph, c, sh, A.L);
+    if (threadIdx.x == 0) A.status[col] = st;
+}
+
+}  // namespace colk
+}  // namespace lica
+
+using namespace lica;
+
+namespace {
+
+colk::Phys make_phys(const lica_col_props* p) {
+    colk::Phys ph;
+    const double pi = std::acos(-1.0);
+    ph.re = p->re;
+    ph.rei = 1.0 / ph.re;
+    ph.denm = 1.0;
+    ph.denp = p->denr;
+    ph.den_diff = ph.denp - ph.denm;
+    ph.vism = 1.0 * ph.rei;
+    ph.visp = p->visr * ph.rei;
+    ph.denscm = ph.denm * 1.0;
+    ph.denscp = ph.denscm * (p->denr * p->scr);
+    ph.densc_diff = ph.denscp - ph.denscm;
+    ph.tcm = 1.0;
+    ph.tcp = p->tcr;
+    ph.tc_diff = ph.tcp - ph.tcm;
+    ph.prm = p->prm;
+    ph.prai = 1.0 / p->prm;
+    ph.surf = (p->weber == 0.0) ? 0.0 : 1.0 / p->weber;
+    ph.gravity = (p->fr == 0.0) ? 0.0 : 1.0 / (p->fr * p->fr);
+    ph.time_st = ph.surf * pi / (ph.denm + ph.denp);
+    ph.time_gv = ph.den_diff / (ph.denm + ph.denp) * ph.gravity / pi;
+    ph.denr = p->denr;
+    ph.ja = p->jakob;
+    ph.t_sat = p->t_sat;
+    ph.cflmax = p->cflmax;
+    ph.iphs = p->iphs;
+    ph.mglobal = p->mglobal;
+    return ph;
+}
+
+struct ScratchCache {
+    std::mutex mu;
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+ScratchCache& scratch_cache() {
+    static ScratchCache s;
+    return s;
+}
+
+
+// Host-side initial state (runs once, before the time loop).
+double h_zp(double h, int n, int k) {
+    if (k <= 0) return 0.0;
+    if (k >= n + 1) return n * h;
+    return (k - 1) * h + 0.5 * h;
+}
+
+double h_box_mean(const double* f, int nf, int k1, int k2, double z1, double z2, double hf) {
+    const double ssdzf = 1.0 / hf;
+    double sum = 0.0, volf = 0.0;
+    for (int rep = 0; rep < 4; ++rep)
+        for (int kk = k1; kk <= k2; ++kk) {
+            const double v = f[kk < 1 ? 1 : (kk > nf ? nf : kk)];
+            const double za = (kk - 1) * hf, zb = kk * hf;
+            if (za <= z1 && zb >= z2) {
+                sum = sum + v;
+                volf = volf + 1.0;
+                break;
+            } else if (za < z1 && zb > z1) {
+                sum = sum + v * (zb - z1) * ssdzf;
+                volf = volf + (zb - z1) * ssdzf;
+            } else if (za >= z1 && zb <= z2) {
+                sum = sum + v;
+                volf = volf + 1.0;
+            } else if (za < z2 && zb > z2) {
+                sum = sum + v * (z2 - za) * ssdzf;
+                volf = volf + (z2 - za) * ssdzf;
+            } else if (za >= z2) {
+                break;
+            }
+        }
+    return sum / volf;
+}
+
+}  // namespace
+
+extern "C" {
+
+// MAKEFLD (1d.f:821-946, IPHS = 1), LVSINIT (two_phase.f:116-388) and GRID_COUPLING(1) for
+// a planar film.  LVSINIT's band generation from the candidate cells |phi| <= CRI reduces,
+// for one plane, to: S-tube = the two cells around the interface, layer m at m-1 cells
+// from it (never k = 1 or nf+1), phi = the signed distance ASSIGN_LVS gives; PSIF is
+// CAL_PSIF_MTP(1, N_MAX) with the column fill, the vapour volume its (1 - PSIF) sum.
+int lica_gpu_column_init(int32_t n, double length, double z0, const lica_col_props* props, lica_col_state* st) {
+    if (n < 8 || !(length > 0.0) || !props || !st || !st->w || !st->p || !st->t || !st->psi_cn || !st->psi_zn ||
+        !st->phi || !st->layer || !st->psif || !st->wo || !st->mflvs || !st->sfgas || !st->sfgas2 || !st->imask ||
+        !st->scal || !st->stats)
+        return LICA_BAD_ARG;
+    const int nf = 2 * n;
+    const double h = length / n, hf = length / nf;
+    for (int k = 0; k <= n + 1; ++k) {
+        st->w[k] = st->p[k] = st->t[k] = st->psi_cn[k] = st->psi_zn[k] = st->wo[k] = 0.0;
+        st->imask[k] = 0;
+    }
+    for (int k = 1; k <= n; ++k) {
+        const double pbody = (h_zp(h, n, k) - z0) + 1e-12;
+        if (pbody > 0.0) {
+            st->t[k] = 1.0;
+            st->w[k] = 1.0;
+            st->w[n + 1] = 1.0;
+        } else {
+            st->t[k] = 16.47 * h_zp(h, n, k);
+            st->t[0] = 0.0;
+            st->w[k] = 0.0;
+            st->w[1] = 0.0;
+        }
+    }
+    auto assign = [&](int k) { return (((k - 1) * hf + 0.5 * hf) - z0) + 1e-12; };
+    // the one crossing among the candidates |phi| <= CRI = 1.2 MAX(SDXF,SDYF,SDZF)
+    const double cri = 1.2 * std::max(std::max(0.5, 0.5), hf);
+    int ks = -1, ncross = 0;
+    for (int k = 1; k < nf; ++k) {
+        const double a = assign(k), b = assign(k + 1);
+        if (std::fabs(a) <= cri && std::fabs(b) <= cri && a * b < 0.0) {
+            ks = k;
+            ++ncross;
+        }
+    }
+    if (ncross != 1 || ks < 2) {
+        lica_set_last_error("lica_gpu_column_init", "need one interface above the first refined cell", __FILE__,
+                            __LINE__);
+        return LICA_BAD_ARG;
+    }
+    for (int q = 0; q < nf + 7; ++q) {
+        st->phi[q] = 0.0;
+        st->layer[q] = 0;
+        st->mflvs[q] = 0.0;
+    }
+    for (int j = 0; j <= 10; ++j) {
+        const int lo = ks - j, hi = ks + 1 + j;
+        if (lo >= 2) st->layer[lo + 2] = 1 + j;
+        if (hi <= nf) st->layer[hi + 2] = 1 + j;
+    }
+    for (int k = 1; k <= nf; ++k)
+        if (st->layer[k + 2] > 0) st->phi[k + 2] = assign(k);
+    auto P = [&](int k) { return st->phi[k + 2]; };
+    std::vector<double> ps(nf + 2, 0.0);
+    for (int k = 1; k <= nf; ++k) {
+        if (st->layer[k + 2] == 0) continue;
+        const double e1 = 0.5 * std::fabs(P(k + 1) - P(k - 1));
+        double t;
+        if (e1 > 1e-8) {
+            const double f1 = std::max(0.5 * (e1 + 0.0 + 0.0) - std::fabs(P(k)), 0.0);
+            t = f1 / e1;
+        } else {
+            t = (P(k) != 0.0) ? 0.0 : 0.5;
+        }
+        double v = (P(k) <= 0.0) ? t : 1.0 - t;
+        if (v < 1e-5) v = 0.0;
+        else if (v > 0.99999) v = 1.0;
+        ps[k] = v;
+    }
+    const double t1 = (P(ks) < 0.0) ? 0.0 : 1.0, t2 = (P(ks + 1) < 0.0) ? 0.0 : 1.0;
+    for (int k = 1; k <= nf; ++k)
+        if (st->layer[k + 2] == 0) ps[k] = (k > ks) ? t2 : t1;
+    const double dvol = 0.5 * 0.5 * hf;
+    double vol = 0.0;
+    for (int k = 1; k <= nf; ++k)
+        for (int r = 0; r < 4; ++r) vol = vol + (1.0 - ps[k]) * dvol;
+    for (int k = 0; k <= nf + 1; ++k) {
+        st->psif[k] = (k >= 1 && k <= nf) ? ps[k] : 0.0;
+        st->sfgas[k] = 0.0;
+        st->sfgas2[k] = 0.0;
+    }
+    // GRID_COUPLING(1)
+    for (int k = 2; k <= n; ++k)
+        st->psi_zn[k] = h_box_mean(st->psif, nf, 2 * k - 2, 2 * k - 1, h_zp(h, n, k - 1), h_zp(h, n, k), hf);
+    for (int k = 1; k <= n; ++k) {
+        if (st->psi_zn[k] < 1e-3) st->psi_zn[k] = 0.0;
+        else if (st->psi_zn[k] > 0.999) st->psi_zn[k] = 1.0;
+    }
+    for (int k = 1; k <= n; ++k)
+        st->psi_cn[k] = h_box_mean(st->psif, nf, 2 * k - 1, 2 * k, (k - 1) * h, k * h, hf);
+    for (int k = 1; k <= n; ++k) {
+        if (st->psi_cn[k] < 1e-3) st->psi_cn[k] = 0.0;
+        else if (st->psi_cn[k] > 0.999) st->psi_cn[k] = 1.0;
+    }
+    st->psi_cn[0] = st->psi_cn[1];
+    st->psi_cn[n + 1] = st->psi_cn[n];
+    st->scal[0] = props->dt0;
+    st->scal[1] = 0.0;
+    st->scal[2] = 0.0;
+    st->scal[3] = vol;
+    st->scal[4] = vol;
+    for (int q = 0; q < 8; ++q) st->stats[q] = 0.0;
+    return LICA_OK;
+}
+
+size_t lica_gpu_column_scratch_bytes(int32_t ncol, int32_t n) {
+    const size_t sf = (size_t)n + 2, sq = 2 * (size_t)n + 2;
+    return (size_t)ncol * ((colk::NFLOW * sf + sq) * sizeof(double) + (sf + 2) * sizeof(int)) + 256;
+}
+
+int lica_gpu_column_steps_device(int32_t ncol, int32_t n, double length, const lica_col_props* props,
+                                 const lica_col_state* st, int32_t nsteps, void* scratch, int32_t* status,
+                                 void* stream) {
+    if (ncol < 1 || n < 8 || n > (1 << 20) || !(length > 0.0) || !props || !st || nsteps < 0 || !status) {
+        lica_set_last_error("lica_gpu_column_steps_device", "bad sizes or null pointers", __FILE__, __LINE__);
+        return LICA_BAD_ARG;
+    }
+    colk::Args A;
+    A.ncol = ncol;
+    A.n = n;
+    A.nsteps = nsteps;
+    A.L = length;
+    A.ph = make_phys(props);
+    A.w = st->w;
+    A.p = st->p;
+    A.t = st->t;
+    A.psi_cn = st->psi_cn;
+    A.psi_zn = st->psi_zn;
+    A.phi = st->phi;
+    A.layer = st->layer;
+    A.psif = st->psif;
+    A.wo = st->wo;
+    A.mflvs = st->mflvs;
+    A.sfgas = st->sfgas;
+    A.sfgas2 = st->sfgas2;
+    A.imask = st->imask;
+    A.scal = st->scal;
+    A.stats = st->stats;
+    A.status = status;
+    void* scr = scratch;
+    if (!scr) {
+        ScratchCache& sc = scratch_cache();
+        std::lock_guard<std::mutex> lk(sc.mu);
+        const size_t need = lica_gpu_column_scratch_bytes(ncol, n);
+        if (need > sc.bytes) {
+            if (sc.ptr) cudaFree(sc.ptr);
+            sc.ptr = nullptr;
+            sc.bytes = 0;
+            LICA_CUDA_TRY(cudaMalloc(&sc.ptr, need));
+            sc.bytes = need;
+        }
+        scr = sc.ptr;
+    }
+    const size_t sf = (size_t)n + 2, sq = 2 * (size_t)n + 2;
+    A.dscr = (double*)scr;
+    A.iscr = (int*)((char*)scr + (size_t)ncol * (colk::NFLOW * sf + sq) * sizeof(double));
+    colk::k_column_steps<<<ncol, colk::NT, 0, (cudaStream_t)stream>>>(A);
+    LICA_CUDA_TRY(cudaGetLastError());
+    lica_count_launches(1);
+    return LICA_OK;
+}
+
+int lica_gpu_column_steps(int32_t ncol, int32_t n, double length, const lica_col_props* props, lica_col_state* st,
+                          int32_t nsteps, int32_t* status) {
+    if (ncol < 1 || n < 8 || !props || !st || !status) return LICA_BAD_ARG;
+    const size_t nc = (size_t)ncol, sf = (size_t)n + 2, sp = 2 * (size_t)n + 7, sq = 2 * (size_t)n + 2;
+    struct F {
+        void* h;
+        size_t bytes;
+    };
+    const F f[] = {{st->w, 8 * nc * sf},      {st->p, 8 * nc * sf},      {st->t, 8 * nc * sf},
+                   {st->psi_cn, 8 * nc * sf}, {st->psi_zn, 8 * nc * sf}, {st->phi, 8 * nc * sp},
+                   {st->layer, 4 * nc * sp},  {st->psif, 8 * nc * sq},   {st->wo, 8 * nc * sf},
+                   {st->mflvs, 8 * nc * sp},  {st->sfgas, 8 * nc * sq},  {st->sfgas2, 8 * nc * sq},
+                   {st->imask, 4 * nc * sf},  {st->scal, 8 * nc * 5},    {st->stats, 8 * nc * 8}};
+    const int nfld = (int)(sizeof(f) / sizeof(f[0]));
+    for (int q = 0; q < nfld; ++q)
+        if (!f[q].h) return LICA_BAD_ARG;
+    size_t off[16], total = 0;
+    for (int q = 0; q < nfld; ++q) {
+        off[q] = total;
+        total += (f[q].bytes + 255) & ~(size_t)255;
+    }
+    const size_t st_off = total;
+    total += (4 * nc + 255) & ~(size_t)255;
+    char* base = nullptr;
+    LICA_CUDA_TRY(cudaMalloc(&base, total));
+    struct Guard {
+        char* p;
+        ~Guard() { cudaFree(p); }
+    } guard{base};
+    for (int q = 0; q < nfld; ++q) LICA_CUDA_TRY(cudaMemcpy(base + off[q], f[q].h, f[q].bytes, cudaMemcpyHostToDevice));
+    lica_col_state d;
+    d.w = (double*)(base + off[0]);
+    d.p = (double*)(base + off[1]);
+    d.t = (double*)(base + off[2]);
+    d.psi_cn = (double*)(base + off[3]);
+    d.psi_zn = (double*)(base + off[4]);
+    d.phi = (double*)(base + off[5]);
+    d.layer = (int32_t*)(base + off[6]);
+    d.psif = (double*)(base + off[7]);
+    d.wo = (double*)(base + off[8]);
+    d.mflvs = (double*)(base + off[9]);
+    d.sfgas = (double*)(base + off[10]);
+    d.sfgas2 = (double*)(base + off[11]);
+    d.imask = (int32_t*)(base + off[12]);
+    d.scal = (double*)(base + off[13]);
+    d.stats = (double*)(base + off[14]);
+    int32_t* dst = (int32_t*)(base + st_off);
+    int rc = lica_gpu_column_steps_device(ncol, n, length, props, &d, nsteps, nullptr, dst, nullptr);
+    if (rc) return rc;
+    LICA_CUDA_TRY(cudaDeviceSynchronize());
+    for (int q = 0; q < nfld; ++q)
+        LICA_CUDA_TRY(cudaMemcpy(f[q].h, base + off[q], f[q].bytes, cudaMemcpyDeviceToHost));
+    LICA_CUDA_TRY(cudaMemcpy(status, dst, 4 * nc, cudaMemcpyDeviceToHost));
+    int worst = LICA_OK;
+    for (size_t c = 0; c < nc; ++c)
+        if (status[c] != LICA_OK) worst = status[c];
+    return worst;
+}
+
+}  // extern "C"

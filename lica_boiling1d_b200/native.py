@@ -29,6 +29,19 @@ class LvsParams(C.Structure):
 _I32 = C.POINTER(C.c_int32)
 
 
+class ColProps(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("re", "visr", "denr", "weber", "fr", "prm", "scr", "tcr", "t_sat",
+                                           "jakob", "cflmax", "dt0")] + [("iphs", C.c_int32), ("mglobal", C.c_int32)]
+
+
+COL_FIELDS = ("w", "p", "t", "psi_cn", "psi_zn", "phi", "layer", "psif", "wo", "mflvs", "sfgas", "sfgas2", "imask",
+              "scal", "stats")
+
+
+class ColState(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in COL_FIELDS]
+
+
 # every symbol include/lica_gpu.h declares, with its ctypes signature
 SIGNATURES = {
     "lica_last_error": (C.c_char_p, []),
@@ -54,6 +67,13 @@ SIGNATURES = {
                                          _D, _I32, _D, C.POINTER(LvsParams)]),
     "lica_gpu_lvs_transport_device": (C.c_int, [C.c_int32, C.c_int32, C.c_double] + [C.c_void_p] * 12 +
                                       [C.POINTER(LvsParams), C.c_void_p]),
+    "lica_gpu_column_init": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.POINTER(ColProps),
+                                       C.POINTER(ColState)]),
+    "lica_gpu_column_scratch_bytes": (C.c_size_t, [C.c_int32, C.c_int32]),
+    "lica_gpu_column_steps_device": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.POINTER(ColProps),
+                                               C.POINTER(ColState), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "lica_gpu_column_steps": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.POINTER(ColProps), C.POINTER(ColState),
+                                        C.c_int32, _I32]),
 }
 
 STATUS = {0: "LICA_OK", 1: "LICA_NOT_CONVERGED", 2: "LICA_BAND_OVERFLOW", 3: "LICA_NAN", 4: "LICA_BAD_ARG",

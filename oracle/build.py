@@ -11,7 +11,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SOURCES = ["mg2d.cpp", "tridiag.cpp", "lvs1d.cpp"]
+SOURCES = ["mg2d.cpp", "tridiag.cpp", "lvs1d.cpp", "column1d.cpp"]
 
 
 def lib_path(native: bool = False) -> str:
@@ -23,7 +23,8 @@ def build(native: bool = False, force: bool = False) -> str:
     srcs = [os.path.join(HERE, s) for s in SOURCES]
     if not force and os.path.exists(out):
         mt = os.path.getmtime(out)
-        if all(os.path.getmtime(s) <= mt for s in srcs + [__file__]):
+        hdrs = [os.path.join(HERE, h) for h in os.listdir(HERE) if h.endswith(".hpp")]
+        if all(os.path.getmtime(s) <= mt for s in srcs + hdrs + [__file__]):
             return out
     os.makedirs(os.path.dirname(out), exist_ok=True)
     arch = "-march=native" if native else "-march=x86-64-v2"

@@ -36,6 +36,9 @@ def lib(native: bool = False):
         L.orc_lvs_alphi_bc.argtypes = [C.c_int, C.c_double, _D]
         L.orc_lvs_band.argtypes = [C.c_int, C.c_double, _D, _INT]
         L.orc_lvs_reinit.argtypes = [C.c_int, C.c_double, _D, _INT, C.c_int]
+        L.orc_col_init.argtypes = [C.c_int, C.c_double, C.c_double, _D, _INT] + [_D] * 6 + [_INT] + [_D] * 5 + \
+            [_INT, _D]
+        L.orc_col_step.argtypes = [C.c_int, C.c_double, _D, _INT] + [_D] * 6 + [_INT] + [_D] * 5 + [_INT, _D, _D]
         _LIBS[key] = L
     return _LIBS[key]
 
@@ -187,3 +190,48 @@ def lvs_reinit(n, length, phi, layer, ilimit):
     phi = np.array(phi, dtype=np.float64, copy=True)
     lib().orc_lvs_reinit(n, length, _p(phi), _pi(np.ascontiguousarray(layer, dtype=np.int32)), ilimit)
     return phi
+
+
+# ---------------------------------------------------------------------------------------
+# 1-D column time step (oracle/column1d.cpp).  State dict of one column with the arrays of
+# lica_col_state: w p t psi_cn psi_zn wo (n+2), phi mflvs (nf+7), layer (nf+7 int32),
+# psif sfgas sfgas2 (nf+2), imask (n+2 int32), scal (5), stats (8).
+# ---------------------------------------------------------------------------------------
+COL_PROPS = ("re", "visr", "denr", "weber", "fr", "prm", "scr", "tcr", "t_sat", "jakob", "cflmax", "dt0")
+COL_ORDER = ("w", "p", "t", "psi_cn", "psi_zn", "phi", "layer", "psif", "wo", "mflvs", "sfgas", "sfgas2", "imask",
+             "scal")
+
+
+def _col_props(props):
+    return (np.array([float(getattr(props, k)) for k in COL_PROPS]),
+            np.array([int(props.iphs), int(props.mglobal)], np.int32))
+
+
+def _col_args(st):
+    return [_pi(st[k]) if st[k].dtype == np.int32 else _p(st[k]) for k in COL_ORDER]
+
+
+def col_empty(n):
+    nf = 2 * n
+    sf, sp, sq = n + 2, nf + 7, nf + 2
+    st = {k: np.zeros(sf) for k in ("w", "p", "t", "psi_cn", "psi_zn", "wo")}
+    st.update({"phi": np.zeros(sp), "mflvs": np.zeros(sp), "layer": np.zeros(sp, np.int32), "psif": np.zeros(sq),
+               "sfgas": np.zeros(sq), "sfgas2": np.zeros(sq), "imask": np.zeros(sf, np.int32), "scal": np.zeros(5),
+               "stats": np.zeros(8)})
+    return st
+
+
+def col_init(n, length, z0, props):
+    st = col_empty(n)
+    pr, ip = _col_props(props)
+    rc = lib().orc_col_init(n, length, z0, _p(pr), _pi(ip), *_col_args(st))
+    if rc:
+        raise ValueError(f"orc_col_init returned {rc}")
+    return st
+
+
+def col_step(st, n, length, props, native=False):
+    """One time step in place.  Returns the status (0 ok, 1 TEMP_EXTP not converged,
+    2 band overflow)."""
+    pr, ip = _col_props(props)
+    return lib(native).orc_col_step(n, length, _p(pr), _pi(ip), *_col_args(st), _p(st["stats"]))

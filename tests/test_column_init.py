@@ -1,0 +1,31 @@
+"""Initial state of the 1-D column: the library's host-side MAKEFLD + LVSINIT +
+GRID_COUPLING(1) (lica_gpu_column_init, no GPU needed) against the oracle, bit for bit,
+and the known answers of a planar film (signed distance, vapour volume = film height)."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+
+@pytest.mark.parametrize("n,z0", [(256, 0.0607), (512, 0.1), (128, 0.3333), (64, 0.05), (16, 0.5)])
+def test_init_matches_oracle(n, z0):
+    from lica_boiling1d_b200.column import ColumnProps, Columns
+    props = ColumnProps()
+    cols = Columns.film(n, 1.0, [z0], props)
+    ref = O.col_init(n, 1.0, z0, props)
+    for k, v in ref.items():
+        if k == "stats":
+            continue
+        assert np.array_equal(cols.arrays[k][0], v), k
+    assert abs(ref["scal"][3] - z0) < 1e-9
+    nf = 2 * n
+    band = ref["layer"] > 0
+    zc = (np.arange(-2, nf + 5) - 0.5) / nf
+    assert np.allclose(ref["phi"][band], zc[band] - z0, atol=1e-11)
+
+
+def test_init_rejects_film_in_first_cell():
+    from lica_boiling1d_b200 import native
+    from lica_boiling1d_b200.column import ColumnProps, Columns
+    with pytest.raises(native.LicaError):
+        Columns.film(64, 1.0, [0.003], ColumnProps())

@@ -1,0 +1,83 @@
+"""Whole RK3 time steps of 1-D boiling columns on the GPU (lica_gpu_column_steps) against
+the oracle (oracle/column1d.cpp), bit for bit: after every launch the complete column
+state -- W, P, T, PSI_CN, PSI_ZN, the level-set band, PSIF, the phase-change fields MFLVS,
+SFGAS, SFGAS2, IMASK_PH, DT/TIME/M/volumes and the step statistics -- must be identical.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def props_for(**kw):
+    from lica_boiling1d_b200.column import ColumnProps
+    return ColumnProps(**kw)
+
+
+def compare(dev, refs, where):
+    host = dev.to(None)
+    for c, ref in enumerate(refs):
+        for k, v in ref.items():
+            a = host.arrays[k][c]
+            assert np.array_equal(a, v), (where, c, k, np.nonzero(a != v)[0][:6], a[a != v][:3], v[a != v][:3])
+
+
+def run(n, z0s, props, steps, per_call=1):
+    import torch
+    from lica_boiling1d_b200.column import Columns
+    dev = Columns.film(n, 1.0, z0s, props).to("cuda")
+    refs = [O.col_init(n, 1.0, z0, props) for z0 in z0s]
+    done = 0
+    while done < steps:
+        k = min(per_call, steps - done)
+        status = dev.steps(k, props)
+        torch.cuda.synchronize()
+        assert int(status.abs().max()) == 0, status
+        for r in refs:
+            for _ in range(k):
+                assert O.col_step(r, n, 1.0, props) == 0
+        done += k
+        compare(dev, refs, f"after step {done}")
+    return dev, refs
+
+
+def test_shipped_column():
+    """The shipped lica.in / grid.in column: 256 flow cells, film 0.0607 thick."""
+    dev, refs = run(256, [0.0607], props_for(), 6)
+    assert refs[0]["stats"][2] > 0          # TEMP_EXTP ran
+    assert refs[0]["scal"][4] > refs[0]["scal"][3] - 1e-9
+
+
+def test_steps_in_one_launch():
+    run(256, [0.0607], props_for(), 8, per_call=4)
+
+
+def test_benchmark_column_config():
+    """512 flow cells, film 0.1, density ratio 1000, viscosity ratio 20, conductivity ratio
+    25, Jakob number of a 10 K superheat."""
+    run(512, [0.1], props_for(denr=1000.0, visr=20.0, tcr=25.0, jakob=0.009), 4)
+
+
+def test_batch_of_columns():
+    run(128, [0.05, 0.1, 0.2, 0.35, 0.5], props_for(denr=800.0, jakob=0.02), 6, per_call=2)
+
+
+def test_without_phase_change():
+    run(128, [0.1, 0.3], props_for(iphs=0), 4, per_call=2)
+
+
+def test_host_path_matches_device_path():
+    import torch
+    from lica_boiling1d_b200.column import Columns
+    props = props_for()
+    host = Columns.film(128, 1.0, [0.08, 0.2], props)
+    dev = host.to("cuda")
+    st_h = host.steps(3, props)
+    st_d = dev.steps(3, props)
+    torch.cuda.synchronize()
+    assert np.array_equal(st_h, st_d.cpu().numpy())
+    back = dev.to(None)
+    for k in host.arrays:
+        assert np.array_equal(host.arrays[k], back.arrays[k]), k
