@@ -246,13 +246,22 @@ int lica_gpu_column_init(int32_t n, double length, double z0, const lica_col_pro
 /* Device scratch the step kernel needs for ncol columns of n cells. */
 size_t lica_gpu_column_scratch_bytes(int32_t ncol, int32_t n);
 
-/* nsteps time steps of every column; device arrays.  scratch: NULL (the library keeps
+/* nsteps time steps of every column; device arrays.  threads: CTA width per column, 64,
+ * 128 or 256 (0: 128); wider CTAs finish one column sooner, narrower ones keep more
+ * columns per SM.  scratch: NULL (the library keeps
  * one) or lica_gpu_column_scratch_bytes() of device memory.  status[ncol] (device) gets
  * LICA_OK, LICA_NOT_CONVERGED (TEMP_EXTP did not converge), LICA_BAND_OVERFLOW or
  * LICA_BAD_ARG per column; a column stops at its first non-OK step.  Enqueues on stream. */
 int lica_gpu_column_steps_device(int32_t ncol, int32_t n, double length, const lica_col_props* props,
-                                 const lica_col_state* st, int32_t nsteps, void* scratch, int32_t* status,
-                                 void* stream);
+                                 const lica_col_state* st, int32_t nsteps, int32_t threads, void* scratch,
+                                 int32_t* status, void* stream);
+
+/* Cycle profile of the step kernel: while prof (device, 11 int64 per column) is set,
+ * thread 0 of each column adds the SM cycles spent in each phase -- 0 time-step choice and
+ * substep entry, 1 CAL_CONTINUITY + CAL_CONT_BC, 2 energy RHS + LHSPS, 3 TEMP_GRAD without
+ * TEMP_EXTP, 4 TEMP_EXTP, 5 CAL_CONTINUITY2 + CAL_CONT_BC, 6 RHSZ, 7 LHSW, 8 BC + FSM_CHOI +
+ * PRESSURE_CORRECTION, 9 CONVRGE1, 10 TRANSPORT + GRID_COUPLING.  NULL turns it off. */
+int lica_gpu_column_profile_device(int64_t* prof);
 
 /* Same on host arrays (copies in, runs, copies out); returns the last non-OK column status. */
 int lica_gpu_column_steps(int32_t ncol, int32_t n, double length, const lica_col_props* props,

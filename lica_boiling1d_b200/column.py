@@ -19,6 +19,9 @@ import numpy as np
 
 from . import native
 
+PHASES = ("dt", "continuity", "energy", "temp_grad", "temp_extp", "continuity2", "rhsz", "lhsw", "pressure",
+          "convrge", "transport")
+
 STATS = ("cfl", "divergence", "extension_iterations", "levelset_subcycles", "mass_corrections", "interface_height",
          "vapour_volume", "dt")
 
@@ -104,7 +107,7 @@ class Columns:
     def _state(self, ptr):
         return native.ColState(*[ptr(self.arrays[k]) for k in native.COL_FIELDS])
 
-    def steps(self, nsteps, props, stream=None, scratch=None):
+    def steps(self, nsteps, props, stream=None, scratch=None, threads=0):
         """Advance every column by nsteps time steps.  Returns the per-column status
         (numpy for host state; a CUDA tensor for device state, filled when the stream
         reaches it)."""
@@ -126,7 +129,7 @@ class Columns:
         status = torch.zeros(self.ncol, dtype=torch.int32, device=dev)
         s = stream if stream is not None else torch.cuda.current_stream(dev)
         rc = L.lica_gpu_column_steps_device(self.ncol, self.n, self.length, C.byref(cp),
-                                            C.byref(self._state(lambda a: a.data_ptr())), int(nsteps),
+                                            C.byref(self._state(lambda a: a.data_ptr())), int(nsteps), int(threads),
                                             C.c_void_p(scratch.data_ptr() if scratch is not None else None),
                                             C.c_void_p(status.data_ptr()), C.c_void_p(s.cuda_stream))
         native.check(rc, "column steps")
@@ -135,3 +138,10 @@ class Columns:
 
 def scratch_bytes(ncol, n):
     return int(native.lib().lica_gpu_column_scratch_bytes(ncol, n))
+
+
+def profile(prof):
+    """Collect per-phase SM cycles into prof (an int64 CUDA tensor of len(PHASES) * ncol,
+    zeroed by the caller) during later steps; None turns the profile off."""
+    native.check(native.lib().lica_gpu_column_profile_device(C.c_void_p(prof.data_ptr() if prof is not None else None)),
+                 "column profile")

@@ -38,7 +38,7 @@ struct Phys {
     int iphs, mglobal;
 };
 
-constexpr int NT = 256;          // threads per column CTA
+constexpr int NT_DEFAULT = 128;  // threads per column CTA unless the caller picks 64 or 256
 constexpr int NFLOW = 30;        // flow-sized scratch arrays per column
 constexpr int XR = 132;          // TEMP_EXTP extension range held in shared memory (+halo)
 
@@ -60,15 +60,26 @@ struct Args {
     int *layer, *imask, *status;
     double* dscr;
     int* iscr;
+    long long* prof;   // optional per-phase cycle totals (PH_COUNT per column) or null
+    int tri_smem;      // 1: the tridiagonal arrays live in dynamic shared memory
 };
+
+// phases of the optional cycle profile
+enum { PH_DT, PH_CONT, PH_ENERGY, PH_TEMPGRAD, PH_EXTP, PH_CONT2, PH_RHSZ, PH_LHSW, PH_PRESS, PH_CONV, PH_TRANSPORT,
+       PH_COUNT };
 
 struct Geo {
     int n, nf;
     double h, hf;
+    double ih, ihalf;   // 1/h (SSDZ, VVDZ inside) and 1/(h/2) (VVDZ at the walls), computed once
+    __device__ Geo(int n_, double L) : n(n_), nf(2 * n_), h(L / n_), hf(L / (2 * n_)) {
+        ih = 1.0 / h;
+        ihalf = 1.0 / (0.5 * h);
+    }
     __device__ double sdz(int k) const { return (k >= 1 && k <= n) ? h : 0.0; }
-    __device__ double ssdz(int) const { return 1.0 / h; }
+    __device__ double ssdz(int) const { return ih; }
     __device__ double vdz(int k) const { return (k == 1 || k == n + 1) ? 0.5 * h : h; }
-    __device__ double vvdz(int k) const { return 1.0 / vdz(k); }
+    __device__ double vvdz(int k) const { return (k == 1 || k == n + 1) ? ihalf : ih; }
     __device__ double z(int k) const { return col::grid_z(h, k); }
     __device__ double zp(int k) const { return col::grid_zp(h, n, k); }
     __device__ double zpf(int k) const { return col::grid_zpf(hf, k); }
@@ -83,13 +94,30 @@ struct Col {
     double *w, *p, *t, *psi_cn, *psi_zn, *phi, *psif, *wo, *mflvs, *sfgas, *sfgas2, *scal, *stats, *psif_mtp;
     int *layer, *imask, *region;   // region indexed k+1, k = -1..n+2
     double* a[NFLOW];
+    long long* prof;
+    long long t0;
+    // cycle profile: thread 0 adds the cycles since the last mark to phase ph
+    __device__ __forceinline__ void mark(int ph) {
+        if (prof && threadIdx.x == 0) {
+            const long long t = clock64();
+            prof[ph] += t - t0;
+            t0 = t;
+        }
+    }
+};
+
+// TEMP_EXTP arrays of one phase over the flow window [xk0, xk0+XR)
+struct XPhase {
+    double tm[XR], dt[XR], dtrk[XR], to[XR], trk[XR], nw[XR];
 };
 
 struct Shared {
     lvs::Win win;
     double red[32];
-    // TEMP_EXTP extension region [xk0, xk0+XR)
-    double x_nphi[XR], x_psih[XR], x_tm[XR], x_dt[XR], x_dtrk[XR], x_to[XR], x_trk[XR], x_new[XR];
+    // flow cells xk0 .. xk0+XR-1 around the band (xk0 = the band window's flow origin):
+    // NPHI, PSIH and PSI_CN of TEMP_GRAD, and the two phases' extension arrays
+    double x_nphi[XR], x_psih[XR], x_pcn[XR];
+    XPhase xp[2];
     int ibuf[8];
     double dbuf[8];
 };
@@ -117,19 +145,53 @@ __device__ __forceinline__ double block_min(double v, Shared& sh) {
 
 // Thomas algorithm of TRDIAG3 (1d.f:3783-3811) on one line, unknowns l1..l2; r becomes the
 // solution.  One thread.
+// The coefficients are read in blocks of PF ahead of the dependent recurrence, so the
+// memory latency overlaps instead of adding to every step of the chain.
+constexpr int PF = 4;
 __device__ void thomas(const double* a, const double* b, const double* c, double* r, double* gam, int l1, int l2) {
     double bet = 1.0 / b[l1];
     double u = r[l1] * bet;
     r[l1] = u;
-    for (int j = l1 + 1; j <= l2; ++j) {
-        gam[j] = c[j - 1] * bet;
-        bet = 1.0 / (b[j] - a[j] * gam[j]);
-        u = (r[j] - a[j] * u) * bet;
-        r[j] = u;
+    double cprev = c[l1];
+    for (int j0 = l1 + 1; j0 <= l2; j0 += PF) {
+        double A[PF], B[PF], Cc[PF], R[PF];
+#pragma unroll
+        for (int q = 0; q < PF; ++q) {
+            const int j = min(j0 + q, l2);
+            A[q] = a[j];
+            B[q] = b[j];
+            Cc[q] = c[j];
+            R[q] = r[j];
+        }
+#pragma unroll
+        for (int q = 0; q < PF; ++q) {
+            const int j = j0 + q;
+            if (j <= l2) {
+                const double gm = cprev * bet;
+                gam[j] = gm;
+                bet = 1.0 / (B[q] - A[q] * gm);
+                u = (R[q] - A[q] * u) * bet;
+                r[j] = u;
+                cprev = Cc[q];
+            }
+        }
     }
-    for (int j = l2 - 1; j >= l1; --j) {
-        u = r[j] - gam[j + 1] * u;
-        r[j] = u;
+    for (int j0 = l2 - 1; j0 >= l1; j0 -= PF) {
+        double G[PF], R[PF];
+#pragma unroll
+        for (int q = 0; q < PF; ++q) {
+            const int j = max(j0 - q, l1);
+            G[q] = gam[j + 1];
+            R[q] = r[j];
+        }
+#pragma unroll
+        for (int q = 0; q < PF; ++q) {
+            const int j = j0 - q;
+            if (j >= l1) {
+                u = R[q] - G[q] * u;
+                r[j] = u;
+            }
+        }
     }
 }
 
@@ -348,9 +410,9 @@ __device__ void lhsps(const Geo& g, const Phys& ph, Col& c, double alpha, double
 }
 
 // TEMP_EXTP_RK3, chphase.f:806-956 (1-D), on the extension range in shared memory: x[i]
-// holds flow cell xk0 + i.  nd = 0: tempo is the DTEMPN array itself.
-__device__ void extp_sweep(const Geo& g, Shared& sh, int xk0, int lo, int hi, double* tempo, int im, double redtl,
-                           int nd) {
+// holds flow cell xk0 + i.  nd = 0: tempo is the DTEMPN array X.dt itself.
+__device__ void extp_sweep(const Geo& g, const Shared& sh, XPhase& X, int xk0, int lo, int hi, double* tempo, int im,
+                           double redtl, int nd) {
     const int lane = threadIdx.x & 31;
     const double sm_grid = fmin(fmin(1.0, 1.0), 2.0 * g.hf);
     for (int i = lo + lane; i <= hi; i += 32) {
@@ -372,10 +434,10 @@ __device__ void extp_sweep(const Geo& g, Shared& sh, int xk0, int lo, int hi, do
                 const double az = fmin(nz, 0.0) * apzp + fmax(nz, 0.0) * apzm;
                 double drhs;
                 if (im == 1) {
-                    drhs = (ax + ay + az) + nd * sh.x_dt[i];
+                    drhs = (ax + ay + az) + nd * X.dt[i];
                     nv = tempo[i] - redtl * drhs * (1 - sh.x_psih[i]);
                 } else {
-                    drhs = (ax + ay + az) - nd * sh.x_dt[i];
+                    drhs = (ax + ay + az) - nd * X.dt[i];
                     nv = tempo[i] - redtl * drhs * sh.x_psih[i];
                 }
                 if (nd == 0 && fabs(nph) <= sm_grid) {
@@ -384,10 +446,10 @@ __device__ void extp_sweep(const Geo& g, Shared& sh, int xk0, int lo, int hi, do
                 }
             }
         }
-        sh.x_new[i] = nv;
+        X.nw[i] = nv;
     }
     __syncwarp();
-    for (int i = lo + lane; i <= hi; i += 32) tempo[i] = sh.x_new[i];
+    for (int i = lo + lane; i <= hi; i += 32) tempo[i] = X.nw[i];
     __syncwarp();
 }
 
@@ -398,80 +460,207 @@ __device__ __forceinline__ double warp_maxd(double v) {
 
 constexpr int kMaxHalvings = 40;
 
-// TEMP_EXTP, chphase.f:467-805 (1-D), warp 0.  Only cells with NPHI != 0 change; they lie
-// in [ka, kb], held with one halo cell on each side in shared memory.  Returns the number
-// of pseudo-time iterations or -1 if a phase does not converge within kMaxHalvings
+struct ExtpLane {
+    int lane, R;
+    bool act, small;
+    double vv, psh, fmn, fmx;
+    int im;
+    // one TEMP_EXTP_RK3 step (chphase.f:806-956) of the cell this lane holds
+    __device__ __forceinline__ double sweep(double x, double hl, double hr, int nd, double dtn, double redtl) const {
+        double xm = __shfl_up_sync(0xffffffffu, x, 1);
+        double xp = __shfl_down_sync(0xffffffffu, x, 1);
+        if (lane == 0) xm = hl;
+        if (lane == R - 1) xp = hr;
+        double nv = x;
+        if (act) {
+            const double apzm = (x - xm) * vv;
+            const double apzp = (xp - x) * vv;
+            const double ax = 0.0, ay = 0.0;
+            const double az = fmn * apzp + fmx * apzm;
+            double drhs;
+            if (im == 1) {
+                drhs = (ax + ay + az) + nd * dtn;
+                nv = x - redtl * drhs * (1 - psh);
+            } else {
+                drhs = (ax + ay + az) - nd * dtn;
+                nv = x - redtl * drhs * psh;
+            }
+            if (nd == 0 && small) {
+                drhs = (ax + ay + az);
+                nv = x - redtl * drhs;
+            }
+        }
+        return nv;
+    }
+};
+
+// TEMP_EXTP's two pseudo-time loops for an extension range of at most 32 cells: lane i
+// holds cell xk0 + lo + i in registers, neighbours come by shuffle, the halo cells (one
+// each side, never updated) are constants.  Same operations and order as extp_sweep.
+// Returns the iteration count, or -1 when kMaxHalvings halvings did not converge.
+__device__ int extp_registers(const Geo& g, const Shared& sh, XPhase& X, int xk0, int lo, int hi, int im,
+                              double eps) {
+    const int lane = threadIdx.x & 31;
+    ExtpLane L;
+    L.lane = lane;
+    L.R = hi - lo + 1;
+    L.im = im;
+    const bool valid = lane < L.R;
+    const int xi = valid ? lo + lane : lo;
+    const int k = xk0 + xi;
+    const double sm_grid = fmin(fmin(1.0, 1.0), 2.0 * g.hf);
+    const double nph = sh.x_nphi[xi];
+    L.act = false;
+    if (valid && nph != 0.0) {
+        double dpz;
+        if (sh.x_nphi[xi - 1] == 0.0) dpz = (sh.x_nphi[xi + 1] - nph) * g.vvdz(k + 1);
+        else if (sh.x_nphi[xi + 1] == 0.0) dpz = (nph - sh.x_nphi[xi - 1]) * g.vvdz(k);
+        else dpz = 0.5 * (sh.x_nphi[xi + 1] - sh.x_nphi[xi - 1]) * g.vvdz(k);
+        L.act = ((0.0 + 0.0) + dpz * dpz) != 0.0;
+    }
+    L.small = fabs(nph) <= sm_grid;
+    L.vv = g.vvdz(k);
+    L.psh = sh.x_psih[xi];
+    const double nz = (im == 1) ? (-1.0) * 1.0 : 1.0;
+    L.fmn = fmin(nz, 0.0);
+    L.fmx = fmax(nz, 0.0);
+    int total = 0;
+    // extension of the normal gradient (nd = 0); its halo values are 0
+    double x = X.dt[xi];
+    double redtl = 0.2 * sm_grid;
+    bool conv = false;
+    for (int halving = 0; halving <= kMaxHalvings && !conv; ++halving) {
+        for (int it = 1; it <= 100; ++it) {
+            ++total;
+            const double rk = x;
+            x = L.sweep(x, 0.0, 0.0, 0, x, redtl);
+            x = L.sweep(x, 0.0, 0.0, 0, x, redtl);
+            x = 0.75 * rk + 0.25 * x;
+            x = L.sweep(x, 0.0, 0.0, 0, x, redtl);
+            x = 1.0 / 3.0 * rk + 2.0 / 3.0 * x;
+            double rat = 0.0;
+            if (valid) {
+                if (rk != 0.0) rat = fabs(x / rk - 1.0);
+                else if (x != 0.0) rat = fabs(rk / x - 1.0);
+            }
+            rat = warp_maxd(rat);
+            if (fabs(rat) < eps) {
+                conv = true;
+                break;
+            }
+        }
+        if (!conv) redtl = 0.5 * redtl;
+    }
+    if (!conv) return -1;
+    const double dtn = x;
+    // extension of the phase temperature (nd = 1); halo = the unchanged neighbours
+    const double hl = X.tm[lo - 1], hr = X.tm[hi + 1];
+    double tm = X.tm[xi];
+    redtl = 0.2 * sm_grid;
+    conv = false;
+    for (int halving = 0; halving <= kMaxHalvings && !conv; ++halving) {
+        for (int it = 1; it <= 100; ++it) {
+            ++total;
+            const double rk = tm;
+            double to = tm;
+            to = L.sweep(to, hl, hr, 1, dtn, redtl);
+            to = L.sweep(to, hl, hr, 1, dtn, redtl);
+            to = 0.75 * rk + 0.25 * to;
+            to = L.sweep(to, hl, hr, 1, dtn, redtl);
+            to = 1.0 / 3.0 * rk + 2.0 / 3.0 * to;
+            tm = to;
+            double rat = 0.0;
+            if (valid && rk != 0.0) rat = fabs(tm / rk - 1.0);
+            rat = warp_maxd(rat);
+            if (fabs(rat) < eps) {
+                conv = true;
+                break;
+            }
+        }
+        if (!conv) redtl = 0.5 * redtl;
+    }
+    if (!conv) return -1;
+    if (valid) {
+        X.dt[xi] = dtn;
+        X.tm[xi] = tm;
+    }
+    __syncwarp();
+    return total;
+}
+
+// TEMP_EXTP, chphase.f:467-805 (1-D), one phase (im = 0 vapour, 1 liquid) on one warp;
+// the two phases are independent and run on warps 0 and 1 at once.  Only cells with
+// NPHI != 0 change; they lie in [xk0+lo, xk0+hi], held with one halo cell each side in
+// shared memory.  temp_g: the phase temperature (global, k = 0..n+1).  Returns the number
+// of pseudo-time iterations or -1 if the phase does not converge within kMaxHalvings
 // halvings of the step.
-__device__ int temp_extp(const Geo& g, const Phys& ph, Col& c, Shared& sh, int ka, int kb) {
+__device__ int temp_extp(const Geo& g, const Phys& ph, Shared& sh, int xk0, int lo, int hi, int im, double* temp_g) {
     const int lane = threadIdx.x & 31;
     const double sm_grid = fmin(fmin(2.0 * 0.5, 2.0 * 0.5), 2.0 * g.hf);
     const double eps = 1e-4;
-    const int xk0 = ka - 1, lo = 1, hi = kb - xk0;   // x index of ka .. kb
-    const double *nphi = c.a[S_NPHI], *psih = c.a[S_PSIH];
+    XPhase& X = sh.xp[im];
     int total = 0;
-    for (int i = lane; i <= hi + 1; i += 32) {
-        sh.x_nphi[i] = nphi[xk0 + i];
-        sh.x_psih[i] = psih[xk0 + i];
+    for (int i = lo - 1 + lane; i <= hi + 1; i += 32) {
+        X.tm[i] = temp_g[xk0 + i];
+        X.dt[i] = 0.0;   // DTEMPN: 0 outside the cells set below (halo included)
     }
     __syncwarp();
-    for (int im = 0; im <= 1; ++im) {
-        double* tm_g = c.a[im ? S_TEMP1 : S_TEMP0];
-        for (int i = lane; i <= hi + 1; i += 32) {
-            sh.x_tm[i] = tm_g[xk0 + i];
-            sh.x_dt[i] = 0.0;   // DTEMPN: 0 outside the cells set below (halo included)
-        }
-        __syncwarp();
-        for (int i = lo + lane; i <= hi; i += 32) {
-            const int k = xk0 + i;
-            const double nph = sh.x_nphi[i];
-            double d = 0.0;
-            const bool ca = ((fabs(nph) > 1.5 * sm_grid) && (nph != 0.0)) ||
-                            ((fabs(c.psi_cn[k] - 0.5) == 0.5) && (nph != 0.0));
-            if (ca) {
-                double dpz, dtdz;
-                if (sh.x_nphi[i - 1] == 0.0) {
-                    dpz = (sh.x_nphi[i + 1] - nph) * g.vvdz(k + 1);
-                    dtdz = (sh.x_tm[i + 1] - sh.x_tm[i]) * g.vvdz(k + 1);
-                } else if (sh.x_nphi[i + 1] == 0.0) {
-                    dpz = (nph - sh.x_nphi[i - 1]) * g.vvdz(k);
-                    dtdz = (sh.x_tm[i] - sh.x_tm[i - 1]) * g.vvdz(k);
-                } else {
-                    dpz = 0.5 * (sh.x_nphi[i + 1] - sh.x_nphi[i - 1]) * g.vvdz(k);
-                    dtdz = 0.5 * (sh.x_tm[i + 1] - sh.x_tm[i - 1]) * g.vvdz(k);
-                }
-                const double dalphi = (0.0 + 0.0) + dpz * dpz;
-                if (dalphi != 0.0) {
-                    const double nz = 1.0;
-                    if (im == 1) d = (0.0 + 0.0) + nz * dtdz * sh.x_psih[i];
-                    else d = (0.0 + 0.0) + nz * dtdz * (1 - sh.x_psih[i]);
-                }
-            } else if (((fabs(nph) <= 1.5 * sm_grid) || (fabs(c.psi_cn[k] - 0.5) != 0.5)) &&
-                       ((nph != 1e-7) && (nph != 0.0))) {
-                if (im == 1) d = (sh.x_tm[i] - ph.t_sat) / nph * sh.x_psih[i];
-                else d = (sh.x_tm[i] - ph.t_sat) / nph * (1.0 - sh.x_psih[i]);
+    for (int i = lo + lane; i <= hi; i += 32) {
+        const double nph = sh.x_nphi[i];
+        double d = 0.0;
+        const int k = xk0 + i;
+        const bool ca = ((fabs(nph) > 1.5 * sm_grid) && (nph != 0.0)) ||
+                        ((fabs(sh.x_pcn[i] - 0.5) == 0.5) && (nph != 0.0));
+        if (ca) {
+            double dpz, dtdz;
+            if (sh.x_nphi[i - 1] == 0.0) {
+                dpz = (sh.x_nphi[i + 1] - nph) * g.vvdz(k + 1);
+                dtdz = (X.tm[i + 1] - X.tm[i]) * g.vvdz(k + 1);
+            } else if (sh.x_nphi[i + 1] == 0.0) {
+                dpz = (nph - sh.x_nphi[i - 1]) * g.vvdz(k);
+                dtdz = (X.tm[i] - X.tm[i - 1]) * g.vvdz(k);
+            } else {
+                dpz = 0.5 * (sh.x_nphi[i + 1] - sh.x_nphi[i - 1]) * g.vvdz(k);
+                dtdz = 0.5 * (X.tm[i + 1] - X.tm[i - 1]) * g.vvdz(k);
             }
-            sh.x_dt[i] = d;
+            const double dalphi = (0.0 + 0.0) + dpz * dpz;
+            if (dalphi != 0.0) {
+                const double nz = 1.0;
+                if (im == 1) d = (0.0 + 0.0) + nz * dtdz * sh.x_psih[i];
+                else d = (0.0 + 0.0) + nz * dtdz * (1 - sh.x_psih[i]);
+            }
+        } else if (((fabs(nph) <= 1.5 * sm_grid) || (fabs(sh.x_pcn[i] - 0.5) != 0.5)) &&
+                   ((nph != 1e-7) && (nph != 0.0))) {
+            if (im == 1) d = (X.tm[i] - ph.t_sat) / nph * sh.x_psih[i];
+            else d = (X.tm[i] - ph.t_sat) / nph * (1.0 - sh.x_psih[i]);
         }
-        __syncwarp();
+        X.dt[i] = d;
+    }
+    __syncwarp();
+    if (hi - lo + 1 <= 32) {
+        const int it = extp_registers(g, sh, X, xk0, lo, hi, im, eps);
+        if (it < 0) return -1;
+        total += it;
+    } else {
         // extension of the normal gradient (nd = 0)
         double redtl = 0.2 * sm_grid;
         bool conv = false;
         for (int halving = 0; halving <= kMaxHalvings && !conv; ++halving) {
             for (int it = 1; it <= 100; ++it) {
                 ++total;
-                for (int i = lo + lane; i <= hi; i += 32) sh.x_dtrk[i] = sh.x_dt[i];
+                for (int i = lo + lane; i <= hi; i += 32) X.dtrk[i] = X.dt[i];
                 __syncwarp();
-                extp_sweep(g, sh, xk0, lo, hi, sh.x_dt, im, redtl, 0);
-                extp_sweep(g, sh, xk0, lo, hi, sh.x_dt, im, redtl, 0);
-                for (int i = lo + lane; i <= hi; i += 32) sh.x_dt[i] = 0.75 * sh.x_dtrk[i] + 0.25 * sh.x_dt[i];
+                extp_sweep(g, sh, X, xk0, lo, hi, X.dt, im, redtl, 0);
+                extp_sweep(g, sh, X, xk0, lo, hi, X.dt, im, redtl, 0);
+                for (int i = lo + lane; i <= hi; i += 32) X.dt[i] = 0.75 * X.dtrk[i] + 0.25 * X.dt[i];
                 __syncwarp();
-                extp_sweep(g, sh, xk0, lo, hi, sh.x_dt, im, redtl, 0);
+                extp_sweep(g, sh, X, xk0, lo, hi, X.dt, im, redtl, 0);
                 double rat = 0.0;
                 for (int i = lo + lane; i <= hi; i += 32) {
-                    const double v = 1.0 / 3.0 * sh.x_dtrk[i] + 2.0 / 3.0 * sh.x_dt[i];
-                    sh.x_dt[i] = v;
-                    if (sh.x_dtrk[i] != 0.0) rat = fmax(fabs(v / sh.x_dtrk[i] - 1.0), rat);
-                    else if (v != 0.0) rat = fmax(fabs(sh.x_dtrk[i] / v - 1.0), rat);
+                    const double v = 1.0 / 3.0 * X.dtrk[i] + 2.0 / 3.0 * X.dt[i];
+                    X.dt[i] = v;
+                    if (X.dtrk[i] != 0.0) rat = fmax(fabs(v / X.dtrk[i] - 1.0), rat);
+                    else if (v != 0.0) rat = fmax(fabs(X.dtrk[i] / v - 1.0), rat);
                 }
                 rat = warp_maxd(rat);
                 __syncwarp();
@@ -489,22 +678,22 @@ __device__ int temp_extp(const Geo& g, const Phys& ph, Col& c, Shared& sh, int k
         for (int halving = 0; halving <= kMaxHalvings && !conv; ++halving) {
             for (int it = 1; it <= 100; ++it) {
                 ++total;
-                for (int i = lane; i <= hi + 1; i += 32) {
-                    sh.x_trk[i] = sh.x_tm[i];
-                    sh.x_to[i] = sh.x_tm[i];
+                for (int i = lo - 1 + lane; i <= hi + 1; i += 32) {
+                    X.trk[i] = X.tm[i];
+                    X.to[i] = X.tm[i];
                 }
                 __syncwarp();
-                extp_sweep(g, sh, xk0, lo, hi, sh.x_to, im, redtl, 1);
-                extp_sweep(g, sh, xk0, lo, hi, sh.x_to, im, redtl, 1);
-                for (int i = lo + lane; i <= hi; i += 32) sh.x_to[i] = 0.75 * sh.x_trk[i] + 0.25 * sh.x_to[i];
+                extp_sweep(g, sh, X, xk0, lo, hi, X.to, im, redtl, 1);
+                extp_sweep(g, sh, X, xk0, lo, hi, X.to, im, redtl, 1);
+                for (int i = lo + lane; i <= hi; i += 32) X.to[i] = 0.75 * X.trk[i] + 0.25 * X.to[i];
                 __syncwarp();
-                extp_sweep(g, sh, xk0, lo, hi, sh.x_to, im, redtl, 1);
+                extp_sweep(g, sh, X, xk0, lo, hi, X.to, im, redtl, 1);
                 double rat = 0.0;
                 for (int i = lo + lane; i <= hi; i += 32) {
-                    const double v = 1.0 / 3.0 * sh.x_trk[i] + 2.0 / 3.0 * sh.x_to[i];
-                    sh.x_to[i] = v;
-                    sh.x_tm[i] = v;
-                    if (sh.x_trk[i] != 0.0) rat = fmax(fabs(v / sh.x_trk[i] - 1.0), rat);
+                    const double v = 1.0 / 3.0 * X.trk[i] + 2.0 / 3.0 * X.to[i];
+                    X.to[i] = v;
+                    X.tm[i] = v;
+                    if (X.trk[i] != 0.0) rat = fmax(fabs(v / X.trk[i] - 1.0), rat);
                 }
                 rat = warp_maxd(rat);
                 __syncwarp();
@@ -516,9 +705,9 @@ __device__ int temp_extp(const Geo& g, const Phys& ph, Col& c, Shared& sh, int k
             if (!conv) redtl = 0.5 * redtl;
         }
         if (!conv) return -1;
-        for (int i = lo + lane; i <= hi; i += 32) tm_g[xk0 + i] = sh.x_tm[i];
-        __syncwarp();
     }
+    for (int i = lo + lane; i <= hi; i += 32) temp_g[xk0 + i] = X.tm[i];
+    __syncwarp();
     return total;
 }
 
@@ -528,7 +717,7 @@ __device__ int temp_extp(const Geo& g, const Phys& ph, Col& c, Shared& sh, int k
 __device__ int temp_grad(const Geo& g, const Phys& ph, Col& c, Shared& sh, double L, double dtconst) {
     const int n = g.n, nf = g.nf;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    double *temp0 = c.a[S_TEMP0], *temp1 = c.a[S_TEMP1], *nphi = c.a[S_NPHI], *psih = c.a[S_PSIH];
+    double *temp0 = c.a[S_TEMP0], *temp1 = c.a[S_TEMP1];
     FOR_K(0, nf + 6) c.mflvs[k] = 0.0;
     FOR_K(0, nf + 1) {
         c.sfgas[k] = 0.0;
@@ -538,8 +727,6 @@ __device__ int temp_grad(const Geo& g, const Phys& ph, Col& c, Shared& sh, doubl
         c.imask[k] = 0;
         temp0[k] = c.t[k];
         temp1[k] = c.t[k];
-        nphi[k] = 0.0;
-        psih[k] = 0.0;
     }
     __syncthreads();
     lvs::Win* s = &sh.win;
@@ -549,18 +736,28 @@ __device__ int temp_grad(const Geo& g, const Phys& ph, Col& c, Shared& sh, doubl
     if (warp == 0) {
         st = lvs::load_band_window(cx, lane, n, L, c.phi, c.layer);
         if (lane == 0) sh.ibuf[0] = st;
+        // NPHI, PSIH, PSI_CN of the flow cells xk0 .. xk0+XR-1 (the window's flow range)
+        for (int j = lane; j < XR; j += 32) {
+            const int k = cx.kw0 + j;
+            sh.x_nphi[j] = 0.0;
+            sh.x_psih[j] = 0.0;
+            sh.x_pcn[j] = (k >= 0 && k <= n + 1) ? c.psi_cn[k] : 0.0;
+        }
     }
     __syncthreads();
     st = sh.ibuf[0];
     if (st != LICA_OK) return -st;
+    const int xk0 = cx.kw0;   // valid on warp 0; shared below through ibuf
     if (warp == 0) {
-        // (1) NPHI / PSIH of the flow cells of the band (:147-211), in list order
+        // (1) NPHI / PSIH of the flow cells of the band (:147-211), in list order; every
+        // band cell's flow cell lies in [xk0+2, xk0+66]
         if (lane == 0) {
             int ic = 0;
             for (int j = s->lstart[1]; j < s->lstart[lvs::NN2 + 1]; ++j) {
                 const int k = cx.w0 + s->lst[j];
                 const int kk = col::kcoump_vel(g.h, g.hf, n, k);
-                if (nphi[kk] == 0.0) {
+                const int x = kk - xk0;
+                if (sh.x_nphi[x] == 0.0) {
                     const int k1 = 2 * kk - 1, k2 = 2 * kk;
                     const double zd = (g.zp(kk) - g.zpf(k1)) / (g.zpf(k2) - g.zpf(k1));
                     const double a1 = cx.p(k1), a2 = cx.p(k2);
@@ -572,47 +769,60 @@ __device__ int temp_grad(const Geo& g, const Phys& ph, Col& c, Shared& sh, doubl
                     if (nsphi > 0.0) ic = 1;
                     if (nsphi < 0.0) ic = 0;
                     if (a1 == 0.0 || a2 == 0.0) nsphi = 0.0;
-                    nphi[kk] = 1e-7;
-                    nphi[kk] = nsphi;
-                    if (fabs(c.psi_cn[kk] - 0.5) != 0.5) psih[kk] = (double)ic;
-                    else psih[kk] = c.psi_cn[kk];
+                    sh.x_nphi[x] = 1e-7;
+                    sh.x_nphi[x] = nsphi;
+                    if (fabs(sh.x_pcn[x] - 0.5) != 0.5) sh.x_psih[x] = (double)ic;
+                    else sh.x_psih[x] = sh.x_pcn[x];
                 }
             }
             for (int j = s->lstart[lvs::N_MAX]; j < s->lstart[lvs::N_MAX + 1]; ++j) {
                 const int k = cx.w0 + s->lst[j];
                 const int kk = col::kcoump_vel(g.h, g.hf, n, k);
+                const int x = kk - xk0;
                 const double dx = 0.25, dy = 0.25;
                 const double dz = g.zpf(k) - g.zp(kk);
                 const double pre = s->phi[s->lst[j]] + sqrt(dx * dx + dy * dy + dz * dz);
-                nphi[kk] = fmin(nphi[kk], pre);
-                psih[kk] = c.psi_cn[kk];
+                sh.x_nphi[x] = fmin(sh.x_nphi[x], pre);
+                sh.x_psih[x] = sh.x_pcn[x];
             }
             // extension range: the cells with NPHI != 0
             int ka = n + 1, kb = 0;
             for (int j = s->lstart[1]; j < s->lstart[lvs::N_MAX + 1]; ++j) {
                 const int kk = col::kcoump_vel(g.h, g.hf, n, cx.w0 + s->lst[j]);
-                if (nphi[kk] != 0.0) {
+                if (sh.x_nphi[kk - xk0] != 0.0) {
                     ka = min(ka, kk);
                     kb = max(kb, kk);
                 }
             }
             sh.ibuf[1] = ka;
             sh.ibuf[2] = kb;
+            sh.ibuf[7] = xk0;
         }
+    }
+    __syncthreads();
+    c.mark(PH_TEMPGRAD);
+    {
+        // (2) TEMP_EXTP: the vapour phase on warp 0, the liquid phase on warp 1
+        const int ka = sh.ibuf[1], kb = sh.ibuf[2], x0 = sh.ibuf[7];
+        if (warp < 2) {
+            int it = 0;
+            if (kb >= ka) it = temp_extp(g, ph, sh, x0, ka - x0, kb - x0, warp, warp ? temp1 : temp0);
+            if (lane == 0) sh.ibuf[3 + warp * 2] = it;   // ibuf[3], ibuf[5]
+        }
+    }
+    __syncthreads();
+    c.mark(PH_EXTP);
+    if (warp == 0) {
+        const int i0 = sh.ibuf[3], i1 = sh.ibuf[5];
+        const int iters = (i0 < 0 || i1 < 0) ? -1 : i0 + i1;
         __syncwarp();
-        const int ka = sh.ibuf[1], kb = sh.ibuf[2];
-        int iters = 0;
-        if (kb >= ka) {
-            if (kb - ka + 3 > XR) iters = -LICA_BAND_OVERFLOW;
-            else iters = temp_extp(g, ph, c, sh, ka, kb);
-        }
         if (lane == 0) sh.ibuf[3] = iters;
         __syncwarp();
         if (iters >= 0) {
             // (3) TF on layers 1..NN1 by TEMPASSIGN (chphase.f:372-463); tf0 in win.rk3, tf1
             // in win.alphio (window-indexed, 0 elsewhere)
-            for (int q = 0; q < lvs::PER; ++q) {
-                const int i = lane + 32 * q, k = cx.w0 + i, m = s->layer[i];
+            for (int i = cx.blo + lane; i <= cx.bhi; i += 32) {
+                const int k = cx.w0 + i, m = s->layer[i];
                 double v0 = 0.0, v1 = 0.0;
                 if (m >= 1 && m <= lvs::NN1) {
                     const int kk = col::kcoump_vel(g.h, g.hf, n, k);
@@ -635,8 +845,8 @@ __device__ int temp_grad(const Geo& g, const Phys& ph, Col& c, Shared& sh, doubl
             }
             __syncwarp();
             // (4)-(6) TF_GRAD: MFDOT on layers 1..NN1-2
-            for (int q = 0; q < lvs::PER; ++q) {
-                const int i = lane + 32 * q, k = cx.w0 + i, m = s->layer[i];
+            for (int i = cx.blo + lane; i <= cx.bhi; i += 32) {
+                const int k = cx.w0 + i, m = s->layer[i];
                 if (m >= 1 && m <= lvs::NN1 - 2) {
                     const double gz = 0.5 * (s->phi[i + 1] - s->phi[i - 1]) * cx.ssdzf;
                     const double agi = 1.0 / sqrt((0.0 + 0.0) + gz * gz);
@@ -652,20 +862,18 @@ __device__ int temp_grad(const Geo& g, const Phys& ph, Col& c, Shared& sh, doubl
                 }
             }
             // PSIF_MTP = CAL_PSIF_MTP(1, NN1) of the band (snapped band values, column fill)
-            for (int q = 0; q < lvs::PER; ++q) {
-                const int i = lane + 32 * q, m = s->layer[i];
+            for (int i = cx.blo + lane; i <= cx.bhi; i += 32) {
+                const int m = s->layer[i];
                 s->start[i] = (m >= 1 && m <= lvs::NN1) ? lvs::psif_band(s, i) : 0.0;
             }
             __syncwarp();
-            if (lane == 0) {
-                int ktop = -1, kbot = -1;
-                for (int k = nf; k >= 1; --k)
-                    if (cx.p(k) * cx.p(k + 1) < 0.0) {
-                        if (ktop < 0) ktop = k;
-                        kbot = k;
-                    }
-                sh.ibuf[4] = ktop;
-                sh.ibuf[5] = kbot;
+            {
+                int ktop, kbot;
+                lvs::window_crossings(cx, ktop, kbot);
+                if (lane == 0) {
+                    sh.ibuf[4] = ktop;
+                    sh.ibuf[5] = kbot;
+                }
             }
             __syncwarp();
             {
@@ -687,8 +895,8 @@ __device__ int temp_grad(const Geo& g, const Phys& ph, Col& c, Shared& sh, doubl
             __syncwarp();
             // VOL_TOT_MFDOT: trial advance of layers 1..NN1-2 by the mass flux, reinit,
             // volume of CAL_PSIF_MTP(1) of the trial band, SFGAS / SFGAS2
-            for (int q = 0; q < lvs::PER; ++q) {
-                const int i = lane + 32 * q, m = s->layer[i];
+            for (int i = cx.blo + lane; i <= cx.bhi; i += 32) {
+                const int m = s->layer[i];
                 s->wf[i] = s->phi[i];   // ALPHI at entry
                 if (m >= 1 && m <= lvs::NN1 - 2) {
                     const double mfd = (s->phi[i] > 0.0) ? s->mf[i] / ph.denr : s->mf[i];
@@ -701,47 +909,24 @@ __device__ int temp_grad(const Geo& g, const Phys& ph, Col& c, Shared& sh, doubl
                 }
             }
             __syncwarp();
-            for (int q = 0; q < lvs::PER; ++q) {
-                const int i = lane + 32 * q, m = s->layer[i];
+            for (int i = cx.blo + lane; i <= cx.bhi; i += 32) {
+                const int m = s->layer[i];
                 if (m >= 1 && m <= lvs::NN1 - 2) s->phi[i] = s->nv[i];
             }
             __syncwarp();
             lvs::reinitialization(cx, lvs::NN2);
-            for (int q = 0; q < lvs::PER; ++q) {
-                const int i = lane + 32 * q, m = s->layer[i];
+            for (int i = cx.blo + lane; i <= cx.bhi; i += 32) {
+                const int m = s->layer[i];
                 s->nv[i] = (m >= 1 && m <= lvs::NN1) ? lvs::psif_band(s, i) : 0.0;
             }
             __syncwarp();
-            if (lane == 0) {
-                int ktop = -1, kbot = -1;
-                for (int k = nf; k >= 1; --k)
-                    if (cx.p(k) * cx.p(k + 1) < 0.0) {
-                        if (ktop < 0) ktop = k;
-                        kbot = k;
-                    }
-                double t1 = 1.0, t2 = 1.0;
-                if (ktop >= 0) {
-                    t1 = (cx.p(ktop) < 0.0) ? 0.0 : 1.0;
-                    t2 = (cx.p(kbot + 1) < 0.0) ? 0.0 : 1.0;
-                }
-                const double dvol = 0.5 * 0.5 * g.hf;
-                double vol = 0.0;
-                for (int k = 1; k <= nf; ++k) {
-                    const int i = k - cx.w0;
-                    double v;
-                    if (cx.in(k) && s->layer[i] >= 1 && s->layer[i] <= lvs::NN1) v = s->nv[i];
-                    else if (ktop < 0) v = 1.0;
-                    else v = (k > kbot) ? t2 : t1;
-                    const double d = (1.0 - v) * dvol;
-                    vol = vol + d;
-                    vol = vol + d;
-                    vol = vol + d;
-                    vol = vol + d;
-                }
-                c.scal[4] = vol;
+            {
+                int ktop, kbot;
+                lvs::window_crossings(cx, ktop, kbot);
+                if (lane == 0) c.scal[4] = lvs::column_vapour_volume(cx, s->nv, ktop, kbot, 0.5 * 0.5 * g.hf);
             }
-            for (int q = 0; q < lvs::PER; ++q) {
-                const int i = lane + 32 * q, k = cx.w0 + i, m = s->layer[i];
+            for (int i = cx.blo + lane; i <= cx.bhi; i += 32) {
+                const int k = cx.w0 + i, m = s->layer[i];
                 if (m >= 1 && m <= lvs::NN1 - 2 && s->mf[i] != 0.0 && fabs(c.psif_mtp[k] - 0.5) != 0.5) {
                     const double d = -(s->nv[i] - c.psif_mtp[k]);
                     if (s->wf[i] > 0.0) {
@@ -806,8 +991,10 @@ __device__ int rhsnlhs(const Geo& g, const Phys& ph, Col& c, Shared& sh, double 
     const double dtconsti = 1. / dtconst;
     double *rhs1 = c.a[S_RHS1], *rhsps = c.a[S_RHSPS], *rk3zo = c.a[S_RK3ZO];
     const double *denf_zi = c.a[S_DENFZI], *psi_c = c.a[S_PSIC], *df_c = c.a[S_DFC];
+    c.mark(PH_DT);
     cal_continuity(g, ph, c, dtconst);
     cal_cont_bc(g, ph, c);
+    c.mark(PH_CONT);
     // PASSIVE_SCALAR (1d.f:3630-3707)
     int iters = 0;
     if (ph.iphs == 1 && m_step != 1) {
@@ -825,10 +1012,13 @@ __device__ int rhsnlhs(const Geo& g, const Phys& ph, Col& c, Shared& sh, double 
         }
         __syncthreads();
         lhsps(g, ph, c, alpha, dt);   // substitute for the undefined LHSPS2
+        c.mark(PH_ENERGY);
         iters = temp_grad(g, ph, c, sh, L, dtconst);
         if (iters < 0) return iters;
+        c.mark(PH_TEMPGRAD);
         cal_continuity2(g, ph, c);
         cal_cont_bc(g, ph, c);
+        c.mark(PH_CONT2);
     } else {
         FOR_K(1, n) {
             const double anps = 0.0, alps = 0.0, anpso = 0.0, tgr = 0.0;
@@ -846,6 +1036,7 @@ __device__ int rhsnlhs(const Geo& g, const Phys& ph, Col& c, Shared& sh, double 
         }
         __syncthreads();
         lhsps(g, ph, c, alpha, dt);
+        c.mark(PH_ENERGY);
     }
     // RHSZ (1d.f:1603-1745) and RHS1 = RHS1 / rho - W (1564-1568)
     {
@@ -876,6 +1067,7 @@ __device__ int rhsnlhs(const Geo& g, const Phys& ph, Col& c, Shared& sh, double 
             rk3zo[k] = rk3z;
         }
         __syncthreads();
+        c.mark(PH_RHSZ);
     }
     // LHSW (1d.f:1749-1809)
     {
@@ -895,6 +1087,7 @@ __device__ int rhsnlhs(const Geo& g, const Phys& ph, Col& c, Shared& sh, double 
         __syncthreads();
         FOR_K(2, n) c.w[k] = gk[k] + c.w[k];
         __syncthreads();
+        c.mark(PH_LHSW);
     }
     // BC + BC_FLUX (1d.f:1812-1923)
     if (threadIdx.x == 0) {
@@ -957,6 +1150,7 @@ __device__ int rhsnlhs(const Geo& g, const Phys& ph, Col& c, Shared& sh, double 
         __syncthreads();
         if (threadIdx.x == 0) c.p[0] = c.p[1];
         __syncthreads();
+        c.mark(PH_PRESS);
     }
     return iters;
 }
@@ -1017,6 +1211,7 @@ __device__ int column_step(const Geo& g, const Phys& ph, Col& c, Shared& sh, dou
             dv = fmax(fabs(d), dv);
         }
         dvmax = block_max(dv, sh);
+        c.mark(PH_CONV);
         // TRANSPORT + GRID_COUPLING(0) on warp 0
         __syncthreads();
         const double dtconst = 2. * (0.5 * (c_gamma[msub] + c_ro[msub])) * c.scal[0];
@@ -1035,6 +1230,7 @@ __device__ int column_step(const Geo& g, const Phys& ph, Col& c, Shared& sh, dou
             }
         }
         __syncthreads();
+        c.mark(PH_TRANSPORT);
         if (sh.ibuf[6] != LICA_OK) return sh.ibuf[6];
         subcycles += sh.dbuf[1];
         imass += sh.dbuf[2];
@@ -1060,8 +1256,12 @@ __device__ int column_step(const Geo& g, const Phys& ph, Col& c, Shared& sh, dou
     return LICA_OK;
 }
 
-__global__ void __launch_bounds__(NT) k_column_steps(const __grid_constant__ Args A) {
+// NTH threads per column; one CTA per SM is enough for the register budget the sequential
+// parts want (no spills), more columns per SM come from smaller NTH.
+template <int NTH>
+__global__ void __launch_bounds__(NTH, 1) k_column_steps(const __grid_constant__ Args A) {
     __shared__ Shared sh;
+    extern __shared__ double dsm[];   // 5 (n+2) doubles when A.tri_smem
     const int col = blockIdx.x;
     if (col >= A.ncol) return;
     const int n = A.n, nf = 2 * n;
@@ -1085,8 +1285,19 @@ __global__ void __launch_bounds__(NT) k_column_steps(const __grid_constant__ Arg
     double* d = A.dscr + col * (NFLOW * sf + sq);
     for (int q = 0; q < NFLOW; ++q) c.a[q] = d + q * sf;
     c.psif_mtp = d + NFLOW * sf;
+    if (A.tri_smem) {
+        // the Thomas coefficient, right-hand-side and elimination arrays: thread 0 walks
+        // them sequentially, so they are kept at shared-memory latency
+        c.a[S_AK] = dsm;
+        c.a[S_BK] = dsm + sf;
+        c.a[S_CK] = dsm + 2 * sf;
+        c.a[S_GK] = dsm + 3 * sf;
+        c.a[S_GAM] = dsm + 4 * sf;
+    }
     c.region = A.iscr + col * (sf + 2);
-    Geo g{n, nf, A.L / n, A.L / nf};
+    c.prof = A.prof ? A.prof + (size_t)col * PH_COUNT : nullptr;
+    c.t0 = clock64();
+    const Geo g(n, A.L);
     int st = LICA_OK;
     for (int s = 0; s < A.nsteps && st == LICA_OK; ++s) st = column_step(g, A.ph, c, sh, A.L);
     if (threadIdx.x == 0) A.status[col] = st;
@@ -1139,6 +1350,9 @@ ScratchCache& scratch_cache() {
     static ScratchCache s;
     return s;
 }
+
+// per-phase cycle profile target (device array of COLUMN_PHASES * ncol int64) or null
+long long* g_col_prof = nullptr;
 
 
 // Host-side initial state (runs once, before the time loop).
@@ -1289,14 +1503,19 @@ int lica_gpu_column_init(int32_t n, double length, double z0, const lica_col_pro
     return LICA_OK;
 }
 
+int lica_gpu_column_profile_device(int64_t* prof) {
+    g_col_prof = (long long*)prof;
+    return LICA_OK;
+}
+
 size_t lica_gpu_column_scratch_bytes(int32_t ncol, int32_t n) {
     const size_t sf = (size_t)n + 2, sq = 2 * (size_t)n + 2;
     return (size_t)ncol * ((colk::NFLOW * sf + sq) * sizeof(double) + (sf + 2) * sizeof(int)) + 256;
 }
 
 int lica_gpu_column_steps_device(int32_t ncol, int32_t n, double length, const lica_col_props* props,
-                                 const lica_col_state* st, int32_t nsteps, void* scratch, int32_t* status,
-                                 void* stream) {
+                                 const lica_col_state* st, int32_t nsteps, int32_t threads, void* scratch,
+                                 int32_t* status, void* stream) {
     if (ncol < 1 || n < 8 || n > (1 << 20) || !(length > 0.0) || !props || !st || nsteps < 0 || !status) {
         lica_set_last_error("lica_gpu_column_steps_device", "bad sizes or null pointers", __FILE__, __LINE__);
         return LICA_BAD_ARG;
@@ -1323,6 +1542,7 @@ int lica_gpu_column_steps_device(int32_t ncol, int32_t n, double length, const l
     A.scal = st->scal;
     A.stats = st->stats;
     A.status = status;
+    A.prof = g_col_prof;
     void* scr = scratch;
     if (!scr) {
         ScratchCache& sc = scratch_cache();
@@ -1340,7 +1560,34 @@ int lica_gpu_column_steps_device(int32_t ncol, int32_t n, double length, const l
     const size_t sf = (size_t)n + 2, sq = 2 * (size_t)n + 2;
     A.dscr = (double*)scr;
     A.iscr = (int*)((char*)scr + (size_t)ncol * (colk::NFLOW * sf + sq) * sizeof(double));
-    colk::k_column_steps<<<ncol, colk::NT, 0, (cudaStream_t)stream>>>(A);
+    // tridiagonal arrays in dynamic shared memory when they fit beside the static part
+    const size_t tri_bytes = 5 * sf * sizeof(double);
+    const size_t kMaxDyn = 227 * 1024 - sizeof(colk::Shared) - 1024;
+    A.tri_smem = tri_bytes <= kMaxDyn ? 1 : 0;
+    const size_t dyn = A.tri_smem ? tri_bytes : 0;
+    const int nth = (threads == 64 || threads == 256) ? threads : colk::NT_DEFAULT;
+    {
+        static std::mutex mu;
+        static size_t set_bytes[3] = {0, 0, 0};
+        std::lock_guard<std::mutex> lk(mu);
+        const int slot = nth == 64 ? 0 : (nth == 128 ? 1 : 2);
+        if (dyn > set_bytes[slot]) {
+            cudaError_t e = cudaSuccess;
+            if (nth == 64)
+                e = cudaFuncSetAttribute(colk::k_column_steps<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+            else if (nth == 128)
+                e = cudaFuncSetAttribute(colk::k_column_steps<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)dyn);
+            else
+                e = cudaFuncSetAttribute(colk::k_column_steps<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)dyn);
+            LICA_CUDA_TRY(e);
+            set_bytes[slot] = dyn;
+        }
+    }
+    if (nth == 64) colk::k_column_steps<64><<<ncol, 64, dyn, (cudaStream_t)stream>>>(A);
+    else if (nth == 128) colk::k_column_steps<128><<<ncol, 128, dyn, (cudaStream_t)stream>>>(A);
+    else colk::k_column_steps<256><<<ncol, 256, dyn, (cudaStream_t)stream>>>(A);
     LICA_CUDA_TRY(cudaGetLastError());
     lica_count_launches(1);
     return LICA_OK;
@@ -1393,7 +1640,7 @@ int lica_gpu_column_steps(int32_t ncol, int32_t n, double length, const lica_col
     d.scal = (double*)(base + off[13]);
     d.stats = (double*)(base + off[14]);
     int32_t* dst = (int32_t*)(base + st_off);
-    int rc = lica_gpu_column_steps_device(ncol, n, length, props, &d, nsteps, nullptr, dst, nullptr);
+    int rc = lica_gpu_column_steps_device(ncol, n, length, props, &d, nsteps, 0, nullptr, dst, nullptr);
     if (rc) return rc;
     LICA_CUDA_TRY(cudaDeviceSynchronize());
     for (int q = 0; q < nfld; ++q)

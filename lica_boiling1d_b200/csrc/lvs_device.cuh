@@ -42,6 +42,8 @@ struct Win {
 
 struct Ctx {
     int n, nf, w0, kw0, lane;
+    int blo = 0, bhi = -1;   // window slots spanned by the band (per-cell loops run over them)
+    int vlo = 0, vhi = -1;   // slots the last VEL_INTP wrote
     double h, hf, ssdzf;
     Win* s;
     __device__ __forceinline__ bool in(int k) const { return k >= w0 && k < w0 + WIN; }
@@ -95,6 +97,25 @@ __device__ inline void alphi_bc(Ctx& c) {
     __syncwarp();
 }
 
+// slot range of the band cells; warp-wide
+__device__ inline void band_range(Ctx& c) {
+    const Win* s = c.s;
+    int lo = WIN, hi = -1;
+    for (int q = 0; q < PER; ++q) {
+        const int i = c.lane + 32 * q, m = s->layer[i];
+        if (m >= 1 && m <= N_MAX) {
+            lo = min(lo, i);
+            hi = max(hi, i);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    c.blo = (hi < 0) ? 0 : lo;
+    c.bhi = hi;
+}
+
 // per-layer lists in ascending window order from s->layer (the CPU restatement loads a
 // column the same way)
 __device__ inline void build_lists(Ctx& c) {
@@ -113,6 +134,7 @@ __device__ inline void build_lists(Ctx& c) {
     }
     if (c.lane == 0) s->lstart[N_MAX + 1] = pos;
     __syncwarp();
+    band_range(c);
 }
 
 // layer numbers from the lists
@@ -123,6 +145,7 @@ __device__ inline void lists_to_layer(Ctx& c) {
     for (int m = 1; m <= N_MAX; ++m)
         for (int j = s->lstart[m] + c.lane; j < s->lstart[m + 1]; j += 32) s->layer[s->lst[j]] = m;
     __syncwarp();
+    band_range(c);
 }
 
 // Window over the band of a column for work outside TRANSPORT (TEMP_GRAD): the same origin
@@ -241,8 +264,8 @@ __device__ __forceinline__ double hjweno(double a, double b, double cc, double d
 // face differences dp(i) = (phi(i+1) - phi(i)) * SSDZF over the window
 __device__ inline void face_diff(Ctx& c) {
     Win* s = c.s;
-    for (int q = 0; q < PER; ++q) {
-        const int i = c.lane + 32 * q;
+    // the WENO stencils of band cells read dp over [blo-3, bhi+2]
+    for (int i = max(0, c.blo - 3) + c.lane; i <= min(WIN - 1, c.bhi + 3); i += 32) {
         const double b = (i + 1 < WIN) ? s->phi[i + 1] : 0.0;
         s->dp[i] = (b - s->phi[i]) * c.ssdzf;
     }
@@ -268,8 +291,7 @@ __device__ __forceinline__ void weno_z(const Win* s, int i, double& dm, double& 
 __device__ inline void transport_rk3(Ctx& c, double dtlvs, int iphs, double denr) {
     Win* s = c.s;
     face_diff(c);
-    for (int q = 0; q < PER; ++q) {
-        const int i = c.lane + 32 * q;
+    for (int i = c.blo + c.lane; i <= c.bhi; i += 32) {
         const int m = s->layer[i];
         if (m < 1 || m > NN1) continue;
         const double uu1 = s->wf[i], uu2 = s->wf[i + 1], uu3 = 0.5 * (uu1 + uu2);
@@ -291,8 +313,7 @@ __device__ inline void transport_rk3(Ctx& c, double dtlvs, int iphs, double denr
         s->nv[i] = pn;
     }
     __syncwarp();
-    for (int q = 0; q < PER; ++q) {
-        const int i = c.lane + 32 * q;
+    for (int i = c.blo + c.lane; i <= c.bhi; i += 32) {
         const int m = s->layer[i];
         if (m >= 1 && m <= NN1) s->phi[i] = s->nv[i];
     }
@@ -315,8 +336,7 @@ __device__ inline void reinit_rk3(Ctx& c, double redtl) {
     Win* s = c.s;
     const double eps = c.hf * c.hf;
     face_diff(c);
-    for (int q = 0; q < PER; ++q) {
-        const int i = c.lane + 32 * q;
+    for (int i = c.blo + c.lane; i <= c.bhi; i += 32) {
         const int m = s->layer[i];
         if (m < 1 || m > NN2) continue;
         const double dz = 0.5 * (s->phi[i + 1] - s->phi[i - 1]) * c.ssdzf;
@@ -336,8 +356,7 @@ __device__ inline void reinit_rk3(Ctx& c, double redtl) {
         s->nv[i] = s->phi[i] + redtl * drhs;
     }
     __syncwarp();
-    for (int q = 0; q < PER; ++q) {
-        const int i = c.lane + 32 * q;
+    for (int i = c.blo + c.lane; i <= c.bhi; i += 32) {
         const int m = s->layer[i];
         if (m >= 1 && m <= NN2) s->phi[i] = s->nv[i];
     }
@@ -347,22 +366,22 @@ __device__ inline void reinit_rk3(Ctx& c, double redtl) {
 // REINITIALIZATION, two_phase.f:2033-2170: ILIMIT pseudo-time SSP-RK3 steps, dtau = h/2.
 __device__ inline void reinitialization(Ctx& c, int ilimit) {
     Win* s = c.s;
-    for (int q = 0; q < PER; ++q) s->alphio[c.lane + 32 * q] = s->phi[c.lane + 32 * q];
+    for (int i = c.blo + c.lane; i <= c.bhi; i += 32) s->alphio[i] = s->phi[i];
     __syncwarp();
     const double redtl = 0.5 * c.hf;
     for (int it = 0; it < ilimit; ++it) {
-        for (int q = 0; q < PER; ++q) s->rk3[c.lane + 32 * q] = s->phi[c.lane + 32 * q];
+        for (int i = c.blo + c.lane; i <= c.bhi; i += 32) s->rk3[i] = s->phi[i];
         __syncwarp();
         reinit_rk3(c, redtl);
         reinit_rk3(c, redtl);
-        for (int q = 0; q < PER; ++q) {
-            const int i = c.lane + 32 * q, m = s->layer[i];
+        for (int i = c.blo + c.lane; i <= c.bhi; i += 32) {
+            const int m = s->layer[i];
             if (m >= 1 && m <= NN2) s->phi[i] = 0.75 * s->rk3[i] + 0.25 * s->phi[i];
         }
         __syncwarp();
         reinit_rk3(c, redtl);
-        for (int q = 0; q < PER; ++q) {
-            const int i = c.lane + 32 * q, m = s->layer[i];
+        for (int i = c.blo + c.lane; i <= c.bhi; i += 32) {
+            const int m = s->layer[i];
             if (m >= 1 && m <= NN2) s->phi[i] = 1.0 / 3.0 * s->rk3[i] + 2.0 / 3.0 * s->phi[i];
         }
         __syncwarp();
@@ -373,8 +392,8 @@ __device__ inline void reinitialization(Ctx& c, int ilimit) {
 __device__ inline void rein_trigger(Ctx& c, double& dmax, double& dmin) {
     const Win* s = c.s;
     double mx = 0.0, mn = 1.0;
-    for (int q = 0; q < PER; ++q) {
-        const int i = c.lane + 32 * q, m = s->layer[i];
+    for (int i = c.blo + c.lane; i <= c.bhi; i += 32) {
+        const int m = s->layer[i];
         if (m < 1 || m > NN1) continue;
         const double dz = 0.5 * (s->phi[i + 1] - s->phi[i - 1]) * c.ssdzf;
         const double v = (0.0 + 0.0) + dz * dz;
@@ -405,8 +424,10 @@ __device__ inline int vel_intp(Ctx& c) {
         }
         return s->wt[j];
     };
-    for (int q = 0; q < PER; ++q) {
-        const int i = c.lane + 32 * q, k = c.w0 + i, m = s->layer[i];
+    // the band slots, and the slots the previous call wrote (reset to 0 when they left it)
+    const int vlo = min(c.blo, c.vhi >= 0 ? c.vlo : c.blo), vhi = max(c.bhi, c.vhi);
+    for (int i = vlo + c.lane; i <= vhi; i += 32) {
+        const int k = c.w0 + i, m = s->layer[i];
         double out = 0.0;
         if (m >= 1 && m <= NN2) {
             const double zz = (k - 1) * c.hf;
@@ -435,6 +456,8 @@ __device__ inline int vel_intp(Ctx& c) {
         s->wf[i] = out;
     }
     __syncwarp();
+    c.vlo = c.blo;
+    c.vhi = c.bhi;
     return __any_sync(0xffffffffu, bad) ? 1 : 0;
 }
 
@@ -456,6 +479,79 @@ __device__ __forceinline__ double psif_band(const Win* s, int i) {
     return ps;
 }
 
+// Interface crossings of the column fill of CAL_PSIF_MTP(1) (two_phase.f:2936-3049):
+// ktop = the largest, kbot = the smallest k in 1..nf with phi(k) phi(k+1) < 0, -1 if none.
+// phi is zero outside the window, so only window cells can cross; warp-wide, every lane
+// gets the result.
+__device__ inline void window_crossings(Ctx& c, int& ktop, int& kbot) {
+    const Win* s = c.s;
+    int top = -1, bot = 1 << 30;
+    // a crossing needs phi != 0 on both cells: band cells (or a band cell next to a ghost)
+    for (int i = c.blo + c.lane; i <= c.bhi; i += 32) {
+        const int k = c.w0 + i;
+        if (k >= 1 && k <= c.nf && i + 1 < WIN && s->phi[i] * s->phi[i + 1] < 0.0) {
+            top = max(top, k);
+            bot = min(bot, k);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        top = max(top, __shfl_xor_sync(0xffffffffu, top, o));
+        bot = min(bot, __shfl_xor_sync(0xffffffffu, bot, o));
+    }
+    ktop = top;
+    kbot = (top < 0) ? -1 : bot;
+}
+
+// Vapour volume of the whole column, sum over k = 1..nf of four replicas of
+// (1 - PSIF) * DVOL in the reference's order (two_phase.f:6230-6290), with PSIF = band_ps on
+// the window cells of layers 1..NN1 and the column fill elsewhere.  Outside the window the
+// fill is constant below and above it (the crossings lie inside), and adding 0.0 leaves
+// the sum unchanged, so only nonzero terms are added.  Lane 0 only.
+__device__ inline double column_vapour_volume(Ctx& c, const double* band_ps, int ktop, int kbot, double dvol) {
+    const Win* s = c.s;
+    double t1 = 1.0, t2 = 1.0;
+    if (ktop >= 0) {
+        t1 = (c.p(ktop) < 0.0) ? 0.0 : 1.0;
+        t2 = (c.p(kbot + 1) < 0.0) ? 0.0 : 1.0;
+    }
+    auto fill = [&](int k) { return (ktop < 0) ? 1.0 : ((k > kbot) ? t2 : t1); };
+    double vt = 0.0;
+    const int wlo = max(1, c.w0), whi = min(c.nf, c.w0 + WIN - 1);
+    // below the window
+    if (wlo > 1) {
+        const double d = (1.0 - fill(1)) * dvol;
+        if (d != 0.0)
+            for (int k = 1; k < wlo; ++k) {
+                vt = vt + d;
+                vt = vt + d;
+                vt = vt + d;
+                vt = vt + d;
+            }
+    }
+    for (int k = wlo; k <= whi; ++k) {
+        const int i = k - c.w0;
+        const double ps = (s->layer[i] >= 1 && s->layer[i] <= NN1) ? band_ps[i] : fill(k);
+        const double d = (1.0 - ps) * dvol;
+        if (d != 0.0) {
+            vt = vt + d;
+            vt = vt + d;
+            vt = vt + d;
+            vt = vt + d;
+        }
+    }
+    if (whi < c.nf) {
+        const double d = (1.0 - fill(c.nf)) * dvol;
+        if (d != 0.0)
+            for (int k = whi + 1; k <= c.nf; ++k) {
+                vt = vt + d;
+                vt = vt + d;
+                vt = vt + d;
+                vt = vt + d;
+            }
+    }
+    return vt;
+}
+
 // GLOBAL_MASS_CORRECTION, two_phase.f:6196-6318 (1-D, DVOL = SDXF*SDYF*SDZF with
 // SDXF = SDYF = 1/2, four (I,J) replicas per z-level): up to 15 uniform shifts of the
 // band phi (layers 1..NN1) towards the target vapour volume.  The first pass sums the
@@ -468,12 +564,14 @@ __device__ inline void global_mass_correction(Ctx& c, double& vol_tot_ori, doubl
     if (iphs == 1) vol_tot_ori = vol_tot_iphs;
     double vol_in = 0.0;
     for (int l = 1; l <= 15; ++l) {
-        for (int q = 0; q < PER; ++q) {
-            const int i = c.lane + 32 * q, m = s->layer[i];
+        for (int i = c.blo + c.lane; i <= c.bhi; i += 32) {
+            const int m = s->layer[i];
             s->nv[i] = (m >= 1 && m <= NN1) ? psif_band(s, i) : 0.0;
         }
         __syncwarp();
         double vol_tot = 0.0;
+        int ktop = -1, kbot = -1;
+        if (l == 1) window_crossings(c, ktop, kbot);
         if (c.lane == 0) {
             double vol_band = 0.0;
             for (int j = s->lstart[1]; j < s->lstart[NN1 + 1]; ++j) {
@@ -484,34 +582,7 @@ __device__ inline void global_mass_correction(Ctx& c, double& vol_tot_ori, doubl
                 vol_band = vol_band + v;
             }
             if (l == 1) {
-                // column fill: crossings k = nf..1 with phi(k)*phi(k+1) < 0; below the
-                // lowest one the phase of the topmost crossing, above it the phase of the
-                // cell over the lowest crossing; no crossing: liquid (PSIF = 1)
-                int ktop = -1, kbot = -1;
-                for (int k = c.nf; k >= 1; --k)
-                    if (c.p(k) * c.p(k + 1) < 0.0) {
-                        if (ktop < 0) ktop = k;
-                        kbot = k;
-                    }
-                double t1 = 1.0, t2 = 1.0;
-                if (ktop >= 0) {
-                    t1 = (c.p(ktop) < 0.0) ? 0.0 : 1.0;
-                    t2 = (c.p(kbot + 1) < 0.0) ? 0.0 : 1.0;
-                }
-                double vt = 0.0;
-                for (int k = 1; k <= c.nf; ++k) {
-                    double ps;
-                    const int i = k - c.w0;
-                    if (c.in(k) && s->layer[i] >= 1 && s->layer[i] <= NN1) ps = s->nv[i];
-                    else if (ktop < 0) ps = 1.0;
-                    else ps = (k > kbot) ? t2 : t1;
-                    const double v = (1.0 - ps) * dvol;
-                    vt = vt + v;
-                    vt = vt + v;
-                    vt = vt + v;
-                    vt = vt + v;
-                }
-                vol_tot = vt;
+                vol_tot = column_vapour_volume(c, s->nv, ktop, kbot, dvol);
                 vol_in = vol_tot - vol_band;
             } else {
                 vol_tot = vol_in + vol_band;
@@ -521,8 +592,8 @@ __device__ inline void global_mass_correction(Ctx& c, double& vol_tot_ori, doubl
         vol_in = __shfl_sync(0xffffffffu, vol_in, 0);
         if (fabs(vol_tot - vol_tot_ori) >= 1e-5) {
             const double cor = recor * (-(vol_tot_ori - vol_tot) / vol_tot_ori);
-            for (int q = 0; q < PER; ++q) {
-                const int i = c.lane + 32 * q, m = s->layer[i];
+            for (int i = c.blo + c.lane; i <= c.bhi; i += 32) {
+                const int m = s->layer[i];
                 if (m >= 1 && m <= NN1) s->phi[i] = s->phi[i] + cor;
             }
             __syncwarp();
@@ -586,6 +657,7 @@ __device__ inline int transport_column(Win* s, int lane, int n, double length, d
         s->phi[i] = (ok && m > 0) ? phi[k + 2] : 0.0;
         s->start[i] = s->phi[i];
         s->mf[i] = ok ? mf[k + 2] : 0.0;
+        s->wf[i] = 0.0;
     }
     if (lane < 7) s->ghost[lane] = 0.0;
     // VEL_INTP(2): UT = (U + UO)/2 with UO = U on the first call (:5567-5600); UO = U after
@@ -605,8 +677,8 @@ __device__ inline int transport_column(Win* s, int lane, int n, double length, d
     for (isub = 1; isub <= 10; ++isub) {
         // subcycle step at CFL 1 on layers 1..NN1 (:800-850)
         double cm = 0.0;
-        for (int q = 0; q < PER; ++q) {
-            const int i = lane + 32 * q, m = s->layer[i];
+        for (int i = c.blo + lane; i <= c.bhi; i += 32) {
+            const int m = s->layer[i];
             if (m < 1 || m > NN1) continue;
             const double cz = fabs(0.5 * (s->wf[i - 1] + s->wf[i])) * c.ssdzf;
             cm = fmax(cm, (0.0 + 0.0) + cz);
@@ -632,18 +704,18 @@ __device__ inline int transport_column(Win* s, int lane, int n, double length, d
         }
         if (time_tran + dtlvs >= P.dtconst) dtlvs = P.dtconst - time_tran;
         time_tran = time_tran + dtlvs;
-        for (int q = 0; q < PER; ++q) s->rk3[lane + 32 * q] = s->phi[lane + 32 * q];
+        for (int i = c.blo + lane; i <= c.bhi; i += 32) s->rk3[i] = s->phi[i];
         __syncwarp();
         transport_rk3(c, dtlvs, P.iphs, P.denr);
         transport_rk3(c, dtlvs, P.iphs, P.denr);
-        for (int q = 0; q < PER; ++q) {
-            const int i = lane + 32 * q, m = s->layer[i];
+        for (int i = c.blo + lane; i <= c.bhi; i += 32) {
+            const int m = s->layer[i];
             if (m >= 1 && m <= NN1) s->phi[i] = 0.75 * s->rk3[i] + 0.25 * s->phi[i];
         }
         __syncwarp();
         transport_rk3(c, dtlvs, P.iphs, P.denr);
-        for (int q = 0; q < PER; ++q) {
-            const int i = lane + 32 * q, m = s->layer[i];
+        for (int i = c.blo + lane; i <= c.bhi; i += 32) {
+            const int m = s->layer[i];
             if (m >= 1 && m <= NN1) s->phi[i] = 1.0 / 3.0 * s->rk3[i] + 2.0 / 3.0 * s->phi[i];
         }
         __syncwarp();
@@ -715,8 +787,8 @@ __device__ inline int transport_column(Win* s, int lane, int n, double length, d
     // cells are snapped at 1e-3 / 0.999 (:5000-5061).
     for (int j = lane; j < WTN; j += 32) s->fmask[j] = 0;
     __syncwarp();
-    for (int q = 0; q < PER; ++q) {
-        const int i = lane + 32 * q, k = w0 + i, m = s->layer[i];
+    for (int i = c.blo + lane; i <= c.bhi; i += 32) {
+        const int k = w0 + i, m = s->layer[i];
         if (m >= 1 && m <= NN1 && k >= 1 && k <= nf) {
             const int j = col::kcoump_vel(c.h, c.hf, n, k) - c.kw0;   // inside the window's face range
             if (j >= 0 && j < WTN) s->fmask[j] = 1;
