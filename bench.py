@@ -8,6 +8,12 @@ multigrid preconditioner, FP64 throughout, set-up (beta coarsening) included.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+The line also carries the RK3 time-step legs ("rk3"): the 1-D boiling column of 512 flow
+cells (film 0.1, density ratio 1000, viscosity ratio 20, conductivity ratio 25, 10 K
+superheat) and a batch of 4096 independent columns of uneven length (128-2048 cells, 2-20 K,
+density ratio 100-1600), whole RK3 steps in one persistent launch, beside the CPU
+restatement's time for the same steps.
+
 Under torchrun each rank solves its own replica (the 2-D multigrid does not shard
 here); value = solves of all ranks / the slowest rank's time.  Rank 0 prints one JSON
 line.  --impl reference times the CPU restatement of the same solve (the reference has
@@ -137,7 +143,139 @@ def run_reference(args):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "iterations": its[-1],
     }
+    line["rk3"] = {"cpu_baseline": rk3_cpu()}
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ RK3 column legs
+C1 = dict(n=512, z0=0.1, denr=1000.0, visr=20.0, tcr=25.0, jakob=0.009)
+C4_NCOL = 4096
+
+
+def c1_props():
+    from lica_boiling1d_b200.column import ColumnProps
+    return ColumnProps(denr=C1["denr"], visr=C1["visr"], tcr=C1["tcr"], jakob=C1["jakob"])
+
+
+def rk3_cpu(max_seconds=12.0):
+    """The CPU restatement's time for the same steps: one column of the 512-cell workload
+    (single thread, as the reference's 1-D case runs), and a sample of the uneven batch run
+    over all host cores (independent columns; the oracle releases the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from lica_boiling1d_b200.column import uneven_batch
+    from oracle import oracle
+    oracle.lib(native=True)
+    props = c1_props()
+    st = oracle.col_init(C1["n"], 1.0, C1["z0"], props)
+    for _ in range(3):
+        oracle.col_step(st, C1["n"], 1.0, props, native=True)
+    t0 = time.perf_counter()
+    k = 0
+    while time.perf_counter() - t0 < max_seconds / 2 and k < 400:
+        oracle.col_step(st, C1["n"], 1.0, props, native=True)
+        k += 1
+    c1 = k / (time.perf_counter() - t0)
+    n, length, z0, bprops = uneven_batch(C4_NCOL, seed=0)
+    sample = list(range(0, C4_NCOL, max(1, C4_NCOL // 256)))
+    states = {c: oracle.col_init(int(n[c]), float(length[c]), float(z0[c]), bprops[c]) for c in sample}
+    cores = os.cpu_count()
+
+    def run(c, steps):
+        for _ in range(steps):
+            oracle.col_step(states[c], int(n[c]), float(length[c]), bprops[c], native=True)
+        return steps
+    with ThreadPoolExecutor(cores) as ex:
+        list(ex.map(lambda c: run(c, 1), sample))          # warm-up step
+        t0 = time.perf_counter()
+        done = sum(ex.map(lambda c: run(c, 2), sample))
+        dt = time.perf_counter() - t0
+    cells = float(np.mean([n[c] for c in sample]))
+    col_steps = done / dt
+    return {"c1_steps_per_s": c1, "c1_sample": f"{k} steps of the 512-cell column, one thread",
+            "batch_column_steps_per_s": col_steps, "batch_steps_per_s": col_steps / C4_NCOL,
+            "batch_cell_updates_per_s": col_steps * cells, "cores": cores,
+            "batch_sample": f"{len(sample)} of the {C4_NCOL} columns x 2 steps on {cores} threads"}
+
+
+def rk3_legs(dev, flush, steps_c1=200, steps_c4=20, warmup=3):
+    import torch
+
+    from lica_boiling1d_b200 import native
+    from lica_boiling1d_b200.column import ColumnBatch, Columns, uneven_batch
+    out = {}
+    props = c1_props()
+    # C1: one column, one persistent launch of steps_c1 steps
+    col = Columns.film(C1["n"], 1.0, [C1["z0"]], props).to(dev)
+    col.steps(warmup, props, threads=256)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    flush.fill_(3)
+    l0 = native.launch_count()
+    e0.record()
+    st = col.steps(steps_c1, props, threads=256)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    launches = native.launch_count() - l0
+    if int(st.max()) != 0:
+        raise RuntimeError(f"column step status {int(st.max())}")
+    ms = e0.elapsed_time(e1)
+    out["column_512"] = {
+        "workload": "1-D boiling column, 512 flow cells (1024 refined), film 0.1 L, density ratio 1000, viscosity "
+                    "ratio 20, conductivity ratio 25, Jakob 0.009 (10 K), CFL 0.5, FP64, one persistent launch",
+        "steps_per_s": steps_c1 / (ms / 1e3), "ms_per_step": ms / steps_c1, "steps": steps_c1, "threads": 256,
+        "cell_updates_per_s": C1["n"] * steps_c1 / (ms / 1e3), "gpu_launches": launches,
+        "interface_height": float(col.to(None).stats[0][5])}
+    # end to end: the host-array C-ABI entry, one step per call (state copied in and out)
+    host = col.to(None)
+    pinned = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in host.arrays.items()}
+    hcol = Columns(C1["n"], 1.0, pinned)
+    ke = 20
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        hcol.steps(1, props)
+    e2e_s = time.perf_counter() - t0
+    bytes_state = sum(a.nbytes for a in pinned.values())
+    out["column_512"]["e2e"] = {"steps_per_s": ke / e2e_s, "h2d_bytes_per_step": bytes_state,
+                                "d2h_bytes_per_step": bytes_state,
+                                "path": "lica_gpu_column_steps (C ABI), host arrays, one step per call"}
+    # C4: the uneven batch, CTA width picked by a short trial of each candidate
+    n, length, z0, bprops = uneven_batch(C4_NCOL, seed=0)
+    batch = ColumnBatch.films(n, length, z0, bprops).to(dev)
+    trial = {}
+    for th in (64, 128):
+        b = batch.to(dev)
+        b.steps(1, threads=th)
+        torch.cuda.synchronize(dev)
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record()
+        b.steps(2, threads=th)
+        a1.record()
+        torch.cuda.synchronize(dev)
+        trial[th] = a0.elapsed_time(a1) / 2
+        del b
+    th = min(trial, key=trial.get)
+    batch.steps(warmup, threads=th)
+    torch.cuda.synchronize(dev)
+    flush.fill_(5)
+    l0 = native.launch_count()
+    e0.record()
+    st = batch.steps(steps_c4, threads=th)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    launches = native.launch_count() - l0
+    if int(st.max()) != 0:
+        raise RuntimeError(f"batch status {int(st.max())}")
+    ms = e0.elapsed_time(e1)
+    cells = int(n.sum())
+    out["batch_4096"] = {
+        "workload": f"{C4_NCOL} independent 1-D boiling columns, uneven 128-2048 flow cells (seeded, {cells} in "
+                    "total), superheat 2-20 K, density ratio 100-1600, FP64, one persistent launch, longest first",
+        "steps_per_s": steps_c4 / (ms / 1e3), "ms_per_step": ms / steps_c4, "steps": steps_c4,
+        "column_steps_per_s": C4_NCOL * steps_c4 / (ms / 1e3), "cell_updates_per_s": cells * steps_c4 / (ms / 1e3),
+        "threads": th, "autotune_ms_per_step": trial, "gpu_launches": launches}
+    return out
 
 
 # ------------------------------------------------------------------ GPU leg
@@ -307,6 +445,12 @@ def run_ours(args):
         cpu = {"value": len(times) / sum(times), "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{len(times)} complete solves of the same workload (~15 s), FP64 C++/OpenMP restatement"}
 
+    rk3 = None
+    if not args.skip_rk3:
+        rk3 = rk3_legs(dev, flush)
+        if rank == 0 and world == 1 and not args.skip_cpu:
+            rk3["cpu_baseline"] = rk3_cpu()
+            rk3["cpu_baseline"]["kind"] = "port"
     return finish(args, locals())
 
 
@@ -327,7 +471,7 @@ def finish(args, v):
                        "l2_flush": "256 MiB write between steps", "parallelism": f"replicas x{v['world']}"},
             "iterations": v["its"][-1], "rel_residual": v["rel"],
             "roofline": v["roofline"], "cpu_baseline": v["cpu"], "e2e": v["e2e"], "gpu_launches": int(v["launches"]),
-            "clocks": v["clk"], "variants": v["variants"],
+            "clocks": v["clk"], "variants": v["variants"], "rk3": v.get("rk3"),
         }
         print(json.dumps(line), flush=True)
     v["solver"].close()
@@ -348,6 +492,7 @@ def main():
     ap.add_argument("--ncoarse", type=int, default=1, help="inner V-cycles of the coarsest-level solve")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end and later legs (profiling runs)")
     ap.add_argument("--no-profile", action="store_true", help="skip the kernel-class timing and later legs")
+    ap.add_argument("--skip-rk3", action="store_true", help="skip the RK3 column legs")
     ap.add_argument("--no-graph", action="store_true",
                     help="launch kernels one by one instead of one CUDA graph per solve (for ncu, which cannot "
                          "profile kernels of a graph with a conditional node)")

@@ -263,6 +263,21 @@ int lica_gpu_column_steps_device(int32_t ncol, int32_t n, double length, const l
  * PRESSURE_CORRECTION, 9 CONVRGE1, 10 TRANSPORT + GRID_COUPLING.  NULL turns it off. */
 int lica_gpu_column_profile_device(int64_t* prof);
 
+/* Batches of columns of uneven size, length and properties (one opaque handle per batch
+ * layout).  Column c has n[c] flow cells over length[c] with props[c]; its arrays are packed
+ * back to back: lica_gpu_column_batch_layout gives per column the offsets (in elements) of
+ * its flow arrays (w, p, t, psi_cn, psi_zn, wo, imask), its phi-like arrays (phi, layer,
+ * mflvs) and its psif-like arrays (psif, sfgas, sfgas2): offsets[3c .. 3c+2]; and the
+ * totals: totals[0..2] elements of each kind, totals[3] scratch bytes.  scal and stats
+ * stay 5 and 8 per column.  The kernel runs the longest columns first. */
+typedef struct lica_col_batch lica_col_batch;
+int lica_gpu_column_batch_create(lica_col_batch** out, int32_t ncol, const int32_t* n, const double* length,
+                                 const lica_col_props* props);
+int lica_gpu_column_batch_destroy(lica_col_batch* batch);
+int lica_gpu_column_batch_layout(const lica_col_batch* batch, int64_t* offsets, int64_t* totals);
+int lica_gpu_column_batch_steps_device(const lica_col_batch* batch, const lica_col_state* st, int32_t nsteps,
+                                       int32_t threads, void* scratch, int32_t* status, void* stream);
+
 /* Same on host arrays (copies in, runs, copies out); returns the last non-OK column status. */
 int lica_gpu_column_steps(int32_t ncol, int32_t n, double length, const lica_col_props* props,
                           lica_col_state* st, int32_t nsteps, int32_t* status);

@@ -145,3 +145,133 @@ def profile(prof):
     zeroed by the caller) during later steps; None turns the profile off."""
     native.check(native.lib().lica_gpu_column_profile_device(C.c_void_p(prof.data_ptr() if prof is not None else None)),
                  "column profile")
+
+
+_FLOW = ("w", "p", "t", "psi_cn", "psi_zn", "wo", "imask")
+_PHI = ("phi", "layer", "mflvs")
+_PSIF = ("psif", "sfgas", "sfgas2")
+_INT = ("layer", "imask")
+
+
+class ColumnBatch:
+    """Columns of uneven size, length and properties, packed back to back
+    (lica_gpu_column_batch_*).  Flat arrays: the flow kind (w, p, t, psi_cn, psi_zn, wo,
+    imask), the phi kind (phi, layer, mflvs), the psif kind (psif, sfgas, sfgas2); scal
+    (ncol, 5) and stats (ncol, 8).  ``offsets[c]`` = the column's start in each kind."""
+
+    def __init__(self, n, length, props, arrays=None, _handle=None):
+        self.n = np.asarray(n, dtype=np.int32)
+        self.length = np.asarray(length, dtype=np.float64)
+        self.props = list(props)
+        self.ncol = len(self.n)
+        if _handle is None:
+            h = C.c_void_p()
+            cp = (native.ColProps * self.ncol)(*[p.c() for p in self.props])
+            native.check(native.lib().lica_gpu_column_batch_create(
+                C.byref(h), self.ncol, self.n.ctypes.data_as(C.POINTER(C.c_int32)),
+                self.length.ctypes.data_as(C.POINTER(C.c_double)), cp), "column batch")
+            _handle = _Handle(h)
+        self._h = _handle
+        off = np.zeros(3 * self.ncol, np.int64)
+        tot = np.zeros(4, np.int64)
+        native.check(native.lib().lica_gpu_column_batch_layout(self._h.ptr, off.ctypes.data_as(C.POINTER(C.c_int64)),
+                                                               tot.ctypes.data_as(C.POINTER(C.c_int64))), "layout")
+        self.offsets = off.reshape(self.ncol, 3)
+        self.totals = tot
+        if arrays is None:
+            arrays = {}
+            for k in _FLOW:
+                arrays[k] = np.zeros(tot[0], np.int32 if k in _INT else np.float64)
+            for k in _PHI:
+                arrays[k] = np.zeros(tot[1], np.int32 if k in _INT else np.float64)
+            for k in _PSIF:
+                arrays[k] = np.zeros(tot[2], np.float64)
+            arrays["scal"] = np.zeros((self.ncol, 5))
+            arrays["stats"] = np.zeros((self.ncol, 8))
+        self.arrays = arrays
+
+    @staticmethod
+    def films(n, length, z0, props):
+        """Each column with a vapour film of thickness z0[c] at the wall (lica_gpu_column_init)."""
+        b = ColumnBatch(n, length, props)
+        for c in range(b.ncol):
+            st = b._column_state(c, lambda a: a.ctypes.data)
+            native.check(native.lib().lica_gpu_column_init(int(b.n[c]), float(b.length[c]), float(z0[c]),
+                                                           C.byref(b.props[c].c()), C.byref(st)), "column init")
+        return b
+
+    def _column_state(self, c, ptr):
+        of, op, oq = (int(x) for x in self.offsets[c])
+        isz = {np.dtype(np.int32): 4, np.dtype(np.float64): 8}
+
+        def at(k, o):
+            a = self.arrays[k]
+            return ptr(a) + o * (4 if k in _INT else 8)
+        f = {k: at(k, of) for k in _FLOW}
+        f.update({k: at(k, op) for k in _PHI})
+        f.update({k: at(k, oq) for k in _PSIF})
+        f["scal"] = ptr(self.arrays["scal"]) + 8 * 5 * c
+        f["stats"] = ptr(self.arrays["stats"]) + 8 * 8 * c
+        del isz
+        return native.ColState(*[f[k] for k in native.COL_FIELDS])
+
+    def column(self, c):
+        """Host copy of column c's arrays in lica_col_state shapes."""
+        host = self if isinstance(self.arrays["w"], np.ndarray) else self.to(None)
+        n = int(self.n[c])
+        of, op, oq = (int(x) for x in self.offsets[c])
+        out = {k: host.arrays[k][of:of + n + 2].copy() for k in _FLOW}
+        out.update({k: host.arrays[k][op:op + 2 * n + 7].copy() for k in _PHI})
+        out.update({k: host.arrays[k][oq:oq + 2 * n + 2].copy() for k in _PSIF})
+        out["scal"] = host.arrays["scal"][c].copy()
+        out["stats"] = host.arrays["stats"][c].copy()
+        return out
+
+    def to(self, device):
+        import torch
+        out = {}
+        for k, v in self.arrays.items():
+            if device is None:
+                out[k] = v.detach().cpu().numpy() if isinstance(v, torch.Tensor) else v.copy()
+            else:
+                out[k] = torch.as_tensor(v if isinstance(v, np.ndarray) else v.cpu().numpy(), device=device).clone()
+        return ColumnBatch(self.n, self.length, self.props, out, self._h)
+
+    def steps(self, nsteps, threads=0, stream=None, scratch=None):
+        """nsteps time steps of every column (device state).  Returns the per-column status."""
+        import torch
+        dev = self.arrays["w"].device
+        status = torch.zeros(self.ncol, dtype=torch.int32, device=dev)
+        s = stream if stream is not None else torch.cuda.current_stream(dev)
+        st = native.ColState(*[self.arrays[k].data_ptr() for k in native.COL_FIELDS])
+        native.check(native.lib().lica_gpu_column_batch_steps_device(
+            self._h.ptr, C.byref(st), int(nsteps), int(threads),
+            C.c_void_p(scratch.data_ptr() if scratch is not None else None), C.c_void_p(status.data_ptr()),
+            C.c_void_p(s.cuda_stream)), "column batch steps")
+        return status
+
+
+class _Handle:
+    def __init__(self, ptr):
+        self.ptr = ptr
+
+    def __del__(self):
+        try:
+            native.lib().lica_gpu_column_batch_destroy(self.ptr)
+        except Exception:
+            pass
+
+
+def uneven_batch(ncol, seed=0, nmin=128, nmax=2048, h=1.0 / 512):
+    """Seeded batch of independent boiling columns: n uniform in [nmin, nmax] flow cells of
+    size h, film 0.1 of the column, wall superheat uniform 2-20 K (Jakob number 0.009 per
+    10 K), liquid/vapour density ratio uniform 100-1600; other properties of the shipped
+    case.  Returns (n, length, z0, props)."""
+    rng = np.random.default_rng(seed)
+    n = rng.integers(nmin, nmax + 1, ncol).astype(np.int32)
+    length = n * h
+    z0 = 0.1 * length + 0.37 * h
+    sup = rng.uniform(2.0, 20.0, ncol)
+    denr = rng.uniform(100.0, 1600.0, ncol)
+    props = [ColumnProps(denr=float(d), jakob=0.009 * float(t) / 10.0) for d, t in zip(denr, sup)]
+    return n, length, z0, props

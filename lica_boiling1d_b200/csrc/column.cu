@@ -52,10 +52,21 @@ enum {
     S_SPARE1, S_SPARE2, S_SPARE3, S_SPARE4
 };
 
+// One column of a batch of uneven columns: size, length, constants and the offsets of
+// its arrays in the packed state (flow, refined phi-like, refined psif-like) and scratch.
+struct ColDesc {
+    int n, pad;
+    double L;
+    Phys ph;
+    long long off_f, off_p, off_q, off_d, off_i;
+};
+
 struct Args {
     int ncol, n, nsteps;
     double L;
     Phys ph;
+    const ColDesc* desc;   // per-column descriptors, or null for ncol columns of size n
+    const int* order;      // launch order (CTA b runs column order[b]), or null
     double *w, *p, *t, *psi_cn, *psi_zn, *phi, *psif, *wo, *mflvs, *sfgas, *sfgas2, *scal, *stats;
     int *layer, *imask, *status;
     double* dscr;
@@ -1262,27 +1273,53 @@ template <int NTH>
 __global__ void __launch_bounds__(NTH, 1) k_column_steps(const __grid_constant__ Args A) {
     __shared__ Shared sh;
     extern __shared__ double dsm[];   // 5 (n+2) doubles when A.tri_smem
-    const int col = blockIdx.x;
-    if (col >= A.ncol) return;
-    const int n = A.n, nf = 2 * n;
-    const size_t sf = (size_t)n + 2, sp = (size_t)nf + 7, sq = (size_t)nf + 2;
+    if ((int)blockIdx.x >= A.ncol) return;
+    const int col = A.order ? A.order[blockIdx.x] : (int)blockIdx.x;
+    int n;
+    double L;
+    Phys ph;
+    size_t of, op, oq, od, oi;
+    if (A.desc) {
+        const ColDesc& D = A.desc[col];
+        n = D.n;
+        L = D.L;
+        ph = D.ph;
+        of = D.off_f;
+        op = D.off_p;
+        oq = D.off_q;
+        od = D.off_d;
+        oi = D.off_i;
+    } else {
+        n = A.n;
+        L = A.L;
+        ph = A.ph;
+        const size_t sf = (size_t)n + 2, sq = 2 * (size_t)n + 2;
+        of = col * sf;
+        op = col * (2 * (size_t)n + 7);
+        oq = col * sq;
+        od = col * (NFLOW * sf + sq);
+        oi = col * (sf + 2);
+    }
+    const int nf = 2 * n;
+    const size_t sf = (size_t)n + 2;
     Col c;
-    c.w = A.w + col * sf;
-    c.p = A.p + col * sf;
-    c.t = A.t + col * sf;
-    c.psi_cn = A.psi_cn + col * sf;
-    c.psi_zn = A.psi_zn + col * sf;
-    c.wo = A.wo + col * sf;
-    c.imask = A.imask + col * sf;
-    c.phi = A.phi + col * sp;
-    c.layer = A.layer + col * sp;
-    c.mflvs = A.mflvs + col * sp;
-    c.psif = A.psif + col * sq;
-    c.sfgas = A.sfgas + col * sq;
-    c.sfgas2 = A.sfgas2 + col * sq;
+    c.w = A.w + of;
+    c.p = A.p + of;
+    c.t = A.t + of;
+    c.psi_cn = A.psi_cn + of;
+    c.psi_zn = A.psi_zn + of;
+    c.wo = A.wo + of;
+    c.imask = A.imask + of;
+    c.phi = A.phi + op;
+    c.layer = A.layer + op;
+    c.mflvs = A.mflvs + op;
+    c.psif = A.psif + oq;
+    c.sfgas = A.sfgas + oq;
+    c.sfgas2 = A.sfgas2 + oq;
     c.scal = A.scal + col * 5;
     c.stats = A.stats + col * 8;
-    double* d = A.dscr + col * (NFLOW * sf + sq);
+    (void)nf;
+    double* d = A.dscr + od;
     for (int q = 0; q < NFLOW; ++q) c.a[q] = d + q * sf;
     c.psif_mtp = d + NFLOW * sf;
     if (A.tri_smem) {
@@ -1294,12 +1331,12 @@ __global__ void __launch_bounds__(NTH, 1) k_column_steps(const __grid_constant__
         c.a[S_GK] = dsm + 3 * sf;
         c.a[S_GAM] = dsm + 4 * sf;
     }
-    c.region = A.iscr + col * (sf + 2);
+    c.region = A.iscr + oi;
     c.prof = A.prof ? A.prof + (size_t)col * PH_COUNT : nullptr;
     c.t0 = clock64();
-    const Geo g(n, A.L);
+    const Geo g(n, L);
     int st = LICA_OK;
-    for (int s = 0; s < A.nsteps && st == LICA_OK; ++s) st = column_step(g, A.ph, c, sh, A.L);
+    for (int s = 0; s < A.nsteps && st == LICA_OK; ++s) st = column_step(g, ph, c, sh, L);
     if (threadIdx.x == 0) A.status[col] = st;
 }
 
@@ -1513,19 +1550,11 @@ size_t lica_gpu_column_scratch_bytes(int32_t ncol, int32_t n) {
     return (size_t)ncol * ((colk::NFLOW * sf + sq) * sizeof(double) + (sf + 2) * sizeof(int)) + 256;
 }
 
-int lica_gpu_column_steps_device(int32_t ncol, int32_t n, double length, const lica_col_props* props,
-                                 const lica_col_state* st, int32_t nsteps, int32_t threads, void* scratch,
-                                 int32_t* status, void* stream) {
-    if (ncol < 1 || n < 8 || n > (1 << 20) || !(length > 0.0) || !props || !st || nsteps < 0 || !status) {
-        lica_set_last_error("lica_gpu_column_steps_device", "bad sizes or null pointers", __FILE__, __LINE__);
-        return LICA_BAD_ARG;
-    }
-    colk::Args A;
-    A.ncol = ncol;
-    A.n = n;
-    A.nsteps = nsteps;
-    A.L = length;
-    A.ph = make_phys(props);
+}  // extern "C"
+
+namespace {
+
+void fill_state(colk::Args& A, const lica_col_state* st) {
     A.w = st->w;
     A.p = st->p;
     A.t = st->t;
@@ -1541,27 +1570,17 @@ int lica_gpu_column_steps_device(int32_t ncol, int32_t n, double length, const l
     A.imask = st->imask;
     A.scal = st->scal;
     A.stats = st->stats;
-    A.status = status;
-    A.prof = g_col_prof;
-    void* scr = scratch;
-    if (!scr) {
-        ScratchCache& sc = scratch_cache();
-        std::lock_guard<std::mutex> lk(sc.mu);
-        const size_t need = lica_gpu_column_scratch_bytes(ncol, n);
-        if (need > sc.bytes) {
-            if (sc.ptr) cudaFree(sc.ptr);
-            sc.ptr = nullptr;
-            sc.bytes = 0;
-            LICA_CUDA_TRY(cudaMalloc(&sc.ptr, need));
-            sc.bytes = need;
-        }
-        scr = sc.ptr;
-    }
-    const size_t sf = (size_t)n + 2, sq = 2 * (size_t)n + 2;
-    A.dscr = (double*)scr;
-    A.iscr = (int*)((char*)scr + (size_t)ncol * (colk::NFLOW * sf + sq) * sizeof(double));
-    // tridiagonal arrays in dynamic shared memory when they fit beside the static part
-    const size_t tri_bytes = 5 * sf * sizeof(double);
+}
+
+bool state_ok(const lica_col_state* st) {
+    return st && st->w && st->p && st->t && st->psi_cn && st->psi_zn && st->phi && st->layer && st->psif && st->wo &&
+           st->mflvs && st->sfgas && st->sfgas2 && st->imask && st->scal && st->stats;
+}
+
+// Launch A over A.ncol CTAs of `threads` threads; nmax = the largest column, which sizes
+// the shared-memory tridiagonal arrays.
+int launch_columns(colk::Args& A, int nmax, int threads, void* stream) {
+    const size_t tri_bytes = 5 * ((size_t)nmax + 2) * sizeof(double);
     const size_t kMaxDyn = 227 * 1024 - sizeof(colk::Shared) - 1024;
     A.tri_smem = tri_bytes <= kMaxDyn ? 1 : 0;
     const size_t dyn = A.tri_smem ? tri_bytes : 0;
@@ -1585,12 +1604,175 @@ int lica_gpu_column_steps_device(int32_t ncol, int32_t n, double length, const l
             set_bytes[slot] = dyn;
         }
     }
-    if (nth == 64) colk::k_column_steps<64><<<ncol, 64, dyn, (cudaStream_t)stream>>>(A);
-    else if (nth == 128) colk::k_column_steps<128><<<ncol, 128, dyn, (cudaStream_t)stream>>>(A);
-    else colk::k_column_steps<256><<<ncol, 256, dyn, (cudaStream_t)stream>>>(A);
+    if (nth == 64) colk::k_column_steps<64><<<A.ncol, 64, dyn, (cudaStream_t)stream>>>(A);
+    else if (nth == 128) colk::k_column_steps<128><<<A.ncol, 128, dyn, (cudaStream_t)stream>>>(A);
+    else colk::k_column_steps<256><<<A.ncol, 256, dyn, (cudaStream_t)stream>>>(A);
     LICA_CUDA_TRY(cudaGetLastError());
     lica_count_launches(1);
     return LICA_OK;
+}
+
+int column_scratch(size_t need, void** out) {
+    ScratchCache& sc = scratch_cache();
+    std::lock_guard<std::mutex> lk(sc.mu);
+    if (need > sc.bytes) {
+        if (sc.ptr) cudaFree(sc.ptr);
+        sc.ptr = nullptr;
+        sc.bytes = 0;
+        LICA_CUDA_TRY(cudaMalloc(&sc.ptr, need));
+        sc.bytes = need;
+    }
+    *out = sc.ptr;
+    return LICA_OK;
+}
+
+}  // namespace
+
+// A batch of columns of uneven size and properties.
+struct lica_col_batch {
+    int ncol = 0, nmax = 0;
+    std::vector<colk::ColDesc> desc;
+    std::vector<int> order;
+    colk::ColDesc* d_desc = nullptr;
+    int* d_order = nullptr;
+    int64_t tot[5] = {0, 0, 0, 0, 0};   // flow, phi-like, psif-like doubles; scratch doubles, scratch ints
+    std::mutex mu;
+};
+
+extern "C" {
+
+int lica_gpu_column_steps_device(int32_t ncol, int32_t n, double length, const lica_col_props* props,
+                                 const lica_col_state* st, int32_t nsteps, int32_t threads, void* scratch,
+                                 int32_t* status, void* stream) {
+    if (ncol < 1 || n < 8 || n > (1 << 20) || !(length > 0.0) || !props || !state_ok(st) || nsteps < 0 || !status) {
+        lica_set_last_error("lica_gpu_column_steps_device", "bad sizes or null pointers", __FILE__, __LINE__);
+        return LICA_BAD_ARG;
+    }
+    colk::Args A{};
+    A.ncol = ncol;
+    A.n = n;
+    A.nsteps = nsteps;
+    A.L = length;
+    A.ph = make_phys(props);
+    A.desc = nullptr;
+    A.order = nullptr;
+    fill_state(A, st);
+    A.status = status;
+    A.prof = g_col_prof;
+    void* scr = scratch;
+    if (!scr) {
+        const int rc = column_scratch(lica_gpu_column_scratch_bytes(ncol, n), &scr);
+        if (rc) return rc;
+    }
+    const size_t sf = (size_t)n + 2, sq = 2 * (size_t)n + 2;
+    A.dscr = (double*)scr;
+    A.iscr = (int*)((char*)scr + (size_t)ncol * (colk::NFLOW * sf + sq) * sizeof(double));
+    return launch_columns(A, n, threads, stream);
+}
+
+int lica_gpu_column_batch_create(lica_col_batch** out, int32_t ncol, const int32_t* n, const double* length,
+                                 const lica_col_props* props) {
+    if (!out || ncol < 1 || !n || !length || !props) return LICA_BAD_ARG;
+    auto* b = new lica_col_batch();
+    b->ncol = ncol;
+    b->desc.resize(ncol);
+    int64_t of = 0, op = 0, oq = 0, od = 0, oi = 0;
+    for (int c = 0; c < ncol; ++c) {
+        if (n[c] < 8 || n[c] > (1 << 20) || !(length[c] > 0.0)) {
+            delete b;
+            lica_set_last_error("lica_gpu_column_batch_create", "column size < 8 or length <= 0", __FILE__, __LINE__);
+            return LICA_BAD_ARG;
+        }
+        colk::ColDesc& D = b->desc[c];
+        D.n = n[c];
+        D.pad = 0;
+        D.L = length[c];
+        D.ph = make_phys(&props[c]);
+        const int64_t sf = n[c] + 2, sq = 2 * (int64_t)n[c] + 2;
+        D.off_f = of;
+        D.off_p = op;
+        D.off_q = oq;
+        D.off_d = od;
+        D.off_i = oi;
+        of += sf;
+        op += 2 * (int64_t)n[c] + 7;
+        oq += sq;
+        od += colk::NFLOW * sf + sq;
+        oi += sf + 2;
+        b->nmax = std::max(b->nmax, (int)n[c]);
+    }
+    b->tot[0] = of;
+    b->tot[1] = op;
+    b->tot[2] = oq;
+    b->tot[3] = od;
+    b->tot[4] = oi;
+    // longest columns first, so the last CTAs to start are the short ones
+    b->order.resize(ncol);
+    for (int c = 0; c < ncol; ++c) b->order[c] = c;
+    std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) { return n[x] > n[y]; });
+    *out = b;
+    return LICA_OK;
+}
+
+int lica_gpu_column_batch_destroy(lica_col_batch* b) {
+    if (!b) return LICA_OK;
+    if (b->d_desc) cudaFree(b->d_desc);
+    if (b->d_order) cudaFree(b->d_order);
+    delete b;
+    return LICA_OK;
+}
+
+int lica_gpu_column_batch_layout(const lica_col_batch* b, int64_t* offsets, int64_t* totals) {
+    if (!b) return LICA_BAD_ARG;
+    if (offsets)
+        for (int c = 0; c < b->ncol; ++c) {
+            offsets[3 * c + 0] = b->desc[c].off_f;
+            offsets[3 * c + 1] = b->desc[c].off_p;
+            offsets[3 * c + 2] = b->desc[c].off_q;
+        }
+    if (totals) {
+        totals[0] = b->tot[0];
+        totals[1] = b->tot[1];
+        totals[2] = b->tot[2];
+        totals[3] = (int64_t)(b->tot[3] * sizeof(double) + b->tot[4] * sizeof(int) + 256);
+    }
+    return LICA_OK;
+}
+
+int lica_gpu_column_batch_steps_device(const lica_col_batch* b, const lica_col_state* st, int32_t nsteps,
+                                       int32_t threads, void* scratch, int32_t* status, void* stream) {
+    if (!b || !state_ok(st) || nsteps < 0 || !status) return LICA_BAD_ARG;
+    {
+        // descriptors and launch order go to the device on first use (the host-side layout
+        // and initial state need no GPU)
+        lica_col_batch* m = const_cast<lica_col_batch*>(b);
+        std::lock_guard<std::mutex> lk(m->mu);
+        if (!m->d_desc) {
+            LICA_CUDA_TRY(cudaMalloc(&m->d_desc, sizeof(colk::ColDesc) * m->ncol));
+            LICA_CUDA_TRY(cudaMalloc(&m->d_order, sizeof(int) * m->ncol));
+            LICA_CUDA_TRY(
+                cudaMemcpy(m->d_desc, m->desc.data(), sizeof(colk::ColDesc) * m->ncol, cudaMemcpyHostToDevice));
+            LICA_CUDA_TRY(cudaMemcpy(m->d_order, m->order.data(), sizeof(int) * m->ncol, cudaMemcpyHostToDevice));
+        }
+    }
+    colk::Args A{};
+    A.ncol = b->ncol;
+    A.n = b->nmax;
+    A.nsteps = nsteps;
+    A.L = 1.0;
+    A.desc = b->d_desc;
+    A.order = b->d_order;
+    fill_state(A, st);
+    A.status = status;
+    A.prof = g_col_prof;
+    void* scr = scratch;
+    if (!scr) {
+        const int rc = column_scratch((size_t)(b->tot[3] * sizeof(double) + b->tot[4] * sizeof(int) + 256), &scr);
+        if (rc) return rc;
+    }
+    A.dscr = (double*)scr;
+    A.iscr = (int*)((char*)scr + (size_t)b->tot[3] * sizeof(double));
+    return launch_columns(A, b->nmax, threads, stream);
 }
 
 int lica_gpu_column_steps(int32_t ncol, int32_t n, double length, const lica_col_props* props, lica_col_state* st,
@@ -1616,12 +1798,19 @@ int lica_gpu_column_steps(int32_t ncol, int32_t n, double length, const lica_col
     }
     const size_t st_off = total;
     total += (4 * nc + 255) & ~(size_t)255;
-    char* base = nullptr;
-    LICA_CUDA_TRY(cudaMalloc(&base, total));
-    struct Guard {
-        char* p;
-        ~Guard() { cudaFree(p); }
-    } guard{base};
+    // device copies in a grow-only buffer kept by the library (one host call at a time)
+    static std::mutex host_mu;
+    static char* host_buf = nullptr;
+    static size_t host_bytes = 0;
+    std::lock_guard<std::mutex> lk(host_mu);
+    if (total > host_bytes) {
+        if (host_buf) cudaFree(host_buf);
+        host_buf = nullptr;
+        host_bytes = 0;
+        LICA_CUDA_TRY(cudaMalloc(&host_buf, total));
+        host_bytes = total;
+    }
+    char* base = host_buf;
     for (int q = 0; q < nfld; ++q) LICA_CUDA_TRY(cudaMemcpy(base + off[q], f[q].h, f[q].bytes, cudaMemcpyHostToDevice));
     lica_col_state d;
     d.w = (double*)(base + off[0]);

@@ -74,6 +74,11 @@ SIGNATURES = {
     "lica_gpu_column_steps_device": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.POINTER(ColProps),
                                                C.POINTER(ColState), C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
                                                C.c_void_p]),
+    "lica_gpu_column_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, _I32, _D, C.POINTER(ColProps)]),
+    "lica_gpu_column_batch_destroy": (C.c_int, [C.c_void_p]),
+    "lica_gpu_column_batch_layout": (C.c_int, [C.c_void_p, _I64, _I64]),
+    "lica_gpu_column_batch_steps_device": (C.c_int, [C.c_void_p, C.POINTER(ColState), C.c_int32, C.c_int32,
+                                                     C.c_void_p, C.c_void_p, C.c_void_p]),
     "lica_gpu_column_steps": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.POINTER(ColProps), C.POINTER(ColState),
                                         C.c_int32, _I32]),
 }

@@ -29,3 +29,19 @@ def test_init_rejects_film_in_first_cell():
     from lica_boiling1d_b200.column import ColumnProps, Columns
     with pytest.raises(native.LicaError):
         Columns.film(64, 1.0, [0.003], ColumnProps())
+
+
+def test_uneven_batch_layout_and_init():
+    """Packed layout of a batch of uneven columns and each column's initial state against
+    the oracle (host code, no GPU)."""
+    from lica_boiling1d_b200.column import ColumnBatch, uneven_batch
+    n, length, z0, props = uneven_batch(7, seed=11, nmin=16, nmax=300)
+    b = ColumnBatch.films(n, length, z0, props)
+    assert b.totals[0] == int((n + 2).sum()) and b.totals[1] == int((2 * n + 7).sum())
+    assert b.totals[2] == int((2 * n + 2).sum())
+    for c in range(len(n)):
+        ref = O.col_init(int(n[c]), float(length[c]), float(z0[c]), props[c])
+        got = b.column(c)
+        for k, v in ref.items():
+            if k != "stats":
+                assert np.array_equal(got[k], v), (c, k)

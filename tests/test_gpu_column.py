@@ -81,3 +81,23 @@ def test_host_path_matches_device_path():
     back = dev.to(None)
     for k in host.arrays:
         assert np.array_equal(host.arrays[k], back.arrays[k]), k
+
+
+def test_uneven_batch():
+    """Columns of different size, length and properties in one launch (longest first),
+    each checked against its own oracle run."""
+    import torch
+    from lica_boiling1d_b200.column import ColumnBatch, uneven_batch
+    n, length, z0, props = uneven_batch(6, seed=3, nmin=16, nmax=160)
+    dev = ColumnBatch.films(n, length, z0, props).to("cuda")
+    refs = [O.col_init(int(n[c]), float(length[c]), float(z0[c]), props[c]) for c in range(len(n))]
+    for call in range(2):
+        status = dev.steps(2, threads=64)
+        torch.cuda.synchronize()
+        assert int(status.abs().max()) == 0
+        for c, r in enumerate(refs):
+            for _ in range(2):
+                assert O.col_step(r, int(n[c]), float(length[c]), props[c]) == 0
+            got = dev.column(c)
+            for k, v in r.items():
+                assert np.array_equal(got[k], v), (call, c, k)
