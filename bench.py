@@ -198,6 +198,27 @@ def rk3_cpu(max_seconds=12.0):
             "batch_sample": f"{len(sample)} of the {C4_NCOL} columns x 2 steps on {cores} threads"}
 
 
+def profile_batch(ncol, steps, threads):
+    """Only the uneven batch: one warm-up launch of one step, then one launch of `steps`
+    steps (for ncu: the second k_column_steps launch is the measured one)."""
+    import torch
+
+    from lica_boiling1d_b200.column import ColumnBatch, uneven_batch
+    torch.cuda.set_device(0)
+    n, length, z0, bprops = uneven_batch(ncol, seed=0)
+    batch = ColumnBatch.films(n, length, z0, bprops).to("cuda")
+    batch.steps(1, threads=threads)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    st = batch.steps(steps, threads=threads)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    print(json.dumps({"profile_batch": ncol, "steps": steps, "threads": threads, "ms_per_step": ms / steps,
+                      "cells": int(n.sum()), "status": int(st.max())}), flush=True)
+
+
 def rk3_legs(dev, flush, steps_c1=200, steps_c4=20, warmup=3):
     import torch
 
@@ -365,6 +386,12 @@ def run_ours(args):
     value = world * args.steps / (total_ms / 1e3)
 
     e2e, roofline, variants, cpu = None, None, {}, None
+    rk3 = None
+    if not args.skip_rk3:
+        rk3 = rk3_legs(dev, flush, steps_c1=args.c1_steps, steps_c4=args.c4_steps)
+        if rank == 0 and world == 1 and not args.skip_cpu:
+            rk3["cpu_baseline"] = rk3_cpu()
+            rk3["cpu_baseline"]["kind"] = "port"
     if args.no_e2e:
         return finish(args, locals())
     # end-to-end through the host C-ABI entry: H2D of p0, f, bx, by; solve; D2H of p
@@ -445,12 +472,6 @@ def run_ours(args):
         cpu = {"value": len(times) / sum(times), "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{len(times)} complete solves of the same workload (~15 s), FP64 C++/OpenMP restatement"}
 
-    rk3 = None
-    if not args.skip_rk3:
-        rk3 = rk3_legs(dev, flush)
-        if rank == 0 and world == 1 and not args.skip_cpu:
-            rk3["cpu_baseline"] = rk3_cpu()
-            rk3["cpu_baseline"]["kind"] = "port"
     return finish(args, locals())
 
 
@@ -493,12 +514,20 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end and later legs (profiling runs)")
     ap.add_argument("--no-profile", action="store_true", help="skip the kernel-class timing and later legs")
     ap.add_argument("--skip-rk3", action="store_true", help="skip the RK3 column legs")
+    ap.add_argument("--c1-steps", type=int, default=200, help="timed steps of the 512-cell column")
+    ap.add_argument("--c4-steps", type=int, default=20, help="timed steps of the 4096-column batch")
+    ap.add_argument("--profile-batch", type=int, default=0,
+                    help="only run NCOL columns of the uneven batch (profiling runs); see --c4-steps, --threads")
+    ap.add_argument("--threads", type=int, default=64, help="column CTA width for --profile-batch")
     ap.add_argument("--no-graph", action="store_true",
                     help="launch kernels one by one instead of one CUDA graph per solve (for ncu, which cannot "
                          "profile kernels of a graph with a conditional node)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.profile_batch:
+        profile_batch(args.profile_batch, args.c4_steps, args.threads)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
