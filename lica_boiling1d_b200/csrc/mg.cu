@@ -44,7 +44,6 @@ namespace mg {
 constexpr int TX = 32;
 constexpr int TY = 32;
 constexpr int NT = 256;          // threads of a CG / set-up grid-kernel CTA
-constexpr int NTG = 512;         // threads of a smoothing grid-kernel CTA (two resident per SM)
 constexpr int NT_CTA = 1024;     // threads of the single-CTA coarse kernel
 constexpr int kMaxLevels = 16;
 constexpr int kSmallCells = 256; // levels with <= this many cells run in warp 0 alone
@@ -83,177 +82,228 @@ struct V2<float> {
     using type = float2;
 };
 
-// Asynchronous global->shared copy of one element (cp.async, 4 or 8 bytes), reading
-// nothing and writing zero when valid is false.
-template <typename T>
-__device__ __forceinline__ void async_copy(T* dst, const T* src, bool valid) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    const int n = valid ? (int)sizeof(T) : 0;
-    if (sizeof(T) == 8)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
-}
-
 __device__ __forceinline__ void async_wait_all() {
     asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
-// Issues the copies of rows [gj0, gj0+RY) x columns [gi0, gi0+RX) of a row-major array
-// (nx columns, nrows rows, x periodic) into the colour-split arrays X0 (red) and X1
-// (black), each RY x RX/2: cell (sx, sy) has colour c = (sx + sy + gj0) & 1 and sits in
-// X_c at [sy][sx >> 1].  Rows outside [0, nrows) read as zero.  gi0 and nx are even, so
-// the pair of cells (2m, 2m+1) wraps as a pair.  Completion: async_wait_all + barrier.
-template <typename T, int RX, int RY>
-__device__ __forceinline__ void load_split(T* __restrict__ X0, T* __restrict__ X1, const T* __restrict__ g, int nx,
-                                           int nrows, int gi0, int gj0) {
-    constexpr int RXh = RX / 2;
-    for (int k = threadIdx.x; k < RY * RXh; k += blockDim.x) {
-        const int sy = k / RXh, m = k - sy * RXh;
-        const int j = gj0 + sy;
-        int i = gi0 + 2 * m;
-        if (i < 0) i += nx; else if (i >= nx) i -= nx;
-        const bool ok = (j >= 0 && j < nrows);
-        const T* src = ok ? g + (size_t)j * nx + i : g;
-        const int odd = (sy + gj0) & 1;
-        async_copy(odd ? X1 + k : X0 + k, src, ok);
-        async_copy(odd ? X0 + k : X1 + k, src + 1, ok);
-    }
-}
-
-// Stencil sums of the colour-c cell at compact position idx = sy*RXh + m, o = (c+sy+gj0)&1:
-// neighbours and the east/north faces live in the other colour's arrays (see load_split).
-template <typename T, int RXh>
-__device__ __forceinline__ void split_sums(const T* __restrict__ uO, const T* __restrict__ axC,
-                                           const T* __restrict__ axO, const T* __restrict__ ayC,
-                                           const T* __restrict__ ayO, int idx, int o, T& s, T& d) {
-    const T aw = axC[idx], ae = axO[idx + o], as = ayC[idx], an = ayO[idx + RXh];
-    const T uw = uO[idx + o - 1], ue = uO[idx + o], us = uO[idx - RXh], un = uO[idx + RXh];
-    T ss = aw * uw;
-    ss += ae * ue;
-    ss += as * us;
-    ss += an * un;
-    T dd = aw;
-    dd += ae;
-    dd += as;
-    dd += an;
-    s = ss;
-    d = dd;
-}
-
-// Colour-c half-sweep over the cells (sx, sy) of the ring-d interior, sx in [d, RX-d),
-// sy in [d, RY-d), whose global row lies in [0, ny): u = (s - f) * dinv.
-template <typename T, int RX, int RY>
-__device__ __forceinline__ void split_half_sweep(T* __restrict__ u0, T* __restrict__ u1, const T* __restrict__ f0,
-                                                 const T* __restrict__ f1, const T* __restrict__ ax0,
-                                                 const T* __restrict__ ax1, const T* __restrict__ ay0,
-                                                 const T* __restrict__ ay1, const T* __restrict__ di0,
-                                                 const T* __restrict__ di1, int c, int dring, int gj0, int ny) {
-    const int lo = dring, hi = RX - dring, hiy = RY - dring;
-    constexpr int RXh = RX / 2;
-    T* uC = c ? u1 : u0;
-    const T* uO = c ? u0 : u1;
-    const T* fC = c ? f1 : f0;
-    const T* dC = c ? di1 : di0;
-    const T* axC = c ? ax1 : ax0;
-    const T* axO = c ? ax0 : ax1;
-    const T* ayC = c ? ay1 : ay0;
-    const T* ayO = c ? ay0 : ay1;
-    const int rows = hiy - lo;
-    for (int k = threadIdx.x; k < rows * RXh; k += blockDim.x) {
-        const int r = k / RXh, m = k - r * RXh;
-        const int sy = lo + r;
-        const int o = (c + sy + gj0) & 1;
-        const int sx = 2 * m + o;
-        const int j = gj0 + sy;
-        if (sx < lo || sx >= hi || j < 0 || j >= ny) continue;
-        const int idx = sy * RXh + m;
-        const T aw = axC[idx], ae = axO[idx + o], as = ayC[idx], an = ayO[idx + RXh];
-        const T uw = uO[idx + o - 1], ue = uO[idx + o], us = uO[idx - RXh], un = uO[idx + RXh];
-        T sm = aw * uw;
-        sm += ae * ue;
-        sm += as * us;
-        sm += an * un;
-        uC[idx] = (sm - fC[idx]) * dC[idx];
-    }
-}
-
-// Residual f - A u of the cell (sx, sy) (inside the region's inner ring).
-template <typename T, int RXh>
-__device__ __forceinline__ T split_residual(const T* u0, const T* u1, const T* f0, const T* f1, const T* ax0,
-                                            const T* ax1, const T* ay0, const T* ay1, int sx, int sy, int gj0) {
-    const int c = (sx + sy + gj0) & 1, o = (c + sy + gj0) & 1;
-    const int idx = sy * RXh + (sx >> 1);
-    T sm, d;
-    split_sums<T, RXh>(c ? u0 : u1, c ? ax1 : ax0, c ? ax0 : ax1, c ? ay1 : ay0, c ? ay0 : ay1, idx, o, sm, d);
-    return (c ? f1 : f0)[idx] - (sm - d * (c ? u1 : u0)[idx]);
-}
-
-template <typename T, int NSW, int TXX, int TYY, bool DOWN>
-struct GridCfg {
-    static constexpr int HMIN = DOWN ? 2 * NSW + 1 : 2 * NSW;
-    static constexpr int H = (HMIN + 1) & ~1;  // even, for aligned vector loads
-    static constexpr int RX = TXX + 2 * H, RY = TYY + 2 * H, RXh = RX / 2;
-    static constexpr int ARR = RY * RXh;        // one colour of one array
-    static constexpr size_t SMEM = sizeof(T) * 10 * ARR;  // u, f, ax, ay, dinv x two colours
+// ------------------------------------------------------------------------------------
+// Register-blocked red-black smoothing kernels (k_down, k_up).
+//
+// A CTA owns a TXX x TYY tile of one level plus a halo of H = 2*nsw cells and runs every
+// half-sweep of one visit inside that region (temporal blocking: the valid part shrinks
+// by one ring per half-sweep and one more for the residual; k_down's first half-sweep
+// starts from zero and needs no neighbour), so a visit reads f and the weights once.
+//
+// Thread t owns column x = t % RXP of the region (threads with x >= RX idle) and rows
+// [s*R, s*R + R) of strip s = t / RXP.  Its cells are held in colour order: A[k] is the red cell of row pair k
+// (row 2k + p with p = x & 1) and B[k] the black one (row 2k + 1 - p).  Their weights,
+// f and 1/d stay in registers for the whole visit; only u goes through shared memory, so
+// an update is four shared loads at fixed offsets, the oracle's nine FP64 operations and
+// one shared store.
+//
+// Shared layout of u: word(s, r, x) = PAD + s*SSTR + r*RXP + x, RXP = 8 (mod 16) and
+// SSTR = R*RXP + 8.  Lanes sit on consecutive x; in every access of a sweep (own cell,
+// west, east, south, north, also across a strip boundary) the 16 lanes of a half-warp
+// then touch 16 distinct 8-byte bank pairs.
+// ------------------------------------------------------------------------------------
+template <int NSW, int TXX, int TYY, int R>
+struct RBCfg {
+    static constexpr int H = 2 * NSW;
+    static constexpr int RX = TXX + 2 * H;
+    static constexpr int RXP = RX + ((8 - RX % 16) + 16) % 16;
+    static constexpr int RY = ((TYY + 2 * H + R - 1) / R) * R;
+    static constexpr int NS = RY / R;
+    static constexpr int NUSED = RXP * NS;  // threads mapped over the padded pitch
+    static constexpr int NTH = (NUSED + 31) / 32 * 32;
+    static constexpr int SSTR = R * RXP + 8;
+    static constexpr int PAD = RXP + 16;
+    static constexpr int WORDS = PAD + NS * SSTR + RXP + 16;
+    static constexpr int K = R / 2;
+    static_assert(R % 2 == 0 && TXX % 16 == 0 && TYY % 2 == 0, "tile shape");
+    static_assert(RXP % 16 == 8 && SSTR % 16 == 8, "bank layout");
 };
 
+// The cells of one thread: colour c (0 red = A, 1 black = B), pair k.
+template <typename T, int K>
+struct RBCells {
+    T f[2][K], di[2][K], aw[2][K], ae[2][K], as[2][K], an[2][K];
+    unsigned valid;  // bit c*K + k: the cell lies inside the domain (rows 0..ny-1)
+    unsigned sweep;  // valid, and not in the region's edge columns x = 0, RX-1
+};
+
+template <class C>
+struct RBGeom {
+    int x, s, p;
+    bool used;
+    int base[2];  // word of A[0] and B[0]
+    int soff[2];  // south offset of A[0], B[0] (a strip boundary adds the 8-word skew)
+    int noff[2];  // north offset of A[K-1], B[K-1]
+    __device__ __forceinline__ RBGeom() {
+        const int t = threadIdx.x;
+        s = t / C::RXP;
+        x = t - s * C::RXP;
+        used = t < C::NUSED && x < C::RX;
+        if (!used) s = x = 0;
+        p = x & 1;
+        base[0] = C::PAD + s * C::SSTR + p * C::RXP + x;
+        base[1] = C::PAD + s * C::SSTR + (1 - p) * C::RXP + x;
+        soff[0] = -C::RXP - 8 * (1 - p);
+        soff[1] = -C::RXP - 8 * p;
+        noff[0] = C::RXP + 8 * p;
+        noff[1] = C::RXP + 8 * (1 - p);
+    }
+    // region row of cell (c, k)
+    __device__ __forceinline__ int row(int c, int k) const { return s * (C::K * 2) + 2 * k + (c ? 1 - p : p); }
+};
+
+// Loads f, 1/d and the four weights of the thread's cells (zero outside the domain rows).
+template <typename T, class C>
+__device__ __forceinline__ void rb_load(RBCells<T, C::K>& cl, const RBGeom<C>& g, const T* __restrict__ f,
+                                        const T* __restrict__ ax, const T* __restrict__ ay,
+                                        const T* __restrict__ dinv, int nx, int ny, int gi0, int gj0) {
+    int i = gi0 + g.x;
+    if (i < 0) i += nx; else if (i >= nx) i -= nx;
+    const int ip = (i + 1 == nx) ? 0 : i + 1;
+    cl.valid = 0u;
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+#pragma unroll
+        for (int k = 0; k < C::K; ++k) {
+            const int j = gj0 + g.row(c, k);
+            const bool ok = g.used && j >= 0 && j < ny;
+            T vf = T(0), vd = T(0), vw = T(0), ve = T(0), vs = T(0), vn = T(0);
+            if (ok) {
+                const int o = j * nx;
+                vf = f[o + i];
+                vd = dinv[o + i];
+                vw = ax[o + i];
+                ve = ax[o + ip];
+                vs = ay[o + i];
+                vn = ay[o + nx + i];
+            }
+            cl.f[c][k] = vf;
+            cl.di[c][k] = vd;
+            cl.aw[c][k] = vw;
+            cl.ae[c][k] = ve;
+            cl.as[c][k] = vs;
+            cl.an[c][k] = vn;
+            cl.valid |= (ok ? 1u : 0u) << (c * C::K + k);
+        }
+    }
+    // The west read of column 0 (east read of column RX-1) lands on the previous (next)
+    // row's far column, a cell of the same colour: the edge columns, outside the valid
+    // part after their first neighbour-dependent update, are never swept.
+    cl.sweep = (g.x >= 1 && g.x < C::RX - 1) ? cl.valid : 0u;
+}
+
+// Stencil sum of cell (c, k) in the oracle's order: s = aw*uw + ae*ue + as*us + an*un.
+template <typename T, class C>
+__device__ __forceinline__ T rb_sum(const RBCells<T, C::K>& cl, const RBGeom<C>& g, const T* __restrict__ pc, int c,
+                                    int k) {
+    const T uw = pc[-1], ue = pc[1];
+    const T us = (k == 0) ? pc[g.soff[c]] : pc[-C::RXP];
+    const T un = (k == C::K - 1) ? pc[g.noff[c]] : pc[C::RXP];
+    T ss = cl.aw[c][k] * uw;
+    ss += cl.ae[c][k] * ue;
+    ss += cl.as[c][k] * us;
+    ss += cl.an[c][k] * un;
+    return ss;
+}
+
+// One half-sweep of colour c over the thread's cells: u = (s - f) * (1/d).
+template <typename T, class C, int c>
+__device__ __forceinline__ void rb_half_sweep(const RBCells<T, C::K>& cl, const RBGeom<C>& g, T* __restrict__ su) {
+#pragma unroll
+    for (int k = 0; k < C::K; ++k) {
+        if (cl.sweep & (1u << (c * C::K + k))) {
+            T* pc = su + g.base[c] + 2 * k * C::RXP;
+            const T ss = rb_sum<T, C>(cl, g, pc, c, k);
+            pc[0] = (ss - cl.f[c][k]) * cl.di[c][k];
+        }
+    }
+}
+
+// The first red half-sweep from a zero iterate: every neighbour is zero and every weight
+// is >= 0, so the oracle's sum is +0 and u = (0 - f) * (1/d) exactly, on every cell of
+// the region (no neighbour read, so the edge columns are valid too).
+template <typename T, class C>
+__device__ __forceinline__ void rb_first_red(const RBCells<T, C::K>& cl, const RBGeom<C>& g, T* __restrict__ su) {
+#pragma unroll
+    for (int k = 0; k < C::K; ++k) {
+        if (cl.valid & (1u << k)) su[g.base[0] + 2 * k * C::RXP] = (T(0) - cl.f[0][k]) * cl.di[0][k];
+    }
+}
+
+// Residual f - (s - d*u) of cell (c, k), d = ((aw + ae) + as) + an as in the oracle.
+template <typename T, class C>
+__device__ __forceinline__ T rb_residual(const RBCells<T, C::K>& cl, const RBGeom<C>& g, const T* __restrict__ su,
+                                         int c, int k, T& u) {
+    const T* pc = su + g.base[c] + 2 * k * C::RXP;
+    const T ss = rb_sum<T, C>(cl, g, pc, c, k);
+    T d = cl.aw[c][k];
+    d += cl.ae[c][k];
+    d += cl.as[c][k];
+    d += cl.an[c][k];
+    u = pc[0];
+    return cl.f[c][k] - (ss - d * u);
+}
+
+template <typename T, class C>
+__device__ __forceinline__ void rb_zero(T* __restrict__ su) {
+    for (int k = threadIdx.x; k < C::WORDS; k += C::NTH) su[k] = T(0);
+}
+
 // ------------------------------------------------------------------------------------
-// k_down: nu1 red-black sweeps from a zero iterate, residual, 2x2 restriction.
+// k_down: nu1 red-black sweeps from a zero iterate, the residual and its 2x2 restriction
+// (fc = (r00 + r10 + r01 + r11) / 4 in the oracle's order; the east partner of an even
+// column is the neighbouring lane).
 // ------------------------------------------------------------------------------------
-template <typename T, int NSW, int TXX, int TYY>
-__global__ void __launch_bounds__(NTG, 2) k_down(const T* __restrict__ f, const T* __restrict__ ax,
-                                                 const T* __restrict__ ay, const T* __restrict__ dinv,
-                                                 T* __restrict__ u_out, T* __restrict__ fc_out, int nx, int ny) {
-    using C = GridCfg<T, NSW, TXX, TYY, true>;
-    constexpr int H = C::H, RX = C::RX, RY = C::RY, RXh = C::RXh, ARR = C::ARR, SKIP = C::H - C::HMIN;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* sm = reinterpret_cast<T*>(smem_raw);
-    T* const u0 = sm;
-    T* const u1 = sm + ARR;
-    T* const f0 = sm + 2 * ARR;
-    T* const f1 = sm + 3 * ARR;
-    T* const ax0 = sm + 4 * ARR;
-    T* const ax1 = sm + 5 * ARR;
-    T* const ay0 = sm + 6 * ARR;
-    T* const ay1 = sm + 7 * ARR;
-    T* const di0 = sm + 8 * ARR;
-    T* const di1 = sm + 9 * ARR;
-    const int gi0 = blockIdx.x * TXX - H, gj0 = blockIdx.y * TYY - H;
-    load_split<T, RX, RY>(f0, f1, f, nx, ny, gi0, gj0);
-    load_split<T, RX, RY>(ax0, ax1, ax, nx, ny, gi0, gj0);
-    load_split<T, RX, RY>(ay0, ay1, ay, nx, ny + 1, gi0, gj0);
-    load_split<T, RX, RY>(di0, di1, dinv, nx, ny, gi0, gj0);
-    for (int k = threadIdx.x; k < 2 * ARR; k += blockDim.x) sm[k] = T(0);
-    async_wait_all();
+template <typename T, int NSW, int TXX, int TYY, int R>
+__global__ void __launch_bounds__(RBCfg<NSW, TXX, TYY, R>::NTH, 2)
+    k_down(const T* __restrict__ f, const T* __restrict__ ax, const T* __restrict__ ay, const T* __restrict__ dinv,
+           T* __restrict__ u_out, T* __restrict__ fc_out, int nx, int ny) {
+    using C = RBCfg<NSW, TXX, TYY, R>;
+    __shared__ __align__(16) T su[C::WORDS];
+    const int gi0 = blockIdx.x * TXX - C::H, gj0 = blockIdx.y * TYY - C::H;
+    const RBGeom<C> g;
+    RBCells<T, C::K> cl;
+    rb_zero<T, C>(su);
+    rb_load<T, C>(cl, g, f, ax, ay, dinv, nx, ny, gi0, gj0);
+    __syncthreads();  // zero fill done
+    rb_first_red<T, C>(cl, g, su);
+    __syncthreads();
+    rb_half_sweep<T, C, 1>(cl, g, su);
     __syncthreads();
 #pragma unroll 1
-    for (int q = 0; q < 2 * NSW; ++q) {
-        split_half_sweep<T, RX, RY>(u0, u1, f0, f1, ax0, ax1, ay0, ay1, di0, di1, q & 1, SKIP + q + 1, gj0, ny);
+    for (int q = 1; q < NSW; ++q) {
+        rb_half_sweep<T, C, 0>(cl, g, su);
+        __syncthreads();
+        rb_half_sweep<T, C, 1>(cl, g, su);
         __syncthreads();
     }
-    using V = typename V2<T>::type;
-    // tile iterate, two cells per vector store
-    for (int k = threadIdx.x; k < TYY * (TXX / 2); k += blockDim.x) {
-        const int ty = k / (TXX / 2), t = k - ty * (TXX / 2);
-        const int sy = H + ty, idx = sy * RXh + H / 2 + t;
-        const int c0 = (sy + gj0) & 1;
-        V v;
-        v.x = (c0 ? u1 : u0)[idx];
-        v.y = (c0 ? u0 : u1)[idx];
-        *reinterpret_cast<V*>(u_out + (size_t)(blockIdx.y * TYY + ty) * nx + blockIdx.x * TXX + 2 * t) = v;
-    }
-    // residual of the 4 children of each coarse cell and their average
+    const bool col_in = g.used && g.x >= C::H && g.x < C::H + TXX;
+    const int ti = blockIdx.x * TXX + g.x - C::H;
     const int ncx = nx >> 1;
-    for (int k = threadIdx.x; k < (TXX / 2) * (TYY / 2); k += blockDim.x) {
-        const int cj = k / (TXX / 2), ci = k - cj * (TXX / 2);
-        const int sx = H + 2 * ci, sy = H + 2 * cj;
-        const T r00 = split_residual<T, RXh>(u0, u1, f0, f1, ax0, ax1, ay0, ay1, sx, sy, gj0);
-        const T r10 = split_residual<T, RXh>(u0, u1, f0, f1, ax0, ax1, ay0, ay1, sx + 1, sy, gj0);
-        const T r01 = split_residual<T, RXh>(u0, u1, f0, f1, ax0, ax1, ay0, ay1, sx, sy + 1, gj0);
-        const T r11 = split_residual<T, RXh>(u0, u1, f0, f1, ax0, ax1, ay0, ay1, sx + 1, sy + 1, gj0);
-        const T fcv = T(0.25) * ((r00 + r10) + (r01 + r11));
-        fc_out[(size_t)(blockIdx.y * (TYY / 2) + cj) * ncx + blockIdx.x * (TXX / 2) + ci] = fcv;
+#pragma unroll
+    for (int k = 0; k < C::K; ++k) {
+        T u0, u1;
+        const T r0 = rb_residual<T, C>(cl, g, su, 0, k, u0);
+        const T r1 = rb_residual<T, C>(cl, g, su, 1, k, u1);
+        // rows of the pair: 2k + p (A) and 2k + 1 - p (B); useful rows are [H, H + TYY)
+        const int y = g.s * R + 2 * k;
+        const bool row_in = col_in && y >= C::H && y < C::H + TYY;
+        if (row_in) {
+            const int tj = blockIdx.y * TYY + y - C::H;
+            u_out[(tj + g.p) * nx + ti] = u0;
+            u_out[(tj + 1 - g.p) * nx + ti] = u1;
+        }
+        // even column: A = row 2k, B = row 2k+1; its partner (odd column): A = row 2k+1, B = row 2k
+        const T oA = __shfl_xor_sync(0xffffffffu, r0, 1);
+        const T oB = __shfl_xor_sync(0xffffffffu, r1, 1);
+        if (row_in && g.p == 0) {
+            const T fcv = T(0.25) * ((r0 + oB) + (r1 + oA));
+            fc_out[((blockIdx.y * TYY + y - C::H) >> 1) * ncx + (ti >> 1)] = fcv;
+        }
     }
 }
 
@@ -262,76 +312,70 @@ __global__ void __launch_bounds__(NTG, 2) k_down(const T* __restrict__ f, const 
 // u_post (out of place: no block reads a tile another block has updated); at level 0
 // also the r.z partial (r = f of level 0, z = u) and, in the last block, beta.
 // ------------------------------------------------------------------------------------
-template <typename T, int NSW, int TXX, int TYY, bool LEVEL0>
-__global__ void __launch_bounds__(NTG, 2) k_up(const T* __restrict__ u_pre, T* __restrict__ u_post,
-                                               const T* __restrict__ uc, const T* __restrict__ f,
-                                               const T* __restrict__ ax, const T* __restrict__ ay,
-                                               const T* __restrict__ dinv, int nx, int ny, State* __restrict__ st,
-                                               double* __restrict__ partials) {
-    using C = GridCfg<T, NSW, TXX, TYY, false>;
-    constexpr int H = C::H, RX = C::RX, RY = C::RY, RXh = C::RXh, ARR = C::ARR, SKIP = C::H - C::HMIN;
-    using V = typename V2<T>::type;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+template <typename T, int NSW, int TXX, int TYY, int R, bool LEVEL0>
+__global__ void __launch_bounds__(RBCfg<NSW, TXX, TYY, R>::NTH, 2)
+    k_up(const T* __restrict__ u_pre, T* __restrict__ u_post, const T* __restrict__ uc, const T* __restrict__ f,
+         const T* __restrict__ ax, const T* __restrict__ ay, const T* __restrict__ dinv, int nx, int ny,
+         State* __restrict__ st, double* __restrict__ partials) {
+    using C = RBCfg<NSW, TXX, TYY, R>;
+    __shared__ __align__(16) T su[C::WORDS];
     __shared__ double red[32];
-    T* sm = reinterpret_cast<T*>(smem_raw);
-    T* const u0 = sm;
-    T* const u1 = sm + ARR;
-    T* const f0 = sm + 2 * ARR;
-    T* const f1 = sm + 3 * ARR;
-    T* const ax0 = sm + 4 * ARR;
-    T* const ax1 = sm + 5 * ARR;
-    T* const ay0 = sm + 6 * ARR;
-    T* const ay1 = sm + 7 * ARR;
-    T* const di0 = sm + 8 * ARR;
-    T* const di1 = sm + 9 * ARR;
-    const int gi0 = blockIdx.x * TXX - H, gj0 = blockIdx.y * TYY - H;
+    const int gi0 = blockIdx.x * TXX - C::H, gj0 = blockIdx.y * TYY - C::H;
     const int ncx = nx >> 1;
-    load_split<T, RX, RY>(f0, f1, f, nx, ny, gi0, gj0);
-    load_split<T, RX, RY>(ax0, ax1, ax, nx, ny, gi0, gj0);
-    load_split<T, RX, RY>(ay0, ay1, ay, nx, ny + 1, gi0, gj0);
-    load_split<T, RX, RY>(di0, di1, dinv, nx, ny, gi0, gj0);
-    for (int k = threadIdx.x; k < ARR; k += blockDim.x) {
-        const int sy = k / RXh, m = k - sy * RXh;
-        const int j = gj0 + sy;
-        int i = gi0 + 2 * m;
+    const RBGeom<C> g;
+    RBCells<T, C::K> cl;
+    rb_zero<T, C>(su);
+    rb_load<T, C>(cl, g, f, ax, ay, dinv, nx, ny, gi0, gj0);
+    T uv[2][C::K];
+    {
+        int i = gi0 + g.x;
         if (i < 0) i += nx; else if (i >= nx) i -= nx;
-        V v;
-        v.x = T(0);
-        v.y = T(0);
-        if (j >= 0 && j < ny) {
-            v = *reinterpret_cast<const V*>(u_pre + (size_t)j * nx + i);
-            const T e = uc[(size_t)(j >> 1) * ncx + (i >> 1)];
-            v.x += e;
-            v.y += e;
-        }
-        if ((sy + gj0) & 1) {
-            u1[k] = v.x;
-            u0[k] = v.y;
-        } else {
-            u0[k] = v.x;
-            u1[k] = v.y;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+#pragma unroll
+            for (int k = 0; k < C::K; ++k) {
+                T v = T(0);
+                if (cl.valid & (1u << (c * C::K + k))) {
+                    const int j = gj0 + g.row(c, k);
+                    v = u_pre[j * nx + i];
+                    v += uc[(j >> 1) * ncx + (i >> 1)];
+                }
+                uv[c][k] = v;
+            }
         }
     }
-    async_wait_all();
+    __syncthreads();  // zero fill done
+    if (g.used) {
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+#pragma unroll
+            for (int k = 0; k < C::K; ++k) su[g.base[c] + 2 * k * C::RXP] = uv[c][k];
+        }
+    }
     __syncthreads();
 #pragma unroll 1
-    for (int q = 0; q < 2 * NSW; ++q) {
-        split_half_sweep<T, RX, RY>(u0, u1, f0, f1, ax0, ax1, ay0, ay1, di0, di1, 1 - (q & 1), SKIP + q + 1, gj0,
-                                    ny);
+    for (int q = 0; q < NSW; ++q) {
+        rb_half_sweep<T, C, 1>(cl, g, su);
+        __syncthreads();
+        rb_half_sweep<T, C, 0>(cl, g, su);
         __syncthreads();
     }
+    const bool col_in = g.used && g.x >= C::H && g.x < C::H + TXX;
+    const int ti = blockIdx.x * TXX + g.x - C::H;
     double acc = 0.0;
-    for (int k = threadIdx.x; k < TYY * (TXX / 2); k += blockDim.x) {
-        const int ty = k / (TXX / 2), t = k - ty * (TXX / 2);
-        const int sy = H + ty, idx = sy * RXh + H / 2 + t;
-        const int c0 = (sy + gj0) & 1;
-        V v;
-        v.x = (c0 ? u1 : u0)[idx];
-        v.y = (c0 ? u0 : u1)[idx];
-        *reinterpret_cast<V*>(u_post + (size_t)(blockIdx.y * TYY + ty) * nx + blockIdx.x * TXX + 2 * t) = v;
-        if (LEVEL0) {
-            acc += double((c0 ? f1 : f0)[idx]) * double(v.x);
-            acc += double((c0 ? f0 : f1)[idx]) * double(v.y);
+#pragma unroll
+    for (int k = 0; k < C::K; ++k) {
+        const int y = g.s * R + 2 * k;
+        if (col_in && y >= C::H && y < C::H + TYY) {
+            const int tj = blockIdx.y * TYY + y - C::H;
+            const T u0 = su[g.base[0] + 2 * k * C::RXP];
+            const T u1 = su[g.base[1] + 2 * k * C::RXP];
+            u_post[(tj + g.p) * nx + ti] = u0;
+            u_post[(tj + 1 - g.p) * nx + ti] = u1;
+            if (LEVEL0) {
+                acc += double(cl.f[0][k]) * double(u0);
+                acc += double(cl.f[1][k]) * double(u1);
+            }
         }
     }
     if (LEVEL0) {
@@ -964,7 +1008,6 @@ struct LevelBuf {
     float* ax32 = nullptr;
     float* ay32 = nullptr;
     float* di32 = nullptr;
-    bool big = false;        // grid kernels on 64x32 tiles (else 32x32)
 };
 
 struct lica_mg {
@@ -1063,39 +1106,25 @@ const T* lvl_di(const LevelBuf& L) {
     return std::is_same<T, float>::value ? (const T*)L.di32 : (const T*)L.di64;
 }
 
-template <typename T, int NS, int TXX, int TYY>
-int set_attrs_tile() {
-    LICA_CUDA_TRY(cudaFuncSetAttribute(k_down<T, NS, TXX, TYY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)GridCfg<T, NS, TXX, TYY, true>::SMEM));
-    LICA_CUDA_TRY(cudaFuncSetAttribute(k_up<T, NS, TXX, TYY, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)GridCfg<T, NS, TXX, TYY, false>::SMEM));
-    LICA_CUDA_TRY(cudaFuncSetAttribute(k_up<T, NS, TXX, TYY, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)GridCfg<T, NS, TXX, TYY, false>::SMEM));
-    return LICA_OK;
-}
+// Smoothing tiles: 32 x 32 cells on levels with at least one tile per SM, 16 x 16 below
+// (more CTAs in flight where the level is small and each tile's latency is the cost);
+// strips of 4 rows per thread.
+constexpr int RB_R = 4;
+constexpr int kSMs = 148;
+bool big_tiles(const LevelBuf& L) { return L.nx % 32 == 0 && L.ny % 32 == 0 && (L.nx / 32) * (L.ny / 32) >= kSMs; }
 
-template <typename T>
-int set_smem_attrs(int nsw) {
-    int st;
-    switch (nsw) {
-        case 1: if ((st = set_attrs_tile<T, 1, 32, 32>()) || (st = set_attrs_tile<T, 1, 64, 32>())) return st; break;
-        case 2: if ((st = set_attrs_tile<T, 2, 32, 32>()) || (st = set_attrs_tile<T, 2, 64, 32>())) return st; break;
-        default: if ((st = set_attrs_tile<T, 3, 32, 32>()) || (st = set_attrs_tile<T, 3, 64, 32>())) return st; break;
-    }
-    return LICA_OK;
-}
-
-template <typename T, int NS, int TXX, int TYY>
+template <typename T, int NS, int TS>
 void down_tile(const LevelBuf& L, const LevelBuf& C, cudaStream_t s) {
-    dim3 grid(L.nx / TXX, L.ny / TYY);
-    k_down<T, NS, TXX, TYY><<<grid, NTG, GridCfg<T, NS, TXX, TYY, true>::SMEM, s>>>(
-        (const T*)L.f, lvl_ax<T>(L), lvl_ay<T>(L), lvl_di<T>(L), (T*)L.u, (T*)C.f, L.nx, L.ny);
+    using Cfg = RBCfg<NS, TS, TS, RB_R>;
+    dim3 grid(L.nx / TS, L.ny / TS);
+    k_down<T, NS, TS, TS, RB_R><<<grid, Cfg::NTH, 0, s>>>((const T*)L.f, lvl_ax<T>(L), lvl_ay<T>(L), lvl_di<T>(L),
+                                                          (T*)L.u, (T*)C.f, L.nx, L.ny);
 }
 
 template <typename T, int NS>
 void down_ns(const LevelBuf& L, const LevelBuf& C, cudaStream_t s) {
-    if (L.big) down_tile<T, NS, 64, 32>(L, C, s);
-    else down_tile<T, NS, 32, 32>(L, C, s);
+    if (big_tiles(L)) down_tile<T, NS, 32>(L, C, s);
+    else down_tile<T, NS, 16>(L, C, s);
 }
 
 template <typename T>
@@ -1113,24 +1142,24 @@ int launch_down(lica_mg* m, int l, cudaStream_t s) {
     return LICA_OK;
 }
 
-template <typename T, int NS, int TXX, int TYY>
+template <typename T, int NS, int TS>
 void up_tile(lica_mg* m, const LevelBuf& L, const T* uc, bool level0, cudaStream_t s) {
-    dim3 grid(L.nx / TXX, L.ny / TYY);
-    const size_t sm = GridCfg<T, NS, TXX, TYY, false>::SMEM;
+    using Cfg = RBCfg<NS, TS, TS, RB_R>;
+    dim3 grid(L.nx / TS, L.ny / TS);
     if (level0)
-        k_up<T, NS, TXX, TYY, true><<<grid, NTG, sm, s>>>((const T*)L.u, (T*)L.up, uc, (const T*)L.f, lvl_ax<T>(L),
-                                                          lvl_ay<T>(L), lvl_di<T>(L), L.nx, L.ny, m->st,
-                                                          m->partials);
+        k_up<T, NS, TS, TS, RB_R, true><<<grid, Cfg::NTH, 0, s>>>((const T*)L.u, (T*)L.up, uc, (const T*)L.f,
+                                                                  lvl_ax<T>(L), lvl_ay<T>(L), lvl_di<T>(L), L.nx,
+                                                                  L.ny, m->st, m->partials);
     else
-        k_up<T, NS, TXX, TYY, false><<<grid, NTG, sm, s>>>((const T*)L.u, (T*)L.up, uc, (const T*)L.f, lvl_ax<T>(L),
-                                                           lvl_ay<T>(L), lvl_di<T>(L), L.nx, L.ny, m->st,
-                                                           m->partials);
+        k_up<T, NS, TS, TS, RB_R, false><<<grid, Cfg::NTH, 0, s>>>((const T*)L.u, (T*)L.up, uc, (const T*)L.f,
+                                                                   lvl_ax<T>(L), lvl_ay<T>(L), lvl_di<T>(L), L.nx,
+                                                                   L.ny, m->st, m->partials);
 }
 
 template <typename T, int NS>
 void up_ns(lica_mg* m, const LevelBuf& L, const T* uc, bool level0, cudaStream_t s) {
-    if (L.big) up_tile<T, NS, 64, 32>(m, L, uc, level0, s);
-    else up_tile<T, NS, 32, 32>(m, L, uc, level0, s);
+    if (big_tiles(L)) up_tile<T, NS, 32>(m, L, uc, level0, s);
+    else up_tile<T, NS, 16>(m, L, uc, level0, s);
 }
 
 template <typename T>
@@ -1479,7 +1508,7 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
     const bool mixed = o.precision == 1;
     const size_t tsz = mixed ? sizeof(float) : sizeof(double);
     // single-CTA levels: from the first level >= 1 whose remaining hierarchy fits in
-    // shared memory and has <= 64*64 cells, or that cannot be tiled
+    // shared memory and has <= 32*32 cells, or that cannot be tiled
     auto cta_bytes = [&](int from) {
         size_t b = 0;
         for (int l = from; l <= m->bottom; ++l) {
@@ -1494,9 +1523,9 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
     };
     int lcta = m->nouter - 1;
     for (int l = 1; l < m->nouter; ++l) {
-        const bool tileable = m->lv[l].nx % TX == 0 && m->lv[l].ny % TY == 0;
+        const bool tileable = m->lv[l].nx % 16 == 0 && m->lv[l].ny % 16 == 0;
         const size_t n = (size_t)m->lv[l].nx * m->lv[l].ny;
-        if (!tileable || (n <= 64 * 64 && cta_bytes(l) <= 226 * 1024)) { lcta = l; break; }
+        if (!tileable || (n <= 32 * 32 && cta_bytes(l) <= 226 * 1024)) { lcta = l; break; }
     }
     if (cta_bytes(lcta) > 227 * 1024) {
         delete m;
@@ -1505,13 +1534,9 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
         return LICA_BAD_ARG;
     }
     for (int l = 0; l < lcta; ++l) {
-        if (m->lv[l].nx % TX || m->lv[l].ny % TY) { delete m; return LICA_BAD_ARG; }
+        if (m->lv[l].nx % 16 || m->lv[l].ny % 16) { delete m; return LICA_BAD_ARG; }
     }
     m->lcta = lcta;
-    for (int l = 0; l < lcta; ++l) {
-        LevelBuf& L = m->lv[l];
-        L.big = false;  // 64x32 tiles need one SM each at FP64; 32x32 keeps two resident
-    }
     // shared-memory layout of the single-CTA kernel
     CtaParams& P = m->cp;
     std::memset(&P, 0, sizeof(P));
@@ -1580,7 +1605,7 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
             TRY_ALLOC(L.di32, sizeof(float) * n);
         }
     }
-    const size_t ntiles = (size_t)(nx / TX) * (ny / TY);
+    const size_t ntiles = (size_t)(nx / 16) * (ny / 16);  // the most blocks of any level-0 grid kernel
     TRY_ALLOC(m->partials, sizeof(double) * 2 * ntiles);
     TRY_ALLOC(m->st, sizeof(State));
     {
@@ -1588,9 +1613,6 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
         if (e != cudaSuccess) return fail(LICA_ERR_NOMEM);
     }
 #undef TRY_ALLOC
-    int st = mixed ? set_smem_attrs<float>(o.nu1) : set_smem_attrs<double>(o.nu1);
-    if (!st && o.nu2 != o.nu1) st = mixed ? set_smem_attrs<float>(o.nu2) : set_smem_attrs<double>(o.nu2);
-    if (st) return fail(st);
     {
         cudaError_t e1 = cudaFuncSetAttribute(k_xupdate<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)xupdate_smem());
