@@ -570,11 +570,20 @@ constexpr size_t xupdate_smem() { return sizeof(double) * 5 * PAREA; }
 // ------------------------------------------------------------------------------------
 // Single-CTA coarse part: outer levels [lcta, lc) in T, the coarsest outer level lc and
 // the inner levels in FP64, all in shared memory.
+//
+// Every level is stored colour-split: cell (i, j) of colour c = (i + j) & 1 sits in X_c at
+// [j * half + (i >> 1)], half = nx / 2, for X = u, f, ax (west faces), ay (south faces,
+// rows 0..ny) and 1/d.  A red (black) half-sweep then reads and writes consecutive words
+// across a warp, and the four children of coarse cell (I, J) are the entries I of rows
+// 2J and 2J+1 of both colours.  u has a zero ghost row below row 0 and above row ny-1,
+// so the wall neighbours need no branch.  Work items are walked with an incremental
+// (row, column) pair: no division per cell.
 // ------------------------------------------------------------------------------------
 struct CtaLevel {
-    int nx, ny;
-    unsigned off_u, off_f, off_ax, off_ay, off_di;  // byte offsets into dynamic smem
-    const void* gax;                                // AX, AY, DINV of this level (T or double)
+    int nx, ny, half;
+    unsigned mag_h, mag_nx;  // division multipliers for half and nx (t / c = umulhi(t, mag), c > 1)
+    unsigned off_u[2], off_f[2], off_ax[2], off_ay[2], off_di[2];  // byte offsets into dynamic smem
+    const void* gax;                                                // AX, AY, DINV of this level (T or double)
     const void* gay;
     const void* gdi;
 };
@@ -583,6 +592,7 @@ struct CtaParams {
     int lcta, lc, bottom;
     int nu1, nu2, ncoarse;
     unsigned off_dense, off_rhs;
+    const double* glu; // bottom-level elimination (multipliers below, U on and above the diagonal)
     const void* f_in;  // f of level lcta (T)
     void* u_out;       // u of level lcta (T)
     CtaLevel lv[kMaxLevels];
@@ -590,49 +600,97 @@ struct CtaParams {
 
 template <typename E>
 struct SL {
-    E* u;
-    E* f;
-    E* ax;
-    E* ay;
-    E* di;
-    int nx, ny;
+    E* u[2];  // row 0 of each colour; rows -1 and ny are zero ghosts
+    E* f[2];
+    E* ax[2];
+    E* ay[2];
+    E* di[2];
+    int nx, ny, h;
+    unsigned mag_h, mag_nx;
 };
 
 template <typename E>
 __device__ __forceinline__ SL<E> make_sl(const CtaParams& P, unsigned char* sm, int l) {
     const CtaLevel& L = P.lv[l];
     SL<E> s;
-    s.u = reinterpret_cast<E*>(sm + L.off_u);
-    s.f = reinterpret_cast<E*>(sm + L.off_f);
-    s.ax = reinterpret_cast<E*>(sm + L.off_ax);
-    s.ay = reinterpret_cast<E*>(sm + L.off_ay);
-    s.di = reinterpret_cast<E*>(sm + L.off_di);
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        s.u[c] = reinterpret_cast<E*>(sm + L.off_u[c]) + L.half;
+        s.f[c] = reinterpret_cast<E*>(sm + L.off_f[c]);
+        s.ax[c] = reinterpret_cast<E*>(sm + L.off_ax[c]);
+        s.ay[c] = reinterpret_cast<E*>(sm + L.off_ay[c]);
+        s.di[c] = reinterpret_cast<E*>(sm + L.off_di[c]);
+    }
     s.nx = L.nx;
     s.ny = L.ny;
+    s.h = L.half;
+    s.mag_h = L.mag_h;
+    s.mag_nx = L.mag_nx;
     return s;
 }
 
 template <bool W>
 __device__ __forceinline__ int g_tid() { return W ? (int)(threadIdx.x & 31) : (int)threadIdx.x; }
 template <bool W>
-__device__ __forceinline__ int g_nthr() { return W ? 32 : (int)blockDim.x; }
+__device__ __forceinline__ constexpr int g_nthr() { return W ? 32 : NT_CTA; }
 template <bool W>
 __device__ __forceinline__ void g_sync() {
     if (W) __syncwarp(); else __syncthreads();
 }
 
+// Items it = t, t + G, ... of a (rows x cols) range as an incremental (row, col) pair.
+__device__ __forceinline__ int div_mag(int t, int cols, unsigned mag) {
+    return cols == 1 ? t : (int)__umulhi((unsigned)t, mag);
+}
+struct ItemWalk {
+    int r, q, dr, dq, cols;
+    __device__ __forceinline__ ItemWalk(int t, int G, int cols_, unsigned mag) : cols(cols_) {
+        r = div_mag(t, cols, mag);
+        q = t - r * cols;
+        dr = div_mag(G, cols, mag);
+        dq = G - dr * cols;
+    }
+    __device__ __forceinline__ void next() {
+        r += dr;
+        q += dq;
+        if (q >= cols) { q -= cols; ++r; }
+    }
+};
+
+// X[c] for a colour c known only at run time, without indexing the pointer pair.
+template <typename P2>
+__device__ __forceinline__ auto pick(const P2& x, int c) -> decltype(x[0]) { return c ? x[1] : x[0]; }
+
+// The arrays one colour's update touches, selected once (no dynamic indexing of the
+// per-colour pointer pairs, which would put them in local memory).
 template <typename E>
-__device__ __forceinline__ void s_sums(const SL<E>& L, int i, int j, E& s, E& d) {
-    const int nx = L.nx, ny = L.ny;
-    const int ip = (i + 1 == nx) ? 0 : i + 1;
-    const int im = (i == 0) ? nx - 1 : i - 1;
-    const E aw = L.ax[j * nx + i];
-    const E ae = L.ax[j * nx + ip];
-    const E as = L.ay[j * nx + i];
-    const E an = L.ay[(j + 1) * nx + i];
-    const E uw = L.u[j * nx + im], ue = L.u[j * nx + ip];
-    const E us = (j > 0) ? L.u[(j - 1) * nx + i] : E(0);
-    const E un = (j < ny - 1) ? L.u[(j + 1) * nx + i] : E(0);
+struct Colour {
+    E* uc;
+    const E *uo, *axc, *axo, *ayc, *ayo, *fc, *dc;
+    int c, h;
+    __device__ __forceinline__ Colour(const SL<E>& L, int c_) : c(c_), h(L.h) {
+        const bool b = c_ != 0;
+        uc = b ? L.u[1] : L.u[0];
+        uo = b ? L.u[0] : L.u[1];
+        axc = b ? L.ax[1] : L.ax[0];
+        axo = b ? L.ax[0] : L.ax[1];
+        ayc = b ? L.ay[1] : L.ay[0];
+        ayo = b ? L.ay[0] : L.ay[1];
+        fc = b ? L.f[1] : L.f[0];
+        dc = b ? L.di[1] : L.di[0];
+    }
+};
+
+// Stencil sums of the colour-c cell (i = 2m + o, j), o = (j + c) & 1, in the oracle's
+// order: s = aw*uw + ae*ue + as*us + an*un and d = aw + ae + as + an.  k is its index.
+template <typename E>
+__device__ __forceinline__ void split_sums(const Colour<E>& V, int j, int m, int k, E& s, E& d) {
+    const int h = V.h, o = (j + V.c) & 1;
+    int w = m - 1 + o, e = m + o;
+    if (w < 0) w += h;
+    if (e >= h) e -= h;
+    const E aw = V.axc[k], ae = V.axo[j * h + e], as = V.ayc[k], an = V.ayo[k + h];
+    const E uw = V.uo[j * h + w], ue = V.uo[j * h + e], us = V.uo[k - h], un = V.uo[k + h];
     E ss = aw * uw;
     ss += ae * ue;
     ss += as * us;
@@ -647,96 +705,103 @@ __device__ __forceinline__ void s_sums(const SL<E>& L, int i, int j, E& s, E& d)
 
 template <typename E, bool W>
 __device__ void s_sweeps(const SL<E>& L, int nsw, bool reverse) {
-    const int half = L.nx >> 1, total = half * L.ny;
+    const int items = L.ny * L.h;
     for (int q = 0; q < 2 * nsw; ++q) {
-        const int colour = reverse ? 1 - (q & 1) : (q & 1);
-        for (int k = g_tid<W>(); k < total; k += g_nthr<W>()) {
-            const int j = k / half, m = k - j * half;
-            const int i = 2 * m + ((j + colour) & 1);
+        const Colour<E> V(L, reverse ? 1 - (q & 1) : (q & 1));
+        ItemWalk wk(g_tid<W>(), g_nthr<W>(), L.h, L.mag_h);
+#pragma unroll 2
+        for (int it = g_tid<W>(); it < items; it += g_nthr<W>()) {
+            const int k = wk.r * L.h + wk.q;
             E s, d;
-            s_sums(L, i, j, s, d);
-            L.u[j * L.nx + i] = (s - L.f[j * L.nx + i]) * L.di[j * L.nx + i];
+            split_sums(V, wk.r, wk.q, k, s, d);
+            V.uc[k] = (s - V.fc[k]) * V.dc[k];
+            wk.next();
         }
         g_sync<W>();
     }
 }
 
+// Residual of the colour-c cell at (j, m), index k: f - (s - d*u).
+template <typename E>
+__device__ __forceinline__ E split_res(const Colour<E>& V, int j, int m) {
+    const int k = j * V.h + m;
+    E s, d;
+    split_sums(V, j, m, k, s, d);
+    return V.fc[k] - (s - d * V.uc[k]);
+}
+
+// fc(I, J) = 0.25*((r00 + r10) + (r01 + r11)) of the residual, and uc = 0.
 template <typename E, typename EC, bool W>
 __device__ void s_restrict(const SL<E>& F, const SL<EC>& C) {
-    const int total = C.nx * C.ny;
-    for (int k = g_tid<W>(); k < total; k += g_nthr<W>()) {
-        const int J = k / C.nx, I = k - J * C.nx;
-        E r[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int i = 2 * I + (q & 1), j = 2 * J + (q >> 1);
-            E s, d;
-            s_sums(F, i, j, s, d);
-            r[q] = F.f[j * F.nx + i] - (s - d * F.u[j * F.nx + i]);
-        }
-        const E fc = E(0.25) * ((r[0] + r[1]) + (r[2] + r[3]));
-        C.f[k] = EC(fc);
-        C.u[k] = EC(0);
+    const int items = C.nx * C.ny;
+    const Colour<E> R(F, 0), B(F, 1);
+    ItemWalk wk(g_tid<W>(), g_nthr<W>(), C.nx, C.mag_nx);
+#pragma unroll 2
+    for (int it = g_tid<W>(); it < items; it += g_nthr<W>()) {
+        const int J = wk.r, I = wk.q;
+        const E r00 = split_res(R, 2 * J, I);
+        const E r10 = split_res(B, 2 * J, I);
+        const E r01 = split_res(B, 2 * J + 1, I);
+        const E r11 = split_res(R, 2 * J + 1, I);
+        const E fc = E(0.25) * ((r00 + r10) + (r01 + r11));
+        const int cc = (I + J) & 1, kc = J * C.h + (I >> 1);
+        pick(C.f, cc)[kc] = EC(fc);
+        pick(C.u, cc)[kc] = EC(0);
+        wk.next();
     }
     g_sync<W>();
 }
 
+// u += P uc (piecewise constant): the four children of coarse cell (I, J).
 template <typename E, typename EC, bool W>
 __device__ void s_prolong(const SL<EC>& C, const SL<E>& F) {
-    const int total = F.nx * F.ny;
-    for (int k = g_tid<W>(); k < total; k += g_nthr<W>()) {
-        const int j = k / F.nx, i = k - j * F.nx;
-        F.u[k] += E(C.u[(j >> 1) * C.nx + (i >> 1)]);
+    const int items = C.nx * C.ny;
+    ItemWalk wk(g_tid<W>(), g_nthr<W>(), C.nx, C.mag_nx);
+#pragma unroll 2
+    for (int it = g_tid<W>(); it < items; it += g_nthr<W>()) {
+        const int J = wk.r, I = wk.q;
+        const E e = E(pick(C.u, (I + J) & 1)[J * C.h + (I >> 1)]);
+        const int k0 = 2 * J * F.h + I, k1 = k0 + F.h;
+        F.u[0][k0] += e;
+        F.u[1][k0] += e;
+        F.u[0][k1] += e;
+        F.u[1][k1] += e;
+        wk.next();
     }
     g_sync<W>();
 }
 
-// Dense Gaussian elimination of the bottom level (same order as the oracle).
+// Plain-index accessors of a colour-split level (the dense solve's assembly).
+template <typename E>
+__device__ __forceinline__ int split_index(const SL<E>& L, int i, int j) { return j * L.h + (i >> 1); }
+
+// Dense solve of the bottom level, unknown row = j*nx + i, with the elimination of the
+// matrix done once per solve (k_dense_factor): the oracle's b[i] -= m*b[k] in its order,
+// then its back substitution s = b[i] - sum_j U[i][j] u[j] (j ascending), u[i] = s / U[i][i].
 template <bool W>
-__device__ void s_dense(const SL<double>& L, double* A, double* b) {
-    const int nx = L.nx, ny = L.ny, n = nx * ny;
-    for (int k = g_tid<W>(); k < n * n; k += g_nthr<W>()) A[k] = 0.0;
-    for (int k = g_tid<W>(); k < n; k += g_nthr<W>()) b[k] = L.f[k];
-    g_sync<W>();
-    for (int row = g_tid<W>(); row < n; row += g_nthr<W>()) {
-        const int j = row / nx, i = row - j * nx;
-        const int ip = (i + 1 == nx) ? 0 : i + 1, im = (i == 0) ? nx - 1 : i - 1;
-        const double aw = L.ax[j * nx + i];
-        const double ae = L.ax[j * nx + ip];
-        const double as = L.ay[j * nx + i];
-        const double an = L.ay[(j + 1) * nx + i];
-        double d = aw;
-        d += ae;
-        d += as;
-        d += an;
-        A[row * n + row] -= d;
-        A[row * n + j * nx + im] += aw;
-        A[row * n + j * nx + ip] += ae;
-        if (j > 0) A[row * n + (j - 1) * nx + i] += as;
-        if (j < ny - 1) A[row * n + (j + 1) * nx + i] += an;
+__device__ void s_dense(const SL<double>& L, const double* A, double* b) {
+    const int nx = L.nx, n = nx * L.ny;
+    for (int k = g_tid<W>(); k < n; k += g_nthr<W>()) {
+        const int j = k / nx, i = k - j * nx;
+        b[k] = pick(L.f, (i + j) & 1)[split_index(L, i, j)];
     }
     g_sync<W>();
-    for (int k = 0; k < n; ++k) {
-        const double piv = A[k * n + k];
-        const int m = n - k - 1;
-        for (int t = g_tid<W>(); t < m * (m + 1); t += g_nthr<W>()) {
-            const int i = k + 1 + t / (m + 1), c = t % (m + 1);
-            const double mult = A[i * n + k] / piv;
-            if (c < m) {
-                const int j = k + 1 + c;
-                A[i * n + j] -= mult * A[k * n + j];
-            } else {
-                b[i] -= mult * b[k];
-            }
-        }
+    for (int k = 0; k + 1 < n; ++k) {
+        const double bk = b[k];
+        for (int i = k + 1 + g_tid<W>(); i < n; i += g_nthr<W>()) b[i] -= A[i * n + k] * bk;
         g_sync<W>();
     }
     if (g_tid<W>() == 0) {
         for (int i = n - 1; i >= 0; --i) {
             double s = b[i];
-            for (int j = i + 1; j < n; ++j) s -= A[i * n + j] * L.u[j];
-            L.u[i] = s / A[i * n + i];
+            for (int j = i + 1; j < n; ++j) s -= A[i * n + j] * b[j];
+            b[i] = s / A[i * n + i];
         }
+    }
+    g_sync<W>();
+    for (int k = g_tid<W>(); k < n; k += g_nthr<W>()) {
+        const int j = k / nx, i = k - j * nx;
+        pick(L.u, (i + j) & 1)[split_index(L, i, j)] = b[k];
     }
     g_sync<W>();
 }
@@ -797,8 +862,10 @@ __device__ void s_outer(const CtaParams& P, unsigned char* sm) {
     }
     {
         const SL<double> L = make_sl<double>(P, sm, P.lc);
-        for (int k = threadIdx.x; k < L.nx * L.ny; k += blockDim.x) L.u[k] = 0.0;
-        __syncthreads();
+        if (P.lcta == P.lc) {  // no restriction wrote u(lc)
+            for (int k = threadIdx.x; k < L.ny * L.h; k += NT_CTA) { L.u[0][k] = 0.0; L.u[1][k] = 0.0; }
+            __syncthreads();
+        }
         if (P.lc == P.bottom) {
             if (threadIdx.x < 32)
                 s_dense<true>(L, reinterpret_cast<double*>(sm + P.off_dense), reinterpret_cast<double*>(sm + P.off_rhs));
@@ -815,59 +882,113 @@ __device__ void s_outer(const CtaParams& P, unsigned char* sm) {
     }
 }
 
+// Asynchronous copy of one 4- or 8-byte element global -> shared (completion:
+// async_wait_all + barrier).
+template <typename E>
+__device__ __forceinline__ void cp_async_elem(E* dst, const E* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if (sizeof(E) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+// Global (row-major, nrows x nx) -> colour-split shared (X0, X1), issued as asynchronous
+// copies so that every level's arrays are in flight at once.
+template <typename E>
+__device__ __forceinline__ void stage_split(E* X0, E* X1, const E* __restrict__ g, int nx, int nrows, unsigned mag_h) {
+    const int h = nx >> 1, items = nrows * h;
+    ItemWalk wk(threadIdx.x, NT_CTA, h, mag_h);
+    for (int it = threadIdx.x; it < items; it += NT_CTA) {
+        const int j = wk.r, m = wk.q;
+        const E* src = g + j * nx + 2 * m;
+        const int k = j * h + m;
+        cp_async_elem((j & 1) ? X1 + k : X0 + k, src);
+        cp_async_elem((j & 1) ? X0 + k : X1 + k, src + 1);
+        wk.next();
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(NT_CTA, 1) k_cta(const __grid_constant__ CtaParams P) {
     extern __shared__ __align__(16) unsigned char sm[];
-    // stage beta of every level handled here, and f of the entry level
+    // stage beta of every level handled here and the bottom elimination, zero the ghost
+    // rows of u, stage f(lcta)
     for (int l = P.lcta; l <= P.bottom; ++l) {
         const CtaLevel& L = P.lv[l];
-        const int n = L.nx * L.ny, nb = L.nx * (L.ny + 1);
         if (l < P.lc) {
-            T* ax = reinterpret_cast<T*>(sm + L.off_ax);
-            T* ay = reinterpret_cast<T*>(sm + L.off_ay);
-            T* di = reinterpret_cast<T*>(sm + L.off_di);
-            const T* gax = reinterpret_cast<const T*>(L.gax);
-            const T* gay = reinterpret_cast<const T*>(L.gay);
-            const T* gdi = reinterpret_cast<const T*>(L.gdi);
-            for (int k = threadIdx.x; k < n; k += blockDim.x) { ax[k] = gax[k]; di[k] = gdi[k]; }
-            for (int k = threadIdx.x; k < nb; k += blockDim.x) ay[k] = gay[k];
+            const SL<T> S = make_sl<T>(P, sm, l);
+            stage_split(S.ax[0], S.ax[1], reinterpret_cast<const T*>(L.gax), L.nx, L.ny, L.mag_h);
+            stage_split(S.ay[0], S.ay[1], reinterpret_cast<const T*>(L.gay), L.nx, L.ny + 1, L.mag_h);
+            stage_split(S.di[0], S.di[1], reinterpret_cast<const T*>(L.gdi), L.nx, L.ny, L.mag_h);
+            for (int k = threadIdx.x; k < L.half; k += NT_CTA) {
+                S.u[0][k - L.half] = T(0); S.u[1][k - L.half] = T(0);
+                S.u[0][L.ny * L.half + k] = T(0); S.u[1][L.ny * L.half + k] = T(0);
+            }
         } else {
-            double* ax = reinterpret_cast<double*>(sm + L.off_ax);
-            double* ay = reinterpret_cast<double*>(sm + L.off_ay);
-            double* di = reinterpret_cast<double*>(sm + L.off_di);
-            const double* gax = reinterpret_cast<const double*>(L.gax);
-            const double* gay = reinterpret_cast<const double*>(L.gay);
-            const double* gdi = reinterpret_cast<const double*>(L.gdi);
-            for (int k = threadIdx.x; k < n; k += blockDim.x) { ax[k] = gax[k]; di[k] = gdi[k]; }
-            for (int k = threadIdx.x; k < nb; k += blockDim.x) ay[k] = gay[k];
+            const SL<double> S = make_sl<double>(P, sm, l);
+            stage_split(S.ax[0], S.ax[1], reinterpret_cast<const double*>(L.gax), L.nx, L.ny, L.mag_h);
+            stage_split(S.ay[0], S.ay[1], reinterpret_cast<const double*>(L.gay), L.nx, L.ny + 1, L.mag_h);
+            stage_split(S.di[0], S.di[1], reinterpret_cast<const double*>(L.gdi), L.nx, L.ny, L.mag_h);
+            for (int k = threadIdx.x; k < L.half; k += NT_CTA) {
+                S.u[0][k - L.half] = 0.0; S.u[1][k - L.half] = 0.0;
+                S.u[0][L.ny * L.half + k] = 0.0; S.u[1][L.ny * L.half + k] = 0.0;
+            }
         }
     }
     {
+        const int nb = P.lv[P.bottom].nx * P.lv[P.bottom].ny;
+        double* A = reinterpret_cast<double*>(sm + P.off_dense);
+        for (int k = threadIdx.x; k < nb * nb; k += NT_CTA) cp_async_elem(A + k, P.glu + k);
+    }
+    {
         const CtaLevel& L = P.lv[P.lcta];
-        const int n = L.nx * L.ny;
         const T* fin = reinterpret_cast<const T*>(P.f_in);
         if (P.lcta < P.lc) {
-            T* f = reinterpret_cast<T*>(sm + L.off_f);
-            T* u = reinterpret_cast<T*>(sm + L.off_u);
-            for (int k = threadIdx.x; k < n; k += blockDim.x) { f[k] = fin[k]; u[k] = T(0); }
+            const SL<T> S = make_sl<T>(P, sm, P.lcta);
+            stage_split(S.f[0], S.f[1], fin, L.nx, L.ny, L.mag_h);
+            for (int k = threadIdx.x; k < L.ny * L.half; k += NT_CTA) { S.u[0][k] = T(0); S.u[1][k] = T(0); }
         } else {
-            double* f = reinterpret_cast<double*>(sm + L.off_f);
-            for (int k = threadIdx.x; k < n; k += blockDim.x) f[k] = double(fin[k]);
+            const SL<double> S = make_sl<double>(P, sm, P.lcta);
+            if (std::is_same<T, double>::value) {
+                stage_split(S.f[0], S.f[1], reinterpret_cast<const double*>(fin), L.nx, L.ny, L.mag_h);
+            } else {
+                const int h = L.half, items = L.ny * h;
+                ItemWalk wk(threadIdx.x, NT_CTA, h, L.mag_h);
+                for (int it = threadIdx.x; it < items; it += NT_CTA) {
+                    const int j = wk.r, m = wk.q, k = j * h + m;
+                    const double a = double(fin[j * L.nx + 2 * m]), b = double(fin[j * L.nx + 2 * m + 1]);
+                    if (j & 1) { S.f[1][k] = a; S.f[0][k] = b; }
+                    else { S.f[0][k] = a; S.f[1][k] = b; }
+                    wk.next();
+                }
+            }
         }
     }
+    async_wait_all();
     __syncthreads();
     s_outer<T>(P, sm);
     __syncthreads();
     {
         const CtaLevel& L = P.lv[P.lcta];
-        const int n = L.nx * L.ny;
         T* uo = reinterpret_cast<T*>(P.u_out);
-        if (P.lcta < P.lc) {
-            const T* u = reinterpret_cast<const T*>(sm + L.off_u);
-            for (int k = threadIdx.x; k < n; k += blockDim.x) uo[k] = u[k];
-        } else {
-            const double* u = reinterpret_cast<const double*>(sm + L.off_u);
-            for (int k = threadIdx.x; k < n; k += blockDim.x) uo[k] = T(u[k]);
+        const int h = L.half, items = L.ny * h;
+        ItemWalk wk(threadIdx.x, NT_CTA, h, L.mag_h);
+        for (int it = threadIdx.x; it < items; it += NT_CTA) {
+            const int j = wk.r, m = wk.q, k = j * h + m;
+            T a, b;
+            if (P.lcta < P.lc) {
+                const SL<T> S = make_sl<T>(P, sm, P.lcta);
+                a = (j & 1) ? S.u[1][k] : S.u[0][k];
+                b = (j & 1) ? S.u[0][k] : S.u[1][k];
+            } else {
+                const SL<double> S = make_sl<double>(P, sm, P.lcta);
+                a = T((j & 1) ? S.u[1][k] : S.u[0][k]);
+                b = T((j & 1) ? S.u[0][k] : S.u[1][k]);
+            }
+            uo[j * L.nx + 2 * m] = a;
+            uo[j * L.nx + 2 * m + 1] = b;
+            wk.next();
         }
     }
 }
@@ -919,6 +1040,47 @@ __global__ void k_scale_beta(const T* __restrict__ bx, const T* __restrict__ by,
             ay[kk] = (j == 0) ? T(0) : ((j == (size_t)ny) ? cy2 * by[kk] : cy * by[kk]);
         }
     }
+}
+
+// Elimination of the bottom level's dense matrix, done once per solve in shared memory:
+// the oracle's dense_solve without its right-hand side (same assembly, pivots and
+// products).  Output: U on and above the diagonal, the multipliers A[i][k] / piv below.
+__global__ void k_dense_factor(const double* __restrict__ ax, const double* __restrict__ ay,
+                               double* __restrict__ out, int nx, int ny) {
+    extern __shared__ __align__(16) double A[];
+    const int n = nx * ny, t = threadIdx.x, G = blockDim.x;
+    for (int k = t; k < n * n; k += G) A[k] = 0.0;
+    __syncthreads();
+    if (t == 0) {
+        for (int row = 0; row < n; ++row) {
+            const int j = row / nx, i = row - j * nx;
+            const int ip = (i + 1 == nx) ? 0 : i + 1, im = (i == 0) ? nx - 1 : i - 1;
+            const double aw = ax[j * nx + i], ae = ax[j * nx + ip], as = ay[j * nx + i], an = ay[(j + 1) * nx + i];
+            double d = aw;
+            d += ae;
+            d += as;
+            d += an;
+            A[row * n + row] -= d;
+            A[row * n + j * nx + im] += aw;
+            A[row * n + j * nx + ip] += ae;
+            if (j > 0) A[row * n + (j - 1) * nx + i] += as;
+            if (j < ny - 1) A[row * n + (j + 1) * nx + i] += an;
+        }
+    }
+    __syncthreads();
+    for (int k = 0; k < n; ++k) {
+        const double piv = A[k * n + k];
+        const int m = n - k - 1;
+        for (int q = t; q < m * m; q += G) {
+            const int i = k + 1 + q / m, j = k + 1 + q % m;
+            const double mult = A[i * n + k] / piv;
+            A[i * n + j] -= mult * A[k * n + j];
+        }
+        __syncthreads();
+        for (int i = k + 1 + t; i < n; i += G) A[i * n + k] = A[i * n + k] / piv;
+        __syncthreads();
+    }
+    for (int k = t; k < n * n; k += G) out[k] = A[k];
 }
 
 __global__ void k_to_float(const double* __restrict__ a, float* __restrict__ b, size_t n) {
@@ -1025,6 +1187,7 @@ struct lica_mg {
     void* zpre = nullptr;    // z after pre-smoothing (T)
     void* z = nullptr;       // z (T): the V-cycle's level-0 output
     double* partials = nullptr;
+    double* dense_lu = nullptr;  // bottom-level elimination, refreshed by every set-up
     State* st = nullptr;
     State* st_host = nullptr;  // pinned
     // host staging for lica_mg_solve_host
@@ -1248,6 +1411,13 @@ int setup_beta(lica_mg* m, const double* bx, const double* by, cudaStream_t s) {
             LICA_CUDA_TRY(cudaGetLastError());
             lica_count_launches(1);
         }
+    }
+    {
+        const LevelBuf& B = m->lv[m->bottom];
+        const int nb = B.nx * B.ny;
+        k_dense_factor<<<1, 256, sizeof(double) * nb * nb, s>>>(B.ax64, B.ay64, m->dense_lu, B.nx, B.ny);
+        LICA_CUDA_TRY(cudaGetLastError());
+        lica_count_launches(1);
     }
     // weights of the levels staged by the single-CTA kernel
     for (int l = m->lcta; l <= m->bottom; ++l) {
@@ -1509,17 +1679,29 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
     const size_t tsz = mixed ? sizeof(float) : sizeof(double);
     // single-CTA levels: from the first level >= 1 whose remaining hierarchy fits in
     // shared memory and has <= 32*32 cells, or that cannot be tiled
-    auto cta_bytes = [&](int from) {
-        size_t b = 0;
-        for (int l = from; l <= m->bottom; ++l) {
-            const size_t e = (l < m->nouter - 1) ? tsz : sizeof(double);
-            const size_t n = (size_t)m->lv[l].nx * m->lv[l].ny;
-            b += e * (4 * n + n + m->lv[l].nx);
-            b = (b + 15) & ~(size_t)15;
+    // per level: u (two colours, each (ny+2) x nx/2 with zero ghost rows), f, ax, 1/d
+    // (ny x nx/2 each) and ay ((ny+1) x nx/2), 16-byte aligned arrays
+    auto level_arrays = [&](int l, auto&& take) {
+        const size_t e = (l < m->nouter - 1) ? tsz : sizeof(double);
+        const size_t h = (size_t)m->lv[l].nx / 2, ny = m->lv[l].ny;
+        CtaLevel C{};
+        for (int c = 0; c < 2; ++c) {
+            C.off_u[c] = take(e * (ny + 2) * h);
+            C.off_f[c] = take(e * ny * h);
+            C.off_ax[c] = take(e * ny * h);
+            C.off_ay[c] = take(e * (ny + 1) * h);
+            C.off_di[c] = take(e * ny * h);
         }
+        return C;
+    };
+    auto cta_bytes = [&](int from) {
+        size_t off = 0;
+        auto take = [&](size_t bytes) { size_t r = off; off = (off + bytes + 15) & ~(size_t)15; return (unsigned)r; };
+        for (int l = from; l <= m->bottom; ++l) level_arrays(l, take);
         const size_t nb = (size_t)m->lv[m->bottom].nx * m->lv[m->bottom].ny;
-        b += sizeof(double) * (nb * nb + nb);
-        return b;
+        take(sizeof(double) * nb * nb);
+        take(sizeof(double) * nb);
+        return off;
     };
     int lcta = m->nouter - 1;
     for (int l = 1; l < m->nouter; ++l) {
@@ -1545,15 +1727,12 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t r = off; off = (off + bytes + 15) & ~(size_t)15; return (unsigned)r; };
     for (int l = lcta; l <= m->bottom; ++l) {
-        const size_t e = (l < m->nouter - 1) ? tsz : sizeof(double);
-        const size_t n = (size_t)m->lv[l].nx * m->lv[l].ny;
         CtaLevel& C = P.lv[l];
-        C.nx = m->lv[l].nx; C.ny = m->lv[l].ny;
-        C.off_u = take(e * n);
-        C.off_f = take(e * n);
-        C.off_ax = take(e * n);
-        C.off_ay = take(e * (n + m->lv[l].nx));
-        C.off_di = take(e * n);
+        C = level_arrays(l, take);
+        C.nx = m->lv[l].nx; C.ny = m->lv[l].ny; C.half = m->lv[l].nx / 2;
+        auto mag = [](unsigned c) { return c > 1 ? (unsigned)((1ull << 32) / c + 1) : 0u; };
+        C.mag_h = mag((unsigned)C.half);
+        C.mag_nx = mag((unsigned)C.nx);
     }
     const size_t nb = (size_t)m->lv[m->bottom].nx * m->lv[m->bottom].ny;
     P.off_dense = take(sizeof(double) * nb * nb);
@@ -1608,6 +1787,11 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
     const size_t ntiles = (size_t)(nx / 16) * (ny / 16);  // the most blocks of any level-0 grid kernel
     TRY_ALLOC(m->partials, sizeof(double) * 2 * ntiles);
     TRY_ALLOC(m->st, sizeof(State));
+    {
+        const size_t nb = (size_t)m->lv[m->bottom].nx * m->lv[m->bottom].ny;
+        TRY_ALLOC(m->dense_lu, sizeof(double) * nb * nb);
+        P.glu = m->dense_lu;
+    }
     {
         cudaError_t e = cudaMallocHost((void**)&m->st_host, sizeof(State));
         if (e != cudaSuccess) return fail(LICA_ERR_NOMEM);
@@ -1668,6 +1852,7 @@ int lica_mg_destroy(lica_mg* m) {
     cudaFree(m->pcg[1]);
     cudaFree(m->xb);
     cudaFree(m->r);
+    cudaFree(m->dense_lu);
     cudaFree(m->zpre);
     cudaFree(m->z);
     cudaFree(m->partials);
