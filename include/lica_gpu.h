@@ -288,6 +288,20 @@ int lica_gpu_lvs_transport_device(int32_t ncol, int32_t n, double length, double
                                   double* psi_zn, int32_t* status, double* stats, const lica_lvs_params* prm,
                                   void* stream);
 
+/* ---------------------------------------------------------------- learned guess
+ * Convolution primitive of the U-Net that supplies the multigrid initial guess (new; the
+ * reference has no learned part): 3x3, stride 1, zero padding 1, NHWC BF16 activations,
+ * BF16 weights W[cout][9*(c0+c1)] (k = tap*(c0+c1) + channel, tap = 3*dy + dx) with FP32
+ * accumulation on the tcgen05 tensor cores.  x1 (c1 channels, may be null with c1 = 0) is
+ * concatenated after x0 (c0 channels) along the channels.  The result (+ bias, ReLU when
+ * relu != 0) goes to channels [out_c0, out_c0 + cout) of the NHWC tensor out (BF16, out_c
+ * channels) and/or out32 (FP32).  c0, c1, cout: multiples of 16 (cout <= 256); the width
+ * is a multiple of 128, or divides 128 with the height a multiple of 128 / width.  *err is
+ * set to 1 if a bounded wait inside the kernel ran out. */
+int lica_unet_conv3x3_device(const void* x0, int32_t c0, const void* x1, int32_t c1, const void* w,
+                             const float* bias, int32_t n, int32_t h, int32_t wd, int32_t cout, int32_t relu,
+                             void* out, float* out32, int32_t out_c, int32_t out_c0, int32_t* err, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -81,6 +81,9 @@ SIGNATURES = {
                                                      C.c_void_p, C.c_void_p, C.c_void_p]),
     "lica_gpu_column_steps": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.POINTER(ColProps), C.POINTER(ColState),
                                         C.c_int32, _I32]),
+    "lica_unet_conv3x3_device": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                           C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
+                                           C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
 }
 
 STATUS = {0: "LICA_OK", 1: "LICA_NOT_CONVERGED", 2: "LICA_BAND_OVERFLOW", 3: "LICA_NAN", 4: "LICA_BAD_ARG",
