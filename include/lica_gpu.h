@@ -302,6 +302,36 @@ int lica_unet_conv3x3_device(const void* x0, int32_t c0, const void* x1, int32_t
                              const float* bias, int32_t n, int32_t h, int32_t wd, int32_t cout, int32_t relu,
                              void* out, float* out32, int32_t out_c, int32_t out_c0, int32_t* err, void* stream);
 
+/* The U-Net of the learned initial guess (new; no counterpart in the reference).  Input per
+ * image: rho and f (row-major h x w, FP64, device); output: the guess x0 of the pressure
+ * solve A p = f (FP64; the network's output times rms(f) h^2 rho, h^2 = hsq), which the
+ * caller passes to lica_mg_solve_* as the initial iterate
+ * (the solver keeps its own tolerance; a guess whose residual exceeds ||f|| should be
+ * replaced by zero).  Network: 3 levels of 32/64/128 channels, two 3x3 convolutions with
+ * ReLU per level and per decoder level, 2x2 average pooling, nearest upsampling, skip
+ * connections, a 1x1 head; BF16 weights and activations, FP32 accumulation on the tcgen05
+ * tensor cores (lica_unet_conv3x3_device).  Parameters: FP32 vector, layer by layer
+ * (weights [cout][tap][cin], then bias), then the head (32 weights, 1 bias).
+ * lica_unet_create: n images of h x w (multiples of 64, >= 64), deterministic He
+ * initialisation from seed.  lica_unet_train_step_device: one Adam step on the loss
+ * mean_images ||f - A x0||^2 / ||f||^2 with A the solver's operator (face coefficients bx,
+ * by as in lica_mg_solve_*), or, given the solver's solutions p_star (A p* = f), on the
+ * relative A-norm error (x0 - p*).(-A)(x0 - p*) / p*.(-A)p*; *loss is the loss before
+ * the step.  lica_unet_grad_device:
+ * parameter gradient of sum(gx0 * x0) (the gradient check). */
+typedef struct lica_unet lica_unet;
+int lica_unet_create(lica_unet** out, int32_t n, int32_t h, int32_t w, uint64_t seed);
+int lica_unet_destroy(lica_unet* net);
+int64_t lica_unet_param_count(const lica_unet* net);
+int lica_unet_get_params(lica_unet* net, float* host, int64_t count);
+int lica_unet_set_params(lica_unet* net, const float* host, int64_t count);
+int lica_unet_guess_device(lica_unet* net, const double* rho, const double* f, double hsq, double* x0, void* stream);
+int lica_unet_grad_device(lica_unet* net, const double* rho, const double* f, double hsq, const double* gx0,
+                          float* grad_host, int64_t count, void* stream);
+int lica_unet_train_step_device(lica_unet* net, const double* rho, const double* f, const double* bx,
+                                const double* by, const double* p_star, double hx, double hy, float lr,
+                                double* loss, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

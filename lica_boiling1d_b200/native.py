@@ -81,6 +81,16 @@ SIGNATURES = {
                                                      C.c_void_p, C.c_void_p, C.c_void_p]),
     "lica_gpu_column_steps": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.POINTER(ColProps), C.POINTER(ColState),
                                         C.c_int32, _I32]),
+    "lica_unet_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.c_int32, C.c_uint64]),
+    "lica_unet_destroy": (C.c_int, [C.c_void_p]),
+    "lica_unet_param_count": (C.c_int64, [C.c_void_p]),
+    "lica_unet_get_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int64]),
+    "lica_unet_set_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int64]),
+    "lica_unet_guess_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]),
+    "lica_unet_grad_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p,
+                                        C.POINTER(C.c_float), C.c_int64, C.c_void_p]),
+    "lica_unet_train_step_device": (C.c_int, [C.c_void_p] + [C.c_void_p] * 5 + [C.c_double, C.c_double, C.c_float,
+                                                                              C.POINTER(C.c_double), C.c_void_p]),
     "lica_unet_conv3x3_device": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
                                            C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
                                            C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),

@@ -34,3 +34,69 @@ def conv3x3(x0, x1, w, bias=None, relu=False, out=None, out_c0=0, want32=False, 
     if int(err.item()):
         raise native.LicaError(5, "lica_unet_conv3x3_device: a bounded wait ran out")
     return out, out32
+
+
+class LearnedGuess:
+    """The U-Net initial guess for n images of h x w (lica_unet_*): guess(), train_step(),
+    parameter get/set.  Device arrays are contiguous FP64 torch tensors of shape (n, h, w)
+    (by: (n, h + 1, w))."""
+
+    def __init__(self, n, h, w, seed=1):
+        import numpy as np  # noqa: F401
+        self.n, self.h, self.w = n, h, w
+        self._h = C.c_void_p()
+        native.check(native.lib().lica_unet_create(C.byref(self._h), n, h, w, seed), "lica_unet_create")
+        self.nparams = int(native.lib().lica_unet_param_count(self._h))
+
+    def close(self):
+        if self._h:
+            native.lib().lica_unet_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_params(self):
+        import numpy as np
+        p = np.empty(self.nparams, dtype=np.float32)
+        native.check(native.lib().lica_unet_get_params(self._h, p.ctypes.data_as(C.POINTER(C.c_float)), p.size),
+                     "lica_unet_get_params")
+        return p
+
+    def set_params(self, p):
+        import numpy as np
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        native.check(native.lib().lica_unet_set_params(self._h, p.ctypes.data_as(C.POINTER(C.c_float)), p.size),
+                     "lica_unet_set_params")
+
+    @staticmethod
+    def _stream(stream):
+        import torch
+        return C.c_void_p(stream or torch.cuda.current_stream().cuda_stream)
+
+    def guess(self, rho, f, hsq, out=None, stream=None):
+        import torch
+        if out is None:
+            out = torch.empty_like(f)
+        native.check(native.lib().lica_unet_guess_device(self._h, _ptr(rho), _ptr(f), float(hsq), _ptr(out),
+                                                         self._stream(stream)), "lica_unet_guess_device")
+        return out
+
+    def grad(self, rho, f, hsq, gx0, stream=None):
+        import numpy as np
+        g = np.empty(self.nparams, dtype=np.float32)
+        native.check(native.lib().lica_unet_grad_device(self._h, _ptr(rho), _ptr(f), float(hsq), _ptr(gx0),
+                                                        g.ctypes.data_as(C.POINTER(C.c_float)), g.size,
+                                                        self._stream(stream)), "lica_unet_grad_device")
+        return g
+
+    def train_step(self, rho, f, bx, by, hx, hy, lr, p_star=None, stream=None):
+        loss = C.c_double()
+        native.check(native.lib().lica_unet_train_step_device(self._h, _ptr(rho), _ptr(f), _ptr(bx), _ptr(by),
+                                                              _ptr(p_star), float(hx), float(hy), float(lr),
+                                                              C.byref(loss), self._stream(stream)),
+                     "lica_unet_train_step_device")
+        return loss.value

@@ -52,3 +52,101 @@ def test_conv3x3_tensor_core(n, h, wd, c0, c1, cout, relu):
     assert np.all(np.abs(got32 - ref) <= 2e-5 * mag + 1e-30), np.abs(got32 - ref).max()
     got16 = out.cpu().double().numpy()
     assert np.all(np.abs(got16 - got32) <= np.abs(got32) * 2.0 ** -8 + 1e-30)
+
+
+def _net_case(n=2, h=64, w=64, seed=5):
+    from lica_boiling1d_b200.inputs import bubble_density, gaussian_rhs
+    rho = np.stack([bubble_density(w, h, nbubbles=3, rmin=4, rmax=12, seed=seed + i) for i in range(n)])
+    f = np.stack([gaussian_rhs(w, h, seed + 100 + i) for i in range(n)])
+    return rho, f
+
+
+def test_unet_forward_matches_oracle():
+    import torch
+    from lica_boiling1d_b200.unet import LearnedGuess
+    from oracle import unet_ref as U
+    rho, f = _net_case()
+    hsq = 1.0 / 64 ** 2
+    net = LearnedGuess(2, 64, 64, seed=11)
+    x0 = net.guess(torch.from_numpy(rho).cuda(), torch.from_numpy(f).cuda(), hsq).cpu().numpy()
+    ref, _ = U.forward(net.get_params().astype(np.float64), rho, f, hsq)
+    err = np.linalg.norm(x0 - ref) / np.linalg.norm(ref)
+    assert err < 2e-2, err
+    net.close()
+
+
+def test_unet_gradient_matches_oracle():
+    """Every parameter tensor's gradient from the GPU's own backward kernels (tensor-core
+    input gradients, CUDA-core weight gradients) against the oracle's hand-derived
+    backward, within 1% relative L2 per tensor.  The upstream gradient is a smooth field
+    (divided by rho, so that the head's gradient, which the output scale multiplies by rho,
+    stays smooth):
+    with a random-sign one every weight gradient is a cancelling sum, and the few ReLU
+    masks that BF16 rounding flips between the two sides then show up at the level of the
+    square root of their share (a few percent) although both are right."""
+    import torch
+    from lica_boiling1d_b200.unet import LearnedGuess
+    from oracle import unet_ref as U
+    rho, f = _net_case()
+    hsq = 1.0 / 64 ** 2
+    net = LearnedGuess(2, 64, 64, seed=11)
+    yy, xx = np.meshgrid(np.arange(64), np.arange(64), indexing="ij")
+    gx0 = 1e3 * (1.0 + 0.5 * np.sin(2 * np.pi * xx / 64) * np.cos(2 * np.pi * yy / 64))[None].repeat(2, 0) / rho
+    g = net.grad(torch.from_numpy(rho).cuda(), torch.from_numpy(f).cuda(), hsq, torch.from_numpy(gx0).cuda())
+    _, cache = U.forward(net.get_params().astype(np.float64), rho, f, hsq)
+    ref = U.backward(cache, gx0, hsq)
+    o = 0
+    for l, (c0, c1, co, _) in enumerate(U.LAYERS):
+        nw = co * 9 * (c0 + c1)
+        for name, k in (("W", nw), ("b", co)):
+            a, b = g[o:o + k].astype(np.float64), ref[o:o + k]
+            if l == 0 and name == "W":  # input channels 2..15 carry zeros
+                a = a.reshape(co, 9, 16)[:, :, :2]
+                b = b.reshape(co, 9, 16)[:, :, :2]
+            rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+            assert rel < 1e-2, (l, name, rel)
+            o += k
+    a, b = g[o:].astype(np.float64), ref[o:]
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-2
+    net.close()
+
+
+def test_learned_guess_gain():
+    """What the trained network gains over the method without it.  Trained on the GPU by
+    its own kernels (400 Adam steps on 128 x 128 solver pairs, A-norm loss), the guess
+    must cut the relative A-norm error and the relative residual of the starting iterate
+    well below those of x0 = 0 (both 1) on held-out problems, and the PCG started from it
+    must reach the same 1e-10 tolerance in no more iterations than from zero."""
+    import torch
+    from lica_boiling1d_b200 import poisson
+    from lica_boiling1d_b200 import train_guess as T
+    from lica_boiling1d_b200.unet import LearnedGuess
+    net = LearnedGuess(4, 128, 128, seed=1)
+    hist = T.train(net, 400, 128, lr=1e-3, lr_final=2e-4, seed=3, log=None, anorm=True)
+    assert np.mean(hist[-50:]) < 0.5 * np.mean(hist[:10])
+    n = 256
+    ev = LearnedGuess(1, n, n)
+    ev.set_params(net.get_params())
+    rng = np.random.default_rng(2024)
+    probs = [T.problem(rng, n) for _ in range(3)]
+    s = poisson.MultigridPoisson(n, n, 1.0 / n, 1.0 / n, nlevels=4, ncoarse=1)
+    errs, ress = [], []
+    for rho, f, bx, by in probs:
+        F, BX, BY = (torch.from_numpy(a.copy()).cuda() for a in (f, bx, by))
+        g = ev.guess(torch.from_numpy(rho[None].copy()).cuda(), F[None], 1.0 / n ** 2)[0].contiguous()
+        ps = torch.zeros_like(F)
+        s.solve(ps, F, BX, BY, rtol=1e-12, max_iters=200)
+        ag, ae = torch.empty_like(g), torch.empty_like(g)
+        s.apply(ag, g, BX, BY)
+        s.apply(ae, g - ps, BX, BY)
+        ress.append(float(torch.linalg.norm(F - ag) / torch.linalg.norm(F)))
+        errs.append(float(torch.sqrt(((g - ps) * -ae).sum() / (ps * -F).sum())))
+    s.close()
+    assert max(errs) < 0.7 and max(ress) < 0.7, (errs, ress)
+    base = T.iterations(n, probs)
+    gu = T.iterations(n, probs, ev)
+    for b, g in zip(base, gu):
+        assert g[2] == 0 and g[1] <= 1e-10
+        assert g[0] <= b[0]
+    net.close()
+    ev.close()
