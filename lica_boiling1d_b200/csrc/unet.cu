@@ -115,9 +115,13 @@ int conv3x3(const __nv_bfloat16* x0, int c0, const __nv_bfloat16* x1, int c1, co
     }
     static std::once_flag attr_once;
     static cudaError_t attr_err = cudaSuccess;
+    static int num_sms = 148;
     std::call_once(attr_once, [] {
-        attr_err = cudaFuncSetAttribute(k_conv3x3_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)conv_smem_bytes(256));
+        attr_err = cudaFuncSetAttribute(k_conv3x3_tcp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)conv_p_smem_bytes(kTileM * 128, 256 * 128));
+        int dev = 0;
+        if (attr_err == cudaSuccess) attr_err = cudaGetDevice(&dev);
+        if (attr_err == cudaSuccess) attr_err = cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
     });
     LICA_CUDA_TRY(attr_err);
     ConvParams P{};
@@ -146,7 +150,17 @@ int conv3x3(const __nv_bfloat16* x0, int c0, const __nv_bfloat16* x1, int c1, co
         mw1 = mw0;
     }
     const int tiles = n * (h / th) * (wd / tw);
-    k_conv3x3_tc<<<tiles, 128, conv_smem_bytes(cout), s>>>(mx0, mx1, mw0, mw1, P);
+    const int cbmax = std::max(P.cblk[0], P.nsrc > 1 ? P.cblk[1] : 0);
+    P.stage_a = kTileM * cbmax * 2;
+    P.stage_b = ((cout * cbmax * 2 + 1023) / 1024) * 1024;
+    P.tiles = tiles;
+    const size_t smem = conv_p_smem_bytes(P.stage_a, P.stage_b);
+    // CTAs per SM: shared memory and tensor memory (two accumulators of tmem_cols each)
+    int per_sm = 0;
+    LICA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv3x3_tcp, kConvThreads, smem));
+    per_sm = std::max(1, std::min(per_sm, 512 / (2 * P.tmem_cols)));
+    const int grid = std::min(tiles, per_sm * num_sms);
+    k_conv3x3_tcp<<<grid, kConvThreads, smem, s>>>(mx0, mx1, mw0, mw1, P);
     LICA_CUDA_TRY(cudaGetLastError());
     lica_count_launches(1);
     return LICA_OK;
@@ -200,14 +214,21 @@ constexpr int kNT = 256;
 using bf16 = __nv_bfloat16;
 
 // ---------------------------------------------------------------- elementwise kernels
-// sigma[n] = sqrt(mean f^2) of each image (one block per image, fixed summation order).
-__global__ void k_rms(const double* __restrict__ f, double* __restrict__ sigma, int npix) {
+// sigma[n] = sqrt(mean f^2) of each image: kRmsParts blocks per image write partial
+// sums, one block per image adds them (fixed order).
+constexpr int kRmsParts = 64;
+__global__ void k_rms_part(const double* __restrict__ f, double* __restrict__ part, int npix) {
     __shared__ double red[32];
-    const double* fi = f + (size_t)blockIdx.x * npix;
+    const double* fi = f + (size_t)blockIdx.y * npix;
     double s = 0.0;
-    for (int k = threadIdx.x; k < npix; k += blockDim.x) s += fi[k] * fi[k];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < npix; k += gridDim.x * blockDim.x) s += fi[k] * fi[k];
     s = block_sum(s, red);
+    if (threadIdx.x == 0) part[blockIdx.y * kRmsParts + blockIdx.x] = s;
+}
+__global__ void k_rms_final(const double* __restrict__ part, double* __restrict__ sigma, int npix) {
     if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int k = 0; k < kRmsParts; ++k) s += part[blockIdx.x * kRmsParts + k];
         const double m = s / npix;
         sigma[blockIdx.x] = m > 0.0 ? sqrt(m) : 1.0;
     }
@@ -229,35 +250,63 @@ __global__ void k_input(const double* __restrict__ rho, const double* __restrict
     }
 }
 
-// 2x2 average: out[n, Y, X, c] = 0.25 * sum of the four children (FP32), NHWC.
+// 8 BF16 <-> 8 floats
+__device__ __forceinline__ void unpack8(const uint4& q, float* v) {
+    const __nv_bfloat162* b = reinterpret_cast<const __nv_bfloat162*>(&q);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float2 f = __bfloat1622float2(b[i]);
+        v[2 * i] = f.x;
+        v[2 * i + 1] = f.y;
+    }
+}
+__device__ __forceinline__ uint4 pack8(const float* v) {
+    uint4 q;
+    uint32_t* w = reinterpret_cast<uint32_t*>(&q);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const __nv_bfloat162 b = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+        w[i] = *reinterpret_cast<const uint32_t*>(&b);
+    }
+    return q;
+}
+
+// 2x2 average: out[n, Y, X, c] = 0.25 * ((a + b) + (c + d)) in FP32, NHWC, 8 channels per thread.
 __global__ void k_pool(const bf16* __restrict__ in, bf16* __restrict__ out, int nimg, int H, int W, int c) {
-    const int Ho = H / 2, Wo = W / 2;
-    const size_t total = (size_t)nimg * Ho * Wo * c;
+    const int Ho = H / 2, Wo = W / 2, c8 = c / 8;
+    const size_t total = (size_t)nimg * Ho * Wo * c8;
     for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
-        const int ch = (int)(q % c);
-        size_t r = q / c;
+        const int ch = (int)(q % c8) * 8;
+        const size_t r = q / c8;  // output pixel
         const int X = (int)(r % Wo);
-        r /= Wo;
-        const int Y = (int)(r % Ho);
-        const int img = (int)(r / Ho);
+        const size_t r2 = r / Wo;
+        const int Y = (int)(r2 % Ho);
+        const int img = (int)(r2 / Ho);
         const size_t b = (((size_t)img * H + 2 * Y) * W + 2 * X) * c + ch;
-        const float s = (__bfloat162float(in[b]) + __bfloat162float(in[b + c])) +
-                        (__bfloat162float(in[b + (size_t)W * c]) + __bfloat162float(in[b + (size_t)W * c + c]));
-        out[q] = __float2bfloat16_rn(0.25f * s);
+        float v00[8], v01[8], v10[8], v11[8], o[8];
+        unpack8(*reinterpret_cast<const uint4*>(in + b), v00);
+        unpack8(*reinterpret_cast<const uint4*>(in + b + c), v01);
+        unpack8(*reinterpret_cast<const uint4*>(in + b + (size_t)W * c), v10);
+        unpack8(*reinterpret_cast<const uint4*>(in + b + (size_t)W * c + c), v11);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) o[i] = 0.25f * ((v00[i] + v01[i]) + (v10[i] + v11[i]));
+        *reinterpret_cast<uint4*>(out + r * c + ch) = pack8(o);
     }
 }
 
-// nearest upsampling x2: out[n, y, x, c] = in[n, y/2, x/2, c].
+// nearest upsampling x2: out[n, y, x, :] = in[n, y/2, x/2, :], 8 channels per thread.
 __global__ void k_up(const bf16* __restrict__ in, bf16* __restrict__ out, int nimg, int H, int W, int c) {
-    const size_t total = (size_t)nimg * H * W * c;
+    const int c8 = c / 8;
+    const size_t total = (size_t)nimg * H * W * c8;
     for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
-        const int ch = (int)(q % c);
-        size_t r = q / c;
+        const int ch = (int)(q % c8) * 8;
+        const size_t r = q / c8;
         const int x = (int)(r % W);
-        r /= W;
-        const int y = (int)(r % H);
-        const int img = (int)(r / H);
-        out[q] = in[(((size_t)img * (H / 2) + y / 2) * (W / 2) + x / 2) * c + ch];
+        const size_t r2 = r / W;
+        const int y = (int)(r2 % H);
+        const int img = (int)(r2 / H);
+        *reinterpret_cast<uint4*>(out + r * c + ch) =
+            *reinterpret_cast<const uint4*>(in + (((size_t)img * (H / 2) + y / 2) * (W / 2) + x / 2) * c + ch);
     }
 }
 
@@ -269,8 +318,14 @@ __global__ void k_head(const bf16* __restrict__ d, const float* __restrict__ wh,
     const size_t total = (size_t)npix * nimg;
     for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < total; p += (size_t)gridDim.x * blockDim.x) {
         float s = bh[0];
-#pragma unroll 8
-        for (int c = 0; c < kHead; ++c) s += wh[c] * __bfloat162float(d[p * kHead + c]);
+        const uint4* dp = reinterpret_cast<const uint4*>(d + p * kHead);
+#pragma unroll
+        for (int q = 0; q < kHead / 8; ++q) {
+            float v[8];
+            unpack8(dp[q], v);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) s += wh[8 * q + i] * v[i];
+        }
         out32[p] = s;
         if (x0) x0[p] = (double)s * sigma[p / npix] * hsq * rho[p];
     }
@@ -584,6 +639,7 @@ struct lica_unet {
     bf16 *p1 = nullptr, *p2 = nullptr, *u2 = nullptr, *u1 = nullptr;
     float* out32 = nullptr;
     double* sigma = nullptr;
+    double* rms_part = nullptr;
     double* x0 = nullptr;   // guess (training)
     double* ax = nullptr;   // A x0, then r, then A r
     double* rr = nullptr;   // per-image ||r||^2 (or the A-norm loss's numerator)
@@ -646,23 +702,24 @@ int launch(size_t n, cudaStream_t s, K kernel, A... args) {
 int forward(lica_unet* u, const double* rho, const double* f, double hsq, double* x0, cudaStream_t s) {
     const int npix = u->h * u->w;
     int st;
-    k_rms<<<u->n, 1024, 0, s>>>(f, u->sigma, npix);
+    k_rms_part<<<dim3(kRmsParts, u->n), kNT, 0, s>>>(f, u->rms_part, npix);
+    k_rms_final<<<u->n, 32, 0, s>>>(u->rms_part, u->sigma, npix);
     LICA_CUDA_TRY(cudaGetLastError());
-    lica_count_launches(1);
+    lica_count_launches(2);
     if ((st = launch(level_pixels(u, 0), s, k_input, rho, f, (const double*)u->sigma, u->x16, npix, u->n))) return st;
     const int h = u->h, w = u->w, n = u->n;
     if ((st = conv_layer(u, 0, u->x16, nullptr, u->y[0], s))) return st;
     if ((st = conv_layer(u, 1, u->y[0], nullptr, u->y[1], s))) return st;
-    if ((st = launch(level_pixels(u, 1) * 32, s, k_pool, (const bf16*)u->y[1], u->p1, n, h, w, 32))) return st;
+    if ((st = launch(level_pixels(u, 1) * 4, s, k_pool, (const bf16*)u->y[1], u->p1, n, h, w, 32))) return st;
     if ((st = conv_layer(u, 2, u->p1, nullptr, u->y[2], s))) return st;
     if ((st = conv_layer(u, 3, u->y[2], nullptr, u->y[3], s))) return st;
-    if ((st = launch(level_pixels(u, 2) * 64, s, k_pool, (const bf16*)u->y[3], u->p2, n, h / 2, w / 2, 64))) return st;
+    if ((st = launch(level_pixels(u, 2) * 8, s, k_pool, (const bf16*)u->y[3], u->p2, n, h / 2, w / 2, 64))) return st;
     if ((st = conv_layer(u, 4, u->p2, nullptr, u->y[4], s))) return st;
     if ((st = conv_layer(u, 5, u->y[4], nullptr, u->y[5], s))) return st;
-    if ((st = launch(level_pixels(u, 1) * 128, s, k_up, (const bf16*)u->y[5], u->u2, n, h / 2, w / 2, 128))) return st;
+    if ((st = launch(level_pixels(u, 1) * 16, s, k_up, (const bf16*)u->y[5], u->u2, n, h / 2, w / 2, 128))) return st;
     if ((st = conv_layer(u, 6, u->u2, u->y[3], u->y[6], s))) return st;
     if ((st = conv_layer(u, 7, u->y[6], nullptr, u->y[7], s))) return st;
-    if ((st = launch(level_pixels(u, 0) * 64, s, k_up, (const bf16*)u->y[7], u->u1, n, h, w, 64))) return st;
+    if ((st = launch(level_pixels(u, 0) * 8, s, k_up, (const bf16*)u->y[7], u->u1, n, h, w, 64))) return st;
     if ((st = conv_layer(u, 8, u->u1, u->y[1], u->y[8], s))) return st;
     if ((st = conv_layer(u, 9, u->y[8], nullptr, u->y[9], s))) return st;
     return launch(level_pixels(u, 0), s, k_head, (const bf16*)u->y[9], (const float*)(u->param + u->hoff),
@@ -868,7 +925,8 @@ int lica_unet_create(lica_unet** out, int32_t n, int32_t h, int32_t w, uint64_t 
     const size_t p0 = level_pixels(u, 0), p1 = level_pixels(u, 1), p2 = level_pixels(u, 2);
     if ((st = dev_alloc(&u->x16, p0 * kIn)) || (st = dev_alloc(&u->p1, p1 * 32)) || (st = dev_alloc(&u->p2, p2 * 64)) ||
         (st = dev_alloc(&u->u2, p1 * 128)) || (st = dev_alloc(&u->u1, p0 * 64)) || (st = dev_alloc(&u->out32, p0)) ||
-        (st = dev_alloc(&u->sigma, n)) || (st = dev_alloc(&u->rr, n)) || (st = dev_alloc(&u->err, 1)))
+        (st = dev_alloc(&u->sigma, n)) || (st = dev_alloc(&u->rms_part, (size_t)n * kRmsParts)) ||
+        (st = dev_alloc(&u->rr, n)) || (st = dev_alloc(&u->err, 1)))
         return fail(st);
     if (cudaMemset(u->err, 0, sizeof(int)) != cudaSuccess) return fail(LICA_ERR_CUDA);
     if ((st = pack_all(u, 0))) return fail(st);
@@ -880,7 +938,7 @@ int lica_unet_create(lica_unet** out, int32_t n, int32_t h, int32_t w, uint64_t 
 int lica_unet_destroy(lica_unet* u) {
     if (!u) return LICA_OK;
     void* ptrs[] = {u->param, u->grad, u->adam_m, u->adam_v, u->x16, u->p1, u->p2, u->u2, u->u1, u->out32,
-                    u->sigma, u->x0, u->ax, u->rr, u->den, u->gout, u->gy, u->gcat, u->dz, u->gsave[0], u->gsave[1],
+                    u->sigma, u->rms_part, u->x0, u->ax, u->rr, u->den, u->gout, u->gy, u->gcat, u->dz, u->gsave[0], u->gsave[1],
                     u->gsave[2], u->gpool, u->part, u->bpart, u->hpart, u->err};
     for (void* p : ptrs) cudaFree(p);
     for (int l = 0; l < kLayers; ++l) {
