@@ -296,8 +296,8 @@ int lica_gpu_lvs_transport_device(int32_t ncol, int32_t n, double length, double
  * concatenated after x0 (c0 channels) along the channels.  The result (+ bias, ReLU when
  * relu != 0) goes to channels [out_c0, out_c0 + cout) of the NHWC tensor out (BF16, out_c
  * channels) and/or out32 (FP32).  c0, c1, cout: multiples of 16 (cout <= 256); the width
- * is a multiple of 128, or divides 128 with the height a multiple of 128 / width.  *err is
- * set to 1 if a bounded wait inside the kernel ran out. */
+ * a multiple of 8, the height of 16.  *err is set to 1 if a bounded wait inside the kernel
+ * ran out. */
 int lica_unet_conv3x3_device(const void* x0, int32_t c0, const void* x1, int32_t c1, const void* w,
                              const float* bias, int32_t n, int32_t h, int32_t wd, int32_t cout, int32_t relu,
                              void* out, float* out32, int32_t out_c, int32_t out_c0, int32_t* err, void* stream);

@@ -89,6 +89,8 @@ int tmem_columns(int cout) {
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
+constexpr int kConvSmemMax = 227 * 1024;
+
 }  // namespace
 
 namespace lica {
@@ -108,17 +110,17 @@ int conv3x3(const __nv_bfloat16* x0, int c0, const __nv_bfloat16* x1, int c1, co
         lica_set_last_error("lica_unet_conv3x3", "arrays must be 16-byte aligned", __FILE__, __LINE__);
         return LICA_BAD_ARG;
     }
-    const int tw = std::min(wd, 128), th = kTileM / tw;
-    if (tw * th != kTileM || wd % tw || h % th) {
-        lica_set_last_error("lica_unet_conv3x3", "image size does not tile by 128 pixels", __FILE__, __LINE__);
+    const int tw = kTileW, th = kTileH;
+    if (wd % tw || h % th) {
+        lica_set_last_error("lica_unet_conv3x3", "image width must be a multiple of 8 and height of 16", __FILE__,
+                            __LINE__);
         return LICA_BAD_ARG;
     }
     static std::once_flag attr_once;
     static cudaError_t attr_err = cudaSuccess;
     static int num_sms = 148;
     std::call_once(attr_once, [] {
-        attr_err = cudaFuncSetAttribute(k_conv3x3_tcp, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)conv_p_smem_bytes(kTileM * 128, 256 * 128));
+        attr_err = cudaFuncSetAttribute(k_conv3x3_tcp, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmemMax);
         int dev = 0;
         if (attr_err == cudaSuccess) attr_err = cudaGetDevice(&dev);
         if (attr_err == cudaSuccess) attr_err = cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
@@ -140,10 +142,10 @@ int conv3x3(const __nv_bfloat16* x0, int c0, const __nv_bfloat16* x1, int c1, co
     P.err = err;
     CUtensorMap mx0, mx1, mw0, mw1;
     int st;
-    if ((st = act_map(&mx0, x0, c0, wd, h, n, P.cblk[0], tw, th))) return st;
+    if ((st = act_map(&mx0, x0, c0, wd, h, n, P.cblk[0], tw, th + 2))) return st;
     if ((st = weight_map(&mw0, w, 9 * P.ctot, cout, P.cblk[0]))) return st;
     if (P.nsrc > 1) {
-        if ((st = act_map(&mx1, x1, c1, wd, h, n, P.cblk[1], tw, th))) return st;
+        if ((st = act_map(&mx1, x1, c1, wd, h, n, P.cblk[1], tw, th + 2))) return st;
         if ((st = weight_map(&mw1, w, 9 * P.ctot, cout, P.cblk[1]))) return st;
     } else {
         mx1 = mx0;
@@ -151,10 +153,12 @@ int conv3x3(const __nv_bfloat16* x0, int c0, const __nv_bfloat16* x1, int c1, co
     }
     const int tiles = n * (h / th) * (wd / tw);
     const int cbmax = std::max(P.cblk[0], P.nsrc > 1 ? P.cblk[1] : 0);
-    P.stage_a = kTileM * cbmax * 2;
-    P.stage_b = ((cout * cbmax * 2 + 1023) / 1024) * 1024;
+    P.stage_a = ((kHaloRows * cbmax * 2 + 1023) / 1024) * 1024;
+    P.stage_b = ((3 * cout * cbmax * 2 + 1023) / 1024) * 1024;
     P.tiles = tiles;
-    const size_t smem = conv_p_smem_bytes(P.stage_a, P.stage_b);
+    P.nstages = std::min<int>(kStages, (int)((kConvSmemMax - 1024 - 256) / (P.stage_a + P.stage_b)));
+    if (P.nstages < 1) return LICA_BAD_ARG;
+    const size_t smem = conv_p_smem_bytes(P.stage_a, P.stage_b, P.nstages);
     // CTAs per SM: shared memory and tensor memory (two accumulators of tmem_cols each)
     int per_sm = 0;
     LICA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv3x3_tcp, kConvThreads, smem));

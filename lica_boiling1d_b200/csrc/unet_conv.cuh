@@ -7,7 +7,10 @@
 // block) is a second box copy.  Up to two input tensors are concatenated along the
 // channels (the decoder's [upsampled, skip] input) without being materialised.
 //
-// A tile is 128 pixels (th rows x tw columns of one image).  Persistent CTAs of 6 warps
+// A tile is 16 x 8 pixels of one image.  Per (dx, channel block) one TMA box of 18 x 8
+// pixels (the tile shifted by dx, with one row of halo above and below) serves the three
+// taps dy = 0, 1, 2: 8 pixel rows are one swizzle atom, so the A operand of tap dy starts
+// dy atoms into the box.  Persistent CTAs of 6 warps
 // walk the tiles t = blockIdx.x, + gridDim.x, ...:
 //   warp 4 lane 0 : TMA producer, streaming the K blocks of consecutive tiles through a
 //                   ring of kStages stages (full/empty mbarriers) without draining it
@@ -16,8 +19,8 @@
 //                   tile overlaps the MMAs of the next
 //   warps 0-3     : epilogue, tensor memory -> registers (warp w reads lanes 32w..32w+31
 //                   = pixels), + bias, optional ReLU, BF16 NHWC store (optionally FP32)
-// Stage sizes follow the layer's channel block (A: 128 x cblk, B: cout x cblk BF16), so
-// narrow layers keep several CTAs per SM.
+// Stage sizes follow the layer's channel block (A: 144 x cblk, B: 3 x cout x cblk BF16),
+// so narrow layers keep several CTAs per SM.
 #pragma once
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -29,6 +32,8 @@ namespace unet {
 
 constexpr int kStages = 4;
 constexpr int kTileM = 128;
+constexpr int kTileW = 8, kTileH = 16;          // pixel tile: 16 rows x 8 columns
+constexpr int kHaloRows = kTileW * (kTileH + 2);  // A box: 18 rows x 8 columns = 144 pixel rows
 
 struct ConvParams {
     int n, h, w;          // image count and size (output = input size)
@@ -45,13 +50,14 @@ struct ConvParams {
     float* out32;         // NHWC FP32 output (or null)
     int* err;             // set to 1 when a bounded wait runs out
     int stage_a, stage_b; // bytes of one pipeline stage's A and B tiles (multiples of 1 KB)
+    int nstages;          // stages in the ring (<= kStages; fewer for wide layers)
     int tiles;            // pixel tiles of the whole launch
 };
 
 constexpr int kConvThreads = 192;
 
-__host__ __device__ inline size_t conv_p_smem_bytes(int stage_a, int stage_b) {
-    return 1024 + (size_t)kStages * (stage_a + stage_b) + 256;
+__host__ __device__ inline size_t conv_p_smem_bytes(int stage_a, int stage_b, int nstages) {
+    return 1024 + (size_t)nstages * (stage_a + stage_b) + 256;
 }
 
 __device__ __forceinline__ void tile_origin(const ConvParams& P, int t, int& img, int& x0, int& y0) {
@@ -71,8 +77,9 @@ __global__ void __launch_bounds__(kConvThreads, 1)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char* base = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char* sa = base;
-    unsigned char* sb = base + kStages * P.stage_a;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sb + kStages * P.stage_b);
+    const int NS = P.nstages;
+    unsigned char* sb = base + NS * P.stage_a;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sb + NS * P.stage_b);
     uint64_t* full = bars;
     uint64_t* empty = bars + kStages;
     uint64_t* tfull = bars + 2 * kStages;   // [2]: accumulator ready for the epilogue
@@ -104,7 +111,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
     const uint32_t tmem = *tmem_slot;
 
     const int nb0 = P.cin[0] / P.cblk[0], nb1 = P.nsrc > 1 ? P.cin[1] / P.cblk[1] : 0;
-    const int nkb = 9 * (nb0 + nb1);
+    const int nkb = 3 * (nb0 + nb1);  // K blocks: (dx, source, channel block); dy inside
 
     if (warp == 4) {
         if (lane == 0) {
@@ -113,25 +120,27 @@ __global__ void __launch_bounds__(kConvThreads, 1)
             for (int t = blockIdx.x; t < P.tiles && ok; t += gridDim.x) {
                 int img, x0, y0;
                 tile_origin(P, t, img, x0, y0);
-                int tap = 0, src = 0, cb = 0;
+                int dx = 0, src = 0, cb = 0;
                 for (int kb = 0; kb < nkb; ++kb, ++g) {
-                    const int s = g % kStages, u = g / kStages;
-                    if (g >= kStages && !tc::mbar_wait(&empty[s], (u - 1) & 1)) {
+                    const int s = g % NS, u = g / NS;
+                    if (g >= NS && !tc::mbar_wait(&empty[s], (u - 1) & 1)) {
                         atomicExch(P.err, 1);
                         ok = false;
                         break;
                     }
                     const int cblk = P.cblk[src];
-                    tc::mbar_expect_tx(&full[s], (uint32_t)(kTileM + P.cout) * cblk * 2);
-                    const int dy = tap / 3, dx = tap - 3 * dy;
+                    const int bsub = P.cout * cblk * 2;  // bytes of one tap's weight slice
+                    tc::mbar_expect_tx(&full[s], (uint32_t)(kHaloRows + 3 * P.cout) * cblk * 2);
                     const void* tmx = src ? (const void*)&tm_x1 : (const void*)&tm_x0;
                     const void* tmw = src ? (const void*)&tm_w1 : (const void*)&tm_w0;
-                    tc::tma_load_4d(sa + s * P.stage_a, tmx, &full[s], cb * cblk, x0 + dx - 1, y0 + dy - 1, img);
-                    tc::tma_load_2d(sb + s * P.stage_b, tmw, &full[s], tap * P.ctot + (src ? P.cin[0] : 0) + cb * cblk,
-                                    0);
+                    // 8 x 18 pixels (the tile and one row above and below), shifted by dx
+                    tc::tma_load_4d(sa + s * P.stage_a, tmx, &full[s], cb * cblk, x0 + dx - 1, y0 - 1, img);
+                    const int col = (src ? P.cin[0] : 0) + cb * cblk;
+                    for (int dy = 0; dy < 3; ++dy)
+                        tc::tma_load_2d(sb + s * P.stage_b + dy * bsub, tmw, &full[s], (3 * dy + dx) * P.ctot + col, 0);
                     if (++cb == (src ? nb1 : nb0)) {
                         cb = 0;
-                        if (++src == P.nsrc) { src = 0; ++tap; }
+                        if (++src == P.nsrc) { src = 0; ++dx; }
                     }
                 }
             }
@@ -151,7 +160,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                 const uint32_t d = tmem + (uint32_t)(acc * P.tmem_cols);
                 int src = 0, cb = 0;
                 for (int kb = 0; kb < nkb; ++kb, ++g) {
-                    const int s = g % kStages, u = g / kStages;
+                    const int s = g % NS, u = g / NS;
                     if (!tc::mbar_wait(&full[s], u & 1)) {
                         atomicExch(P.err, 1);
                         ok = false;
@@ -160,10 +169,14 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                     tc::tc_fence_after();
                     const int cblk = P.cblk[src];
                     const uint32_t rb = (uint32_t)cblk * 2;
-                    const uint64_t da = tc::smem_desc(sa + s * P.stage_a, rb);
-                    const uint64_t db = tc::smem_desc(sb + s * P.stage_b, rb);
-                    for (int k = 0; k < cblk / 16; ++k)
-                        tc::mma_bf16(d, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, (kb | k) != 0);
+                    // tap dy: the A operand starts dy rows of the tile (8 pixel rows = one
+                    // swizzle atom) further into the halo box
+                    for (int dy = 0; dy < 3; ++dy) {
+                        const uint64_t da = tc::smem_desc(sa + s * P.stage_a + dy * 8 * (int)rb, rb);
+                        const uint64_t db = tc::smem_desc(sb + s * P.stage_b + dy * P.cout * (int)rb, rb);
+                        for (int k = 0; k < cblk / 16; ++k)
+                            tc::mma_bf16(d, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, (kb | dy | k) != 0);
+                    }
                     tc::mma_commit(&empty[s]);
                     if (++cb == (src ? nb1 : nb0)) {
                         cb = 0;

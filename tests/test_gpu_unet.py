@@ -33,7 +33,7 @@ def _ref(x, w, bias, relu):
     (1, 16, 32, 128, 64, 64, 1),    # decoder input: [upsampled, skip]
     (1, 32, 16, 64, 32, 32, 0),     # two sources with different swizzles
     (1, 16, 16, 64, 0, 192, 0),     # N = 192 (256 tensor-memory columns)
-    (1, 4, 256, 32, 0, 16, 1),      # 128 x 1 tiles
+    (2, 48, 24, 32, 0, 16, 1),      # several tiles per image, N = 16
 ])
 def test_conv3x3_tensor_core(n, h, wd, c0, c1, cout, relu):
     import torch
