@@ -465,6 +465,20 @@ def run_ours(args):
         variants["mixed"] = {"value": ke / (mms / 1e3), "unit": UNIT, "iterations": itm[-1],
                              "note": "FP32 smoothing/restriction/prolongation, FP64 residual, CG and coarsest solve"}
         sm.close()
+        if not args.skip_learned:
+            lg = learned_leg(args, dev, case, n, nlevels, f, bx, by, p, flush, stream, ke)
+            if "unavailable" in lg:
+                variants["learned"] = lg
+            else:
+                its0 = its[-1]
+                variants["learned"] = {
+                    "value": lg["fp64"]["value"], "unit": UNIT, "iterations": lg["fp64"]["iterations"],
+                    "vcycles_saved": its0 - lg["fp64"]["iterations"], "guess": lg["guess"],
+                    "note": "FP64 MG-PCG from the U-Net guess (guess + check + solve per step)"}
+                variants["mixed_learned"] = {
+                    "value": lg["mixed"]["value"], "unit": UNIT, "iterations": lg["mixed"]["iterations"],
+                    "vcycles_saved": itm[-1] - lg["mixed"]["iterations"],
+                    "note": "mixed-precision MG-PCG from the U-Net guess (guess + check + solve per step)"}
 
     if rank == 0 and world == 1 and not args.skip_cpu and n == N:
         threads = os.cpu_count()
@@ -473,6 +487,85 @@ def run_ours(args):
                "sample": f"{len(times)} complete solves of the same workload (~15 s), FP64 C++/OpenMP restatement"}
 
     return finish(args, locals())
+
+
+UNET_LAYERS = [(16, 0, 32, 0), (32, 0, 32, 0), (32, 0, 64, 1), (64, 0, 64, 1), (64, 0, 128, 2), (128, 0, 128, 2),
+               (128, 64, 64, 1), (64, 0, 64, 1), (64, 32, 32, 0), (32, 0, 32, 0)]
+
+
+def unet_flops(n):
+    """Tensor-core FLOPs of one U-Net guess at n x n (the executed 3x3 MMAs, layer 0's 16
+    padded input channels included) plus the 1x1 head."""
+    tot = sum(2.0 * (n >> lv) ** 2 * 9 * (c0 + c1) * co for c0, c1, co, lv in UNET_LAYERS)
+    return tot + 2.0 * n * n * 32
+
+
+def learned_leg(args, dev, case, n, nlevels, f, bx, by, p, flush, stream, reps):
+    """The learned initial guess (shipped weights, trained by the project's own kernels)
+    feeding the FP64 and the mixed-precision MG-PCG to the same tolerance; each timed step
+    is guess + residual check (zero fallback) + solve."""
+    import torch
+
+    from lica_boiling1d_b200 import poisson, train_guess
+    from lica_boiling1d_b200.unet import LearnedGuess
+    if not os.path.exists(train_guess.WEIGHTS):
+        return {"unavailable": "no trained weights in the package"}
+    net = LearnedGuess(1, n, n)
+    train_guess.load(net)
+    rho = torch.from_numpy(case.rho[None].copy()).to(dev)
+    F, BX, BY = f[None], bx[None], by[None]
+    x0 = torch.empty_like(F)
+    out = {}
+    # the guess alone
+    for _ in range(3):
+        net.guess(rho, F, case.hx * case.hy, out=x0)
+    evg = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    for k in range(reps):
+        flush.fill_(k & 0xFF)
+        evg[k][0].record(stream)
+        net.guess(rho, F, case.hx * case.hy, out=x0)
+        evg[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    gms = sum(a.elapsed_time(b) for a, b in evg) / reps
+    fl = unet_flops(n)
+    peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peak = float(json.load(fh)["bf16_tflops"])
+        peak_src = "measured (cuBLAS bf16 burst)"
+    except Exception:
+        peak, peak_src = 1590.0, "fallback"
+    ach = fl / (gms / 1e3) / 1e12
+    out["guess"] = {"ms": gms, "gflop": fl / 1e9,
+                    "roofline": {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                                 "frac": ach / peak, "peak_source": peak_src},
+                    "note": "10 tcgen05 convolutions (BF16, FP32 accumulate) + pooling/upsampling/head"}
+    _, rel0 = net.guess_checked(rho, F, BX, BY, case.hx, case.hy, out=x0)
+    out["guess"]["rel_residual"] = float(rel0[0])
+    for prec in ("fp64", "mixed"):
+        s = poisson.MultigridPoisson(n, n, case.hx, case.hy, nlevels=nlevels, ncoarse=args.ncoarse, precision=prec)
+        for _ in range(3):
+            net.guess_checked(rho, F, BX, BY, case.hx, case.hy, out=x0)
+            p.copy_(x0[0])
+            s.solve(p, f, bx, by, rtol=RTOL)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+        its = []
+        for k in range(reps):
+            flush.fill_(k & 0xFF)
+            evs[k][0].record(stream)
+            net.guess_checked(rho, F, BX, BY, case.hx, case.hy, out=x0)
+            p.copy_(x0[0])
+            it, rel, st = s.solve(p, f, bx, by, rtol=RTOL)
+            evs[k][1].record(stream)
+            its.append(it)
+            if st != 0:
+                raise RuntimeError(f"solve from the learned guess: status {st}")
+        torch.cuda.synchronize(dev)
+        ms = sum(a.elapsed_time(b) for a, b in evs)
+        out[prec] = {"value": reps / (ms / 1e3), "unit": UNIT, "iterations": its[-1], "rel_residual": rel}
+        s.close()
+    net.close()
+    return out
 
 
 def finish(args, v):
@@ -514,6 +607,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end and later legs (profiling runs)")
     ap.add_argument("--no-profile", action="store_true", help="skip the kernel-class timing and later legs")
     ap.add_argument("--skip-rk3", action="store_true", help="skip the RK3 column legs")
+    ap.add_argument("--skip-learned", action="store_true", help="skip the learned-guess legs")
     ap.add_argument("--c1-steps", type=int, default=200, help="timed steps of the 512-cell column")
     ap.add_argument("--c4-steps", type=int, default=20, help="timed steps of the 4096-column batch")
     ap.add_argument("--profile-batch", type=int, default=0,

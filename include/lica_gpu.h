@@ -326,6 +326,10 @@ int64_t lica_unet_param_count(const lica_unet* net);
 int lica_unet_get_params(lica_unet* net, float* host, int64_t count);
 int lica_unet_set_params(lica_unet* net, const float* host, int64_t count);
 int lica_unet_guess_device(lica_unet* net, const double* rho, const double* f, double hsq, double* x0, void* stream);
+/* The guess with its relative residual ||f - A x0|| / ||f|| per image in rel0 (host
+ * array of n); an image whose guess is no better than zero gets x0 = 0 (the fallback). */
+int lica_unet_guess_checked_device(lica_unet* net, const double* rho, const double* f, const double* bx,
+                                   const double* by, double hx, double hy, double* x0, double* rel0, void* stream);
 int lica_unet_grad_device(lica_unet* net, const double* rho, const double* f, double hsq, const double* gx0,
                           float* grad_host, int64_t count, void* stream);
 int lica_unet_train_step_device(lica_unet* net, const double* rho, const double* f, const double* bx,

@@ -984,6 +984,35 @@ int lica_unet_guess_device(lica_unet* u, const double* rho, const double* f, dou
     return check_err(u, s);
 }
 
+int lica_unet_guess_checked_device(lica_unet* u, const double* rho, const double* f, const double* bx,
+                                   const double* by, double hx, double hy, double* x0, double* rel0, void* stream) {
+    if (!u || !rho || !f || !bx || !by || !x0 || !rel0 || !(hx > 0) || !(hy > 0)) return LICA_BAD_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    int st;
+    const size_t p0 = level_pixels(u, 0);
+    if (!u->ax) {
+        if ((st = dev_alloc(&u->ax, p0))) return st;
+    }
+    if ((st = forward(u, rho, f, hx * hy, x0, s))) return st;
+    if ((st = launch(p0, s, k_apply_op, (const double*)x0, bx, by, u->ax, u->n, u->h, u->w, 1.0 / (hx * hx),
+                     1.0 / (hy * hy))))
+        return st;
+    const int npix = u->h * u->w;
+    k_residual<<<u->n, 1024, 0, s>>>(f, u->ax, u->rr, npix);
+    LICA_CUDA_TRY(cudaGetLastError());
+    lica_count_launches(1);
+    std::vector<double> rr(u->n), sg(u->n);
+    LICA_CUDA_TRY(cudaMemcpyAsync(rr.data(), u->rr, sizeof(double) * u->n, cudaMemcpyDeviceToHost, s));
+    LICA_CUDA_TRY(cudaMemcpyAsync(sg.data(), u->sigma, sizeof(double) * u->n, cudaMemcpyDeviceToHost, s));
+    if ((st = check_err(u, s))) return st;
+    for (int i = 0; i < u->n; ++i) {
+        rel0[i] = sqrt(rr[i] / (sg[i] * sg[i] * npix));
+        if (!(rel0[i] < 1.0))  // no better than zero (or not finite): start from zero
+            LICA_CUDA_TRY(cudaMemsetAsync(x0 + (size_t)i * npix, 0, sizeof(double) * npix, s));
+    }
+    return LICA_OK;
+}
+
 int lica_unet_grad_device(lica_unet* u, const double* rho, const double* f, double hsq, const double* gx0,
                           float* grad_host, int64_t count, void* stream) {
     if (!u || !rho || !f || !gx0 || !grad_host || count != (int64_t)u->nparams || !(hsq > 0)) return LICA_BAD_ARG;

@@ -87,6 +87,8 @@ SIGNATURES = {
     "lica_unet_get_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int64]),
     "lica_unet_set_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int64]),
     "lica_unet_guess_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]),
+    "lica_unet_guess_checked_device": (C.c_int, [C.c_void_p] * 5 + [C.c_double, C.c_double, C.c_void_p, _D,
+                                                                      C.c_void_p]),
     "lica_unet_grad_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p,
                                         C.POINTER(C.c_float), C.c_int64, C.c_void_p]),
     "lica_unet_train_step_device": (C.c_int, [C.c_void_p] + [C.c_void_p] * 5 + [C.c_double, C.c_double, C.c_float,

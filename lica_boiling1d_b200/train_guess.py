@@ -86,11 +86,8 @@ def iterations(n, problems, guess_net=None, rtol=1e-10, nlevels=None, precision=
         p = torch.zeros_like(F)
         if guess_net is not None:
             R = torch.from_numpy(np.ascontiguousarray(rho)).cuda()
-            g = guess_net.guess(R[None], F[None], 1.0 / n ** 2)[0].contiguous()
-            ag = torch.empty_like(g)
-            s.apply(ag, g, BX, BY)
-            if torch.linalg.norm(F - ag) < torch.linalg.norm(F):  # else: fall back to zero
-                p.copy_(g)
+            g, _ = guess_net.guess_checked(R[None], F[None], BX[None], BY[None], 1.0 / n, 1.0 / n)
+            p.copy_(g[0])
         it, rel, st = s.solve(p, F, BX, BY, rtol=rtol, max_iters=200)
         out.append((it, rel, st))
     s.close()

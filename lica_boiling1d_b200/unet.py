@@ -85,6 +85,19 @@ class LearnedGuess:
                                                          self._stream(stream)), "lica_unet_guess_device")
         return out
 
+    def guess_checked(self, rho, f, bx, by, hx, hy, out=None, stream=None):
+        """The guess and its relative residual per image; images whose guess is no better
+        than zero get x0 = 0.  Returns (x0, rel0 numpy array)."""
+        import numpy as np
+        import torch
+        if out is None:
+            out = torch.empty_like(f)
+        rel = np.empty(self.n)
+        native.check(native.lib().lica_unet_guess_checked_device(
+            self._h, _ptr(rho), _ptr(f), _ptr(bx), _ptr(by), float(hx), float(hy), _ptr(out),
+            rel.ctypes.data_as(C.POINTER(C.c_double)), self._stream(stream)), "lica_unet_guess_checked_device")
+        return out, rel
+
     def grad(self, rho, f, hsq, gx0, stream=None):
         import numpy as np
         g = np.empty(self.nparams, dtype=np.float32)
