@@ -568,6 +568,34 @@ def learned_leg(args, dev, case, n, nlevels, f, bx, by, p, flush, stream, reps):
     return out
 
 
+def profile_guess(reps):
+    """A few U-Net guesses on the 1024 x 1024 workload (for ncu captures of the tensor-core
+    convolutions); prints the mean guess time."""
+    import torch
+
+    from lica_boiling1d_b200 import train_guess
+    from lica_boiling1d_b200.inputs import bubble_poisson_case
+    from lica_boiling1d_b200.unet import LearnedGuess
+    case = bubble_poisson_case(N)
+    net = LearnedGuess(1, N, N)
+    if os.path.exists(train_guess.WEIGHTS):
+        train_guess.load(net)
+    rho = torch.from_numpy(case.rho[None].copy()).cuda()
+    f = torch.from_numpy(case.f[None].copy()).cuda()
+    x0 = torch.empty_like(f)
+    net.guess(rho, f, case.hx * case.hy, out=x0)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        net.guess(rho, f, case.hx * case.hy, out=x0)
+    b.record()
+    torch.cuda.synchronize()
+    print(f"U-Net guess {N}x{N}: {a.elapsed_time(b) / reps:.3f} ms over {reps} guesses "
+          f"({unet_flops(N) / 1e9:.1f} GFLOP each)")
+    net.close()
+
+
 def finish(args, v):
     import torch.distributed as dist
     if v["rank"] == 0:
@@ -608,6 +636,8 @@ def main():
     ap.add_argument("--no-profile", action="store_true", help="skip the kernel-class timing and later legs")
     ap.add_argument("--skip-rk3", action="store_true", help="skip the RK3 column legs")
     ap.add_argument("--skip-learned", action="store_true", help="skip the learned-guess legs")
+    ap.add_argument("--profile-guess", type=int, default=0,
+                    help="only run this many U-Net guesses at 1024x1024 (profiling) and exit")
     ap.add_argument("--c1-steps", type=int, default=200, help="timed steps of the 512-cell column")
     ap.add_argument("--c4-steps", type=int, default=20, help="timed steps of the 4096-column batch")
     ap.add_argument("--profile-batch", type=int, default=0,
@@ -621,6 +651,9 @@ def main():
         args.warmup = 3
     if args.profile_batch:
         profile_batch(args.profile_batch, args.c4_steps, args.threads)
+        return
+    if args.profile_guess:
+        profile_guess(args.profile_guess)
         return
     if args.impl == "reference":
         run_reference(args)
