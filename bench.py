@@ -465,6 +465,32 @@ def run_ours(args):
         variants["mixed"] = {"value": ke / (mms / 1e3), "unit": UNIT, "iterations": itm[-1],
                              "note": "FP32 smoothing/restriction/prolongation, FP64 residual, CG and coarsest solve"}
         sm.close()
+        if not args.skip_2048 and n == N:
+            c2 = bubble_poisson_case(2 * N)
+            f2, bx2, by2 = t(c2.f), t(c2.bx), t(c2.by)
+            p2 = torch.zeros_like(f2)
+            for prec in ("fp64", "mixed"):
+                s2 = poisson.MultigridPoisson(2 * N, 2 * N, c2.hx, c2.hy, nlevels=nlevels + 1, ncoarse=args.ncoarse,
+                                              precision=prec)
+                for _ in range(3):
+                    p2.zero_()
+                    s2.solve(p2, f2, bx2, by2, rtol=RTOL)
+                ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                       for _ in range(ke)]
+                it2 = []
+                for k in range(ke):
+                    flush.fill_(k & 0xFF)
+                    p2.zero_()
+                    ev2[k][0].record(stream)
+                    it2.append(s2.solve(p2, f2, bx2, by2, rtol=RTOL)[0])
+                    ev2[k][1].record(stream)
+                torch.cuda.synchronize(dev)
+                ms2 = sum(a.elapsed_time(b) for a, b in ev2)
+                variants[f"{prec}_2048"] = {"value": ke / (ms2 / 1e3), "unit": UNIT, "iterations": it2[-1],
+                                            "note": "the same 64 bubbles in the unit domain at 2048x2048 (radii "
+                                                    "16-96 cells), 7 levels"}
+                s2.close()
+            del f2, bx2, by2, p2
         if not args.skip_learned:
             lg = learned_leg(args, dev, case, n, nlevels, f, bx, by, p, flush, stream, ke)
             if "unavailable" in lg:
@@ -636,6 +662,7 @@ def main():
     ap.add_argument("--no-profile", action="store_true", help="skip the kernel-class timing and later legs")
     ap.add_argument("--skip-rk3", action="store_true", help="skip the RK3 column legs")
     ap.add_argument("--skip-learned", action="store_true", help="skip the learned-guess legs")
+    ap.add_argument("--skip-2048", action="store_true", help="skip the 2048x2048 solves")
     ap.add_argument("--profile-guess", type=int, default=0,
                     help="only run this many U-Net guesses at 1024x1024 (profiling) and exit")
     ap.add_argument("--c1-steps", type=int, default=200, help="timed steps of the 512-cell column")
