@@ -72,7 +72,8 @@ struct Args {
     double* dscr;
     int* iscr;
     long long* prof;   // optional per-phase cycle totals (PH_COUNT per column) or null
-    int tri_smem;      // 1: the tridiagonal arrays live in dynamic shared memory
+    int tri_smem;      // 1: the tridiagonal arrays of columns with n <= tri_cap live in dynamic shared memory
+    int tri_cap;       // longest column whose arrays fit the dynamic shared memory (longer ones use scratch)
 };
 
 // phases of the optional cycle profile
@@ -1322,7 +1323,7 @@ __global__ void __launch_bounds__(NTH, 1) k_column_steps(const __grid_constant__
     double* d = A.dscr + od;
     for (int q = 0; q < NFLOW; ++q) c.a[q] = d + q * sf;
     c.psif_mtp = d + NFLOW * sf;
-    if (A.tri_smem) {
+    if (A.tri_smem && n <= A.tri_cap) {
         // the Thomas coefficient, right-hand-side and elimination arrays: thread 0 walks
         // them sequentially, so they are kept at shared-memory latency
         c.a[S_AK] = dsm;
@@ -1579,12 +1580,25 @@ bool state_ok(const lica_col_state* st) {
 
 // Launch A over A.ncol CTAs of `threads` threads; nmax = the largest column, which sizes
 // the shared-memory tridiagonal arrays.
+template <int NTH>
+int column_ctas_by_registers() {
+    int occ = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, colk::k_column_steps<NTH>, NTH, 0);
+    return std::max(occ, 1);
+}
+
 int launch_columns(colk::Args& A, int nmax, int threads, void* stream) {
-    const size_t tri_bytes = 5 * ((size_t)nmax + 2) * sizeof(double);
-    const size_t kMaxDyn = 227 * 1024 - sizeof(colk::Shared) - 1024;
-    A.tri_smem = tri_bytes <= kMaxDyn ? 1 : 0;
-    const size_t dyn = A.tri_smem ? tri_bytes : 0;
     const int nth = (threads == 64 || threads == 256) ? threads : colk::NT_DEFAULT;
+    // Shared-memory tridiagonal arrays for columns up to tri_cap cells, sized so that the
+    // CTAs the registers allow per SM still fit (longer columns keep them in scratch; the
+    // arithmetic is the same either way).
+    const int ctas = nth == 64 ? column_ctas_by_registers<64>()
+                               : (nth == 128 ? column_ctas_by_registers<128>() : column_ctas_by_registers<256>());
+    const long budget = (long)(228 * 1024) / ctas - (long)sizeof(colk::Shared) - 2048;
+    const long cap = std::min<long>(nmax, budget / (5 * (long)sizeof(double)) - 2);
+    A.tri_cap = cap >= 64 ? (int)cap : 0;
+    A.tri_smem = A.tri_cap > 0 ? 1 : 0;
+    const size_t dyn = A.tri_smem ? 5 * ((size_t)A.tri_cap + 2) * sizeof(double) : 0;
     {
         static std::mutex mu;
         static size_t set_bytes[3] = {0, 0, 0};

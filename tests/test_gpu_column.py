@@ -101,3 +101,27 @@ def test_uneven_batch():
             got = dev.column(c)
             for k, v in r.items():
                 assert np.array_equal(got[k], v), (call, c, k)
+
+
+def test_long_columns_with_tridiagonal_arrays_in_scratch():
+    """Columns longer than the shared-memory cap of a 64-thread launch keep their Thomas
+    arrays in global scratch: still bit-identical to the oracle, beside short columns that
+    use shared memory in the same launch."""
+    import torch
+    from lica_boiling1d_b200.column import ColumnBatch, uneven_batch
+    n, length, z0, props = uneven_batch(3, seed=11, nmin=1200, nmax=1600)
+    n = np.concatenate([n, [96, 128]])
+    length = np.concatenate([length, [96 / 512, 128 / 512]])
+    z0 = np.concatenate([z0, [0.1 * 96 / 512 + 0.37 / 512, 0.1 * 128 / 512 + 0.37 / 512]])
+    props = list(props) + [props[0], props[1]]
+    dev = ColumnBatch.films(n, length, z0, props).to("cuda")
+    refs = [O.col_init(int(n[c]), float(length[c]), float(z0[c]), props[c]) for c in range(len(n))]
+    status = dev.steps(2, threads=64)
+    torch.cuda.synchronize()
+    assert int(status.abs().max()) == 0
+    for c, r in enumerate(refs):
+        for _ in range(2):
+            assert O.col_step(r, int(n[c]), float(length[c]), props[c]) == 0
+        got = dev.column(c)
+        for k, v in r.items():
+            assert np.array_equal(got[k], v), (c, k)
