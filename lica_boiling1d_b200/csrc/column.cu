@@ -1271,7 +1271,9 @@ __device__ int column_step(const Geo& g, const Phys& ph, Col& c, Shared& sh, dou
 // NTH threads per column; one CTA per SM is enough for the register budget the sequential
 // parts want (no spills), more columns per SM come from smaller NTH.
 template <int NTH>
-__global__ void __launch_bounds__(NTH, 1) k_column_steps(const __grid_constant__ Args A) {
+// The 64-thread form is bounded for 5 CTAs per SM (about 200 registers): latency-bound
+// columns gain more from columns in flight than they lose to a few spilled registers.
+__global__ void __launch_bounds__(NTH, NTH == 64 ? 5 : 1) k_column_steps(const __grid_constant__ Args A) {
     __shared__ Shared sh;
     extern __shared__ double dsm[];   // 5 (n+2) doubles when A.tri_smem
     if ((int)blockIdx.x >= A.ncol) return;
