@@ -219,10 +219,10 @@ def profile_batch(ncol, steps, threads):
                       "cells": int(n.sum()), "status": int(st.max())}), flush=True)
 
 
-def rk3_legs(dev, flush, steps_c1=200, steps_c4=20, warmup=3):
+def rk3_legs(dev, flush, steps_c1=200, steps_c4=20, warmup=3, rank=0, world=1, slowest=lambda x: x):
     import torch
 
-    from lica_boiling1d_b200 import native
+    from lica_boiling1d_b200 import native, shard
     from lica_boiling1d_b200.column import ColumnBatch, Columns, uneven_batch
     out = {}
     props = c1_props()
@@ -261,9 +261,12 @@ def rk3_legs(dev, flush, steps_c1=200, steps_c4=20, warmup=3):
     out["column_512"]["e2e"] = {"steps_per_s": ke / e2e_s, "h2d_bytes_per_step": bytes_state,
                                 "d2h_bytes_per_step": bytes_state,
                                 "path": "lica_gpu_column_steps (C ABI), host arrays, one step per call"}
-    # C4: the uneven batch, CTA width picked by a short trial of each candidate
-    n, length, z0, bprops = uneven_batch(C4_NCOL, seed=0)
-    batch = ColumnBatch.films(n, length, z0, bprops).to(dev)
+    # C4: the uneven batch (over N ranks: contiguous blocks balanced by cells, no collective
+    # per step), CTA width picked by a short trial of each candidate
+    n_all, length, z0, bprops = uneven_batch(C4_NCOL, seed=0)
+    lo, hi = shard.partition(n_all, world)[rank]
+    n = n_all[lo:hi]
+    batch = ColumnBatch.films(n, length[lo:hi], z0[lo:hi], bprops[lo:hi]).to(dev)
     trial = {}
     for th in (64, 128):
         b = batch.to(dev)
@@ -288,14 +291,21 @@ def rk3_legs(dev, flush, steps_c1=200, steps_c4=20, warmup=3):
     launches = native.launch_count() - l0
     if int(st.max()) != 0:
         raise RuntimeError(f"batch status {int(st.max())}")
-    ms = e0.elapsed_time(e1)
-    cells = int(n.sum())
+    ms = slowest(e0.elapsed_time(e1))
+    cells = int(n_all.sum())
+    # the one gather at the end: interface height and vapour volume of every column
+    fin = batch.to(None).arrays
+    hist = shard.gather_histories([(lo + c, float(fin["stats"][c][5]), float(fin["scal"][c][4]))
+                                   for c in range(len(n))], world)
     out["batch_4096"] = {
         "workload": f"{C4_NCOL} independent 1-D boiling columns, uneven 128-2048 flow cells (seeded, {cells} in "
-                    "total), superheat 2-20 K, density ratio 100-1600, FP64, one persistent launch, longest first",
+                    "total), superheat 2-20 K, density ratio 100-1600, FP64, one persistent launch per rank, "
+                    "longest first",
         "steps_per_s": steps_c4 / (ms / 1e3), "ms_per_step": ms / steps_c4, "steps": steps_c4,
         "column_steps_per_s": C4_NCOL * steps_c4 / (ms / 1e3), "cell_updates_per_s": cells * steps_c4 / (ms / 1e3),
-        "threads": th, "autotune_ms_per_step": trial, "gpu_launches": launches}
+        "threads": th, "autotune_ms_per_step": trial, "gpu_launches": launches,
+        "ranks": world, "sharding": "contiguous column blocks balanced by cells, strong scaling of the fixed batch",
+        "gathered_columns": len(hist)}
     return out
 
 
@@ -311,7 +321,7 @@ ALG_BYTES_PER_CELL = {  # FP64, level 0: each distinct array read or written onc
 # DRAM bytes per level-0 launch from one ncu capture at 1024x1024 FP64
 # (dram__bytes_read.sum + dram__bytes_write.sum; profiles/mg_k_down_k_up_level0_1024_fp64.md),
 # scaled by cells for other sizes.
-NCU_DRAM_BYTES_1024 = {"down0": 33.587456e6 + 0.027392e6, "up0": 44.082944e6 + 0.560128e6}
+NCU_DRAM_BYTES_1024 = {"down0": 33.571840e6 + 0.037888e6, "up0": 44.064768e6 + 0.158976e6}
 
 
 def run_ours(args):
@@ -388,7 +398,8 @@ def run_ours(args):
     e2e, roofline, variants, cpu = None, None, {}, None
     rk3 = None
     if not args.skip_rk3:
-        rk3 = rk3_legs(dev, flush, steps_c1=args.c1_steps, steps_c4=args.c4_steps)
+        rk3 = rk3_legs(dev, flush, steps_c1=args.c1_steps, steps_c4=args.c4_steps, rank=rank, world=world,
+                       slowest=slowest)
         if rank == 0 and world == 1 and not args.skip_cpu:
             rk3["cpu_baseline"] = rk3_cpu()
             rk3["cpu_baseline"]["kind"] = "port"
