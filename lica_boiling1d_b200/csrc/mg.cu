@@ -16,7 +16,7 @@
 //                level 0 the r.z partial of the CG update
 //   * The levels below 64x64 run in one CTA with everything in shared memory
 //     (k_cta): remaining outer levels, the coarsest outer level solved in FP64 by inner
-//     V-cycles that end in a dense elimination; levels <= 16x16 run in warp 0 alone.
+//     V-cycles that end in a dense elimination; levels <= 8x8 run in warp 0 alone.
 //   * CG vector updates are fused with the stencil they need (k_pupdate: p = z + beta p
 //     and p.Ap; k_xupdate: x += alpha p and the true residual f - A x with its norm).
 //     Grid-wide sums use a deterministic last-block reduction, which also computes the
@@ -44,9 +44,9 @@ namespace mg {
 constexpr int TX = 32;
 constexpr int TY = 32;
 constexpr int NT = 256;          // threads of a CG / set-up grid-kernel CTA
-constexpr int NT_CTA = 1024;     // threads of the single-CTA coarse kernel
+constexpr int NT_CTA = 512;      // threads of the single-CTA coarse kernel (fewer idle warps per barrier than 1024)
 constexpr int kMaxLevels = 16;
-constexpr int kSmallCells = 256; // levels with <= this many cells run in warp 0 alone
+constexpr int kSmallCells = 64;  // levels with <= this many cells run in warp 0 alone
 constexpr int kMaxDense = 64;    // bottom-level unknowns solved by dense elimination
 
 struct State {
