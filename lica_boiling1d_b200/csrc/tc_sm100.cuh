@@ -20,9 +20,13 @@
 namespace lica {
 namespace tc {
 
-// Iteration cap of every spin wait (a few seconds at most); on expiry the wait reports
-// failure and the caller sets the kernel's error flag and leaves.
-constexpr uint32_t kSpinCap = 1u << 22;
+// Bound of every wait: after kWaitNs of %globaltimer time the wait reports failure and
+// the caller sets the kernel's error flag and leaves.  Each try_wait carries a suspend-time
+// hint, so a waiting thread sleeps in the barrier unit until the phase completes instead
+// of re-issuing the test (a spinning producer or epilogue thread otherwise competes with
+// the MMA thread for the barrier and shared-memory pipeline).
+constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s
+constexpr uint32_t kSuspendHintNs = 1000000u;  // 1 ms per try_wait at most
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -39,19 +43,45 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendHintNs)
         : "memory");
     return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity; false if the cap ran out.
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait for the phase with the given parity; false if kWaitNs ran out.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (uint32_t it = 0; it < kSpinCap; ++it)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (global_ns() - t0 > kWaitNs) return false;
+    return true;
+}
+
+// The same wait for a whole converged warp: lane 0 waits, the result is broadcast.
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity, int lane) {
+    int ok = 1;
+    if (lane == 0) ok = mbar_wait(bar, parity) ? 1 : 0;
+    return __shfl_sync(0xffffffffu, ok, 0) != 0;
+}
+
+// One lane of a converged warp (the lowest active lane, the same lane every call).
+__device__ __forceinline__ bool elect_one() {
+    uint32_t p;
+    asm volatile(
+        "{\n\t.reg .pred e;\n\t"
+        "elect.sync _|e, 0xffffffff;\n\t"
+        "selp.u32 %0, 1, 0, e;\n\t}"
+        : "=r"(p));
+    return p != 0;
 }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {

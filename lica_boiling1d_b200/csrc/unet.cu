@@ -154,11 +154,28 @@ int conv3x3(const __nv_bfloat16* x0, int c0, const __nv_bfloat16* x1, int c1, co
     const int tiles = n * (h / th) * (wd / tw);
     const int cbmax = std::max(P.cblk[0], P.nsrc > 1 ? P.cblk[1] : 0);
     P.stage_a = ((kHaloRows * cbmax * 2 + 1023) / 1024) * 1024;
-    P.stage_b = ((3 * cout * cbmax * 2 + 1023) / 1024) * 1024;
     P.tiles = tiles;
-    P.nstages = std::min<int>(kStages, (int)((kConvSmemMax - 1024 - 256) / (P.stage_a + P.stage_b)));
+    // Resident weights: the whole cout x (9 ctot) matrix (one box per tap, input and
+    // channel block) stays in shared memory for all tiles of the CTA when it fits beside
+    // a ring of at least three A stages and every box starts on its swizzle atom; the
+    // ring then carries only the activation halo boxes.
+    const int wres = 18 * cout * P.ctot;
+    bool resident = kConvSmemMax - 1024 - kBarBytes - wres >= 3 * P.stage_a;
+    for (int tap = 0; tap < 9; ++tap)
+        for (int src = 0; src < P.nsrc; ++src)
+            for (int c = src ? c0 : 0; c < (src ? P.ctot : c0); c += P.cblk[src])
+                if ((2 * cout * (tap * P.ctot + c)) % (16 * P.cblk[src])) resident = false;
+    if (resident) {
+        P.wres = wres;
+        P.stage_b = 0;
+        P.nstages = std::min<int>(kStages, (kConvSmemMax - 1024 - kBarBytes - wres) / P.stage_a);
+    } else {
+        P.wres = 0;
+        P.stage_b = ((3 * cout * cbmax * 2 + 1023) / 1024) * 1024;
+        P.nstages = std::min<int>(kStages, (int)((kConvSmemMax - 1024 - kBarBytes) / (P.stage_a + P.stage_b)));
+    }
     if (P.nstages < 1) return LICA_BAD_ARG;
-    const size_t smem = conv_p_smem_bytes(P.stage_a, P.stage_b, P.nstages);
+    const size_t smem = conv_p_smem_bytes(P.stage_a, P.stage_b, P.nstages, P.wres);
     // CTAs per SM: shared memory and tensor memory (two accumulators of tmem_cols each)
     int per_sm = 0;
     LICA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv3x3_tcp, kConvThreads, smem));

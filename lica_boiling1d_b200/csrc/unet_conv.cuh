@@ -30,7 +30,9 @@
 namespace lica {
 namespace unet {
 
-constexpr int kStages = 4;
+constexpr int kStages = 32;  // cap of the stage ring: deep enough for ~5 tiles of loads in flight per SM
+constexpr int kBarBytes = 1024;  // mbarriers and the tensor-memory slot, after the tiles
+static_assert((2 * kStages + 5) * 8 + 4 <= kBarBytes, "barrier region too small");
 constexpr int kTileM = 128;
 constexpr int kTileW = 8, kTileH = 16;          // pixel tile: 16 rows x 8 columns
 constexpr int kHaloRows = kTileW * (kTileH + 2);  // A box: 18 rows x 8 columns = 144 pixel rows
@@ -51,13 +53,14 @@ struct ConvParams {
     int* err;             // set to 1 when a bounded wait runs out
     int stage_a, stage_b; // bytes of one pipeline stage's A and B tiles (multiples of 1 KB)
     int nstages;          // stages in the ring (<= kStages; fewer for wide layers)
+    int wres;             // bytes of the resident weights (0: weight slices stream with A)
     int tiles;            // pixel tiles of the whole launch
 };
 
 constexpr int kConvThreads = 192;
 
-__host__ __device__ inline size_t conv_p_smem_bytes(int stage_a, int stage_b, int nstages) {
-    return 1024 + (size_t)nstages * (stage_a + stage_b) + 256;
+__host__ __device__ inline size_t conv_p_smem_bytes(int stage_a, int stage_b, int nstages, int wres) {
+    return 1024 + (size_t)nstages * (stage_a + stage_b) + (size_t)wres + kBarBytes;
 }
 
 __device__ __forceinline__ void tile_origin(const ConvParams& P, int t, int& img, int& x0, int& y0) {
@@ -79,12 +82,15 @@ __global__ void __launch_bounds__(kConvThreads, 1)
     unsigned char* sa = base;
     const int NS = P.nstages;
     unsigned char* sb = base + NS * P.stage_a;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sb + NS * P.stage_b);
+    // resident weights (P.wres > 0): [tap][channel block][cout rows][cblk], loaded once
+    unsigned char* sw = sb + NS * P.stage_b;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sw + P.wres);
     uint64_t* full = bars;
     uint64_t* empty = bars + kStages;
-    uint64_t* tfull = bars + 2 * kStages;   // [2]: accumulator ready for the epilogue
+    uint64_t* tfull = bars + 2 * kStages;       // [2]: accumulator ready for the epilogue
     uint64_t* tempty = bars + 2 * kStages + 2;  // [2]: accumulator drained by the epilogue
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 4);
+    uint64_t* wready = bars + 2 * kStages + 4;  // resident weights landed
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 5);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -96,6 +102,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
             tc::mbar_init(&tfull[a], 1);
             tc::mbar_init(&tempty[a], 128);
         }
+        tc::mbar_init(wready, 1);
         tc::fence_barrier_init();
         tc::prefetch_tmap(&tm_x0);
         tc::prefetch_tmap(&tm_w0);
@@ -113,78 +120,128 @@ __global__ void __launch_bounds__(kConvThreads, 1)
     const int nb0 = P.cin[0] / P.cblk[0], nb1 = P.nsrc > 1 ? P.cin[1] / P.cblk[1] : 0;
     const int nkb = 3 * (nb0 + nb1);  // K blocks: (dx, source, channel block); dy inside
 
+    // Warps 4 and 5 run their loops with all 32 lanes (warp-uniform control and descriptor
+    // arithmetic); one elected lane issues the copies, MMAs and commits.
     if (warp == 4) {
-        if (lane == 0) {
-            int g = 0;  // K blocks issued over all tiles
-            bool ok = true;
-            for (int t = blockIdx.x; t < P.tiles && ok; t += gridDim.x) {
-                int img, x0, y0;
-                tile_origin(P, t, img, x0, y0);
-                int dx = 0, src = 0, cb = 0;
-                for (int kb = 0; kb < nkb; ++kb, ++g) {
-                    const int s = g % NS, u = g / NS;
-                    if (g >= NS && !tc::mbar_wait(&empty[s], (u - 1) & 1)) {
-                        atomicExch(P.err, 1);
-                        ok = false;
-                        break;
+        // TMA producer
+        if (P.wres) {
+            if (tc::elect_one()) {
+                tc::mbar_expect_tx(wready, (uint32_t)P.wres);
+                for (int tap = 0; tap < 9; ++tap)
+                    for (int src = 0; src < P.nsrc; ++src) {
+                        const int cblk = P.cblk[src], off = src ? P.cin[0] : 0;
+                        const void* tmw = src ? (const void*)&tm_w1 : (const void*)&tm_w0;
+                        for (int cb = 0; cb < (src ? nb1 : nb0); ++cb) {
+                            const int c = tap * P.ctot + off + cb * cblk;
+                            tc::tma_load_2d(sw + 2 * P.cout * c, tmw, wready, c, 0);
+                        }
                     }
-                    const int cblk = P.cblk[src];
+            }
+            __syncwarp();
+        }
+        int s = 0, g = 0;  // ring stage, K blocks issued over all tiles
+        uint32_t ph = 0;   // parity of the stage's current use
+        bool ok = true;
+        for (int t = blockIdx.x; t < P.tiles && ok; t += gridDim.x) {
+            int img, x0, y0;
+            tile_origin(P, t, img, x0, y0);
+            int dx = 0, src = 0, cb = 0;
+            for (int kb = 0; kb < nkb; ++kb, ++g) {
+                if (g >= NS && !tc::mbar_wait_warp(&empty[s], ph ^ 1u, lane)) {
+                    if (lane == 0) atomicExch(P.err, 1);
+                    ok = false;
+                    break;
+                }
+                const int cblk = P.cblk[src];
+                if (tc::elect_one()) {
                     const int bsub = P.cout * cblk * 2;  // bytes of one tap's weight slice
-                    tc::mbar_expect_tx(&full[s], (uint32_t)(kHaloRows + 3 * P.cout) * cblk * 2);
+                    tc::mbar_expect_tx(&full[s], (uint32_t)(kHaloRows + (P.wres ? 0 : 3 * P.cout)) * cblk * 2);
                     const void* tmx = src ? (const void*)&tm_x1 : (const void*)&tm_x0;
-                    const void* tmw = src ? (const void*)&tm_w1 : (const void*)&tm_w0;
                     // 8 x 18 pixels (the tile and one row above and below), shifted by dx
                     tc::tma_load_4d(sa + s * P.stage_a, tmx, &full[s], cb * cblk, x0 + dx - 1, y0 - 1, img);
-                    const int col = (src ? P.cin[0] : 0) + cb * cblk;
-                    for (int dy = 0; dy < 3; ++dy)
-                        tc::tma_load_2d(sb + s * P.stage_b + dy * bsub, tmw, &full[s], (3 * dy + dx) * P.ctot + col, 0);
-                    if (++cb == (src ? nb1 : nb0)) {
-                        cb = 0;
-                        if (++src == P.nsrc) { src = 0; ++dx; }
+                    if (!P.wres) {
+                        const void* tmw = src ? (const void*)&tm_w1 : (const void*)&tm_w0;
+                        const int col = (src ? P.cin[0] : 0) + cb * cblk;
+                        for (int dy = 0; dy < 3; ++dy)
+                            tc::tma_load_2d(sb + s * P.stage_b + dy * bsub, tmw, &full[s], (3 * dy + dx) * P.ctot + col,
+                                            0);
                     }
                 }
+                __syncwarp();
+                if (++cb == (src ? nb1 : nb0)) {
+                    cb = 0;
+                    if (++src == P.nsrc) { src = 0; ++dx; }
+                }
+                if (++s == NS) { s = 0; ph ^= 1u; }
             }
         }
     } else if (warp == 5) {
-        if (lane == 0) {
-            const uint32_t idesc = tc::idesc_bf16_f32(kTileM, (uint32_t)P.cout);
-            int g = 0, it = 0;
-            bool ok = true;
-            for (int t = blockIdx.x; t < P.tiles && ok; t += gridDim.x, ++it) {
-                const int acc = it & 1, use = it >> 1;
-                if (it >= 2 && !tc::mbar_wait(&tempty[acc], (use - 1) & 1)) {
-                    atomicExch(P.err, 1);
+        // MMA issuer
+        const uint32_t idesc = tc::idesc_bf16_f32(kTileM, (uint32_t)P.cout);
+        // descriptors of stage 0 (A, streamed B) or of the resident weights per input; the
+        // descriptor of an address a + 16 j is desc(a) + j (all shared addresses < 256 KB)
+        const uint64_t a_base0 = tc::smem_desc(sa, 2u * P.cblk[0]), a_base1 = tc::smem_desc(sa, 2u * P.cblk[1]);
+        unsigned char* bb = P.wres ? sw : sb;
+        const uint64_t b_base0 = tc::smem_desc(bb, 2u * P.cblk[0]), b_base1 = tc::smem_desc(bb, 2u * P.cblk[1]);
+        const uint32_t b_dy_res = (uint32_t)(3 * P.cout * P.ctot) / 8u;  // 3 taps of 2 cout ctot bytes
+        int s = 0, it = 0;
+        uint32_t ph = 0;
+        bool ok = !P.wres || tc::mbar_wait_warp(wready, 0, lane);
+        if (!ok && lane == 0) atomicExch(P.err, 1);
+        for (int t = blockIdx.x; t < P.tiles && ok; t += gridDim.x, ++it) {
+            const int acc = it & 1, use = it >> 1;
+            if (it >= 2 && !tc::mbar_wait_warp(&tempty[acc], (uint32_t)(use - 1) & 1u, lane)) {
+                if (lane == 0) atomicExch(P.err, 1);
+                break;
+            }
+            tc::tc_fence_after();
+            const uint32_t d = tmem + (uint32_t)(acc * P.tmem_cols);
+            int dx = 0, src = 0, cb = 0;
+            for (int kb = 0; kb < nkb; ++kb) {
+                // the stage's producer is the TMA unit (async proxy, completion through the
+                // mbarrier): no tcgen05 fence is needed before the MMAs read it
+                if (!tc::mbar_wait_warp(&full[s], ph, lane)) {
+                    if (lane == 0) atomicExch(P.err, 1);
+                    ok = false;
                     break;
                 }
-                tc::tc_fence_after();
-                const uint32_t d = tmem + (uint32_t)(acc * P.tmem_cols);
-                int src = 0, cb = 0;
-                for (int kb = 0; kb < nkb; ++kb, ++g) {
-                    const int s = g % NS, u = g / NS;
-                    if (!tc::mbar_wait(&full[s], u & 1)) {
-                        atomicExch(P.err, 1);
-                        ok = false;
-                        break;
-                    }
-                    tc::tc_fence_after();
-                    const int cblk = P.cblk[src];
-                    const uint32_t rb = (uint32_t)cblk * 2;
-                    // tap dy: the A operand starts dy rows of the tile (8 pixel rows = one
-                    // swizzle atom) further into the halo box
-                    for (int dy = 0; dy < 3; ++dy) {
-                        const uint64_t da = tc::smem_desc(sa + s * P.stage_a + dy * 8 * (int)rb, rb);
-                        const uint64_t db = tc::smem_desc(sb + s * P.stage_b + dy * P.cout * (int)rb, rb);
-                        for (int k = 0; k < cblk / 16; ++k)
-                            tc::mma_bf16(d, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, (kb | dy | k) != 0);
-                    }
-                    tc::mma_commit(&empty[s]);
-                    if (++cb == (src ? nb1 : nb0)) {
-                        cb = 0;
-                        if (++src == P.nsrc) src = 0;
-                    }
+                const int cblk = P.cblk[src];
+                const int col = (src ? P.cin[0] : 0) + cb * cblk;
+                // descriptor offsets in 16-byte units.  A: tap dy starts dy rows of the tile
+                // (8 pixel rows = one swizzle atom of 8 * 2 cblk bytes) into the halo box.
+                // B: the (dy, dx) weight box, resident or in the stage.
+                const uint64_t a = (src ? a_base1 : a_base0) + (uint32_t)(s * P.stage_a) / 16u;
+                const uint32_t a_dy = (uint32_t)cblk;
+                uint64_t b;
+                uint32_t b_dy;
+                if (P.wres) {
+                    b = (src ? b_base1 : b_base0) + (uint32_t)(P.cout * (dx * P.ctot + col)) / 8u;
+                    b_dy = b_dy_res;
+                } else {
+                    b = (src ? b_base1 : b_base0) + (uint32_t)(s * P.stage_b) / 16u;
+                    b_dy = (uint32_t)(P.cout * cblk) / 8u;
                 }
-                tc::mma_commit(&tfull[acc]);  // also after a failed wait: tracks the MMAs in flight
+                const int nk = cblk / 16;
+                if (tc::elect_one()) {
+#pragma unroll
+                    for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            if (k < nk)
+                                tc::mma_bf16(d, a + dy * a_dy + 2 * k, b + dy * b_dy + 2 * k, idesc,
+                                             (kb | dy | k) != 0);
+                    tc::mma_commit(&empty[s]);
+                }
+                __syncwarp();
+                if (++cb == (src ? nb1 : nb0)) {
+                    cb = 0;
+                    if (++src == P.nsrc) { src = 0; ++dx; }
+                }
+                if (++s == NS) { s = 0; ph ^= 1u; }
             }
+            // also after a failed wait: tracks the MMAs in flight
+            if (tc::elect_one()) tc::mma_commit(&tfull[acc]);
+            __syncwarp();
         }
     } else {
         // epilogue warps 0-3: pixel m = threadIdx.x = tensor-memory lane
