@@ -160,19 +160,29 @@ int conv3x3(const __nv_bfloat16* x0, int c0, const __nv_bfloat16* x1, int c1, co
     // a ring of at least three A stages and every box starts on its swizzle atom; the
     // ring then carries only the activation halo boxes.
     const int wres = 18 * cout * P.ctot;
-    bool resident = kConvSmemMax - 1024 - kBarBytes - wres >= 3 * P.stage_a;
+    bool resident = kConvSmemMax - 1024 - kBarBytes - wres >= 3 * P.stage_a;  // three 1-box stages
     for (int tap = 0; tap < 9; ++tap)
         for (int src = 0; src < P.nsrc; ++src)
             for (int c = src ? c0 : 0; c < (src ? P.ctot : c0); c += P.cblk[src])
                 if ((2 * cout * (tap * P.ctot + c)) % (16 * P.cblk[src])) resident = false;
+    const int avail = kConvSmemMax - 1024 - kBarBytes;
     if (resident) {
         P.wres = wres;
         P.stage_b = 0;
-        P.nstages = std::min<int>(kStages, (kConvSmemMax - 1024 - kBarBytes - wres) / P.stage_a);
+        // all three dx boxes per stage when at least two such stages fit
+        const int stage3 = ((3 * kHaloRows * cbmax * 2 + 1023) / 1024) * 1024;
+        if ((avail - wres) / stage3 >= 2) {
+            P.kdx = 3;
+            P.stage_a = stage3;
+        } else {
+            P.kdx = 1;
+        }
+        P.nstages = std::min<int>(kStages, (avail - wres) / P.stage_a);
     } else {
         P.wres = 0;
+        P.kdx = 1;
         P.stage_b = ((3 * cout * cbmax * 2 + 1023) / 1024) * 1024;
-        P.nstages = std::min<int>(kStages, (int)((kConvSmemMax - 1024 - kBarBytes) / (P.stage_a + P.stage_b)));
+        P.nstages = std::min<int>(kStages, avail / (P.stage_a + P.stage_b));
     }
     if (P.nstages < 1) return LICA_BAD_ARG;
     const size_t smem = conv_p_smem_bytes(P.stage_a, P.stage_b, P.nstages, P.wres);

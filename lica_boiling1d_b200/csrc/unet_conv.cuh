@@ -19,8 +19,12 @@
 //                   tile overlaps the MMAs of the next
 //   warps 0-3     : epilogue, tensor memory -> registers (warp w reads lanes 32w..32w+31
 //                   = pixels), + bias, optional ReLU, BF16 NHWC store (optionally FP32)
-// Stage sizes follow the layer's channel block (A: 144 x cblk, B: 3 x cout x cblk BF16),
-// so narrow layers keep several CTAs per SM.
+// Stage sizes follow the layer's channel block (A: kdx x 144 x cblk, B: 3 x cout x cblk
+// BF16).  When the whole weight matrix fits in shared memory beside the ring it is loaded
+// once per CTA (resident weights), the stages carry only activations, and a stage holds
+// all three dx boxes of its channel block (kdx = 3): every K block is then 9 taps of MMAs,
+// which amortises the fixed cost of a pipeline step (barrier wait, issue, commit) over
+// three times as many tensor-core instructions.
 #pragma once
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -54,6 +58,8 @@ struct ConvParams {
     int stage_a, stage_b; // bytes of one pipeline stage's A and B tiles (multiples of 1 KB)
     int nstages;          // stages in the ring (<= kStages; fewer for wide layers)
     int wres;             // bytes of the resident weights (0: weight slices stream with A)
+    int kdx;              // dx taps per K block: 3 (all three halo boxes in one stage; resident
+                          // weights only) or 1
     int tiles;            // pixel tiles of the whole launch
 };
 
@@ -118,7 +124,8 @@ __global__ void __launch_bounds__(kConvThreads, 1)
     const uint32_t tmem = *tmem_slot;
 
     const int nb0 = P.cin[0] / P.cblk[0], nb1 = P.nsrc > 1 ? P.cin[1] / P.cblk[1] : 0;
-    const int nkb = 3 * (nb0 + nb1);  // K blocks: (dx, source, channel block); dy inside
+    const int kdx = P.kdx;
+    const int nkb = (3 / kdx) * (nb0 + nb1);  // K blocks: (dx group, source, channel block)
 
     // Warps 4 and 5 run their loops with all 32 lanes (warp-uniform control and descriptor
     // arithmetic); one elected lane issues the copies, MMAs and commits.
@@ -155,10 +162,14 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                 const int cblk = P.cblk[src];
                 if (tc::elect_one()) {
                     const int bsub = P.cout * cblk * 2;  // bytes of one tap's weight slice
-                    tc::mbar_expect_tx(&full[s], (uint32_t)(kHaloRows + (P.wres ? 0 : 3 * P.cout)) * cblk * 2);
+                    tc::mbar_expect_tx(&full[s],
+                                       (uint32_t)(kdx * kHaloRows + (P.wres ? 0 : 3 * P.cout)) * cblk * 2);
                     const void* tmx = src ? (const void*)&tm_x1 : (const void*)&tm_x0;
-                    // 8 x 18 pixels (the tile and one row above and below), shifted by dx
-                    tc::tma_load_4d(sa + s * P.stage_a, tmx, &full[s], cb * cblk, x0 + dx - 1, y0 - 1, img);
+                    // 8 x 18 pixels (the tile and one row above and below), shifted by dx; the
+                    // kdx boxes of a stage follow each other (each a whole number of atoms)
+                    for (int j = 0; j < kdx; ++j)
+                        tc::tma_load_4d(sa + s * P.stage_a + j * kHaloRows * cblk * 2, tmx, &full[s], cb * cblk,
+                                        x0 + dx + j - 1, y0 - 1, img);
                     if (!P.wres) {
                         const void* tmw = src ? (const void*)&tm_w1 : (const void*)&tm_w0;
                         const int col = (src ? P.cin[0] : 0) + cb * cblk;
@@ -170,7 +181,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                 __syncwarp();
                 if (++cb == (src ? nb1 : nb0)) {
                     cb = 0;
-                    if (++src == P.nsrc) { src = 0; ++dx; }
+                    if (++src == P.nsrc) { src = 0; dx += kdx; }
                 }
                 if (++s == NS) { s = 0; ph ^= 1u; }
             }
@@ -222,20 +233,27 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                     b_dy = (uint32_t)(P.cout * cblk) / 8u;
                 }
                 const int nk = cblk / 16;
+                // next dx box of the stage: 144 rows of 2 cblk bytes further (A); the weight
+                // box of tap dx + 1 is ctot columns further (resident weights only: kdx = 3)
+                const uint32_t a_dx = 18u * (uint32_t)cblk, b_dx = (uint32_t)(P.cout * P.ctot) / 8u;
                 if (tc::elect_one()) {
 #pragma unroll
-                    for (int dy = 0; dy < 3; ++dy)
+                    for (int j = 0; j < 3; ++j)
+                        if (j < kdx)
 #pragma unroll
-                        for (int k = 0; k < 4; ++k)
-                            if (k < nk)
-                                tc::mma_bf16(d, a + dy * a_dy + 2 * k, b + dy * b_dy + 2 * k, idesc,
-                                             (kb | dy | k) != 0);
+                            for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+                                for (int k = 0; k < 4; ++k)
+                                    if (k < nk)
+                                        tc::mma_bf16(d, a + j * a_dx + dy * a_dy + 2 * k,
+                                                     b + j * b_dx + dy * b_dy + 2 * k, idesc,
+                                                     (kb | j | dy | k) != 0);
                     tc::mma_commit(&empty[s]);
                 }
                 __syncwarp();
                 if (++cb == (src ? nb1 : nb0)) {
                     cb = 0;
-                    if (++src == P.nsrc) { src = 0; ++dx; }
+                    if (++src == P.nsrc) { src = 0; dx += kdx; }
                 }
                 if (++s == NS) { s = 0; ph ^= 1u; }
             }
