@@ -160,12 +160,12 @@ int conv3x3(const __nv_bfloat16* x0, int c0, const __nv_bfloat16* x1, int c1, co
     // a ring of at least three A stages and every box starts on its swizzle atom; the
     // ring then carries only the activation halo boxes.
     const int wres = 18 * cout * P.ctot;
-    bool resident = kConvSmemMax - 1024 - kBarBytes - wres >= 3 * P.stage_a;  // three 1-box stages
+    const int avail = kConvSmemMax - 1024 - kBarBytes - kBiasBytes;
+    bool resident = avail - wres >= 3 * P.stage_a;  // beside three 1-box stages
     for (int tap = 0; tap < 9; ++tap)
         for (int src = 0; src < P.nsrc; ++src)
             for (int c = src ? c0 : 0; c < (src ? P.ctot : c0); c += P.cblk[src])
                 if ((2 * cout * (tap * P.ctot + c)) % (16 * P.cblk[src])) resident = false;
-    const int avail = kConvSmemMax - 1024 - kBarBytes;
     if (resident) {
         P.wres = wres;
         P.stage_b = 0;

@@ -65,8 +65,46 @@ struct ConvParams {
 
 constexpr int kConvThreads = 192;
 
+constexpr int kBiasBytes = 1024;  // the bias (cout <= 256 floats), after the barriers
+
 __host__ __device__ inline size_t conv_p_smem_bytes(int stage_a, int stage_b, int nstages, int wres) {
-    return 1024 + (size_t)nstages * (stage_a + stage_b) + (size_t)wres + kBarBytes;
+    return 1024 + (size_t)nstages * (stage_a + stage_b) + (size_t)wres + kBarBytes + kBiasBytes;
+}
+
+// Bias, ReLU, BF16 (and FP32) stores of the columns c0 .. c0 + min(ncols, NC) - 1 of one
+// pixel held in registers.
+template <int NC>
+__device__ __forceinline__ void conv_epilogue_store(const ConvParams& P, const float* sbias, size_t pix, int c0,
+                                                    const uint32_t* r, int ncols) {
+#pragma unroll
+    for (int g = 0; g < NC / 16; ++g) {
+        if (16 * g < ncols) {
+            float v[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                float a = __uint_as_float(r[16 * g + i]) + sbias[c0 + 16 * g + i];
+                if (P.relu) a = fmaxf(a, 0.f);
+                v[i] = a;
+            }
+            const size_t o = pix * P.out_c + P.out_c0 + c0 + 16 * g;
+            if (P.out) {
+                uint32_t pk[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+                    pk[i] = *reinterpret_cast<const uint32_t*>(&b2);
+                }
+                uint4* dst = reinterpret_cast<uint4*>(P.out + o);
+                dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+            }
+            if (P.out32) {
+                float4* dst = reinterpret_cast<float4*>(P.out32 + o);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) dst[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+            }
+        }
+    }
 }
 
 __device__ __forceinline__ void tile_origin(const ConvParams& P, int t, int& img, int& x0, int& y0) {
@@ -97,6 +135,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
     uint64_t* tempty = bars + 2 * kStages + 2;  // [2]: accumulator drained by the epilogue
     uint64_t* wready = bars + 2 * kStages + 4;  // resident weights landed
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 5);
+    float* sbias = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(bars) + kBarBytes);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -136,7 +175,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                 tc::mbar_expect_tx(wready, (uint32_t)P.wres);
                 for (int tap = 0; tap < 9; ++tap)
                     for (int src = 0; src < P.nsrc; ++src) {
-                        const int cblk = P.cblk[src], off = src ? P.cin[0] : 0;
+                        const int cblk = (src ? P.cblk[1] : P.cblk[0]), off = src ? P.cin[0] : 0;
                         const void* tmw = src ? (const void*)&tm_w1 : (const void*)&tm_w0;
                         for (int cb = 0; cb < (src ? nb1 : nb0); ++cb) {
                             const int c = tap * P.ctot + off + cb * cblk;
@@ -159,7 +198,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                     ok = false;
                     break;
                 }
-                const int cblk = P.cblk[src];
+                const int cblk = (src ? P.cblk[1] : P.cblk[0]);
                 if (tc::elect_one()) {
                     const int bsub = P.cout * cblk * 2;  // bytes of one tap's weight slice
                     tc::mbar_expect_tx(&full[s],
@@ -216,7 +255,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                     ok = false;
                     break;
                 }
-                const int cblk = P.cblk[src];
+                const int cblk = (src ? P.cblk[1] : P.cblk[0]);
                 const int col = (src ? P.cin[0] : 0) + cb * cblk;
                 // descriptor offsets in 16-byte units.  A: tap dy starts dy rows of the tile
                 // (8 pixel rows = one swizzle atom of 8 * 2 cblk bytes) into the halo box.
@@ -263,6 +302,8 @@ __global__ void __launch_bounds__(kConvThreads, 1)
         }
     } else {
         // epilogue warps 0-3: pixel m = threadIdx.x = tensor-memory lane
+        for (int i = threadIdx.x; i < P.cout; i += 128) sbias[i] = P.bias ? P.bias[i] : 0.f;
+        asm volatile("bar.sync 1, 128;" ::: "memory");  // the four epilogue warps
         int it = 0;
         for (int t = blockIdx.x; t < P.tiles; t += gridDim.x, ++it) {
             const int acc = it & 1, use = it >> 1;
@@ -280,35 +321,28 @@ __global__ void __launch_bounds__(kConvThreads, 1)
             const int y = y0 + m / P.tw, x = x0 + m % P.tw;
             const size_t pix = ((size_t)img * P.h + y) * P.w + x;
             const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(acc * P.tmem_cols);
-            for (int c0 = 0; c0 < P.cout; c0 += 16) {
-                float v[16];
-                tc::tmem_ld16(taddr + (uint32_t)c0, v);
-#pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    float a = v[i] + (P.bias ? P.bias[c0 + i] : 0.f);
-                    if (P.relu) a = fmaxf(a, 0.f);
-                    v[i] = a;
+            // whole 32-column chunks (the accumulator has tmem_cols >= the rounded-up cout)
+            if (P.cout <= 64) {
+                // the whole accumulator in registers: release it before the stores
+                uint32_t r[64];
+                tc::tmem_ld32_nowait(taddr, r);
+                if (P.cout > 32) tc::tmem_ld32_nowait(taddr + 32u, r + 32);
+                tc::tmem_wait_ld();
+                tc::tmem_pin<64>(r);
+                tc::tc_fence_before();
+                tc::mbar_arrive(&tempty[acc]);
+                conv_epilogue_store<64>(P, sbias, pix, 0, r, P.cout);
+            } else {
+                for (int c0 = 0; c0 < P.cout; c0 += 32) {
+                    uint32_t r[32];
+                    tc::tmem_ld32_nowait(taddr + (uint32_t)c0, r);
+                    tc::tmem_wait_ld();
+                    tc::tmem_pin<32>(r);
+                    conv_epilogue_store<32>(P, sbias, pix, c0, r, P.cout - c0);
                 }
-                if (P.out) {
-                    uint32_t pk[8];
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
-                        pk[i] = *reinterpret_cast<const uint32_t*>(&b2);
-                    }
-                    uint4* dst = reinterpret_cast<uint4*>(P.out + pix * P.out_c + P.out_c0 + c0);
-                    dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-                    dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
-                }
-                if (P.out32) {
-                    float4* dst = reinterpret_cast<float4*>(P.out32 + pix * P.out_c + P.out_c0 + c0);
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-                        dst[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
-                }
+                tc::tc_fence_before();
+                tc::mbar_arrive(&tempty[acc]);
             }
-            tc::tc_fence_before();
-            tc::mbar_arrive(&tempty[acc]);
         }
     }
     __syncwarp();
