@@ -96,10 +96,21 @@ constexpr int kConvSmemMax = 227 * 1024;
 namespace lica {
 namespace unet {
 
+// Fused consumers of a convolution's BF16 output (see ConvParams).
+struct ConvFuse {
+    __nv_bfloat16* pool = nullptr;
+    const float* head_w = nullptr;
+    float* head_out = nullptr;
+    double* head_x0 = nullptr;
+    const double* head_rho = nullptr;
+    const double* head_sigma = nullptr;
+    double hsq = 0.0;
+};
+
 // out[:, :, :, out_c0 : out_c0 + cout] = conv3x3([x0, x1]) (+ bias, ReLU), NHWC BF16.
 int conv3x3(const __nv_bfloat16* x0, int c0, const __nv_bfloat16* x1, int c1, const __nv_bfloat16* w,
             const float* bias, int n, int h, int wd, int cout, int relu, __nv_bfloat16* out, float* out32, int out_c,
-            int out_c0, int* err, cudaStream_t s) {
+            int out_c0, int* err, cudaStream_t s, const ConvFuse* fuse = nullptr) {
     if (n < 1 || h < 1 || wd < 1 || c0 <= 0 || c0 % 16 || c1 < 0 || c1 % 16 || (c1 > 0 && !x1) || cout < 16 ||
         cout > 256 || cout % 16 || out_c0 < 0 || out_c0 % 8 || out_c % 8 || out_c0 + cout > out_c) {
         lica_set_last_error("lica_unet_conv3x3", "unsupported channel counts", __FILE__, __LINE__);
@@ -140,6 +151,25 @@ int conv3x3(const __nv_bfloat16* x0, int c0, const __nv_bfloat16* x1, int c1, co
     P.out = out;
     P.out32 = out32;
     P.err = err;
+    if (fuse) {
+        if ((fuse->pool || fuse->head_w) && (cout > 64 || out_c0 != 0 || out_c != cout)) {
+            lica_set_last_error("lica_unet_conv3x3", "fused pool/head need cout <= 64 and a dense output", __FILE__,
+                                __LINE__);
+            return LICA_BAD_ARG;
+        }
+        if (fuse->head_w && (cout != 32 || !fuse->head_out || (fuse->head_x0 && (!fuse->head_rho || !fuse->head_sigma)))) {
+            lica_set_last_error("lica_unet_conv3x3", "fused head needs 32 channels and its outputs", __FILE__,
+                                __LINE__);
+            return LICA_BAD_ARG;
+        }
+        P.pool = fuse->pool;
+        P.head_w = fuse->head_w;
+        P.head_out = fuse->head_out;
+        P.head_x0 = fuse->head_x0;
+        P.head_rho = fuse->head_rho;
+        P.head_sigma = fuse->head_sigma;
+        P.hsq = fuse->hsq;
+    }
     CUtensorMap mx0, mx1, mw0, mw1;
     int st;
     if ((st = act_map(&mx0, x0, c0, wd, h, n, P.cblk[0], tw, th + 2))) return st;
@@ -208,7 +238,7 @@ int lica_unet_conv3x3_device(const void* x0, int32_t c0, const void* x1, int32_t
     if (!x0 || !w || !err || (!out && !out32)) return LICA_BAD_ARG;
     return lica::unet::conv3x3((const __nv_bfloat16*)x0, c0, (const __nv_bfloat16*)x1, c1,
                                (const __nv_bfloat16*)w, bias, n, h, wd, cout, relu, (__nv_bfloat16*)out, out32, out_c,
-                               out_c0, err, (cudaStream_t)stream);
+                               out_c0, err, (cudaStream_t)stream, nullptr);
 }
 
 }  // extern "C"
@@ -247,7 +277,7 @@ using bf16 = __nv_bfloat16;
 // ---------------------------------------------------------------- elementwise kernels
 // sigma[n] = sqrt(mean f^2) of each image: kRmsParts blocks per image write partial
 // sums, one block per image adds them (fixed order).
-constexpr int kRmsParts = 64;
+constexpr int kRmsParts = 512;
 __global__ void k_rms_part(const double* __restrict__ f, double* __restrict__ part, int npix) {
     __shared__ double red[32];
     const double* fi = f + (size_t)blockIdx.y * npix;
@@ -257,9 +287,11 @@ __global__ void k_rms_part(const double* __restrict__ f, double* __restrict__ pa
     if (threadIdx.x == 0) part[blockIdx.y * kRmsParts + blockIdx.x] = s;
 }
 __global__ void k_rms_final(const double* __restrict__ part, double* __restrict__ sigma, int npix) {
+    __shared__ double red[32];
+    double s = 0.0;
+    for (int k = threadIdx.x; k < kRmsParts; k += blockDim.x) s += part[blockIdx.x * kRmsParts + k];
+    s = block_sum(s, red);
     if (threadIdx.x == 0) {
-        double s = 0.0;
-        for (int k = 0; k < kRmsParts; ++k) s += part[blockIdx.x * kRmsParts + k];
         const double m = s / npix;
         sigma[blockIdx.x] = m > 0.0 ? sqrt(m) : 1.0;
     }
@@ -281,50 +313,6 @@ __global__ void k_input(const double* __restrict__ rho, const double* __restrict
     }
 }
 
-// 8 BF16 <-> 8 floats
-__device__ __forceinline__ void unpack8(const uint4& q, float* v) {
-    const __nv_bfloat162* b = reinterpret_cast<const __nv_bfloat162*>(&q);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const float2 f = __bfloat1622float2(b[i]);
-        v[2 * i] = f.x;
-        v[2 * i + 1] = f.y;
-    }
-}
-__device__ __forceinline__ uint4 pack8(const float* v) {
-    uint4 q;
-    uint32_t* w = reinterpret_cast<uint32_t*>(&q);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const __nv_bfloat162 b = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
-        w[i] = *reinterpret_cast<const uint32_t*>(&b);
-    }
-    return q;
-}
-
-// 2x2 average: out[n, Y, X, c] = 0.25 * ((a + b) + (c + d)) in FP32, NHWC, 8 channels per thread.
-__global__ void k_pool(const bf16* __restrict__ in, bf16* __restrict__ out, int nimg, int H, int W, int c) {
-    const int Ho = H / 2, Wo = W / 2, c8 = c / 8;
-    const size_t total = (size_t)nimg * Ho * Wo * c8;
-    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
-        const int ch = (int)(q % c8) * 8;
-        const size_t r = q / c8;  // output pixel
-        const int X = (int)(r % Wo);
-        const size_t r2 = r / Wo;
-        const int Y = (int)(r2 % Ho);
-        const int img = (int)(r2 / Ho);
-        const size_t b = (((size_t)img * H + 2 * Y) * W + 2 * X) * c + ch;
-        float v00[8], v01[8], v10[8], v11[8], o[8];
-        unpack8(*reinterpret_cast<const uint4*>(in + b), v00);
-        unpack8(*reinterpret_cast<const uint4*>(in + b + c), v01);
-        unpack8(*reinterpret_cast<const uint4*>(in + b + (size_t)W * c), v10);
-        unpack8(*reinterpret_cast<const uint4*>(in + b + (size_t)W * c + c), v11);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) o[i] = 0.25f * ((v00[i] + v01[i]) + (v10[i] + v11[i]));
-        *reinterpret_cast<uint4*>(out + r * c + ch) = pack8(o);
-    }
-}
-
 // nearest upsampling x2: out[n, y, x, :] = in[n, y/2, x/2, :], 8 channels per thread.
 __global__ void k_up(const bf16* __restrict__ in, bf16* __restrict__ out, int nimg, int H, int W, int c) {
     const int c8 = c / 8;
@@ -338,27 +326,6 @@ __global__ void k_up(const bf16* __restrict__ in, bf16* __restrict__ out, int ni
         const int img = (int)(r2 / H);
         *reinterpret_cast<uint4*>(out + r * c + ch) =
             *reinterpret_cast<const uint4*>(in + (((size_t)img * (H / 2) + y / 2) * (W / 2) + x / 2) * c + ch);
-    }
-}
-
-// head: out32 = wh . d1b + bh; x0 = out32 * sigma * hsq * rho (the local 1/beta scale: the
-// pressure inside a light bubble is larger by the density ratio).
-__global__ void k_head(const bf16* __restrict__ d, const float* __restrict__ wh, const float* __restrict__ bh,
-                       const double* __restrict__ sigma, const double* __restrict__ rho, double hsq,
-                       float* __restrict__ out32, double* __restrict__ x0, int npix, int nimg) {
-    const size_t total = (size_t)npix * nimg;
-    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < total; p += (size_t)gridDim.x * blockDim.x) {
-        float s = bh[0];
-        const uint4* dp = reinterpret_cast<const uint4*>(d + p * kHead);
-#pragma unroll
-        for (int q = 0; q < kHead / 8; ++q) {
-            float v[8];
-            unpack8(dp[q], v);
-#pragma unroll
-            for (int i = 0; i < 8; ++i) s += wh[8 * q + i] * v[i];
-        }
-        out32[p] = s;
-        if (x0) x0[p] = (double)s * sigma[p / npix] * hsq * rho[p];
     }
 }
 
@@ -715,10 +682,11 @@ int pack_all(lica_unet* u, cudaStream_t s) {
     return LICA_OK;
 }
 
-int conv_layer(lica_unet* u, int l, const bf16* x0, const bf16* x1, bf16* out, cudaStream_t s) {
+int conv_layer(lica_unet* u, int l, const bf16* x0, const bf16* x1, bf16* out, cudaStream_t s,
+               const ConvFuse* fuse = nullptr) {
     const LayerDef& L = kNet[l];
     return conv3x3(x0, L.cin0, x1, L.cin1, u->wb[l], u->param + u->boff[l], u->n, u->h >> L.level, u->w >> L.level,
-                   L.cout, 1, out, nullptr, L.cout, 0, u->err, s);
+                   L.cout, 1, out, nullptr, L.cout, 0, u->err, s, fuse);
 }
 
 template <typename K, typename... A>
@@ -729,22 +697,32 @@ int launch(size_t n, cudaStream_t s, K kernel, A... args) {
     return LICA_OK;
 }
 
-// Forward pass: input tensor from (rho, f), every activation kept, the guess x0 (if given).
-int forward(lica_unet* u, const double* rho, const double* f, double hsq, double* x0, cudaStream_t s) {
+// Forward pass: input tensor from (rho, f), every activation kept (the last one, d1b, only
+// with keep_last: the head is fused into its convolution), the head output and the guess
+// x0 (if given).  The 2x2 poolings are fused into the convolutions that produce e1b and e2b.
+int forward(lica_unet* u, const double* rho, const double* f, double hsq, double* x0, cudaStream_t s,
+            bool keep_last = true) {
     const int npix = u->h * u->w;
     int st;
     k_rms_part<<<dim3(kRmsParts, u->n), kNT, 0, s>>>(f, u->rms_part, npix);
-    k_rms_final<<<u->n, 32, 0, s>>>(u->rms_part, u->sigma, npix);
+    k_rms_final<<<u->n, kNT, 0, s>>>(u->rms_part, u->sigma, npix);
     LICA_CUDA_TRY(cudaGetLastError());
     lica_count_launches(2);
     if ((st = launch(level_pixels(u, 0), s, k_input, rho, f, (const double*)u->sigma, u->x16, npix, u->n))) return st;
     const int h = u->h, w = u->w, n = u->n;
+    ConvFuse pool1, pool2, head;
+    pool1.pool = u->p1;
+    pool2.pool = u->p2;
+    head.head_w = u->param + u->hoff;
+    head.head_out = u->out32;
+    head.head_x0 = x0;
+    head.head_rho = rho;
+    head.head_sigma = u->sigma;
+    head.hsq = hsq;
     if ((st = conv_layer(u, 0, u->x16, nullptr, u->y[0], s))) return st;
-    if ((st = conv_layer(u, 1, u->y[0], nullptr, u->y[1], s))) return st;
-    if ((st = launch(level_pixels(u, 1) * 4, s, k_pool, (const bf16*)u->y[1], u->p1, n, h, w, 32))) return st;
+    if ((st = conv_layer(u, 1, u->y[0], nullptr, u->y[1], s, &pool1))) return st;
     if ((st = conv_layer(u, 2, u->p1, nullptr, u->y[2], s))) return st;
-    if ((st = conv_layer(u, 3, u->y[2], nullptr, u->y[3], s))) return st;
-    if ((st = launch(level_pixels(u, 2) * 8, s, k_pool, (const bf16*)u->y[3], u->p2, n, h / 2, w / 2, 64))) return st;
+    if ((st = conv_layer(u, 3, u->y[2], nullptr, u->y[3], s, &pool2))) return st;
     if ((st = conv_layer(u, 4, u->p2, nullptr, u->y[4], s))) return st;
     if ((st = conv_layer(u, 5, u->y[4], nullptr, u->y[5], s))) return st;
     if ((st = launch(level_pixels(u, 1) * 16, s, k_up, (const bf16*)u->y[5], u->u2, n, h / 2, w / 2, 128))) return st;
@@ -752,10 +730,7 @@ int forward(lica_unet* u, const double* rho, const double* f, double hsq, double
     if ((st = conv_layer(u, 7, u->y[6], nullptr, u->y[7], s))) return st;
     if ((st = launch(level_pixels(u, 0) * 8, s, k_up, (const bf16*)u->y[7], u->u1, n, h, w, 64))) return st;
     if ((st = conv_layer(u, 8, u->u1, u->y[1], u->y[8], s))) return st;
-    if ((st = conv_layer(u, 9, u->y[8], nullptr, u->y[9], s))) return st;
-    return launch(level_pixels(u, 0), s, k_head, (const bf16*)u->y[9], (const float*)(u->param + u->hoff),
-                  (const float*)(u->param + u->hoff + kHead), (const double*)u->sigma, rho, hsq, u->out32, x0, npix,
-                  n);
+    return conv_layer(u, 9, u->y[8], nullptr, keep_last ? u->y[9] : nullptr, s, &head);
 }
 
 int alloc_training(lica_unet* u) {
@@ -1006,7 +981,7 @@ int lica_unet_set_params(lica_unet* u, const float* host, int64_t count) {
 int lica_unet_guess_device(lica_unet* u, const double* rho, const double* f, double hsq, double* x0, void* stream) {
     if (!u || !rho || !f || !x0 || !(hsq > 0)) return LICA_BAD_ARG;
     cudaStream_t s = (cudaStream_t)stream;
-    int st = forward(u, rho, f, hsq, x0, s);
+    int st = forward(u, rho, f, hsq, x0, s, false);
     if (st) return st;
     return check_err(u, s);
 }
@@ -1020,7 +995,7 @@ int lica_unet_guess_checked_device(lica_unet* u, const double* rho, const double
     if (!u->ax) {
         if ((st = dev_alloc(&u->ax, p0))) return st;
     }
-    if ((st = forward(u, rho, f, hx * hy, x0, s))) return st;
+    if ((st = forward(u, rho, f, hx * hy, x0, s, false))) return st;
     if ((st = launch(p0, s, k_apply_op, (const double*)x0, bx, by, u->ax, u->n, u->h, u->w, 1.0 / (hx * hx),
                      1.0 / (hy * hy))))
         return st;

@@ -61,21 +61,32 @@ struct ConvParams {
     int kdx;              // dx taps per K block: 3 (all three halo boxes in one stage; resident
                           // weights only) or 1
     int tiles;            // pixel tiles of the whole launch
+    // fused consumers of the BF16 output (cout <= 64, out_c0 = 0), or null:
+    __nv_bfloat16* pool;       // 2x2 average, NHWC (h/2, w/2, cout): 0.25 ((a + b) + (c + d)) in FP32
+    const float* head_w;       // 1x1 head over cout = 32 channels: [wh (32), bh]
+    float* head_out;           // head output per pixel, FP32 (bh + sum_c wh[c] y[c], c ascending)
+    double* head_x0;           // (or null) x0 = head_out * sigma[img] * hsq * rho
+    const double* head_rho;
+    const double* head_sigma;
+    double hsq;
 };
 
 constexpr int kConvThreads = 192;
 
-constexpr int kBiasBytes = 1024;  // the bias (cout <= 256 floats), after the barriers
+constexpr int kBiasBytes = 2048;  // the bias (cout <= 256 floats) and the head [wh, bh], after the barriers
 
 __host__ __device__ inline size_t conv_p_smem_bytes(int stage_a, int stage_b, int nstages, int wres) {
     return 1024 + (size_t)nstages * (stage_a + stage_b) + (size_t)wres + kBarBytes + kBiasBytes;
 }
 
 // Bias, ReLU, BF16 (and FP32) stores of the columns c0 .. c0 + min(ncols, NC) - 1 of one
-// pixel held in registers.
+// pixel held in registers, and the fused consumers of the BF16 values: the 2x2 pool (the
+// four pixels of a block are lanes l, l^1, l^8, l^9 of one warp; the lane with both bits
+// clear stores) and the head's running dot product.  Called by whole warps.
 template <int NC>
-__device__ __forceinline__ void conv_epilogue_store(const ConvParams& P, const float* sbias, size_t pix, int c0,
-                                                    const uint32_t* r, int ncols) {
+__device__ __forceinline__ void conv_epilogue_store(const ConvParams& P, const float* sbias, const float* shead,
+                                                    size_t pix, size_t ppix, int lane, int c0, const uint32_t* r,
+                                                    int ncols, float& head) {
 #pragma unroll
     for (int g = 0; g < NC / 16; ++g) {
         if (16 * g < ncols) {
@@ -87,13 +98,13 @@ __device__ __forceinline__ void conv_epilogue_store(const ConvParams& P, const f
                 v[i] = a;
             }
             const size_t o = pix * P.out_c + P.out_c0 + c0 + 16 * g;
-            if (P.out) {
-                uint32_t pk[8];
+            uint32_t pk[8];
 #pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
-                    pk[i] = *reinterpret_cast<const uint32_t*>(&b2);
-                }
+            for (int i = 0; i < 8; ++i) {
+                const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+                pk[i] = *reinterpret_cast<const uint32_t*>(&b2);
+            }
+            if (P.out) {
                 uint4* dst = reinterpret_cast<uint4*>(P.out + o);
                 dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
                 dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
@@ -102,6 +113,38 @@ __device__ __forceinline__ void conv_epilogue_store(const ConvParams& P, const f
                 float4* dst = reinterpret_cast<float4*>(P.out32 + o);
 #pragma unroll
                 for (int i = 0; i < 4; ++i) dst[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+            }
+            if (P.pool || P.head_w) {
+                float vb[16];  // the stored BF16 values
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&pk[i]));
+                    vb[2 * i] = f.x;
+                    vb[2 * i + 1] = f.y;
+                }
+                if (P.pool) {
+                    float q[16];
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) {
+                        const float pair = vb[i] + __shfl_xor_sync(0xffffffffu, vb[i], 1);  // a + b | c + d
+                        q[i] = 0.25f * (pair + __shfl_xor_sync(0xffffffffu, pair, 8));
+                    }
+                    if ((lane & 9) == 0) {
+                        uint32_t qk[8];
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) {
+                            const __nv_bfloat162 b2 = __floats2bfloat162_rn(q[2 * i], q[2 * i + 1]);
+                            qk[i] = *reinterpret_cast<const uint32_t*>(&b2);
+                        }
+                        uint4* dst = reinterpret_cast<uint4*>(P.pool + ppix * P.cout + c0 + 16 * g);
+                        dst[0] = make_uint4(qk[0], qk[1], qk[2], qk[3]);
+                        dst[1] = make_uint4(qk[4], qk[5], qk[6], qk[7]);
+                    }
+                }
+                if (P.head_w) {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) head += shead[c0 + 16 * g + i] * vb[i];
+                }
             }
         }
     }
@@ -136,6 +179,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
     uint64_t* wready = bars + 2 * kStages + 4;  // resident weights landed
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 5);
     float* sbias = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(bars) + kBarBytes);
+    float* shead = sbias + 256;  // [wh (32), bh]
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -303,6 +347,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
     } else {
         // epilogue warps 0-3: pixel m = threadIdx.x = tensor-memory lane
         for (int i = threadIdx.x; i < P.cout; i += 128) sbias[i] = P.bias ? P.bias[i] : 0.f;
+        if (P.head_w && threadIdx.x <= 32) shead[threadIdx.x] = P.head_w[threadIdx.x];
         asm volatile("bar.sync 1, 128;" ::: "memory");  // the four epilogue warps
         int it = 0;
         for (int t = blockIdx.x; t < P.tiles; t += gridDim.x, ++it) {
@@ -320,6 +365,8 @@ __global__ void __launch_bounds__(kConvThreads, 1)
             const int m = threadIdx.x;
             const int y = y0 + m / P.tw, x = x0 + m % P.tw;
             const size_t pix = ((size_t)img * P.h + y) * P.w + x;
+            const size_t ppix = ((size_t)img * (P.h / 2) + y / 2) * (P.w / 2) + x / 2;
+            float head = P.head_w ? shead[32] : 0.f;
             const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(acc * P.tmem_cols);
             // whole 32-column chunks (the accumulator has tmem_cols >= the rounded-up cout)
             if (P.cout <= 64) {
@@ -331,14 +378,19 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                 tc::tmem_pin<64>(r);
                 tc::tc_fence_before();
                 tc::mbar_arrive(&tempty[acc]);
-                conv_epilogue_store<64>(P, sbias, pix, 0, r, P.cout);
+                conv_epilogue_store<64>(P, sbias, shead, pix, ppix, lane, 0, r, P.cout, head);
+                if (P.head_w) {
+                    P.head_out[pix] = head;
+                    if (P.head_x0)
+                        P.head_x0[pix] = (double)head * P.head_sigma[img] * P.hsq * P.head_rho[pix];
+                }
             } else {
                 for (int c0 = 0; c0 < P.cout; c0 += 32) {
                     uint32_t r[32];
                     tc::tmem_ld32_nowait(taddr + (uint32_t)c0, r);
                     tc::tmem_wait_ld();
                     tc::tmem_pin<32>(r);
-                    conv_epilogue_store<32>(P, sbias, pix, c0, r, P.cout - c0);
+                    conv_epilogue_store<32>(P, sbias, shead, pix, ppix, lane, c0, r, P.cout - c0, head);
                 }
                 tc::tc_fence_before();
                 tc::mbar_arrive(&tempty[acc]);
