@@ -12,13 +12,16 @@
 // taps dy = 0, 1, 2: 8 pixel rows are one swizzle atom, so the A operand of tap dy starts
 // dy atoms into the box.  Persistent CTAs of 6 warps
 // walk the tiles t = blockIdx.x, + gridDim.x, ...:
-//   warp 4 lane 0 : TMA producer, streaming the K blocks of consecutive tiles through a
-//                   ring of kStages stages (full/empty mbarriers) without draining it
-//   warp 5 lane 0 : MMA issuer, 128 x cout x 16 per instruction, FP32 accumulators in
-//                   tensor memory, two of them (tile parity) so that the epilogue of one
-//                   tile overlaps the MMAs of the next
-//   warps 0-3     : epilogue, tensor memory -> registers (warp w reads lanes 32w..32w+31
-//                   = pixels), + bias, optional ReLU, BF16 NHWC store (optionally FP32)
+//   warp 4        : TMA producer, streaming the K blocks of consecutive tiles through a
+//                   ring of stages (full/empty mbarriers) without draining it
+//   warp 5        : MMA issuer, 128 x cout x 16 per instruction, FP32 accumulators in
+//                   tensor memory, two of them (tile parity)
+//   warps 0-3, 6-9: epilogue, one group of four warps per accumulator so that two tiles
+//                   drain while the next is multiplied: tensor memory -> registers (warp w
+//                   reads lanes 32 (w % 4) + 0..31 = pixels), + bias, optional ReLU, BF16
+//                   NHWC store (optionally FP32), optional fused 2x2 pool or 1x1 head
+// Warps 4 and 5 run their loops converged; one elected lane issues each TMA copy, MMA and
+// commit.
 // Stage sizes follow the layer's channel block (A: kdx x 144 x cblk, B: 3 x cout x cblk
 // BF16).  When the whole weight matrix fits in shared memory beside the ring it is loaded
 // once per CTA (resident weights), the stages carry only activations, and a stage holds
@@ -71,7 +74,7 @@ struct ConvParams {
     double hsq;
 };
 
-constexpr int kConvThreads = 192;
+constexpr int kConvThreads = 320;  // epilogue warps 0-3 and 6-9, producer warp 4, MMA warp 5
 
 constexpr int kBiasBytes = 2048;  // the bias (cout <= 256 floats) and the head [wh, bh], after the barriers
 
@@ -345,13 +348,18 @@ __global__ void __launch_bounds__(kConvThreads, 1)
             __syncwarp();
         }
     } else {
-        // epilogue warps 0-3: pixel m = threadIdx.x = tensor-memory lane
-        for (int i = threadIdx.x; i < P.cout; i += 128) sbias[i] = P.bias ? P.bias[i] : 0.f;
-        if (P.head_w && threadIdx.x <= 32) shead[threadIdx.x] = P.head_w[threadIdx.x];
-        asm volatile("bar.sync 1, 128;" ::: "memory");  // the four epilogue warps
-        int it = 0;
-        for (int t = blockIdx.x; t < P.tiles; t += gridDim.x, ++it) {
-            const int acc = it & 1, use = it >> 1;
+        // epilogue: two groups of four warps, group e = warps 0-3 / 6-9 drains accumulator e
+        // (the tiles it = e, e + 2, ...); warp w reads tensor-memory lanes 32 (w % 4) + lane,
+        // pixel m = that lane
+        const int e = warp < 4 ? 0 : 1, quarter = warp & 3;
+        if (e == 0) {
+            for (int i = threadIdx.x; i < P.cout; i += 128) sbias[i] = P.bias ? P.bias[i] : 0.f;
+            if (P.head_w && threadIdx.x <= 32) shead[threadIdx.x] = P.head_w[threadIdx.x];
+        }
+        asm volatile("bar.sync 1, 256;" ::: "memory");  // the eight epilogue warps
+        int it = e;
+        for (int t = blockIdx.x + e * gridDim.x; t < P.tiles; t += 2 * gridDim.x, it += 2) {
+            const int acc = e, use = it >> 1;
             int ok = 1;
             if (lane == 0) ok = tc::mbar_wait(&tfull[acc], use & 1) ? 1 : 0;
             ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -362,12 +370,12 @@ __global__ void __launch_bounds__(kConvThreads, 1)
             tc::tc_fence_after();
             int img, x0, y0;
             tile_origin(P, t, img, x0, y0);
-            const int m = threadIdx.x;
+            const int m = quarter * 32 + lane;
             const int y = y0 + m / P.tw, x = x0 + m % P.tw;
             const size_t pix = ((size_t)img * P.h + y) * P.w + x;
             const size_t ppix = ((size_t)img * (P.h / 2) + y / 2) * (P.w / 2) + x / 2;
             float head = P.head_w ? shead[32] : 0.f;
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(acc * P.tmem_cols);
+            const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * P.tmem_cols);
             // whole 32-column chunks (the accumulator has tmem_cols >= the rounded-up cout)
             if (P.cout <= 64) {
                 // the whole accumulator in registers: release it before the stores
