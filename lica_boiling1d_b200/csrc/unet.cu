@@ -170,37 +170,45 @@ int conv3x3(const __nv_bfloat16* x0, int c0, const __nv_bfloat16* x1, int c1, co
         P.head_sigma = fuse->head_sigma;
         P.hsq = fuse->hsq;
     }
-    CUtensorMap mx0, mx1, mw0, mw1;
-    int st;
-    if ((st = act_map(&mx0, x0, c0, wd, h, n, P.cblk[0], tw, th + 2))) return st;
-    if ((st = weight_map(&mw0, w, 9 * P.ctot, cout, P.cblk[0]))) return st;
-    if (P.nsrc > 1) {
-        if ((st = act_map(&mx1, x1, c1, wd, h, n, P.cblk[1], tw, th + 2))) return st;
-        if ((st = weight_map(&mw1, w, 9 * P.ctot, cout, P.cblk[1]))) return st;
-    } else {
-        mx1 = mx0;
-        mw1 = mw0;
-    }
-    const int tiles = n * (h / th) * (wd / tw);
     const int cbmax = std::max(P.cblk[0], P.nsrc > 1 ? P.cblk[1] : 0);
-    P.stage_a = ((kHaloRows * cbmax * 2 + 1023) / 1024) * 1024;
-    P.tiles = tiles;
+    const auto round_kb = [](int b) { return ((b + 1023) / 1024) * 1024; };
     // Resident weights: the whole cout x (9 ctot) matrix (one box per tap, input and
     // channel block) stays in shared memory for all tiles of the CTA when it fits beside
-    // a ring of at least three A stages and every box starts on its swizzle atom; the
-    // ring then carries only the activation halo boxes.
+    // the ring and every box starts on its swizzle atom; the ring then carries only the
+    // activation boxes.
     const int wres = 18 * cout * P.ctot;
     const int avail = kConvSmemMax - 1024 - kBarBytes - kBiasBytes;
-    bool resident = avail - wres >= 3 * P.stage_a;  // beside three 1-box stages
-    for (int tap = 0; tap < 9; ++tap)
-        for (int src = 0; src < P.nsrc; ++src)
-            for (int c = src ? c0 : 0; c < (src ? P.ctot : c0); c += P.cblk[src])
-                if ((2 * cout * (tap * P.ctot + c)) % (16 * P.cblk[src])) resident = false;
-    if (resident) {
+    const auto boxes_aligned = [&](bool wide) {
+        for (int tap = 0; tap < 9; ++tap)
+            for (int src = 0; src < P.nsrc; ++src)
+                for (int c = src ? c0 : 0; c < (src ? P.ctot : c0); c += P.cblk[src]) {
+                    const int at = wide ? 3 * (tap / 3) * P.ctot + 3 * c + (tap % 3) * P.cblk[src] : tap * P.ctot + c;
+                    if ((2 * cout * at) % (16 * P.cblk[src])) return false;
+                }
+        return true;
+    };
+    // wide mode (N = 3 cout): resident weights beside at least two window stages.  Chosen
+    // for 32 output channels from at least 64 input channels, where one N = 96 MMA
+    // replaces three N = 32 ones and the tile's 9 ctot / 16 of them dominate; for fewer
+    // input channels or 64 outputs the 14-column tiles and the shifted-sum epilogue cost
+    // more than they save.
+    const int stage_w = round_kb(kWideRows * cbmax * 2);
+    P.stage_a = round_kb(kHaloRows * cbmax * 2);
+    if (cout == 32 && P.ctot >= 64 && wd >= kWideBoxW && h >= kWideBoxH && avail - wres >= 2 * stage_w && boxes_aligned(true)) {
+        P.wide = 1;
+        P.tw = kWideTileW;
+        P.th = kWideTileH;
+        P.tmem_cols = tmem_columns(3 * cout);
+        P.wres = wres;
+        P.stage_a = stage_w;
+        P.stage_b = 0;
+        P.kdx = 3;
+        P.nstages = std::min<int>(kStages, (avail - wres) / stage_w);
+    } else if (avail - wres >= 3 * P.stage_a && boxes_aligned(false)) {
         P.wres = wres;
         P.stage_b = 0;
         // all three dx boxes per stage when at least two such stages fit
-        const int stage3 = ((3 * kHaloRows * cbmax * 2 + 1023) / 1024) * 1024;
+        const int stage3 = round_kb(3 * kHaloRows * cbmax * 2);
         if ((avail - wres) / stage3 >= 2) {
             P.kdx = 3;
             P.stage_a = stage3;
@@ -211,9 +219,23 @@ int conv3x3(const __nv_bfloat16* x0, int c0, const __nv_bfloat16* x1, int c1, co
     } else {
         P.wres = 0;
         P.kdx = 1;
-        P.stage_b = ((3 * cout * cbmax * 2 + 1023) / 1024) * 1024;
+        P.stage_b = round_kb(3 * cout * cbmax * 2);
         P.nstages = std::min<int>(kStages, avail / (P.stage_a + P.stage_b));
     }
+    const int box_w = P.wide ? kWideBoxW : tw, box_h = P.wide ? kWideBoxH : th + 2;
+    CUtensorMap mx0, mx1, mw0, mw1;
+    int st;
+    if ((st = act_map(&mx0, x0, c0, wd, h, n, P.cblk[0], box_w, box_h))) return st;
+    if ((st = weight_map(&mw0, w, 9 * P.ctot, cout, P.cblk[0]))) return st;
+    if (P.nsrc > 1) {
+        if ((st = act_map(&mx1, x1, c1, wd, h, n, P.cblk[1], box_w, box_h))) return st;
+        if ((st = weight_map(&mw1, w, 9 * P.ctot, cout, P.cblk[1]))) return st;
+    } else {
+        mx1 = mx0;
+        mw1 = mw0;
+    }
+    const int tiles = n * (h / P.th) * ((wd + P.tw - 1) / P.tw);
+    P.tiles = tiles;
     if (P.nstages < 1) return LICA_BAD_ARG;
     const size_t smem = conv_p_smem_bytes(P.stage_a, P.stage_b, P.nstages, P.wres);
     // CTAs per SM: shared memory and tensor memory (two accumulators of tmem_cols each)

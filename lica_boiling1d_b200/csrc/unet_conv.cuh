@@ -43,6 +43,9 @@ static_assert((2 * kStages + 5) * 8 + 4 <= kBarBytes, "barrier region too small"
 constexpr int kTileM = 128;
 constexpr int kTileW = 8, kTileH = 16;          // pixel tile: 16 rows x 8 columns
 constexpr int kHaloRows = kTileW * (kTileH + 2);  // A box: 18 rows x 8 columns = 144 pixel rows
+// wide mode: A box of 10 rows x 16 columns (160 pixel rows), output tile 8 rows x 14 columns
+constexpr int kWideBoxW = 16, kWideBoxH = 10, kWideRows = kWideBoxW * kWideBoxH;
+constexpr int kWideTileW = 14, kWideTileH = 8;
 
 struct ConvParams {
     int n, h, w;          // image count and size (output = input size)
@@ -64,6 +67,10 @@ struct ConvParams {
     int kdx;              // dx taps per K block: 3 (all three halo boxes in one stage; resident
                           // weights only) or 1
     int tiles;            // pixel tiles of the whole launch
+    int wide;             // 1: one MMA covers the three dx taps (N = 3 cout, resident weights in
+                          // the order [dy][channel block][dx]); the A box is the 16-column
+                          // window x0 - 1 .. x0 + 14 and the epilogue adds the partial sums
+                          // E_dx shifted by dx pixels (lanes) to the 14 output columns
     // fused consumers of the BF16 output (cout <= 64, out_c0 = 0), or null:
     __nv_bfloat16* pool;       // 2x2 average, NHWC (h/2, w/2, cout): 0.25 ((a + b) + (c + d)) in FP32
     const float* head_w;       // 1x1 head over cout = 32 channels: [wh (32), bh]
@@ -88,8 +95,9 @@ __host__ __device__ inline size_t conv_p_smem_bytes(int stage_a, int stage_b, in
 // clear stores) and the head's running dot product.  Called by whole warps.
 template <int NC>
 __device__ __forceinline__ void conv_epilogue_store(const ConvParams& P, const float* sbias, const float* shead,
-                                                    size_t pix, size_t ppix, int lane, int c0, const uint32_t* r,
-                                                    int ncols, float& head) {
+                                                    size_t pix, size_t ppix, int lane, bool valid, int c0,
+                                                    const uint32_t* r, int ncols, float& head) {
+    const int yx = P.wide ? 16 : 8;  // lane distance of the pixel below
 #pragma unroll
     for (int g = 0; g < NC / 16; ++g) {
         if (16 * g < ncols) {
@@ -107,12 +115,12 @@ __device__ __forceinline__ void conv_epilogue_store(const ConvParams& P, const f
                 const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
                 pk[i] = *reinterpret_cast<const uint32_t*>(&b2);
             }
-            if (P.out) {
+            if (P.out && valid) {
                 uint4* dst = reinterpret_cast<uint4*>(P.out + o);
                 dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
                 dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
             }
-            if (P.out32) {
+            if (P.out32 && valid) {
                 float4* dst = reinterpret_cast<float4*>(P.out32 + o);
 #pragma unroll
                 for (int i = 0; i < 4; ++i) dst[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
@@ -130,9 +138,9 @@ __device__ __forceinline__ void conv_epilogue_store(const ConvParams& P, const f
 #pragma unroll
                     for (int i = 0; i < 16; ++i) {
                         const float pair = vb[i] + __shfl_xor_sync(0xffffffffu, vb[i], 1);  // a + b | c + d
-                        q[i] = 0.25f * (pair + __shfl_xor_sync(0xffffffffu, pair, 8));
+                        q[i] = 0.25f * (pair + __shfl_xor_sync(0xffffffffu, pair, yx));
                     }
-                    if ((lane & 9) == 0) {
+                    if (valid && (lane & (1 | yx)) == 0) {
                         uint32_t qk[8];
 #pragma unroll
                         for (int i = 0; i < 8; ++i) {
@@ -154,7 +162,7 @@ __device__ __forceinline__ void conv_epilogue_store(const ConvParams& P, const f
 }
 
 __device__ __forceinline__ void tile_origin(const ConvParams& P, int t, int& img, int& x0, int& y0) {
-    const int tiles_x = P.w / P.tw, tiles_y = P.h / P.th;
+    const int tiles_x = (P.w + P.tw - 1) / P.tw, tiles_y = P.h / P.th;
     const int tx = t % tiles_x;
     t /= tiles_x;
     const int ty = t % tiles_y;
@@ -210,7 +218,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
     const uint32_t tmem = *tmem_slot;
 
     const int nb0 = P.cin[0] / P.cblk[0], nb1 = P.nsrc > 1 ? P.cin[1] / P.cblk[1] : 0;
-    const int kdx = P.kdx;
+    const int kdx = P.kdx;  // 3 in wide mode (every K block covers the three dx taps)
     const int nkb = (3 / kdx) * (nb0 + nb1);  // K blocks: (dx group, source, channel block)
 
     // Warps 4 and 5 run their loops with all 32 lanes (warp-uniform control and descriptor
@@ -224,9 +232,12 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                     for (int src = 0; src < P.nsrc; ++src) {
                         const int cblk = (src ? P.cblk[1] : P.cblk[0]), off = src ? P.cin[0] : 0;
                         const void* tmw = src ? (const void*)&tm_w1 : (const void*)&tm_w0;
+                        const int dy = tap / 3, dx = tap % 3;
                         for (int cb = 0; cb < (src ? nb1 : nb0); ++cb) {
-                            const int c = tap * P.ctot + off + cb * cblk;
-                            tc::tma_load_2d(sw + 2 * P.cout * c, tmw, wready, c, 0);
+                            const int col = off + cb * cblk, c = tap * P.ctot + col;
+                            // narrow: [tap][column]; wide: [dy][column block][dx]
+                            const int at = P.wide ? 3 * dy * P.ctot + 3 * col + dx * cblk : c;
+                            tc::tma_load_2d(sw + 2 * P.cout * at, tmw, wready, c, 0);
                         }
                     }
             }
@@ -246,7 +257,15 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                     break;
                 }
                 const int cblk = (src ? P.cblk[1] : P.cblk[0]);
-                if (tc::elect_one()) {
+                if (P.wide) {
+                    // the 16 x 10 window (output columns x0 .. x0 + 13 need inputs x0 - 1 ..
+                    // x0 + 14; rows y0 - 1 .. y0 + 8)
+                    if (tc::elect_one()) {
+                        tc::mbar_expect_tx(&full[s], (uint32_t)kWideRows * cblk * 2);
+                        const void* tmx = src ? (const void*)&tm_x1 : (const void*)&tm_x0;
+                        tc::tma_load_4d(sa + s * P.stage_a, tmx, &full[s], cb * cblk, x0 - 1, y0 - 1, img);
+                    }
+                } else if (tc::elect_one()) {
                     const int bsub = P.cout * cblk * 2;  // bytes of one tap's weight slice
                     tc::mbar_expect_tx(&full[s],
                                        (uint32_t)(kdx * kHaloRows + (P.wres ? 0 : 3 * P.cout)) * cblk * 2);
@@ -274,7 +293,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
         }
     } else if (warp == 5) {
         // MMA issuer
-        const uint32_t idesc = tc::idesc_bf16_f32(kTileM, (uint32_t)P.cout);
+        const uint32_t idesc = tc::idesc_bf16_f32(kTileM, (uint32_t)(P.wide ? 3 * P.cout : P.cout));
         // descriptors of stage 0 (A, streamed B) or of the resident weights per input; the
         // descriptor of an address a + 16 j is desc(a) + j (all shared addresses < 256 KB)
         const uint64_t a_base0 = tc::smem_desc(sa, 2u * P.cblk[0]), a_base1 = tc::smem_desc(sa, 2u * P.cblk[1]);
@@ -308,10 +327,15 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                 // (8 pixel rows = one swizzle atom of 8 * 2 cblk bytes) into the halo box.
                 // B: the (dy, dx) weight box, resident or in the stage.
                 const uint64_t a = (src ? a_base1 : a_base0) + (uint32_t)(s * P.stage_a) / 16u;
-                const uint32_t a_dy = (uint32_t)cblk;
+                // wide: one image row of the window is 16 pixel rows = two atoms
+                const uint32_t a_dy = (uint32_t)(P.wide ? 2 * cblk : cblk);
                 uint64_t b;
                 uint32_t b_dy;
-                if (P.wres) {
+                if (P.wide) {
+                    // the three dx boxes of (dy, column block) are one 3 cout-row operand
+                    b = (src ? b_base1 : b_base0) + (uint32_t)(3 * P.cout * col) / 8u;
+                    b_dy = b_dy_res;
+                } else if (P.wres) {
                     b = (src ? b_base1 : b_base0) + (uint32_t)(P.cout * (dx * P.ctot + col)) / 8u;
                     b_dy = b_dy_res;
                 } else {
@@ -322,10 +346,11 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                 // next dx box of the stage: 144 rows of 2 cblk bytes further (A); the weight
                 // box of tap dx + 1 is ctot columns further (resident weights only: kdx = 3)
                 const uint32_t a_dx = 18u * (uint32_t)cblk, b_dx = (uint32_t)(P.cout * P.ctot) / 8u;
+                const int nj = P.wide ? 1 : kdx;  // A boxes in the stage
                 if (tc::elect_one()) {
 #pragma unroll
                     for (int j = 0; j < 3; ++j)
-                        if (j < kdx)
+                        if (j < nj)
 #pragma unroll
                             for (int dy = 0; dy < 3; ++dy)
 #pragma unroll
@@ -371,13 +396,44 @@ __global__ void __launch_bounds__(kConvThreads, 1)
             int img, x0, y0;
             tile_origin(P, t, img, x0, y0);
             const int m = quarter * 32 + lane;
-            const int y = y0 + m / P.tw, x = x0 + m % P.tw;
+            // wide: lane m holds the window column m % 16 (input x0 - 1 + m % 16) whose output
+            // column is x0 + m % 16 once the shifted partial sums are added; 14 are valid
+            const int xx = P.wide ? (m & 15) : m % P.tw, yy = P.wide ? (m >> 4) : m / P.tw;
+            const int y = y0 + yy, x = x0 + xx;
+            const bool valid = !P.wide || (xx < kWideTileW && x < P.w);
             const size_t pix = ((size_t)img * P.h + y) * P.w + x;
             const size_t ppix = ((size_t)img * (P.h / 2) + y / 2) * (P.w / 2) + x / 2;
             float head = P.head_w ? shead[32] : 0.f;
             const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * P.tmem_cols);
             // whole 32-column chunks (the accumulator has tmem_cols >= the rounded-up cout)
-            if (P.cout <= 64) {
+            if (P.wide) {
+                // D[x] = (E_0[x] + E_1[x + 1]) + E_2[x + 2], 32 output channels at a time
+                for (int c0 = 0; c0 < P.cout; c0 += 32) {
+                    uint32_t r[32], e1[32], e2[32];
+                    tc::tmem_ld32_nowait(taddr + (uint32_t)c0, r);
+                    tc::tmem_ld32_nowait(taddr + (uint32_t)(P.cout + c0), e1);
+                    tc::tmem_ld32_nowait(taddr + (uint32_t)(2 * P.cout + c0), e2);
+                    tc::tmem_wait_ld();
+                    tc::tmem_pin<32>(r);
+                    tc::tmem_pin<32>(e1);
+                    tc::tmem_pin<32>(e2);
+                    if (c0 + 32 >= P.cout) {
+                        tc::tc_fence_before();
+                        tc::mbar_arrive(&tempty[acc]);
+                    }
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) {
+                        const float a = __uint_as_float(r[i]) + __shfl_down_sync(0xffffffffu, __uint_as_float(e1[i]), 1);
+                        r[i] = __float_as_uint(a + __shfl_down_sync(0xffffffffu, __uint_as_float(e2[i]), 2));
+                    }
+                    conv_epilogue_store<32>(P, sbias, shead, pix, ppix, lane, valid, c0, r, P.cout - c0, head);
+                }
+                if (P.head_w && valid) {
+                    P.head_out[pix] = head;
+                    if (P.head_x0)
+                        P.head_x0[pix] = (double)head * P.head_sigma[img] * P.hsq * P.head_rho[pix];
+                }
+            } else if (P.cout <= 64) {
                 // the whole accumulator in registers: release it before the stores
                 uint32_t r[64];
                 tc::tmem_ld32_nowait(taddr, r);
@@ -386,7 +442,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                 tc::tmem_pin<64>(r);
                 tc::tc_fence_before();
                 tc::mbar_arrive(&tempty[acc]);
-                conv_epilogue_store<64>(P, sbias, shead, pix, ppix, lane, 0, r, P.cout, head);
+                conv_epilogue_store<64>(P, sbias, shead, pix, ppix, lane, true, 0, r, P.cout, head);
                 if (P.head_w) {
                     P.head_out[pix] = head;
                     if (P.head_x0)
@@ -398,7 +454,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                     tc::tmem_ld32_nowait(taddr + (uint32_t)c0, r);
                     tc::tmem_wait_ld();
                     tc::tmem_pin<32>(r);
-                    conv_epilogue_store<32>(P, sbias, shead, pix, ppix, lane, c0, r, P.cout - c0, head);
+                    conv_epilogue_store<32>(P, sbias, shead, pix, ppix, lane, true, c0, r, P.cout - c0, head);
                 }
                 tc::tc_fence_before();
                 tc::mbar_arrive(&tempty[acc]);

@@ -34,6 +34,8 @@ def _ref(x, w, bias, relu):
     (1, 32, 16, 64, 32, 32, 0),     # two sources with different swizzles
     (1, 16, 16, 64, 0, 192, 0),     # N = 192 (256 tensor-memory columns)
     (2, 48, 24, 32, 0, 16, 1),      # several tiles per image, N = 16
+    (1, 16, 40, 64, 0, 32, 1),      # 14-column output tiles (N = 3 x 32), last one ragged (28..39)
+    (2, 32, 24, 64, 32, 32, 0),     # two sources, ragged 14-column tiles
 ])
 def test_conv3x3_tensor_core(n, h, wd, c0, c1, cout, relu):
     import torch
