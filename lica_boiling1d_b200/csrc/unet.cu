@@ -335,24 +335,27 @@ __global__ void k_input(const double* __restrict__ rho, const double* __restrict
     }
 }
 
-// nearest upsampling x2: out[n, y, x, :] = in[n, y/2, x/2, :], 8 channels per thread.
+// nearest upsampling x2 (H x W the output size): each thread copies one 8-channel group
+// of an input pixel to its 2 x 2 output pixels.
 __global__ void k_up(const bf16* __restrict__ in, bf16* __restrict__ out, int nimg, int H, int W, int c) {
-    const int c8 = c / 8;
-    const size_t total = (size_t)nimg * H * W * c8;
+    const int c8 = c / 8, Hi = H / 2, Wi = W / 2;
+    const size_t total = (size_t)nimg * Hi * Wi * c8;
     for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
         const int ch = (int)(q % c8) * 8;
-        const size_t r = q / c8;
-        const int x = (int)(r % W);
-        const size_t r2 = r / W;
-        const int y = (int)(r2 % H);
-        const int img = (int)(r2 / H);
-        *reinterpret_cast<uint4*>(out + r * c + ch) =
-            *reinterpret_cast<const uint4*>(in + (((size_t)img * (H / 2) + y / 2) * (W / 2) + x / 2) * c + ch);
+        const size_t r = q / c8;  // input pixel
+        const int X = (int)(r % Wi);
+        const size_t r2 = r / Wi;
+        const int Y = (int)(r2 % Hi);
+        const int img = (int)(r2 / Hi);
+        const uint4 v = *reinterpret_cast<const uint4*>(in + r * c + ch);
+        bf16* o = out + (((size_t)img * H + 2 * Y) * W + 2 * X) * c + ch;
+        *reinterpret_cast<uint4*>(o) = v;
+        *reinterpret_cast<uint4*>(o + c) = v;
+        *reinterpret_cast<uint4*>(o + (size_t)W * c) = v;
+        *reinterpret_cast<uint4*>(o + (size_t)W * c + c) = v;
     }
 }
 
-// ---------------------------------------------------------------- backward kernels
-// g_d1b[p, c] = gout[p] * wh[c]
 __global__ void k_head_bwd(const float* __restrict__ gout, const float* __restrict__ wh, bf16* __restrict__ g,
                            size_t total) {
     for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < total; p += (size_t)gridDim.x * blockDim.x)
@@ -747,10 +750,10 @@ int forward(lica_unet* u, const double* rho, const double* f, double hsq, double
     if ((st = conv_layer(u, 3, u->y[2], nullptr, u->y[3], s, &pool2))) return st;
     if ((st = conv_layer(u, 4, u->p2, nullptr, u->y[4], s))) return st;
     if ((st = conv_layer(u, 5, u->y[4], nullptr, u->y[5], s))) return st;
-    if ((st = launch(level_pixels(u, 1) * 16, s, k_up, (const bf16*)u->y[5], u->u2, n, h / 2, w / 2, 128))) return st;
+    if ((st = launch(level_pixels(u, 2) * 16, s, k_up, (const bf16*)u->y[5], u->u2, n, h / 2, w / 2, 128))) return st;
     if ((st = conv_layer(u, 6, u->u2, u->y[3], u->y[6], s))) return st;
     if ((st = conv_layer(u, 7, u->y[6], nullptr, u->y[7], s))) return st;
-    if ((st = launch(level_pixels(u, 0) * 8, s, k_up, (const bf16*)u->y[7], u->u1, n, h, w, 64))) return st;
+    if ((st = launch(level_pixels(u, 1) * 8, s, k_up, (const bf16*)u->y[7], u->u1, n, h, w, 64))) return st;
     if ((st = conv_layer(u, 8, u->u1, u->y[1], u->y[8], s))) return st;
     return conv_layer(u, 9, u->y[8], nullptr, keep_last ? u->y[9] : nullptr, s, &head);
 }
