@@ -12,7 +12,9 @@ The line also carries the RK3 time-step legs ("rk3"): the 1-D boiling column of 
 cells (film 0.1, density ratio 1000, viscosity ratio 20, conductivity ratio 25, 10 K
 superheat) and a batch of 4096 independent columns of uneven length (128-2048 cells, 2-20 K,
 density ratio 100-1600), whole RK3 steps in one persistent launch, beside the CPU
-restatement's time for the same steps.
+restatement's time for the same steps; and the 2-D film-boiling step on 512 x 1536 (level
+set 1024 x 3072) with FP64 and mixed-precision pressure solves, its fields after one step
+compared with the FP64 CPU restatement.
 
 Under torchrun each rank solves its own replica (the 2-D multigrid does not shard
 here); value = solves of all ranks / the slowest rank's time.  Rank 0 prints one JSON
@@ -219,7 +221,8 @@ def profile_batch(ncol, steps, threads):
                       "cells": int(n.sum()), "status": int(st.max())}), flush=True)
 
 
-def rk3_legs(dev, flush, steps_c1=200, steps_c4=20, warmup=3, rank=0, world=1, slowest=lambda x: x):
+def rk3_legs(dev, flush, steps_c1=200, steps_c4=20, warmup=3, rank=0, world=1, slowest=lambda x: x, film_steps=10,
+             film_compare=False):
     import torch
 
     from lica_boiling1d_b200 import native, shard
@@ -306,6 +309,74 @@ def rk3_legs(dev, flush, steps_c1=200, steps_c4=20, warmup=3, rank=0, world=1, s
         "threads": th, "autotune_ms_per_step": trial, "gpu_launches": launches,
         "ranks": world, "sharding": "contiguous column blocks balanced by cells, strong scaling of the fixed batch",
         "gathered_columns": len(hist)}
+    if film_steps > 0:
+        out["film_2d"] = film_leg(dev, flush, steps=film_steps, compare=film_compare)
+    return out
+
+
+# ------------------------------------------------------------------ 2-D film boiling
+FILM = dict(nx=512, ny=1536, y0=64.0, amp=4.0)
+
+
+def film_leg(dev, flush, steps=10, warmup=2, compare=True):
+    """One RK3 step of 2-D film boiling on 512 x 1536 (level set 1024 x 3072; interface
+    y = 64 h + 4 h cos(2 pi x), superheat 5 K via Ja), FP64 and with mixed-precision pressure
+    solves: steps/s, pressure-solve iterations, and (compare) each field after one step against
+    the FP64 CPU restatement, whose time is the CPU baseline.  The state starts from the
+    hydrostatic pressure of the initial film."""
+    import torch
+
+    from lica_boiling1d_b200 import film2d as G
+    from lica_boiling1d_b200 import native
+    P = G.default_props()
+    nx, ny = FILM["nx"], FILM["ny"]
+    st0 = G.initial_state(nx, ny, FILM["y0"], FILM["amp"], props=P)
+    dt = G.stable_dt(nx, P)
+    out = {"workload": f"2-D film boiling, {nx} x {ny} MAC flow grid, level set {2 * nx} x {2 * ny}, interface "
+                       f"y = {FILM['y0']:.0f} h + {FILM['amp']:.0f} h cos(2 pi x / Lx), liquid/vapour ratios of the "
+                       "film-boiling benchmark (density 40, viscosity 20, conductivity 40, specific heat 2), "
+                       "superheat 5 K (Ja 0.1), Re 69.2, Fr 1; one RK3 step = 3 substeps (3 incremental MG-PCG "
+                       "pressure solves to 1e-8) + 2 reinitialisation iterations, FP64 physics",
+           "dt": dt, "inputs_vs_l2": "state and scratch (about 220 MB) larger than L2, plus a 256 MiB flush"}
+    first = {}
+    for prec in ("fp64", "mixed"):
+        gpu = G.Film2D(nx, ny, P, precision=prec)
+        state = G.to_device(st0)
+        gpu.step(state, dt)
+        torch.cuda.synchronize(dev)
+        first[prec] = G.to_host(state)
+        for _ in range(warmup):
+            gpu.step(state, dt)
+        torch.cuda.synchronize(dev)
+        flush.fill_(7)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = native.launch_count()
+        its = []
+        e0.record()
+        for _ in range(steps):
+            its.append(gpu.step(state, dt)["iterations"])
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1)
+        gpu.close()
+        out[prec] = {"steps_per_s": steps / (ms / 1e3), "ms_per_step": ms / steps, "steps": steps,
+                     "flow_cell_updates_per_s": nx * ny * steps / (ms / 1e3),
+                     "ls_cell_updates_per_s": 4 * nx * ny * steps / (ms / 1e3),
+                     "mg_iterations_per_substep": its[-1], "gpu_launches": native.launch_count() - l0}
+    if compare:
+        from oracle import film2d as F
+        t0 = time.perf_counter()
+        ref, info = F.step(st0, dt, P, F.oracle_mg(G.levels_for(nx, ny), P["rtol"]))
+        cpu_s = time.perf_counter() - t0
+        errs = {}
+        for prec in ("fp64", "mixed"):
+            errs[prec] = {k: float(np.linalg.norm(first[prec][k] - ref[k]) / max(np.linalg.norm(ref[k]), 1e-300))
+                          for k in ref}
+        out["rel_l2_error_vs_fp64_oracle"] = errs
+        out["oracle_mg_iterations"] = info["iterations"]
+        out["cpu_baseline"] = {"steps_per_s": 1.0 / cpu_s, "kind": "port", "cores": os.cpu_count(),
+                               "sample": "one step of the same workload: numpy restatement (one thread) with the "
+                                         "C++/OpenMP multigrid for the pressure solves"}
     return out
 
 
@@ -399,7 +470,8 @@ def run_ours(args):
     rk3 = None
     if not args.skip_rk3:
         rk3 = rk3_legs(dev, flush, steps_c1=args.c1_steps, steps_c4=args.c4_steps, rank=rank, world=world,
-                       slowest=slowest)
+                       slowest=slowest, film_steps=args.film_steps,
+                       film_compare=(rank == 0 and world == 1 and not args.skip_cpu))
         if rank == 0 and world == 1 and not args.skip_cpu:
             rk3["cpu_baseline"] = rk3_cpu()
             rk3["cpu_baseline"]["kind"] = "port"
@@ -678,6 +750,7 @@ def main():
                     help="only run this many U-Net guesses at 1024x1024 (profiling) and exit")
     ap.add_argument("--c1-steps", type=int, default=200, help="timed steps of the 512-cell column")
     ap.add_argument("--c4-steps", type=int, default=20, help="timed steps of the 4096-column batch")
+    ap.add_argument("--film-steps", type=int, default=10, help="timed steps of the 2-D film (0: skip the leg)")
     ap.add_argument("--profile-batch", type=int, default=0,
                     help="only run NCOL columns of the uneven batch (profiling runs); see --c4-steps, --threads")
     ap.add_argument("--threads", type=int, default=64, help="column CTA width for --profile-batch")

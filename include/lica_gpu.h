@@ -336,6 +336,47 @@ int lica_unet_train_step_device(lica_unet* net, const double* rho, const double*
                                 const double* by, const double* p_star, double hx, double hy, float lr,
                                 double* loss, void* stream);
 
+/* ----------------------------------------------------------------------------------
+ * 2-D film boiling: one RK3 time step (three substeps and the level-set
+ * reinitialisation) on an nx x ny MAC grid (x periodic, Lx = 1, h = 1/nx; heated no-slip
+ * wall at the bottom, outflow top with p = 0 on the face) with the level set on the
+ * 2 nx x 2 ny refined grid.  Generalises the reference's 1-D step rows to 2-D: RK3COEF
+ * (1d.f:1310-1322), RHSZ/LHSW (1603-1809, explicit), PRESSURE_CORRECTION through the 2-D
+ * multigrid (lica_mg_*), TEMP_GRAD/TF_GRAD/VOL_TOT_MFDOT (chphase.f) as a smeared mass
+ * flux, PASSIVE_SCALAR/TEMPASSIGN, TRANSPORT_RK3 + HJWENO and REINITIALIZATION + GODUNOV
+ * (two_phase.f).  Device arrays (row-major, x fastest): u (ny, nx) on the face west of
+ * cell i; v (ny + 1, nx) on the face below cell row j (v[0] = 0, v[ny] the top face);
+ * p = the modified pressure p + rho_l g y (ny, nx); th = (T - T_sat) / dT_wall (ny, nx);
+ * phi (2 ny, 2 nx), liquid where phi > 0.  nx, ny multiples of 32 that halve evenly
+ * nlevels - 1 times (the multigrid's rule); precision 0: FP64 pressure solves, 1: mixed.
+ * lica_film2d_step_device enqueues on the stream and waits for each pressure solve;
+ * returns the first non-OK solve status (LICA_NOT_CONVERGED) or LICA_OK.
+ * ---------------------------------------------------------------------------------- */
+typedef struct lica_film2d lica_film2d;
+
+typedef struct {
+    double re, visr, denr, prm, scr, tcr, jakob, fr; /* Re; liquid/vapour viscosity, density,
+                                                        specific-heat and conductivity ratios;
+                                                        Pr; Ja; Fr (gravity 1/Fr^2, 0: off) */
+    double rtol;       /* pressure-solve relative residual */
+    int32_t max_iters; /* pressure-solve iteration cap */
+    int32_t nreinit;   /* reinitialisation iterations after the step */
+} lica_film2d_props;
+
+typedef struct {
+    int32_t iterations[3];  /* pressure-solve iterations of each substep */
+    int32_t status[3];
+    double rel_residual[3];
+} lica_film2d_stats;
+
+int lica_film2d_create(lica_film2d** out, int32_t nx, int32_t ny, const lica_film2d_props* props,
+                       int32_t nlevels, int32_t precision);
+int lica_film2d_destroy(lica_film2d* film);
+int lica_film2d_step_device(lica_film2d* film, double* u, double* v, double* p, double* th, double* phi, double dt,
+                            lica_film2d_stats* stats, void* stream);
+/* Copies the interfacial mass flux per cell of the last substep into out (device, ny x nx). */
+int lica_film2d_mdot_device(lica_film2d* film, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

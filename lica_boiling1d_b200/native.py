@@ -42,6 +42,15 @@ class ColState(C.Structure):
     _fields_ = [(k, C.c_void_p) for k in COL_FIELDS]
 
 
+class Film2DProps(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("re", "visr", "denr", "prm", "scr", "tcr", "jakob", "fr", "rtol")] + \
+        [("max_iters", C.c_int32), ("nreinit", C.c_int32)]
+
+
+class Film2DStats(C.Structure):
+    _fields_ = [("iterations", C.c_int32 * 3), ("status", C.c_int32 * 3), ("rel_residual", C.c_double * 3)]
+
+
 # every symbol include/lica_gpu.h declares, with its ctypes signature
 SIGNATURES = {
     "lica_last_error": (C.c_char_p, []),
@@ -96,6 +105,11 @@ SIGNATURES = {
     "lica_unet_conv3x3_device": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
                                            C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
                                            C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
+    "lica_film2d_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.POINTER(Film2DProps), C.c_int32,
+                                     C.c_int32]),
+    "lica_film2d_destroy": (C.c_int, [C.c_void_p]),
+    "lica_film2d_step_device": (C.c_int, [C.c_void_p] * 6 + [C.c_double, C.POINTER(Film2DStats), C.c_void_p]),
+    "lica_film2d_mdot_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 STATUS = {0: "LICA_OK", 1: "LICA_NOT_CONVERGED", 2: "LICA_BAND_OVERFLOW", 3: "LICA_NAN", 4: "LICA_BAD_ARG",
