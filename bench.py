@@ -705,6 +705,30 @@ def profile_guess(reps):
     net.close()
 
 
+def profile_film(steps):
+    """A few 2-D film-boiling steps on 512 x 1536 (for ncu launch lists of the step's kernels);
+    prints the mean step time."""
+    import torch
+
+    from lica_boiling1d_b200 import film2d as G
+    P = G.default_props()
+    nx, ny = FILM["nx"], FILM["ny"]
+    st0 = G.initial_state(nx, ny, FILM["y0"], FILM["amp"], props=P)
+    dt = G.stable_dt(nx, P)
+    gpu = G.Film2D(nx, ny, P)
+    state = G.to_device(st0)
+    gpu.step(state, dt)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        gpu.step(state, dt)
+    b.record()
+    torch.cuda.synchronize()
+    print(f"2-D film step {nx}x{ny}: {a.elapsed_time(b) / steps:.3f} ms over {steps} steps")
+    gpu.close()
+
+
 def finish(args, v):
     import torch.distributed as dist
     if v["rank"] == 0:
@@ -751,6 +775,7 @@ def main():
     ap.add_argument("--c1-steps", type=int, default=200, help="timed steps of the 512-cell column")
     ap.add_argument("--c4-steps", type=int, default=20, help="timed steps of the 4096-column batch")
     ap.add_argument("--film-steps", type=int, default=10, help="timed steps of the 2-D film (0: skip the leg)")
+    ap.add_argument("--profile-film", type=int, default=0, help="run N 2-D film steps only (ncu launch lists)")
     ap.add_argument("--profile-batch", type=int, default=0,
                     help="only run NCOL columns of the uneven batch (profiling runs); see --c4-steps, --threads")
     ap.add_argument("--threads", type=int, default=64, help="column CTA width for --profile-batch")
@@ -765,6 +790,9 @@ def main():
         return
     if args.profile_guess:
         profile_guess(args.profile_guess)
+        return
+    if args.profile_film:
+        profile_film(args.profile_film)
         return
     if args.impl == "reference":
         run_reference(args)

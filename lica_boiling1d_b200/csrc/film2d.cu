@@ -45,7 +45,7 @@ constexpr double kRo[4] = {0.0, 0.0, -17.0 / 60.0, -5.0 / 12.0};
 // Constants of the step (the CPU restatement computes the same expressions).
 struct Const {
     int nx, ny, nxf, nyf;
-    double h, hf, ih, ih2, inv2h, ihsq, ihf, eps_h, inv2e, hf2, redtl;
+    double h, hf, ih, ih2, inv2h, ihsq, ihf, eps_h, inv2e, hf2, redtl, band;
     double denm, den_diff, vism, vis_diff, denscm, densc_diff, tcm, tc_diff, pei, cmd, cvol, gravity, denp;
 };
 
@@ -66,6 +66,7 @@ Const make_const(int nx, int ny, const lica_film2d_props& P) {
     c.inv2e = 1.0 / (2.0 * c.eps_h);
     c.hf2 = c.hf * c.hf;
     c.redtl = 0.5 * c.hf;
+    c.band = 8.0 * c.hf;
     c.denm = 1.0;
     c.den_diff = P.denr - 1.0;
     c.vism = 1.0 / P.re;
@@ -316,13 +317,22 @@ __device__ __forceinline__ void face_diffs(const double* __restrict__ phi, int I
     }
 }
 
-// Level-set transport substep: phi_out = phi + dt (gam L + ro L_old), L = -(u phi_x + v phi_y)
-// with upwinded WENO5 derivatives and the MAC velocity interpolated to the refined centre.
+// Level-set transport substep on the band |phi| < band (BAND_GENERATION's role): phi_out =
+// phi + dt (gam L + ro L_old), L = -(u phi_x + v phi_y) with upwinded WENO5 derivatives and
+// the MAC velocity interpolated to the refined centre; cells outside keep phi and store L = 0.
 __global__ void k_ls_transport(const double* __restrict__ phi, const double* __restrict__ u,
                                const double* __restrict__ v, double* __restrict__ phi_out,
                                double* __restrict__ rphi, double dt, double gam, double ro, const Const c) {
     const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
     if (I >= c.nxf || J >= c.nyf) return;
+    const size_t k = (size_t)J * c.nxf + I;
+    const double ph0 = phi[k];
+    if (!(fabs(ph0) < c.band)) {
+        // outside the band: unchanged, no stored right-hand side
+        phi_out[k] = ph0;
+        rphi[k] = 0.0;
+        return;
+    }
     const int nx = c.nx, ny = c.ny;
     const int m = I >> 1, a = I & 1, jp = J >> 1, b = J & 1;
     double uf, vf;
@@ -357,8 +367,7 @@ __global__ void k_ls_transport(const double* __restrict__ phi, const double* __r
     const double px = (uf >= 0.0) ? dmx : dplx;
     const double py = (vf >= 0.0) ? dmy : dply;
     const double L = -(uf * px + vf * py);
-    const size_t k = (size_t)J * c.nxf + I;
-    phi_out[k] = phi[k] + dt * (gam * L + ro * rphi[k]);
+    phi_out[k] = ph0 + dt * (gam * L + ro * rphi[k]);
     rphi[k] = L;
 }
 
@@ -372,12 +381,19 @@ __device__ __forceinline__ double godunov(double sg, double ap, double am) {
     return ap;
 }
 
-// One reinitialisation stage s = phi + redtl sg (1 - |grad phi|_Godunov), written as
-// out = crk * rk + cs * s (crk = 0, cs = 1: the plain stage).
+// One reinitialisation stage s = phi + redtl sg (1 - |grad phi|_Godunov) on the band
+// |a0| < band, written as out = s, 0.75 rk + 0.25 s or rk / 3 + 2 s / 3 (combine 0, 1, 2);
+// cells outside the band keep phi.
 __global__ void k_reinit_stage(const double* __restrict__ phi, const double* __restrict__ a0v,
                                const double* __restrict__ rk, double* __restrict__ out, int combine, const Const c) {
     const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
     if (I >= c.nxf || J >= c.nyf) return;
+    const size_t k = (size_t)J * c.nxf + I;
+    const double a0 = a0v[k];
+    if (!(fabs(a0) < c.band)) {
+        out[k] = phi[k];  // outside the band: unchanged (and not combined)
+        return;
+    }
     double dx[6], dy[6];
     face_diffs(phi, I, J, c, dx, dy);
     double dmx, dplx, dmy, dply;
@@ -386,8 +402,6 @@ __global__ void k_reinit_stage(const double* __restrict__ phi, const double* __r
     const double gx = 0.5 * (dx[2] + dx[3]);
     const double gz = 0.5 * (dy[2] + dy[3]);
     const double dal = gx * gx + gz * gz;
-    const size_t k = (size_t)J * c.nxf + I;
-    const double a0 = a0v[k];
     const double sg = a0 / sqrt(a0 * a0 + dal * c.hf2);
     const double ax = godunov(sg, dplx, dmx);
     const double az = godunov(sg, dply, dmy);

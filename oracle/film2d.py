@@ -33,7 +33,10 @@ the reference's wall-normal z):
     1133-1495, 2477-2500) in x and y, velocity bilinearly interpolated from the MAC faces to
     the refined centres (VEL_INTP's role), simple upwinding by the sign of each component;
   * reinitialisation: REINITIALIZATION's SSP-RK3 pseudo-time iterations with GODUNOV and
-    Peng's smoothed sign (two_phase.f:2033-2474), on the whole refined grid.
+    Peng's smoothed sign (two_phase.f:2033-2474);
+  * both on the band |phi| < 8 refined cells (BAND_GENERATION's role, two_phase.f:1622-2030):
+    cells outside keep their value (the properties see phi only within one flow cell of the
+    interface).
 Documented simplifications: surface tension is off (We = infinity; 2-D curvature is not
 built), the interface recession term of the phase change is not applied (the interface
 moves with the one-fluid velocity, which carries the expansion flow of S), and the viscous
@@ -97,6 +100,7 @@ class Derived:
         self.gravity = 0.0 if P["fr"] == 0.0 else 1.0 / (P["fr"] * P["fr"])
         self.denp = P["denr"]
         self.nreinit = int(P["nreinit"])
+        self.band = 8.0 * self.hf  # transport / reinitialisation band |phi| < band (BAND_GENERATION's role)
         self.rtol = P["rtol"]
 
 
@@ -384,6 +388,7 @@ def godunov(sg, ap, am):
 
 
 def reinit_stage(phi, a0, D):
+    """One stage on the band |a0| < D.band; cells outside keep phi."""
     nj = phi.shape[0]
     dmx, dplx, dmy, dply, dpx, dpy = weno_xy(phi, D)
     tky = _take_y(dpy, nj)
@@ -394,18 +399,19 @@ def reinit_stage(phi, a0, D):
     ax = godunov(sg, dplx, dmx)
     az = godunov(sg, dply, dmy)
     drhs = sg * (1.0 - np.sqrt(ax * ax + az * az))
-    return phi + (0.5 * D.hf) * drhs
+    return np.where(np.abs(a0) < D.band, phi + (0.5 * D.hf) * drhs, phi)
 
 
 def reinitialize(phi, D):
     a0 = phi.copy()
+    band = np.abs(a0) < D.band
     for _ in range(D.nreinit):
         rk = phi
         phi = reinit_stage(phi, a0, D)
         phi = reinit_stage(phi, a0, D)
-        phi = 0.75 * rk + 0.25 * phi
+        phi = np.where(band, 0.75 * rk + 0.25 * phi, phi)
         phi = reinit_stage(phi, a0, D)
-        phi = (1.0 / 3.0) * rk + (2.0 / 3.0) * phi
+        phi = np.where(band, (1.0 / 3.0) * rk + (2.0 / 3.0) * phi, phi)
     return phi
 
 
@@ -453,8 +459,9 @@ def step(state, dt, props, mg_solve, mg_levels=6):
         rth = e
         th = np.where(psi > 0.5, 0.0, thn)
         uf, vf = refined_velocity(u, v)
-        L = ls_rhs(phi, uf, vf, D)
-        phi = phi + dt * (gam * L + ro * rphi)
+        band = np.abs(phi) < D.band
+        L = np.where(band, ls_rhs(phi, uf, vf, D), 0.0)
+        phi = np.where(band, phi + dt * (gam * L + ro * rphi), phi)
         rphi = L
     phi = reinitialize(phi, D)
     return dict(u=u, v=v, p=p, th=th, phi=phi), info
