@@ -139,6 +139,14 @@ int lica_mg_solve_device(lica_mg* mg, double* p, const double* f, const double* 
  * stream may be NULL (the context's own stream); the call returns when p is on the host. */
 int lica_mg_solve_host(lica_mg* mg, double* p, const double* f, const double* bx, const double* by,
                        double rtol, int32_t max_iters, lica_mg_result* res, void* stream);
+/* A sequence of independent solves from host arrays (count systems, each with its own p, f,
+ * bx, by): the upload of system k + 1 and the download of system k - 1 overlap the solve of
+ * system k (two staging buffers on the device, separate upload and download streams; pinned
+ * host arrays are needed for the overlap).  res holds count results; returns the first
+ * non-OK solve status, or LICA_OK. */
+int lica_mg_solve_host_batch(lica_mg* mg, int32_t count, double* const* p, const double* const* f,
+                             const double* const* bx, const double* const* by, double rtol, int32_t max_iters,
+                             lica_mg_result* res);
 
 /* One application of the preconditioner, z = M r (device arrays). */
 int lica_mg_precond_device(lica_mg* mg, double* z, const double* r, const double* bx, const double* by,

@@ -1193,6 +1193,13 @@ struct lica_mg {
     // host staging for lica_mg_solve_host
     double *d_p = nullptr, *d_f = nullptr, *d_bx = nullptr, *d_by = nullptr;
     cudaStream_t own_stream = nullptr;
+    // lica_mg_solve_host_batch: double-buffered input staging [2] (p0, f, bx, by in one block),
+    // output staging [2], upload and download streams and their ordering events
+    double* b_in[2] = {nullptr, nullptr};
+    double* b_out[2] = {nullptr, nullptr};
+    cudaStream_t b_up = nullptr, b_down = nullptr;
+    cudaEvent_t b_ev_in[2] = {nullptr, nullptr}, b_ev_used[2] = {nullptr, nullptr};
+    cudaEvent_t b_ev_solved[2] = {nullptr, nullptr}, b_ev_out[2] = {nullptr, nullptr};
     cudaStream_t cap_stream = nullptr;  // graphs are captured here, launched on the caller's stream
     // graph cache
     cudaGraphExec_t gexec = nullptr;
@@ -1811,10 +1818,18 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
             return fail(LICA_ERR_CUDA);
         }
     }
-    cudaError_t e = mixed ? cudaFuncSetAttribute(k_cta<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)m->cta_smem)
-                          : cudaFuncSetAttribute(k_cta<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)m->cta_smem);
+    // The dynamic shared-memory cap is per function, shared by every solver instance: set it
+    // to the device's opt-in maximum (an instance with a smaller coarse level must not lower
+    // it under another instance's launches), and check this instance's need against it.
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess && m->cta_smem > (size_t)optin) {
+        lica_set_last_error("lica_mg_create", "coarse levels exceed the shared memory of one CTA", __FILE__, __LINE__);
+        return fail(LICA_BAD_ARG);
+    }
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_cta<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_cta<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
     if (e != cudaSuccess) {
         lica_set_last_error("cudaFuncSetAttribute(k_cta)", cudaGetErrorString(e), __FILE__, __LINE__);
         return fail(LICA_ERR_CUDA);
@@ -1862,6 +1877,15 @@ int lica_mg_destroy(lica_mg* m) {
     cudaFree(m->d_f);
     cudaFree(m->d_bx);
     cudaFree(m->d_by);
+    for (int b = 0; b < 2; ++b) {
+        cudaFree(m->b_in[b]);
+        cudaFree(m->b_out[b]);
+        cudaEvent_t evs[] = {m->b_ev_in[b], m->b_ev_used[b], m->b_ev_solved[b], m->b_ev_out[b]};
+        for (cudaEvent_t e : evs)
+            if (e) cudaEventDestroy(e);
+    }
+    if (m->b_up) cudaStreamDestroy(m->b_up);
+    if (m->b_down) cudaStreamDestroy(m->b_down);
     if (m->own_stream) cudaStreamDestroy(m->own_stream);
     if (m->cap_stream) cudaStreamDestroy(m->cap_stream);
     delete m;
@@ -1894,6 +1918,77 @@ int lica_mg_solve_host(lica_mg* m, double* p, const double* f, const double* bx,
     LICA_CUDA_TRY(cudaMemcpyAsync(p, m->d_p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
     LICA_CUDA_TRY(cudaStreamSynchronize(s));
     return st;
+}
+
+int lica_mg_solve_host_batch(lica_mg* m, int32_t count, double* const* p, const double* const* f,
+                             const double* const* bx, const double* const* by, double rtol, int32_t max_iters,
+                             lica_mg_result* res) {
+    if (!m || count < 0 || (count > 0 && (!p || !f || !bx || !by || !res))) return LICA_BAD_ARG;
+    for (int32_t k = 0; k < count; ++k)
+        if (!p[k] || !f[k] || !bx[k] || !by[k]) return LICA_BAD_ARG;
+    if (count == 0) return LICA_OK;
+    const size_t n = (size_t)m->nx * m->ny, nb = n + m->nx, nin = 3 * n + nb;
+    if (!m->own_stream) LICA_CUDA_TRY(cudaStreamCreateWithFlags(&m->own_stream, cudaStreamNonBlocking));
+    if (!m->d_p) {
+        LICA_CUDA_TRY(cudaMalloc((void**)&m->d_p, sizeof(double) * n));
+        LICA_CUDA_TRY(cudaMalloc((void**)&m->d_f, sizeof(double) * n));
+        LICA_CUDA_TRY(cudaMalloc((void**)&m->d_bx, sizeof(double) * n));
+        LICA_CUDA_TRY(cudaMalloc((void**)&m->d_by, sizeof(double) * nb));
+    }
+    if (!m->b_up) {
+        LICA_CUDA_TRY(cudaStreamCreateWithFlags(&m->b_up, cudaStreamNonBlocking));
+        LICA_CUDA_TRY(cudaStreamCreateWithFlags(&m->b_down, cudaStreamNonBlocking));
+        for (int b = 0; b < 2; ++b) {
+            LICA_CUDA_TRY(cudaMalloc((void**)&m->b_in[b], sizeof(double) * nin));
+            LICA_CUDA_TRY(cudaMalloc((void**)&m->b_out[b], sizeof(double) * n));
+            cudaEvent_t* evs[] = {&m->b_ev_in[b], &m->b_ev_used[b], &m->b_ev_solved[b], &m->b_ev_out[b]};
+            for (cudaEvent_t* e : evs) LICA_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+            // nothing in flight yet: the first waits on these events pass
+            LICA_CUDA_TRY(cudaEventRecord(m->b_ev_used[b], m->b_up));
+            LICA_CUDA_TRY(cudaEventRecord(m->b_ev_out[b], m->b_down));
+        }
+    }
+    cudaStream_t s = m->own_stream;
+    // upload of system k into input staging k % 2 once the solve of k - 2 has consumed it
+    auto upload = [&](int32_t k) -> int {
+        const int b = k & 1;
+        double* in = m->b_in[b];
+        LICA_CUDA_TRY(cudaStreamWaitEvent(m->b_up, m->b_ev_used[b], 0));
+        LICA_CUDA_TRY(cudaMemcpyAsync(in, p[k], sizeof(double) * n, cudaMemcpyHostToDevice, m->b_up));
+        LICA_CUDA_TRY(cudaMemcpyAsync(in + n, f[k], sizeof(double) * n, cudaMemcpyHostToDevice, m->b_up));
+        LICA_CUDA_TRY(cudaMemcpyAsync(in + 2 * n, bx[k], sizeof(double) * n, cudaMemcpyHostToDevice, m->b_up));
+        LICA_CUDA_TRY(cudaMemcpyAsync(in + 3 * n, by[k], sizeof(double) * nb, cudaMemcpyHostToDevice, m->b_up));
+        LICA_CUDA_TRY(cudaEventRecord(m->b_ev_in[b], m->b_up));
+        return LICA_OK;
+    };
+    int st = upload(0), worst = LICA_OK;
+    if (st) return st;
+    for (int32_t k = 0; k < count; ++k) {
+        const int b = k & 1;
+        // the next system's upload runs during this solve
+        if (k + 1 < count && (st = upload(k + 1))) return st;
+        double* in = m->b_in[b];
+        LICA_CUDA_TRY(cudaStreamWaitEvent(s, m->b_ev_in[b], 0));
+        LICA_CUDA_TRY(cudaMemcpyAsync(m->d_p, in, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        LICA_CUDA_TRY(cudaMemcpyAsync(m->d_f, in + n, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        LICA_CUDA_TRY(cudaMemcpyAsync(m->d_bx, in + 2 * n, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        LICA_CUDA_TRY(cudaMemcpyAsync(m->d_by, in + 3 * n, sizeof(double) * nb, cudaMemcpyDeviceToDevice, s));
+        LICA_CUDA_TRY(cudaEventRecord(m->b_ev_used[b], s));
+        st = solve_impl(m, m->d_p, m->d_f, m->d_bx, m->d_by, rtol, max_iters, &res[k], s);
+        if (st == LICA_ERR_CUDA || st == LICA_BAD_ARG) return st;
+        if (st != LICA_OK && worst == LICA_OK) worst = st;
+        // the result leaves through output staging k % 2 (free once the download of k - 2 ended)
+        LICA_CUDA_TRY(cudaStreamWaitEvent(s, m->b_ev_out[b], 0));
+        LICA_CUDA_TRY(cudaMemcpyAsync(m->b_out[b], m->d_p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        LICA_CUDA_TRY(cudaEventRecord(m->b_ev_solved[b], s));
+        LICA_CUDA_TRY(cudaStreamWaitEvent(m->b_down, m->b_ev_solved[b], 0));
+        LICA_CUDA_TRY(cudaMemcpyAsync(p[k], m->b_out[b], sizeof(double) * n, cudaMemcpyDeviceToHost, m->b_down));
+        LICA_CUDA_TRY(cudaEventRecord(m->b_ev_out[b], m->b_down));
+    }
+    LICA_CUDA_TRY(cudaStreamSynchronize(m->b_down));
+    LICA_CUDA_TRY(cudaStreamSynchronize(m->b_up));
+    LICA_CUDA_TRY(cudaStreamSynchronize(s));
+    return worst;
 }
 
 int lica_mg_precond_device(lica_mg* m, double* z, const double* r, const double* bx, const double* by,

@@ -64,6 +64,8 @@ SIGNATURES = {
     "lica_mg_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.c_double, C.c_double,
                                  C.POINTER(MgOptions)]),
     "lica_mg_destroy": (C.c_int, [C.c_void_p]),
+    "lica_mg_solve_host_batch": (C.c_int, [C.c_void_p, C.c_int32] + [C.POINTER(C.c_void_p)] * 4 +
+                                 [C.c_double, C.c_int32, C.POINTER(MgResult)]),
     "lica_mg_solve_device": (C.c_int, [C.c_void_p] * 5 + [C.c_double, C.c_int32, C.POINTER(MgResult),
                                                            C.c_void_p]),
     "lica_mg_solve_host": (C.c_int, [C.c_void_p, _D, _D, _D, _D, C.c_double, C.c_int32, C.POINTER(MgResult),

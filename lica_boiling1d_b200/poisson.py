@@ -130,6 +130,27 @@ class MultigridPoisson:
         native.check(code, "lica_mg_solve", ok=(0, 1))
         return res.iterations, res.rel_residual, res.status
 
+    def solve_batch(self, ps, fs, bxs, bys, rtol=1e-10, max_iters=200):
+        """Independent solves A p_k = f_k from host arrays (lica_mg_solve_host_batch): the
+        upload of the next system and the download of the previous one overlap each solve
+        (pinned arrays give the overlap).  Solves in place on each p_k; returns a list of
+        (iterations, rel_residual, status)."""
+        cnt = len(ps)
+        if not (len(fs) == len(bxs) == len(bys) == cnt):
+            raise ValueError("ps, fs, bxs, bys must have the same length")
+        for k in range(cnt):
+            self._check_shapes(ps[k], fs[k], bxs[k], bys[k])
+            for a in (ps[k], fs[k], bxs[k], bys[k]):
+                assert isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous
+
+        def ptrs(arrs):
+            return (C.c_void_p * cnt)(*[a.ctypes.data for a in arrs])
+        res = (native.MgResult * cnt)()
+        code = native.lib().lica_mg_solve_host_batch(self._h, cnt, ptrs(ps), ptrs(fs), ptrs(bxs), ptrs(bys), rtol,
+                                                     max_iters, res)
+        native.check(code, "lica_mg_solve_host_batch", ok=(0, 1))
+        return [(r.iterations, r.rel_residual, r.status) for r in res]
+
     KERNEL_CLASSES = ("down0", "down", "up0", "up", "cta", "pupdate", "xupdate", "setup")
 
     def profile(self, enable=True):

@@ -209,3 +209,45 @@ def test_misaligned_device_arrays_rejected():
     with pytest.raises(native.LicaError) as e:
         s.solve(p, _t(c.f), _t(c.bx), _t(c.by))
     assert e.value.code == 4
+
+
+def test_host_batch_matches_single_solves():
+    """lica_mg_solve_host_batch (uploads and downloads overlapping the solves) gives each
+    system exactly the single host-entry solution."""
+    import torch
+    from lica_boiling1d_b200 import poisson
+    from lica_boiling1d_b200.inputs import bubble_poisson_case
+    c = bubble_poisson_case(128, nbubbles=6, seed=3)
+    s = poisson.MultigridPoisson(128, 128, c.hx, c.hy, nlevels=3)
+    rng = np.random.default_rng(1)
+    fs = [np.ascontiguousarray(c.f * (1.0 + 0.5 * k) + 0.01 * rng.standard_normal(c.f.shape)) for k in range(5)]
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    ps = [pin(np.zeros_like(c.f)) for _ in fs]
+    res = s.solve_batch(ps, [pin(f) for f in fs], [pin(c.bx)] * 5, [pin(c.by)] * 5, rtol=TOL)
+    for k, f in enumerate(fs):
+        q = np.zeros_like(c.f)
+        it, rel, st = s.solve(q, f, c.bx, c.by, rtol=TOL)
+        assert res[k][2] == 0 and res[k][0] == it
+        np.testing.assert_array_equal(ps[k], q)
+    s.close()
+
+
+def test_solvers_of_different_sizes_coexist():
+    """A solver keeps working after another, with smaller coarse levels, is created and
+    destroyed (the coarse kernel's shared-memory cap is per function, not per solver)."""
+    from lica_boiling1d_b200 import poisson
+    from lica_boiling1d_b200.inputs import bubble_poisson_case
+    big = bubble_poisson_case(256, nbubbles=8, seed=4)
+    a = poisson.MultigridPoisson(256, 256, big.hx, big.hy, nlevels=4)
+    p1 = np.zeros_like(big.f)
+    it1, rel1, st1 = a.solve(p1, big.f, big.bx, big.by, rtol=TOL)
+    small = bubble_poisson_case(64, ny=192, nbubbles=2, seed=5)
+    b = poisson.MultigridPoisson(64, 192, small.hx, small.hy, nlevels=3)
+    q = np.zeros_like(small.f)
+    assert b.solve(q, small.f, small.bx, small.by, rtol=TOL)[2] == 0
+    b.close()
+    p2 = np.zeros_like(big.f)
+    it2, rel2, st2 = a.solve(p2, big.f, big.bx, big.by, rtol=TOL)
+    assert st1 == st2 == 0 and it1 == it2
+    np.testing.assert_array_equal(p1, p2)
+    a.close()
