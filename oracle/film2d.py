@@ -55,9 +55,6 @@ import numpy as np
 GAMMA = (0.0, 8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0)
 RO = (0.0, 0.0, -17.0 / 60.0, -5.0 / 12.0)
 
-PROP_KEYS = ("re", "visr", "denr", "prm", "scr", "tcr", "jakob", "fr", "rtol")
-
-
 def default_props():
     """The 2-D film-boiling benchmark's liquid/vapour ratios (Welch and Wilson's case: rho 200/5,
     mu 0.1/0.005, k 40/1, c_p 400/200, h_fg 1e4, superheat 5 K): density 40, viscosity 20,
