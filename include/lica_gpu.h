@@ -352,7 +352,8 @@ int lica_unet_train_step_device(lica_unet* net, const double* rho, const double*
  * (1d.f:1310-1322), RHSZ/LHSW (1603-1809, explicit), PRESSURE_CORRECTION through the 2-D
  * multigrid (lica_mg_*), TEMP_GRAD/TF_GRAD/VOL_TOT_MFDOT (chphase.f) as a smeared mass
  * flux, PASSIVE_SCALAR/TEMPASSIGN, TRANSPORT_RK3 + HJWENO and REINITIALIZATION + GODUNOV
- * (two_phase.f).  Device arrays (row-major, x fastest): u (ny, nx) on the face west of
+ * (two_phase.f), surface tension by CAL_CUR's curvature as a continuum surface force.
+ * Device arrays (row-major, x fastest): u (ny, nx) on the face west of
  * cell i; v (ny + 1, nx) on the face below cell row j (v[0] = 0, v[ny] the top face);
  * p = the modified pressure p + rho_l g y (ny, nx); th = (T - T_sat) / dT_wall (ny, nx);
  * phi (2 ny, 2 nx), liquid where phi > 0.  nx, ny multiples of 32 that halve evenly
@@ -366,6 +367,7 @@ typedef struct {
     double re, visr, denr, prm, scr, tcr, jakob, fr; /* Re; liquid/vapour viscosity, density,
                                                         specific-heat and conductivity ratios;
                                                         Pr; Ja; Fr (gravity 1/Fr^2, 0: off) */
+    double we;         /* Weber number (surface tension 1/We, 0: off) */
     double rtol;       /* pressure-solve relative residual */
     int32_t max_iters; /* pressure-solve iteration cap */
     int32_t nreinit;   /* reinitialisation iterations after the step */

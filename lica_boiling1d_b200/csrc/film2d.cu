@@ -16,8 +16,9 @@
 //   (PASSIVE_SCALAR / TEMPASSIGN's role); TRANSPORT_RK3 with the reference's HJWENO in x and y
 //   (two_phase.f:1133-1495, 2477-2500); REINITIALIZATION's SSP-RK3 pseudo-time iterations with
 //   GODUNOV and Peng's smoothed sign (two_phase.f:2033-2474).
-// Simplifications: no surface tension (2-D curvature is not built), no interface recession
-// term, explicit viscous terms.
+// Surface tension is the continuum surface force -sigma kappa grad psi / rho_f with the
+// curvature of the refined level set (CAL_CUR / INTER_CUR's role, two_phase.f:3317-4432).
+// Simplifications: no interface recession term, explicit viscous terms.
 //
 // Every kernel is one thread per output cell, 32 x 8 thread blocks (coalesced rows), and
 // evaluates each expression in a fixed order; the library is compiled without FMA
@@ -45,8 +46,8 @@ constexpr double kRo[4] = {0.0, 0.0, -17.0 / 60.0, -5.0 / 12.0};
 // Constants of the step (the CPU restatement computes the same expressions).
 struct Const {
     int nx, ny, nxf, nyf;
-    double h, hf, ih, ih2, inv2h, ihsq, ihf, eps_h, inv2e, hf2, redtl, band;
-    double denm, den_diff, vism, vis_diff, denscm, densc_diff, tcm, tc_diff, pei, cmd, cvol, gravity, denp;
+    double h, hf, ih, ih2, inv2h, ihsq, ihf, eps_h, inv2e, hf2, redtl, band, ih2f, ihfsq, q4;
+    double denm, den_diff, vism, vis_diff, denscm, densc_diff, tcm, tc_diff, pei, cmd, cvol, gravity, denp, surf;
 };
 
 Const make_const(int nx, int ny, const lica_film2d_props& P) {
@@ -80,6 +81,10 @@ Const make_const(int nx, int ny, const lica_film2d_props& P) {
     c.cvol = 1.0 / 1.0 - 1.0 / P.denr;
     c.gravity = (P.fr == 0.0) ? 0.0 : 1.0 / (P.fr * P.fr);
     c.denp = P.denr;
+    c.surf = (P.we == 0.0) ? 0.0 : 1.0 / P.we;
+    c.ih2f = 0.5 / c.hf;
+    c.ihfsq = 1.0 / (c.hf * c.hf);
+    c.q4 = 0.25 * c.ihfsq;
     return c;
 }
 
@@ -112,6 +117,37 @@ __global__ void k_props(const double* __restrict__ phi, double* __restrict__ psi
     tc[k] = c.tcm + c.tc_diff * ps;
 }
 
+// Curvature kappa = div(grad phi / |grad phi|) per flow cell (CAL_CUR's role in 2-D): central
+// differences on the refined grid (x periodic, y indices clamped) where |phi| < 2 h, the four
+// sub-cells averaged, limited to |kappa| <= 1/h.
+__device__ __forceinline__ double curv_refined(const double* __restrict__ phi, int I, int J, const Const& c) {
+    const int nxf = c.nxf, nyf = c.nyf;
+    const double* row = phi + (size_t)J * nxf;
+    const double C = row[I];
+    if (!(fabs(C) < 2.0 * c.h)) return 0.0;
+    const int Ie = (I + 1 == nxf) ? 0 : I + 1, Iw = (I == 0) ? nxf - 1 : I - 1;
+    const double* up = phi + (size_t)(J + 1 < nyf ? J + 1 : nyf - 1) * nxf;
+    const double* dn = phi + (size_t)(J > 0 ? J - 1 : 0) * nxf;
+    const double E = row[Ie], W = row[Iw], N = up[I], S = dn[I];
+    const double fx = (E - W) * c.ih2f;
+    const double fy = (N - S) * c.ih2f;
+    const double fxx = (E - 2.0 * C + W) * c.ihfsq;
+    const double fyy = (N - 2.0 * C + S) * c.ihfsq;
+    const double fxy = ((up[Ie] - up[Iw]) - (dn[Ie] - dn[Iw])) * c.q4;
+    const double g2 = fx * fx + fy * fy;
+    if (!(g2 > 1e-12)) return 0.0;
+    const double num = (fxx * (fy * fy) - 2.0 * (fx * fy) * fxy) + fyy * (fx * fx);
+    return num / (g2 * sqrt(g2));
+}
+
+__global__ void k_curv(const double* __restrict__ phi, double* __restrict__ kap, const Const c) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= c.nx || j >= c.ny) return;
+    const double q = (curv_refined(phi, 2 * i, 2 * j, c) + curv_refined(phi, 2 * i + 1, 2 * j, c)) +
+                     (curv_refined(phi, 2 * i, 2 * j + 1, c) + curv_refined(phi, 2 * i + 1, 2 * j + 1, c));
+    kap[(size_t)j * c.nx + i] = fmin(fmax(0.25 * q, -c.ih), c.ih);
+}
+
 // Face coefficients beta = 1/rho: bx by harmonic mean (x periodic), by on rows 0..ny.
 __global__ void k_beta(const double* __restrict__ den, double* __restrict__ bx, double* __restrict__ by, const Const c) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -128,6 +164,7 @@ __global__ void k_beta(const double* __restrict__ den, double* __restrict__ bx, 
 // substep.
 __global__ void k_momentum(const double* __restrict__ u, const double* __restrict__ v,
                            const double* __restrict__ den, const double* __restrict__ vis,
+                           const double* __restrict__ psi, const double* __restrict__ kap,
                            const double* __restrict__ p, const double* __restrict__ bx,
                            const double* __restrict__ by, double* __restrict__ us, double* __restrict__ vs,
                            double* __restrict__ ru, double* __restrict__ rv, double dt, double gam, double ro,
@@ -163,7 +200,9 @@ __global__ void k_momentum(const double* __restrict__ u, const double* __restric
         const double tys = mus * ((uc - usv) * ih + (vrow[i] - vrow[iw]) * ih);
         const double rho = 0.5 * (den[(size_t)j * nx + iw] + den[k]);
         const double visc = ((txe - txw) * ih + (tyn - tys) * ih) / rho;
-        const double nu = visc - conv;
+        // surface tension -sigma kappa grad psi on the face (continuum surface force)
+        const double kapf = 0.5 * (kap[(size_t)j * nx + iw] + kap[k]);
+        const double nu = visc - conv - (c.surf * kapf) * ((psi[k] - psi[(size_t)j * nx + iw]) * ih) / rho;
         us[k] = uc + dt * (gam * nu + ro * ru[k]) - adt * (bx[k] * ((p[k] - p[(size_t)j * nx + iw]) * ih));
         ru[k] = nu;
     }
@@ -188,7 +227,10 @@ __global__ void k_momentum(const double* __restrict__ u, const double* __restric
         const double dlo = den[k], dhi = (j + 1 < ny) ? den[k + nx] : den[(size_t)(ny - 1) * nx + i];
         const double rho = 0.5 * (dlo + dhi);
         const double visc = ((txe - txw) * ih + (tyn - tys) * ih) / rho;
-        const double nv = visc - conv + c.gravity * (c.denp / rho - 1.0);
+        const size_t khi = (j + 1 < ny) ? k + nx : (size_t)(ny - 1) * nx + i;
+        const double kapf = 0.5 * (kap[k] + kap[khi]);
+        const double nv = visc - conv + c.gravity * (c.denp / rho - 1.0) -
+                          (c.surf * kapf) * ((psi[khi] - psi[k]) * ih) / rho;
         const size_t kf = (size_t)jf * nx + i;
         const double gp = (jf < ny) ? (p[kf] - p[k]) * ih : (0.0 - p[k]) * c.ih2;  // p = 0 on the top face
         vs[kf] = vc + dt * (gam * nv + ro * rv[k]) - adt * (by[kf] * gp);
@@ -426,7 +468,7 @@ struct lica_film2d {
     // flow-grid scratch
     double *psi = nullptr, *den = nullptr, *vis = nullptr, *densc = nullptr, *tc = nullptr, *bx = nullptr,
            *by = nullptr, *us = nullptr, *vs = nullptr, *ru = nullptr, *rv = nullptr, *rth = nullptr, *f = nullptr,
-           *mdot = nullptr, *th2 = nullptr, *dp = nullptr;
+           *mdot = nullptr, *th2 = nullptr, *dp = nullptr, *kap = nullptr;
     // refined-grid scratch
     double *rphi = nullptr, *ph[3] = {nullptr, nullptr, nullptr};
 };
@@ -445,7 +487,7 @@ int dalloc(double** p, size_t n) {
 void free_all(lica_film2d* F) {
     if (F->mg) lica_mg_destroy(F->mg);
     double* ptrs[] = {F->psi, F->den, F->vis, F->densc, F->tc, F->bx, F->by, F->us, F->vs, F->ru, F->rv, F->rth, F->f,
-                      F->mdot, F->th2, F->dp, F->rphi, F->ph[0], F->ph[1], F->ph[2]};
+                      F->mdot, F->th2, F->dp, F->kap, F->rphi, F->ph[0], F->ph[1], F->ph[2]};
     for (double* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -484,7 +526,7 @@ int lica_film2d_create(lica_film2d** out, int32_t nx, int32_t ny, const lica_fil
     }
     const size_t n = (size_t)nx * ny, nv = n + nx, nf = 4 * n;
     double** flow[] = {&F->psi, &F->den, &F->vis, &F->densc, &F->tc, &F->bx, &F->us, &F->ru, &F->rv, &F->rth,
-                       &F->f, &F->mdot, &F->th2, &F->dp};
+                       &F->f, &F->mdot, &F->th2, &F->dp, &F->kap};
     for (double** p : flow)
         if ((st = dalloc(p, n))) break;
     if (!st) st = dalloc(&F->by, nv);
@@ -526,11 +568,12 @@ int lica_film2d_step_device(lica_film2d* F, double* u, double* v, double* p, dou
         const double adt = alpha * dt, iadt = 1.0 / (alpha * dt);
         k_props<<<gflow, blk, 0, s>>>(phc, F->psi, F->den, F->vis, F->densc, F->tc, c);
         k_beta<<<gflow, blk, 0, s>>>(F->den, F->bx, F->by, c);
-        k_momentum<<<gflow, blk, 0, s>>>(u, v, F->den, F->vis, p, F->bx, F->by, F->us, F->vs, F->ru, F->rv, dt, gam,
-                                         ro, adt, c);
+        k_curv<<<gflow, blk, 0, s>>>(phc, F->kap, c);
+        k_momentum<<<gflow, blk, 0, s>>>(u, v, F->den, F->vis, F->psi, F->kap, p, F->bx, F->by, F->us, F->vs, F->ru,
+                                         F->rv, dt, gam, ro, adt, c);
         k_source_rhs<<<gflow, blk, 0, s>>>(thc, F->psi, F->tc, F->us, F->vs, F->f, F->mdot, iadt, c);
         LICA_CUDA_TRY(cudaGetLastError());
-        launches += 4;
+        launches += 5;
         // the pressure increment, from zero
         LICA_CUDA_TRY(cudaMemsetAsync(F->dp, 0, n * sizeof(double), s));
         lica_mg_result r{};

@@ -7,8 +7,8 @@ RK3COEF substeps (1d.f:1310-1322), explicit momentum (RHSZ / LHSW's terms, 1d.f:
 the projection with the phase-change volume source (PRESSURE_CORRECTION, CAL_CONTINUITY2),
 the smeared interfacial mass flux (TEMP_GRAD / TF_GRAD / VOL_TOT_MFDOT, chphase.f), the energy
 update (PASSIVE_SCALAR / TEMPASSIGN), TRANSPORT_RK3 with HJWENO and REINITIALIZATION with
-GODUNOV (two_phase.f).  No surface tension, no interface recession term, explicit viscous
-terms.
+GODUNOV (two_phase.f), and surface tension as a continuum surface force with the level set's
+curvature (CAL_CUR).  No interface recession term, explicit viscous terms.
 
 Fields (torch CUDA float64, contiguous, x fastest): u (ny, nx) on the face west of each cell,
 v (ny + 1, nx) on the face below each cell row, p (the modified pressure p + rho_l g y), th =
@@ -28,12 +28,12 @@ def default_props():
     mu 0.1/0.005, k 40/1, c_p 400/200, h_fg 1e4, superheat 5 K): density 40, viscosity 20,
     conductivity 40, specific heat 2, Ja = c_p,v dT / h_fg = 0.1, Pr_v = 1, and Re = 69.2 and
     Fr = 1 on the velocity sqrt(g Lx) with Lx the most dangerous Rayleigh-Taylor wavelength
-    (0.0787 m).  The pressure solves stop at a relative residual of 1e-8: with the interface's
+    (0.0787 m), We = rho_v U^2 Lx / sigma = 3.04 (sigma 0.1 N/m).  The pressure solves stop at a relative residual of 1e-8: with the interface's
     phase-change source on the right-hand side the multigrid-preconditioned CG stalls between
     1e-10 and 1e-9 at 512 x 1536 (the vapour film is a thin, 40 times more mobile layer sealed by
     the wall), and 1e-8 is met in about 12 iterations."""
-    return dict(re=69.2, visr=20.0, denr=40.0, prm=1.0, scr=2.0, tcr=40.0, jakob=0.1, fr=1.0, rtol=1e-8,
-                nreinit=2)
+    return dict(re=69.2, visr=20.0, denr=40.0, prm=1.0, scr=2.0, tcr=40.0, jakob=0.1, fr=1.0, we=3.04,
+                rtol=1e-8, nreinit=2)
 
 
 def initial_state(nx, ny, y0_cells=64.0, amp_cells=4.0, props=None):
@@ -114,7 +114,7 @@ class Film2D:
         self.props = dict(default_props() if props is None else props)
         P = self.props
         self._p = native.Film2DProps(re=P["re"], visr=P["visr"], denr=P["denr"], prm=P["prm"], scr=P["scr"],
-                                     tcr=P["tcr"], jakob=P["jakob"], fr=P["fr"], rtol=P["rtol"],
+                                     tcr=P["tcr"], jakob=P["jakob"], fr=P["fr"], we=P.get("we", 0.0), rtol=P["rtol"],
                                      max_iters=max_iters, nreinit=int(P["nreinit"]))
         self.nlevels = levels_for(nx, ny) if nlevels is None else nlevels
         if precision not in ("fp64", "mixed"):

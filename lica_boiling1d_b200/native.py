@@ -43,7 +43,8 @@ class ColState(C.Structure):
 
 
 class Film2DProps(C.Structure):
-    _fields_ = [(k, C.c_double) for k in ("re", "visr", "denr", "prm", "scr", "tcr", "jakob", "fr", "rtol")] + \
+    _fields_ = [(k, C.c_double) for k in ("re", "visr", "denr", "prm", "scr", "tcr", "jakob", "fr", "we",
+                                          "rtol")] + \
         [("max_iters", C.c_int32), ("nreinit", C.c_int32)]
 
 

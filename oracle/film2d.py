@@ -37,10 +37,13 @@ the reference's wall-normal z):
   * both on the band |phi| < 8 refined cells (BAND_GENERATION's role, two_phase.f:1622-2030):
     cells outside keep their value (the properties see phi only within one flow cell of the
     interface).
-Documented simplifications: surface tension is off (We = infinity; 2-D curvature is not
-built), the interface recession term of the phase change is not applied (the interface
-moves with the one-fluid velocity, which carries the expansion flow of S), and the viscous
-terms are explicit.
+  * surface tension: the continuum surface force -sigma kappa grad psi / rho_f on every face
+    (sigma = 1/We), kappa = div(grad phi / |grad phi|) from central differences of the refined
+    level set near the interface, averaged to the flow cells (the 2-D analogue of CAL_CUR /
+    CAL_CUR_INTEGRAL / INTER_CUR, two_phase.f:3317-4432).
+Documented simplifications: the interface recession term of the phase change is not applied
+(the interface moves with the one-fluid velocity, which carries the expansion flow of S),
+and the viscous terms are explicit.
 
 Every expression is written in the CUDA kernels' evaluation order (left to right, explicit
 parentheses; the kernels are compiled without FMA contraction), so all fields agree bit for
@@ -60,12 +63,12 @@ def default_props():
     mu 0.1/0.005, k 40/1, c_p 400/200, h_fg 1e4, superheat 5 K): density 40, viscosity 20,
     conductivity 40, specific heat 2, Ja = c_p,v dT / h_fg = 0.1, Pr_v = 1, and Re = 69.2 and
     Fr = 1 on the velocity sqrt(g Lx) with Lx the most dangerous Rayleigh-Taylor wavelength
-    (0.0787 m).  The pressure solves stop at a relative residual of 1e-8: with the interface's
+    (0.0787 m), We = rho_v U^2 Lx / sigma = 3.04 (sigma 0.1 N/m).  The pressure solves stop at a relative residual of 1e-8: with the interface's
     phase-change source on the right-hand side the multigrid-preconditioned CG stalls between
     1e-10 and 1e-9 at 512 x 1536 (the vapour film is a thin, 40 times more mobile layer sealed by
     the wall), and 1e-8 is met in about 12 iterations."""
-    return dict(re=69.2, visr=20.0, denr=40.0, prm=1.0, scr=2.0, tcr=40.0, jakob=0.1, fr=1.0, rtol=1e-8,
-                nreinit=2)
+    return dict(re=69.2, visr=20.0, denr=40.0, prm=1.0, scr=2.0, tcr=40.0, jakob=0.1, fr=1.0, we=3.04,
+                rtol=1e-8, nreinit=2)
 
 
 class Derived:
@@ -96,6 +99,10 @@ class Derived:
         self.cvol = 1.0 / 1.0 - 1.0 / P["denr"]
         self.gravity = 0.0 if P["fr"] == 0.0 else 1.0 / (P["fr"] * P["fr"])
         self.denp = P["denr"]
+        self.surf = 0.0 if P.get("we", 0.0) == 0.0 else 1.0 / P["we"]
+        self.ih2f = 0.5 / self.hf
+        self.ihfsq = 1.0 / (self.hf * self.hf)
+        self.q4 = 0.25 * self.ihfsq
         self.nreinit = int(P["nreinit"])
         self.band = 8.0 * self.hf  # transport / reinitialisation band |phi| < band (BAND_GENERATION's role)
         self.rtol = P["rtol"]
@@ -211,7 +218,32 @@ def mass_source(th, psi, tc, D):
     return md * D.cvol, md
 
 
-def momentum_u(u, v, den, vis, D):
+def curvature(phi, D):
+    """Curvature kappa = div(grad phi / |grad phi|) per flow cell (CAL_CUR's role in 2-D):
+    second-order central differences on the refined grid (x periodic, y indices clamped),
+    computed where |phi| < 2 h (zero elsewhere), averaged over the four sub-cells and limited
+    to |kappa| <= 1/h."""
+    nj = phi.shape[0]
+    idx = np.arange(nj)
+    up = phi[np.minimum(idx + 1, nj - 1)]
+    dn = phi[np.maximum(idx - 1, 0)]
+    E, W = np.roll(phi, -1, axis=1), np.roll(phi, 1, axis=1)
+    NE, NW = np.roll(up, -1, axis=1), np.roll(up, 1, axis=1)
+    SE, SW = np.roll(dn, -1, axis=1), np.roll(dn, 1, axis=1)
+    fx = (E - W) * D.ih2f
+    fy = (up - dn) * D.ih2f
+    fxx = (E - 2.0 * phi + W) * D.ihfsq
+    fyy = (up - 2.0 * phi + dn) * D.ihfsq
+    fxy = ((NE - NW) - (SE - SW)) * D.q4
+    g2 = fx * fx + fy * fy
+    num = (fxx * (fy * fy) - 2.0 * (fx * fy) * fxy) + fyy * (fx * fx)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        k = np.where((np.abs(phi) < 2.0 * D.h) & (g2 > 1e-12), num / (g2 * np.sqrt(g2)), 0.0)
+    kc = 0.25 * ((k[0::2, 0::2] + k[0::2, 1::2]) + (k[1::2, 0::2] + k[1::2, 1::2]))
+    return np.minimum(np.maximum(kc, -D.ih), D.ih)
+
+
+def momentum_u(u, v, den, vis, D, psi=None, kap=None):
     ih = D.ih
     ue, uw = _e(u), _w(u)
     un = _rows_n(u, u[-1])
@@ -233,10 +265,14 @@ def momentum_u(u, v, den, vis, D):
     tys = mus * ((u - us) * ih + (v[:-1] - vw[:-1]) * ih)
     rho = 0.5 * (_w(den) + den)
     visc = ((txe - txw) * ih + (tyn - tys) * ih) / rho
-    return visc - conv
+    if kap is None:
+        return visc - conv
+    # surface tension -sigma kappa grad psi on the face (continuum surface force)
+    kf = 0.5 * (_w(kap) + kap)
+    return visc - conv - (D.surf * kf) * ((psi - _w(psi)) * ih) / rho
 
 
-def momentum_v(u, v, den, vis, D):
+def momentum_v(u, v, den, vis, D, psi=None, kap=None):
     """Right-hand side on the faces j = 1..ny (returned as ny rows)."""
     ih = D.ih
     vc = v[1:]
@@ -262,7 +298,11 @@ def momentum_v(u, v, den, vis, D):
     dhi = _rows_n(den, den[-1])
     rho = 0.5 * (dlo + dhi)
     visc = ((txe - txw) * ih + (tyn - tys) * ih) / rho
-    return visc - conv + D.gravity * (D.denp / rho - 1.0)
+    if kap is None:
+        return visc - conv + D.gravity * (D.denp / rho - 1.0)
+    kf = 0.5 * (kap + _rows_n(kap, kap[-1]))
+    pshi = _rows_n(psi, psi[-1])
+    return visc - conv + D.gravity * (D.denp / rho - 1.0) - (D.surf * kf) * ((pshi - psi) * ih) / rho
 
 
 def energy_rhs(th, u, v, densc, tc, D):
@@ -430,8 +470,9 @@ def step(state, dt, props, mg_solve, mg_levels=6):
         iadt = 1.0 / (alpha * dt)
         psi, den, vis, densc, tc, bx, by = properties(phi, D)
         S, md = mass_source(th, psi, tc, D)
-        nu = momentum_u(u, v, den, vis, D)
-        nv = momentum_v(u, v, den, vis, D)
+        kap = curvature(phi, D)
+        nu = momentum_u(u, v, den, vis, D, psi, kap)
+        nv = momentum_v(u, v, den, vis, D, psi, kap)
         # predictor with the current pressure gradient (p = 0 on the top face)
         us = u + dt * (gam * nu + ro * ru) - adt * (bx * ((p - _w(p)) * D.ih))
         vs = np.zeros_like(v)

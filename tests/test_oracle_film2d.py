@@ -110,3 +110,23 @@ def test_product_inputs_match_the_restatement():
     for k in a:
         np.testing.assert_array_equal(a[k], b[k])
     assert F.default_props() == G.default_props()
+
+
+def test_curvature_of_a_circle():
+    """kappa = div(grad phi / |grad phi|) of phi = r - R is 1/r near the circle."""
+    nx, ny = 64, 64
+    D = F.Derived(nx, ny, F.default_props())
+    hf = D.hf
+    xf = (np.arange(2 * nx) + 0.5) * hf
+    yf = (np.arange(2 * ny) + 0.5) * hf
+    R = 0.25
+    phi = np.sqrt((xf[None, :] - 0.5) ** 2 + (yf[:, None] - 0.5) ** 2) - R
+    kap = F.curvature(phi, D)
+    psi = F.properties(phi, D)[0]
+    band = (psi > 0.05) & (psi < 0.95)
+    assert band.sum() > 50
+    assert np.abs(kap[band] * R - 1.0).max() < 0.1
+    # zero beyond the curvature band (|phi| < 2 h on the refined centres)
+    xc = (np.arange(nx) + 0.5) * D.h
+    dist = np.abs(np.sqrt((xc[None, :] - 0.5) ** 2 + (xc[:, None] - 0.5) ** 2) - R)
+    assert np.abs(kap[dist > 3 * D.h]).max() == 0.0
