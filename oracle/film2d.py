@@ -48,7 +48,9 @@ and the viscous terms are explicit.
 Every expression is written in the CUDA kernels' evaluation order (left to right, explicit
 parentheses; the kernels are compiled without FMA contraction), so all fields agree bit for
 bit except through the iterative pressure solve, which both sides converge to the same
-relative residual.
+relative residual.  film2d.cpp restates this file in C++/OpenMP (step_native): bit-identical to
+step() wherever the multigrid's OpenMP reductions run serially (below 65536 cells), and the
+fast CPU baseline.
 
 Layout (row-major, x fastest): u (ny, nx) on the face west of cell i; v (ny + 1, nx) on the
 face below cell row j (v[0] = 0 wall, v[ny] top); p, theta (ny, nx); phi (2 ny, 2 nx).
@@ -514,6 +516,31 @@ def oracle_mg(levels, rtol=1e-10, ncoarse=2):
                                           max_cycles=200)
         return p, cyc, rel, st
     return solve
+
+
+def step_native(state, dt, props, levels, native=False):
+    """The same step through the C++/OpenMP restatement (film2d.cpp, bit-identical to step());
+    returns (new state, info with iterations, rel, status, S, mdot)."""
+    import ctypes as C
+    from . import oracle as orc
+    L = orc.lib(native)
+    D = C.POINTER(C.c_double)
+    I = C.POINTER(C.c_int)
+    f = L.orc_film2d_step
+    f.argtypes = [C.c_int, C.c_int, D, C.c_double, C.c_int, C.c_int, C.c_double] + [D] * 5 + [I, D, I, D, D]
+    ny, nx = state["p"].shape
+    out = {k: np.array(state[k], dtype=np.float64, copy=True, order="C") for k in ("u", "v", "p", "th", "phi")}
+    P = np.array([props[k] for k in ("re", "visr", "denr", "prm", "scr", "tcr", "jakob", "fr")] +
+                 [props.get("we", 0.0)], dtype=np.float64)
+    its = (C.c_int * 3)()
+    rels = (C.c_double * 3)()
+    sts = (C.c_int * 3)()
+    S = np.zeros((ny, nx))
+    md = np.zeros((ny, nx))
+    ptr = lambda a: a.ctypes.data_as(D)  # noqa: E731
+    f(nx, ny, ptr(P), props["rtol"], int(props["nreinit"]), levels, dt, ptr(out["u"]), ptr(out["v"]), ptr(out["p"]),
+      ptr(out["th"]), ptr(out["phi"]), its, rels, sts, ptr(S), ptr(md))
+    return out, dict(iterations=list(its), rel=list(rels), status=list(sts), S=S, mdot=md)
 
 
 def divergence(u, v, h):

@@ -130,3 +130,19 @@ def test_curvature_of_a_circle():
     xc = (np.arange(nx) + 0.5) * D.h
     dist = np.abs(np.sqrt((xc[None, :] - 0.5) ** 2 + (xc[:, None] - 0.5) ** 2) - R)
     assert np.abs(kap[dist > 3 * D.h]).max() == 0.0
+
+
+def test_cpp_restatement_is_bit_identical_to_numpy():
+    """oracle/film2d.cpp (C++/OpenMP, the fast CPU baseline) reproduces the numpy restatement bit
+    for bit over two steps (at this size the multigrid's reductions run serially)."""
+    P = F.default_props()
+    st = F.initial_state(NX, NY, y0_cells=8, amp_cells=2, props=P)
+    dt = F.stable_dt(NX, P)
+    a, b = st, st
+    for _ in range(2):
+        a, ia = F.step(a, dt, P, F.oracle_mg(3, P["rtol"]))
+        b, ib = F.step_native(b, dt, P, 3)
+        assert ia["iterations"] == ib["iterations"] and ib["status"] == [0, 0, 0]
+        for k in a:
+            np.testing.assert_array_equal(a[k], b[k])
+        np.testing.assert_array_equal(ia["mdot"], ib["mdot"])
