@@ -33,7 +33,8 @@ enum lica_status {
     LICA_NAN = 3,           /* non-finite value met */
     LICA_BAD_ARG = 4,       /* argument outside what the entry point supports */
     LICA_ERR_CUDA = 5,      /* a CUDA runtime call failed (see lica_last_error) */
-    LICA_ERR_NOMEM = 6
+    LICA_ERR_NOMEM = 6,
+    LICA_ERR_IO = 7         /* a file could not be opened, read or written, or a record is malformed */
 };
 
 /* Message for the last LICA_ERR_CUDA / LICA_BAD_ARG on the calling thread. */
@@ -250,6 +251,53 @@ typedef struct {
  * 1d.f:821-946 with IPHS = 1, LVSINIT two_phase.f:116-388, GRID_COUPLING(1)); host arrays
  * of one column. */
 int lica_gpu_column_init(int32_t n, double length, double z0, const lica_col_props* props, lica_col_state* st);
+
+/* ------------------------------------------------------------------------------------
+ * fld###### restart files of one column (host code, no GPU): the reference's ASCII field
+ * file, record for record.  The column is the reference's 1-D case (N1 = N2 = 2, N3 = n+1;
+ * N1F = N2F = 3, N3F = 2n+1); each field is written on all its (I, J) replicas and read from
+ * I = J = 1.  The band lists are the cells of each layer in ascending K, four replicas each.
+ * ---------------------------------------------------------------------------------- */
+typedef struct {
+    int64_t ihist;                 /* IHIST, the number in the file name */
+    int64_t m;                     /* M, the time-step counter (written: scal[2]) */
+    double time, dt;               /* TIME, DT (written: scal[1], scal[0]; read: DT_O) */
+    double qvol_ori;               /* QVOL_ORI, the flow-rate reference of ICH = 1 runs */
+    int32_t ips, ipx, ipy, ipz;    /* IPS (1: PRM, SCR, TCR and T follow), IPX, IPY, IPZ */
+    double pra;                    /* PRA = PRM (read only) */
+    double denr, visr, fr, surf_j, fk, re_air; /* FORMAT 1012 (written: props, and fk) */
+    double prm, scr, tcr;          /* FORMAT 1006 (read only; written from props) */
+    int32_t n_max;                 /* N_MAX, band layers listed (read only; written: 11) */
+    int32_t contact, contact_old, lvson;           /* the level set's contact state */
+    double vol_tot_ori;            /* VOL_TOT_ORI (read only; written: scal[3]) */
+    double contact_start, contact_time, t_con;
+} lica_fld_info;
+
+/* lica.in switches applied after a read. */
+typedef struct {
+    int32_t ireset; /* IRESET = 1: TIME starts from 0 (1d.f:175-178) */
+    int32_t idtold; /* IDTOLD = 1: DT = the file's DT_O, else props->dt0 (1d.f:1080-1085) */
+    int32_t ipzero; /* IPZERO = 1: P = 0 after the read (1d.f:1055) */
+} lica_fld_options;
+
+/* The reference's file name for IHIST (1d.f:1155-1163): "fld" and six digits; out gets
+ * 10 bytes with the terminating NUL.  LICA_BAD_ARG for IHIST outside 0..999999. */
+int lica_fld_name(int64_t ihist, char* out, int32_t cap);
+
+/* WRITEFIELD (1d.f:1121-1232) of one column's host state.  From info: ihist, qvol_ori,
+ * ips, ipx, ipy, ipz, fk and the contact fields; the rest comes from props and st. */
+int lica_col_fld_write(const char* path, int32_t n, const lica_col_props* props, const lica_col_state* st,
+                       const lica_fld_info* info);
+
+/* The column size n (= N3 - 1) of a file; LICA_BAD_ARG if it is not a column. */
+int lica_col_fld_dims(const char* path, int32_t* n);
+
+/* PREFLD (1d.f:972-1098) into one column's host state, then the start-up that follows a
+ * read: LVSINIT's read branch (two_phase.f:148-205: the band from the lists, ALPHI_BC,
+ * CAL_PSIF(1, N_MAX)), GRID_COUPLING(1), VOL_TOT_IPHS = VOL_TOT_ORI, the options above and
+ * M = 0 (the time loop starts again at M = 1).  info receives the file's header values. */
+int lica_col_fld_read(const char* path, int32_t n, double length, const lica_col_props* props,
+                      const lica_fld_options* opt, lica_col_state* st, lica_fld_info* info);
 
 /* Device scratch the step kernel needs for ncol columns of n cells. */
 size_t lica_gpu_column_scratch_bytes(int32_t ncol, int32_t n);

@@ -22,7 +22,7 @@ FLAGS = [
 
 
 def sources():
-    return sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")))
+    return sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")) + glob.glob(os.path.join(HERE, "csrc", "*.cpp")))
 
 
 def deps():

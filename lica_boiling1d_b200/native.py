@@ -42,6 +42,20 @@ class ColState(C.Structure):
     _fields_ = [(k, C.c_void_p) for k in COL_FIELDS]
 
 
+class FldInfo(C.Structure):
+    _fields_ = [("ihist", C.c_int64), ("m", C.c_int64), ("time", C.c_double), ("dt", C.c_double),
+                ("qvol_ori", C.c_double), ("ips", C.c_int32), ("ipx", C.c_int32), ("ipy", C.c_int32),
+                ("ipz", C.c_int32), ("pra", C.c_double)] + \
+        [(k, C.c_double) for k in ("denr", "visr", "fr", "surf_j", "fk", "re_air", "prm", "scr", "tcr")] + \
+        [("n_max", C.c_int32), ("contact", C.c_int32), ("contact_old", C.c_int32), ("lvson", C.c_int32),
+         ("vol_tot_ori", C.c_double), ("contact_start", C.c_double), ("contact_time", C.c_double),
+         ("t_con", C.c_double)]
+
+
+class FldOptions(C.Structure):
+    _fields_ = [("ireset", C.c_int32), ("idtold", C.c_int32), ("ipzero", C.c_int32)]
+
+
 class Film2DProps(C.Structure):
     _fields_ = [(k, C.c_double) for k in ("re", "visr", "denr", "prm", "scr", "tcr", "jakob", "fr", "we",
                                           "rtol")] + \
@@ -81,6 +95,12 @@ SIGNATURES = {
                                       [C.POINTER(LvsParams), C.c_void_p]),
     "lica_gpu_column_init": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.POINTER(ColProps),
                                        C.POINTER(ColState)]),
+    "lica_fld_name": (C.c_int, [C.c_int64, C.c_char_p, C.c_int32]),
+    "lica_col_fld_write": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(ColProps), C.POINTER(ColState),
+                                     C.POINTER(FldInfo)]),
+    "lica_col_fld_dims": (C.c_int, [C.c_char_p, _I32]),
+    "lica_col_fld_read": (C.c_int, [C.c_char_p, C.c_int32, C.c_double, C.POINTER(ColProps), C.POINTER(FldOptions),
+                                    C.POINTER(ColState), C.POINTER(FldInfo)]),
     "lica_gpu_column_scratch_bytes": (C.c_size_t, [C.c_int32, C.c_int32]),
     "lica_gpu_column_profile_device": (C.c_int, [C.c_void_p]),
     "lica_gpu_column_steps_device": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.POINTER(ColProps),
@@ -116,7 +136,7 @@ SIGNATURES = {
 }
 
 STATUS = {0: "LICA_OK", 1: "LICA_NOT_CONVERGED", 2: "LICA_BAND_OVERFLOW", 3: "LICA_NAN", 4: "LICA_BAD_ARG",
-          5: "LICA_ERR_CUDA", 6: "LICA_ERR_NOMEM"}
+          5: "LICA_ERR_CUDA", 6: "LICA_ERR_NOMEM", 7: "LICA_ERR_IO"}
 
 
 class LicaError(RuntimeError):

@@ -1,0 +1,86 @@
+"""Restart files of 1-D columns in the reference's ``fld######`` format (WRITEFIELD,
+1d.f:1121-1232; PREFLD, 1d.f:972-1098), through the library's host-side reader and writer
+(lica_col_fld_*).
+
+``write_field`` writes one column of a ``Columns`` state (host or device) as the file the
+reference writes every NPRINT steps; ``read_field`` reads such a file into a one-column
+``Columns`` state that starts the time loop the way the reference does after IREAD = 1:
+the band rebuilt from the lists, PSIF / PSI_CN / PSI_ZN recomputed, VOL_TOT_IPHS =
+VOL_TOT_ORI and the step counter M back at 0.  The file keeps 13 significant digits
+(ES20.12), so a resumed run continues from the written state rounded to that precision.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import native
+from .column import Columns
+
+# lica.in's switches and the reference's contact-state defaults (1d.f:573-582)
+DEFAULT_OPTIONS = dict(ireset=1, idtold=0, ipzero=0)
+DEFAULT_INFO = dict(ihist=0, qvol_ori=0.0, fk=0.0, ips=1, ipx=1, ipy=1, ipz=3, contact=0, contact_old=0,
+                    contact_start=0.0, contact_time=0.0, lvson=1, t_con=100.0)
+
+
+def field_name(ihist):
+    """The reference's name for history record IHIST: "fld" and six digits."""
+    buf = C.create_string_buffer(16)
+    native.check(native.lib().lica_fld_name(int(ihist), buf, len(buf)), "lica_fld_name")
+    return buf.value.decode()
+
+
+def _host_column(cols, column):
+    host = cols.to(None) if cols.on_device else cols
+    one = {k: np.ascontiguousarray(v[column]) for k, v in host.arrays.items()}
+    return one
+
+
+def _state(arrays):
+    return native.ColState(*[arrays[k].ctypes.data for k in native.COL_FIELDS])
+
+
+def write_field(cols, path, props, *, column=0, **info):
+    """Write column `column` of `cols` to `path` (a directory gets the file name of
+    ``info['ihist']``).  info: ihist, qvol_ori, fk, ips, ipx, ipy, ipz and the contact state
+    (DEFAULT_INFO).  Returns the path written."""
+    unknown = set(info) - set(DEFAULT_INFO)
+    if unknown:
+        raise TypeError(f"unknown fld fields: {sorted(unknown)}")
+    vals = dict(DEFAULT_INFO, **info)
+    if os.path.isdir(path):
+        path = os.path.join(path, field_name(vals["ihist"]))
+    one = _host_column(cols, column)
+    fi = native.FldInfo(**vals)
+    cp = props.c()
+    native.check(native.lib().lica_col_fld_write(os.fsencode(path), cols.n, C.byref(cp), C.byref(_state(one)),
+                                                 C.byref(fi)), "lica_col_fld_write")
+    return path
+
+
+def field_size(path):
+    """The column size n of a restart file."""
+    n = C.c_int32()
+    native.check(native.lib().lica_col_fld_dims(os.fsencode(path), C.byref(n)), "lica_col_fld_dims")
+    return int(n.value)
+
+
+def read_field(path, length, props, **options):
+    """Read a restart file into a one-column host ``Columns`` of the column `length`.
+    options: ireset, idtold, ipzero (DEFAULT_OPTIONS, lica.in's).  Returns (cols, header)
+    with the file's header values as a dict."""
+    unknown = set(options) - set(DEFAULT_OPTIONS)
+    if unknown:
+        raise TypeError(f"unknown options: {sorted(unknown)}")
+    n = field_size(path)
+    cols = Columns.empty(1, n, length)
+    one = {k: np.ascontiguousarray(v[0]) for k, v in cols.arrays.items()}
+    fi = native.FldInfo()
+    opt = native.FldOptions(**dict(DEFAULT_OPTIONS, **options))
+    cp = props.c()
+    native.check(native.lib().lica_col_fld_read(os.fsencode(path), n, float(length), C.byref(cp), C.byref(opt),
+                                                C.byref(_state(one)), C.byref(fi)), "lica_col_fld_read")
+    for k in cols.arrays:
+        cols.arrays[k][0] = one[k]
+    header = {name: getattr(fi, name) for name, _ in native.FldInfo._fields_}
+    return cols, header

@@ -911,6 +911,35 @@ int orc_col_init(int n, double L, double z0, const double* props, const int* ipr
     return 0;
 }
 
+// The start-up after a restart read, for one column: LVSINIT's read branch
+// (two_phase.f:148-205) on the band PREFLD listed -- phi holds the listed values and 0
+// elsewhere, layer the list each cell came from -- ALPHI_BC, CAL_PSIF(1, N_MAX) with its
+// global snap (two_phase.f:2711-2722), then GRID_COUPLING(1) (1d.f:138).
+int orc_col_resume(int n, double L, double* phi, const int* layer, double* psif, double* psi_cn, double* psi_zn) {
+    Col c;
+    c.init(n, L);
+    std::memcpy(c.phi.data(), phi, sizeof(double) * (c.nf + 7));
+    for (int m = 1; m <= N_MAX; ++m)
+        for (int k = -2; k <= c.nf + 4; ++k)
+            if (layer[k + GL] == m) c.band[m].push_back(k);
+    c.rebuild_layer();
+    alphi_bc(c);
+    std::vector<double> ps = cal_psif_mtp(c, 1, N_MAX);
+    for (int k = 0; k <= c.nf + 1; ++k) {
+        double v = (k >= 1 && k <= c.nf) ? ps[k] : 0.0;
+        if (v < 1e-5) v = 0.0;
+        else if (v > 0.99999) v = 1.0;
+        psif[k] = v;
+    }
+    for (int k = 0; k <= n + 1; ++k) {
+        psi_cn[k] = 0.0;
+        psi_zn[k] = 0.0;
+    }
+    grid_coupling(n, L, psif, c.layer.data(), 1, psi_cn, psi_zn);
+    std::memcpy(phi, c.phi.data(), sizeof(double) * (c.nf + 7));
+    return 0;
+}
+
 // One time step of MAIN (1d.f:190-250): DETERMINE_DT, three RK3 substeps of RHSNLHS,
 // CONVRGE1, TRANSPORT and GRID_COUPLING(0), TIME += DT.
 //   stats[8]: CFL of the flow, max |div u - source| (last substep), TEMP_EXTP iterations,

@@ -38,6 +38,7 @@ def lib(native: bool = False):
         L.orc_lvs_reinit.argtypes = [C.c_int, C.c_double, _D, _INT, C.c_int]
         L.orc_col_init.argtypes = [C.c_int, C.c_double, C.c_double, _D, _INT] + [_D] * 6 + [_INT] + [_D] * 5 + \
             [_INT, _D]
+        L.orc_col_resume.argtypes = [C.c_int, C.c_double, _D, _INT, _D, _D, _D]
         L.orc_col_step.argtypes = [C.c_int, C.c_double, _D, _INT] + [_D] * 6 + [_INT] + [_D] * 5 + [_INT, _D, _D]
         _LIBS[key] = L
     return _LIBS[key]
