@@ -253,6 +253,32 @@ typedef struct {
 int lica_gpu_column_init(int32_t n, double length, double z0, const lica_col_props* props, lica_col_state* st);
 
 /* ------------------------------------------------------------------------------------
+ * Non-uniform grids (host code, no GPU)
+ * ---------------------------------------------------------------------------------- */
+
+/* One section of the grid generator (grid.f:118-128): XYZ(N), N = ngi..ngf, into
+ * xyz[N - 1].  iopt 1: UNIFORM (grid.f:326-345); 2: GEOPRO (348-380), fac1 = ER, fac2 =
+ * YESEXP (1 expansion, else compression); any other: HYPTAN (383-420), fac1 = GAM, fac2 =
+ * XSI (1 clusters at xyzi, 0.5 at both ends, 0 at xyzf).  Double precision. */
+int lica_grid_section(int32_t iopt, double xyzi, double xyzf, int32_t ngi, int32_t ngf, double fac1, double fac2,
+                      double* xyz);
+
+/* GEOMETRIC (1d.f:4808-4882) for one wall-bounded direction with n faces z[1..n] (z[0]
+ * unused): SDZ(0..n), VDZ(1..n), SSDZ(0..n), VVDZ(1..n), ZP(0..n), each array n+1 long
+ * and indexed by the Fortran index (entries the reference leaves unset are 0).  The VVDZ
+ * and SSDZ of a column are the vvdz / ssdz arguments of lica_gpu_poisson. */
+int lica_grid_metrics(int32_t n, const double* z, double* sdz, double* vdz, double* ssdz, double* vvdz, double* zp);
+
+/* A pressure system on a wall-normal (y) grid of faces yface[0..ny], stretched, x uniform
+ * and periodic: POISSON's operator (1d.f:3535-3541) in 2-D, multiplied by each row's
+ * height so that it is symmetric, written as the multigrid's arrays for hy = 1:
+ * bx_out = bx dy_j, by_out = by / (centre distance) (top row: by / dy_{ny-1}), f_out =
+ * f dy_j.  Solve with lica_mg_create(nx, ny, hx, 1.0, ...); p is the solution of the
+ * stretched system. */
+int lica_mg_stretched_system(int32_t nx, int32_t ny, const double* yface, const double* bx, const double* by,
+                             const double* f, double* bx_out, double* by_out, double* f_out);
+
+/* ------------------------------------------------------------------------------------
  * fld###### restart files of one column (host code, no GPU): the reference's ASCII field
  * file, record for record.  The column is the reference's 1-D case (N1 = N2 = 2, N3 = n+1;
  * N1F = N2F = 3, N3F = 2n+1); each field is written on all its (I, J) replicas and read from

@@ -95,6 +95,10 @@ SIGNATURES = {
                                       [C.POINTER(LvsParams), C.c_void_p]),
     "lica_gpu_column_init": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.POINTER(ColProps),
                                        C.POINTER(ColState)]),
+    "lica_grid_section": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                    _D]),
+    "lica_grid_metrics": (C.c_int, [C.c_int32, _D, _D, _D, _D, _D, _D]),
+    "lica_mg_stretched_system": (C.c_int, [C.c_int32, C.c_int32, _D, _D, _D, _D, _D, _D, _D]),
     "lica_fld_name": (C.c_int, [C.c_int64, C.c_char_p, C.c_int32]),
     "lica_col_fld_write": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(ColProps), C.POINTER(ColState),
                                      C.POINTER(FldInfo)]),

@@ -72,6 +72,36 @@ def uniform_column_geometry(n3m, zl=1.0, m1=2, m2=2):
     return dict(m1=m1, m2=m2, m3=m3, n1m=m1 - 1, n2m=m2 - 1, n3m=n3m, vvdz=vvdz, ssdz=ssdz, fixkl=fixkl, kpv=kpv)
 
 
+def column_geometry(z, m1=2, m2=2):
+    """GEOM arrays of a 1-D column on the faces z[0..n3m] (Z(1)..Z(N3), any spacing), for
+    lica_gpu_poisson: VVDZ and SSDZ from GEOMETRIC (1d.f:4808-4882, lica_grid_metrics),
+    FIXKL(1) = 1 and KPV(K) = K + 1 for IPZ != 1 (INDICES 1d.f:4975-5029)."""
+    from .grid import metrics
+    z = np.asarray(z, dtype=np.float64)
+    n3m = len(z) - 1
+    m3 = n3m + 1
+    g = metrics(z)
+    vvdz = np.ascontiguousarray(g["vvdz"][1:m3 + 1])
+    ssdz = np.zeros(m3 + 1)
+    ssdz[1:n3m + 1] = g["ssdz"][1:n3m + 1]
+    fixkl = np.zeros(m3 - 1)
+    fixkl[0] = 1.0
+    kpv = np.arange(1, m3 + 3, dtype=np.int64)
+    return dict(m1=m1, m2=m2, m3=m3, n1m=m1 - 1, n2m=m2 - 1, n3m=n3m, vvdz=vvdz, ssdz=ssdz, fixkl=fixkl, kpv=kpv)
+
+
+def stretched_system(yface, bx, by, f):
+    """(bx', by', f') of a pressure system on the stretched wall-normal faces yface[0..ny]
+    (lica_mg_stretched_system): solve them with MultigridPoisson(nx, ny, hx, 1.0)."""
+    ny, nx = f.shape
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (yface, bx, by, f)]
+    assert arrs[0].shape == (ny + 1,) and arrs[1].shape == (ny, nx) and arrs[2].shape == (ny + 1, nx)
+    out = [np.empty_like(arrs[1]), np.empty_like(arrs[2]), np.empty_like(arrs[3])]
+    native.check(native.lib().lica_mg_stretched_system(nx, ny, *(a.ctypes.data_as(_D) for a in arrs + out)),
+                 "lica_mg_stretched_system")
+    return tuple(out)
+
+
 PRECISION = {"fp64": 0, "mixed": 1}
 
 
