@@ -51,5 +51,5 @@ def test_multigrid_on_a_stretched_system(precision):
     p = np.zeros((ny, nx))
     it, rel, st = mg.solve(p, fs, bxs, bys, rtol=1e-10, max_iters=200)
     mg.close()
-    assert st == 0 and it < 80
+    assert st == 0 and it < 50
     assert np.abs(p - x).max() <= 1e-9 * np.abs(x).max()
