@@ -31,29 +31,37 @@ def field_name(ihist):
 
 
 def _host_column(cols, column):
+    """Column `column` of a Columns or ColumnBatch state as host arrays, and its size n."""
+    from .column import ColumnBatch
+    if isinstance(cols, ColumnBatch):
+        return {k: np.ascontiguousarray(v) for k, v in cols.column(column).items()}, int(cols.n[column])
     host = cols.to(None) if cols.on_device else cols
-    one = {k: np.ascontiguousarray(v[column]) for k, v in host.arrays.items()}
-    return one
+    return {k: np.ascontiguousarray(v[column]) for k, v in host.arrays.items()}, cols.n
 
 
 def _state(arrays):
     return native.ColState(*[arrays[k].ctypes.data for k in native.COL_FIELDS])
 
 
-def write_field(cols, path, props, *, column=0, **info):
-    """Write column `column` of `cols` to `path` (a directory gets the file name of
-    ``info['ihist']``).  info: ihist, qvol_ori, fk, ips, ipx, ipy, ipz and the contact state
-    (DEFAULT_INFO).  Returns the path written."""
+def write_field(cols, path, props=None, *, column=0, **info):
+    """Write column `column` of `cols` (a ``Columns`` or an uneven ``ColumnBatch``, host or
+    device) to `path` (a directory gets the file name of ``info['ihist']``).  props: the
+    column's properties (a batch's own by default).  info: ihist, qvol_ori, fk, ips, ipx,
+    ipy, ipz and the contact state (DEFAULT_INFO).  Returns the path written."""
     unknown = set(info) - set(DEFAULT_INFO)
     if unknown:
         raise TypeError(f"unknown fld fields: {sorted(unknown)}")
     vals = dict(DEFAULT_INFO, **info)
     if os.path.isdir(path):
         path = os.path.join(path, field_name(vals["ihist"]))
-    one = _host_column(cols, column)
+    one, n = _host_column(cols, column)
+    if props is None:
+        if not hasattr(cols, "props"):
+            raise TypeError("write_field: props is required for a Columns state")
+        props = cols.props[column]
     fi = native.FldInfo(**vals)
     cp = props.c()
-    native.check(native.lib().lica_col_fld_write(os.fsencode(path), cols.n, C.byref(cp), C.byref(_state(one)),
+    native.check(native.lib().lica_col_fld_write(os.fsencode(path), n, C.byref(cp), C.byref(_state(one)),
                                                  C.byref(fi)), "lica_col_fld_write")
     return path
 

@@ -185,6 +185,23 @@ def test_fortran_input_forms(tmp_path):
     assert p[6] == -7250.0
 
 
+def test_columns_of_an_uneven_batch(tmp_path):
+    """Each column of an uneven batch (its own size and properties) written from the batch
+    equals the oracle's WRITEFIELD of that column's state."""
+    from lica_boiling1d_b200 import restart as R
+    from lica_boiling1d_b200.column import ColumnBatch, uneven_batch
+    n, length, z0, props = uneven_batch(4, seed=3, nmin=16, nmax=96)
+    b = ColumnBatch.films(n, length, z0, props)
+    for c in range(4):
+        d = tmp_path / f"c{c}"
+        d.mkdir()
+        path = R.write_field(b, str(d), column=c, ihist=c)
+        st = b.column(c)
+        assert open(path).read() == F.write_column(st, int(n[c]), props[c], dict(R.DEFAULT_INFO, ihist=c))
+        cols, _ = R.read_field(path, float(length[c]), props[c])
+        assert cols.n == int(n[c]) and np.array_equal(cols.arrays["layer"][0], st["layer"])
+
+
 def test_field_names():
     from lica_boiling1d_b200 import native
     from lica_boiling1d_b200 import restart as R
