@@ -8,6 +8,9 @@ reference writes every NPRINT steps; ``read_field`` reads such a file into a one
 the band rebuilt from the lists, PSIF / PSI_CN / PSI_ZN recomputed, VOL_TOT_IPHS =
 VOL_TOT_ORI and the step counter M back at 0.  The file keeps 13 significant digits
 (ES20.12), so a resumed run continues from the written state rounded to that precision.
+
+``save_checkpoint`` / ``load_checkpoint`` keep a complete state (columns, uneven column
+batches, the 2-D film) bit for bit in a binary .npz, so that a run continues exactly.
 """
 import ctypes as C
 import os
@@ -92,3 +95,71 @@ def read_field(path, length, props, **options):
         cols.arrays[k][0] = one[k]
     header = {name: getattr(fi, name) for name, _ in native.FldInfo._fields_}
     return cols, header
+
+
+# ------------------------------------------------------------------------------------
+# Binary checkpoints: the complete state, bit for bit (the fld file keeps 13 digits and
+# only the fields the reference writes).
+
+CHECKPOINT_VERSION = 1
+
+
+def _props_dict(p):
+    from dataclasses import asdict
+    return asdict(p)
+
+
+def save_checkpoint(path, state, props=None):
+    """Save a ``Columns``, a ``ColumnBatch`` (host or device) or a 2-D film state (the dict
+    of Film2D's fields, host or device, with `props` its property dict) to `path` (.npz).
+    Every array is saved exactly; resuming from it continues the run bit for bit."""
+    import json
+
+    from .column import ColumnBatch, Columns
+    meta = dict(version=CHECKPOINT_VERSION)
+    arrays = {}
+    if isinstance(state, ColumnBatch):
+        host = state.to(None) if not isinstance(state.arrays["w"], np.ndarray) else state
+        meta.update(kind="column_batch", props=[_props_dict(p) for p in state.props])
+        arrays.update({"a_" + k: v for k, v in host.arrays.items()})
+        arrays.update(n=state.n, length=state.length)
+    elif isinstance(state, Columns):
+        if props is None:
+            raise TypeError("save_checkpoint: props is required for a Columns state")
+        host = state.to(None) if state.on_device else state
+        meta.update(kind="columns", n=state.n, length=state.length, props=_props_dict(props))
+        arrays.update({"a_" + k: v for k, v in host.arrays.items()})
+    elif isinstance(state, dict) and set(state) >= {"u", "v", "p", "th", "phi"}:
+        meta.update(kind="film2d", props=dict(props or {}))
+        for k in ("u", "v", "p", "th", "phi"):
+            v = state[k]
+            arrays["a_" + k] = v if isinstance(v, np.ndarray) else v.detach().cpu().numpy()
+    else:
+        raise TypeError("save_checkpoint: a Columns, ColumnBatch or film state dict is expected")
+    with open(path, "wb") as f:
+        np.savez(f, meta=np.array(json.dumps(meta)), **arrays)
+    return path
+
+
+def load_checkpoint(path):
+    """(state, props) saved by save_checkpoint, on the host: a ``Columns`` with its
+    ColumnProps, a ``ColumnBatch`` (its props inside), or a film dict with its property
+    dict."""
+    import json
+
+    from .column import ColumnBatch, ColumnProps, Columns
+    with np.load(path, allow_pickle=False) as z:
+        meta = json.loads(str(z["meta"]))
+        if meta.get("version") != CHECKPOINT_VERSION:
+            raise ValueError(f"{path}: checkpoint version {meta.get('version')} is not {CHECKPOINT_VERSION}")
+        arrays = {k[2:]: z[k].copy() for k in z.files if k.startswith("a_")}
+        kind = meta["kind"]
+        if kind == "columns":
+            return Columns(meta["n"], meta["length"], arrays), ColumnProps(**meta["props"])
+        if kind == "column_batch":
+            props = [ColumnProps(**p) for p in meta["props"]]
+            b = ColumnBatch(z["n"].copy(), z["length"].copy(), props, arrays)
+            return b, None
+        if kind == "film2d":
+            return arrays, meta["props"]
+    raise ValueError(f"{path}: unknown checkpoint kind {kind!r}")

@@ -202,6 +202,46 @@ def test_columns_of_an_uneven_batch(tmp_path):
         assert cols.n == int(n[c]) and np.array_equal(cols.arrays["layer"][0], st["layer"])
 
 
+def test_binary_checkpoints_are_exact(tmp_path):
+    """save_checkpoint / load_checkpoint keep every array of a column state, an uneven batch
+    and a 2-D film state bit for bit, and a column resumed from one continues exactly."""
+    from lica_boiling1d_b200 import film2d
+    from lica_boiling1d_b200 import restart as R
+    from lica_boiling1d_b200.column import ColumnBatch, uneven_batch
+    n, props = 64, _props(denr=800.0, jakob=0.02)
+    st = _evolved(n, 0.15, 6, props)
+    path = R.save_checkpoint(str(tmp_path / "c.npz"), _cols(st, n), props)
+    cols, p2 = R.load_checkpoint(path)
+    assert p2 == props and cols.n == n and cols.length == 1.0
+    for k, v in st.items():
+        a = cols.arrays[k][0]
+        assert a.dtype == v.dtype and np.array_equal(a, v), k
+    resumed = {k: v[0].copy() for k, v in cols.arrays.items()}
+    for _ in range(3):
+        assert O.col_step(st, n, 1.0, props) == 0 and O.col_step(resumed, n, 1.0, p2) == 0
+    for k, v in st.items():
+        assert np.array_equal(resumed[k], v), k
+
+    nb, length, z0, bprops = uneven_batch(3, seed=5, nmin=16, nmax=80)
+    b = ColumnBatch.films(nb, length, z0, bprops)
+    path = R.save_checkpoint(str(tmp_path / "b.npz"), b)
+    b2, _ = R.load_checkpoint(path)
+    assert np.array_equal(b2.n, b.n) and np.array_equal(b2.length, b.length) and b2.props == b.props
+    assert np.array_equal(b2.offsets, b.offsets)
+    for k, v in b.arrays.items():
+        assert np.array_equal(b2.arrays[k], v), k
+
+    fp = film2d.default_props()
+    fs = film2d.initial_state(64, 96, 24.0, 2.0, fp)
+    path = R.save_checkpoint(str(tmp_path / "f.npz"), fs, fp)
+    f2, fp2 = R.load_checkpoint(path)
+    assert fp2 == fp
+    for k in film2d.FIELDS:
+        assert np.array_equal(f2[k], fs[k]), k
+    with pytest.raises(TypeError):
+        R.save_checkpoint(str(tmp_path / "x.npz"), {"w": 1})
+
+
 def test_field_names():
     from lica_boiling1d_b200 import native
     from lica_boiling1d_b200 import restart as R
