@@ -397,7 +397,9 @@ int orc_film2d_step(int nx, int ny, const double* props, double rtol, int nreini
         std::fill(dp.begin(), dp.end(), 0.0);
         int cyc = 0;
         double rel = 0.0;
-        const int st = orc_mg_solve(nx, ny, d.h, d.h, nlevels, 2, 2, 2, 1, 2, 0, f.data(), P.bx.data(), P.by.data(),
+        // V(2,2), 2 coarse cycles, flags 5 = symmetric smoothing + piecewise-constant
+        // prolongation (the GPU multigrid's cycle), PCG
+        const int st = orc_mg_solve(nx, ny, d.h, d.h, nlevels, 2, 2, 2, 5, 2, 0, f.data(), P.bx.data(), P.by.data(),
                                     dp.data(), rtol, 200, &cyc, &rel, hist.data());
         if (iters) iters[k - 1] = cyc;
         if (rels) rels[k - 1] = rel;

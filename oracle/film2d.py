@@ -508,12 +508,13 @@ def step(state, dt, props, mg_solve, mg_levels=6):
 
 
 def oracle_mg(levels, rtol=1e-10, ncoarse=2):
-    """The oracle's 2-D multigrid (oracle/mg2d.cpp) as step()'s pressure solver."""
+    """The oracle's 2-D multigrid (oracle/mg2d.cpp) as step()'s pressure solver, with the GPU
+    multigrid's cycle: symmetric smoothing and piecewise-constant prolongation (flags 5)."""
     from . import oracle as orc
 
     def solve(f, bx, by, h, p0):
         p, cyc, rel, _, st = orc.mg_solve(f, bx, by, h, h, nlevels=levels, ncoarse=ncoarse, p0=p0, rtol=rtol,
-                                          max_cycles=200)
+                                          max_cycles=200, sym=5)
         return p, cyc, rel, st
     return solve
 
