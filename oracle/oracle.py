@@ -51,9 +51,11 @@ def _p(a):
 METHODS = {"vcycle": 0, "defect": 1, "pcg": 2}
 
 
-def mg_solve(f, bx, by, hx, hy, *, nlevels=6, nu1=2, nu2=2, ncoarse=2, sym=True, method="pcg", rtol=1e-10,
+def mg_solve(f, bx, by, hx, hy, *, nlevels=6, nu1=2, nu2=2, ncoarse=2, sym=5, method="pcg", rtol=1e-10,
              max_cycles=100, mixed=False, p0=None, native=False):
-    """Multigrid solve of A p = f (see oracle/mg2d.cpp).  Returns (p, cycles, rel, hist, status)."""
+    """Multigrid solve of A p = f (see oracle/mg2d.cpp).  sym: the cycle flags (1 symmetric
+    smoothing, 2 R = P^T/4 of bilinear P, 4 piecewise-constant P, 8 y-line relaxation); the
+    default 5 is the GPU multigrid's cycle.  Returns (p, cycles, rel, hist, status)."""
     ny, nx = f.shape
     f = np.ascontiguousarray(f, dtype=np.float64)
     bx = np.ascontiguousarray(bx, dtype=np.float64)
@@ -86,8 +88,8 @@ def mg_smooth(u, f, bx, by, hx, hy, nsweeps, reverse=False):
     return u
 
 
-def mg_precond(r, bx, by, hx, hy, *, nlevels=6, nu1=2, nu2=2, ncoarse=2, sym=True, mixed=False):
-    """z = M r, one V-cycle preconditioner application."""
+def mg_precond(r, bx, by, hx, hy, *, nlevels=6, nu1=2, nu2=2, ncoarse=2, sym=5, mixed=False):
+    """z = M r, one V-cycle preconditioner application (sym: the cycle flags of mg_solve)."""
     ny, nx = r.shape
     z = np.empty((ny, nx))
     st = lib().orc_mg_precond(nx, ny, hx, hy, nlevels, nu1, nu2, ncoarse, int(sym), int(mixed),
