@@ -9,8 +9,8 @@ network works on dimensionless fields (f / rms(f), output scaled by rms(f) h^2 r
 weights trained on small grids apply at any resolution.
 
 Evaluation: PCG iterations to the same tolerance from x0 = 0 and from the guess; a guess
-whose residual is not below ||f|| is replaced by zero (the fallback), so the solver stays
-the judge of every solution.
+whose residual is not below ||f|| is replaced by zero (the fallback), so the solver alone
+decides when a solution is accepted.
 
 Usage: python -m lica_boiling1d_b200.train_guess --steps 3000 --out <weights.npy>
 """
