@@ -163,3 +163,40 @@ def load_checkpoint(path):
         if kind == "film2d":
             return arrays, meta["props"]
     raise ValueError(f"{path}: unknown checkpoint kind {kind!r}")
+
+
+# ------------------------------------------------------------------------------------
+# History records: WRITEHISTORY (1d.f:1235-1254), written every NPIN steps (1d.f:261-265)
+
+
+def _fortran_es(x, w, d):
+    x = float(x)
+    if np.isnan(x):
+        s = "NaN"
+    elif np.isinf(x):
+        s = ("-Infinity" if x < 0 else "Infinity") if w >= 9 else ("-Inf" if x < 0 else "Inf")
+    else:
+        m, e = ("%.*E" % (d, x)).split("E")
+        e = int(e)
+        s = m + ("E%+03d" % e if abs(e) <= 99 else "%+04d" % e)
+    return s.rjust(w) if len(s) <= w else "*" * w
+
+
+def _fortran_f(x, w, d):
+    s = "%.*f" % (d, float(x))
+    return s.rjust(w) if len(s) <= w else "*" * w
+
+
+def history_record(cols, column=0):
+    """The record WRITEHISTORY writes to fort.13 after a step, FORMAT(F13.5,4ES15.7):
+    TIME, DT, CFLM (the step's CFL number), DVMAX (CONVRGE1's largest |div u - source|)
+    and QMMAX, which the reference never assigns (written here as 0)."""
+    from .column import ColumnBatch
+    if isinstance(cols, ColumnBatch):
+        one = cols.column(column)
+        scal, stats = one["scal"], one["stats"]
+    else:
+        host = cols.to(None) if cols.on_device else cols
+        scal, stats = host.arrays["scal"][column], host.arrays["stats"][column]
+    return (_fortran_f(scal[1], 13, 5) + _fortran_es(scal[0], 15, 7) + _fortran_es(stats[0], 15, 7) +
+            _fortran_es(stats[1], 15, 7) + _fortran_es(0.0, 15, 7) + "\n")

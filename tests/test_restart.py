@@ -242,6 +242,19 @@ def test_binary_checkpoints_are_exact(tmp_path):
         R.save_checkpoint(str(tmp_path / "x.npz"), {"w": 1})
 
 
+def test_history_record():
+    """WRITEHISTORY's record (FORMAT(F13.5,4ES15.7)) of the column's last step."""
+    from lica_boiling1d_b200 import restart as R
+    n, props = 64, _props()
+    st = _evolved(n, 0.1, 3, props)
+    rec = R.history_record(_cols(st, n))
+    assert len(rec) == 13 + 4 * 15 + 1 and rec.endswith("\n")
+    f = [rec[:13]] + [rec[13 + 15 * q:28 + 15 * q] for q in range(4)]
+    assert f[0] == "%13.5f" % st["scal"][1]
+    assert float(f[1]) == float("%.7E" % st["scal"][0]) and float(f[2]) == float("%.7E" % st["stats"][0])
+    assert float(f[3]) == float("%.7E" % st["stats"][1]) and f[4] == "  0.0000000E+00"
+
+
 def test_field_names():
     from lica_boiling1d_b200 import native
     from lica_boiling1d_b200 import restart as R
