@@ -269,6 +269,19 @@ int lica_grid_section(int32_t iopt, double xyzi, double xyzf, int32_t ngi, int32
  * and SSDZ of a column are the vvdz / ssdz arguments of lica_gpu_poisson. */
 int lica_grid_metrics(int32_t n, const double* z, double* sdz, double* vdz, double* ssdz, double* vvdz, double* zp);
 
+/* GEOM_COUPLING's z tables (1d.f:5037-5370) between flow faces z[1..n3] (any spacing) and
+ * the uniform level-set faces zf[1..n3f] (z[0], zf[0] unused); ZP and ZPF as GEOMETRIC and
+ * GEOMETRIC_LVS compute them.  KCOU1/KCOU2(K) of flow face K and KCOUMP1/KCOUMP2(K) of flow
+ * centre K are the refined faces (KF-1, KF) that it coincides with (within 1e-10), or
+ * (KF-1, KF-1) with ZF(KF) the first refined face above it; ghosts extrapolated as the
+ * reference does.  Outputs: kcou1, kcou2 [n3+4] for K = -1..n3+2 at [K+1]; kcoump1,
+ * kcoump2 [n3+3] for K = -1..n3+1 at [K+1]; kcou_vel, kcoump_vel [n3f+1] for K = 1..n3f
+ * at [K] (the flow centre at or below ZF(K), ZPF(K)).  The box of flow cell K runs over
+ * refined cells KCOU2(K)..KCOU1(K+1), of face K over KCOUMP2(K-1)..KCOUMP1(K).
+ * LICA_BAD_ARG where the reference prints its coupling problem. */
+int lica_grid_coupling_z(int32_t n3, const double* z, int32_t n3f, const double* zf, int32_t* kcou1, int32_t* kcou2,
+                         int32_t* kcoump1, int32_t* kcoump2, int32_t* kcou_vel, int32_t* kcoump_vel);
+
 /* A pressure system on a wall-normal (y) grid of faces yface[0..ny], stretched, x uniform
  * and periodic: POISSON's operator (1d.f:3535-3541) in 2-D, multiplied by each row's
  * height so that it is symmetric, written as the multigrid's arrays for hy = 1:

@@ -5,8 +5,11 @@
 // solver is built (-fdefault-real-8).  lica_grid_metrics is GEOMETRIC (1d.f:4808-4882) for
 // one wall-bounded direction.  lica_mg_stretched_system writes a pressure system on a
 // wall-normal grid stretched in y in the form the uniform-grid multigrid solves.
+// lica_grid_coupling_z is GEOM_COUPLING's z tables (1d.f:5037-5370) between a flow grid of
+// any spacing and the uniform level-set grid.
 #include <cmath>
 #include <string>
+#include <vector>
 
 #include "lica_gpu.h"
 
@@ -89,6 +92,90 @@ int lica_grid_metrics(int32_t n, const double* z, double* sdz, double* vdz, doub
     for (int k = 1; k <= nm; ++k) zp[k] = z[k] + 0.5 * sdz[k];
     zp[n] = z[n];
     zp[0] = z[1];
+    return LICA_OK;
+}
+
+namespace {
+
+// The first refined face at or above x (GEOM_COUPLING's face search): (KF-1, KF) when
+// ZF(KF) = x within 1e-10, (KF-1, KF-1) when ZF(KF) is the first face above x.
+bool face_pair(double x, int n3f, const double* zf, int32_t& a, int32_t& b) {
+    for (int kf = 1; kf <= n3f; ++kf) {
+        if (std::fabs(zf[kf] - x) <= 1e-10) {
+            a = kf - 1;
+            b = kf;
+            return true;
+        } else if (zf[kf] > x) {
+            a = kf - 1;
+            b = kf - 1;
+            return true;
+        }
+    }
+    return false;
+}
+
+// KCOU_VEL / KCOUMP_VEL: the flow centre at or below zz, by the reference's test order.
+int centre_below(double zz, int n3m, const double* zp) {
+    for (int kk = 1; kk <= n3m; ++kk) {
+        if (std::fabs(zz - zp[kk]) <= 1e-10) return kk;
+        if (zp[1] > zz) return 1;
+        if (zp[kk] > zz) return kk - 1;
+        if (zp[n3m] < zz) return n3m;
+    }
+    return -1;
+}
+
+}  // namespace
+
+int lica_grid_coupling_z(int32_t n3, const double* z, int32_t n3f, const double* zf, int32_t* kcou1, int32_t* kcou2,
+                         int32_t* kcoump1, int32_t* kcoump2, int32_t* kcou_vel, int32_t* kcoump_vel) {
+    if (n3 < 4 || n3f < 3 || !z || !zf || !kcou1 || !kcou2 || !kcoump1 || !kcoump2 || !kcou_vel || !kcoump_vel)
+        return bad("lica_grid_coupling_z", "need n3 >= 4 flow faces, n3f >= 3 refined faces and every array",
+                   __LINE__);
+    const int n3m = n3 - 1;
+    // GEOMETRIC's ZP (1d.f:4873-4876) and GEOMETRIC_LVS's ZPF (1d.f:4928-4938)
+    std::vector<double> zp(n3 + 1), zpf(n3f + 1);
+    for (int k = 1; k <= n3m; ++k) zp[k] = z[k] + 0.5 * (z[k + 1] - z[k]);
+    zp[n3] = z[n3];
+    zp[0] = z[1];
+    const double sdzf = zf[2] - zf[1];
+    for (int k = 1; k <= n3f; ++k) zpf[k] = zf[k] + 0.5 * sdzf;
+    auto K1 = [&](int k) -> int32_t& { return kcou1[k + 1]; };
+    auto K2 = [&](int k) -> int32_t& { return kcou2[k + 1]; };
+    auto M1 = [&](int k) -> int32_t& { return kcoump1[k + 1]; };
+    auto M2 = [&](int k) -> int32_t& { return kcoump2[k + 1]; };
+    // KCOU_VEL / KCOUMP_VEL (1d.f:5142-5190)
+    for (int k = 1; k <= n3f; ++k) {
+        const int a = centre_below(zf[k], n3m, zp.data()), b = centre_below(zpf[k], n3m, zp.data());
+        if (a < 0 || b < 0) return bad("lica_grid_coupling_z", "Z-DIR FLOW_SOLVER->REFINED COUPLING PROBLEM", __LINE__);
+        kcou_vel[k] = a;
+        kcoump_vel[k] = b;
+    }
+    kcou_vel[0] = kcoump_vel[0] = 0;
+    // KCOU1 / KCOU2 of the faces and KCOUMP1 / KCOUMP2 of the centres (1d.f:5308-5363)
+    for (int k = 1; k <= n3; ++k)
+        if (!face_pair(z[k], n3f, zf, K1(k), K2(k)))
+            return bad("lica_grid_coupling_z", "CAL KCOU HAVE PROBLEM: a flow face above the refined grid", __LINE__);
+    K1(0) = K1(1) - (K1(n3m) - K1(n3m - 1));
+    K1(-1) = K1(0) - (K1(n3m - 1) - K1(n3m - 2));
+    K1(n3 + 1) = K1(n3) + (K1(2) - K1(1));
+    K1(n3 + 2) = K1(n3 + 1) + (K1(3) - K1(2));
+    K2(0) = K2(1) - (K2(n3m) - K2(n3m - 1));
+    K2(-1) = K2(0) - (K2(n3m - 1) - K2(n3m - 2));
+    K2(n3 + 1) = K2(n3) + (K2(2) - K2(1));
+    K2(n3 + 2) = K2(n3 + 1) + (K2(3) - K2(2));
+    for (int k = 1; k <= n3m; ++k)
+        if (!face_pair(zp[k], n3f, zf, M1(k), M2(k)))
+            return bad("lica_grid_coupling_z", "CAL KCOUMP HAVE PROBLEM: a flow centre above the refined grid",
+                       __LINE__);
+    M1(0) = M1(1) - (M1(n3m) - M1(n3m - 1));
+    M1(-1) = M1(0) - (M1(n3m - 1) - M1(n3m - 2));
+    M1(n3) = M1(n3m) + (M1(n3m) - M1(n3m - 1));
+    M1(n3 + 1) = M1(n3) + (M1(2) - M1(1));
+    M2(0) = M2(1) - (M2(n3m) - M2(n3m - 1));
+    M2(-1) = M2(0) - (M2(n3m - 1) - M2(n3m - 2));
+    M2(n3) = M2(n3m) + (M2(n3m) - M2(n3m - 1));
+    M2(n3 + 1) = M2(n3) + (M2(2) - M2(1));
     return LICA_OK;
 }
 

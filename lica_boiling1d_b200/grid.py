@@ -140,3 +140,19 @@ def metrics(z):
                                                                                     "zp"))),
                  "lica_grid_metrics")
     return outs
+
+
+def coupling_z(z, zf):
+    """GEOM_COUPLING's z tables (lica_grid_coupling_z) for flow faces z (Z(1)..Z(N3)) and
+    uniform refined faces zf (ZF(1)..ZF(N3F)): dict of int32 arrays kcou1, kcou2 (index K+1,
+    K = -1..N3+2), kcoump1, kcoump2 (K+1, K = -1..N3+1), kcou_vel, kcoump_vel (K = 1..N3F)."""
+    z = np.concatenate([[0.0], np.asarray(z, dtype=np.float64)])
+    zf = np.concatenate([[0.0], np.asarray(zf, dtype=np.float64)])
+    n3, n3f = len(z) - 1, len(zf) - 1
+    out = dict(kcou1=np.zeros(n3 + 4, np.int32), kcou2=np.zeros(n3 + 4, np.int32),
+               kcoump1=np.zeros(n3 + 3, np.int32), kcoump2=np.zeros(n3 + 3, np.int32),
+               kcou_vel=np.zeros(n3f + 1, np.int32), kcoump_vel=np.zeros(n3f + 1, np.int32))
+    I32 = C.POINTER(C.c_int32)
+    native.check(native.lib().lica_grid_coupling_z(n3, _p(z), n3f, _p(zf), *(out[k].ctypes.data_as(I32) for k in (
+        "kcou1", "kcou2", "kcoump1", "kcoump2", "kcou_vel", "kcoump_vel"))), "lica_grid_coupling_z")
+    return out

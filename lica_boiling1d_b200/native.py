@@ -98,6 +98,7 @@ SIGNATURES = {
     "lica_grid_section": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                     _D]),
     "lica_grid_metrics": (C.c_int, [C.c_int32, _D, _D, _D, _D, _D, _D]),
+    "lica_grid_coupling_z": (C.c_int, [C.c_int32, _D, C.c_int32, _D] + [_I32] * 6),
     "lica_mg_stretched_system": (C.c_int, [C.c_int32, C.c_int32, _D, _D, _D, _D, _D, _D, _D]),
     "lica_fld_name": (C.c_int, [C.c_int64, C.c_char_p, C.c_int32]),
     "lica_col_fld_write": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(ColProps), C.POINTER(ColState),

@@ -7,7 +7,9 @@ in double precision (the solver is built with -fdefault-real-8), with the C libr
 tanh and pow through the math module.  Also the stretched wall-normal pressure operator:
 POISSON's AK / CK = VVDZ SSDZ DENF_ZI (1d.f:3535-3541) in 2-D with x uniform and periodic,
 both assembled directly (a sparse matrix, the known answer) and rescaled row by row into
-the uniform multigrid's arrays.
+the uniform multigrid's arrays.  And GEOM_COUPLING's z tables (1d.f:5037-5370) between a
+flow grid of any spacing and the uniform level-set grid, with INTER_PSI's box mean over
+general refined faces.
 
 Parity with grid.f is pinned by the generator's formulas and known answers (end points,
 progression ratios, symmetry); grid.f itself was not run (no Fortran compiler).
@@ -133,3 +135,95 @@ def stretched_operator(yface, bx, by, hx):
             cols.append(r)
             vals.append(diag)
     return sp.csr_matrix((vals, (rows, cols)), shape=(nx * ny, nx * ny))
+
+
+def coupling_z(z, zf):
+    """GEOM_COUPLING's z tables (1d.f:5142-5190, 5308-5363) for flow faces z[0..n3-1] =
+    Z(1..N3) and refined faces zf[0..n3f-1] = ZF(1..N3F); the same layout as the library's."""
+    Z = [0.0] + [float(v) for v in z]
+    ZF = [0.0] + [float(v) for v in zf]
+    n3, n3f = len(Z) - 1, len(ZF) - 1
+    n3m = n3 - 1
+    ZP = [0.0] * (n3 + 1)
+    for k in range(1, n3m + 1):
+        ZP[k] = Z[k] + 0.5 * (Z[k + 1] - Z[k])
+    ZP[n3] = Z[n3]
+    ZP[0] = Z[1]
+    sdzf = ZF[2] - ZF[1]
+    ZPF = [0.0] + [ZF[k] + 0.5 * sdzf for k in range(1, n3f + 1)]
+
+    def centre_below(zz):
+        for kk in range(1, n3m + 1):
+            if abs(zz - ZP[kk]) <= 1e-10:
+                return kk
+            if ZP[1] > zz:
+                return 1
+            if ZP[kk] > zz:
+                return kk - 1
+            if ZP[n3m] < zz:
+                return n3m
+        raise ValueError("Z-DIR FLOW_SOLVER->REFINED COUPLING PROBLEM")
+
+    def pair(x):
+        for kf in range(1, n3f + 1):
+            if abs(ZF[kf] - x) <= 1e-10:
+                return kf - 1, kf
+            if ZF[kf] > x:
+                return kf - 1, kf - 1
+        raise ValueError("CAL KCOU HAVE PROBLEM")
+
+    kv = np.zeros(n3f + 1, np.int32)
+    kmv = np.zeros(n3f + 1, np.int32)
+    for k in range(1, n3f + 1):
+        kv[k] = centre_below(ZF[k])
+        kmv[k] = centre_below(ZPF[k])
+    K1, K2 = {}, {}
+    for k in range(1, n3 + 1):
+        K1[k], K2[k] = pair(Z[k])
+    for T in (K1, K2):
+        T[0] = T[1] - (T[n3m] - T[n3m - 1])
+        T[-1] = T[0] - (T[n3m - 1] - T[n3m - 2])
+        T[n3 + 1] = T[n3] + (T[2] - T[1])
+        T[n3 + 2] = T[n3 + 1] + (T[3] - T[2])
+    M1, M2 = {}, {}
+    for k in range(1, n3m + 1):
+        M1[k], M2[k] = pair(ZP[k])
+    for T in (M1, M2):
+        T[0] = T[1] - (T[n3m] - T[n3m - 1])
+        T[-1] = T[0] - (T[n3m - 1] - T[n3m - 2])
+        T[n3] = T[n3m] + (T[n3m] - T[n3m - 1])
+        T[n3 + 1] = T[n3] + (T[2] - T[1])
+    return dict(kcou1=np.array([K1[k] for k in range(-1, n3 + 3)], np.int32),
+                kcou2=np.array([K2[k] for k in range(-1, n3 + 3)], np.int32),
+                kcoump1=np.array([M1[k] for k in range(-1, n3 + 2)], np.int32),
+                kcoump2=np.array([M2[k] for k in range(-1, n3 + 2)], np.int32), kcou_vel=kv, kcoump_vel=kmv)
+
+
+def box_mean(f, zf, k1, k2, z1, z2):
+    """The z part of INTER_PSI (two_phase.f:5123-5538) over [z1, z2] and refined cells
+    k1..k2 with refined faces zf (zf[k - 1] = ZF(k)) and values f[k] (k = 1..n3f-1): the
+    overlap-weighted mean, by the reference's case analysis, once per (II, JJ) replica."""
+    nf = len(zf) - 1
+    ssdzf = 1.0 / (zf[1] - zf[0])
+    s = 0.0
+    volf = 0.0
+    for _rep in range(4):
+        for kk in range(k1, k2 + 1):
+            v = f[min(max(kk, 1), nf)]
+            za, zb = zf[kk - 1], zf[kk]
+            if za <= z1 and zb >= z2:
+                s = s + v
+                volf = volf + 1.0
+                break
+            elif za < z1 and zb > z1:
+                s = s + v * (zb - z1) * ssdzf
+                volf = volf + (zb - z1) * ssdzf
+            elif za >= z1 and zb <= z2:
+                s = s + v
+                volf = volf + 1.0
+            elif za < z2 and zb > z2:
+                s = s + v * (z2 - za) * ssdzf
+                volf = volf + (z2 - za) * ssdzf
+            elif za >= z2:
+                break
+    return s / volf

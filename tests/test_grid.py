@@ -265,3 +265,69 @@ def test_yline_relaxation_keeps_the_rate_on_anisotropic_cells(gam):
                                     max_cycles=200)
     assert st == 0 and cyc < 50
     assert np.abs(p - x).max() <= 1e-9 * np.abs(x).max()
+
+
+def _coupling_grids(n=48):
+    zf = np.arange(2 * n + 1) / (2.0 * n)
+    return zf, {
+        "uniform": np.arange(n + 1) / float(n),
+        "tanh": OG.section(3, 0.0, 1.0, 1, n + 1, 2.0, 1.0, np.zeros(n + 1)),
+        "geometric": OG.section(2, 0.0, 1.0, 1, n + 1, 1.03, 1.0, np.zeros(n + 1)),
+        # faces on refined faces, 1 to 3 refined cells per flow cell
+        "snapped": np.concatenate([[0.0], np.cumsum(np.resize([1, 2, 3], n))]) / np.cumsum(np.resize([1, 2, 3], n))[-1],
+    }
+
+
+def test_coupling_tables_match_the_oracle():
+    from lica_boiling1d_b200 import grid as G
+    zf, grids = _coupling_grids()
+    for name, z in grids.items():
+        zz = z if name != "snapped" else np.round(z * 96) / 96
+        a, b = G.coupling_z(zz, zf), OG.coupling_z(zz, zf)
+        for k in a:
+            assert np.array_equal(a[k], b[k]), (name, k)
+
+
+def test_coupling_tables_of_the_uniform_column():
+    """The uniform column's closed forms: flow cell K covers refined cells 2K-1..2K, face K's
+    box 2K-2..2K-1, and KCOUMP_VEL(k) is the flow centre at or below the refined centre."""
+    from lica_boiling1d_b200 import grid as G
+    n = 64
+    t = G.coupling_z(np.arange(n + 1) / n, np.arange(2 * n + 1) / (2.0 * n))
+    K = np.arange(1, n + 1)
+    assert np.array_equal(t["kcou2"][K + 1], 2 * K - 1) and np.array_equal(t["kcou1"][K + 2], 2 * K)
+    K = np.arange(2, n + 1)
+    assert np.array_equal(t["kcoump2"][K], 2 * K - 2) and np.array_equal(t["kcoump1"][K + 1], 2 * K - 1)
+    k = np.arange(1, 2 * n + 1)
+    zpf = (k - 0.5) / (2.0 * n)
+    assert np.array_equal(t["kcoump_vel"][1:2 * n + 1], np.clip(np.floor(zpf * n + 0.5), 1, n).astype(np.int32))
+
+
+def test_box_means_over_stretched_flow_cells():
+    """INTER_PSI's box over flow cell K (refined cells KCOU2(K)..KCOU1(K+1)) is the
+    overlap-weighted mean of the refined values, for faces on and off the refined faces,
+    and the flow-cell means conserve the refined field's integral."""
+    from lica_boiling1d_b200 import grid as G
+    zf, grids = _coupling_grids()
+    rng = np.random.default_rng(3)
+    nf = len(zf) - 1
+    f = np.concatenate([[0.0], rng.random(nf)])
+    for name, z in grids.items():
+        if name == "snapped":
+            z = np.round(z * 96) / 96
+        t = G.coupling_z(z, zf)
+        total = 0.0
+        for K in range(1, len(z)):
+            z1, z2 = z[K - 1], z[K]
+            m = OG.box_mean(f, zf, int(t["kcou2"][K + 1]), int(t["kcou1"][K + 2]), z1, z2)
+            ov = np.clip(np.minimum(zf[1:], z2) - np.maximum(zf[:-1], z1), 0.0, None)
+            assert abs(m - (ov * f[1:]).sum() / ov.sum()) <= 1e-13, (name, K)
+            total += m * (z2 - z1)
+        assert abs(total - f[1:].sum() / nf) <= 1e-13, name
+
+
+def test_coupling_rejects_a_flow_grid_beyond_the_level_set():
+    from lica_boiling1d_b200 import native
+    from lica_boiling1d_b200 import grid as G
+    with pytest.raises(native.LicaError):
+        G.coupling_z(np.linspace(0.0, 1.2, 33), np.linspace(0.0, 1.0, 65))
