@@ -31,3 +31,25 @@ def test_library_exports_every_declared_symbol():
 
 def test_python_binding_covers_header():
     assert set(declared_symbols()) == set(native.SIGNATURES), set(declared_symbols()) ^ set(native.SIGNATURES)
+
+
+def test_fortran_module_is_current_and_complete():
+    """include/lica_gpu.f90 is what include/make_fortran_module.py writes from the header
+    (not compiled here: the image has no Fortran compiler), with one bind(c) interface of
+    the right arity per declared entry point."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_fortran_module",
+                                                  os.path.join(ROOT, "include", "make_fortran_module.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    text = gen.generate()
+    assert open(os.path.join(ROOT, "include", "lica_gpu.f90")).read() == text
+    _, _, _, funcs = gen.parse(open(os.path.join(ROOT, "include", "lica_gpu.h")).read())
+    assert sorted(f for f, _, _ in funcs) == declared_symbols()
+    flat = re.sub(r"&\s*\n\s*", "", text)
+    for name, _, params in funcs:
+        m = re.search(r"function %s\(([^)]*)\)\s*bind\(c, name=\"%s\"\)" % (name, name), flat)
+        assert m, name
+        args = [a.strip() for a in m.group(1).split(",") if a.strip()]
+        assert args == [p for p, _ in params], name
+    assert all(len(line) <= 100 for line in text.splitlines())
