@@ -45,3 +45,17 @@ def test_uneven_batch_layout_and_init():
         for k, v in ref.items():
             if k != "stats":
                 assert np.array_equal(got[k], v), (c, k)
+
+
+def test_oracle_column_trajectory_is_pinned():
+    """The oracle's column state after 0, 3 and 6 steps equals the committed golden
+    (tests/golden/make_column_golden.py) bit for bit."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_column_golden as M
+    gold = np.load(os.path.join(os.path.dirname(__file__), "golden", "column_oracle_n64.npz"))
+    for name, z0, kw in M.CASES:
+        got = M.trajectory(z0, kw)
+        for k, v in got.items():
+            assert np.array_equal(v, gold[f"{name}_{k}"]), (name, k)
