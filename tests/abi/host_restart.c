@@ -1,7 +1,8 @@
 /* A compiled host driving the library through include/lica_gpu.h alone, as a Fortran or C
  * solver would: the initial column (MAKEFLD + LVSINIT + GRID_COUPLING), its fld restart file
- * written and read back (WRITEFIELD / PREFLD), and the POISSON metrics of a stretched grid
- * from the generator's sections (grid.f, GEOMETRIC).  Host entry points only: no GPU.
+ * written and read back (WRITEFIELD / PREFLD), the POISSON metrics of a stretched grid from
+ * the generator's sections (grid.f, GEOMETRIC), its coupling tables to the level-set grid
+ * (GEOM_COUPLING) and its 2-D pressure system for the multigrid.  Host entry points only: no GPU.
  * Usage: host_restart <directory>.  Prints "ok" and exits 0, or names the failed check. */
 #include <math.h>
 #include <stdio.h>
@@ -80,6 +81,21 @@ int main(int argc, char** argv) {
     for (int k = 1; k <= 64; ++k) total += sdz[k];
     if (fabs(total - 1.0) > 1e-14 || !(sdz[1] < sdz[64]) || vdz[1] != 0.5 * sdz[1] || vdz[65] != 0.5 * sdz[64])
         return fail("stretched metrics");
+    /* GEOM_COUPLING's tables of that grid against a uniform 129-face level-set grid */
+    double zf[130];
+    for (int k = 1; k <= 129; ++k) zf[k] = (k - 1) / 128.0;
+    int32_t kc1[69], kc2[69], km1[68], km2[68], kv[130], kmv[130];
+    if (lica_grid_coupling_z(65, z, 129, zf, kc1, kc2, km1, km2, kv, kmv) != LICA_OK) return fail("coupling tables");
+    for (int k = 1; k <= 64; ++k)
+        if (kc2[k + 1] > kc1[k + 2] + 1 || zf[kc2[k + 1]] > z[k] + 1e-12 || zf[kc1[k + 2] + 1] < z[k + 1] - 1e-12)
+            return fail("flow cell boxes cover their cells");
+    /* the stretched pressure system of a 32 x 64 field on those faces */
+    static double bx[64 * 32], by[65 * 32], f[64 * 32], bxo[64 * 32], byo[65 * 32], fo[64 * 32];
+    for (int q = 0; q < 64 * 32; ++q) bx[q] = f[q] = 1.0;
+    for (int q = 0; q < 65 * 32; ++q) by[q] = 1.0;
+    if (lica_mg_stretched_system(32, 64, z + 1, bx, by, f, bxo, byo, fo) != LICA_OK) return fail("stretched system");
+    if (fabs(fo[0] - sdz[1]) > 1e-15 || fabs(byo[64 * 32] - 1.0 / sdz[64]) > 1e-9 * byo[64 * 32])
+        return fail("stretched system values");
     printf("ok\n");
     return 0;
 }
