@@ -47,7 +47,7 @@ def test_es_and_i_edit_descriptors():
     assert F.format_i(123456789) == "********"
 
 
-def test_library_formats_like_the_oracle():
+def test_library_formats_like_the_oracle(tmp_path):
     """Values of every exponent range, signed zeros and non-finite values through the
     library's writer: the W records equal the oracle's ES20.12 text."""
     from lica_boiling1d_b200 import restart as R
@@ -57,13 +57,8 @@ def test_library_formats_like_the_oracle():
     vals = [1.0, -2.5e-3, 0.0, -0.0, 1e-300, -1.5e200, 5e-324, 1.7976931348623157e308, 0.1, 1 / 3, -2 / 3,
             9.9999999999995e-5, 12345.678901234567, float("nan"), float("inf"), -1e100, 1e99]
     st["w"][1:1 + len(vals)] = vals
-    path = R.write_field(_cols(st, n), os.path.join(os.environ.get("TMPDIR", "/tmp"), f"fldfmt{os.getpid()}"),
-                         props)
-    try:
-        text = open(path).read()
-    finally:
-        os.remove(path)
-    assert text == F.write_column(st, n, props, dict(R.DEFAULT_INFO))
+    path = R.write_field(_cols(st, n), str(tmp_path / "fldfmt"), props)
+    assert open(path).read() == F.write_column(st, n, props, dict(R.DEFAULT_INFO))
 
 
 @pytest.mark.parametrize("n,z0,steps", [(16, 0.3, 0), (32, 0.2, 5), (128, 0.1, 12), (256, 0.0607, 3)])
