@@ -314,7 +314,8 @@ typedef struct {
 
 /* lica.in switches applied after a read. */
 typedef struct {
-    int32_t ireset; /* IRESET = 1: TIME starts from 0 (1d.f:175-178) */
+    int32_t ireset; /* IRESET = 1: TIME starts from 0 in the state (1d.f:175-178); the run's
+                       IHIST, the caller's counter, restarts from 0 too (info keeps the file's) */
     int32_t idtold; /* IDTOLD = 1: DT = the file's DT_O, else props->dt0 (1d.f:1080-1085) */
     int32_t ipzero; /* IPZERO = 1: P = 0 after the read (1d.f:1055) */
 } lica_fld_options;
