@@ -105,7 +105,7 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ CPU legs (oracle)
-def cpu_solves(case, max_seconds, max_solves):
+def cpu_solves(case, max_seconds, max_solves, mixed=False):
     """Time the CPU restatement of the same solve (OpenMP on all host cores)."""
     from oracle import oracle
     oracle.lib(native=True)
@@ -114,12 +114,21 @@ def cpu_solves(case, max_seconds, max_solves):
     while len(times) < max_solves:
         t0 = time.perf_counter()
         _, it, rel, _, st = oracle.mg_solve(case.f, case.bx, case.by, case.hx, case.hy, nlevels=NLEVELS, ncoarse=1,
-                                           sym=5, method="pcg", rtol=RTOL, max_cycles=200, native=True)
+                                           sym=5, method="pcg", mixed=mixed, rtol=RTOL, max_cycles=200, native=True)
         times.append(time.perf_counter() - t0)
         its.append(it)
         if time.perf_counter() - t_all > max_seconds:
             break
     return times, its
+
+
+def bench_config(n, nlevels, ncoarse, precision, world):
+    """The workload's config dict, the same in both arms."""
+    workload = WORKLOAD if n == N else WORKLOAD.replace("1024x1024", f"{n}x{n}").replace(
+        "6-level", f"{nlevels}-level")
+    return {"workload": workload, "nx": n, "ny": n, "nlevels": nlevels, "nu1": 2, "nu2": 2, "ncoarse": ncoarse,
+            "rtol": RTOL, "solver": "MG-PCG", "precision": precision, "l2_flush": "256 MiB write between steps",
+            "parallelism": f"replicas x{world}"}
 
 
 def run_reference(args):
@@ -130,54 +139,66 @@ def run_reference(args):
     threads = os.cpu_count()
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
     case = bubble_poisson_case(N)
-    cpu_solves(case, 1e9, max(1, args.warmup))  # warm-up (also builds the native oracle)
-    times, its = cpu_solves(case, 1e9, args.steps)
+    mixed = args.precision == "mixed"
+    cpu_solves(case, 1e9, max(1, args.warmup), mixed)  # warm-up (also builds the native oracle)
+    times, its = cpu_solves(case, 1e9, args.steps, mixed)
     total = sum(times)
     value = len(times) / total
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": len(times), "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "nx": N, "ny": N, "nlevels": NLEVELS, "rtol": RTOL, "solver": "MG-PCG",
-                   "parallelism": "host threads"},
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f64+f32", "data": "synthetic",
+        "config": bench_config(N, NLEVELS, args.ncoarse, args.precision, args.gpus),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
                          "sample": f"{len(times)} complete solves (one per step), FP64 C++/OpenMP restatement"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "iterations": its[-1],
     }
-    line["rk3"] = {"cpu_baseline": rk3_cpu()}
+    line["rk3"] = {"cpu_baseline": rk3_cpu()[0]}
     print(json.dumps(line), flush=True)
 
 
 # ------------------------------------------------------------------ RK3 column legs
-C1 = dict(n=512, z0=0.1, denr=1000.0, visr=20.0, tcr=25.0, jakob=0.009)
+C1 = dict(n=512, z0=0.1, denr=1000.0, visr=20.0, tcr=25.0, jakob=0.009, cflmax=0.3, steps=2000)
 C4_NCOL = 4096
 
 
 def c1_props():
     from lica_boiling1d_b200.column import ColumnProps
-    return ColumnProps(denr=C1["denr"], visr=C1["visr"], tcr=C1["tcr"], jakob=C1["jakob"])
+    return ColumnProps(denr=C1["denr"], visr=C1["visr"], tcr=C1["tcr"], jakob=C1["jakob"], cflmax=C1["cflmax"])
 
 
-def rk3_cpu(max_seconds=12.0):
-    """The CPU restatement's time for the same steps: one column of the 512-cell workload
-    (single thread, as the reference's 1-D case runs), and a sample of the uneven batch run
-    over all host cores (independent columns; the oracle releases the GIL)."""
+def c1_oracle(steps):
+    """Config 1 on the CPU restatement, one thread (as the reference's 1-D case runs): the
+    final state, the per-step interface history (TIME, place, VOL_TOT_IPHS, DT) and the
+    seconds the steps took."""
+    from oracle import oracle
+    props = c1_props()
+    st = oracle.col_init(C1["n"], 1.0, C1["z0"], props)
+    hist = np.zeros((steps, 4))
+    t0 = time.perf_counter()
+    for s in range(steps):
+        tb = float(st["scal"][1])
+        if oracle.col_step(st, C1["n"], 1.0, props, native=True) != 0:
+            raise RuntimeError(f"oracle column step {s + 1} failed")
+        hist[s] = oracle.col_history_record(st, tb, native=True)
+    return st, hist, time.perf_counter() - t0
+
+
+def rk3_cpu(c1_steps=C1["steps"]):
+    """The CPU restatement's time for the same steps: the whole config-1 run of the 512-cell
+    column (single thread), and a sample of the uneven batch run over all host cores
+    (independent columns; the oracle releases the GIL).  Returns the figures and, apart,
+    the config-1 final state and history."""
     from concurrent.futures import ThreadPoolExecutor
 
     from lica_boiling1d_b200.column import uneven_batch
     from oracle import oracle
     oracle.lib(native=True)
-    props = c1_props()
-    st = oracle.col_init(C1["n"], 1.0, C1["z0"], props)
-    for _ in range(3):
-        oracle.col_step(st, C1["n"], 1.0, props, native=True)
-    t0 = time.perf_counter()
-    k = 0
-    while time.perf_counter() - t0 < max_seconds / 2 and k < 400:
-        oracle.col_step(st, C1["n"], 1.0, props, native=True)
-        k += 1
-    c1 = k / (time.perf_counter() - t0)
+    c1_state, c1_hist, c1_s = c1_oracle(c1_steps)
+    c1 = c1_steps / c1_s
+    k = c1_steps
     n, length, z0, bprops = uneven_batch(C4_NCOL, seed=0)
     sample = list(range(0, C4_NCOL, max(1, C4_NCOL // 256)))
     states = {c: oracle.col_init(int(n[c]), float(length[c]), float(z0[c]), bprops[c]) for c in sample}
@@ -194,10 +215,10 @@ def rk3_cpu(max_seconds=12.0):
         dt = time.perf_counter() - t0
     cells = float(np.mean([n[c] for c in sample]))
     col_steps = done / dt
-    return {"c1_steps_per_s": c1, "c1_sample": f"{k} steps of the 512-cell column, one thread",
+    return {"c1_steps_per_s": c1, "c1_sample": f"all {k} steps of config 1 (512-cell column, CFL 0.3), one thread",
             "batch_column_steps_per_s": col_steps, "batch_steps_per_s": col_steps / C4_NCOL,
             "batch_cell_updates_per_s": col_steps * cells, "cores": cores,
-            "batch_sample": f"{len(sample)} of the {C4_NCOL} columns x 2 steps on {cores} threads"}
+            "batch_sample": f"{len(sample)} of the {C4_NCOL} columns x 2 steps on {cores} threads"}, (c1_state, c1_hist)
 
 
 def profile_batch(ncol, steps, threads):
@@ -221,37 +242,46 @@ def profile_batch(ncol, steps, threads):
                       "cells": int(n.sum()), "status": int(st.max())}), flush=True)
 
 
-def rk3_legs(dev, flush, steps_c1=200, steps_c4=20, warmup=3, rank=0, world=1, slowest=lambda x: x, film_steps=10,
-             film_compare=False):
+def rk3_legs(dev, flush, steps_c1=C1["steps"], steps_c4=1000, warmup=3, rank=0, world=1, slowest=lambda x: x,
+             film_steps=10, film_compare=False):
     import torch
 
+    from lica_boiling1d_b200 import column as colmod
     from lica_boiling1d_b200 import native, shard
     from lica_boiling1d_b200.column import ColumnBatch, Columns, uneven_batch
     out = {}
     props = c1_props()
-    # C1: one column, one persistent launch of steps_c1 steps
-    col = Columns.film(C1["n"], 1.0, [C1["z0"]], props).to(dev)
-    col.steps(warmup, props, threads=256)
+    # C1: one column from its initial state, one persistent launch of steps_c1 steps that
+    # records the interface history (warm-up on a separate copy)
+    col0 = Columns.film(C1["n"], 1.0, [C1["z0"]], props)
+    warm = col0.to(dev)
+    warm.steps(warmup, props, threads=256)
+    col = col0.to(dev)
+    hist = torch.zeros((1, steps_c1, 4), dtype=torch.float64, device=dev)
     torch.cuda.synchronize(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     flush.fill_(3)
     l0 = native.launch_count()
+    colmod.history(hist)
     e0.record()
     st = col.steps(steps_c1, props, threads=256)
     e1.record()
     torch.cuda.synchronize(dev)
+    colmod.history(None)
     launches = native.launch_count() - l0
     if int(st.max()) != 0:
         raise RuntimeError(f"column step status {int(st.max())}")
     ms = e0.elapsed_time(e1)
     out["column_512"] = {
-        "workload": "1-D boiling column, 512 flow cells (1024 refined), film 0.1 L, density ratio 1000, viscosity "
-                    "ratio 20, conductivity ratio 25, Jakob 0.009 (10 K), CFL 0.5, FP64, one persistent launch",
+        "workload": "config 1: 1-D boiling column, 512 uniform flow cells (1024 refined), film 0.1 L, density ratio "
+                    "1000, viscosity ratio 20, conductivity ratio 25, Jakob 0.009 (10 K), RK3 at CFL 0.3, "
+                    f"{steps_c1} steps from the initial state in one persistent launch, FP64, 1-D POISSON exact",
         "steps_per_s": steps_c1 / (ms / 1e3), "ms_per_step": ms / steps_c1, "steps": steps_c1, "threads": 256,
         "cell_updates_per_s": C1["n"] * steps_c1 / (ms / 1e3), "gpu_launches": launches,
         "interface_height": float(col.to(None).stats[0][5])}
+    out["_c1_gpu"] = (col.to(None), hist[0].cpu().numpy())
     # end to end: the host-array C-ABI entry, one step per call (state copied in and out)
-    host = col.to(None)
+    host = warm.to(None)
     pinned = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in host.arrays.items()}
     hcol = Columns(C1["n"], 1.0, pinned)
     ke = 20
@@ -301,9 +331,9 @@ def rk3_legs(dev, flush, steps_c1=200, steps_c4=20, warmup=3, rank=0, world=1, s
     hist = shard.gather_histories([(lo + c, float(fin["stats"][c][5]), float(fin["scal"][c][4]))
                                    for c in range(len(n))], world)
     out["batch_4096"] = {
-        "workload": f"{C4_NCOL} independent 1-D boiling columns, uneven 128-2048 flow cells (seeded, {cells} in "
-                    "total), superheat 2-20 K, density ratio 100-1600, FP64, one persistent launch per rank, "
-                    "longest first",
+        "workload": f"config 4: {C4_NCOL} independent 1-D boiling columns, uneven 128-2048 flow cells (seeded, "
+                    f"{cells} in total), superheat 2-20 K, density ratio 100-1600, FP64 (the 1-D pressure solve is "
+                    f"the exact Thomas sweep), {steps_c4} RK3 steps in one persistent launch per rank, longest first",
         "steps_per_s": steps_c4 / (ms / 1e3), "ms_per_step": ms / steps_c4, "steps": steps_c4,
         "column_steps_per_s": C4_NCOL * steps_c4 / (ms / 1e3), "cell_updates_per_s": cells * steps_c4 / (ms / 1e3),
         "threads": th, "autotune_ms_per_step": trial, "gpu_launches": launches,
@@ -474,9 +504,20 @@ def run_ours(args):
         rk3 = rk3_legs(dev, flush, steps_c1=args.c1_steps, steps_c4=args.c4_steps, rank=rank, world=world,
                        slowest=slowest, film_steps=args.film_steps,
                        film_compare=(rank == 0 and world == 1 and not args.skip_cpu))
+        c1_gpu_state, c1_gpu_hist = rk3.pop("_c1_gpu")
         if rank == 0 and world == 1 and not args.skip_cpu:
-            rk3["cpu_baseline"] = rk3_cpu()
+            rk3["cpu_baseline"], (c1_ref, c1_ref_hist) = rk3_cpu(args.c1_steps)
             rk3["cpu_baseline"]["kind"] = "port"
+            same = {k: bool(np.array_equal(c1_gpu_state.arrays[k][0], v)) for k, v in c1_ref.items()}
+            rk3["column_512"]["vs_oracle"] = {
+                "history_steps_compared": int(c1_ref_hist.shape[0]),
+                "history_bit_identical": bool(np.array_equal(c1_gpu_hist, c1_ref_hist)),
+                "history_max_abs_diff": {name: float(np.abs(c1_gpu_hist[:, q] - c1_ref_hist[:, q]).max())
+                                         for q, name in enumerate(("time", "place", "vapour_volume", "dt"))},
+                "final_state_bit_identical": all(same.values()),
+                "final_interface_place": float(c1_ref_hist[-1, 1]),
+                "final_vapour_volume": float(c1_ref_hist[-1, 2]),
+                "note": "interface history = the reference's 0interface.dat (TIME, place) and VOL_TOT_IPHS per step"}
     if args.no_e2e:
         return finish(args, locals())
     # end-to-end through the host C-ABI entry: H2D of p0, f, bx, by; solve; D2H of p
@@ -755,17 +796,12 @@ def finish(args, v):
     import torch.distributed as dist
     if v["rank"] == 0:
         n = v["n"]
-        workload = WORKLOAD if n == N else WORKLOAD.replace("1024x1024", f"{n}x{n}").replace(
-            "6-level", f"{v['nlevels']}-level")
         line = {
             "metric": METRIC, "value": v["value"], "unit": UNIT, "n_gpus": v["world"], "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": v["total_ms"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32",
             "data": "synthetic",
-            "config": {"workload": workload, "nx": n, "ny": n, "nlevels": v["nlevels"], "nu1": 2, "nu2": 2,
-                       "ncoarse": args.ncoarse,
-                       "rtol": RTOL, "solver": "MG-PCG", "precision": args.precision,
-                       "l2_flush": "256 MiB write between steps", "parallelism": f"replicas x{v['world']}"},
+            "config": bench_config(n, v["nlevels"], args.ncoarse, args.precision, v["world"]),
             "iterations": v["its"][-1], "rel_residual": v["rel"],
             "roofline": v["roofline"], "cpu_baseline": v["cpu"], "e2e": v["e2e"], "gpu_launches": int(v["launches"]),
             "clocks": v["clk"], "variants": v["variants"], "rk3": v.get("rk3"),
@@ -794,8 +830,8 @@ def main():
     ap.add_argument("--skip-2048", action="store_true", help="skip the 2048x2048 solves")
     ap.add_argument("--profile-guess", type=int, default=0,
                     help="only run this many U-Net guesses at 1024x1024 (profiling) and exit")
-    ap.add_argument("--c1-steps", type=int, default=200, help="timed steps of the 512-cell column")
-    ap.add_argument("--c4-steps", type=int, default=20, help="timed steps of the 4096-column batch")
+    ap.add_argument("--c1-steps", type=int, default=C1["steps"], help="timed steps of the 512-cell column")
+    ap.add_argument("--c4-steps", type=int, default=1000, help="timed steps of the 4096-column batch")
     ap.add_argument("--film-steps", type=int, default=10, help="timed steps of the 2-D film (0: skip the leg)")
     ap.add_argument("--profile-film", type=int, default=0, help="run N 2-D film steps only (ncu launch lists)")
     ap.add_argument("--profile-batch", type=int, default=0,

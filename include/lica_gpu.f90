@@ -488,6 +488,13 @@ module lica_gpu
       type(c_ptr), value :: prof
     end function lica_gpu_column_profile_device
 
+    integer(c_int) function lica_gpu_column_history_device(hist, capacity) &
+        bind(c, name="lica_gpu_column_history_device")
+      import
+      type(c_ptr), value :: hist
+      integer(c_int32_t), value :: capacity
+    end function lica_gpu_column_history_device
+
     integer(c_int) function lica_gpu_column_batch_create(out, ncol, n, length, props) &
         bind(c, name="lica_gpu_column_batch_create")
       import

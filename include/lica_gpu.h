@@ -76,7 +76,9 @@ int lica_gpu_trdiag3p_device(const double* A, const double* B, const double* C, 
  * kernel and bit-identical results as lica_gpu_trdiag3_device; its scratch is a fixed
  * 2 MiB device array inside this library, so ld * l2 must not exceed 262144 (else
  * LICA_BAD_ARG).  The first call on a device sets up the scratch address and should be
- * made before any stream capture.  Enqueues on `stream` and returns without waiting.
+ * made before any stream capture; the address is kept for the life of the process, so do
+ * not use this entry point on a device after cudaDeviceReset.  Enqueues on `stream` and
+ * returns without waiting.
  * Calls that overlap on the GPU share the scratch and race: serialise them (one stream
  * per device). */
 int lica_gpu_trdiag3_noalloc_device(const double* A, const double* B, const double* C, double* R, double* UU,
@@ -358,6 +360,16 @@ int lica_gpu_column_steps_device(int32_t ncol, int32_t n, double length, const l
  * TEMP_EXTP, 4 TEMP_EXTP, 5 CAL_CONTINUITY2 + CAL_CONT_BC, 6 RHSZ, 7 LHSW, 8 BC + FSM_CHOI +
  * PRESSURE_CORRECTION, 9 CONVRGE1, 10 TRANSPORT + GRID_COUPLING.  NULL turns it off. */
 int lica_gpu_column_profile_device(int64_t* prof);
+
+/* Interface history of the step kernels (the reference's per-step record of 0interface.dat,
+ * chphase.f:1419-1438, and VOL_TOT_IPHS, chphase.f:1457): while hist (device, 4 * capacity
+ * doubles per column) is set, every launch of lica_gpu_column_steps_device /
+ * lica_gpu_column_batch_steps_device writes for step s < capacity of column c, at
+ * hist[4 (c capacity + s) ..]: TIME before the step (the value the reference writes), the
+ * interface position `place` of VOL_TOT_MFDOT in the third substep (zpf(k) + |phi(k)| at
+ * the last sign change of the trial level set; 0 in a step without phase change), the
+ * vapour volume VOL_TOT_IPHS and DT.  NULL turns it off. */
+int lica_gpu_column_history_device(double* hist, int32_t capacity);
 
 /* Batches of columns of uneven size, length and properties (one opaque handle per batch
  * layout).  Column c has n[c] flow cells over length[c] with props[c]; its arrays are packed

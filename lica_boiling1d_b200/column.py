@@ -147,6 +147,23 @@ def profile(prof):
                  "column profile")
 
 
+HISTORY = ("time", "place", "vapour_volume", "dt")
+
+
+def history(hist):
+    """Record the reference's per-step interface history (0interface.dat's TIME and place,
+    chphase.f:1419-1438; VOL_TOT_IPHS, chphase.f:1457; and DT) of later step launches into
+    hist, a float64 CUDA tensor of shape (ncol, capacity, 4): step s of a launch goes to
+    hist[c, s].  None turns it off."""
+    if hist is None:
+        rc = native.lib().lica_gpu_column_history_device(None, 0)
+    else:
+        if hist.dim() != 3 or hist.shape[2] != len(HISTORY) or not hist.is_contiguous():
+            raise ValueError("hist: need a contiguous (ncol, capacity, 4) tensor")
+        rc = native.lib().lica_gpu_column_history_device(C.c_void_p(hist.data_ptr()), int(hist.shape[1]))
+    native.check(rc, "column history")
+
+
 _FLOW = ("w", "p", "t", "psi_cn", "psi_zn", "wo", "imask")
 _PHI = ("phi", "layer", "mflvs")
 _PSIF = ("psif", "sfgas", "sfgas2")

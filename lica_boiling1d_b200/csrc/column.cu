@@ -72,9 +72,14 @@ struct Args {
     double* dscr;
     int* iscr;
     long long* prof;   // optional per-phase cycle totals (PH_COUNT per column) or null
+    double* hist;      // optional interface history (HIST_REC doubles per column and step) or null
+    int hist_cap;      // steps of one launch the history holds per column
     int tri_smem;      // 1: the tridiagonal arrays of columns with n <= tri_cap live in dynamic shared memory
     int tri_cap;       // longest column whose arrays fit the dynamic shared memory (longer ones use scratch)
 };
+
+// one record of the optional interface history: TIME before the step, place, VOL_TOT_IPHS, DT
+constexpr int HIST_REC = 4;
 
 // phases of the optional cycle profile
 enum { PH_DT, PH_CONT, PH_ENERGY, PH_TEMPGRAD, PH_EXTP, PH_CONT2, PH_RHSZ, PH_LHSW, PH_PRESS, PH_CONV, PH_TRANSPORT,
@@ -927,6 +932,21 @@ __device__ int temp_grad(const Geo& g, const Phys& ph, Col& c, Shared& sh, doubl
             }
             __syncwarp();
             lvs::reinitialization(cx, lvs::NN2);
+            {
+                // the interface position of 0interface.dat (chphase.f:1419-1431): zpf(k) +
+                // |phi(k)| of the last sign change over k = 1..N3FM of the trial phi (0 off
+                // the band; phi(nf+1) is ALPHI_BC's ghost)
+                int kb = 0;
+                for (int i = lane; i < lvs::WIN; i += 32) {
+                    const int k = cx.w0 + i;
+                    if (k < 1 || k > nf) continue;
+                    const double a = s->phi[i];
+                    const double b = (i + 1 < lvs::WIN) ? s->phi[i + 1] : (k == nf ? s->ghost[3] : 0.0);
+                    if (a * b < 0.0) kb = k;
+                }
+                for (int o = 16; o > 0; o >>= 1) kb = max(kb, __shfl_xor_sync(0xffffffffu, kb, o));
+                if (lane == 0) sh.dbuf[5] = (kb > 0) ? g.zpf(kb) + fabs(s->phi[kb - cx.w0]) : 0.0;
+            }
             for (int i = cx.blo + lane; i <= cx.bhi; i += 32) {
                 const int m = s->layer[i];
                 s->nv[i] = (m >= 1 && m <= lvs::NN1) ? lvs::psif_band(s, i) : 0.0;
@@ -1339,7 +1359,23 @@ __global__ void __launch_bounds__(NTH, NTH == 64 ? 5 : 1) k_column_steps(const _
     c.t0 = clock64();
     const Geo g(n, L);
     int st = LICA_OK;
-    for (int s = 0; s < A.nsteps && st == LICA_OK; ++s) st = column_step(g, ph, c, sh, L);
+    double* hist = A.hist ? A.hist + (size_t)col * A.hist_cap * HIST_REC : nullptr;
+    for (int s = 0; s < A.nsteps && st == LICA_OK; ++s) {
+        // thread 0 alone writes and reads sh.dbuf[5] (place) and the history record
+        double time0 = 0.0;
+        if (threadIdx.x == 0) {
+            sh.dbuf[5] = 0.0;
+            time0 = c.scal[1];
+        }
+        st = column_step(g, ph, c, sh, L);
+        if (hist && s < A.hist_cap && threadIdx.x == 0 && st == LICA_OK) {
+            double* r = hist + (size_t)s * HIST_REC;
+            r[0] = time0;
+            r[1] = sh.dbuf[5];
+            r[2] = c.scal[4];
+            r[3] = c.scal[0];
+        }
+    }
     if (threadIdx.x == 0) A.status[col] = st;
 }
 
@@ -1393,6 +1429,9 @@ ScratchCache& scratch_cache() {
 
 // per-phase cycle profile target (device array of COLUMN_PHASES * ncol int64) or null
 long long* g_col_prof = nullptr;
+// interface history target (device array of 4 * capacity doubles per column) or null
+double* g_col_hist = nullptr;
+int g_col_hist_cap = 0;
 
 
 // Host-side initial state (runs once, before the time loop).
@@ -1543,6 +1582,13 @@ int lica_gpu_column_init(int32_t n, double length, double z0, const lica_col_pro
     return LICA_OK;
 }
 
+int lica_gpu_column_history_device(double* hist, int32_t capacity) {
+    if (hist && capacity < 1) return LICA_BAD_ARG;
+    g_col_hist = hist;
+    g_col_hist_cap = hist ? capacity : 0;
+    return LICA_OK;
+}
+
 int lica_gpu_column_profile_device(int64_t* prof) {
     g_col_prof = (long long*)prof;
     return LICA_OK;
@@ -1675,6 +1721,8 @@ int lica_gpu_column_steps_device(int32_t ncol, int32_t n, double length, const l
     fill_state(A, st);
     A.status = status;
     A.prof = g_col_prof;
+    A.hist = g_col_hist;
+    A.hist_cap = g_col_hist_cap;
     void* scr = scratch;
     if (!scr) {
         const int rc = column_scratch(lica_gpu_column_scratch_bytes(ncol, n), &scr);
@@ -1781,6 +1829,8 @@ int lica_gpu_column_batch_steps_device(const lica_col_batch* b, const lica_col_s
     fill_state(A, st);
     A.status = status;
     A.prof = g_col_prof;
+    A.hist = g_col_hist;
+    A.hist_cap = g_col_hist_cap;
     void* scr = scratch;
     if (!scr) {
         const int rc = column_scratch((size_t)(b->tot[3] * sizeof(double) + b->tot[4] * sizeof(int) + 256), &scr);

@@ -216,7 +216,9 @@ int lica_gpu_trdiag3p_device(const double* A, const double* B, const double* C, 
 // lica_gpu_trdiag3_device, with the forward-sweep coefficients kept in the fixed scratch
 // array above instead of cudaMalloc'd memory.  The first call on a device looks up the
 // scratch address (cudaGetSymbolAddress) and should come before any stream capture.
-// Returns after enqueueing the kernel on `stream` (no synchronisation).  Calls that
+// The address is kept per device ordinal for the life of the process: do not call this
+// entry point again on a device after cudaDeviceReset (the module may be reloaded at
+// another address).  Returns after enqueueing the kernel on `stream` (no synchronisation).  Calls that
 // overlap on the GPU (different streams, or different host threads on one device) share
 // the scratch and race.  The scratch needs no clearing: each line writes every
 // coefficient before it reads it.
@@ -230,7 +232,10 @@ int lica_gpu_trdiag3_noalloc_device(const double* A, const double* B, const doub
     }
     int dev = -1;
     LICA_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return LICA_BAD_ARG;
+    if (dev < 0 || dev >= kMaxDevices) {
+        lica_set_last_error("lica_gpu_trdiag3_noalloc_device", "device ordinal outside 0..127", __FILE__, __LINE__);
+        return LICA_BAD_ARG;
+    }
     double* gam = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_noalloc_mu);

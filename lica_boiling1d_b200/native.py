@@ -108,6 +108,7 @@ SIGNATURES = {
                                     C.POINTER(ColState), C.POINTER(FldInfo)]),
     "lica_gpu_column_scratch_bytes": (C.c_size_t, [C.c_int32, C.c_int32]),
     "lica_gpu_column_profile_device": (C.c_int, [C.c_void_p]),
+    "lica_gpu_column_history_device": (C.c_int, [C.c_void_p, C.c_int32]),
     "lica_gpu_column_steps_device": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.POINTER(ColProps),
                                                C.POINTER(ColState), C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
                                                C.c_void_p]),

@@ -32,6 +32,9 @@ extern "C" int orc_lvs_init(int n, double L, double z0, double* phi, int* layer,
 
 namespace {
 
+// place of the latest VOL_TOT_MFDOT on this thread (0 until one runs in a step)
+thread_local double g_place = 0.0;
+
 // lica.in inputs of the two-phase / heat block (INPUT_SIMULATION 1d.f:346-379).
 struct ColProps {
     double re, visr, denr, weber, fr, prm, scr, tcr, t_sat, jakob, cflmax, dt0;
@@ -603,6 +606,12 @@ int temp_grad(const Geo& g, double L, const Phys& ph, const ColView& s, double d
                 t.p(k) = a;
             }
         reinitialization(t, NN2);
+        // the interface position the reference prints and appends to 0interface.dat
+        // (chphase.f:1419-1431): zpf(k) + |phi(k)| of the last sign change of the trial
+        // band phi over k = 1..N3FM (phi outside the band is 0 here, so it makes none)
+        g_place = 0.0;
+        for (int k = 1; k <= nf; ++k)
+            if (t.p(k) * t.p(k + 1) < 0.0) g_place = g.zpf(k) + std::fabs(t.p(k));
         std::vector<double> psif_mtp2 = cal_psif_mtp(t, 1);
         const double dvol = 0.5 * 0.5 * g.hf;
         double vol = 0.0;
@@ -954,6 +963,7 @@ int orc_col_step(int n, double L, const double* props, const int* iprops, double
     Geo g(n, L);
     ColView s = view(n, L, w, p, t, psi_cn, psi_zn, phi, layer, psif, wo, mflvs, sfgas, sfgas2, imask, scal);
     Work wk(n);
+    g_place = 0.0;
     scal[2] = scal[2] + 1.0;
     const int m_step = (int)scal[2];
     if (m_step == 1)
@@ -997,5 +1007,11 @@ int orc_col_step(int n, double L, const double* props, const int* iprops, double
     stats[7] = scal[0];
     return 0;
 }
+
+// The record the reference appends to 0interface.dat at the end of the last substep of a
+// step (chphase.f:1432-1438, TIME before MAIN adds DT at 1d.f:260) for the step just taken
+// by orc_col_step on this thread: place of VOL_TOT_MFDOT in the third substep (0 when the
+// step ran no phase change).
+double orc_col_last_place() { return g_place; }
 
 }  // extern "C"

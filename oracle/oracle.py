@@ -40,6 +40,8 @@ def lib(native: bool = False):
             [_INT, _D]
         L.orc_col_resume.argtypes = [C.c_int, C.c_double, _D, _INT, _D, _D, _D]
         L.orc_col_step.argtypes = [C.c_int, C.c_double, _D, _INT] + [_D] * 6 + [_INT] + [_D] * 5 + [_INT, _D, _D]
+        L.orc_col_last_place.restype = C.c_double
+        L.orc_col_last_place.argtypes = []
         _LIBS[key] = L
     return _LIBS[key]
 
@@ -238,3 +240,10 @@ def col_step(st, n, length, props, native=False):
     2 band overflow)."""
     pr, ip = _col_props(props)
     return lib(native).orc_col_step(n, length, _p(pr), _pi(ip), *_col_args(st), _p(st["stats"]))
+
+
+def col_history_record(st, time_before, native=False):
+    """The reference's per-step interface record for the step col_step just took on this
+    thread: (TIME before the step, place of 0interface.dat (chphase.f:1419-1438), the vapour
+    volume VOL_TOT_IPHS (chphase.f:1457), DT)."""
+    return (time_before, lib(native).orc_col_last_place(), float(st["scal"][4]), float(st["scal"][0]))
