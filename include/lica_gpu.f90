@@ -14,6 +14,7 @@ module lica_gpu
   integer(c_int), parameter :: LICA_ERR_CUDA = 5
   integer(c_int), parameter :: LICA_ERR_NOMEM = 6
   integer(c_int), parameter :: LICA_ERR_IO = 7
+  integer(c_int), parameter :: LICA_STALLED = 8
   integer(c_int), parameter :: LICA_MG_DOWN0 = 0
   integer(c_int), parameter :: LICA_MG_DOWN = 1
   integer(c_int), parameter :: LICA_MG_UP0 = 2

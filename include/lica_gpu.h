@@ -34,7 +34,10 @@ enum lica_status {
     LICA_BAD_ARG = 4,       /* argument outside what the entry point supports */
     LICA_ERR_CUDA = 5,      /* a CUDA runtime call failed (see lica_last_error) */
     LICA_ERR_NOMEM = 6,
-    LICA_ERR_IO = 7         /* a file could not be opened, read or written, or a record is malformed */
+    LICA_ERR_IO = 7,        /* a file could not be opened, read or written, or a record is malformed */
+    LICA_STALLED = 8        /* an iterative solve stopped at FP64's attainable accuracy: its true
+                               residual rose after falling within 1000x the tolerance, and the
+                               iterate before the rise is returned */
 };
 
 /* Message for the last LICA_ERR_CUDA / LICA_BAD_ARG on the calling thread. */

@@ -582,7 +582,7 @@ int lica_film2d_step_device(lica_film2d* F, double* u, double* v, double* p, dou
         local.iterations[k - 1] = r.iterations;
         local.rel_residual[k - 1] = r.rel_residual;
         local.status[k - 1] = r.status;
-        if (st != LICA_OK && st != LICA_NOT_CONVERGED) return st;
+        if (st != LICA_OK && st != LICA_NOT_CONVERGED && st != LICA_STALLED) return st;
         k_correct<<<gflow, blk, 0, s>>>(F->us, F->vs, F->dp, F->bx, F->by, u, v, p, adt, c);
         k_energy<<<gflow, blk, 0, s>>>(thc, u, v, F->densc, F->tc, F->psi, thn, F->rth, dt, gam, ro, c);
         k_ls_transport<<<gref, blk, 0, s>>>(phc, u, v, phn, F->rphi, dt, gam, ro, c);

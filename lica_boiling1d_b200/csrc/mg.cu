@@ -48,6 +48,7 @@ constexpr int NT_CTA = 512;      // threads of the single-CTA coarse kernel (few
 constexpr int kMaxLevels = 16;
 constexpr int kSmallCells = 64;  // levels with <= this many cells run in warp 0 alone
 constexpr int kMaxDense = 64;    // bottom-level unknowns solved by dense elimination
+constexpr double kStallFactor = 1e3;  // a rise of the residual below this x tol ends the PCG (LICA_STALLED)
 
 struct State {
     double fscale;  // ||f||_2 (1 if f = 0)
@@ -56,9 +57,11 @@ struct State {
     double alpha, beta;
     double tol;
     double sums[2];
+    double rel_prev;  // rel of the previous iterate
     int it, max_it;
     int status;     // lica_status
     int cont;       // 1 while the loop should continue
+    int back;       // 1: stalled, the answer is the iterate before the last one (it was decremented)
     unsigned cnt[4];
 };
 
@@ -552,10 +555,24 @@ __global__ void __launch_bounds__(NT) k_xupdate(double* __restrict__ x0, double*
         const double rel = sqrt(tot) / st->fscale;
         st->rel = rel;
         int cont = 0;
-        if (!isfinite(rel)) st->status = LICA_NAN;
-        else if (rel <= st->tol) st->status = LICA_OK;
-        else if (st->it >= st->max_it) st->status = LICA_NOT_CONVERGED;
-        else cont = 1;
+        if (!isfinite(rel)) {
+            st->status = LICA_NAN;
+        } else if (rel <= st->tol) {
+            st->status = LICA_OK;
+        } else if (!first && rel >= st->rel_prev && st->rel_prev <= kStallFactor * st->tol) {
+            // the true residual rose near the tolerance: FP64's attainable accuracy is
+            // reached (past it the search directions lose conjugacy and the iteration
+            // diverges).  The previous iterate is in the other x buffer: report it.
+            st->status = LICA_STALLED;
+            st->it = st->it - 1;
+            st->back = 1;
+            st->rel = st->rel_prev;
+        } else if (st->it >= st->max_it) {
+            st->status = LICA_NOT_CONVERGED;
+        } else {
+            cont = 1;
+        }
+        st->rel_prev = rel;
         st->cont = cont;
         if (use_cond) cudaGraphSetConditional(cond, cont ? 1u : 0u);
     }
@@ -1133,6 +1150,8 @@ __global__ void k_init_state(State* st, double tol, int max_it) {
     st->alpha = 0.0;
     st->beta = 0.0;
     st->rel = 0.0;
+    st->rel_prev = 0.0;
+    st->back = 0;
     st->sums[0] = st->sums[1] = 0.0;
     for (int k = 0; k < 4; ++k) st->cnt[k] = 0u;
 }
@@ -1617,7 +1636,7 @@ int solve_impl(lica_mg* m, double* x, const double* f, const double* bx, const d
         }
         LICA_CUDA_TRY(cudaGraphLaunch(m->gexec, s));
         if ((st = read_state(m, s))) return st;
-        lica_count_launches(m->setup_nodes + (int64_t)m->st_host->it * m->body_nodes);
+        lica_count_launches(m->setup_nodes + (int64_t)(m->st_host->it + m->st_host->back) * m->body_nodes);
     } else {
         cudaGraphConditionalHandle h{};
         if ((st = enqueue_setup(m, x, f, bx, by, rtol, max_it, h, 0, s))) return st;

@@ -142,7 +142,7 @@ SIGNATURES = {
 }
 
 STATUS = {0: "LICA_OK", 1: "LICA_NOT_CONVERGED", 2: "LICA_BAND_OVERFLOW", 3: "LICA_NAN", 4: "LICA_BAD_ARG",
-          5: "LICA_ERR_CUDA", 6: "LICA_ERR_NOMEM", 7: "LICA_ERR_IO"}
+          5: "LICA_ERR_CUDA", 6: "LICA_ERR_NOMEM", 7: "LICA_ERR_IO", 8: "LICA_STALLED"}
 
 
 class LicaError(RuntimeError):

@@ -157,7 +157,7 @@ class MultigridPoisson:
             s = stream if stream is not None else torch.cuda.current_stream()
             code = native.lib().lica_mg_solve_device(self._h, p.data_ptr(), f.data_ptr(), bx.data_ptr(),
                                                      by.data_ptr(), rtol, max_iters, C.byref(res), s.cuda_stream)
-        native.check(code, "lica_mg_solve", ok=(0, 1))
+        native.check(code, "lica_mg_solve", ok=(0, 1, 8))
         return res.iterations, res.rel_residual, res.status
 
     def solve_batch(self, ps, fs, bxs, bys, rtol=1e-10, max_iters=200):
@@ -178,7 +178,7 @@ class MultigridPoisson:
         res = (native.MgResult * cnt)()
         code = native.lib().lica_mg_solve_host_batch(self._h, cnt, ptrs(ps), ptrs(fs), ptrs(bxs), ptrs(bys), rtol,
                                                      max_iters, res)
-        native.check(code, "lica_mg_solve_host_batch", ok=(0, 1))
+        native.check(code, "lica_mg_solve_host_batch", ok=(0, 1, 8))
         return [(r.iterations, r.rel_residual, r.status) for r in res]
 
     KERNEL_CLASSES = ("down0", "down", "up0", "up", "cta", "pupdate", "xupdate", "setup")

@@ -490,7 +490,12 @@ int orc_mg_smooth(int nx, int ny, double hx, double hy, const double* bx, const 
 // Convergence: ||f - A p||_2 / ||f||_2 <= rtol, with the true FP64 residual checked
 // after every cycle.  res_hist (length max_cycles+1, may be null) receives the
 // relative residual before the first cycle and after each cycle.
-// Returns 0 converged, 1 not converged within max_cycles, 3 non-finite, 4 bad argument.
+// PCG stops when FP64's attainable accuracy is reached: if the true residual rises at
+// an iteration while the previous one is within 1000 rtol, the previous iterate is the
+// result (the GPU solver's rule; past that point the recomputed residual is rounding
+// noise, the directions lose conjugacy and the iteration diverges).
+// Returns 0 converged, 1 not converged within max_cycles, 3 non-finite, 4 bad argument,
+// 8 stalled at the attainable accuracy.
 int orc_mg_solve(int nx, int ny, double hx, double hy, int nlevels, int nu1, int nu2, int ncoarse,
                  int sym, int method, int mixed, const double* f, const double* bx, const double* by,
                  double* p, double rtol, int max_cycles, int* cycles_out, double* rel_out,
@@ -511,11 +516,21 @@ int orc_mg_solve(int nx, int ny, double hx, double hy, int nlevels, int nu1, int
     double rel = std::sqrt(dot(r, r)) / fscale;
     if (res_hist) res_hist[0] = rel;
     int c = 0, status = 1;
-    double rz = 0.0;
+    double rz = 0.0, rel_prev = rel;
+    std::vector<double> x_prev;
     while (true) {
         if (!std::isfinite(rel)) { status = 3; break; }
         if (rel <= rtol) { status = 0; break; }
+        if (method == 2 && c > 0 && rel >= rel_prev && rel_prev <= 1e3 * rtol) {
+            x = x_prev;
+            rel = rel_prev;
+            --c;
+            status = 8;
+            break;
+        }
         if (c >= max_cycles) break;
+        rel_prev = rel;
+        if (method == 2) x_prev = x;
         if (method == 0) {
             std::memcpy(L0.f.data(), fv.data(), n * sizeof(double));
             std::memcpy(L0.u.data(), x.data(), n * sizeof(double));

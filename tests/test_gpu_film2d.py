@@ -1,8 +1,10 @@
 """The 2-D film-boiling step on the GPU (lica_film2d_*) against the CPU restatement
 (oracle/film2d.py): every field after one and two RK3 steps.  Away from the pressure solves
 both sides evaluate the same expressions in the same order (no FMA contraction); the solves
-stop at the same relative residual (1e-8, the step's default), so the fields agree to about
-that level: 1e-6 relative L2 per field is the bar."""
+stop at the same relative residual, 1e-10 (the step's default), and differ only in the
+order of their dot products.  The bar is 1e-10 relative L2 for every field (the level set
+and the pressure included): at this size the fields move by under 4e-11 between solver
+paths that both reach 1e-10."""
 import numpy as np
 import pytest
 
@@ -11,6 +13,7 @@ from oracle import film2d as F
 pytestmark = pytest.mark.gpu
 
 NX, NY = 64, 192
+TOL = 1e-10
 
 
 def _rel(a, b):
@@ -44,18 +47,20 @@ def _run(nsteps, precision="fp64", nx=NX, ny=NY):
 def test_step_matches_oracle_fp64(nsteps):
     got, ref, infos, rinfo, md = _run(nsteps)
     for info in infos:
-        assert info["status"] == [0, 0, 0] and max(info["rel"]) <= 1e-8, info
+        assert info["status"] == [0, 0, 0] and max(info["rel"]) <= TOL, info
     errs = {k: _rel(got[k], ref[k]) for k in ref}
-    assert all(e <= 1e-6 for e in errs.values()), errs
-    assert np.abs(got["phi"] - ref["phi"]).max() <= 1e-8
-    assert _rel(md, rinfo["mdot"]) <= 1e-6
+    assert all(e <= TOL for e in errs.values()), errs
+    assert np.abs(got["phi"] - ref["phi"]).max() <= 1e-12
+    assert _rel(md, rinfo["mdot"]) <= TOL
 
 
 def test_step_mixed_precision_pressure():
+    """FP32 smoothing inside the FP64 PCG: the solves meet the same 1e-10 residual, so the
+    fields meet the FP64 oracle's at the same bar."""
     got, ref, infos, rinfo, md = _run(1, precision="mixed")
-    assert infos[0]["status"] == [0, 0, 0]
+    assert infos[0]["status"] == [0, 0, 0] and max(infos[0]["rel"]) <= TOL
     errs = {k: _rel(got[k], ref[k]) for k in ref}
-    assert all(e <= 1e-6 for e in errs.values()), errs
+    assert all(e <= TOL for e in errs.values()), errs
 
 
 def test_bad_sizes_rejected():

@@ -146,3 +146,36 @@ def test_cpp_restatement_is_bit_identical_to_numpy():
         for k in a:
             np.testing.assert_array_equal(a[k], b[k])
         np.testing.assert_array_equal(ia["mdot"], ib["mdot"])
+
+
+class _FirstSystem(Exception):
+    pass
+
+
+def test_pressure_solve_stops_at_fp64_floor_at_config_size():
+    """At the config's 512 x 1536 the first substep's pressure increment is so large against
+    its right-hand side (||A|| ||dp|| / ||f|| ~ 1e7) that FP64 cannot hold a solution with a
+    1e-10 relative residual: rounding the converged increment by random half-ulps alone gives
+    a residual above 1e-10.  The PCG then stops at that floor (LICA_STALLED, status 8) with
+    the iterate before the residual rose, instead of diverging as an unguarded PCG does."""
+    from oracle import oracle as orc
+    nx, ny = 512, 1536
+    P = F.default_props()
+    st = F.initial_state(nx, ny, y0_cells=64, amp_cells=4)
+    dt = F.stable_dt(nx, P)
+    got = {}
+
+    def capture(f, bx, by, h, p0):
+        got.update(f=f, bx=bx, by=by, h=h)
+        raise _FirstSystem
+
+    with pytest.raises(_FirstSystem):
+        F.step(st, dt, P, capture)
+    f, bx, by, h = got["f"], got["bx"], got["by"], got["h"]
+    p, it, rel, hist, status = orc.mg_solve(f, bx, by, h, h, nlevels=6, ncoarse=2, rtol=1e-10, max_cycles=60)
+    assert status == 8 and 1e-10 < rel < 1e-9 and it <= 16, (status, rel, it)
+    assert rel == hist[-1] == hist.min()
+    rng = np.random.default_rng(0)
+    delta = rng.uniform(-0.5, 0.5, p.shape) * np.spacing(np.abs(p))
+    floor = np.linalg.norm(orc.mg_apply(delta, bx, by, h, h)) / np.linalg.norm(f)
+    assert floor > 1e-10, floor
