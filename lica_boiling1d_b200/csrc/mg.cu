@@ -29,9 +29,12 @@
 //     restatement in FP64 and in FP32; only the dot products differ (summation order).
 #include "common.cuh"
 
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -62,6 +65,7 @@ struct State {
     int status;     // lica_status
     int cont;       // 1 while the loop should continue
     int back;       // 1: stalled, the answer is the iterate before the last one (it was decremented)
+    int kerr;       // 1: a bounded wait inside a kernel ran out (the solve ends with LICA_ERR_CUDA)
     unsigned cnt[4];
 };
 
@@ -261,18 +265,13 @@ __device__ __forceinline__ void rb_zero(T* __restrict__ su) {
 // (fc = (r00 + r10 + r01 + r11) / 4 in the oracle's order; the east partner of an even
 // column is the neighbouring lane).
 // ------------------------------------------------------------------------------------
+// The part after the loads, for the tile whose first interior cell is (ti0, tj0); su is
+// zero-filled and the thread's cells are loaded; every thread calls it.
 template <typename T, int NSW, int TXX, int TYY, int R>
-__global__ void __launch_bounds__(RBCfg<NSW, TXX, TYY, R>::NTH, 2)
-    k_down(const T* __restrict__ f, const T* __restrict__ ax, const T* __restrict__ ay, const T* __restrict__ dinv,
-           T* __restrict__ u_out, T* __restrict__ fc_out, int nx, int ny) {
+__device__ __forceinline__ void down_body(const RBCells<T, RBCfg<NSW, TXX, TYY, R>::K>& cl,
+                                          const RBGeom<RBCfg<NSW, TXX, TYY, R>>& g, T* __restrict__ su,
+                                          T* __restrict__ u_out, T* __restrict__ fc_out, int nx, int ti0, int tj0) {
     using C = RBCfg<NSW, TXX, TYY, R>;
-    __shared__ __align__(16) T su[C::WORDS];
-    const int gi0 = blockIdx.x * TXX - C::H, gj0 = blockIdx.y * TYY - C::H;
-    const RBGeom<C> g;
-    RBCells<T, C::K> cl;
-    rb_zero<T, C>(su);
-    rb_load<T, C>(cl, g, f, ax, ay, dinv, nx, ny, gi0, gj0);
-    __syncthreads();  // zero fill done
     rb_first_red<T, C>(cl, g, su);
     __syncthreads();
     rb_half_sweep<T, C, 1>(cl, g, su);
@@ -285,7 +284,7 @@ __global__ void __launch_bounds__(RBCfg<NSW, TXX, TYY, R>::NTH, 2)
         __syncthreads();
     }
     const bool col_in = g.used && g.x >= C::H && g.x < C::H + TXX;
-    const int ti = blockIdx.x * TXX + g.x - C::H;
+    const int ti = ti0 + g.x - C::H;
     const int ncx = nx >> 1;
 #pragma unroll
     for (int k = 0; k < C::K; ++k) {
@@ -296,7 +295,7 @@ __global__ void __launch_bounds__(RBCfg<NSW, TXX, TYY, R>::NTH, 2)
         const int y = g.s * R + 2 * k;
         const bool row_in = col_in && y >= C::H && y < C::H + TYY;
         if (row_in) {
-            const int tj = blockIdx.y * TYY + y - C::H;
+            const int tj = tj0 + y - C::H;
             u_out[(tj + g.p) * nx + ti] = u0;
             u_out[(tj + 1 - g.p) * nx + ti] = u1;
         }
@@ -305,9 +304,24 @@ __global__ void __launch_bounds__(RBCfg<NSW, TXX, TYY, R>::NTH, 2)
         const T oB = __shfl_xor_sync(0xffffffffu, r1, 1);
         if (row_in && g.p == 0) {
             const T fcv = T(0.25) * ((r0 + oB) + (r1 + oA));
-            fc_out[((blockIdx.y * TYY + y - C::H) >> 1) * ncx + (ti >> 1)] = fcv;
+            fc_out[((tj0 + y - C::H) >> 1) * ncx + (ti >> 1)] = fcv;
         }
     }
+}
+
+template <typename T, int NSW, int TXX, int TYY, int R>
+__global__ void __launch_bounds__(RBCfg<NSW, TXX, TYY, R>::NTH, 2)
+    k_down(const T* __restrict__ f, const T* __restrict__ ax, const T* __restrict__ ay, const T* __restrict__ dinv,
+           T* __restrict__ u_out, T* __restrict__ fc_out, int nx, int ny) {
+    using C = RBCfg<NSW, TXX, TYY, R>;
+    __shared__ __align__(16) T su[C::WORDS];
+    const int gi0 = blockIdx.x * TXX - C::H, gj0 = blockIdx.y * TYY - C::H;
+    const RBGeom<C> g;
+    RBCells<T, C::K> cl;
+    rb_zero<T, C>(su);
+    rb_load<T, C>(cl, g, f, ax, ay, dinv, nx, ny, gi0, gj0);
+    __syncthreads();  // zero fill done
+    down_body<T, NSW, TXX, TYY, R>(cl, g, su, u_out, fc_out, nx, blockIdx.x * TXX, blockIdx.y * TYY);
 }
 
 // ------------------------------------------------------------------------------------
@@ -315,6 +329,50 @@ __global__ void __launch_bounds__(RBCfg<NSW, TXX, TYY, R>::NTH, 2)
 // u_post (out of place: no block reads a tile another block has updated); at level 0
 // also the r.z partial (r = f of level 0, z = u) and, in the last block, beta.
 // ------------------------------------------------------------------------------------
+// The part after the loads: uv holds u_pre + P uc of the thread's cells (0 off the
+// domain), su is zero-filled; returns the tile's r.z partial (LEVEL0) or 0.
+template <typename T, int NSW, int TXX, int TYY, int R, bool LEVEL0>
+__device__ __forceinline__ double up_body(const RBCells<T, RBCfg<NSW, TXX, TYY, R>::K>& cl,
+                                          const RBGeom<RBCfg<NSW, TXX, TYY, R>>& g,
+                                          const T (&uv)[2][RBCfg<NSW, TXX, TYY, R>::K], T* __restrict__ su,
+                                          T* __restrict__ u_post, int nx, int ti0, int tj0) {
+    using C = RBCfg<NSW, TXX, TYY, R>;
+    if (g.used) {
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+#pragma unroll
+            for (int k = 0; k < C::K; ++k) su[g.base[c] + 2 * k * C::RXP] = uv[c][k];
+        }
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int q = 0; q < NSW; ++q) {
+        rb_half_sweep<T, C, 1>(cl, g, su);
+        __syncthreads();
+        rb_half_sweep<T, C, 0>(cl, g, su);
+        __syncthreads();
+    }
+    const bool col_in = g.used && g.x >= C::H && g.x < C::H + TXX;
+    const int ti = ti0 + g.x - C::H;
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < C::K; ++k) {
+        const int y = g.s * R + 2 * k;
+        if (col_in && y >= C::H && y < C::H + TYY) {
+            const int tj = tj0 + y - C::H;
+            const T u0 = su[g.base[0] + 2 * k * C::RXP];
+            const T u1 = su[g.base[1] + 2 * k * C::RXP];
+            u_post[(tj + g.p) * nx + ti] = u0;
+            u_post[(tj + 1 - g.p) * nx + ti] = u1;
+            if (LEVEL0) {
+                acc += double(cl.f[0][k]) * double(u0);
+                acc += double(cl.f[1][k]) * double(u1);
+            }
+        }
+    }
+    return acc;
+}
+
 template <typename T, int NSW, int TXX, int TYY, int R, bool LEVEL0>
 __global__ void __launch_bounds__(RBCfg<NSW, TXX, TYY, R>::NTH, 2)
     k_up(const T* __restrict__ u_pre, T* __restrict__ u_post, const T* __restrict__ uc, const T* __restrict__ f,
@@ -348,39 +406,8 @@ __global__ void __launch_bounds__(RBCfg<NSW, TXX, TYY, R>::NTH, 2)
         }
     }
     __syncthreads();  // zero fill done
-    if (g.used) {
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-#pragma unroll
-            for (int k = 0; k < C::K; ++k) su[g.base[c] + 2 * k * C::RXP] = uv[c][k];
-        }
-    }
-    __syncthreads();
-#pragma unroll 1
-    for (int q = 0; q < NSW; ++q) {
-        rb_half_sweep<T, C, 1>(cl, g, su);
-        __syncthreads();
-        rb_half_sweep<T, C, 0>(cl, g, su);
-        __syncthreads();
-    }
-    const bool col_in = g.used && g.x >= C::H && g.x < C::H + TXX;
-    const int ti = blockIdx.x * TXX + g.x - C::H;
-    double acc = 0.0;
-#pragma unroll
-    for (int k = 0; k < C::K; ++k) {
-        const int y = g.s * R + 2 * k;
-        if (col_in && y >= C::H && y < C::H + TYY) {
-            const int tj = blockIdx.y * TYY + y - C::H;
-            const T u0 = su[g.base[0] + 2 * k * C::RXP];
-            const T u1 = su[g.base[1] + 2 * k * C::RXP];
-            u_post[(tj + g.p) * nx + ti] = u0;
-            u_post[(tj + 1 - g.p) * nx + ti] = u1;
-            if (LEVEL0) {
-                acc += double(cl.f[0][k]) * double(u0);
-                acc += double(cl.f[1][k]) * double(u1);
-            }
-        }
-    }
+    const double acc =
+        up_body<T, NSW, TXX, TYY, R, LEVEL0>(cl, g, uv, su, u_post, nx, blockIdx.x * TXX, blockIdx.y * TYY);
     if (LEVEL0) {
         const double b = block_sum(acc, red);
         double tot;
@@ -390,6 +417,14 @@ __global__ void __launch_bounds__(RBCfg<NSW, TXX, TYY, R>::NTH, 2)
         }
     }
 }
+
+}  // namespace mg
+}  // namespace lica
+
+#include "mg_tma.cuh"
+
+namespace lica {
+namespace mg {
 
 // ------------------------------------------------------------------------------------
 // CG kernels (FP64 vectors) on TX x TY tiles with a 2-cell halo (one ring is used; the
@@ -555,7 +590,9 @@ __global__ void __launch_bounds__(NT) k_xupdate(double* __restrict__ x0, double*
         const double rel = sqrt(tot) / st->fscale;
         st->rel = rel;
         int cont = 0;
-        if (!isfinite(rel)) {
+        if (st->kerr) {
+            st->status = LICA_ERR_CUDA;
+        } else if (!isfinite(rel)) {
             st->status = LICA_NAN;
         } else if (rel <= st->tol) {
             st->status = LICA_OK;
@@ -1152,6 +1189,7 @@ __global__ void k_init_state(State* st, double tol, int max_it) {
     st->rel = 0.0;
     st->rel_prev = 0.0;
     st->back = 0;
+    st->kerr = 0;
     st->sums[0] = st->sums[1] = 0.0;
     for (int k = 0; k < 4; ++k) st->cnt[k] = 0u;
 }
@@ -1189,10 +1227,13 @@ struct LevelBuf {
     float* ax32 = nullptr;
     float* ay32 = nullptr;
     float* di32 = nullptr;
+    bool tma = false;        // smoothed by the persistent TMA-staged kernels (k_smooth_tma)
+    TmMaps tm_down{}, tm_up{};
 };
 
 struct lica_mg {
     int nx, ny;
+    int nsm = 148;  // SMs of the device (persistent grids)
     double hx, hy;
     lica_mg_options o;
     int nouter = 0, lcta = 0, bottom = 0;
@@ -1238,6 +1279,78 @@ struct lica_mg {
 namespace {
 
 bool is_mixed(const lica_mg* m) { return m->o.precision == 1; }
+
+PFN_cuTensorMapEncodeTiled_v12000 mg_encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// A 2-D map of a row-major w x h array (FP32 or FP64) with a bw x bh box, zero fill.
+int tm_map(CUtensorMap* mp, const void* base, bool f32, int w, int h, int bw, int bh) {
+    auto fn = mg_encode_fn();
+    if (!fn) {
+        lica_set_last_error("cuTensorMapEncodeTiled", "driver entry point unavailable", __FILE__, __LINE__);
+        return LICA_ERR_CUDA;
+    }
+    const cuuint64_t es = f32 ? 4 : 8;
+    cuuint64_t dims[2] = {(cuuint64_t)w, (cuuint64_t)h};
+    cuuint64_t strides[1] = {(cuuint64_t)w * es};
+    cuuint32_t box[2] = {(cuuint32_t)bw, (cuuint32_t)bh};
+    cuuint32_t el[2] = {1, 1};
+    const CUresult r = fn(mp, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2,
+                          const_cast<void*>(base), dims, strides, box, el, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        lica_set_last_error("cuTensorMapEncodeTiled", "multigrid tile map rejected", __FILE__, __LINE__);
+        return LICA_BAD_ARG;
+    }
+    return LICA_OK;
+}
+
+// Tensor maps of the levels the persistent TMA kernels smooth: levels with 32 x 32 tiles,
+// at least two tile columns and two tiles per resident CTA slot, V(2,2) cycles.
+int build_tma(lica_mg* m) {
+    const bool f32 = is_mixed(m);
+    for (int l = 0; l < m->lcta; ++l) {
+        LevelBuf& L = m->lv[l];
+        LevelBuf& C = m->lv[l + 1];
+        const int ntx = L.nx / TM_TS, nty = L.ny / TM_TS;
+        if (m->o.nu1 != 2 || m->o.nu2 != 2 || L.nx % TM_TS || L.ny % TM_TS || ntx < 2 || ntx * nty < 4 * m->nsm)
+            continue;
+        const void* ax = f32 ? (const void*)L.ax32 : (const void*)L.ax64;
+        const void* ay = f32 ? (const void*)L.ay32 : (const void*)L.ay64;
+        const void* di = f32 ? (const void*)L.di32 : (const void*)L.di64;
+        const void* uc = (l + 1 == m->lcta) ? C.u : C.up;
+        int st;
+        for (TmMaps* M : {&L.tm_down, &L.tm_up}) {
+            if ((st = tm_map(&M->f, L.f, f32, L.nx, L.ny, TM_RX, TM_RY)) ||
+                (st = tm_map(&M->fw, L.f, f32, L.nx, L.ny, TM_WW, TM_RY)) ||
+                (st = tm_map(&M->d, di, f32, L.nx, L.ny, TM_RX, TM_RY)) ||
+                (st = tm_map(&M->dw, di, f32, L.nx, L.ny, TM_WW, TM_RY)) ||
+                (st = tm_map(&M->ax, ax, f32, L.nx, L.ny, TM_AXW, TM_RY)) ||
+                (st = tm_map(&M->axw, ax, f32, L.nx, L.ny, TM_WW, TM_RY)) ||
+                (st = tm_map(&M->ay, ay, f32, L.nx, L.ny + 1, TM_RX, TM_AYH)) ||
+                (st = tm_map(&M->ayw, ay, f32, L.nx, L.ny + 1, TM_WW, TM_AYH)))
+                return st;
+        }
+        if ((st = tm_map(&L.tm_up.u, L.u, f32, L.nx, L.ny, TM_RX, TM_RY)) ||
+            (st = tm_map(&L.tm_up.uw, L.u, f32, L.nx, L.ny, TM_WW, TM_RY)) ||
+            (st = tm_map(&L.tm_up.c, uc, f32, C.nx, C.ny, TM_CW, TM_CH)) ||
+            (st = tm_map(&L.tm_up.cw, uc, f32, C.nx, C.ny, TM_CWW, TM_CH)))
+            return st;
+        L.tma = true;
+    }
+    return LICA_OK;
+}
 
 // Profiling: bracket one kernel launch with events when profiling is on.
 cudaEvent_t pool_event(lica_mg* m) {
@@ -1316,11 +1429,39 @@ void down_ns(const LevelBuf& L, const LevelBuf& C, cudaStream_t s) {
     else down_tile<T, NS, 16>(L, C, s);
 }
 
+// The persistent TMA-staged smoothing kernels (levels with L.tma): k_down's work (up =
+// false) or k_up's (up = true), two CTAs per SM walking the level's 32 x 32 tiles.
+template <typename T>
+void launch_tma(lica_mg* m, int l, bool up, cudaStream_t s) {
+    LevelBuf& L = m->lv[l];
+    TmArgs<T> A;
+    A.m = up ? L.tm_up : L.tm_down;
+    A.out = (T*)(up ? L.up : L.u);
+    A.fc = up ? nullptr : (T*)m->lv[l + 1].f;
+    A.nx = L.nx;
+    A.ny = L.ny;
+    A.ntx = L.nx / TM_TS;
+    A.nty = L.ny / TM_TS;
+    A.st = m->st;
+    A.partials = m->partials;
+    const int grid = std::min(A.ntx * A.nty, 2 * m->nsm);
+    const size_t smem = TmStage<T>::BYTES;
+    if (!up) k_smooth_tma<T, false, false><<<grid, TmCfg::NTH, smem, s>>>(A);
+    else if (l == 0) k_smooth_tma<T, true, true><<<grid, TmCfg::NTH, smem, s>>>(A);
+    else k_smooth_tma<T, true, false><<<grid, TmCfg::NTH, smem, s>>>(A);
+}
+
 template <typename T>
 int launch_down(lica_mg* m, int l, cudaStream_t s) {
     LevelBuf& L = m->lv[l];
     LevelBuf& C = m->lv[l + 1];
     ProfScope ps(m, l == 0 ? LICA_MG_DOWN0 : LICA_MG_DOWN, s);
+    if (L.tma) {
+        launch_tma<T>(m, l, false, s);
+        LICA_CUDA_TRY(cudaGetLastError());
+        lica_count_launches(1);
+        return LICA_OK;
+    }
     switch (m->o.nu1) {
         case 1: down_ns<T, 1>(L, C, s); break;
         case 2: down_ns<T, 2>(L, C, s); break;
@@ -1357,6 +1498,12 @@ int launch_up(lica_mg* m, int l, cudaStream_t s) {
     LevelBuf& C = m->lv[l + 1];
     const T* uc = (const T*)((l + 1 == m->lcta) ? C.u : C.up);
     ProfScope ps(m, l == 0 ? LICA_MG_UP0 : LICA_MG_UP, s);
+    if (L.tma) {
+        launch_tma<T>(m, l, true, s);
+        LICA_CUDA_TRY(cudaGetLastError());
+        lica_count_launches(1);
+        return LICA_OK;
+    }
     switch (m->o.nu2) {
         case 1: up_ns<T, 1>(m, L, uc, l == 0, s); break;
         case 2: up_ns<T, 2>(m, L, uc, l == 0, s); break;
@@ -1853,6 +2000,28 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
         lica_set_last_error("cudaFuncSetAttribute(k_cta)", cudaGetErrorString(e), __FILE__, __LINE__);
         return fail(LICA_ERR_CUDA);
     }
+    // the persistent TMA-staged smoothing kernels of the large levels
+    e = cudaDeviceGetAttribute(&m->nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_smooth_tma<double, false, false>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, TmStage<double>::BYTES);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_smooth_tma<double, true, false>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, TmStage<double>::BYTES);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_smooth_tma<double, true, true>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, TmStage<double>::BYTES);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_smooth_tma<float, false, false>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, TmStage<float>::BYTES);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_smooth_tma<float, true, false>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, TmStage<float>::BYTES);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_smooth_tma<float, true, true>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, TmStage<float>::BYTES);
+    if (e != cudaSuccess) {
+        lica_set_last_error("cudaFuncSetAttribute(k_smooth_tma)", cudaGetErrorString(e), __FILE__, __LINE__);
+        return fail(LICA_ERR_CUDA);
+    }
+    m->lv[0].u = m->zpre;
+    m->lv[0].up = m->z;
+    m->lv[0].f = m->r;
+    if (int st = build_tma(m)) return fail(st);
     *out = m;
     return LICA_OK;
 }

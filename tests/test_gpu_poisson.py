@@ -100,9 +100,11 @@ def test_operator_bitwise():
     np.testing.assert_array_equal(out.cpu().numpy(), ref)
 
 
-@pytest.mark.parametrize("n,nlevels", [(128, 3), (256, 4), (1024, 6)])
+@pytest.mark.parametrize("n,nlevels", [(128, 3), (256, 4), (1024, 6), (2048, 7)])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_preconditioner_bitwise(n, nlevels, precision):
+    """One V-cycle.  1024^2 smooths level 0, and 2048^2 levels 0 and 1, with the persistent
+    TMA-staged kernels; the smaller levels with the per-tile ones."""
     import torch
     c = bubble_poisson_case(n)
     ref = oracle.mg_precond(c.f, c.bx, c.by, c.hx, c.hy, nlevels=nlevels, ncoarse=2, sym=5,
@@ -132,6 +134,25 @@ def test_solve_matches_oracle_1024(use_graph, precision):
     # the reported residual is the true FP64 residual
     r = c.f - oracle.mg_apply(pg, c.bx, c.by, c.hx, c.hy)
     assert np.linalg.norm(r) / np.linalg.norm(c.f) == pytest.approx(rel, rel=1e-6)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_solve_matches_oracle_2048(precision):
+    """The 2048^2 solve of the mixed-precision config: same 64 bubbles (radii 16-96 cells),
+    7 levels, 1e-10; the GPU solution within 1e-10 relative L2 of the oracle's."""
+    import torch
+    c = bubble_poisson_case(2048)
+    mixed = precision == "mixed"
+    p_ref, it_ref, rel_ref, _, st_ref = oracle.mg_solve(c.f, c.bx, c.by, c.hx, c.hy, nlevels=7, ncoarse=1, sym=5,
+                                                       method="pcg", mixed=mixed, rtol=TOL, max_cycles=100)
+    s = _solver(2048, 7, precision, ncoarse=1)
+    p = torch.zeros((2048, 2048), dtype=torch.float64, device="cuda")
+    it, rel, st = s.solve(p, _t(c.f), _t(c.bx), _t(c.by), rtol=TOL, max_iters=100)
+    assert st == 0 and st_ref == 0
+    assert rel <= TOL
+    assert abs(it - it_ref) <= 1, (it, it_ref)
+    pg = p.cpu().numpy()
+    assert np.linalg.norm(pg - p_ref) / np.linalg.norm(p_ref) <= TOL
 
 
 def test_solve_golden_sparse_direct():
