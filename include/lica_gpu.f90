@@ -567,6 +567,136 @@ module lica_gpu
       type(c_ptr), value :: stream
     end function lica_gpu_lvs_transport_device
 
+    integer(c_int) function lica_gpu_reinitialization(ncol, n, length, phi, layer, ilimit, &
+        status) bind(c, name="lica_gpu_reinitialization")
+      import
+      integer(c_int32_t), value :: ncol
+      integer(c_int32_t), value :: n
+      real(c_double), value :: length
+      real(c_double), intent(inout) :: phi(*)
+      integer(c_int32_t), intent(in) :: layer(*)
+      integer(c_int32_t), value :: ilimit
+      integer(c_int32_t), intent(inout) :: status(*)
+    end function lica_gpu_reinitialization
+
+    integer(c_int) function lica_gpu_reinitialization_device(ncol, n, length, phi, layer, &
+        ilimit, status, stream) bind(c, name="lica_gpu_reinitialization_device")
+      import
+      integer(c_int32_t), value :: ncol
+      integer(c_int32_t), value :: n
+      real(c_double), value :: length
+      type(c_ptr), value :: phi
+      type(c_ptr), value :: layer
+      integer(c_int32_t), value :: ilimit
+      type(c_ptr), value :: status
+      type(c_ptr), value :: stream
+    end function lica_gpu_reinitialization_device
+
+    integer(c_int) function lica_gpu_grid_coupling(ncol, n, length, ini_psi, psif, layer, &
+        psi_cn, psi_zn) bind(c, name="lica_gpu_grid_coupling")
+      import
+      integer(c_int32_t), value :: ncol
+      integer(c_int32_t), value :: n
+      real(c_double), value :: length
+      integer(c_int32_t), value :: ini_psi
+      real(c_double), intent(in) :: psif(*)
+      integer(c_int32_t), intent(in) :: layer(*)
+      real(c_double), intent(inout) :: psi_cn(*)
+      real(c_double), intent(inout) :: psi_zn(*)
+    end function lica_gpu_grid_coupling
+
+    integer(c_int) function lica_gpu_grid_coupling_device(ncol, n, length, ini_psi, psif, &
+        layer, psi_cn, psi_zn, stream) bind(c, name="lica_gpu_grid_coupling_device")
+      import
+      integer(c_int32_t), value :: ncol
+      integer(c_int32_t), value :: n
+      real(c_double), value :: length
+      integer(c_int32_t), value :: ini_psi
+      type(c_ptr), value :: psif
+      type(c_ptr), value :: layer
+      type(c_ptr), value :: psi_cn
+      type(c_ptr), value :: psi_zn
+      type(c_ptr), value :: stream
+    end function lica_gpu_grid_coupling_device
+
+    integer(c_int) function lica_gpu_temp_grad(ncol, n, length, props, dtconst, t, psi_cn, phi, &
+        layer, mflvs, sfgas, sfgas2, imask, vol_tot_iphs, iterations, status) &
+        bind(c, name="lica_gpu_temp_grad")
+      import
+      integer(c_int32_t), value :: ncol
+      integer(c_int32_t), value :: n
+      real(c_double), value :: length
+      type(lica_col_props), intent(in) :: props
+      real(c_double), value :: dtconst
+      real(c_double), intent(in) :: t(*)
+      real(c_double), intent(in) :: psi_cn(*)
+      real(c_double), intent(in) :: phi(*)
+      integer(c_int32_t), intent(in) :: layer(*)
+      real(c_double), intent(inout) :: mflvs(*)
+      real(c_double), intent(inout) :: sfgas(*)
+      real(c_double), intent(inout) :: sfgas2(*)
+      integer(c_int32_t), intent(inout) :: imask(*)
+      real(c_double), intent(inout) :: vol_tot_iphs(*)
+      integer(c_int32_t), intent(inout) :: iterations(*)
+      integer(c_int32_t), intent(inout) :: status(*)
+    end function lica_gpu_temp_grad
+
+    integer(c_int) function lica_gpu_temp_grad_device(ncol, n, length, props, dtconst, t, &
+        psi_cn, phi, layer, mflvs, sfgas, sfgas2, imask, vol_tot_iphs, iterations, status, &
+        scratch, stream) bind(c, name="lica_gpu_temp_grad_device")
+      import
+      integer(c_int32_t), value :: ncol
+      integer(c_int32_t), value :: n
+      real(c_double), value :: length
+      type(lica_col_props), intent(in) :: props
+      real(c_double), value :: dtconst
+      type(c_ptr), value :: t
+      type(c_ptr), value :: psi_cn
+      type(c_ptr), value :: phi
+      type(c_ptr), value :: layer
+      type(c_ptr), value :: mflvs
+      type(c_ptr), value :: sfgas
+      type(c_ptr), value :: sfgas2
+      type(c_ptr), value :: imask
+      type(c_ptr), value :: vol_tot_iphs
+      type(c_ptr), value :: iterations
+      type(c_ptr), value :: status
+      type(c_ptr), value :: scratch
+      type(c_ptr), value :: stream
+    end function lica_gpu_temp_grad_device
+
+    integer(c_int) function lica_gpu_pressure_correction(ncol, n, length, props, dtconst, w, p, &
+        denf_zi, sfgas) bind(c, name="lica_gpu_pressure_correction")
+      import
+      integer(c_int32_t), value :: ncol
+      integer(c_int32_t), value :: n
+      real(c_double), value :: length
+      type(lica_col_props), intent(in) :: props
+      real(c_double), value :: dtconst
+      real(c_double), intent(inout) :: w(*)
+      real(c_double), intent(inout) :: p(*)
+      real(c_double), intent(in) :: denf_zi(*)
+      real(c_double), intent(in) :: sfgas(*)
+    end function lica_gpu_pressure_correction
+
+    integer(c_int) function lica_gpu_pressure_correction_device(ncol, n, length, props, &
+        dtconst, w, p, denf_zi, sfgas, status, scratch, stream) &
+        bind(c, name="lica_gpu_pressure_correction_device")
+      import
+      integer(c_int32_t), value :: ncol
+      integer(c_int32_t), value :: n
+      real(c_double), value :: length
+      type(lica_col_props), intent(in) :: props
+      real(c_double), value :: dtconst
+      type(c_ptr), value :: w
+      type(c_ptr), value :: p
+      type(c_ptr), value :: denf_zi
+      type(c_ptr), value :: sfgas
+      type(c_ptr), value :: status
+      type(c_ptr), value :: scratch
+      type(c_ptr), value :: stream
+    end function lica_gpu_pressure_correction_device
+
     integer(c_int) function lica_unet_conv3x3_device(x0, c0, x1, c1, w, bias, n, h, wd, cout, &
         relu, out, out32, out_c, out_c0, err, stream) bind(c, name="lica_unet_conv3x3_device")
       import

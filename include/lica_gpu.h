@@ -399,6 +399,69 @@ int lica_gpu_lvs_transport_device(int32_t ncol, int32_t n, double length, double
                                   double* psi_zn, int32_t* status, double* stats, const lica_lvs_params* prm,
                                   void* stream);
 
+/* ------------------------------------------------------------------------------------
+ * Single subroutines of the step, for a host that replaces the reference's routines one at
+ * a time.  Batches of ncol columns of n flow cells over length, in the column layout of
+ * lica_col_state (flow arrays n+2 per column, phi-like nf+7 at k+2, psif-like nf+2 at k).
+ * Host arrays (copied in and out) or, with _device, device arrays and a stream (enqueues
+ * and returns).  Each runs the same device code as the fused step, so a sequence of them
+ * gives the step's results bit for bit.
+ * ---------------------------------------------------------------------------------- */
+
+/* REINITIALIZATION(NN1, NN2, ILIMIT, LLVS) (two_phase.f:2033-2474; called from TRANSPORT,
+ * two_phase.f:906,928, and VOL_TOT_MFDOT, chphase.f:1415): ILIMIT SSP-RK3 pseudo-time
+ * iterations of the Sussman/Peng reinitialisation with dtau = h_f/2 on the band layers
+ * 1..NN2 = 1..N_MAX-1 (HJ-WENO5 on 1..NN1 = 1..N_MAX-3, first order beyond).  phi is
+ * ALPHI_EXT as the caller holds it (every cell is read; the reference's call sites hold it
+ * zero off the band), layer the band (cell k in layer m = 1..N_MAX, 0 off the band); only
+ * the band cells of phi are written.  status[ncol]: LICA_OK, LICA_BAND_OVERFLOW (the band
+ * spans more than 112 refined cells; phi unchanged) or LICA_BAD_ARG (a band cell outside
+ * k = 1..nf). */
+int lica_gpu_reinitialization(int32_t ncol, int32_t n, double length, double* phi, const int32_t* layer,
+                              int32_t ilimit, int32_t* status);
+int lica_gpu_reinitialization_device(int32_t ncol, int32_t n, double length, double* phi, const int32_t* layer,
+                                     int32_t ilimit, int32_t* status, void* stream);
+
+/* GRID_COUPLING(INI_PSI, PSI_XN, PSI_YN, PSI_ZN, PSI_CN) (two_phase.f:4863-5118; called from
+ * MAIN, 1d.f:244, and LVSINIT): the flow-grid liquid fractions from PSIF by box integrals
+ * over the refined cells (INTER_PSI), snapped at 1e-3 / 0.999.  ini_psi = 1: every flow
+ * cell; 0: the flow cells of the band cells of layers 1..NN1 (layer may be NULL with
+ * ini_psi = 1).  psi_cn, psi_zn are updated in place (cells the mask leaves are only
+ * snapped).  PSI_XN and PSI_YN are zero in the 1-D column. */
+int lica_gpu_grid_coupling(int32_t ncol, int32_t n, double length, int32_t ini_psi, const double* psif,
+                           const int32_t* layer, double* psi_cn, double* psi_zn);
+int lica_gpu_grid_coupling_device(int32_t ncol, int32_t n, double length, int32_t ini_psi, const double* psif,
+                                  const int32_t* layer, double* psi_cn, double* psi_zn, void* stream);
+
+/* TEMP_GRAD(PSI_CN) (chphase.f:55-368; called from PASSIVE_SCALAR, 1d.f:3667) with the
+ * routines it calls -- PHINSINTP, TEMP_EXTP(_RK3), TEMPASSIGN, TF_GRAD, VOL_TOT_MFDOT --
+ * and CAL_PSI_TMP(1): reads T, PSI_CN and the band (phi, layer) and the module values
+ * DTCONST and the lica.in properties; writes MFLVS (nf+7 per column), SFGAS, SFGAS2
+ * (nf+2), IMASK_PH (n+2) and VOL_TOT_IPHS (vol_tot_iphs[ncol], in: the previous value);
+ * iterations[ncol] gets the TEMP_EXTP pseudo-time iterations.  status: LICA_OK,
+ * LICA_NOT_CONVERGED (TEMP_EXTP's retries ran out) or LICA_BAND_OVERFLOW.  The _device
+ * form takes scratch (NULL: the library's) of lica_gpu_column_scratch_bytes(ncol, n). */
+int lica_gpu_temp_grad(int32_t ncol, int32_t n, double length, const lica_col_props* props, double dtconst,
+                       const double* t, const double* psi_cn, const double* phi, const int32_t* layer, double* mflvs,
+                       double* sfgas, double* sfgas2, int32_t* imask, double* vol_tot_iphs, int32_t* iterations,
+                       int32_t* status);
+int lica_gpu_temp_grad_device(int32_t ncol, int32_t n, double length, const lica_col_props* props, double dtconst,
+                              const double* t, const double* psi_cn, const double* phi, const int32_t* layer,
+                              double* mflvs, double* sfgas, double* sfgas2, int32_t* imask, double* vol_tot_iphs,
+                              int32_t* iterations, int32_t* status, void* scratch, void* stream);
+
+/* PRESSURE_CORRECTION(U, V, W, P, DENF_Y, DENF_C, DENF_XI, DENF_YI, DENF_ZI) (1d.f:3403-3488;
+ * called from RHSNLHS, 1d.f:1589) of the 1-D column: DIVGS (3180-3303, with the
+ * phase-change source from SFGAS when props->iphs = 1, and DTCONST), POISSON (3492-3578),
+ * UCALC (3582-3627) and the shift P -= P(1,1,1) with the ghost copies.  W and P (n+2 per
+ * column) in place; DENF_ZI (n+2) and SFGAS (nf+2) read.  U, V, DENF_XI, DENF_YI, DENF_Y
+ * and DENF_C play no part in the 1-D column. */
+int lica_gpu_pressure_correction(int32_t ncol, int32_t n, double length, const lica_col_props* props, double dtconst,
+                                 double* w, double* p, const double* denf_zi, const double* sfgas);
+int lica_gpu_pressure_correction_device(int32_t ncol, int32_t n, double length, const lica_col_props* props,
+                                        double dtconst, double* w, double* p, const double* denf_zi,
+                                        const double* sfgas, int32_t* status, void* scratch, void* stream);
+
 /* ---------------------------------------------------------------- learned guess
  * Convolution primitive of the U-Net that supplies the multigrid initial guess (new; the
  * reference has no learned part): 3x3, stride 1, zero padding 1, NHWC BF16 activations,

@@ -1014,6 +1014,9 @@ __device__ void cal_continuity2(const Geo& g, const Phys& ph, Col& c) {
 
 // One substep of RHSNLHS (1d.f:1444-1600).  Returns the TEMP_EXTP iterations or a negative
 // lica_status.
+__device__ void pressure_correction(const Geo& g, const Phys& ph, Col& c, Shared& sh, double dtconst,
+                                    double dtconsti, const double* denf_zi);
+
 __device__ int rhsnlhs(const Geo& g, const Phys& ph, Col& c, Shared& sh, double L, int msub, int m_step) {
     const int n = g.n;
     const double dt = c.scal[0];
@@ -1134,11 +1137,21 @@ __device__ int rhsnlhs(const Geo& g, const Phys& ph, Col& c, Shared& sh, double 
         c.w[n + 1] = c.w[n + 1] + ubc_avg;
     }
     __syncthreads();
-    // FSM_CHOI (1d.f:3365-3400) and DIVGS (1d.f:3180-3303)
+    // FSM_CHOI (1d.f:3365-3400), then PRESSURE_CORRECTION
+    FOR_K(2, n) c.w[k] = c.w[k] + dtconst * ((c.p[k] - c.p[k - 1]) * g.vvdz(k)) * denf_zi[k];
+    __syncthreads();
+    pressure_correction(g, ph, c, sh, dtconst, dtconsti, denf_zi);
+    c.mark(PH_PRESS);
+    return iters;
+}
+
+// PRESSURE_CORRECTION (1d.f:3403-3488): DIVGS (3180-3303), POISSON (3492-3578), UCALC
+// (3582-3627) and the shift P -= P(1) with the ghost copies.  All threads call it.
+__device__ void pressure_correction(const Geo& g, const Phys& ph, Col& c, Shared& sh, double dtconst,
+                                    double dtconsti, const double* denf_zi) {
+    const int n = g.n;
     {
         double* divg = c.a[S_DIVG];
-        FOR_K(2, n) c.w[k] = c.w[k] + dtconst * ((c.p[k] - c.p[k - 1]) * g.vvdz(k)) * denf_zi[k];
-        __syncthreads();
         FOR_K(1, n) {
             double d = (k <= n - 1) ? (c.w[k + 1] - c.w[k]) * g.ssdz(k) : 0.0;
             if (ph.iphs == 1) {
@@ -1182,9 +1195,7 @@ __device__ int rhsnlhs(const Geo& g, const Phys& ph, Col& c, Shared& sh, double 
         __syncthreads();
         if (threadIdx.x == 0) c.p[0] = c.p[1];
         __syncthreads();
-        c.mark(PH_PRESS);
     }
-    return iters;
 }
 
 // One time step (1d.f:190-250).  Returns a lica_status.
@@ -1377,6 +1388,63 @@ __global__ void __launch_bounds__(NTH, NTH == 64 ? 5 : 1) k_column_steps(const _
         }
     }
     if (threadIdx.x == 0) A.status[col] = st;
+}
+
+// Single routines of the step on a batch of equal columns, for hosts that call the
+// reference's subroutines one at a time: the step kernel's own device code, one CTA per
+// column.
+enum { RT_TEMP_GRAD = 0, RT_PRESSURE_CORRECTION = 1 };
+
+struct RoutineArgs {
+    int ncol, n, routine;
+    double L, dtconst;
+    Phys ph;
+    double *w, *p, *t, *psi_cn, *phi, *mflvs, *sfgas, *sfgas2, *vol;
+    const double* denf_zi;
+    int *layer, *imask, *status, *iters;
+    double* dscr;   // NFLOW (n+2) + 2n+2 doubles per column
+};
+
+__global__ void __launch_bounds__(NT_DEFAULT, 1) k_col_routine(const __grid_constant__ RoutineArgs A) {
+    __shared__ Shared sh;
+    const int col = blockIdx.x;
+    if (col >= A.ncol) return;
+    const int n = A.n;
+    const size_t sf = (size_t)n + 2, sp = 2 * (size_t)n + 7, sq = 2 * (size_t)n + 2;
+    Col c{};
+    double* d = A.dscr + col * (NFLOW * sf + sq);
+    for (int q = 0; q < NFLOW; ++q) c.a[q] = d + q * sf;
+    c.psif_mtp = d + NFLOW * sf;
+    c.scal = c.a[S_SPARE4];   // VOL_TOT_IPHS in c.scal[4]
+    const Geo g(n, A.L);
+    if (A.routine == RT_TEMP_GRAD) {
+        c.t = A.t + col * sf;
+        c.psi_cn = A.psi_cn + col * sf;
+        c.phi = A.phi + col * sp;
+        c.layer = A.layer + col * sp;
+        c.mflvs = A.mflvs + col * sp;
+        c.sfgas = A.sfgas + col * sq;
+        c.sfgas2 = A.sfgas2 + col * sq;
+        c.imask = A.imask + col * sf;
+        if (threadIdx.x == 0) {
+            c.scal[4] = A.vol[col];
+            sh.dbuf[5] = 0.0;
+        }
+        __syncthreads();
+        const int it = temp_grad(g, A.ph, c, sh, A.L, A.dtconst);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            A.status[col] = it < 0 ? -it : LICA_OK;
+            A.iters[col] = it < 0 ? 0 : it;
+            A.vol[col] = c.scal[4];
+        }
+    } else {
+        c.w = A.w + col * sf;
+        c.p = A.p + col * sf;
+        c.sfgas = A.sfgas + col * sq;
+        pressure_correction(g, A.ph, c, sh, A.dtconst, 1. / A.dtconst, A.denf_zi + col * sf);
+        if (threadIdx.x == 0) A.status[col] = LICA_OK;
+    }
 }
 
 }  // namespace colk
@@ -1905,6 +1973,168 @@ int lica_gpu_column_steps(int32_t ncol, int32_t n, double length, const lica_col
     for (size_t c = 0; c < nc; ++c)
         if (status[c] != LICA_OK) worst = status[c];
     return worst;
+}
+
+// ---- single routines (drop-ins for the reference's subroutines, batches of columns)
+}  // extern "C"
+
+namespace {
+
+int routine_launch(colk::RoutineArgs& A, void* scratch, void* stream) {
+    void* scr = scratch;
+    if (!scr) {
+        const int rc = column_scratch(lica_gpu_column_scratch_bytes(A.ncol, A.n), &scr);
+        if (rc) return rc;
+    }
+    A.dscr = (double*)scr;
+    colk::k_col_routine<<<A.ncol, colk::NT_DEFAULT, 0, (cudaStream_t)stream>>>(A);
+    LICA_CUDA_TRY(cudaGetLastError());
+    lica_count_launches(1);
+    return LICA_OK;
+}
+
+// Device copies of host arrays for the host-array drop-ins; freed on scope exit.
+struct HostCopies {
+    std::vector<void*> ptrs;
+    ~HostCopies() {
+        for (void* p : ptrs) cudaFree(p);
+    }
+    template <typename T>
+    int in(T** d, const T* h, size_t n) {
+        void* p = nullptr;
+        LICA_CUDA_TRY(cudaMalloc(&p, sizeof(T) * n));
+        ptrs.push_back(p);
+        if (h) LICA_CUDA_TRY(cudaMemcpy(p, h, sizeof(T) * n, cudaMemcpyHostToDevice));
+        *d = (T*)p;
+        return LICA_OK;
+    }
+};
+
+template <typename T>
+int copy_out(T* h, const T* d, size_t n) {
+    LICA_CUDA_TRY(cudaMemcpy(h, d, sizeof(T) * n, cudaMemcpyDeviceToHost));
+    return LICA_OK;
+}
+
+int worst_status(const int32_t* status, int32_t ncol) {
+    int worst = LICA_OK;
+    for (int c = 0; c < ncol; ++c)
+        if (status[c] != LICA_OK) worst = status[c];
+    return worst;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lica_gpu_temp_grad_device(int32_t ncol, int32_t n, double length, const lica_col_props* props, double dtconst,
+                              const double* t, const double* psi_cn, const double* phi, const int32_t* layer,
+                              double* mflvs, double* sfgas, double* sfgas2, int32_t* imask, double* vol_tot_iphs,
+                              int32_t* iterations, int32_t* status, void* scratch, void* stream) {
+    if (ncol < 1 || n < 8 || n > (1 << 20) || !(length > 0.0) || !props || !(dtconst > 0.0) || !t || !psi_cn ||
+        !phi || !layer || !mflvs || !sfgas || !sfgas2 || !imask || !vol_tot_iphs || !iterations || !status) {
+        lica_set_last_error("lica_gpu_temp_grad_device", "bad sizes or null pointers", __FILE__, __LINE__);
+        return LICA_BAD_ARG;
+    }
+    colk::RoutineArgs A{};
+    A.ncol = ncol;
+    A.n = n;
+    A.routine = colk::RT_TEMP_GRAD;
+    A.L = length;
+    A.dtconst = dtconst;
+    A.ph = make_phys(props);
+    A.t = const_cast<double*>(t);
+    A.psi_cn = const_cast<double*>(psi_cn);
+    A.phi = const_cast<double*>(phi);
+    A.layer = const_cast<int32_t*>(layer);
+    A.mflvs = mflvs;
+    A.sfgas = sfgas;
+    A.sfgas2 = sfgas2;
+    A.imask = imask;
+    A.vol = vol_tot_iphs;
+    A.iters = iterations;
+    A.status = status;
+    return routine_launch(A, scratch, stream);
+}
+
+int lica_gpu_temp_grad(int32_t ncol, int32_t n, double length, const lica_col_props* props, double dtconst,
+                       const double* t, const double* psi_cn, const double* phi, const int32_t* layer, double* mflvs,
+                       double* sfgas, double* sfgas2, int32_t* imask, double* vol_tot_iphs, int32_t* iterations,
+                       int32_t* status) {
+    if (ncol < 1 || n < 8 || n > (1 << 20) || !t || !psi_cn || !phi || !layer || !mflvs || !sfgas || !sfgas2 ||
+        !imask || !vol_tot_iphs || !iterations || !status) {
+        lica_set_last_error("lica_gpu_temp_grad", "bad sizes or null pointers", __FILE__, __LINE__);
+        return LICA_BAD_ARG;
+    }
+    const size_t nc = (size_t)ncol, sf = (size_t)n + 2, sp = 2 * (size_t)n + 7, sq = 2 * (size_t)n + 2;
+    HostCopies H;
+    double *dt_, *dcn, *dphi, *dmf, *dsf, *dsf2, *dvol;
+    int32_t *dlay, *dim, *dit, *dst;
+    int rc;
+    if ((rc = H.in(&dt_, t, nc * sf)) || (rc = H.in(&dcn, psi_cn, nc * sf)) || (rc = H.in(&dphi, phi, nc * sp)) ||
+        (rc = H.in(&dlay, layer, nc * sp)) || (rc = H.in(&dmf, (const double*)nullptr, nc * sp)) ||
+        (rc = H.in(&dsf, (const double*)nullptr, nc * sq)) || (rc = H.in(&dsf2, (const double*)nullptr, nc * sq)) ||
+        (rc = H.in(&dim, (const int32_t*)nullptr, nc * sf)) || (rc = H.in(&dvol, vol_tot_iphs, nc)) ||
+        (rc = H.in(&dit, (const int32_t*)nullptr, nc)) || (rc = H.in(&dst, (const int32_t*)nullptr, nc)))
+        return rc;
+    if ((rc = lica_gpu_temp_grad_device(ncol, n, length, props, dtconst, dt_, dcn, dphi, dlay, dmf, dsf, dsf2, dim,
+                                        dvol, dit, dst, nullptr, nullptr)))
+        return rc;
+    LICA_CUDA_TRY(cudaDeviceSynchronize());
+    if ((rc = copy_out(mflvs, dmf, nc * sp)) || (rc = copy_out(sfgas, dsf, nc * sq)) ||
+        (rc = copy_out(sfgas2, dsf2, nc * sq)) || (rc = copy_out(imask, dim, nc * sf)) ||
+        (rc = copy_out(vol_tot_iphs, dvol, nc)) || (rc = copy_out(iterations, dit, nc)) ||
+        (rc = copy_out(status, dst, nc)))
+        return rc;
+    return worst_status(status, ncol);
+}
+
+int lica_gpu_pressure_correction_device(int32_t ncol, int32_t n, double length, const lica_col_props* props,
+                                        double dtconst, double* w, double* p, const double* denf_zi,
+                                        const double* sfgas, int32_t* status, void* scratch, void* stream) {
+    if (ncol < 1 || n < 8 || n > (1 << 20) || !(length > 0.0) || !props || !(dtconst > 0.0) || !w || !p ||
+        !denf_zi || !sfgas || !status) {
+        lica_set_last_error("lica_gpu_pressure_correction_device", "bad sizes or null pointers", __FILE__, __LINE__);
+        return LICA_BAD_ARG;
+    }
+    colk::RoutineArgs A{};
+    A.ncol = ncol;
+    A.n = n;
+    A.routine = colk::RT_PRESSURE_CORRECTION;
+    A.L = length;
+    A.dtconst = dtconst;
+    A.ph = make_phys(props);
+    A.w = w;
+    A.p = p;
+    A.denf_zi = denf_zi;
+    A.sfgas = const_cast<double*>(sfgas);
+    A.status = status;
+    return routine_launch(A, scratch, stream);
+}
+
+int lica_gpu_pressure_correction(int32_t ncol, int32_t n, double length, const lica_col_props* props, double dtconst,
+                                 double* w, double* p, const double* denf_zi, const double* sfgas) {
+    if (ncol < 1 || n < 8 || n > (1 << 20) || !w || !p || !denf_zi || !sfgas) {
+        lica_set_last_error("lica_gpu_pressure_correction", "bad sizes or null pointers", __FILE__, __LINE__);
+        return LICA_BAD_ARG;
+    }
+    const size_t nc = (size_t)ncol, sf = (size_t)n + 2, sq = 2 * (size_t)n + 2;
+    HostCopies H;
+    double *dw, *dp, *dden, *dsf;
+    int32_t* dst;
+    int rc;
+    if ((rc = H.in(&dw, (const double*)w, nc * sf)) || (rc = H.in(&dp, (const double*)p, nc * sf)) ||
+        (rc = H.in(&dden, denf_zi, nc * sf)) || (rc = H.in(&dsf, sfgas, nc * sq)) ||
+        (rc = H.in(&dst, (const int32_t*)nullptr, nc)))
+        return rc;
+    if ((rc = lica_gpu_pressure_correction_device(ncol, n, length, props, dtconst, dw, dp, dden, dsf, dst, nullptr,
+                                                  nullptr)))
+        return rc;
+    LICA_CUDA_TRY(cudaDeviceSynchronize());
+    if ((rc = copy_out(w, (const double*)dw, nc * sf)) || (rc = copy_out(p, (const double*)dp, nc * sf))) return rc;
+    std::vector<int32_t> st(nc);
+    if ((rc = copy_out(st.data(), (const int32_t*)dst, nc))) return rc;
+    return worst_status(st.data(), ncol);
 }
 
 }  // extern "C"

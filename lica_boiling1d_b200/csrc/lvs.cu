@@ -45,6 +45,77 @@ __global__ void __launch_bounds__(32 * WARPS)
     if (lane == 0) status[col] = st;
 }
 
+// REINITIALIZATION(NN1, NN2, ILIMIT) (two_phase.f:2033-2474) of one column per warp: ILIMIT
+// SSP-RK3 pseudo-time iterations on band layers 1..NN2 (WENO on 1..NN1); ALPHI_EXT is the
+// caller's phi array (the reference's call sites hold it zero off the band); only the
+// cells of layers 1..NN2 are written.
+__global__ void __launch_bounds__(32 * WARPS)
+    k_reinitialization(int ncol, int n, double length, double* __restrict__ phi, const int* __restrict__ layer,
+                       int ilimit, int* __restrict__ status) {
+    __shared__ Win win[WARPS];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int col = blockIdx.x * WARPS + warp;
+    if (col >= ncol) return;
+    const size_t sp = 2 * (size_t)n + 7;
+    double* ph = phi + col * sp;
+    Ctx c;
+    c.s = &win[warp];
+    const int st = load_band_window(c, lane, n, length, ph, layer + col * sp, false);
+    if (st == LICA_OK) {
+        reinitialization(c, ilimit);
+        for (int i = c.blo + lane; i <= c.bhi; i += 32) {
+            const int m = c.s->layer[i];
+            if (m >= 1 && m <= NN2) ph[c.w0 + i + 2] = c.s->phi[i];
+        }
+    }
+    if (lane == 0) status[col] = st;
+}
+
+// GRID_COUPLING(INI_PSI) (two_phase.f:4863-5118) of one column per CTA.  ini = 1: every flow
+// cell; ini = 0: the flow cells KCOUMP_VEL(k) of the refined cells of band layers 1..NN1
+// (MASK_GLOBAL) -- the cells k = 2K-4 .. 2K+5 are the only ones that can map to flow cell
+// K.  PSI_ZN(K), K >= 2: box mean of PSIF over [ZP(K-1), ZP(K)]; PSI_CN(K) over [Z(K),
+// Z(K+1)]; every cell snapped at 1e-3 / 0.999; PSI_CN(0) = PSI_CN(1), PSI_CN(n+1) = PSI_CN(n).
+__global__ void __launch_bounds__(128)
+    k_grid_coupling(int ncol, int n, double length, int ini, const double* __restrict__ psif,
+                    const int* __restrict__ layer, double* __restrict__ psi_cn, double* __restrict__ psi_zn) {
+    const int col = blockIdx.x;
+    if (col >= ncol) return;
+    const int nf = 2 * n;
+    const double h = length / n, hf = length / nf;
+    const double* pf = psif + col * (size_t)(nf + 2);
+    const int* lay = layer + col * (size_t)(nf + 7);
+    double* cn = psi_cn + col * (size_t)(n + 2);
+    double* zn = psi_zn + col * (size_t)(n + 2);
+    for (int kk = 1 + (int)threadIdx.x; kk <= n; kk += (int)blockDim.x) {
+        bool mk = ini != 0;
+        if (!mk)
+            for (int k = max(1, 2 * kk - 4); k <= min(nf, 2 * kk + 5); ++k) {
+                const int m = lay[k + 2];
+                if (m >= 1 && m <= NN1 && col::kcoump_vel(h, hf, n, k) == kk) {
+                    mk = true;
+                    break;
+                }
+            }
+        double z = zn[kk];
+        if (kk >= 2 && mk) z = col::box_mean(pf, nf, 2 * kk - 2, 2 * kk - 1, col::grid_zp(h, n, kk - 1),
+                                             col::grid_zp(h, n, kk), hf);
+        if (z < 1e-3) z = 0.0;
+        else if (z > 0.999) z = 1.0;
+        zn[kk] = z;
+        double v = cn[kk];
+        if (mk) v = col::box_mean(pf, nf, 2 * kk - 1, 2 * kk, col::grid_z(h, kk), col::grid_z(h, kk + 1), hf);
+        if (v < 1e-3) v = 0.0;
+        else if (v > 0.999) v = 1.0;
+        cn[kk] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        cn[0] = cn[1];
+        cn[n + 1] = cn[n];
+    }
+}
+
 }  // namespace lvs
 }  // namespace lica
 
@@ -153,6 +224,102 @@ int lica_gpu_lvs_transport(int32_t ncol, int32_t n, double length, double* phi, 
     for (size_t c = 0; c < nc; ++c)
         if (status[c] != LICA_OK) worst = status[c];
     return worst;
+}
+
+int lica_gpu_reinitialization_device(int32_t ncol, int32_t n, double length, double* phi, const int32_t* layer,
+                                     int32_t ilimit, int32_t* status, void* stream) {
+    if (ncol < 1 || n < 8 || n > (1 << 24) || !(length > 0.0) || !phi || !layer || ilimit < 0 || !status) {
+        lica_set_last_error("lica_gpu_reinitialization_device", "bad sizes or null pointers", __FILE__, __LINE__);
+        return LICA_BAD_ARG;
+    }
+    const unsigned blocks = (unsigned)((ncol + WARPS - 1) / WARPS);
+    k_reinitialization<<<blocks, 32 * WARPS, 0, (cudaStream_t)stream>>>(ncol, n, length, phi, layer, ilimit, status);
+    LICA_CUDA_TRY(cudaGetLastError());
+    lica_count_launches(1);
+    return LICA_OK;
+}
+
+int lica_gpu_reinitialization(int32_t ncol, int32_t n, double length, double* phi, const int32_t* layer,
+                              int32_t ilimit, int32_t* status) {
+    if (ncol < 1 || n < 8 || n > (1 << 24) || !(length > 0.0) || !phi || !layer || ilimit < 0 || !status) {
+        lica_set_last_error("lica_gpu_reinitialization", "bad sizes or null pointers", __FILE__, __LINE__);
+        return LICA_BAD_ARG;
+    }
+    const size_t nc = (size_t)ncol, sp = 2 * (size_t)n + 7;
+    double* dphi = nullptr;
+    int32_t *dlay = nullptr, *dst = nullptr;
+    int rc = LICA_OK;
+    auto done = [&](int code) {
+        cudaFree(dphi);
+        cudaFree(dlay);
+        cudaFree(dst);
+        return code;
+    };
+    if (cudaMalloc((void**)&dphi, 8 * nc * sp) != cudaSuccess || cudaMalloc((void**)&dlay, 4 * nc * sp) != cudaSuccess ||
+        cudaMalloc((void**)&dst, 4 * nc) != cudaSuccess) {
+        lica_set_last_error("cudaMalloc", "lica_gpu_reinitialization buffers", __FILE__, __LINE__);
+        return done(LICA_ERR_NOMEM);
+    }
+    if (cudaMemcpy(dphi, phi, 8 * nc * sp, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dlay, layer, 4 * nc * sp, cudaMemcpyHostToDevice) != cudaSuccess)
+        return done(LICA_ERR_CUDA);
+    if ((rc = lica_gpu_reinitialization_device(ncol, n, length, dphi, dlay, ilimit, dst, nullptr))) return done(rc);
+    if (cudaMemcpy(phi, dphi, 8 * nc * sp, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(status, dst, 4 * nc, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return done(LICA_ERR_CUDA);
+    int worst = LICA_OK;
+    for (size_t c = 0; c < nc; ++c)
+        if (status[c] != LICA_OK) worst = status[c];
+    return done(worst);
+}
+
+int lica_gpu_grid_coupling_device(int32_t ncol, int32_t n, double length, int32_t ini_psi, const double* psif,
+                                  const int32_t* layer, double* psi_cn, double* psi_zn, void* stream) {
+    if (ncol < 1 || n < 8 || n > (1 << 24) || !(length > 0.0) || !psif || !psi_cn || !psi_zn ||
+        (ini_psi == 0 && !layer)) {
+        lica_set_last_error("lica_gpu_grid_coupling_device", "bad sizes or null pointers", __FILE__, __LINE__);
+        return LICA_BAD_ARG;
+    }
+    k_grid_coupling<<<ncol, 128, 0, (cudaStream_t)stream>>>(ncol, n, length, ini_psi, psif, layer, psi_cn, psi_zn);
+    LICA_CUDA_TRY(cudaGetLastError());
+    lica_count_launches(1);
+    return LICA_OK;
+}
+
+int lica_gpu_grid_coupling(int32_t ncol, int32_t n, double length, int32_t ini_psi, const double* psif,
+                           const int32_t* layer, double* psi_cn, double* psi_zn) {
+    if (ncol < 1 || n < 8 || n > (1 << 24) || !(length > 0.0) || !psif || !psi_cn || !psi_zn ||
+        (ini_psi == 0 && !layer)) {
+        lica_set_last_error("lica_gpu_grid_coupling", "bad sizes or null pointers", __FILE__, __LINE__);
+        return LICA_BAD_ARG;
+    }
+    const size_t nc = (size_t)ncol, sp = 2 * (size_t)n + 7, sq = 2 * (size_t)n + 2, sf = (size_t)n + 2;
+    double *dpf = nullptr, *dcn = nullptr, *dzn = nullptr;
+    int32_t* dlay = nullptr;
+    auto done = [&](int code) {
+        cudaFree(dpf);
+        cudaFree(dcn);
+        cudaFree(dzn);
+        cudaFree(dlay);
+        return code;
+    };
+    if (cudaMalloc((void**)&dpf, 8 * nc * sq) != cudaSuccess || cudaMalloc((void**)&dcn, 8 * nc * sf) != cudaSuccess ||
+        cudaMalloc((void**)&dzn, 8 * nc * sf) != cudaSuccess ||
+        (layer && cudaMalloc((void**)&dlay, 4 * nc * sp) != cudaSuccess)) {
+        lica_set_last_error("cudaMalloc", "lica_gpu_grid_coupling buffers", __FILE__, __LINE__);
+        return done(LICA_ERR_NOMEM);
+    }
+    if (cudaMemcpy(dpf, psif, 8 * nc * sq, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dcn, psi_cn, 8 * nc * sf, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dzn, psi_zn, 8 * nc * sf, cudaMemcpyHostToDevice) != cudaSuccess ||
+        (layer && cudaMemcpy(dlay, layer, 4 * nc * sp, cudaMemcpyHostToDevice) != cudaSuccess))
+        return done(LICA_ERR_CUDA);
+    int rc = lica_gpu_grid_coupling_device(ncol, n, length, ini_psi, dpf, dlay, dcn, dzn, nullptr);
+    if (rc) return done(rc);
+    if (cudaMemcpy(psi_cn, dcn, 8 * nc * sf, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(psi_zn, dzn, 8 * nc * sf, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return done(LICA_ERR_CUDA);
+    return done(LICA_OK);
 }
 
 }  // extern "C"

@@ -152,7 +152,10 @@ __device__ inline void lists_to_layer(Ctx& c) {
 // rule as TRANSPORT, phi = band values and 0 elsewhere (ghosts included: TEMP_GRAD builds
 // ALPHI_EXT from the band alone, chphase.f:121-139), ascending band lists.  Returns
 // LICA_OK, LICA_BAD_ARG (band cell outside k = 1..nf) or LICA_BAND_OVERFLOW.
-__device__ inline int load_band_window(Ctx& c, int lane, int n, double length, const double* phi, const int* layer) {
+// band_only = false: every window cell takes the caller's phi (the drop-in REINITIALIZATION,
+// whose stencils read ALPHI_EXT as the caller holds it).
+__device__ inline int load_band_window(Ctx& c, int lane, int n, double length, const double* phi, const int* layer,
+                                       bool band_only = true) {
     Win* s = c.s;
     c.n = n;
     c.nf = 2 * n;
@@ -183,7 +186,7 @@ __device__ inline int load_band_window(Ctx& c, int lane, int n, double length, c
         const bool ok = (k >= -2 && k <= nf + 4);
         const int m = ok ? layer[k + 2] : 0;
         s->layer[i] = m;
-        s->phi[i] = (ok && m > 0) ? phi[k + 2] : 0.0;
+        s->phi[i] = (ok && (m > 0 || !band_only)) ? phi[k + 2] : 0.0;
     }
     __syncwarp();
     build_lists(c);

@@ -119,6 +119,19 @@ SIGNATURES = {
                                                      C.c_void_p, C.c_void_p, C.c_void_p]),
     "lica_gpu_column_steps": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.POINTER(ColProps), C.POINTER(ColState),
                                         C.c_int32, _I32]),
+    "lica_gpu_reinitialization": (C.c_int, [C.c_int32, C.c_int32, C.c_double, _D, _I32, C.c_int32, _I32]),
+    "lica_gpu_reinitialization_device": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_void_p, C.c_void_p,
+                                                   C.c_int32, C.c_void_p, C.c_void_p]),
+    "lica_gpu_grid_coupling": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_int32, _D, _I32, _D, _D]),
+    "lica_gpu_grid_coupling_device": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_int32] + [C.c_void_p] * 5),
+    "lica_gpu_temp_grad": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.POINTER(ColProps), C.c_double, _D, _D, _D,
+                                     _I32, _D, _D, _D, _I32, _D, _I32, _I32]),
+    "lica_gpu_temp_grad_device": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.POINTER(ColProps), C.c_double] +
+                                  [C.c_void_p] * 13),
+    "lica_gpu_pressure_correction": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.POINTER(ColProps), C.c_double,
+                                               _D, _D, _D, _D]),
+    "lica_gpu_pressure_correction_device": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.POINTER(ColProps),
+                                                      C.c_double] + [C.c_void_p] * 7),
     "lica_unet_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.c_int32, C.c_uint64]),
     "lica_unet_destroy": (C.c_int, [C.c_void_p]),
     "lica_unet_param_count": (C.c_int64, [C.c_void_p]),

@@ -1008,6 +1008,41 @@ int orc_col_step(int n, double L, const double* props, const int* iprops, double
     return 0;
 }
 
+// TEMP_GRAD (chphase.f:55-368, with TEMP_EXTP, TF_GRAD and VOL_TOT_MFDOT) of one column as a
+// single routine: reads T, PSI_CN and the band (phi, layer); writes MFLVS, SFGAS, SFGAS2,
+// IMASK_PH and VOL_TOT_IPHS (*vol).  Returns the TEMP_EXTP iterations, or -1 when it did
+// not converge.
+int orc_col_temp_grad(int n, double L, const double* props, const int* iprops, double dtconst, const double* t,
+                      const double* psi_cn, const double* phi, const int* layer, double* mflvs, double* sfgas,
+                      double* sfgas2, int* imask, double* vol) {
+    const ColProps cp = props_of(props, iprops);
+    const Phys ph(cp);
+    Geo g(n, L);
+    std::vector<double> tv(t, t + n + 2), cn(psi_cn, psi_cn + n + 2), pv(phi, phi + 2 * n + 7);
+    std::vector<int> lv(layer, layer + 2 * n + 7);
+    double scal[5] = {0.0, 0.0, 0.0, 0.0, *vol};
+    ColView s = view(n, L, nullptr, nullptr, tv.data(), cn.data(), nullptr, pv.data(), lv.data(), nullptr, nullptr,
+                     mflvs, sfgas, sfgas2, imask, scal);
+    const int it = temp_grad(g, L, ph, s, dtconst);
+    *vol = scal[4];
+    return it;
+}
+
+// PRESSURE_CORRECTION (1d.f:3403-3488: DIVGS, POISSON, UCALC, the shift by P(1)) of one
+// column as a single routine: W and P in place; DENF_ZI and (IPHS = 1) SFGAS read.
+int orc_col_pressure_correction(int n, double L, const double* props, const int* iprops, double dtconst, double* w,
+                                double* p, const double* denf_zi, const double* sfgas) {
+    const ColProps cp = props_of(props, iprops);
+    const Phys ph(cp);
+    Geo g(n, L);
+    ColView s = view(n, L, w, p, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                     const_cast<double*>(sfgas), nullptr, nullptr, nullptr);
+    Work wk(n);
+    for (int k = 0; k <= n + 1; ++k) wk.denf_zi[k] = denf_zi[k];
+    pressure_correction(g, s, dtconst, 1. / dtconst, wk, ph);
+    return 0;
+}
+
 // The record the reference appends to 0interface.dat at the end of the last substep of a
 // step (chphase.f:1432-1438, TIME before MAIN adds DT at 1d.f:260) for the step just taken
 // by orc_col_step on this thread: place of VOL_TOT_MFDOT in the third substep (0 when the

@@ -240,4 +240,29 @@ int orc_lvs_reinit(int n, double L, double* phi, const int* layer, int ilimit) {
     return 0;
 }
 
+// REINITIALIZATION(NN1, NN2, ILIMIT) (two_phase.f:2033-2474) of one column as a single
+// routine: ALPHI_EXT is the caller's phi array (every cell, ghosts included), the band
+// the cells whose layer is 1..N_MAX (ascending k per layer); ILIMIT SSP-RK3 iterations on
+// layers 1..NN2.  Only the band cells are written back.
+int orc_reinitialization(int n, double L, double* phi, const int* layer, int ilimit) {
+    Col c;
+    c.init(n, L);
+    for (int k = -2; k <= c.nf + 4; ++k) c.phi[k + GL] = phi[k + GL];
+    for (int m = 1; m <= N_MAX; ++m)
+        for (int k = -2; k <= c.nf + 4; ++k)
+            if (layer[k + GL] == m) c.band[m].push_back(k);
+    c.rebuild_layer();
+    reinitialization(c, ilimit);
+    for (int m = 1; m <= N_MAX; ++m)
+        for (int k : c.band[m]) phi[k + GL] = c.p(k);
+    return 0;
+}
+
+// GRID_COUPLING(INI_PSI) (two_phase.f:4863-5118) of one column as a single routine.
+int orc_grid_coupling(int n, double L, int ini, const double* psif, const int* layer, double* psi_cn,
+                      double* psi_zn) {
+    grid_coupling(n, L, psif, layer, ini, psi_cn, psi_zn);
+    return 0;
+}
+
 }  // extern "C"

@@ -42,6 +42,11 @@ def lib(native: bool = False):
         L.orc_col_step.argtypes = [C.c_int, C.c_double, _D, _INT] + [_D] * 6 + [_INT] + [_D] * 5 + [_INT, _D, _D]
         L.orc_col_last_place.restype = C.c_double
         L.orc_col_last_place.argtypes = []
+        L.orc_reinitialization.argtypes = [C.c_int, C.c_double, _D, _INT, C.c_int]
+        L.orc_grid_coupling.argtypes = [C.c_int, C.c_double, C.c_int, _D, _INT, _D, _D]
+        L.orc_col_temp_grad.argtypes = [C.c_int, C.c_double, _D, _INT, C.c_double, _D, _D, _D, _INT, _D, _D, _D,
+                                        _INT, _D]
+        L.orc_col_pressure_correction.argtypes = [C.c_int, C.c_double, _D, _INT, C.c_double, _D, _D, _D, _D]
         _LIBS[key] = L
     return _LIBS[key]
 
@@ -247,3 +252,40 @@ def col_history_record(st, time_before, native=False):
     thread: (TIME before the step, place of 0interface.dat (chphase.f:1419-1438), the vapour
     volume VOL_TOT_IPHS (chphase.f:1457), DT)."""
     return (time_before, lib(native).orc_col_last_place(), float(st["scal"][4]), float(st["scal"][0]))
+
+
+# ---------------------------------------------------------------------------------------
+# Single routines of the column step (the per-subroutine drop-ins' checkers)
+# ---------------------------------------------------------------------------------------
+def reinitialization(n, length, phi, layer, ilimit):
+    """REINITIALIZATION (two_phase.f:2033-2474) of one column: phi (nf+7) in place."""
+    lib().orc_reinitialization(n, length, _p(phi), _pi(layer), int(ilimit))
+    return phi
+
+
+def grid_coupling(n, length, ini, psif, layer, psi_cn, psi_zn):
+    """GRID_COUPLING(INI_PSI) (two_phase.f:4863-5118) of one column: psi_cn, psi_zn in place."""
+    lib().orc_grid_coupling(n, length, int(ini), _p(psif), _pi(layer), _p(psi_cn), _p(psi_zn))
+    return psi_cn, psi_zn
+
+
+def col_temp_grad(n, length, props, dtconst, t, psi_cn, phi, layer, vol):
+    """TEMP_GRAD (chphase.f:55-368) of one column: returns (iterations, mflvs, sfgas, sfgas2,
+    imask, VOL_TOT_IPHS); iterations -1 when TEMP_EXTP did not converge."""
+    pr, ip = _col_props(props)
+    nf = 2 * n
+    mflvs, sfgas, sfgas2 = np.zeros(nf + 7), np.zeros(nf + 2), np.zeros(nf + 2)
+    imask = np.zeros(n + 2, np.int32)
+    v = np.array([float(vol)])
+    it = lib().orc_col_temp_grad(n, length, _p(pr), _pi(ip), float(dtconst), _p(np.ascontiguousarray(t)),
+                                 _p(np.ascontiguousarray(psi_cn)), _p(np.ascontiguousarray(phi)),
+                                 _pi(np.ascontiguousarray(layer)), _p(mflvs), _p(sfgas), _p(sfgas2), _pi(imask), _p(v))
+    return it, mflvs, sfgas, sfgas2, imask, float(v[0])
+
+
+def col_pressure_correction(n, length, props, dtconst, w, p, denf_zi, sfgas):
+    """PRESSURE_CORRECTION (1d.f:3403-3488) of one column: w, p in place."""
+    pr, ip = _col_props(props)
+    lib().orc_col_pressure_correction(n, length, _p(pr), _pi(ip), float(dtconst), _p(w), _p(p),
+                                      _p(np.ascontiguousarray(denf_zi)), _p(np.ascontiguousarray(sfgas)))
+    return w, p
