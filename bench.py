@@ -370,34 +370,59 @@ def film_leg(dev, flush, steps=10, warmup=2, compare=True):
                        "above 1e-10: LICA_STALLED) + 2 reinitialisation iterations, FP64 physics",
            "dt": dt, "inputs_vs_l2": "state and scratch (about 220 MB) larger than L2, plus a 256 MiB flush"}
     first = {}
-    for prec in ("fp64", "mixed"):
+    net = None
+    from lica_boiling1d_b200 import train_guess
+    arms = ["fp64", "mixed"]
+    if os.path.exists(train_guess.FILM_WEIGHTS):
+        from lica_boiling1d_b200.unet import LearnedGuess
+        net = LearnedGuess(1, ny, nx)
+        train_guess.load(net, train_guess.FILM_WEIGHTS)
+        arms.append("mixed_learned")
+    for arm in arms:
+        prec = "fp64" if arm == "fp64" else "mixed"
         gpu = G.Film2D(nx, ny, P, precision=prec)
+        if arm == "mixed_learned":
+            gpu.set_guess(net)
         state = G.to_device(st0)
         gpu.step(state, dt)
         torch.cuda.synchronize(dev)
-        first[prec] = G.to_host(state)
+        first[arm] = G.to_host(state)
         for _ in range(warmup):
             gpu.step(state, dt)
         torch.cuda.synchronize(dev)
         flush.fill_(7)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         l0 = native.launch_count()
-        its, rels, stats = [], [], []
+        its, rels, stats, grels = [], [], [], []
         e0.record()
         for _ in range(steps):
             inf = gpu.step(state, dt)
             its.append(inf["iterations"])
             rels.append(inf["rel"])
             stats.append(inf["status"])
+            grels.append(inf["guess_rel"])
         e1.record()
         torch.cuda.synchronize(dev)
         ms = e0.elapsed_time(e1)
         gpu.close()
-        out[prec] = {"steps_per_s": steps / (ms / 1e3), "ms_per_step": ms / steps, "steps": steps,
-                     "flow_cell_updates_per_s": nx * ny * steps / (ms / 1e3),
-                     "ls_cell_updates_per_s": 4 * nx * ny * steps / (ms / 1e3),
-                     "mg_iterations_per_substep": its[-1], "mg_rel_residual_per_substep": rels[-1],
-                     "mg_status_per_substep": stats[-1], "gpu_launches": native.launch_count() - l0}
+        out[arm] = {"steps_per_s": steps / (ms / 1e3), "ms_per_step": ms / steps, "steps": steps,
+                    "flow_cell_updates_per_s": nx * ny * steps / (ms / 1e3),
+                    "ls_cell_updates_per_s": 4 * nx * ny * steps / (ms / 1e3),
+                    "mg_iterations_per_substep": its[-1], "mg_rel_residual_per_substep": rels[-1],
+                    "mg_status_per_substep": stats[-1], "gpu_launches": native.launch_count() - l0}
+        if arm == "mixed_learned":
+            out[arm]["guess_rel_per_substep"] = grels[-1]
+            out[arm]["mean_iterations_saved_vs_mixed"] = float(np.mean(out["mixed"]["_its"]) - np.mean(its))
+            out[arm]["note"] = ("mixed-precision MG-PCG started from the U-Net guess trained on the film's own "
+                                "(density, rhs -> increment) pairs; zero where the guess is no better")
+        out[arm]["_its"] = its
+    if net is not None:
+        net.close()
+    for arm in arms:
+        out[arm].pop("_its", None)
+    out["ratio_mixed_learned_vs_fp64"] = (out["mixed_learned"]["steps_per_s"] / out["fp64"]["steps_per_s"]
+                                          if "mixed_learned" in out else None)
+    out["ratio_mixed_vs_fp64"] = out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"]
     if compare:
         from oracle import film2d as F
         F.step_native(G.initial_state(64, 192, 8.0, 2.0, props=P), G.stable_dt(64, P), P, 3)  # load the library
@@ -405,9 +430,9 @@ def film_leg(dev, flush, steps=10, warmup=2, compare=True):
         ref, info = F.step_native(st0, dt, P, G.levels_for(nx, ny))
         cpu_s = time.perf_counter() - t0
         errs = {}
-        for prec in ("fp64", "mixed"):
-            errs[prec] = {k: float(np.linalg.norm(first[prec][k] - ref[k]) / max(np.linalg.norm(ref[k]), 1e-300))
-                          for k in ref}
+        for arm in arms:
+            errs[arm] = {k: float(np.linalg.norm(first[arm][k] - ref[k]) / max(np.linalg.norm(ref[k]), 1e-300))
+                         for k in ref}
         out["rel_l2_error_vs_fp64_oracle"] = errs
         out["oracle_mg_iterations"] = info["iterations"]
         out["cpu_baseline"] = {"steps_per_s": 1.0 / cpu_s, "kind": "port", "cores": os.cpu_count(),

@@ -139,6 +139,7 @@ module lica_gpu
     integer(c_int32_t) :: iterations(3)
     integer(c_int32_t) :: status(3)
     real(c_double) :: rel_residual(3)
+    real(c_double) :: guess_rel(3)
   end type lica_film2d_stats
 
   interface
@@ -847,5 +848,19 @@ module lica_gpu
       type(c_ptr), value :: out
       type(c_ptr), value :: stream
     end function lica_film2d_mdot_device
+
+    integer(c_int) function lica_film2d_set_guess(film, net) &
+        bind(c, name="lica_film2d_set_guess")
+      import
+      type(c_ptr), value :: film
+      type(c_ptr), value :: net
+    end function lica_film2d_set_guess
+
+    integer(c_int) function lica_film2d_capture_device(film, systems) &
+        bind(c, name="lica_film2d_capture_device")
+      import
+      type(c_ptr), value :: film
+      type(c_ptr), value :: systems
+    end function lica_film2d_capture_device
   end interface
 end module lica_gpu

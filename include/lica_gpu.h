@@ -543,6 +543,8 @@ typedef struct {
     int32_t iterations[3];  /* pressure-solve iterations of each substep */
     int32_t status[3];
     double rel_residual[3];
+    double guess_rel[3];    /* ||f - A x0|| / ||f|| of the learned guess each solve started
+                               from (1 without a guess, or when the guess fell back to zero) */
 } lica_film2d_stats;
 
 int lica_film2d_create(lica_film2d** out, int32_t nx, int32_t ny, const lica_film2d_props* props,
@@ -552,6 +554,17 @@ int lica_film2d_step_device(lica_film2d* film, double* u, double* v, double* p, 
                             lica_film2d_stats* stats, void* stream);
 /* Copies the interfacial mass flux per cell of the last substep into out (device, ny x nx). */
 int lica_film2d_mdot_device(lica_film2d* film, double* out, void* stream);
+/* The learned initial guess of the three pressure solves (new; no counterpart in the
+ * reference): net, a U-Net of one ny x nx image (lica_unet_create(&net, 1, ny, nx, ...)),
+ * predicts each increment from the substep's density and right-hand side; a guess no
+ * better than zero is replaced by zero, and the solve keeps its own tolerance.  NULL
+ * detaches it.  The film step does not own net. */
+int lica_film2d_set_guess(lica_film2d* film, lica_unet* net);
+/* Training pairs from the film's own solves: while systems (device) is set, every step
+ * writes for substep k = 0..2, at systems + k (4 nx ny + (ny + 1) nx): the density (ny x nx),
+ * the right-hand side f, bx (ny x nx), by ((ny + 1) x nx) and the solved increment dp.  NULL
+ * turns it off. */
+int lica_film2d_capture_device(lica_film2d* film, double* systems);
 
 #ifdef __cplusplus
 }

@@ -471,6 +471,9 @@ struct lica_film2d {
            *mdot = nullptr, *th2 = nullptr, *dp = nullptr, *kap = nullptr;
     // refined-grid scratch
     double *rphi = nullptr, *ph[3] = {nullptr, nullptr, nullptr};
+    // optional learned initial guess of the pressure solves, and the training-pair capture
+    lica_unet* guess = nullptr;
+    double* capture = nullptr;
 };
 
 namespace {
@@ -574,8 +577,17 @@ int lica_film2d_step_device(lica_film2d* F, double* u, double* v, double* p, dou
         k_source_rhs<<<gflow, blk, 0, s>>>(thc, F->psi, F->tc, F->us, F->vs, F->f, F->mdot, iadt, c);
         LICA_CUDA_TRY(cudaGetLastError());
         launches += 5;
-        // the pressure increment, from zero
-        LICA_CUDA_TRY(cudaMemsetAsync(F->dp, 0, n * sizeof(double), s));
+        // the pressure increment, from the learned guess (zero if it is no better) or zero
+        local.guess_rel[k - 1] = 1.0;
+        if (F->guess) {
+            double rel0 = 1.0;
+            const int gs = lica_unet_guess_checked_device(F->guess, F->den, F->f, F->bx, F->by, c.h, c.h, F->dp,
+                                                          &rel0, s);
+            if (gs != LICA_OK) return gs;
+            local.guess_rel[k - 1] = rel0 < 1.0 ? rel0 : 1.0;
+        } else {
+            LICA_CUDA_TRY(cudaMemsetAsync(F->dp, 0, n * sizeof(double), s));
+        }
         lica_mg_result r{};
         const int st =
             lica_mg_solve_device(F->mg, F->dp, F->f, F->bx, F->by, F->props.rtol, F->props.max_iters, &r, s);
@@ -583,6 +595,15 @@ int lica_film2d_step_device(lica_film2d* F, double* u, double* v, double* p, dou
         local.rel_residual[k - 1] = r.rel_residual;
         local.status[k - 1] = r.status;
         if (st != LICA_OK && st != LICA_NOT_CONVERGED && st != LICA_STALLED) return st;
+        if (F->capture) {
+            double* q = F->capture + (size_t)(k - 1) * (4 * n + (size_t)(F->ny + 1) * F->nx);
+            const size_t nb = (size_t)(F->ny + 1) * F->nx;
+            LICA_CUDA_TRY(cudaMemcpyAsync(q, F->den, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            LICA_CUDA_TRY(cudaMemcpyAsync(q + n, F->f, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            LICA_CUDA_TRY(cudaMemcpyAsync(q + 2 * n, F->bx, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            LICA_CUDA_TRY(cudaMemcpyAsync(q + 3 * n, F->by, nb * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            LICA_CUDA_TRY(cudaMemcpyAsync(q + 3 * n + nb, F->dp, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        }
         k_correct<<<gflow, blk, 0, s>>>(F->us, F->vs, F->dp, F->bx, F->by, u, v, p, adt, c);
         k_energy<<<gflow, blk, 0, s>>>(thc, u, v, F->densc, F->tc, F->psi, thn, F->rth, dt, gam, ro, c);
         k_ls_transport<<<gref, blk, 0, s>>>(phc, u, v, phn, F->rphi, dt, gam, ro, c);
@@ -621,6 +642,18 @@ int lica_film2d_step_device(lica_film2d* F, double* u, double* v, double* p, dou
     if (stats) *stats = local;
     for (int k = 0; k < 3; ++k)
         if (local.status[k] != LICA_OK) return local.status[k];
+    return LICA_OK;
+}
+
+int lica_film2d_set_guess(lica_film2d* F, lica_unet* net) {
+    if (!F) return LICA_BAD_ARG;
+    F->guess = net;
+    return LICA_OK;
+}
+
+int lica_film2d_capture_device(lica_film2d* F, double* systems) {
+    if (!F) return LICA_BAD_ARG;
+    F->capture = systems;
     return LICA_OK;
 }
 

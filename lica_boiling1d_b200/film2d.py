@@ -150,7 +150,37 @@ class Film2D:
         code = native.lib().lica_film2d_step_device(self._h, *(state[k].data_ptr() for k in FIELDS), float(dt),
                                                     C.byref(st), s.cuda_stream)
         native.check(code, "lica_film2d_step_device", ok=(0, 1, 8))
-        return dict(iterations=list(st.iterations), status=list(st.status), rel=list(st.rel_residual), code=code)
+        return dict(iterations=list(st.iterations), status=list(st.status), rel=list(st.rel_residual),
+                    guess_rel=list(st.guess_rel), code=code)
+
+    def set_guess(self, net):
+        """Start the three pressure solves from the learned guess of net (a LearnedGuess of
+        one ny x nx image; zero where the guess is no better than zero); None: from zero."""
+        if net is not None and (net.n, net.h, net.w) != (1, self.ny, self.nx):
+            raise ValueError(f"the guess must be a LearnedGuess(1, {self.ny}, {self.nx})")
+        self._guess = net   # keep it alive while attached
+        native.check(native.lib().lica_film2d_set_guess(self._h, net._h if net is not None else None),
+                     "lica_film2d_set_guess")
+
+    def capture(self, systems):
+        """Record every step's three pressure systems into systems, a float64 CUDA tensor of
+        3 * (4 nx ny + (ny + 1) nx) values (per substep: density, f, bx, by, dp); None: off."""
+        if systems is not None and systems.numel() < 3 * (4 * self.nx * self.ny + (self.ny + 1) * self.nx):
+            raise ValueError("capture buffer too small")
+        self._systems = systems
+        native.check(native.lib().lica_film2d_capture_device(
+            self._h, C.c_void_p(systems.data_ptr()) if systems is not None else None), "lica_film2d_capture_device")
+
+    def unpack_capture(self, systems):
+        """The captured systems as a list of 3 dicts of (ny, nx) / (ny + 1, nx) tensors."""
+        n, nb = self.nx * self.ny, (self.ny + 1) * self.nx
+        out = []
+        for k in range(3):
+            q = systems[k * (4 * n + nb):(k + 1) * (4 * n + nb)]
+            out.append(dict(rho=q[:n].view(self.ny, self.nx), f=q[n:2 * n].view(self.ny, self.nx),
+                            bx=q[2 * n:3 * n].view(self.ny, self.nx), by=q[3 * n:3 * n + nb].view(self.ny + 1, self.nx),
+                            dp=q[3 * n + nb:4 * n + nb].view(self.ny, self.nx)))
+        return out
 
     def mdot(self, stream=None):
         """The interfacial mass flux per cell of the last substep, (ny, nx) on the device."""

@@ -63,7 +63,8 @@ class Film2DProps(C.Structure):
 
 
 class Film2DStats(C.Structure):
-    _fields_ = [("iterations", C.c_int32 * 3), ("status", C.c_int32 * 3), ("rel_residual", C.c_double * 3)]
+    _fields_ = [("iterations", C.c_int32 * 3), ("status", C.c_int32 * 3), ("rel_residual", C.c_double * 3),
+                ("guess_rel", C.c_double * 3)]
 
 
 # every symbol include/lica_gpu.h declares, with its ctypes signature
@@ -150,6 +151,8 @@ SIGNATURES = {
     "lica_film2d_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.POINTER(Film2DProps), C.c_int32,
                                      C.c_int32]),
     "lica_film2d_destroy": (C.c_int, [C.c_void_p]),
+    "lica_film2d_set_guess": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "lica_film2d_capture_device": (C.c_int, [C.c_void_p, C.c_void_p]),
     "lica_film2d_step_device": (C.c_int, [C.c_void_p] * 6 + [C.c_double, C.POINTER(Film2DStats), C.c_void_p]),
     "lica_film2d_mdot_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
 }

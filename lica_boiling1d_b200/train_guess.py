@@ -24,6 +24,7 @@ from .inputs import bubble_density, face_beta
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 WEIGHTS = os.path.join(HERE, "weights", "unet_guess.npy")
+FILM_WEIGHTS = os.path.join(HERE, "weights", "unet_guess_film.npy")
 
 
 def problem(rng, n, ny=None, *, bubbles_per_1024sq=64, rmin=8.0, rmax=48.0):
@@ -73,6 +74,53 @@ def train(net, steps, n, lr=1e-3, seed=0, log_every=100, log=print, lr_final=Non
     return hist
 
 
+def film_pairs(nx, ny, steps, props=None, warm=2):
+    """(rho, f, bx, by, dp) pressure systems of the 2-D film step's own solves: a film of nx x ny
+    (interface at ny/24 cells, amplitude nx/128 cells -- config 3's shape at any size) run for
+    warm + steps RK3 steps on the GPU; the three substeps' systems of each of the last steps,
+    as CUDA tensors (a list of dicts)."""
+    import torch
+    from . import film2d as G
+    P = G.default_props() if props is None else props
+    st = G.to_device(G.initial_state(nx, ny, ny / 24.0, nx / 128.0, props=P))
+    dt = G.stable_dt(nx, P)
+    film = G.Film2D(nx, ny, P)
+    buf = torch.zeros(3 * (4 * nx * ny + (ny + 1) * nx), dtype=torch.float64, device="cuda")
+    out = []
+    try:
+        for k in range(warm + steps):
+            film.capture(buf if k >= warm else None)
+            film.step(st, dt)
+            if k >= warm:
+                out += [{key: v.clone() for key, v in sysk.items()} for sysk in film.unpack_capture(buf)]
+    finally:
+        film.capture(None)
+        film.close()
+    return out
+
+
+def train_film(net, steps, nx, ny, lr=1e-3, lr_final=1e-4, seed=0, pool_steps=64, log_every=100, log=print):
+    """Adam steps of the A-norm loss on the film's own (rho, f -> dp) pairs: a pool of
+    3 pool_steps systems from consecutive film steps, net.n drawn per step.  Returns the
+    loss history."""
+    import torch
+    rng = np.random.default_rng(seed)
+    pool = film_pairs(nx, ny, pool_steps)
+    h = 1.0 / nx
+    hist = []
+    t0 = time.time()
+    for it in range(steps):
+        lr_it = lr * (lr_final / lr) ** (it / max(1, steps - 1))
+        pick = rng.choice(len(pool), size=net.n, replace=False)
+        rho, f, bx, by, dp = (torch.stack([pool[i][k] for i in pick]).contiguous()
+                              for k in ("rho", "f", "bx", "by", "dp"))
+        loss = net.train_step(rho, f, bx, by, h, h, lr_it, p_star=dp)
+        hist.append(loss)
+        if log and (it % log_every == 0 or it == steps - 1):
+            log(f"film step {it:5d}  loss {np.mean(hist[-log_every:]):.4e}  ({time.time() - t0:.1f} s)")
+    return hist
+
+
 def iterations(n, problems, guess_net=None, rtol=1e-10, nlevels=None, precision="fp64"):
     """PCG iterations (and final relative residuals) of each problem from x0 = 0, or from
     the network's guess with the zero fallback."""
@@ -114,8 +162,17 @@ def main():
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--eval-n", type=int, default=1024)
     ap.add_argument("--eval-count", type=int, default=4)
+    ap.add_argument("--film", action="store_true",
+                    help="train on the 2-D film step's own pressure systems (writes the film weights)")
+    ap.add_argument("--film-nx", type=int, default=256)
     a = ap.parse_args()
     from .unet import LearnedGuess
+    if a.film:
+        nx, ny = a.film_nx, 3 * a.film_nx
+        net = LearnedGuess(a.batch, ny, nx, seed=a.seed + 1)
+        train_film(net, a.steps, nx, ny, lr=a.lr, lr_final=a.lr_final, seed=a.seed)
+        save(net, a.out if a.out != WEIGHTS else FILM_WEIGHTS)
+        return
     net = LearnedGuess(a.batch, a.n, a.n, seed=a.seed + 1)
     train(net, a.steps, a.n, lr=a.lr, lr_final=a.lr_final, seed=a.seed)
     save(net, a.out)
