@@ -523,6 +523,9 @@ __global__ void __launch_bounds__(NT) k_pupdate(double* __restrict__ p0, double*
 // sets the loop condition.  x ping-pongs like p: x_old = xx[it&1], x_new = xx[(it+1)&1]
 // (xx[0] is the caller's array); p is the buffer k_pupdate just wrote, pp[(it+1)&1].
 // first = 1: the set-up pass, r = f - A x0 and ||f||, nothing written to x.
+__device__ __noinline__ void xupdate_finish(State* __restrict__ st, double tot, int first,
+                                            cudaGraphConditionalHandle cond, int use_cond);
+
 template <typename TR>
 __global__ void __launch_bounds__(NT) k_xupdate(double* __restrict__ x0, double* __restrict__ x1,
                                                 const double* __restrict__ p0, const double* __restrict__ p1,
@@ -576,7 +579,14 @@ __global__ void __launch_bounds__(NT) k_xupdate(double* __restrict__ x0, double*
     if (first) {
         if (grid_sum_last(bf, partials + gridDim.x * gridDim.y, &st->cnt[3], &tot, red)) st->sums[1] = tot;
     }
-    if (grid_sum_last(b, partials, &st->cnt[2], &tot, red)) {
+    if (grid_sum_last(b, partials, &st->cnt[2], &tot, red)) xupdate_finish(st, tot, first, cond, use_cond);
+}
+
+// The last block of k_xupdate: ||f|| on the set-up pass, the iteration count, rel, the
+// status and the loop condition.
+__device__ __noinline__ void xupdate_finish(State* __restrict__ st, double tot, int first,
+                                            cudaGraphConditionalHandle cond, int use_cond) {
+    {
         __threadfence();
         if (first) {
             // the ||f|| sum finished in an earlier (or this) block: read it through L2
@@ -614,6 +624,14 @@ __global__ void __launch_bounds__(NT) k_xupdate(double* __restrict__ x0, double*
         if (use_cond) cudaGraphSetConditional(cond, cont ? 1u : 0u);
     }
 }
+
+}  // namespace mg
+}  // namespace lica
+
+#include "mg_cg_tma.cuh"
+
+namespace lica {
+namespace mg {
 
 template <typename TZ>
 constexpr size_t pupdate_smem() {
@@ -1234,6 +1252,11 @@ struct LevelBuf {
 struct lica_mg {
     int nx, ny;
     int nsm = 148;  // SMs of the device (persistent grids)
+    // the persistent TMA-staged CG kernels (level 0 with at least one 32 x 32 tile per SM)
+    bool cg_tma = false;
+    CgMaps cgm{};
+    const void* cg_x = nullptr;  // the caller's x and f the maps cgm.x[0], cgm.xw[0], cgm.f describe
+    const void* cg_f = nullptr;
     double hx, hy;
     lica_mg_options o;
     int nouter = 0, lcta = 0, bottom = 0;
@@ -1607,10 +1630,56 @@ int setup_beta(lica_mg* m, const double* bx, const double* by, cudaStream_t s) {
     return LICA_OK;
 }
 
+// Maps of the caller's x (the first x buffer) and f for the TMA CG kernels, re-encoded when
+// the pointers change.
+int cg_maps_for(lica_mg* m, const double* x, const double* f) {
+    if (m->cg_x == x && m->cg_f == f) return LICA_OK;
+    const int nx = m->nx, ny = m->ny;
+    int st;
+    if ((st = tm_map(&m->cgm.x[0], x, false, nx, ny, CG_BW, CG_BH)) ||
+        (st = tm_map(&m->cgm.xw[0], x, false, nx, ny, CG_WW, CG_BH)) ||
+        (st = tm_map(&m->cgm.f, f, false, nx, ny, CG_BW, CG_BH)))
+        return st;
+    m->cg_x = x;
+    m->cg_f = f;
+    return LICA_OK;
+}
+
+template <typename TZ, bool XUP>
+int launch_cg_tma(lica_mg* m, double* x, cudaGraphConditionalHandle h, int use_cond, cudaStream_t s) {
+    LevelBuf& L = m->lv[0];
+    CgArgs A;
+    A.m = m->cgm;
+    A.pbuf[0] = m->pcg[0];
+    A.pbuf[1] = m->pcg[1];
+    A.xbuf[0] = x;
+    A.xbuf[1] = m->xb;
+    A.r_out = m->r;
+    A.nx = L.nx;
+    A.ny = L.ny;
+    A.ntx = L.nx / CG_TS;
+    A.nty = L.ny / CG_TS;
+    A.st = m->st;
+    A.partials = m->partials;
+    A.cond = h;
+    A.use_cond = use_cond;
+    const int grid = std::min(A.ntx * A.nty, m->nsm);
+    k_cg_tma<TZ, XUP><<<grid, CG_NT, CgLayout<TZ, XUP>::BYTES, s>>>(A);
+    LICA_CUDA_TRY(cudaGetLastError());
+    lica_count_launches(1);
+    return LICA_OK;
+}
+
 template <typename TR>
 int launch_xupdate(lica_mg* m, double* x, const double* f, int first, cudaGraphConditionalHandle h, int use_cond,
                    cudaStream_t s) {
     LevelBuf& L = m->lv[0];
+    if (m->cg_tma && !first) {
+        ProfScope ps(m, LICA_MG_XUPDATE, s);
+        int st = cg_maps_for(m, x, f);
+        if (st) return st;
+        return launch_cg_tma<TR, true>(m, x, h, use_cond, s);
+    }
     dim3 grid(L.nx / TX, L.ny / TY);
     ProfScope ps(m, LICA_MG_XUPDATE, s);
     k_xupdate<TR><<<grid, NT, xupdate_smem(), s>>>(x, m->xb, m->pcg[0], m->pcg[1], f, L.ax64, L.ay64, (TR*)m->r, L.nx, L.ny,
@@ -1623,6 +1692,10 @@ int launch_xupdate(lica_mg* m, double* x, const double* f, int first, cudaGraphC
 template <typename TZ>
 int launch_pupdate(lica_mg* m, cudaStream_t s) {
     LevelBuf& L = m->lv[0];
+    if (m->cg_tma) {
+        ProfScope ps(m, LICA_MG_PUPDATE, s);
+        return launch_cg_tma<TZ, false>(m, nullptr, cudaGraphConditionalHandle{}, 0, s);
+    }
     dim3 grid(L.nx / TX, L.ny / TY);
     ProfScope ps(m, LICA_MG_PUPDATE, s);
     k_pupdate<TZ><<<grid, NT, pupdate_smem<TZ>(), s>>>(m->pcg[0], m->pcg[1], (const TZ*)m->z, L.ax64, L.ay64, L.nx, L.ny, m->st,
@@ -2022,6 +2095,44 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
     m->lv[0].up = m->z;
     m->lv[0].f = m->r;
     if (int st = build_tma(m)) return fail(st);
+    {
+        // the TMA CG kernels: level 0 in 32 x 32 tiles, two tile columns, a tile per SM
+        const int ntx = nx / CG_TS, nty = ny / CG_TS;
+        if (nx % CG_TS == 0 && ny % CG_TS == 0 && ntx >= 2 && ntx * nty >= m->nsm) {
+            LevelBuf& L0 = m->lv[0];
+            const bool f32 = is_mixed(m);
+            int st;
+            CgMaps& M = m->cgm;
+            if ((st = tm_map(&M.p[0], m->pcg[0], false, nx, ny, CG_BW, CG_BH)) ||
+                (st = tm_map(&M.pw[0], m->pcg[0], false, nx, ny, CG_WW, CG_BH)) ||
+                (st = tm_map(&M.p[1], m->pcg[1], false, nx, ny, CG_BW, CG_BH)) ||
+                (st = tm_map(&M.pw[1], m->pcg[1], false, nx, ny, CG_WW, CG_BH)) ||
+                (st = tm_map(&M.x[1], m->xb, false, nx, ny, CG_BW, CG_BH)) ||
+                (st = tm_map(&M.xw[1], m->xb, false, nx, ny, CG_WW, CG_BH)) ||
+                (st = tm_map(&M.z, m->z, f32, nx, ny, CG_BW, CG_BH)) ||
+                (st = tm_map(&M.zw, m->z, f32, nx, ny, CG_WW, CG_BH)) ||
+                (st = tm_map(&M.ax, L0.ax64, false, nx, ny, CG_BW, CG_BH)) ||
+                (st = tm_map(&M.axw, L0.ax64, false, nx, ny, CG_WW, CG_BH)) ||
+                (st = tm_map(&M.ay, L0.ay64, false, nx, ny + 1, CG_BW, CG_BH)))
+                return fail(st);
+            cudaError_t ce = cudaFuncSetAttribute(k_cg_tma<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  CgLayout<double, false>::BYTES);
+            if (ce == cudaSuccess) ce = cudaFuncSetAttribute(k_cg_tma<float, false>,
+                                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                             CgLayout<float, false>::BYTES);
+            if (ce == cudaSuccess) ce = cudaFuncSetAttribute(k_cg_tma<double, true>,
+                                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                             CgLayout<double, true>::BYTES);
+            if (ce == cudaSuccess) ce = cudaFuncSetAttribute(k_cg_tma<float, true>,
+                                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                             CgLayout<float, true>::BYTES);
+            if (ce != cudaSuccess) {
+                lica_set_last_error("cudaFuncSetAttribute(k_cg_tma)", cudaGetErrorString(ce), __FILE__, __LINE__);
+                return fail(LICA_ERR_CUDA);
+            }
+            m->cg_tma = true;
+        }
+    }
     *out = m;
     return LICA_OK;
 }

@@ -1,0 +1,227 @@
+// Persistent, TMA-staged forms of the two PCG vector kernels on level 0 (k_cg_tma): the
+// same arithmetic as k_pupdate / k_xupdate, cell for cell, with the tiles streamed through a
+// two-stage shared-memory ring.  A CTA (one per SM, 512 threads) walks tiles t, t + grid,
+// ...; while it computes tile t the TMA copies of tile t + grid are in flight, so the
+// per-tile load latency of the one-tile-per-CTA kernels is hidden.
+//
+// Tile 32 x 32; a box covers global columns gi0 = 32 tx - 4 .. gi0 + 39 (16-byte aligned
+// for FP32 and FP64) and rows gj0 = 32 ty - 1 .. gj0 + 33: the tile and the one-cell ring
+// the stencil reads.  x is periodic: the first and last tile columns also copy the 4
+// columns at the far end of the row.  Rows off the domain are zero-filled by the TMA, as
+// the per-tile kernels' loads fill them.
+//
+// k_pupdate_tma: p_new = z + beta p_old on the tile and its ring, then p_new.(A p_new) on
+//   the tile; the last CTA sets alpha = rz / p.Ap.
+// k_xupdate_tma: x_new = x + alpha p on the tile and its ring, r = f - A x_new on the tile
+//   (stored as TR), ||r||^2; the last CTA runs xupdate_finish.
+// Every wait is bounded (tc::mbar_wait); one that runs out sets State::kerr.
+#pragma once
+
+namespace lica {
+namespace mg {
+
+constexpr int CG_TS = 32;
+constexpr int CG_BW = 40;      // box width (columns gi0 .. gi0 + 39)
+constexpr int CG_BH = 34;      // box height (rows gj0 .. gj0 + 33)
+constexpr int CG_X0 = 4;       // box column of tile column 0
+constexpr int CG_WW = 4;       // wrap strip width
+constexpr int CG_NT = 512;
+constexpr int CG_RW = 34;      // ring array: columns -1 .. 32, rows -1 .. 32
+
+struct CgMaps {
+    // by iteration parity: p_old / x read from [par], written to [par ^ 1]
+    CUtensorMap p[2], pw[2], x[2], xw[2], z, zw, f, ax, axw, ay;
+};
+
+struct CgArgs {
+    CgMaps m;
+    double* pbuf[2];   // the two p buffers (p_new is written to pbuf[par ^ 1])
+    double* xbuf[2];   // the two x buffers (x_new to xbuf[par ^ 1])
+    void* r_out;       // r (TR) for the preconditioner
+    int nx, ny, ntx, nty;
+    State* st;
+    double* partials;
+    cudaGraphConditionalHandle cond;
+    int use_cond;
+};
+
+// One ring stage, boxes A, B, C, AX, AY and the wrap strips of A, B, AX.
+//   k_pupdate's: A = p_old, B = z (TB = the V-cycle's type), C unused.
+//   k_xupdate's: A = x, B = p (TB = double), C = f.
+template <typename TB>
+struct CgStage {
+    static constexpr int al(int b) { return (b + 127) / 128 * 128; }
+    static constexpr int B8 = al(CG_BW * CG_BH * 8);
+    static constexpr int BT = al(CG_BW * CG_BH * (int)sizeof(TB));
+    static constexpr int W8 = al(CG_WW * CG_BH * 8);
+    static constexpr int WT = al(CG_WW * CG_BH * (int)sizeof(TB));
+    static constexpr int A = 0;
+    static constexpr int B = A + B8;
+    static constexpr int C = B + BT;
+    static constexpr int AX = C + B8;
+    static constexpr int AY = AX + B8;
+    static constexpr int WA = AY + B8;
+    static constexpr int WB = WA + W8;
+    static constexpr int WAX = WB + WT;
+    static constexpr int BYTES = WAX + W8;
+};
+
+template <typename TZ, bool XUP>
+struct CgLayout {
+    using TB = typename std::conditional<XUP, double, TZ>::type;
+    using S = CgStage<TB>;
+    static constexpr int RING = S::al(CG_RW * CG_RW * 8);   // p_new / x_new on the tile and its ring
+    static constexpr int BYTES = 2 * S::BYTES + RING + 128;  // + room to align the base
+    // transaction bytes of one tile's copies (whole boxes, filled parts included)
+    static constexpr uint32_t TX_MAIN =
+        (uint32_t)(CG_BW * CG_BH * (3 * 8 + (int)sizeof(TB) + (XUP ? 8 : 0)));
+    static constexpr uint32_t TX_WRAP = (uint32_t)(CG_WW * CG_BH * (2 * 8 + (int)sizeof(TB)));
+};
+
+// The value at box row br, global column i (box column bc = i - gi0) of a staged array.
+template <typename T>
+__device__ __forceinline__ T cg_at(const unsigned char* st, int off, int woff, int br, int bc, int i, int nx) {
+    const T* box = reinterpret_cast<const T*>(st + off);
+    const T* wrap = reinterpret_cast<const T*>(st + woff);
+    if (i < 0) return wrap[br * CG_WW + i + CG_WW];
+    if (i >= nx) return wrap[br * CG_WW + i - nx];
+    return box[br * CG_BW + bc];
+}
+
+// Thread 0: the copies of one tile into stage buffer sb (bar: its barrier).
+template <typename TZ, bool XUP>
+__device__ __forceinline__ void cg_issue(const CgArgs& A, unsigned char* sb, uint64_t* bar, int tile, int par) {
+    using Lay = CgLayout<TZ, XUP>;
+    using S = typename Lay::S;
+    const int tx = tile % A.ntx, ty = tile / A.ntx;
+    const int gi0 = tx * CG_TS - CG_X0, gj0 = ty * CG_TS - 1;
+    const bool edge = (tx == 0 || tx == A.ntx - 1);
+    tc::mbar_expect_tx(bar, Lay::TX_MAIN + (edge ? Lay::TX_WRAP : 0u));
+    if (XUP) {
+        tc::tma_load_2d(sb + S::A, &A.m.x[par], bar, gi0, gj0);
+        tc::tma_load_2d(sb + S::B, &A.m.p[par ^ 1], bar, gi0, gj0);
+        tc::tma_load_2d(sb + S::C, &A.m.f, bar, gi0, gj0);
+    } else {
+        tc::tma_load_2d(sb + S::A, &A.m.p[par], bar, gi0, gj0);
+        tc::tma_load_2d(sb + S::B, &A.m.z, bar, gi0, gj0);
+    }
+    tc::tma_load_2d(sb + S::AX, &A.m.ax, bar, gi0, gj0);
+    tc::tma_load_2d(sb + S::AY, &A.m.ay, bar, gi0, gj0);
+    if (edge) {
+        const int wx = (tx == 0) ? A.nx - CG_WW : 0;
+        if (XUP) {
+            tc::tma_load_2d(sb + S::WA, &A.m.xw[par], bar, wx, gj0);
+            tc::tma_load_2d(sb + S::WB, &A.m.pw[par ^ 1], bar, wx, gj0);
+        } else {
+            tc::tma_load_2d(sb + S::WA, &A.m.pw[par], bar, wx, gj0);
+            tc::tma_load_2d(sb + S::WB, &A.m.zw, bar, wx, gj0);
+        }
+        tc::tma_load_2d(sb + S::WAX, &A.m.axw, bar, wx, gj0);
+    }
+}
+
+// XUP = false: k_pupdate's work (TZ = the V-cycle's type); XUP = true: k_xupdate's (TZ = TR).
+template <typename TZ, bool XUP>
+__global__ void __launch_bounds__(CG_NT, 1) k_cg_tma(const __grid_constant__ CgArgs A) {
+    using Lay = CgLayout<TZ, XUP>;
+    using S = typename Lay::S;
+    extern __shared__ __align__(16) unsigned char cg_smem_raw[];
+    unsigned char* sm = cg_smem_raw + ((128u - (tc::smem_u32(cg_smem_raw) & 127u)) & 127u);
+    unsigned char* stage[2] = {sm, sm + S::BYTES};
+    double* ring = reinterpret_cast<double*>(sm + 2 * S::BYTES);
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ double red[32];
+    const int ntiles = A.ntx * A.nty;
+    const int par = A.st->it & 1;
+    const double coef = XUP ? A.st->alpha : A.st->beta;
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&bar[0], 1);
+        tc::mbar_init(&bar[1], 1);
+        tc::fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && (int)blockIdx.x < ntiles) cg_issue<TZ, XUP>(A, stage[0], &bar[0], blockIdx.x, par);
+    double acc = 0.0;
+    bool failed = false;
+    int i = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
+        const int s = i & 1;
+        // the next tile into the other stage (its last reader finished before the barrier
+        // that closed the previous iteration)
+        const bool next = tile + (int)gridDim.x < ntiles;
+        if (threadIdx.x == 0 && next) cg_issue<TZ, XUP>(A, stage[s ^ 1], &bar[s ^ 1], tile + gridDim.x, par);
+        const int ok = tc::mbar_wait(&bar[s], (uint32_t)((i >> 1) & 1)) ? 1 : 0;
+        if (!__syncthreads_and(ok)) {
+            // let the copies of the next tile land (bounded) before the CTA leaves
+            if (threadIdx.x == 0 && next) (void)tc::mbar_wait(&bar[s ^ 1], (uint32_t)(((i + 1) >> 1) & 1));
+            failed = true;
+            break;
+        }
+        const unsigned char* sb = stage[s];
+        const int tx = tile % A.ntx, ty = tile / A.ntx;
+        const int gi0 = tx * CG_TS - CG_X0, gj0 = ty * CG_TS - 1;
+        // the updated vector on the tile and its ring (box rows 0..33, columns 3..36)
+        for (int k = threadIdx.x; k < CG_RW * CG_RW; k += CG_NT) {
+            const int rr = k / CG_RW, rc = k - rr * CG_RW;
+            const int bc = rc + CG_X0 - 1, gi = gi0 + bc;
+            double v;
+            if (XUP) {
+                const double xv = cg_at<double>(sb, S::A, S::WA, rr, bc, gi, A.nx);
+                const double pv = cg_at<double>(sb, S::B, S::WB, rr, bc, gi, A.nx);
+                v = xv + coef * pv;
+            } else {
+                const double pv = cg_at<double>(sb, S::A, S::WA, rr, bc, gi, A.nx);
+                const TZ zv = cg_at<TZ>(sb, S::B, S::WB, rr, bc, gi, A.nx);
+                v = double(zv) + coef * pv;
+            }
+            ring[k] = v;
+        }
+        __syncthreads();
+        // the stencil on the tile
+        for (int k = threadIdx.x; k < CG_TS * CG_TS; k += CG_NT) {
+            const int ty_ = k / CG_TS, tx_ = k - ty_ * CG_TS;
+            const int br = ty_ + 1, bc = tx_ + CG_X0, gi = gi0 + bc;
+            const int c = (ty_ + 1) * CG_RW + tx_ + 1;
+            const double aw = cg_at<double>(sb, S::AX, S::WAX, br, bc, gi, A.nx);
+            const double ae = cg_at<double>(sb, S::AX, S::WAX, br, bc + 1, gi + 1, A.nx);
+            const double* ayb = reinterpret_cast<const double*>(sb + S::AY);
+            const double as = ayb[br * CG_BW + bc], an = ayb[(br + 1) * CG_BW + bc];
+            double ss = aw * ring[c - 1];
+            ss += ae * ring[c + 1];
+            ss += as * ring[c - CG_RW];
+            ss += an * ring[c + CG_RW];
+            double dd = aw;
+            dd += ae;
+            dd += as;
+            dd += an;
+            const double v = ring[c];
+            const size_t g = (size_t)(ty * CG_TS + ty_) * A.nx + tx * CG_TS + tx_;
+            if (XUP) {
+                const double fv = reinterpret_cast<const double*>(sb + S::C)[br * CG_BW + bc];
+                const double r = fv - (ss - dd * v);
+                acc += r * r;
+                A.xbuf[par ^ 1][g] = v;
+                reinterpret_cast<TZ*>(A.r_out)[g] = TZ(r);
+            } else {
+                const double q = ss - dd * v;
+                acc += v * q;
+                A.pbuf[par ^ 1][g] = v;
+            }
+        }
+        __syncthreads();   // the ring and this stage are free again
+    }
+    if (failed) {
+        if (threadIdx.x == 0) atomicExch(&A.st->kerr, 1);
+        return;
+    }
+    const double b = block_sum(acc, red);
+    double tot;
+    if (XUP) {
+        if (grid_sum_last(b, A.partials, &A.st->cnt[2], &tot, red)) xupdate_finish(A.st, tot, 0, A.cond, A.use_cond);
+    } else {
+        if (grid_sum_last(b, A.partials, &A.st->cnt[1], &tot, red)) A.st->alpha = A.st->rz / tot;
+    }
+}
+
+}  // namespace mg
+}  // namespace lica
