@@ -418,14 +418,6 @@ __global__ void __launch_bounds__(RBCfg<NSW, TXX, TYY, R>::NTH, 2)
     }
 }
 
-}  // namespace mg
-}  // namespace lica
-
-#include "mg_tma.cuh"
-
-namespace lica {
-namespace mg {
-
 // ------------------------------------------------------------------------------------
 // CG kernels (FP64 vectors) on TX x TY tiles with a 2-cell halo (one ring is used; the
 // second keeps every row segment an aligned vector load).
@@ -1245,8 +1237,6 @@ struct LevelBuf {
     float* ax32 = nullptr;
     float* ay32 = nullptr;
     float* di32 = nullptr;
-    bool tma = false;        // smoothed by the persistent TMA-staged kernels (k_smooth_tma)
-    TmMaps tm_down{}, tm_up{};
 };
 
 struct lica_mg {
@@ -1339,42 +1329,6 @@ int tm_map(CUtensorMap* mp, const void* base, bool f32, int w, int h, int bw, in
     return LICA_OK;
 }
 
-// Tensor maps of the levels the persistent TMA kernels smooth: levels with 32 x 32 tiles,
-// at least two tile columns and two tiles per resident CTA slot, V(2,2) cycles.
-int build_tma(lica_mg* m) {
-    const bool f32 = is_mixed(m);
-    for (int l = 0; l < m->lcta; ++l) {
-        LevelBuf& L = m->lv[l];
-        LevelBuf& C = m->lv[l + 1];
-        const int ntx = L.nx / TM_TS, nty = L.ny / TM_TS;
-        if (m->o.nu1 != 2 || m->o.nu2 != 2 || L.nx % TM_TS || L.ny % TM_TS || ntx < 2 || ntx * nty < 4 * m->nsm)
-            continue;
-        const void* ax = f32 ? (const void*)L.ax32 : (const void*)L.ax64;
-        const void* ay = f32 ? (const void*)L.ay32 : (const void*)L.ay64;
-        const void* di = f32 ? (const void*)L.di32 : (const void*)L.di64;
-        const void* uc = (l + 1 == m->lcta) ? C.u : C.up;
-        int st;
-        for (TmMaps* M : {&L.tm_down, &L.tm_up}) {
-            if ((st = tm_map(&M->f, L.f, f32, L.nx, L.ny, TM_RX, TM_RY)) ||
-                (st = tm_map(&M->fw, L.f, f32, L.nx, L.ny, TM_WW, TM_RY)) ||
-                (st = tm_map(&M->d, di, f32, L.nx, L.ny, TM_RX, TM_RY)) ||
-                (st = tm_map(&M->dw, di, f32, L.nx, L.ny, TM_WW, TM_RY)) ||
-                (st = tm_map(&M->ax, ax, f32, L.nx, L.ny, TM_AXW, TM_RY)) ||
-                (st = tm_map(&M->axw, ax, f32, L.nx, L.ny, TM_WW, TM_RY)) ||
-                (st = tm_map(&M->ay, ay, f32, L.nx, L.ny + 1, TM_RX, TM_AYH)) ||
-                (st = tm_map(&M->ayw, ay, f32, L.nx, L.ny + 1, TM_WW, TM_AYH)))
-                return st;
-        }
-        if ((st = tm_map(&L.tm_up.u, L.u, f32, L.nx, L.ny, TM_RX, TM_RY)) ||
-            (st = tm_map(&L.tm_up.uw, L.u, f32, L.nx, L.ny, TM_WW, TM_RY)) ||
-            (st = tm_map(&L.tm_up.c, uc, f32, C.nx, C.ny, TM_CW, TM_CH)) ||
-            (st = tm_map(&L.tm_up.cw, uc, f32, C.nx, C.ny, TM_CWW, TM_CH)))
-            return st;
-        L.tma = true;
-    }
-    return LICA_OK;
-}
-
 // Profiling: bracket one kernel launch with events when profiling is on.
 cudaEvent_t pool_event(lica_mg* m) {
     if (!m->event_pool.empty()) {
@@ -1452,39 +1406,11 @@ void down_ns(const LevelBuf& L, const LevelBuf& C, cudaStream_t s) {
     else down_tile<T, NS, 16>(L, C, s);
 }
 
-// The persistent TMA-staged smoothing kernels (levels with L.tma): k_down's work (up =
-// false) or k_up's (up = true), two CTAs per SM walking the level's 32 x 32 tiles.
-template <typename T>
-void launch_tma(lica_mg* m, int l, bool up, cudaStream_t s) {
-    LevelBuf& L = m->lv[l];
-    TmArgs<T> A;
-    A.m = up ? L.tm_up : L.tm_down;
-    A.out = (T*)(up ? L.up : L.u);
-    A.fc = up ? nullptr : (T*)m->lv[l + 1].f;
-    A.nx = L.nx;
-    A.ny = L.ny;
-    A.ntx = L.nx / TM_TS;
-    A.nty = L.ny / TM_TS;
-    A.st = m->st;
-    A.partials = m->partials;
-    const int grid = std::min(A.ntx * A.nty, 2 * m->nsm);
-    const size_t smem = TmStage<T>::BYTES;
-    if (!up) k_smooth_tma<T, false, false><<<grid, TmCfg::NTH, smem, s>>>(A);
-    else if (l == 0) k_smooth_tma<T, true, true><<<grid, TmCfg::NTH, smem, s>>>(A);
-    else k_smooth_tma<T, true, false><<<grid, TmCfg::NTH, smem, s>>>(A);
-}
-
 template <typename T>
 int launch_down(lica_mg* m, int l, cudaStream_t s) {
     LevelBuf& L = m->lv[l];
     LevelBuf& C = m->lv[l + 1];
     ProfScope ps(m, l == 0 ? LICA_MG_DOWN0 : LICA_MG_DOWN, s);
-    if (L.tma) {
-        launch_tma<T>(m, l, false, s);
-        LICA_CUDA_TRY(cudaGetLastError());
-        lica_count_launches(1);
-        return LICA_OK;
-    }
     switch (m->o.nu1) {
         case 1: down_ns<T, 1>(L, C, s); break;
         case 2: down_ns<T, 2>(L, C, s); break;
@@ -1521,12 +1447,6 @@ int launch_up(lica_mg* m, int l, cudaStream_t s) {
     LevelBuf& C = m->lv[l + 1];
     const T* uc = (const T*)((l + 1 == m->lcta) ? C.u : C.up);
     ProfScope ps(m, l == 0 ? LICA_MG_UP0 : LICA_MG_UP, s);
-    if (L.tma) {
-        launch_tma<T>(m, l, true, s);
-        LICA_CUDA_TRY(cudaGetLastError());
-        lica_count_launches(1);
-        return LICA_OK;
-    }
     switch (m->o.nu2) {
         case 1: up_ns<T, 1>(m, L, uc, l == 0, s); break;
         case 2: up_ns<T, 2>(m, L, uc, l == 0, s); break;
@@ -2073,28 +1993,14 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
         lica_set_last_error("cudaFuncSetAttribute(k_cta)", cudaGetErrorString(e), __FILE__, __LINE__);
         return fail(LICA_ERR_CUDA);
     }
-    // the persistent TMA-staged smoothing kernels of the large levels
     e = cudaDeviceGetAttribute(&m->nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_smooth_tma<double, false, false>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, TmStage<double>::BYTES);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_smooth_tma<double, true, false>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, TmStage<double>::BYTES);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_smooth_tma<double, true, true>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, TmStage<double>::BYTES);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_smooth_tma<float, false, false>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, TmStage<float>::BYTES);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_smooth_tma<float, true, false>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, TmStage<float>::BYTES);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_smooth_tma<float, true, true>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, TmStage<float>::BYTES);
     if (e != cudaSuccess) {
-        lica_set_last_error("cudaFuncSetAttribute(k_smooth_tma)", cudaGetErrorString(e), __FILE__, __LINE__);
+        lica_set_last_error("cudaDeviceGetAttribute", cudaGetErrorString(e), __FILE__, __LINE__);
         return fail(LICA_ERR_CUDA);
     }
     m->lv[0].u = m->zpre;
     m->lv[0].up = m->z;
     m->lv[0].f = m->r;
-    if (int st = build_tma(m)) return fail(st);
     {
         // the TMA CG kernels: level 0 in 32 x 32 tiles, two tile columns, a tile per SM
         const int ntx = nx / CG_TS, nty = ny / CG_TS;

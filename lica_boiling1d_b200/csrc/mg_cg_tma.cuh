@@ -16,6 +16,11 @@
 //   (stored as TR), ||r||^2; the last CTA runs xupdate_finish.
 // Every wait is bounded (tc::mbar_wait); one that runs out sets State::kerr.
 #pragma once
+#include <cuda.h>
+
+#include <type_traits>
+
+#include "tc_sm100.cuh"
 
 namespace lica {
 namespace mg {
