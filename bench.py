@@ -300,19 +300,8 @@ def rk3_legs(dev, flush, steps_c1=C1["steps"], steps_c4=1000, warmup=3, rank=0, 
     lo, hi = shard.partition(n_all, world)[rank]
     n = n_all[lo:hi]
     batch = ColumnBatch.films(n, length[lo:hi], z0[lo:hi], bprops[lo:hi]).to(dev)
-    trial = {}
-    for th in (64, 128):
-        b = batch.to(dev)
-        b.steps(1, threads=th)
-        torch.cuda.synchronize(dev)
-        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a0.record()
-        b.steps(2, threads=th)
-        a1.record()
-        torch.cuda.synchronize(dev)
-        trial[th] = a0.elapsed_time(a1) / 2
-        del b
-    th = min(trial, key=trial.get)
+    from lica_boiling1d_b200 import autotune
+    th, trial = autotune.tune(batch, force=True)
     batch.steps(warmup, threads=th)
     torch.cuda.synchronize(dev)
     flush.fill_(5)
@@ -336,7 +325,9 @@ def rk3_legs(dev, flush, steps_c1=C1["steps"], steps_c4=1000, warmup=3, rank=0, 
                     f"the exact Thomas sweep), {steps_c4} RK3 steps in one persistent launch per rank, longest first",
         "steps_per_s": steps_c4 / (ms / 1e3), "ms_per_step": ms / steps_c4, "steps": steps_c4,
         "column_steps_per_s": C4_NCOL * steps_c4 / (ms / 1e3), "cell_updates_per_s": cells * steps_c4 / (ms / 1e3),
-        "threads": th, "autotune_ms_per_step": trial, "gpu_launches": launches,
+        "threads": th, "autotune_ms_per_step": trial,
+        "autotune": "lica_boiling1d_b200.autotune: CTA width 64/128/256 timed on a copy of the batch, cached per GPU",
+        "gpu_launches": launches,
         "ranks": world, "sharding": "contiguous column blocks balanced by cells, strong scaling of the fixed batch",
         "gathered_columns": len(hist)}
     if film_steps > 0:

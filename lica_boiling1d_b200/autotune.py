@@ -1,0 +1,97 @@
+"""Launch-shape autotuner of the batched column step (lica_gpu_column_batch_steps_device).
+
+The step kernel runs one CTA per column, persistent over all the steps of a launch.  Its
+launch shape is the CTA width -- 64, 128 or 256 threads -- which also fixes how many
+columns share an SM (the 64-thread form is bounded for 5 CTAs per SM, the wider ones run
+one or two) and how long a column may be for its Thomas arrays to sit in shared memory
+(the kernel sizes that cap from the CTAs the registers allow per SM).  Which shape is
+fastest depends on the batch: many short columns favour narrow CTAs and more columns per
+SM, a few long ones wide CTAs that finish each column sooner.
+
+``tune(batch)`` times one warm-up step and ``trial_steps`` steps of each shape on a copy of
+the batch's device state (the batch itself does not advance), keeps the fastest, and
+caches the choice per GPU and batch shape: in memory, and in a JSON file
+(``$LICA_TUNE_CACHE``, default ``~/.cache/lica_b200/column_tune.json``) so a later process
+on the same GPU model skips the trial.  ``ColumnBatch.steps(threads=0)`` calls it.
+"""
+import json
+import os
+import threading
+
+SHAPES = (64, 128, 256)
+_lock = threading.Lock()
+_memo = {}
+
+
+def _cache_path():
+    return os.environ.get("LICA_TUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "lica_b200", "column_tune.json"))
+
+
+def _gpu_name(device):
+    import torch
+    return torch.cuda.get_device_name(device)
+
+
+def batch_key(batch):
+    """Shape of a batch for the cache: column count, total and longest column, and the
+    column-length quartiles (the work per CTA and its spread)."""
+    import numpy as np
+    n = np.asarray(batch.n)
+    q = np.percentile(n, [25, 50, 75]).astype(int).tolist()
+    return f"ncol={batch.ncol},cells={int(n.sum())},nmax={int(n.max())},q={q[0]}/{q[1]}/{q[2]}"
+
+
+def _load():
+    try:
+        with open(_cache_path()) as fh:
+            return json.load(fh)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(entries):
+    path = _cache_path()
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        tmp = path + f".{os.getpid()}.tmp"
+        with open(tmp, "w") as fh:
+            json.dump(entries, fh, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+    except OSError:
+        pass   # a read-only home: the in-memory cache still holds the choice
+
+
+def tune(batch, trial_steps=2, force=False):
+    """The fastest CTA width for this batch on its GPU: (threads, {threads: ms per step} of
+    the trial, or None when the choice came from the cache)."""
+    import torch
+    dev = batch.arrays["w"].device
+    key = f"{_gpu_name(dev)}|{batch_key(batch)}"
+    with _lock:
+        if not force:
+            if key in _memo:
+                return _memo[key], None
+            disk = _load()
+            if key in disk and int(disk[key]["threads"]) in SHAPES:
+                _memo[key] = int(disk[key]["threads"])
+                return _memo[key], None
+    times = {}
+    for th in SHAPES:
+        trial = batch.to(dev)
+        trial.steps(1, threads=th)
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        trial.steps(trial_steps, threads=th)
+        b.record()
+        torch.cuda.synchronize(dev)
+        times[th] = a.elapsed_time(b) / trial_steps
+        del trial
+    best = min(times, key=times.get)
+    with _lock:
+        _memo[key] = best
+        disk = _load()
+        disk[key] = {"threads": best, "ms_per_step": {str(k): v for k, v in times.items()}}
+        _store(disk)
+    return best, times

@@ -255,8 +255,14 @@ class ColumnBatch:
         return ColumnBatch(self.n, self.length, self.props, out, self._h)
 
     def steps(self, nsteps, threads=0, stream=None, scratch=None):
-        """nsteps time steps of every column (device state).  Returns the per-column status."""
+        """nsteps time steps of every column (device state).  threads: the CTA width (64,
+        128 or 256), or 0 for the autotuner's choice for this batch on this GPU (timed once
+        on a copy of the state, then cached; see autotune.py).  Returns the per-column
+        status."""
         import torch
+        if threads == 0:
+            from . import autotune
+            threads = autotune.tune(self)[0]
         dev = self.arrays["w"].device
         status = torch.zeros(self.ncol, dtype=torch.int32, device=dev)
         s = stream if stream is not None else torch.cuda.current_stream(dev)
