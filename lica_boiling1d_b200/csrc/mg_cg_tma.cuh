@@ -30,7 +30,7 @@ constexpr int CG_BW = 40;      // box width (columns gi0 .. gi0 + 39)
 constexpr int CG_BH = 34;      // box height (rows gj0 .. gj0 + 33)
 constexpr int CG_X0 = 4;       // box column of tile column 0
 constexpr int CG_WW = 4;       // wrap strip width
-constexpr int CG_NT = 512;
+constexpr int CG_NT = 512;   // 32 rows x 16 column pairs of a tile
 constexpr int CG_RW = 34;      // ring array: columns -1 .. 32, rows -1 .. 32
 
 struct CgMaps {
@@ -82,16 +82,6 @@ struct CgLayout {
         (uint32_t)(CG_BW * CG_BH * (3 * 8 + (int)sizeof(TB) + (XUP ? 8 : 0)));
     static constexpr uint32_t TX_WRAP = (uint32_t)(CG_WW * CG_BH * (2 * 8 + (int)sizeof(TB)));
 };
-
-// The value at box row br, global column i (box column bc = i - gi0) of a staged array.
-template <typename T>
-__device__ __forceinline__ T cg_at(const unsigned char* st, int off, int woff, int br, int bc, int i, int nx) {
-    const T* box = reinterpret_cast<const T*>(st + off);
-    const T* wrap = reinterpret_cast<const T*>(st + woff);
-    if (i < 0) return wrap[br * CG_WW + i + CG_WW];
-    if (i >= nx) return wrap[br * CG_WW + i - nx];
-    return box[br * CG_BW + bc];
-}
 
 // Thread 0: the copies of one tile into stage buffer sb (bar: its barrier).
 template <typename TZ, bool XUP>
@@ -162,55 +152,73 @@ __global__ void __launch_bounds__(CG_NT, 1) k_cg_tma(const __grid_constant__ CgA
             failed = true;
             break;
         }
-        const unsigned char* sb = stage[s];
+        unsigned char* sb = stage[s];
         const int tx = tile % A.ntx, ty = tile / A.ntx;
-        const int gi0 = tx * CG_TS - CG_X0, gj0 = ty * CG_TS - 1;
-        // the updated vector on the tile and its ring (box rows 0..33, columns 3..36)
-        for (int k = threadIdx.x; k < CG_RW * CG_RW; k += CG_NT) {
-            const int rr = k / CG_RW, rc = k - rr * CG_RW;
-            const int bc = rc + CG_X0 - 1, gi = gi0 + bc;
-            double v;
-            if (XUP) {
-                const double xv = cg_at<double>(sb, S::A, S::WA, rr, bc, gi, A.nx);
-                const double pv = cg_at<double>(sb, S::B, S::WB, rr, bc, gi, A.nx);
-                v = xv + coef * pv;
-            } else {
-                const double pv = cg_at<double>(sb, S::A, S::WA, rr, bc, gi, A.nx);
-                const TZ zv = cg_at<TZ>(sb, S::B, S::WB, rr, bc, gi, A.nx);
-                v = double(zv) + coef * pv;
+        // edge tiles: the wrapped column -1 (first tile column) or nx (last) into the boxes,
+        // so that the passes below index the boxes alone
+        if (tx == 0 || tx == A.ntx - 1) {
+            const int bc = (tx == 0) ? CG_X0 - 1 : CG_X0 + CG_TS;   // box column of the wrapped cell
+            const int wc = (tx == 0) ? CG_WW - 1 : 0;               // its column in the strip
+            for (int r = threadIdx.x; r < CG_BH; r += CG_NT) {
+                double* a = reinterpret_cast<double*>(sb + S::A);
+                a[r * CG_BW + bc] = reinterpret_cast<const double*>(sb + S::WA)[r * CG_WW + wc];
+                typename Lay::TB* b = reinterpret_cast<typename Lay::TB*>(sb + S::B);
+                b[r * CG_BW + bc] = reinterpret_cast<const typename Lay::TB*>(sb + S::WB)[r * CG_WW + wc];
+                if (tx == A.ntx - 1) {   // the east weight of the last column is ax at nx (= ax at 0)
+                    double* ax = reinterpret_cast<double*>(sb + S::AX);
+                    ax[r * CG_BW + bc] = reinterpret_cast<const double*>(sb + S::WAX)[r * CG_WW + wc];
+                }
             }
-            ring[k] = v;
+            // order these shared-memory writes before the next TMA copy into this stage
+            tc::fence_async_smem();
+            __syncthreads();
+        }
+        // the updated vector on the tile and its ring: box rows 0..33, columns 3..36
+        {
+            const double* av = reinterpret_cast<const double*>(sb + S::A);
+            const typename Lay::TB* bv = reinterpret_cast<const typename Lay::TB*>(sb + S::B);
+            for (int k = threadIdx.x; k < CG_RW * CG_RW; k += CG_NT) {
+                const int rr = k / CG_RW, rc = k - rr * CG_RW;
+                const int q = rr * CG_BW + rc + CG_X0 - 1;
+                double v;
+                if (XUP) v = av[q] + coef * double(bv[q]);
+                else v = double(bv[q]) + coef * av[q];
+                ring[k] = v;
+            }
         }
         __syncthreads();
-        // the stencil on the tile
-        for (int k = threadIdx.x; k < CG_TS * CG_TS; k += CG_NT) {
-            const int ty_ = k / CG_TS, tx_ = k - ty_ * CG_TS;
-            const int br = ty_ + 1, bc = tx_ + CG_X0, gi = gi0 + bc;
-            const int c = (ty_ + 1) * CG_RW + tx_ + 1;
-            const double aw = cg_at<double>(sb, S::AX, S::WAX, br, bc, gi, A.nx);
-            const double ae = cg_at<double>(sb, S::AX, S::WAX, br, bc + 1, gi + 1, A.nx);
-            const double* ayb = reinterpret_cast<const double*>(sb + S::AY);
-            const double as = ayb[br * CG_BW + bc], an = ayb[(br + 1) * CG_BW + bc];
-            double ss = aw * ring[c - 1];
-            ss += ae * ring[c + 1];
-            ss += as * ring[c - CG_RW];
-            ss += an * ring[c + CG_RW];
-            double dd = aw;
-            dd += ae;
-            dd += as;
-            dd += an;
-            const double v = ring[c];
-            const size_t g = (size_t)(ty * CG_TS + ty_) * A.nx + tx * CG_TS + tx_;
-            if (XUP) {
-                const double fv = reinterpret_cast<const double*>(sb + S::C)[br * CG_BW + bc];
-                const double r = fv - (ss - dd * v);
-                acc += r * r;
-                A.xbuf[par ^ 1][g] = v;
-                reinterpret_cast<TZ*>(A.r_out)[g] = TZ(r);
-            } else {
-                const double q = ss - dd * v;
-                acc += v * q;
-                A.pbuf[par ^ 1][g] = v;
+        // the stencil on the tile: thread t owns cells 2 (t % 16) and 2 (t % 16) + 1 of row t / 16
+        {
+            const int ty_ = threadIdx.x >> 4, tx0 = (threadIdx.x & 15) * 2;
+            const int br = ty_ + 1, bc = tx0 + CG_X0;
+            const double* axb = reinterpret_cast<const double*>(sb + S::AX) + br * CG_BW + bc;
+            const double* ayb = reinterpret_cast<const double*>(sb + S::AY) + br * CG_BW + bc;
+            const double* rg = ring + (ty_ + 1) * CG_RW + tx0 + 1;
+            const size_t g = (size_t)(ty * CG_TS + ty_) * A.nx + tx * CG_TS + tx0;
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const double aw = axb[e], ae = axb[e + 1], as = ayb[e], an = ayb[e + CG_BW];
+                const double* c = rg + e;
+                double ss = aw * c[-1];
+                ss += ae * c[1];
+                ss += as * c[-CG_RW];
+                ss += an * c[CG_RW];
+                double dd = aw;
+                dd += ae;
+                dd += as;
+                dd += an;
+                const double v = c[0];
+                if (XUP) {
+                    const double fv = reinterpret_cast<const double*>(sb + S::C)[br * CG_BW + bc + e];
+                    const double r = fv - (ss - dd * v);
+                    acc += r * r;
+                    A.xbuf[par ^ 1][g + e] = v;
+                    reinterpret_cast<TZ*>(A.r_out)[g + e] = TZ(r);
+                } else {
+                    const double q = ss - dd * v;
+                    acc += v * q;
+                    A.pbuf[par ^ 1][g + e] = v;
+                }
             }
         }
         __syncthreads();   // the ring and this stage are free again
