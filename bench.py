@@ -433,6 +433,15 @@ def film_leg(dev, flush, steps=10, warmup=2, compare=True):
     return out
 
 
+def oracle_error(case, nlevels, p_gpu, mixed=False):
+    """Relative L2 difference of a GPU solution from the FP64 oracle's solve of the same
+    system to the same tolerance (the oracle's C++ multigrid-PCG with the GPU's cycle)."""
+    from oracle import oracle
+    p_ref, _, _, _, st = oracle.mg_solve(case.f, case.bx, case.by, case.hx, case.hy, nlevels=nlevels, ncoarse=1,
+                                         sym=5, method="pcg", mixed=False, rtol=RTOL, max_cycles=200, native=True)
+    return float(np.linalg.norm(p_gpu - p_ref) / np.linalg.norm(p_ref))
+
+
 # ------------------------------------------------------------------ GPU leg
 ALG_BYTES_PER_CELL = {  # FP64, level 0: each distinct array read or written once per cell
     "down0": 8 * (3 + 1 + 0.25),       # read f, bx, by; write u, f_coarse
@@ -515,6 +524,7 @@ def run_ours(args):
     barrier()
     launches = native.launch_count() - l0
     clk = clocks.stop()
+    p_last = p.cpu().numpy()
     total_ms = sum(a.elapsed_time(b) for a, b in ev)
     total_ms = slowest(total_ms)
     value = world * args.steps / (total_ms / 1e3)
@@ -629,7 +639,9 @@ def run_ours(args):
             evm[k][1].record(stream)
         torch.cuda.synchronize(dev)
         mms = sum(a.elapsed_time(b) for a, b in evm)
+        err_mixed = oracle_error(case, nlevels, p.cpu().numpy()) if not args.skip_cpu else None
         variants["mixed"] = {"value": ke / (mms / 1e3), "unit": UNIT, "iterations": itm[-1],
+                             "rel_l2_error_vs_fp64_oracle": err_mixed,
                              "note": "FP32 smoothing/restriction/prolongation, FP64 residual, CG and coarsest solve"}
         sm.close()
         if not args.skip_2048 and n == N:
@@ -653,7 +665,9 @@ def run_ours(args):
                     ev2[k][1].record(stream)
                 torch.cuda.synchronize(dev)
                 ms2 = sum(a.elapsed_time(b) for a, b in ev2)
+                err2 = oracle_error(c2, nlevels + 1, p2.cpu().numpy()) if not args.skip_cpu else None
                 variants[f"{prec}_2048"] = {"value": ke / (ms2 / 1e3), "unit": UNIT, "iterations": it2[-1],
+                                            "rel_l2_error_vs_fp64_oracle": err2,
                                             "note": "the same 64 bubbles in the unit domain at 2048x2048 (radii "
                                                     "16-96 cells), 7 levels"}
                 s2.close()
@@ -673,6 +687,7 @@ def run_ours(args):
                     "vcycles_saved": itm[-1] - lg["mixed"]["iterations"],
                     "note": "mixed-precision MG-PCG from the U-Net guess (guess + check + solve per step)"}
 
+    err_headline = oracle_error(case, nlevels, p_last) if (rank == 0 and not args.skip_cpu) else None
     if rank == 0 and world == 1 and not args.skip_cpu and n == N:
         threads = os.cpu_count()
         times, cits = cpu_solves(case, 15.0, 30)
@@ -824,6 +839,7 @@ def finish(args, v):
             "data": "synthetic",
             "config": bench_config(n, v["nlevels"], args.ncoarse, args.precision, v["world"]),
             "iterations": v["its"][-1], "rel_residual": v["rel"],
+            "rel_l2_error_vs_fp64_oracle": v.get("err_headline"),
             "roofline": v["roofline"], "cpu_baseline": v["cpu"], "e2e": v["e2e"], "gpu_launches": int(v["launches"]),
             "clocks": v["clk"], "variants": v["variants"], "rk3": v.get("rk3"),
         }

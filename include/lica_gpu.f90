@@ -120,6 +120,21 @@ module lica_gpu
     integer(c_int32_t) :: ipzero
   end type lica_fld_options
 
+  type, bind(c) :: lica_col_geometry
+    type(c_ptr) :: z
+    type(c_ptr) :: zp
+    type(c_ptr) :: sdz
+    type(c_ptr) :: vdz
+    type(c_ptr) :: ssdz
+    type(c_ptr) :: vvdz
+    type(c_ptr) :: kcou1
+    type(c_ptr) :: kcou2
+    type(c_ptr) :: kcoump1
+    type(c_ptr) :: kcoump2
+    type(c_ptr) :: kcou_vel
+    type(c_ptr) :: kcoump_vel
+  end type lica_col_geometry
+
   type, bind(c) :: lica_film2d_props
     real(c_double) :: re
     real(c_double) :: visr
@@ -544,6 +559,57 @@ module lica_gpu
       integer(c_int32_t), value :: nsteps
       integer(c_int32_t), intent(inout) :: status(*)
     end function lica_gpu_column_steps
+
+    integer(c_int) function lica_gpu_column_init_geometry(n, length, z0, props, geo, st) &
+        bind(c, name="lica_gpu_column_init_geometry")
+      import
+      integer(c_int32_t), value :: n
+      real(c_double), value :: length
+      real(c_double), value :: z0
+      type(lica_col_props), intent(in) :: props
+      type(lica_col_geometry), intent(in) :: geo
+      type(lica_col_state), intent(inout) :: st
+    end function lica_gpu_column_init_geometry
+
+    integer(c_int) function lica_gpu_column_geometry_create(out, n, length, geo) &
+        bind(c, name="lica_gpu_column_geometry_create")
+      import
+      type(c_ptr), intent(out) :: out
+      integer(c_int32_t), value :: n
+      real(c_double), value :: length
+      type(lica_col_geometry), intent(in) :: geo
+    end function lica_gpu_column_geometry_create
+
+    integer(c_int) function lica_gpu_column_geometry_destroy(geo) &
+        bind(c, name="lica_gpu_column_geometry_destroy")
+      import
+      type(c_ptr), value :: geo
+    end function lica_gpu_column_geometry_destroy
+
+    integer(c_int) function lica_gpu_column_steps_geometry_device(geo, ncol, props, st, nsteps, &
+        threads, scratch, status, stream) bind(c, name="lica_gpu_column_steps_geometry_device")
+      import
+      type(c_ptr), value :: geo
+      integer(c_int32_t), value :: ncol
+      type(lica_col_props), intent(in) :: props
+      type(lica_col_state), intent(in) :: st
+      integer(c_int32_t), value :: nsteps
+      integer(c_int32_t), value :: threads
+      type(c_ptr), value :: scratch
+      type(c_ptr), value :: status
+      type(c_ptr), value :: stream
+    end function lica_gpu_column_steps_geometry_device
+
+    integer(c_int) function lica_gpu_column_steps_geometry(geo, ncol, props, st, nsteps, status) &
+        bind(c, name="lica_gpu_column_steps_geometry")
+      import
+      type(c_ptr), value :: geo
+      integer(c_int32_t), value :: ncol
+      type(lica_col_props), intent(in) :: props
+      type(lica_col_state), intent(inout) :: st
+      integer(c_int32_t), value :: nsteps
+      integer(c_int32_t), intent(inout) :: status(*)
+    end function lica_gpu_column_steps_geometry
 
     integer(c_int) function lica_gpu_lvs_transport_device(ncol, n, length, phi, layer, psif, &
         wo, w, mflvs, vol_tot_ori, vol_tot_iphs, psi_cn, psi_zn, status, stats, prm, stream) &

@@ -393,6 +393,43 @@ int lica_gpu_column_batch_steps_device(const lica_col_batch* batch, const lica_c
 int lica_gpu_column_steps(int32_t ncol, int32_t n, double length, const lica_col_props* props,
                           lica_col_state* st, int32_t nsteps, int32_t* status);
 
+/* Stretched columns: a flow grid of n cells on faces Z(1..n+1) (GEOMETRIC, 1d.f:4808-4882;
+ * any spacing whose cells are at least one refined cell, length/(2n), wide) under the
+ * uniform level-set grid of 2n cells (GEOMETRIC_LVS, 1d.f:4885), coupled by the z tables of
+ * GEOM_COUPLING (1d.f:5037-5370).  Host arrays, Fortran index as offset:
+ *   z, zp, sdz, vdz, ssdz, vvdz : n+2 doubles, k = 0..n+1 (z[k] = Z(k), z[0] unused)
+ *   kcou1, kcou2               : n+5 int32, K = -1..n+3 at [K+1]
+ *   kcoump1, kcoump2           : n+4 int32, K = -1..n+2 at [K+1]
+ *   kcou_vel, kcoump_vel       : 2n+2 int32, k = 0..2n+1 at [k]
+ * (lica_grid_metrics and lica_grid_coupling_z produce them).  Every routine of the step
+ * that the uniform column evaluates in closed form -- CAL_DENVIS's upwind boxes, the
+ * GRID_COUPLING boxes, PHINSINTP, VEL_INTP, TEMP_GRAD's flow lookups, the metric factors --
+ * reads these instead. */
+typedef struct {
+    const double *z, *zp, *sdz, *vdz, *ssdz, *vvdz;
+    const int32_t *kcou1, *kcou2, *kcoump1, *kcoump2, *kcou_vel, *kcoump_vel;
+} lica_col_geometry;
+
+/* lica_gpu_column_init on a stretched column (MAKEFLD's profile at ZP, GRID_COUPLING(1)'s
+ * boxes from the tables); LICA_BAD_ARG for a geometry that does not rise from 0 to length,
+ * has a cell narrower than a refined cell, or a table entry outside the grid. */
+int lica_gpu_column_init_geometry(int32_t n, double length, double z0, const lica_col_props* props,
+                                  const lica_col_geometry* geo, lica_col_state* st);
+
+/* A checked device copy of a geometry (the same checks); every column of the steps below
+ * is that column. */
+typedef struct lica_col_geo lica_col_geo;
+int lica_gpu_column_geometry_create(lica_col_geo** out, int32_t n, double length, const lica_col_geometry* geo);
+int lica_gpu_column_geometry_destroy(lica_col_geo* geo);
+
+/* lica_gpu_column_steps_device / lica_gpu_column_steps for ncol stretched columns of the
+ * geometry's n and length. */
+int lica_gpu_column_steps_geometry_device(const lica_col_geo* geo, int32_t ncol, const lica_col_props* props,
+                                          const lica_col_state* st, int32_t nsteps, int32_t threads, void* scratch,
+                                          int32_t* status, void* stream);
+int lica_gpu_column_steps_geometry(const lica_col_geo* geo, int32_t ncol, const lica_col_props* props,
+                                   lica_col_state* st, int32_t nsteps, int32_t* status);
+
 int lica_gpu_lvs_transport_device(int32_t ncol, int32_t n, double length, double* phi, int32_t* layer,
                                   double* psif, double* wo, const double* w, const double* mflvs,
                                   double* vol_tot_ori, const double* vol_tot_iphs, double* psi_cn,

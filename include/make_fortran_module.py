@@ -45,7 +45,7 @@ def parse(txt):
             decl = " ".join(decl.split())
             if not decl:
                 continue
-            m = re.match(r"(\w+)\s*(.*)", decl)
+            m = re.match(r"(?:const\s+)?(\w+)\s*(.*)", decl)
             ctype, rest = m.group(1), m.group(2)
             for d in rest.split(","):
                 d = d.strip()

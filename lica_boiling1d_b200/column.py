@@ -58,13 +58,54 @@ def _shapes(ncol, n):
             "sfgas2": (sq, np.float64), "imask": (sf, np.int32), "scal": (5, np.float64), "stats": (8, np.float64)}
 
 
-class Columns:
-    """State of ncol columns of n flow cells over a column of the given length."""
+class ColumnGeometry:
+    """The flow grid of a stretched column: n cells on the faces Z(1..n+1) = faces (rising
+    from 0 to the column length, no cell narrower than length / 2n) under the uniform
+    level-set grid of 2n cells -- GEOMETRIC's arrays and GEOM_COUPLING's z tables
+    (lica_col_geometry), and their checked device copy (lica_gpu_column_geometry_create),
+    made on first use."""
 
-    def __init__(self, n, length, arrays):
+    def __init__(self, faces):
+        from .grid import column_geometry
+        faces = np.ascontiguousarray(faces, dtype=np.float64)
+        self.n, self.length = len(faces) - 1, float(faces[-1])
+        self.faces = faces
+        self.arrays = column_geometry(faces, self.length)
+        self._h = None
+
+    @staticmethod
+    def tanh(n, length, gam):
+        """HYPTAN clustering at both walls (grid.f:383-420, XSI = 0.5): n cells."""
+        from .grid import Section, section
+        faces = np.zeros(n + 1)
+        section(Section(3, 0.0, float(length), 1, n + 1, 3, float(gam), 0.5), faces)
+        return ColumnGeometry(faces)
+
+    def c(self):
+        """The lica_col_geometry of the host arrays (valid while self lives)."""
+        return native.ColGeometry(*[self.arrays[k].ctypes.data for k in native.GEO_FIELDS])
+
+    def handle(self):
+        if self._h is None:
+            h = C.c_void_p()
+            g = self.c()
+            native.check(native.lib().lica_gpu_column_geometry_create(C.byref(h), self.n, self.length, C.byref(g)),
+                         "lica_gpu_column_geometry_create")
+            self._h = _GeoHandle(h.value)
+        return self._h.ptr
+
+
+class Columns:
+    """State of ncol columns of n flow cells over a column of the given length; geometry:
+    a ColumnGeometry all the columns share (a stretched flow grid), or None (uniform)."""
+
+    def __init__(self, n, length, arrays, geometry=None):
         self.n, self.length = int(n), float(length)
         self.arrays = arrays
         self.ncol = arrays["w"].shape[0]
+        self.geometry = geometry
+        if geometry is not None and (geometry.n != self.n or abs(geometry.length - self.length) > 1e-12 * self.length):
+            raise ValueError("the geometry's size or length differs from the columns'")
 
     def __getattr__(self, k):
         a = self.__dict__.get("arrays")
@@ -77,20 +118,26 @@ class Columns:
         return not isinstance(self.arrays["w"], np.ndarray)
 
     @staticmethod
-    def empty(ncol, n, length):
-        return Columns(n, length, {k: np.zeros((ncol, m), dt) for k, (m, dt) in _shapes(ncol, n).items()})
+    def empty(ncol, n, length, geometry=None):
+        return Columns(n, length, {k: np.zeros((ncol, m), dt) for k, (m, dt) in _shapes(ncol, n).items()}, geometry)
 
     @staticmethod
-    def film(n, length, z0s, props):
+    def film(n, length, z0s, props, geometry=None):
         """Columns each holding a vapour film of thickness z0 at the wall (MAKEFLD +
-        LVSINIT + GRID_COUPLING(1), lica_gpu_column_init)."""
+        LVSINIT + GRID_COUPLING(1), lica_gpu_column_init; lica_gpu_column_init_geometry
+        on a stretched grid)."""
         z0s = np.atleast_1d(np.asarray(z0s, dtype=np.float64))
-        cols = Columns.empty(len(z0s), n, length)
+        cols = Columns.empty(len(z0s), n, length, geometry)
         cp = props.c()
+        g = geometry.c() if geometry is not None else None
         for c, z0 in enumerate(z0s):
             st = native.ColState(*[cols.arrays[k][c].ctypes.data for k in native.COL_FIELDS])
-            native.check(native.lib().lica_gpu_column_init(n, length, float(z0), C.byref(cp), C.byref(st)),
-                         "lica_gpu_column_init")
+            if g is None:
+                rc = native.lib().lica_gpu_column_init(n, length, float(z0), C.byref(cp), C.byref(st))
+            else:
+                rc = native.lib().lica_gpu_column_init_geometry(n, length, float(z0), C.byref(cp), C.byref(g),
+                                                                C.byref(st))
+            native.check(rc, "lica_gpu_column_init")
         return cols
 
     def to(self, device):
@@ -102,7 +149,7 @@ class Columns:
                 out[k] = v.detach().cpu().numpy() if isinstance(v, torch.Tensor) else v.copy()
             else:
                 out[k] = torch.as_tensor(v if isinstance(v, np.ndarray) else v.cpu().numpy(), device=device).clone()
-        return Columns(self.n, self.length, out)
+        return Columns(self.n, self.length, out, self.geometry)
 
     def _state(self, ptr):
         return native.ColState(*[ptr(self.arrays[k]) for k in native.COL_FIELDS])
@@ -119,19 +166,29 @@ class Columns:
                 if a.dtype != dt or not a.flags.c_contiguous or a.shape != (self.ncol, m):
                     raise TypeError(f"{k}: need a C-contiguous {np.dtype(dt).name} array of shape {(self.ncol, m)}")
             status = np.zeros(self.ncol, np.int32)
-            rc = L.lica_gpu_column_steps(self.ncol, self.n, self.length, C.byref(cp),
-                                         C.byref(self._state(lambda a: a.ctypes.data)), int(nsteps),
-                                         status.ctypes.data_as(C.POINTER(C.c_int32)))
+            st = self._state(lambda a: a.ctypes.data)
+            sp = status.ctypes.data_as(C.POINTER(C.c_int32))
+            if self.geometry is None:
+                rc = L.lica_gpu_column_steps(self.ncol, self.n, self.length, C.byref(cp), C.byref(st), int(nsteps), sp)
+            else:
+                rc = L.lica_gpu_column_steps_geometry(self.geometry.handle(), self.ncol, C.byref(cp), C.byref(st),
+                                                      int(nsteps), sp)
             native.check(rc, "column steps", ok=(0, 1, 2, 4))
             return status
         import torch
         dev = self.arrays["w"].device
         status = torch.zeros(self.ncol, dtype=torch.int32, device=dev)
         s = stream if stream is not None else torch.cuda.current_stream(dev)
-        rc = L.lica_gpu_column_steps_device(self.ncol, self.n, self.length, C.byref(cp),
-                                            C.byref(self._state(lambda a: a.data_ptr())), int(nsteps), int(threads),
-                                            C.c_void_p(scratch.data_ptr() if scratch is not None else None),
-                                            C.c_void_p(status.data_ptr()), C.c_void_p(s.cuda_stream))
+        st = self._state(lambda a: a.data_ptr())
+        scr = C.c_void_p(scratch.data_ptr() if scratch is not None else None)
+        if self.geometry is None:
+            rc = L.lica_gpu_column_steps_device(self.ncol, self.n, self.length, C.byref(cp), C.byref(st), int(nsteps),
+                                                int(threads), scr, C.c_void_p(status.data_ptr()),
+                                                C.c_void_p(s.cuda_stream))
+        else:
+            rc = L.lica_gpu_column_steps_geometry_device(self.geometry.handle(), self.ncol, C.byref(cp), C.byref(st),
+                                                         int(nsteps), int(threads), scr,
+                                                         C.c_void_p(status.data_ptr()), C.c_void_p(s.cuda_stream))
         native.check(rc, "column steps")
         return status
 
@@ -281,6 +338,17 @@ class _Handle:
     def __del__(self):
         try:
             native.lib().lica_gpu_column_batch_destroy(self.ptr)
+        except Exception:
+            pass
+
+
+class _GeoHandle:
+    def __init__(self, ptr):
+        self.ptr = ptr
+
+    def __del__(self):
+        try:
+            native.lib().lica_gpu_column_geometry_destroy(self.ptr)
         except Exception:
             pass
 

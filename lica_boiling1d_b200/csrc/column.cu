@@ -76,6 +76,8 @@ struct Args {
     int hist_cap;      // steps of one launch the history holds per column
     int tri_smem;      // 1: the tridiagonal arrays of columns with n <= tri_cap live in dynamic shared memory
     int tri_cap;       // longest column whose arrays fit the dynamic shared memory (longer ones use scratch)
+    int has_geo;       // 1: every column is the stretched column geo describes (device arrays)
+    col::ColGeoDev geo;
 };
 
 // one record of the optional interface history: TIME before the step, place, VOL_TOT_IPHS, DT
@@ -85,20 +87,31 @@ constexpr int HIST_REC = 4;
 enum { PH_DT, PH_CONT, PH_ENERGY, PH_TEMPGRAD, PH_EXTP, PH_CONT2, PH_RHSZ, PH_LHSW, PH_PRESS, PH_CONV, PH_TRANSPORT,
        PH_COUNT };
 
+// The column's wall-normal geometry: GEOMETRIC's arrays and GEOM_COUPLING's z tables of a
+// stretched column (cg), or the closed forms of the uniform one.
 struct Geo {
     int n, nf;
     double h, hf;
     double ih, ihalf;   // 1/h (SSDZ, VVDZ inside) and 1/(h/2) (VVDZ at the walls), computed once
-    __device__ Geo(int n_, double L) : n(n_), nf(2 * n_), h(L / n_), hf(L / (2 * n_)) {
+    const col::ColGeoDev* cg;
+    __device__ Geo(int n_, double L, const col::ColGeoDev* cg_ = nullptr)
+        : n(n_), nf(2 * n_), h(L / n_), hf(L / (2 * n_)), cg(cg_) {
         ih = 1.0 / h;
         ihalf = 1.0 / (0.5 * h);
     }
-    __device__ double sdz(int k) const { return (k >= 1 && k <= n) ? h : 0.0; }
-    __device__ double ssdz(int) const { return ih; }
-    __device__ double vdz(int k) const { return (k == 1 || k == n + 1) ? 0.5 * h : h; }
-    __device__ double vvdz(int k) const { return (k == 1 || k == n + 1) ? ihalf : ih; }
-    __device__ double z(int k) const { return col::grid_z(h, k); }
-    __device__ double zp(int k) const { return col::grid_zp(h, n, k); }
+    __device__ double sdz(int k) const { return cg ? cg->sdz[k] : ((k >= 1 && k <= n) ? h : 0.0); }
+    __device__ double ssdz(int k) const { return cg ? cg->ssdz[k] : ih; }
+    __device__ double vdz(int k) const { return cg ? cg->vdz[k] : ((k == 1 || k == n + 1) ? 0.5 * h : h); }
+    __device__ double vvdz(int k) const { return cg ? cg->vvdz[k] : ((k == 1 || k == n + 1) ? ihalf : ih); }
+    __device__ double z(int k) const { return cg ? cg->z[k] : col::grid_z(h, k); }
+    __device__ double zp(int k) const { return cg ? cg->zp[k] : col::grid_zp(h, n, k); }
+    // GEOM_COUPLING's refined faces (uniform column: face K is refined face 2K-1, centre K
+    // refined face 2K) and KCOUMP_VEL of a refined cell
+    __device__ int kcou1(int k) const { return cg ? cg->kcou1[k + 1] : 2 * k - 2; }
+    __device__ int kcou2(int k) const { return cg ? cg->kcou2[k + 1] : 2 * k - 1; }
+    __device__ int kcoump1(int k) const { return cg ? cg->kcoump1[k + 1] : 2 * k - 1; }
+    __device__ int kcoump2(int k) const { return cg ? cg->kcoump2[k + 1] : 2 * k; }
+    __device__ int kcoump_vel(int k) const { return cg ? cg->kcoump_vel[k] : col::kcoump_vel(h, hf, n, k); }
     __device__ double zpf(int k) const { return col::grid_zpf(hf, k); }
     __device__ double akw(int k) const { return -vvdz(k) * ssdz(k - 1); }
     __device__ double ckw(int k) const { return -vvdz(k) * ssdz(k); }
@@ -258,13 +271,13 @@ __device__ void cal_continuity(const Geo& g, const Phys& ph, Col& c, double dtco
                     if (wt >= 0.0) {
                         z1 = g.zp(k) - wt * dtconst;
                         z2 = g.zp(k);
-                        k1 = 2 * (k - 1);
-                        k2 = 2 * k - 1;
+                        k1 = g.kcoump2(k - 1);
+                        k2 = g.kcoump1(k);
                     } else {
                         z1 = g.zp(k);
                         z2 = g.zp(k) - wt * dtconst;
-                        k1 = 2 * k;
-                        k2 = 2 * k + 1;
+                        k1 = g.kcoump2(k);
+                        k2 = g.kcoump1(k + 1);
                     }
                     ps = col::box_mean(c.psif, nf, k1, k2, z1, z2, g.hf);
                 }
@@ -289,13 +302,13 @@ __device__ void cal_continuity(const Geo& g, const Phys& ph, Col& c, double dtco
                     if (wt >= 0.0) {
                         z1 = g.z(k + 1) - wt * dtconst;
                         z2 = g.z(k + 1);
-                        k1 = 2 * k - 1;
-                        k2 = 2 * k;
+                        k1 = g.kcou2(k);
+                        k2 = g.kcou1(k + 1);
                     } else {
                         z1 = g.z(k + 1);
                         z2 = g.z(k + 1) - wt * dtconst;
-                        k1 = 2 * k + 1;
-                        k2 = 2 * k + 2;
+                        k1 = g.kcou2(k + 1);
+                        k2 = g.kcou1(k + 2);
                     }
                     ps = col::box_mean(c.psif, nf, k1, k2, z1, z2, g.hf);
                 }
@@ -772,11 +785,11 @@ __device__ int temp_grad(const Geo& g, const Phys& ph, Col& c, Shared& sh, doubl
             int ic = 0;
             for (int j = s->lstart[1]; j < s->lstart[lvs::NN2 + 1]; ++j) {
                 const int k = cx.w0 + s->lst[j];
-                const int kk = col::kcoump_vel(g.h, g.hf, n, k);
+                const int kk = g.kcoump_vel(k);
                 const int x = kk - xk0;
                 if (sh.x_nphi[x] == 0.0) {
-                    const int k1 = 2 * kk - 1, k2 = 2 * kk;
-                    const double zd = (g.zp(kk) - g.zpf(k1)) / (g.zpf(k2) - g.zpf(k1));
+                    const int k1 = g.kcou2(kk), k2 = g.kcoump2(kk);   // PHINSINTP's KCOU2(KO), KCOUMP2(KO)
+                    const double zd = (k1 == k2) ? 0.0 : (g.zp(kk) - g.zpf(k1)) / (g.zpf(k2) - g.zpf(k1));
                     const double a1 = cx.p(k1), a2 = cx.p(k2);
                     const double c00 = a1 * (1.0 - 0.5) + a1 * 0.5;
                     const double c01 = a2 * (1.0 - 0.5) + a2 * 0.5;
@@ -794,7 +807,7 @@ __device__ int temp_grad(const Geo& g, const Phys& ph, Col& c, Shared& sh, doubl
             }
             for (int j = s->lstart[lvs::N_MAX]; j < s->lstart[lvs::N_MAX + 1]; ++j) {
                 const int k = cx.w0 + s->lst[j];
-                const int kk = col::kcoump_vel(g.h, g.hf, n, k);
+                const int kk = g.kcoump_vel(k);
                 const int x = kk - xk0;
                 const double dx = 0.25, dy = 0.25;
                 const double dz = g.zpf(k) - g.zp(kk);
@@ -805,7 +818,7 @@ __device__ int temp_grad(const Geo& g, const Phys& ph, Col& c, Shared& sh, doubl
             // extension range: the cells with NPHI != 0
             int ka = n + 1, kb = 0;
             for (int j = s->lstart[1]; j < s->lstart[lvs::N_MAX + 1]; ++j) {
-                const int kk = col::kcoump_vel(g.h, g.hf, n, cx.w0 + s->lst[j]);
+                const int kk = g.kcoump_vel(cx.w0 + s->lst[j]);
                 if (sh.x_nphi[kk - xk0] != 0.0) {
                     ka = min(ka, kk);
                     kb = max(kb, kk);
@@ -842,7 +855,7 @@ __device__ int temp_grad(const Geo& g, const Phys& ph, Col& c, Shared& sh, doubl
                 const int k = cx.w0 + i, m = s->layer[i];
                 double v0 = 0.0, v1 = 0.0;
                 if (m >= 1 && m <= lvs::NN1) {
-                    const int kk = col::kcoump_vel(g.h, g.hf, n, k);
+                    const int kk = g.kcoump_vel(k);
                     int kk1, kk2;
                     double zd;
                     if (g.zp(kk) > g.zpf(k)) {
@@ -978,7 +991,7 @@ __device__ int temp_grad(const Geo& g, const Phys& ph, Col& c, Shared& sh, doubl
     // (7) CAL_PSI_TMP(1) and IMASK_PH on the z faces (chphase.f:297-357)
     double* psi_tmp = c.a[S_PSITMP];
     FOR_K(1, n) {
-        const double v = col::box_mean(c.psif_mtp, nf, 2 * k - 1, 2 * k, g.z(k), g.z(k + 1), g.hf);
+        const double v = col::box_mean(c.psif_mtp, nf, g.kcou2(k), g.kcou1(k + 1), g.z(k), g.z(k + 1), g.hf);
         psi_tmp[k] = (v <= 1e-3) ? 0.0 : (v >= 0.999 ? 1.0 : v);
     }
     __syncthreads();
@@ -995,11 +1008,12 @@ __device__ void cal_continuity2(const Geo& g, const Phys& ph, Col& c) {
     FOR_K(1, n) {
         if (k >= 2) {
             double v = psi_z[k];
-            if (reg[k] == 2) v = v - col::box_mean(c.sfgas2, nf, 2 * k - 1, 2 * k, g.zp(k - 1), g.zp(k), g.hf);
+            if (reg[k] == 2)
+                v = v - col::box_mean(c.sfgas2, nf, g.kcou2(k), g.kcou1(k + 1), g.zp(k - 1), g.zp(k), g.hf);
             psi_z[k] = (v > 1.0) ? 1.0 : (v < 0.0 ? 0.0 : v);
         }
         double v = psi_c[k];
-        if (reg[k] == 2) v = v - col::box_mean(c.sfgas2, nf, 2 * k - 1, 2 * k, g.z(k), g.z(k + 1), g.hf);
+        if (reg[k] == 2) v = v - col::box_mean(c.sfgas2, nf, g.kcou2(k), g.kcou1(k + 1), g.z(k), g.z(k + 1), g.hf);
         psi_c[k] = (v > 1.0) ? 1.0 : (v < 0.0 ? 0.0 : v);
     }
     __syncthreads();
@@ -1155,7 +1169,7 @@ __device__ void pressure_correction(const Geo& g, const Phys& ph, Col& c, Shared
         FOR_K(1, n) {
             double d = (k <= n - 1) ? (c.w[k + 1] - c.w[k]) * g.ssdz(k) : 0.0;
             if (ph.iphs == 1) {
-                const double ssum = col::box_mean(c.sfgas, g.nf, 2 * k - 1, 2 * k, g.z(k), g.z(k + 1), g.hf);
+                const double ssum = col::box_mean(c.sfgas, g.nf, g.kcou2(k), g.kcou1(k + 1), g.z(k), g.z(k + 1), g.hf);
                 d = d - ssum * (ph.den_diff / (ph.denp * ph.denm));
             }
             if (k >= 2) d = d * dtconsti;
@@ -1248,7 +1262,7 @@ __device__ int column_step(const Geo& g, const Phys& ph, Col& c, Shared& sh, dou
         FOR_K(1, n) {
             double d = (c.w[k + 1] - c.w[k]) * g.ssdz(k);
             if (ph.iphs == 1) {
-                const double ssum = col::box_mean(c.sfgas, g.nf, 2 * k - 1, 2 * k, g.z(k), g.z(k + 1), g.hf);
+                const double ssum = col::box_mean(c.sfgas, g.nf, g.kcou2(k), g.kcou1(k + 1), g.z(k), g.z(k + 1), g.hf);
                 d = d - ssum * (ph.den_diff / ph.denp);
             }
             dv = fmax(fabs(d), dv);
@@ -1263,7 +1277,7 @@ __device__ int column_step(const Geo& g, const Phys& ph, Col& c, Shared& sh, dou
             double lst[4] = {0, 0, 0, 0};
             double* st4 = c.stats + 4;   // scratch for the transport statistics
             const int st = lvs::transport_column(&sh.win, lane, n, L, c.phi, c.layer, c.psif, c.wo, c.w, c.mflvs,
-                                                 &c.scal[3], c.scal[4], c.psi_cn, c.psi_zn, st4, P);
+                                                 &c.scal[3], c.scal[4], c.psi_cn, c.psi_zn, st4, P, g.cg);
             __syncwarp();
             if (lane == 0) {
                 for (int q = 0; q < 4; ++q) lst[q] = st4[q];
@@ -1368,7 +1382,7 @@ __global__ void __launch_bounds__(NTH, NTH == 64 ? 5 : 1) k_column_steps(const _
     c.region = A.iscr + oi;
     c.prof = A.prof ? A.prof + (size_t)col * PH_COUNT : nullptr;
     c.t0 = clock64();
-    const Geo g(n, L);
+    const Geo g(n, L, A.has_geo ? &A.geo : nullptr);
     int st = LICA_OK;
     double* hist = A.hist ? A.hist + (size_t)col * A.hist_cap * HIST_REC : nullptr;
     for (int s = 0; s < A.nsteps && st == LICA_OK; ++s) {
@@ -1545,25 +1559,29 @@ extern "C" {
 // for one plane, to: S-tube = the two cells around the interface, layer m at m-1 cells
 // from it (never k = 1 or nf+1), phi = the signed distance ASSIGN_LVS gives; PSIF is
 // CAL_PSIF_MTP(1, N_MAX) with the column fill, the vapour volume its (1 - PSIF) sum.
-int lica_gpu_column_init(int32_t n, double length, double z0, const lica_col_props* props, lica_col_state* st) {
+// geo: the flow grid of a stretched column (host arrays), or null for the uniform one.
+static int column_init(int32_t n, double length, double z0, const lica_col_props* props,
+                       const lica_col_geometry* geo, lica_col_state* st) {
     if (n < 8 || !(length > 0.0) || !props || !st || !st->w || !st->p || !st->t || !st->psi_cn || !st->psi_zn ||
         !st->phi || !st->layer || !st->psif || !st->wo || !st->mflvs || !st->sfgas || !st->sfgas2 || !st->imask ||
         !st->scal || !st->stats)
         return LICA_BAD_ARG;
     const int nf = 2 * n;
     const double h = length / n, hf = length / nf;
+    auto zp = [&](int k) { return geo ? geo->zp[k] : h_zp(h, n, k); };
+    auto zc = [&](int k) { return geo ? geo->z[k] : (k - 1) * h; };
     for (int k = 0; k <= n + 1; ++k) {
         st->w[k] = st->p[k] = st->t[k] = st->psi_cn[k] = st->psi_zn[k] = st->wo[k] = 0.0;
         st->imask[k] = 0;
     }
     for (int k = 1; k <= n; ++k) {
-        const double pbody = (h_zp(h, n, k) - z0) + 1e-12;
+        const double pbody = (zp(k) - z0) + 1e-12;
         if (pbody > 0.0) {
             st->t[k] = 1.0;
             st->w[k] = 1.0;
             st->w[n + 1] = 1.0;
         } else {
-            st->t[k] = 16.47 * h_zp(h, n, k);
+            st->t[k] = 16.47 * zp(k);
             st->t[0] = 0.0;
             st->w[k] = 0.0;
             st->w[1] = 0.0;
@@ -1628,13 +1646,15 @@ int lica_gpu_column_init(int32_t n, double length, double z0, const lica_col_pro
     }
     // GRID_COUPLING(1)
     for (int k = 2; k <= n; ++k)
-        st->psi_zn[k] = h_box_mean(st->psif, nf, 2 * k - 2, 2 * k - 1, h_zp(h, n, k - 1), h_zp(h, n, k), hf);
+        st->psi_zn[k] = h_box_mean(st->psif, nf, geo ? geo->kcoump2[k] : 2 * k - 2,
+                                   geo ? geo->kcoump1[k + 1] : 2 * k - 1, zp(k - 1), zp(k), hf);
     for (int k = 1; k <= n; ++k) {
         if (st->psi_zn[k] < 1e-3) st->psi_zn[k] = 0.0;
         else if (st->psi_zn[k] > 0.999) st->psi_zn[k] = 1.0;
     }
     for (int k = 1; k <= n; ++k)
-        st->psi_cn[k] = h_box_mean(st->psif, nf, 2 * k - 1, 2 * k, (k - 1) * h, k * h, hf);
+        st->psi_cn[k] = h_box_mean(st->psif, nf, geo ? geo->kcou2[k + 1] : 2 * k - 1, geo ? geo->kcou1[k + 2] : 2 * k,
+                                   zc(k), zc(k + 1), hf);
     for (int k = 1; k <= n; ++k) {
         if (st->psi_cn[k] < 1e-3) st->psi_cn[k] = 0.0;
         else if (st->psi_cn[k] > 0.999) st->psi_cn[k] = 1.0;
@@ -1648,6 +1668,45 @@ int lica_gpu_column_init(int32_t n, double length, double z0, const lica_col_pro
     st->scal[4] = vol;
     for (int q = 0; q < 8; ++q) st->stats[q] = 0.0;
     return LICA_OK;
+}
+
+// A stretched column's geometry is accepted when its faces rise, span [0, length], no cell
+// is narrower than a refined cell (the level-set band's flow-face window assumes it), the
+// velocity tables name flow cells and the box tables stay near the refined grid (the box
+// sums clamp their reads to it).
+static int geometry_ok(int32_t n, double length, const lica_col_geometry* geo) {
+    if (!geo || !geo->z || !geo->zp || !geo->sdz || !geo->vdz || !geo->ssdz || !geo->vvdz || !geo->kcou1 ||
+        !geo->kcou2 || !geo->kcoump1 || !geo->kcoump2 || !geo->kcou_vel || !geo->kcoump_vel)
+        return 0;
+    const double hf = length / (2.0 * n);
+    if (std::fabs(geo->z[1]) > 1e-12 * length || std::fabs(geo->z[n + 1] - length) > 1e-12 * length) return 0;
+    for (int k = 1; k <= n; ++k)
+        if (!(geo->z[k + 1] - geo->z[k] >= hf * (1.0 - 1e-12))) return 0;
+    for (int k = 1; k <= 2 * n; ++k)
+        if (geo->kcou_vel[k] < 1 || geo->kcou_vel[k] > n || geo->kcoump_vel[k] < 1 || geo->kcoump_vel[k] > n + 1)
+            return 0;
+    for (int k = -1; k <= n + 2; ++k) {
+        const int a = geo->kcou1[k + 1], b = geo->kcou2[k + 1];
+        if (a < -8 || a > 2 * n + 8 || b < -8 || b > 2 * n + 8) return 0;
+    }
+    for (int k = -1; k <= n + 1; ++k) {
+        const int a = geo->kcoump1[k + 1], b = geo->kcoump2[k + 1];
+        if (a < -8 || a > 2 * n + 8 || b < -8 || b > 2 * n + 8) return 0;
+    }
+    return 1;
+}
+
+int lica_gpu_column_init(int32_t n, double length, double z0, const lica_col_props* props, lica_col_state* st) {
+    return column_init(n, length, z0, props, nullptr, st);
+}
+
+int lica_gpu_column_init_geometry(int32_t n, double length, double z0, const lica_col_props* props,
+                                  const lica_col_geometry* geo, lica_col_state* st) {
+    if (n < 8 || !(length > 0.0) || !geometry_ok(n, length, geo)) {
+        lica_set_last_error("lica_gpu_column_init_geometry", "bad column geometry", __FILE__, __LINE__);
+        return LICA_BAD_ARG;
+    }
+    return column_init(n, length, z0, props, geo, st);
 }
 
 int lica_gpu_column_history_device(double* hist, int32_t capacity) {
@@ -1771,14 +1830,28 @@ struct lica_col_batch {
 
 extern "C" {
 
-int lica_gpu_column_steps_device(int32_t ncol, int32_t n, double length, const lica_col_props* props,
-                                 const lica_col_state* st, int32_t nsteps, int32_t threads, void* scratch,
-                                 int32_t* status, void* stream) {
+}  // extern "C"
+
+// A stretched column's geometry on the device (lica_gpu_column_geometry_create).
+struct lica_col_geo {
+    int n = 0;
+    double length = 0.0;
+    void* buf = nullptr;
+    col::ColGeoDev dev{};
+};
+
+namespace {
+
+int column_steps_device(int32_t ncol, int32_t n, double length, const lica_col_props* props, const lica_col_state* st,
+                        int32_t nsteps, int32_t threads, void* scratch, int32_t* status, void* stream,
+                        const lica_col_geo* geo) {
     if (ncol < 1 || n < 8 || n > (1 << 20) || !(length > 0.0) || !props || !state_ok(st) || nsteps < 0 || !status) {
         lica_set_last_error("lica_gpu_column_steps_device", "bad sizes or null pointers", __FILE__, __LINE__);
         return LICA_BAD_ARG;
     }
     colk::Args A{};
+    A.has_geo = geo ? 1 : 0;
+    if (geo) A.geo = geo->dev;
     A.ncol = ncol;
     A.n = n;
     A.nsteps = nsteps;
@@ -1800,6 +1873,79 @@ int lica_gpu_column_steps_device(int32_t ncol, int32_t n, double length, const l
     A.dscr = (double*)scr;
     A.iscr = (int*)((char*)scr + (size_t)ncol * (colk::NFLOW * sf + sq) * sizeof(double));
     return launch_columns(A, n, threads, stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+int lica_gpu_column_steps_device(int32_t ncol, int32_t n, double length, const lica_col_props* props,
+                                 const lica_col_state* st, int32_t nsteps, int32_t threads, void* scratch,
+                                 int32_t* status, void* stream) {
+    return column_steps_device(ncol, n, length, props, st, nsteps, threads, scratch, status, stream, nullptr);
+}
+
+int lica_gpu_column_geometry_create(lica_col_geo** out, int32_t n, double length, const lica_col_geometry* host) {
+    if (!out) return LICA_BAD_ARG;
+    *out = nullptr;
+    if (n < 8 || n > (1 << 20) || !(length > 0.0) || !geometry_ok(n, length, host)) {
+        lica_set_last_error("lica_gpu_column_geometry_create", "bad column geometry", __FILE__, __LINE__);
+        return LICA_BAD_ARG;
+    }
+    // one device buffer: six double arrays of n+2, then the int tables (n+5, n+5, n+4, n+4,
+    // 2n+2, 2n+2), each 256-byte aligned
+    const size_t nd = (size_t)n + 2;
+    const size_t ni[6] = {(size_t)n + 5, (size_t)n + 5, (size_t)n + 4, (size_t)n + 4, 2 * (size_t)n + 2,
+                          2 * (size_t)n + 2};
+    const double* hd[6] = {host->z, host->zp, host->sdz, host->vdz, host->ssdz, host->vvdz};
+    const int32_t* hi[6] = {host->kcou1, host->kcou2, host->kcoump1, host->kcoump2, host->kcou_vel, host->kcoump_vel};
+    auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    size_t total = 6 * up(nd * sizeof(double));
+    for (int q = 0; q < 6; ++q) total += up(ni[q] * sizeof(int32_t));
+    auto* g = new lica_col_geo();
+    g->n = n;
+    g->length = length;
+    if (cudaMalloc(&g->buf, total) != cudaSuccess) {
+        delete g;
+        lica_set_last_error("lica_gpu_column_geometry_create", "cudaMalloc failed", __FILE__, __LINE__);
+        return LICA_ERR_CUDA;
+    }
+    char* p = (char*)g->buf;
+    const double* dd[6];
+    const int* di[6];
+    for (int q = 0; q < 6; ++q) {
+        dd[q] = (const double*)p;
+        if (cudaMemcpy(p, hd[q], nd * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+            lica_gpu_column_geometry_destroy(g);
+            return LICA_ERR_CUDA;
+        }
+        p += up(nd * sizeof(double));
+    }
+    for (int q = 0; q < 6; ++q) {
+        di[q] = (const int*)p;
+        if (cudaMemcpy(p, hi[q], ni[q] * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
+            lica_gpu_column_geometry_destroy(g);
+            return LICA_ERR_CUDA;
+        }
+        p += up(ni[q] * sizeof(int32_t));
+    }
+    g->dev = col::ColGeoDev{dd[0], dd[1], dd[2], dd[3], dd[4], dd[5], di[0], di[1], di[2], di[3], di[4], di[5]};
+    *out = g;
+    return LICA_OK;
+}
+
+int lica_gpu_column_geometry_destroy(lica_col_geo* g) {
+    if (!g) return LICA_OK;
+    if (g->buf) cudaFree(g->buf);
+    delete g;
+    return LICA_OK;
+}
+
+int lica_gpu_column_steps_geometry_device(const lica_col_geo* geo, int32_t ncol, const lica_col_props* props,
+                                          const lica_col_state* st, int32_t nsteps, int32_t threads, void* scratch,
+                                          int32_t* status, void* stream) {
+    if (!geo) return LICA_BAD_ARG;
+    return column_steps_device(ncol, geo->n, geo->length, props, st, nsteps, threads, scratch, status, stream, geo);
 }
 
 int lica_gpu_column_batch_create(lica_col_batch** out, int32_t ncol, const int32_t* n, const double* length,
@@ -1909,8 +2055,12 @@ int lica_gpu_column_batch_steps_device(const lica_col_batch* b, const lica_col_s
     return launch_columns(A, b->nmax, threads, stream);
 }
 
-int lica_gpu_column_steps(int32_t ncol, int32_t n, double length, const lica_col_props* props, lica_col_state* st,
-                          int32_t nsteps, int32_t* status) {
+}  // extern "C"
+
+namespace {
+
+int column_steps_host(int32_t ncol, int32_t n, double length, const lica_col_props* props, lica_col_state* st,
+                      int32_t nsteps, int32_t* status, const lica_col_geo* geo) {
     if (ncol < 1 || n < 8 || !props || !st || !status) return LICA_BAD_ARG;
     const size_t nc = (size_t)ncol, sf = (size_t)n + 2, sp = 2 * (size_t)n + 7, sq = 2 * (size_t)n + 2;
     struct F {
@@ -1963,7 +2113,7 @@ int lica_gpu_column_steps(int32_t ncol, int32_t n, double length, const lica_col
     d.scal = (double*)(base + off[13]);
     d.stats = (double*)(base + off[14]);
     int32_t* dst = (int32_t*)(base + st_off);
-    int rc = lica_gpu_column_steps_device(ncol, n, length, props, &d, nsteps, 0, nullptr, dst, nullptr);
+    int rc = column_steps_device(ncol, n, length, props, &d, nsteps, 0, nullptr, dst, nullptr, geo);
     if (rc) return rc;
     LICA_CUDA_TRY(cudaDeviceSynchronize());
     for (int q = 0; q < nfld; ++q)
@@ -1973,6 +2123,21 @@ int lica_gpu_column_steps(int32_t ncol, int32_t n, double length, const lica_col
     for (size_t c = 0; c < nc; ++c)
         if (status[c] != LICA_OK) worst = status[c];
     return worst;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lica_gpu_column_steps(int32_t ncol, int32_t n, double length, const lica_col_props* props, lica_col_state* st,
+                          int32_t nsteps, int32_t* status) {
+    return column_steps_host(ncol, n, length, props, st, nsteps, status, nullptr);
+}
+
+int lica_gpu_column_steps_geometry(const lica_col_geo* geo, int32_t ncol, const lica_col_props* props,
+                                   lica_col_state* st, int32_t nsteps, int32_t* status) {
+    if (!geo) return LICA_BAD_ARG;
+    return column_steps_host(ncol, geo->n, geo->length, props, st, nsteps, status, geo);
 }
 
 // ---- single routines (drop-ins for the reference's subroutines, batches of columns)

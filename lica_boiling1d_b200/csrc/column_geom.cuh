@@ -9,6 +9,15 @@
 namespace lica {
 namespace col {
 
+// Wall-normal geometry of a stretched column (device arrays, shared by the columns of a
+// launch): GEOMETRIC's arrays (1d.f:4808-4882) and GEOM_COUPLING's z tables
+// (1d.f:5037-5370) in the layout of lica_col_geometry (include/lica_gpu.h).  The level-set
+// grid stays uniform.  A null pointer is the uniform column of the closed forms below.
+struct ColGeoDev {
+    const double *z, *zp, *sdz, *vdz, *ssdz, *vvdz;
+    const int *kcou1, *kcou2, *kcoump1, *kcoump2, *kcou_vel, *kcoump_vel;
+};
+
 __device__ __forceinline__ double grid_z(double h, int k) { return (k - 1) * h; }
 __device__ __forceinline__ double grid_zp(double h, int n, int k) {
     if (k <= 0) return 0.0;

@@ -18,7 +18,9 @@ constexpr int PER = WIN / 32;       // window cells per lane
 constexpr int WARPS = 4;            // columns per CTA
 constexpr int HALO = 8;             // room kept between the band and the window edge on entry
 constexpr int EDGE = 4;             // room the band must keep after a regeneration
-constexpr int WTN = 72;             // flow-face window of the time-averaged velocity
+constexpr int WTN = 132;            // flow-face window of the time-averaged velocity: the faces
+                                    // of 128 refined cells and the stencil margin on any flow
+                                    // grid whose cells are at least one refined cell wide
 
 struct Win {
     double phi[WIN];
@@ -41,6 +43,7 @@ struct Win {
 };
 
 struct Ctx {
+    const col::ColGeoDev* cg = nullptr;   // the flow grid's geometry (null: uniform)
     int n, nf, w0, kw0, lane;
     int blo = 0, bhi = -1;   // window slots spanned by the band (per-cell loops run over them)
     int vlo = 0, vhi = -1;   // slots the last VEL_INTP wrote
@@ -49,6 +52,21 @@ struct Ctx {
     __device__ __forceinline__ bool in(int k) const { return k >= w0 && k < w0 + WIN; }
     __device__ __forceinline__ double p(int k) const { return in(k) ? s->phi[k - w0] : 0.0; }
 };
+
+// The first flow face of the window's flow range (WT, the GRID_COUPLING mask, TEMP_GRAD's
+// flow arrays): band cell k reads faces KCOU_VEL(k)-1..+2.  Uniform column: KCOU_VEL = k/2
+// clamped to 1..n, so faces floor(w0/2)-1 .. floor((w0+127)/2)+2 suffice; stretched: from
+// KCOU_VEL of the window's first refined cell.
+__device__ __forceinline__ int flow_origin(const Ctx& c, int w0) {
+    if (!c.cg) return ((w0 >= 0) ? w0 / 2 : -((1 - w0) / 2)) - 2;
+    const int k = w0 < 1 ? 1 : (w0 > c.nf ? c.nf : w0);
+    return c.cg->kcou_vel[k] - 2;
+}
+
+// KCOUMP_VEL(k) of refined cell k: the table, or the uniform column's search
+__device__ __forceinline__ int ctx_kcoump_vel(const Ctx& c, int k) {
+    return c.cg ? c.cg->kcoump_vel[k] : col::kcoump_vel(c.h, c.hf, c.n, k);
+}
 
 __device__ __forceinline__ double warp_max(double v) {
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -180,7 +198,7 @@ __device__ inline int load_band_window(Ctx& c, int lane, int n, double length, c
     w0 = max(w0, -2);
     w0 = min(w0, max(-2, nf + 4 - (WIN - 1)));
     c.w0 = w0;
-    c.kw0 = ((w0 >= 0) ? w0 / 2 : -((1 - w0) / 2)) - 2;
+    c.kw0 = flow_origin(c, w0);
     for (int q = 0; q < PER; ++q) {
         const int i = lane + 32 * q, k = w0 + i;
         const bool ok = (k >= -2 && k <= nf + 4);
@@ -416,8 +434,9 @@ __device__ inline int vel_intp(Ctx& c) {
     Win* s = c.s;
     const int n = c.n;
     const double h = c.h;
-    auto zp = [&](int k) { return (k - 1) * h + 0.5 * h; };
-    auto vdz = [&](int k) { return (k == 1 || k == n + 1) ? 0.5 * h : h; };
+    const col::ColGeoDev* cg = c.cg;
+    auto zp = [&](int k) { return cg ? cg->zp[k] : (k - 1) * h + 0.5 * h; };
+    auto vdz = [&](int k) { return cg ? cg->vdz[k] : ((k == 1 || k == n + 1) ? 0.5 * h : h); };
     int bad = 0;
     auto wtv = [&](int k) {
         const int j = k - c.kw0;
@@ -438,11 +457,15 @@ __device__ inline int vel_intp(Ctx& c) {
             // k/2 - 2 has ZP(q) at least 2.5 flow cells under zz and fails all four tests
             // but the two that do not depend on q, so starting there gives the same KK.
             int kk = 1;
-            for (int qq = max(1, k / 2 - 2); qq <= n; ++qq) {
-                if (fabs(zz - zp(qq)) <= 1e-10) { kk = qq; break; }
-                if (zp(1) > zz) { kk = 1; break; }
-                if (zp(qq) > zz) { kk = qq - 1; break; }
-                if (zp(n) < zz) { kk = n; break; }
+            if (cg) {
+                kk = cg->kcou_vel[k];   // the same search, tabulated by GEOM_COUPLING
+            } else {
+                for (int qq = max(1, k / 2 - 2); qq <= n; ++qq) {
+                    if (fabs(zz - zp(qq)) <= 1e-10) { kk = qq; break; }
+                    if (zp(1) > zz) { kk = 1; break; }
+                    if (zp(qq) > zz) { kk = qq - 1; break; }
+                    if (zp(n) < zz) { kk = n; break; }
+                }
             }
             const double z2 = zp(kk), z1 = z2 - vdz(kk);
             double z3, z4;
@@ -616,8 +639,10 @@ struct Params {
 // outside k = 1..nf) nothing of the column is written.
 __device__ inline int transport_column(Win* s, int lane, int n, double length, double* phi, int* layer, double* psif,
                                 double* wo, const double* w, const double* mf, double* vol_ori, double vol_iphs,
-                                double* psi_cn, double* psi_zn, double* stats, const Params& P) {
+                                double* psi_cn, double* psi_zn, double* stats, const Params& P,
+                                const col::ColGeoDev* cg = nullptr) {
     Ctx c;
+    c.cg = cg;
     c.n = n;
     c.nf = 2 * n;
     c.h = length / n;
@@ -646,9 +671,7 @@ __device__ inline int transport_column(Win* s, int lane, int n, double length, d
     w0 = max(w0, -2);
     w0 = min(w0, max(-2, nf + 4 - (WIN - 1)));
     c.w0 = w0;
-    // flow-face window of WT: band cell k reads faces KCOU_VEL(k)-1..+2 with KCOU_VEL = k/2
-    // clamped to 1..n, so faces floor(w0/2)-1 .. floor((w0+127)/2)+2 suffice
-    c.kw0 = ((w0 >= 0) ? w0 / 2 : -((1 - w0) / 2)) - 2;
+    c.kw0 = flow_origin(c, w0);
 
     // ALPHI_EXT = 0 outside the band, band phi inside (:750-767); ALPHI at entry for the
     // phase test of the source
@@ -793,7 +816,7 @@ __device__ inline int transport_column(Win* s, int lane, int n, double length, d
     for (int i = c.blo + lane; i <= c.bhi; i += 32) {
         const int k = w0 + i, m = s->layer[i];
         if (m >= 1 && m <= NN1 && k >= 1 && k <= nf) {
-            const int j = col::kcoump_vel(c.h, c.hf, n, k) - c.kw0;   // inside the window's face range
+            const int j = ctx_kcoump_vel(c, k) - c.kw0;   // inside the window's face range
             if (j >= 0 && j < WTN) s->fmask[j] = 1;
         }
     }
@@ -802,14 +825,21 @@ __device__ inline int transport_column(Win* s, int lane, int n, double length, d
         const int j = kk - c.kw0;
         const bool mk = (j >= 0 && j < WTN) && s->fmask[j] != 0;
         double zn = psi_zn[kk];
+        const col::ColGeoDev* cg = c.cg;
+        // INTER_PSI over the face box [ZP(K-1), ZP(K)], refined cells KCOUMP2(K-1)..KCOUMP1(K)
         if (kk >= 2 && mk)
-            zn = col::box_mean(psif, nf, 2 * kk - 2, 2 * kk - 1, col::grid_zp(c.h, n, kk - 1), col::grid_zp(c.h, n, kk),
-                               c.hf);
+            zn = col::box_mean(psif, nf, cg ? cg->kcoump2[kk] : 2 * kk - 2, cg ? cg->kcoump1[kk + 1] : 2 * kk - 1,
+                               cg ? cg->zp[kk - 1] : col::grid_zp(c.h, n, kk - 1),
+                               cg ? cg->zp[kk] : col::grid_zp(c.h, n, kk), c.hf);
         if (zn < 1e-3) zn = 0.0;
         else if (zn > 0.999) zn = 1.0;
         psi_zn[kk] = zn;
         double cn = psi_cn[kk];
-        if (mk) cn = col::box_mean(psif, nf, 2 * kk - 1, 2 * kk, col::grid_z(c.h, kk), col::grid_z(c.h, kk + 1), c.hf);
+        // over the cell box [Z(K), Z(K+1)], refined cells KCOU2(K)..KCOU1(K+1)
+        if (mk)
+            cn = col::box_mean(psif, nf, cg ? cg->kcou2[kk + 1] : 2 * kk - 1, cg ? cg->kcou1[kk + 2] : 2 * kk,
+                               cg ? cg->z[kk] : col::grid_z(c.h, kk), cg ? cg->z[kk + 1] : col::grid_z(c.h, kk + 1),
+                               c.hf);
         if (cn < 1e-3) cn = 0.0;
         else if (cn > 0.999) cn = 1.0;
         psi_cn[kk] = cn;

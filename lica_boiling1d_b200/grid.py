@@ -156,3 +156,19 @@ def coupling_z(z, zf):
     native.check(native.lib().lica_grid_coupling_z(n3, _p(z), n3f, _p(zf), *(out[k].ctypes.data_as(I32) for k in (
         "kcou1", "kcou2", "kcoump1", "kcoump2", "kcou_vel", "kcoump_vel"))), "lica_grid_coupling_z")
     return out
+
+
+def column_geometry(faces, length):
+    """The wall-normal geometry of a 1-D column of n = len(faces) - 1 flow cells on the
+    given faces Z(1..n+1) (a stretched grid), against the uniform level-set grid of 2n cells
+    over the same length: GEOMETRIC's arrays z, zp, sdz, vdz, ssdz, vvdz (float64, n+2,
+    Fortran index; z[k] = Z(k)) and GEOM_COUPLING's z tables kcou1, kcou2, kcoump1, kcoump2,
+    kcou_vel, kcoump_vel (int32) -- the layout of lica_col_geometry.  Host code only."""
+    faces = np.asarray(faces, dtype=np.float64)
+    n = len(faces) - 1
+    nf = 2 * n
+    zf = np.arange(nf + 1, dtype=np.float64) * (float(length) / nf)   # ZF(k) = (k - 1) hf
+    geo = metrics(faces)
+    geo["z"] = np.concatenate([[0.0], faces])
+    geo.update(coupling_z(faces, zf))
+    return geo

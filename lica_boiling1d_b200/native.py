@@ -42,6 +42,14 @@ class ColState(C.Structure):
     _fields_ = [(k, C.c_void_p) for k in COL_FIELDS]
 
 
+GEO_FIELDS = ("z", "zp", "sdz", "vdz", "ssdz", "vvdz", "kcou1", "kcou2", "kcoump1", "kcoump2", "kcou_vel",
+              "kcoump_vel")
+
+
+class ColGeometry(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in GEO_FIELDS]
+
+
 class FldInfo(C.Structure):
     _fields_ = [("ihist", C.c_int64), ("m", C.c_int64), ("time", C.c_double), ("dt", C.c_double),
                 ("qvol_ori", C.c_double), ("ips", C.c_int32), ("ipx", C.c_int32), ("ipy", C.c_int32),
@@ -120,6 +128,16 @@ SIGNATURES = {
                                                      C.c_void_p, C.c_void_p, C.c_void_p]),
     "lica_gpu_column_steps": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.POINTER(ColProps), C.POINTER(ColState),
                                         C.c_int32, _I32]),
+    "lica_gpu_column_init_geometry": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.POINTER(ColProps),
+                                                C.POINTER(ColGeometry), C.POINTER(ColState)]),
+    "lica_gpu_column_geometry_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_double,
+                                                  C.POINTER(ColGeometry)]),
+    "lica_gpu_column_geometry_destroy": (C.c_int, [C.c_void_p]),
+    "lica_gpu_column_steps_geometry_device": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(ColProps),
+                                                        C.POINTER(ColState), C.c_int32, C.c_int32, C.c_void_p,
+                                                        C.c_void_p, C.c_void_p]),
+    "lica_gpu_column_steps_geometry": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(ColProps), C.POINTER(ColState),
+                                                 C.c_int32, _I32]),
     "lica_gpu_reinitialization": (C.c_int, [C.c_int32, C.c_int32, C.c_double, _D, _I32, C.c_int32, _I32]),
     "lica_gpu_reinitialization_device": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_void_p, C.c_void_p,
                                                    C.c_int32, C.c_void_p, C.c_void_p]),

@@ -29,6 +29,10 @@ extern "C" int orc_lvs_transport(int n, double L, double* phi, int* layer, doubl
                                  double* psi_zn, double* stats);
 extern "C" int orc_lvs_init(int n, double L, double z0, double* phi, int* layer, double* psif, double* wo,
                             double* vol_tot_ori);
+extern "C" int orc_lvs_transport_geo(int n, double L, double* phi, int* layer, double* psif, double* wo,
+                                     const double* w, const double* mflvs, int iphs, double denr, double dtconst,
+                                     int first, int m_step, double* vol_tot_ori, double vol_tot_iphs, int mglobal,
+                                     double* psi_cn, double* psi_zn, double* stats, const void* geo);
 
 namespace {
 
@@ -97,15 +101,24 @@ struct ColView {
 struct Geo {
     int n, nf;
     double h, hf;
-    explicit Geo(int n_, double L) : n(n_), nf(2 * n_), h(L / n_), hf(L / (2 * n_)) {}
-    double sdz(int k) const { return (k >= 1 && k <= n) ? h : 0.0; }
-    double ssdz(int k) const { return 1.0 / h; }                                   // SSDZ(1..n)
-    double vdz(int k) const { return (k == 1 || k == n + 1) ? 0.5 * h : h; }
-    double vvdz(int k) const { return 1.0 / vdz(k); }
-    double z(int k) const { return grid_z(h, k); }
-    double zp(int k) const { return grid_zp(h, n, k); }
+    const ColGeo* cg = nullptr;   // null: the uniform column
+    explicit Geo(int n_, double L, const ColGeo* cg_ = nullptr)
+        : n(n_), nf(2 * n_), h(L / n_), hf(L / (2 * n_)), cg(cg_) {}
+    double sdz(int k) const { return cg ? cg->sdz[k] : ((k >= 1 && k <= n) ? h : 0.0); }
+    double ssdz(int k) const { return cg ? cg->ssdz[k] : 1.0 / h; }                 // SSDZ(1..n)
+    double vdz(int k) const { return cg ? cg->vdz[k] : ((k == 1 || k == n + 1) ? 0.5 * h : h); }
+    double vvdz(int k) const { return cg ? cg->vvdz[k] : 1.0 / vdz(k); }
+    double z(int k) const { return cg ? cg->z[k] : grid_z(h, k); }
+    double zp(int k) const { return cg ? cg->zp[k] : grid_zp(h, n, k); }
     double zf(int k) const { return grid_zf(hf, k); }
     double zpf(int k) const { return grid_zf(hf, k) + 0.5 * hf; }
+    // GEOM_COUPLING's refined faces (uniform column: face K is refined face 2K-1, centre K
+    // refined face 2K)
+    int kcou1(int k) const { return cg ? cg->kcou1[k + 1] : 2 * k - 2; }
+    int kcou2(int k) const { return cg ? cg->kcou2[k + 1] : 2 * k - 1; }
+    int kcoump1(int k) const { return cg ? cg->kcoump1[k + 1] : 2 * k - 1; }
+    int kcoump2(int k) const { return cg ? cg->kcoump2[k + 1] : 2 * k; }
+    int kcoump_vel(int k) const { return cg ? cg->kcoump_vel[k] : ::kcoump_vel(h, hf, n, k); }
     // LHSINIT, 1d.f:1927-1990
     double akw(int k) const { return -vvdz(k) * ssdz(k - 1); }
     double ckw(int k) const { return -vvdz(k) * ssdz(k); }
@@ -195,13 +208,13 @@ void cal_continuity(const Geo& g, const Phys& ph, const ColView& s, double dtcon
         if (uu >= 0.0) {
             z1 = g.zp(k) - uu * dtconst;
             z2 = g.zp(k);
-            k1 = 2 * (k - 1);   // KCOUMP2(K-1)
-            k2 = 2 * k - 1;     // KCOUMP1(K)
+            k1 = g.kcoump2(k - 1);
+            k2 = g.kcoump1(k);
         } else {
             z1 = g.zp(k);
             z2 = g.zp(k) - uu * dtconst;
-            k1 = 2 * k;         // KCOUMP2(K)
-            k2 = 2 * k + 1;     // KCOUMP1(K+1)
+            k1 = g.kcoump2(k);
+            k2 = g.kcoump1(k + 1);
         }
         return box_mean(s.psif, nf, k1, k2, z1, z2, g.hf);
     };
@@ -252,13 +265,13 @@ void cal_continuity(const Geo& g, const Phys& ph, const ColView& s, double dtcon
         if (uu >= 0.0) {
             z1 = g.z(k + 1) - uu * dtconst;
             z2 = g.z(k + 1);
-            k1 = 2 * k - 1;     // KCOU2(K)
-            k2 = 2 * k;         // KCOU1(K+1)
+            k1 = g.kcou2(k);
+            k2 = g.kcou1(k + 1);
         } else {
             z1 = g.z(k + 1);
             z2 = g.z(k + 1) - uu * dtconst;
-            k1 = 2 * k + 1;     // KCOU2(K+1)
-            k2 = 2 * k + 2;     // KCOU1(K+2)
+            k1 = g.kcou2(k + 1);
+            k2 = g.kcou1(k + 2);
         }
         return box_mean(s.psif, nf, k1, k2, z1, z2, g.hf);
     };
@@ -347,6 +360,7 @@ void lhsps(const Geo& g, const Phys& ph, const ColView& s, double alpha, Work& w
 // zero everywhere, band values on the band, no ghost boundary condition.
 void load_band(const Geo& g, double L, const ColView& s, Col& c) {
     c.init(g.n, L);
+    c.cg = g.cg;
     for (int k = -2; k <= g.nf + 4; ++k) {
         const int m = s.layer[k + GL];
         c.phi[k + GL] = (m >= 1 && m <= N_MAX) ? s.phi[k + GL] : 0.0;
@@ -362,8 +376,8 @@ void load_band(const Geo& g, double L, const ColView& s, Col& c) {
 // replicas); zero if any stencil value is zero; IC keeps its previous value when the
 // result is exactly zero.
 double phinsintp(const Geo& g, const Col& c, int kk, int& ic) {
-    const int k1 = 2 * kk - 1, k2 = 2 * kk;
-    const double zd = (g.zp(kk) - g.zpf(k1)) / (g.zpf(k2) - g.zpf(k1));
+    const int k1 = g.kcou2(kk), k2 = g.kcoump2(kk);   // PHINSINTP's K1 = KCOU2(KO), K2 = KCOUMP2(KO)
+    const double zd = (k1 == k2) ? 0.0 : (g.zp(kk) - g.zpf(k1)) / (g.zpf(k2) - g.zpf(k1));
     const double a1 = const_cast<Col&>(c).p(k1), a2 = const_cast<Col&>(c).p(k2);
     const double c00 = a1 * (1.0 - 0.5) + a1 * 0.5;
     const double c01 = a2 * (1.0 - 0.5) + a2 * 0.5;
@@ -533,7 +547,7 @@ int temp_grad(const Geo& g, double L, const Phys& ph, const ColView& s, double d
     int ic = 0;
     for (int m = 1; m <= NN2; ++m)
         for (int k : c.band[m]) {
-            const int kk = kcoump_vel(g.h, g.hf, n, k);
+            const int kk = g.kcoump_vel(k);
             if (nphi[kk] == 0.0) {
                 const double nsphi = phinsintp(g, c, kk, ic);
                 nphi[kk] = 1e-7;
@@ -543,7 +557,7 @@ int temp_grad(const Geo& g, double L, const Phys& ph, const ColView& s, double d
             }
         }
     for (int k : c.band[N_MAX]) {
-        const int kk = kcoump_vel(g.h, g.hf, n, k);
+        const int kk = g.kcoump_vel(k);
         const double dx = 0.25, dy = 0.25;            // XPF - XP of either replica, squared below
         const double dz = g.zpf(k) - g.zp(kk);
         const double pre = c.p(k) + std::sqrt(dx * dx + dy * dy + dz * dz);
@@ -559,7 +573,7 @@ int temp_grad(const Geo& g, double L, const Phys& ph, const ColView& s, double d
     std::vector<double> tf0(nf + 7, 0.0), tf1(nf + 7, 0.0);
     for (int m = 1; m <= NN1; ++m)
         for (int k : c.band[m]) {
-            const int kk = kcoump_vel(g.h, g.hf, n, k);
+            const int kk = g.kcoump_vel(k);
             int kk1, kk2;
             double zd;
             if (g.zp(kk) > g.zpf(k)) {
@@ -638,7 +652,7 @@ int temp_grad(const Geo& g, double L, const Phys& ph, const ColView& s, double d
     // (7) CAL_PSI_TMP(1) and the phase-change mask (chphase.f:297-357, z faces only)
     std::vector<double> psi_tmp(n + 2, 1.0);
     for (int k = 1; k <= n; ++k) {
-        const double v = box_mean(psif_mtp.data(), nf, 2 * k - 1, 2 * k, g.z(k), g.z(k + 1), g.hf);
+        const double v = box_mean(psif_mtp.data(), nf, g.kcou2(k), g.kcou1(k + 1), g.z(k), g.z(k + 1), g.hf);
         if (v <= 1e-3) psi_tmp[k] = 0.0;
         else if (v >= 0.999) psi_tmp[k] = 1.0;
         else psi_tmp[k] = v;
@@ -655,7 +669,7 @@ void cal_continuity2(const Geo& g, const Phys& ph, const ColView& s, Work& wk) {
     if (ph.denm != ph.denp || ph.vism != ph.visp) make_region(g, s, wk);
     for (int k = 2; k <= n; ++k)
         if (wk.reg(k) == 2) {
-            const double ssum = box_mean(s.sfgas2, nf, 2 * k - 1, 2 * k, g.zp(k - 1), g.zp(k), g.hf);
+            const double ssum = box_mean(s.sfgas2, nf, g.kcou2(k), g.kcou1(k + 1), g.zp(k - 1), g.zp(k), g.hf);
             wk.psi_z[k] = wk.psi_z[k] - ssum;
         }
     for (int k = 2; k <= n; ++k) {
@@ -664,7 +678,7 @@ void cal_continuity2(const Geo& g, const Phys& ph, const ColView& s, Work& wk) {
     }
     for (int k = 1; k <= n; ++k)
         if (wk.reg(k) == 2) {
-            const double ssum = box_mean(s.sfgas2, nf, 2 * k - 1, 2 * k, g.z(k), g.z(k + 1), g.hf);
+            const double ssum = box_mean(s.sfgas2, nf, g.kcou2(k), g.kcou1(k + 1), g.z(k), g.z(k + 1), g.hf);
             wk.psi_c[k] = wk.psi_c[k] - ssum;
         }
     for (int k = 1; k <= n; ++k) {
@@ -763,7 +777,7 @@ void divgs(const Geo& g, const Phys& ph, const ColView& s, double dtconsti, Work
     wk.divgsum[n] = 0.0;
     if (ph.iphs == 1)
         for (int k = 1; k <= n; ++k) {
-            const double ssum = box_mean(s.sfgas, g.nf, 2 * k - 1, 2 * k, g.z(k), g.z(k + 1), g.hf);
+            const double ssum = box_mean(s.sfgas, g.nf, g.kcou2(k), g.kcou1(k + 1), g.z(k), g.z(k + 1), g.hf);
             wk.divgsum[k] = wk.divgsum[k] - ssum * (ph.den_diff / (ph.denp * ph.denm));
         }
     for (int k = 2; k <= n; ++k) wk.divgsum[k] = wk.divgsum[k] * dtconsti;
@@ -844,7 +858,7 @@ double convrge1(const Geo& g, const Phys& ph, const ColView& s) {
     for (int k = 1; k <= g.n; ++k) {
         double d = (s.w[k + 1] - s.w[k]) * g.ssdz(k);
         if (ph.iphs == 1) {
-            const double ssum = box_mean(s.sfgas, g.nf, 2 * k - 1, 2 * k, g.z(k), g.z(k + 1), g.hf);
+            const double ssum = box_mean(s.sfgas, g.nf, g.kcou2(k), g.kcou1(k + 1), g.z(k), g.z(k + 1), g.hf);
             d = d - ssum * (ph.den_diff / ph.denp);
         }
         dvmax = std::max(std::fabs(d), dvmax);
@@ -876,11 +890,11 @@ static ColProps props_of(const double* props, const int* iprops) {
 
 // MAKEFLD (1d.f:821-946, IPHS = 1 branch) + LVSINIT (two_phase.f:116-388) +
 // GRID_COUPLING(1) for a planar film of thickness z0 at the wall.
-int orc_col_init(int n, double L, double z0, const double* props, const int* iprops, double* w, double* p,
-                 double* t, double* psi_cn, double* psi_zn, double* phi, int* layer, double* psif, double* wo,
-                 double* mflvs, double* sfgas, double* sfgas2, int* imask, double* scal) {
+static int col_init(int n, double L, double z0, const double* props, const int* iprops, double* w, double* p,
+                    double* t, double* psi_cn, double* psi_zn, double* phi, int* layer, double* psif, double* wo,
+                    double* mflvs, double* sfgas, double* sfgas2, int* imask, double* scal, const ColGeo* cg) {
     const ColProps cp = props_of(props, iprops);
-    Geo g(n, L);
+    Geo g(n, L, cg);
     const int nf = g.nf;
     for (int k = 0; k <= n + 1; ++k) {
         w[k] = 0.0;
@@ -906,7 +920,7 @@ int orc_col_init(int n, double L, double z0, const double* props, const int* ipr
     double vol = 0.0;
     const int rc = orc_lvs_init(n, L, z0, phi, layer, psif, wo, &vol);
     if (rc) return rc;
-    grid_coupling(n, L, psif, layer, 1, psi_cn, psi_zn);
+    grid_coupling(n, L, psif, layer, 1, psi_cn, psi_zn, cg);
     for (int k = 0; k < nf + 7; ++k) mflvs[k] = 0.0;
     for (int k = 0; k <= nf + 1; ++k) {
         sfgas[k] = 0.0;
@@ -918,6 +932,22 @@ int orc_col_init(int n, double L, double z0, const double* props, const int* ipr
     scal[3] = vol;
     scal[4] = vol;
     return 0;
+}
+
+int orc_col_init(int n, double L, double z0, const double* props, const int* iprops, double* w, double* p,
+                 double* t, double* psi_cn, double* psi_zn, double* phi, int* layer, double* psif, double* wo,
+                 double* mflvs, double* sfgas, double* sfgas2, int* imask, double* scal) {
+    return col_init(n, L, z0, props, iprops, w, p, t, psi_cn, psi_zn, phi, layer, psif, wo, mflvs, sfgas, sfgas2,
+                    imask, scal, nullptr);
+}
+
+// The same on a stretched flow grid; geo holds the pointers of a ColGeo (lvs1d_core.hpp),
+// in its member order.
+int orc_col_init_geo(int n, double L, double z0, const double* props, const int* iprops, double* w, double* p,
+                     double* t, double* psi_cn, double* psi_zn, double* phi, int* layer, double* psif, double* wo,
+                     double* mflvs, double* sfgas, double* sfgas2, int* imask, double* scal, const void* geo) {
+    return col_init(n, L, z0, props, iprops, w, p, t, psi_cn, psi_zn, phi, layer, psif, wo, mflvs, sfgas, sfgas2,
+                    imask, scal, static_cast<const ColGeo*>(geo));
 }
 
 // The start-up after a restart read, for one column: LVSINIT's read branch
@@ -955,12 +985,12 @@ int orc_col_resume(int n, double L, double* phi, const int* layer, double* psif,
 //             level-set subcycles (sum), reinitialisation/mass triggers (IMASS sum),
 //             interface height, vapour volume VOL_TOT_IPHS, DT.
 // Returns 0, 1 (TEMP_EXTP did not converge) or 2 (band overflow).
-int orc_col_step(int n, double L, const double* props, const int* iprops, double* w, double* p, double* t,
-                 double* psi_cn, double* psi_zn, double* phi, int* layer, double* psif, double* wo, double* mflvs,
-                 double* sfgas, double* sfgas2, int* imask, double* scal, double* stats) {
+static int col_step(int n, double L, const double* props, const int* iprops, double* w, double* p, double* t,
+                    double* psi_cn, double* psi_zn, double* phi, int* layer, double* psif, double* wo, double* mflvs,
+                    double* sfgas, double* sfgas2, int* imask, double* scal, double* stats, const ColGeo* cg) {
     const ColProps cp = props_of(props, iprops);
     const Phys ph(cp);
-    Geo g(n, L);
+    Geo g(n, L, cg);
     ColView s = view(n, L, w, p, t, psi_cn, psi_zn, phi, layer, psif, wo, mflvs, sfgas, sfgas2, imask, scal);
     Work wk(n);
     g_place = 0.0;
@@ -982,9 +1012,9 @@ int orc_col_step(int n, double L, const double* props, const int* iprops, double
         iters += it;
         dvmax = convrge1(g, ph, s);
         double lst[4];
-        const int rc = orc_lvs_transport(n, L, phi, layer, psif, wo, w, mflvs, ph.iphs, ph.denr, dtconst,
-                                         (m_step == 1 && msub == 1) ? 1 : 0, m_step, &scal[3], scal[4], ph.mglobal,
-                                         psi_cn, psi_zn, lst);
+        const int rc = orc_lvs_transport_geo(n, L, phi, layer, psif, wo, w, mflvs, ph.iphs, ph.denr, dtconst,
+                                             (m_step == 1 && msub == 1) ? 1 : 0, m_step, &scal[3], scal[4],
+                                             ph.mglobal, psi_cn, psi_zn, lst, cg);
         if (rc) return rc;
         subcycles += lst[0];
         imass += (lst[0] > 0) ? lst[3] : 0.0;
@@ -1006,6 +1036,21 @@ int orc_col_step(int n, double L, const double* props, const int* iprops, double
     stats[6] = scal[4];
     stats[7] = scal[0];
     return 0;
+}
+
+int orc_col_step(int n, double L, const double* props, const int* iprops, double* w, double* p, double* t,
+                 double* psi_cn, double* psi_zn, double* phi, int* layer, double* psif, double* wo, double* mflvs,
+                 double* sfgas, double* sfgas2, int* imask, double* scal, double* stats) {
+    return col_step(n, L, props, iprops, w, p, t, psi_cn, psi_zn, phi, layer, psif, wo, mflvs, sfgas, sfgas2, imask,
+                    scal, stats, nullptr);
+}
+
+// One time step on a stretched flow grid (geo: a ColGeo, lvs1d_core.hpp).
+int orc_col_step_geo(int n, double L, const double* props, const int* iprops, double* w, double* p, double* t,
+                     double* psi_cn, double* psi_zn, double* phi, int* layer, double* psif, double* wo, double* mflvs,
+                     double* sfgas, double* sfgas2, int* imask, double* scal, double* stats, const void* geo) {
+    return col_step(n, L, props, iprops, w, p, t, psi_cn, psi_zn, phi, layer, psif, wo, mflvs, sfgas, sfgas2, imask,
+                    scal, stats, static_cast<const ColGeo*>(geo));
 }
 
 // TEMP_GRAD (chphase.f:55-368, with TEMP_EXTP, TF_GRAD and VOL_TOT_MFDOT) of one column as a

@@ -105,12 +105,13 @@ int orc_lvs_init(int n, double L, double z0, double* phi, int* layer, double* ps
 //   m_step  : time step number M (the MOD(M,50) mass trigger, :903)
 //   psi_cn  : out, PSI_CN(k) k = 0..n+1;  psi_zn: out, PSI_ZN(k) k = 0..n+1
 //   stats   : out [0] subcycles, [1] DALPHIMAX, [2] DALPHIMIN, [3] IMASS
-int orc_lvs_transport(int n, double L, double* phi, int* layer, double* psif, double* wo, const double* w,
-                      const double* mflvs, int iphs, double denr, double dtconst, int first, int m_step,
-                      double* vol_tot_ori, double vol_tot_iphs, int mglobal, double* psi_cn, double* psi_zn,
-                      double* stats) {
+static int transport(int n, double L, double* phi, int* layer, double* psif, double* wo, const double* w,
+                     const double* mflvs, int iphs, double denr, double dtconst, int first, int m_step,
+                     double* vol_tot_ori, double vol_tot_iphs, int mglobal, double* psi_cn, double* psi_zn,
+                     double* stats, const ColGeo* cg) {
     State s;
     load(s, n, L, phi, layer, psif, wo);
+    s.c.cg = cg;
     Col& c = s.c;
     const int nf = c.nf;
     // ALPHI_EXT = 0, band values copied in (:750-767)
@@ -196,7 +197,7 @@ int orc_lvs_transport(int n, double L, double* phi, int* layer, double* psif, do
     if (imass == 0 && iphs == 1) vo = vol_tot_iphs;
     *vol_tot_ori = vo;
     // GRID_COUPLING(0)
-    grid_coupling(n, L, s.psif.data(), c.layer.data(), 0, psi_cn, psi_zn);
+    grid_coupling(n, L, s.psif.data(), c.layer.data(), 0, psi_cn, psi_zn, cg);
     stats[0] = isub;
     stats[1] = dmax;
     stats[2] = dmin;
@@ -208,6 +209,23 @@ done_noupdate:
     stats[0] = 0;
     store(s, phi, layer, psif, wo);
     return 0;
+}
+
+int orc_lvs_transport(int n, double L, double* phi, int* layer, double* psif, double* wo, const double* w,
+                      const double* mflvs, int iphs, double denr, double dtconst, int first, int m_step,
+                      double* vol_tot_ori, double vol_tot_iphs, int mglobal, double* psi_cn, double* psi_zn,
+                      double* stats) {
+    return transport(n, L, phi, layer, psif, wo, w, mflvs, iphs, denr, dtconst, first, m_step, vol_tot_ori,
+                     vol_tot_iphs, mglobal, psi_cn, psi_zn, stats, nullptr);
+}
+
+// The same on a stretched flow grid (geo: a ColGeo, lvs1d_core.hpp).
+int orc_lvs_transport_geo(int n, double L, double* phi, int* layer, double* psif, double* wo, const double* w,
+                          const double* mflvs, int iphs, double denr, double dtconst, int first, int m_step,
+                          double* vol_tot_ori, double vol_tot_iphs, int mglobal, double* psi_cn, double* psi_zn,
+                          double* stats, const void* geo) {
+    return transport(n, L, phi, layer, psif, wo, w, mflvs, iphs, denr, dtconst, first, m_step, vol_tot_ori,
+                     vol_tot_iphs, mglobal, psi_cn, psi_zn, stats, static_cast<const ColGeo*>(geo));
 }
 
 // Unit entry points on one column (tests): ALPHI_BC, BAND_GENERATION and

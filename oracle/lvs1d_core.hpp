@@ -11,6 +11,18 @@
 
 namespace {
 
+// Wall-normal geometry of a stretched column: GEOMETRIC's arrays (1d.f:4808-4882) and
+// GEOM_COUPLING's z tables (1d.f:5037-5370) as lica_grid_metrics and lica_grid_coupling_z
+// write them (the level-set grid stays uniform).  Flow arrays are n+2 long, indexed by the
+// Fortran index: z (faces 1..n+1), zp (0..n+1), sdz, ssdz (1..n), vdz, vvdz (1..n+1).
+// kcou1/kcou2: faces K = -1..n+2 at [K+1]; kcoump1/kcoump2: centres K = -1..n+1 at [K+1];
+// kcou_vel, kcoump_vel: refined faces / centres K = 1..nf at [K].  A null geometry is the
+// uniform column.
+struct ColGeo {
+    const double *z, *zp, *sdz, *vdz, *ssdz, *vvdz;
+    const int *kcou1, *kcou2, *kcoump1, *kcoump2, *kcou_vel, *kcoump_vel;
+};
+
 constexpr int N_MAX = 11;          // M_MAX, 1dmodulesX.f:21
 constexpr int NN1 = N_MAX - 3;     // two_phase.f:737
 constexpr int NN2 = N_MAX - 1;     // two_phase.f:738
@@ -19,6 +31,7 @@ constexpr int GL = 2;              // offset of k = -2 (three ghost cells below 
 struct Col {
     int n = 0, nf = 0;       // flow cells, refined cells
     double L = 1.0, h = 0, hf = 0, ssdzf = 0;
+    const ColGeo* cg = nullptr;  // the flow grid's geometry (null: uniform)
     std::vector<double> phi;     // ALPHI_EXT(k), k = -2..nf+4 at [k + GL] (nf+7 values)
     std::vector<int> layer;      // band layer of refined cell k (0 = outside), same indexing
     std::vector<std::vector<int>> band;  // band[n] = z-levels of layer n (1-based k), reference order
@@ -248,8 +261,9 @@ void rein_trigger(Col& c, double& dmax, double& dmin) {
 // Lagrange weights at ZZ = ZF(k) on nodes ZP(KK-1..KK+2), KK = KCOU_VEL(k).
 void vel_intp(Col& c, const std::vector<double>& wt, std::vector<double>& wf) {
     const int n = c.n;
-    auto zp = [&](int k) { return (k - 1) * c.h + 0.5 * c.h; };
-    auto vdz = [&](int k) { return (k == 1 || k == n + 1) ? 0.5 * c.h : c.h; };
+    const ColGeo* cg = c.cg;
+    auto zp = [&](int k) { return cg ? cg->zp[k] : (k - 1) * c.h + 0.5 * c.h; };
+    auto vdz = [&](int k) { return cg ? cg->vdz[k] : ((k == 1 || k == n + 1) ? 0.5 * c.h : c.h); };
     auto wtv = [&](int k) { return (k < 0 || k > n + 1) ? 0.0 : wt[k]; };
     std::fill(wf.begin(), wf.end(), 0.0);
     for (int m = 1; m <= NN2; ++m)
@@ -432,23 +446,31 @@ inline double box_mean(const double* f, int nf, int k1, int k2, double z1, doubl
 // refined cells 2K-2..2K-1; PSI_CN(K): over [Z(K),Z(K+1)], cells 2K-1..2K; snaps at
 // 1e-3 / 0.999; PSI_CN(0) = PSI_CN(1), PSI_CN(n+1) = PSI_CN(n).
 inline void grid_coupling(int n, double L, const double* psif, const int* layer /* [k+GL] or null */, int ini,
-                          double* psi_cn, double* psi_zn) {
+                          double* psi_cn, double* psi_zn, const ColGeo* cg = nullptr) {
     const int nf = 2 * n;
     const double h = L / n, hf = L / nf;
+    auto zp = [&](int k) { return cg ? cg->zp[k] : grid_zp(h, n, k); };
+    auto zf = [&](int k) { return cg ? cg->z[k] : grid_z(h, k); };
     std::vector<int> mask(n + 2, ini ? 1 : 0);
     if (!ini)
         for (int k = 1; k <= nf; ++k) {
             const int m = layer[k + GL];
-            if (m >= 1 && m <= NN1) mask[kcoump_vel(h, hf, n, k)] = 1;
+            if (m >= 1 && m <= NN1) mask[cg ? cg->kcoump_vel[k] : kcoump_vel(h, hf, n, k)] = 1;
         }
+    // INTER_PSI over the face box [ZP(K-1), ZP(K)], refined cells KCOUMP2(K-1)..KCOUMP1(K)
     for (int k = 2; k <= n; ++k)
-        if (mask[k]) psi_zn[k] = box_mean(psif, nf, 2 * k - 2, 2 * k - 1, grid_zp(h, n, k - 1), grid_zp(h, n, k), hf);
+        if (mask[k])
+            psi_zn[k] = box_mean(psif, nf, cg ? cg->kcoump2[k] : 2 * k - 2, cg ? cg->kcoump1[k + 1] : 2 * k - 1,
+                                 zp(k - 1), zp(k), hf);
     for (int k = 1; k <= n; ++k) {
         if (psi_zn[k] < 1e-3) psi_zn[k] = 0.0;
         else if (psi_zn[k] > 0.999) psi_zn[k] = 1.0;
     }
+    // over the cell box [Z(K), Z(K+1)], refined cells KCOU2(K)..KCOU1(K+1)
     for (int k = 1; k <= n; ++k)
-        if (mask[k]) psi_cn[k] = box_mean(psif, nf, 2 * k - 1, 2 * k, grid_z(h, k), grid_z(h, k + 1), hf);
+        if (mask[k])
+            psi_cn[k] = box_mean(psif, nf, cg ? cg->kcou2[k + 1] : 2 * k - 1, cg ? cg->kcou1[k + 2] : 2 * k, zf(k),
+                                 zf(k + 1), hf);
     for (int k = 1; k <= n; ++k) {
         if (psi_cn[k] < 1e-3) psi_cn[k] = 0.0;
         else if (psi_cn[k] > 0.999) psi_cn[k] = 1.0;

@@ -40,6 +40,8 @@ def lib(native: bool = False):
             [_INT, _D]
         L.orc_col_resume.argtypes = [C.c_int, C.c_double, _D, _INT, _D, _D, _D]
         L.orc_col_step.argtypes = [C.c_int, C.c_double, _D, _INT] + [_D] * 6 + [_INT] + [_D] * 5 + [_INT, _D, _D]
+        L.orc_col_init_geo.argtypes = L.orc_col_init.argtypes + [C.c_void_p]
+        L.orc_col_step_geo.argtypes = L.orc_col_step.argtypes + [C.c_void_p]
         L.orc_col_last_place.restype = C.c_double
         L.orc_col_last_place.argtypes = []
         L.orc_reinitialization.argtypes = [C.c_int, C.c_double, _D, _INT, C.c_int]
@@ -289,3 +291,38 @@ def col_pressure_correction(n, length, props, dtconst, w, p, denf_zi, sfgas):
     lib().orc_col_pressure_correction(n, length, _p(pr), _pi(ip), float(dtconst), _p(w), _p(p),
                                       _p(np.ascontiguousarray(denf_zi)), _p(np.ascontiguousarray(sfgas)))
     return w, p
+
+
+# ---------------------------------------------------------------------------------------
+# Stretched columns: the geometry (GEOMETRIC arrays, GEOM_COUPLING z tables) of ColGeo
+# ---------------------------------------------------------------------------------------
+class _ColGeo(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in ("z", "zp", "sdz", "vdz", "ssdz", "vvdz", "kcou1", "kcou2", "kcoump1",
+                                           "kcoump2", "kcou_vel", "kcoump_vel")]
+
+
+def col_geo(geo):
+    """A ColGeo over the arrays of geo (a dict of z, zp, sdz, vdz, ssdz, vvdz (float64, n+2)
+    and kcou1, kcou2, kcoump1, kcoump2, kcou_vel, kcoump_vel (int32)); keeps them alive."""
+    arrs = {k: np.ascontiguousarray(geo[k], dtype=np.int32 if k.startswith("kcou") else np.float64)
+            for k in _ColGeo._fields_ and [f[0] for f in _ColGeo._fields_]}
+    g = _ColGeo(*[arrs[f[0]].ctypes.data for f in _ColGeo._fields_])
+    g._keep = arrs
+    return g
+
+
+def col_init_geo(n, length, z0, props, geo):
+    st = col_empty(n)
+    pr, ip = _col_props(props)
+    g = col_geo(geo)
+    rc = lib().orc_col_init_geo(n, length, z0, _p(pr), _pi(ip), *_col_args(st), C.byref(g))
+    if rc:
+        raise ValueError(f"orc_col_init_geo returned {rc}")
+    return st
+
+
+def col_step_geo(st, n, length, props, geo, native=False):
+    """One time step of a stretched column in place (geo as col_geo takes it)."""
+    pr, ip = _col_props(props)
+    g = col_geo(geo)
+    return lib(native).orc_col_step_geo(n, length, _p(pr), _pi(ip), *_col_args(st), _p(st["stats"]), C.byref(g))

@@ -59,3 +59,58 @@ def test_oracle_column_trajectory_is_pinned():
         got = M.trajectory(z0, kw)
         for k, v in got.items():
             assert np.array_equal(v, gold[f"{name}_{k}"]), (name, k)
+
+
+@pytest.mark.parametrize("n,gam,z0", [(64, 1.0, 0.1), (128, 2.0, 0.25), (96, 1.5, 0.3), (128, 0.0, 0.3)])
+def test_stretched_init_matches_oracle(n, gam, z0):
+    """lica_gpu_column_init_geometry (host code) on a wall-clustered flow grid (gam = 0:
+    uniform faces through the tables) against the oracle, bit for bit; uniform faces of a
+    power-of-two column (whose face and centre coordinates are exact) give the closed-form
+    column's state exactly."""
+    from lica_boiling1d_b200.column import ColumnGeometry, ColumnProps, Columns
+    props = ColumnProps(denr=1000.0, visr=20.0, tcr=25.0, jakob=0.009)
+    g = ColumnGeometry.tanh(n, 1.0, gam) if gam > 0 else ColumnGeometry(np.arange(n + 1) / n)
+    cols = Columns.film(n, 1.0, [z0], props, geometry=g)
+    ref = O.col_init_geo(n, 1.0, z0, props, g.arrays)
+    for k, v in ref.items():
+        if k != "stats":
+            assert np.array_equal(cols.arrays[k][0], v), k
+    if gam == 0:
+        u = O.col_init(n, 1.0, z0, props)
+        for k in u:
+            assert np.array_equal(u[k], ref[k]), k
+
+
+def test_oracle_table_path_equals_closed_forms():
+    """The oracle's stretched step on uniform faces reproduces its uniform step bit for bit
+    over 12 steps (the table path of every routine against the pinned closed forms)."""
+    from lica_boiling1d_b200.column import ColumnGeometry, ColumnProps
+    n, z0 = 64, 0.1
+    props = ColumnProps(denr=1000.0, visr=20.0, tcr=25.0, jakob=0.009, cflmax=0.3)
+    g = ColumnGeometry(np.arange(n + 1) / n)
+    a, b = O.col_init(n, 1.0, z0, props), O.col_init_geo(n, 1.0, z0, props, g.arrays)
+    for _ in range(12):
+        assert O.col_step(a, n, 1.0, props) == 0
+        assert O.col_step_geo(b, n, 1.0, props, g.arrays) == 0
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_stretched_geometry_checks():
+    """A cell narrower than a refined cell, or faces that do not end at the length, are
+    refused (LICA_BAD_ARG), never run."""
+    from lica_boiling1d_b200 import native
+    from lica_boiling1d_b200.column import ColumnGeometry, ColumnProps, Columns
+    n = 32
+    faces = np.arange(n + 1) / n
+    faces[1] = 0.25 / (2 * n)            # first cell a quarter of a refined cell
+    with pytest.raises(native.LicaError):
+        Columns.film(n, 1.0, [0.3], ColumnProps(), geometry=ColumnGeometry(faces))
+    import ctypes as C
+    g = ColumnGeometry(np.arange(n + 1) / n)
+    st = Columns.empty(1, n, 2.0)
+    cs = native.ColState(*[st.arrays[k][0].ctypes.data for k in native.COL_FIELDS])
+    gc, cp = g.c(), ColumnProps().c()
+    assert native.lib().lica_gpu_column_init_geometry(n, 2.0, 0.3, C.byref(cp), C.byref(gc), C.byref(cs)) == 4   # LICA_BAD_ARG
+    with pytest.raises(ValueError):
+        Columns.film(n, 2.0, [0.3], ColumnProps(), geometry=g)

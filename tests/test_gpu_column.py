@@ -125,3 +125,51 @@ def test_long_columns_with_tridiagonal_arrays_in_scratch():
         got = dev.column(c)
         for k, v in r.items():
             assert np.array_equal(got[k], v), (c, k)
+
+
+@pytest.mark.parametrize("n,gam,z0s,steps", [(64, 1.0, [0.1], 40), (128, 2.0, [0.06, 0.25], 12)])
+def test_stretched_column(n, gam, z0s, steps):
+    """A flow grid clustered at both walls (HYPTAN, XSI = 0.5): the step reads GEOMETRIC's
+    arrays and GEOM_COUPLING's z tables; every launch bit for bit against the oracle on the
+    same geometry (40 steps in launches of 1, 3 and 36)."""
+    import torch
+    from lica_boiling1d_b200.column import ColumnGeometry, Columns
+    props = props_for(denr=1000.0, visr=20.0, tcr=25.0, jakob=0.009, cflmax=0.3)
+    g = ColumnGeometry.tanh(n, 1.0, gam)
+    assert np.diff(g.faces).max() / np.diff(g.faces).min() > 1.5
+    dev = Columns.film(n, 1.0, z0s, props, geometry=g).to("cuda")
+    refs = [O.col_init_geo(n, 1.0, z0, props, g.arrays) for z0 in z0s]
+    done = 0
+    for k in (1, 3, steps - 4):
+        status = dev.steps(k, props)
+        torch.cuda.synchronize()
+        assert int(status.abs().max()) == 0, status
+        for r in refs:
+            for _ in range(k):
+                assert O.col_step_geo(r, n, 1.0, props, g.arrays) == 0
+        done += k
+        compare(dev, refs, f"stretched, after step {done}")
+    assert refs[0]["stats"][3] > 0   # the level set moved
+
+
+def test_uniform_geometry_tables_match_closed_forms():
+    """A 'stretched' column whose faces are uniform takes the table path of every routine
+    and must step exactly as the closed-form uniform column does (a power-of-two column,
+    whose coordinates are exact either way); the host-array entry
+    (lica_gpu_column_steps_geometry) matches the device one."""
+    import torch
+    from lica_boiling1d_b200.column import ColumnGeometry, Columns
+    n = 128
+    props = props_for(denr=1000.0, visr=20.0, tcr=25.0, jakob=0.009, cflmax=0.3)
+    g = ColumnGeometry(np.arange(n + 1) / n)
+    a = Columns.film(n, 1.0, [0.1, 0.3], props).to("cuda")
+    b = Columns.film(n, 1.0, [0.1, 0.3], props, geometry=g)
+    bd = b.to("cuda")
+    sa, sb = a.steps(6, props), bd.steps(6, props)
+    sh = b.steps(6, props)
+    torch.cuda.synchronize()
+    assert int(sa.abs().max()) == 0 and int(sb.abs().max()) == 0 and int(np.abs(sh).max()) == 0
+    ha, hb = a.to(None), bd.to(None)
+    for k in ha.arrays:
+        assert np.array_equal(ha.arrays[k], hb.arrays[k]), k
+        assert np.array_equal(b.arrays[k], hb.arrays[k]), k
