@@ -611,6 +611,49 @@ module lica_gpu
       integer(c_int32_t), intent(inout) :: status(*)
     end function lica_gpu_column_steps_geometry
 
+    integer(c_int) function lica_gpu_lvs_transport_geometry_device(geo, ncol, phi, layer, psif, &
+        wo, w, mflvs, vol_tot_ori, vol_tot_iphs, psi_cn, psi_zn, status, stats, prm, stream) &
+        bind(c, name="lica_gpu_lvs_transport_geometry_device")
+      import
+      type(c_ptr), value :: geo
+      integer(c_int32_t), value :: ncol
+      type(c_ptr), value :: phi
+      type(c_ptr), value :: layer
+      type(c_ptr), value :: psif
+      type(c_ptr), value :: wo
+      type(c_ptr), value :: w
+      type(c_ptr), value :: mflvs
+      type(c_ptr), value :: vol_tot_ori
+      type(c_ptr), value :: vol_tot_iphs
+      type(c_ptr), value :: psi_cn
+      type(c_ptr), value :: psi_zn
+      type(c_ptr), value :: status
+      type(c_ptr), value :: stats
+      type(lica_lvs_params), intent(in) :: prm
+      type(c_ptr), value :: stream
+    end function lica_gpu_lvs_transport_geometry_device
+
+    integer(c_int) function lica_gpu_lvs_transport_geometry(geo, ncol, phi, layer, psif, wo, w, &
+        mflvs, vol_tot_ori, vol_tot_iphs, psi_cn, psi_zn, status, stats, prm) &
+        bind(c, name="lica_gpu_lvs_transport_geometry")
+      import
+      type(c_ptr), value :: geo
+      integer(c_int32_t), value :: ncol
+      real(c_double), intent(inout) :: phi(*)
+      integer(c_int32_t), intent(inout) :: layer(*)
+      real(c_double), intent(inout) :: psif(*)
+      real(c_double), intent(inout) :: wo(*)
+      real(c_double), intent(in) :: w(*)
+      real(c_double), intent(in) :: mflvs(*)
+      real(c_double), intent(inout) :: vol_tot_ori(*)
+      real(c_double), intent(in) :: vol_tot_iphs(*)
+      real(c_double), intent(inout) :: psi_cn(*)
+      real(c_double), intent(inout) :: psi_zn(*)
+      integer(c_int32_t), intent(inout) :: status(*)
+      real(c_double), intent(inout) :: stats(*)
+      type(lica_lvs_params), intent(in) :: prm
+    end function lica_gpu_lvs_transport_geometry
+
     integer(c_int) function lica_gpu_lvs_transport_device(ncol, n, length, phi, layer, psif, &
         wo, w, mflvs, vol_tot_ori, vol_tot_iphs, psi_cn, psi_zn, status, stats, prm, stream) &
         bind(c, name="lica_gpu_lvs_transport_device")

@@ -430,6 +430,19 @@ int lica_gpu_column_steps_geometry_device(const lica_col_geo* geo, int32_t ncol,
 int lica_gpu_column_steps_geometry(const lica_col_geo* geo, int32_t ncol, const lica_col_props* props,
                                    lica_col_state* st, int32_t nsteps, int32_t* status);
 
+/* lica_gpu_lvs_transport[_device] on ncol stretched columns of the geometry's n and length:
+ * VEL_INTP's 4-point stencil on the stretched flow faces (KCOU_VEL), GRID_COUPLING(0)'s
+ * boxes from the tables. */
+int lica_gpu_lvs_transport_geometry_device(const lica_col_geo* geo, int32_t ncol, double* phi, int32_t* layer,
+                                           double* psif, double* wo, const double* w, const double* mflvs,
+                                           double* vol_tot_ori, const double* vol_tot_iphs, double* psi_cn,
+                                           double* psi_zn, int32_t* status, double* stats, const lica_lvs_params* prm,
+                                           void* stream);
+int lica_gpu_lvs_transport_geometry(const lica_col_geo* geo, int32_t ncol, double* phi, int32_t* layer, double* psif,
+                                    double* wo, const double* w, const double* mflvs, double* vol_tot_ori,
+                                    const double* vol_tot_iphs, double* psi_cn, double* psi_zn, int32_t* status,
+                                    double* stats, const lica_lvs_params* prm);
+
 int lica_gpu_lvs_transport_device(int32_t ncol, int32_t n, double length, double* phi, int32_t* layer,
                                   double* psif, double* wo, const double* w, const double* mflvs,
                                   double* vol_tot_ori, const double* vol_tot_iphs, double* psi_cn,

@@ -1832,14 +1832,6 @@ extern "C" {
 
 }  // extern "C"
 
-// A stretched column's geometry on the device (lica_gpu_column_geometry_create).
-struct lica_col_geo {
-    int n = 0;
-    double length = 0.0;
-    void* buf = nullptr;
-    col::ColGeoDev dev{};
-};
-
 namespace {
 
 int column_steps_device(int32_t ncol, int32_t n, double length, const lica_col_props* props, const lica_col_state* st,

@@ -78,3 +78,12 @@ __device__ __forceinline__ double box_mean(const double* f, int nf, int k1, int 
 
 }  // namespace col
 }  // namespace lica
+
+// A stretched column's geometry on the device (lica_gpu_column_geometry_create): the
+// column size and length it was checked for and one buffer holding its arrays.
+struct lica_col_geo {
+    int n = 0;
+    double length = 0.0;
+    void* buf = nullptr;
+    lica::col::ColGeoDev dev{};
+};

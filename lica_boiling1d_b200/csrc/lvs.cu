@@ -33,7 +33,8 @@ __global__ void __launch_bounds__(32 * WARPS)
                     double* __restrict__ psif, double* __restrict__ wo, const double* __restrict__ w,
                     const double* __restrict__ mf, double* __restrict__ vol_ori, const double* __restrict__ vol_iphs,
                     double* __restrict__ psi_cn, double* __restrict__ psi_zn, int* __restrict__ status,
-                    double* __restrict__ stats, Params P) {
+                    double* __restrict__ stats, Params P, const __grid_constant__ col::ColGeoDev geo,
+                    int has_geo) {
     __shared__ Win win[WARPS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int col = blockIdx.x * WARPS + warp;
@@ -41,7 +42,8 @@ __global__ void __launch_bounds__(32 * WARPS)
     const size_t nf = 2 * (size_t)n, sp = nf + 7, sf = nf + 2, sw = (size_t)n + 2;
     const int st = transport_column(&win[warp], lane, n, length, phi + col * sp, layer + col * sp, psif + col * sf,
                                     wo + col * sw, w + col * sw, mf + col * sp, vol_ori + col, vol_iphs[col],
-                                    psi_cn + col * sw, psi_zn + col * sw, stats + 4 * (size_t)col, P);
+                                    psi_cn + col * sw, psi_zn + col * sw, stats + 4 * (size_t)col, P,
+                                    has_geo ? &geo : nullptr);
     if (lane == 0) status[col] = st;
 }
 
@@ -144,14 +146,10 @@ int check_args(int32_t ncol, int32_t n, double length, const lica_lvs_params* pr
     return LICA_OK;
 }
 
-}  // namespace
-
-extern "C" {
-
-int lica_gpu_lvs_transport_device(int32_t ncol, int32_t n, double length, double* phi, int32_t* layer, double* psif,
-                                  double* wo, const double* w, const double* mflvs, double* vol_tot_ori,
-                                  const double* vol_tot_iphs, double* psi_cn, double* psi_zn, int32_t* status,
-                                  double* stats, const lica_lvs_params* prm, void* stream) {
+int transport_device(int32_t ncol, int32_t n, double length, double* phi, int32_t* layer, double* psif, double* wo,
+                     const double* w, const double* mflvs, double* vol_tot_ori, const double* vol_tot_iphs,
+                     double* psi_cn, double* psi_zn, int32_t* status, double* stats, const lica_lvs_params* prm,
+                     void* stream, const lica_col_geo* geo) {
     int st = check_args(ncol, n, length, prm);
     if (st) return st;
     if (!phi || !layer || !psif || !wo || !w || !mflvs || !vol_tot_ori || !vol_tot_iphs || !psi_cn || !psi_zn ||
@@ -159,18 +157,19 @@ int lica_gpu_lvs_transport_device(int32_t ncol, int32_t n, double length, double
         return LICA_BAD_ARG;
     Params P{prm->iphs, prm->first, prm->m_step, prm->mglobal, prm->denr, prm->dtconst};
     const unsigned blocks = (unsigned)((ncol + WARPS - 1) / WARPS);
+    const col::ColGeoDev g = geo ? geo->dev : col::ColGeoDev{};
     k_lvs_transport<<<blocks, 32 * WARPS, 0, (cudaStream_t)stream>>>(ncol, n, length, phi, layer, psif, wo, w, mflvs,
                                                                       vol_tot_ori, vol_tot_iphs, psi_cn, psi_zn,
-                                                                      status, stats, P);
+                                                                      status, stats, P, g, geo ? 1 : 0);
     LICA_CUDA_TRY(cudaGetLastError());
     lica_count_launches(1);
     return LICA_OK;
 }
 
-int lica_gpu_lvs_transport(int32_t ncol, int32_t n, double length, double* phi, int32_t* layer, double* psif,
-                           double* wo, const double* w, const double* mflvs, double* vol_tot_ori,
-                           const double* vol_tot_iphs, double* psi_cn, double* psi_zn, int32_t* status, double* stats,
-                           const lica_lvs_params* prm) {
+int transport_host(int32_t ncol, int32_t n, double length, double* phi, int32_t* layer, double* psif, double* wo,
+                   const double* w, const double* mflvs, double* vol_tot_ori, const double* vol_tot_iphs,
+                   double* psi_cn, double* psi_zn, int32_t* status, double* stats, const lica_lvs_params* prm,
+                   const lica_col_geo* geo) {
     int st = check_args(ncol, n, length, prm);
     if (st) return st;
     if (!phi || !layer || !psif || !wo || !w || !mflvs || !vol_tot_ori || !vol_tot_iphs || !psi_cn || !psi_zn ||
@@ -207,11 +206,11 @@ int lica_gpu_lvs_transport(int32_t ncol, int32_t n, double length, double* phi, 
                {o_vo, vol_tot_ori, 8 * nc},  {o_vi, vol_tot_iphs, 8 * nc}, {o_cn, psi_cn, 8 * nc * sw},
                {o_zn, psi_zn, 8 * nc * sw},  {o_stats, stats, 8 * 4 * nc}};
     for (const Cp& cp : ins) LICA_CUDA_TRY(cudaMemcpy(base + cp.o, cp.h, cp.bytes, cudaMemcpyHostToDevice));
-    st = lica_gpu_lvs_transport_device(ncol, n, length, (double*)(base + o_phi), (int32_t*)(base + o_lay),
-                                       (double*)(base + o_psif), (double*)(base + o_wo), (const double*)(base + o_w),
-                                       (const double*)(base + o_mf), (double*)(base + o_vo),
-                                       (const double*)(base + o_vi), (double*)(base + o_cn), (double*)(base + o_zn),
-                                       (int32_t*)(base + o_st), (double*)(base + o_stats), prm, nullptr);
+    st = transport_device(ncol, n, length, (double*)(base + o_phi), (int32_t*)(base + o_lay),
+                          (double*)(base + o_psif), (double*)(base + o_wo), (const double*)(base + o_w),
+                          (const double*)(base + o_mf), (double*)(base + o_vo), (const double*)(base + o_vi),
+                          (double*)(base + o_cn), (double*)(base + o_zn), (int32_t*)(base + o_st),
+                          (double*)(base + o_stats), prm, nullptr, geo);
     if (st) return st;
     struct Out {
         void* h;
@@ -224,6 +223,45 @@ int lica_gpu_lvs_transport(int32_t ncol, int32_t n, double length, double* phi, 
     for (size_t c = 0; c < nc; ++c)
         if (status[c] != LICA_OK) worst = status[c];
     return worst;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lica_gpu_lvs_transport_device(int32_t ncol, int32_t n, double length, double* phi, int32_t* layer, double* psif,
+                                  double* wo, const double* w, const double* mflvs, double* vol_tot_ori,
+                                  const double* vol_tot_iphs, double* psi_cn, double* psi_zn, int32_t* status,
+                                  double* stats, const lica_lvs_params* prm, void* stream) {
+    return transport_device(ncol, n, length, phi, layer, psif, wo, w, mflvs, vol_tot_ori, vol_tot_iphs, psi_cn, psi_zn,
+                            status, stats, prm, stream, nullptr);
+}
+
+int lica_gpu_lvs_transport(int32_t ncol, int32_t n, double length, double* phi, int32_t* layer, double* psif,
+                           double* wo, const double* w, const double* mflvs, double* vol_tot_ori,
+                           const double* vol_tot_iphs, double* psi_cn, double* psi_zn, int32_t* status, double* stats,
+                           const lica_lvs_params* prm) {
+    return transport_host(ncol, n, length, phi, layer, psif, wo, w, mflvs, vol_tot_ori, vol_tot_iphs, psi_cn, psi_zn,
+                          status, stats, prm, nullptr);
+}
+
+int lica_gpu_lvs_transport_geometry_device(const lica_col_geo* geo, int32_t ncol, double* phi, int32_t* layer,
+                                           double* psif, double* wo, const double* w, const double* mflvs,
+                                           double* vol_tot_ori, const double* vol_tot_iphs, double* psi_cn,
+                                           double* psi_zn, int32_t* status, double* stats, const lica_lvs_params* prm,
+                                           void* stream) {
+    if (!geo) return LICA_BAD_ARG;
+    return transport_device(ncol, geo->n, geo->length, phi, layer, psif, wo, w, mflvs, vol_tot_ori, vol_tot_iphs,
+                            psi_cn, psi_zn, status, stats, prm, stream, geo);
+}
+
+int lica_gpu_lvs_transport_geometry(const lica_col_geo* geo, int32_t ncol, double* phi, int32_t* layer, double* psif,
+                                    double* wo, const double* w, const double* mflvs, double* vol_tot_ori,
+                                    const double* vol_tot_iphs, double* psi_cn, double* psi_zn, int32_t* status,
+                                    double* stats, const lica_lvs_params* prm) {
+    if (!geo) return LICA_BAD_ARG;
+    return transport_host(ncol, geo->n, geo->length, phi, layer, psif, wo, w, mflvs, vol_tot_ori, vol_tot_iphs, psi_cn,
+                          psi_zn, status, stats, prm, geo);
 }
 
 int lica_gpu_reinitialization_device(int32_t ncol, int32_t n, double length, double* phi, const int32_t* layer,

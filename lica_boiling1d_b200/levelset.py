@@ -76,14 +76,18 @@ def _check(batch, arrays):
             raise ValueError(f"{name}: shape {tuple(a.shape)}, expected {sh[name]}")
 
 
-def transport(batch, w, mflvs, vol_tot_iphs, *, iphs, denr, dtconst, first, m_step, mglobal=1, stream=None):
+def transport(batch, w, mflvs, vol_tot_iphs, *, iphs, denr, dtconst, first, m_step, mglobal=1, stream=None,
+              geometry=None):
     """One TRANSPORT + GRID_COUPLING(0) of every column, updating ``batch`` in place.
 
     w: W on the flow faces (ncol, n+2); mflvs: interfacial mass flux per refined cell
     (ncol, nf+7), used when iphs = 1; vol_tot_iphs: (ncol,).  Returns (status, stats):
     per-column lica_status and [subcycles, max |grad phi|, min |grad phi|, IMASS].
     Host batches take numpy arrays; device batches take CUDA tensors (and a torch
-    stream, default: the current one)."""
+    stream, default: the current one).  geometry: a column.ColumnGeometry of the batch's
+    n and length for stretched flow grids (lica_gpu_lvs_transport_geometry[_device])."""
+    if geometry is not None and (geometry.n != batch.n or abs(geometry.length - batch.length) > 1e-12 * batch.length):
+        raise ValueError("the geometry's size or length differs from the batch's")
     prm = _params(iphs, first, m_step, mglobal, denr, dtconst)
     L = native.lib()
     st_arrays = {k: getattr(batch, k) for k in FIELDS}
@@ -99,10 +103,13 @@ def transport(batch, w, mflvs, vol_tot_iphs, *, iphs, denr, dtconst, first, m_st
         status = np.zeros(batch.ncol, np.int32)
         stats = np.zeros((batch.ncol, 4))
         d = lambda a: a.ctypes.data_as(_D)  # noqa: E731
-        rc = L.lica_gpu_lvs_transport(batch.ncol, batch.n, batch.length, d(batch.phi),
-                                      batch.layer.ctypes.data_as(_I32), d(batch.psif), d(batch.wo), d(w), d(mflvs),
-                                      d(batch.vol_tot_ori), d(vi), d(batch.psi_cn), d(batch.psi_zn),
-                                      status.ctypes.data_as(_I32), d(stats), C.byref(prm))
+        args = (d(batch.phi), batch.layer.ctypes.data_as(_I32), d(batch.psif), d(batch.wo), d(w), d(mflvs),
+                d(batch.vol_tot_ori), d(vi), d(batch.psi_cn), d(batch.psi_zn), status.ctypes.data_as(_I32),
+                d(stats), C.byref(prm))
+        if geometry is None:
+            rc = L.lica_gpu_lvs_transport(batch.ncol, batch.n, batch.length, *args)
+        else:
+            rc = L.lica_gpu_lvs_transport_geometry(geometry.handle(), batch.ncol, *args)
         native.check(rc, "TRANSPORT", ok=(0, 2))
         return status, stats
     import torch
@@ -117,10 +124,12 @@ def transport(batch, w, mflvs, vol_tot_iphs, *, iphs, denr, dtconst, first, m_st
     status = torch.zeros(batch.ncol, dtype=torch.int32, device=dev)
     stats = torch.zeros((batch.ncol, 4), dtype=torch.float64, device=dev)
     s = stream if stream is not None else torch.cuda.current_stream(dev)
-    rc = L.lica_gpu_lvs_transport_device(batch.ncol, batch.n, batch.length, batch.phi.data_ptr(),
-                                         batch.layer.data_ptr(), batch.psif.data_ptr(), batch.wo.data_ptr(),
-                                         w.data_ptr(), mflvs.data_ptr(), batch.vol_tot_ori.data_ptr(),
-                                         vol_tot_iphs.data_ptr(), batch.psi_cn.data_ptr(), batch.psi_zn.data_ptr(),
-                                         status.data_ptr(), stats.data_ptr(), C.byref(prm), C.c_void_p(s.cuda_stream))
+    args = (batch.phi.data_ptr(), batch.layer.data_ptr(), batch.psif.data_ptr(), batch.wo.data_ptr(), w.data_ptr(),
+            mflvs.data_ptr(), batch.vol_tot_ori.data_ptr(), vol_tot_iphs.data_ptr(), batch.psi_cn.data_ptr(),
+            batch.psi_zn.data_ptr(), status.data_ptr(), stats.data_ptr(), C.byref(prm), C.c_void_p(s.cuda_stream))
+    if geometry is None:
+        rc = L.lica_gpu_lvs_transport_device(batch.ncol, batch.n, batch.length, *args)
+    else:
+        rc = L.lica_gpu_lvs_transport_geometry_device(geometry.handle(), batch.ncol, *args)
     native.check(rc, "TRANSPORT")
     return status, stats

@@ -138,6 +138,10 @@ SIGNATURES = {
                                                         C.c_void_p, C.c_void_p]),
     "lica_gpu_column_steps_geometry": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(ColProps), C.POINTER(ColState),
                                                  C.c_int32, _I32]),
+    "lica_gpu_lvs_transport_geometry": (C.c_int, [C.c_void_p, C.c_int32, _D, _I32, _D, _D, _D, _D, _D, _D, _D, _D,
+                                                  _I32, _D, C.POINTER(LvsParams)]),
+    "lica_gpu_lvs_transport_geometry_device": (C.c_int, [C.c_void_p, C.c_int32] + [C.c_void_p] * 12 +
+                                               [C.POINTER(LvsParams), C.c_void_p]),
     "lica_gpu_reinitialization": (C.c_int, [C.c_int32, C.c_int32, C.c_double, _D, _I32, C.c_int32, _I32]),
     "lica_gpu_reinitialization_device": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_void_p, C.c_void_p,
                                                    C.c_int32, C.c_void_p, C.c_void_p]),

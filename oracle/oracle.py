@@ -33,6 +33,7 @@ def lib(native: bool = False):
         L.orc_lvs_init.argtypes = [C.c_int, C.c_double, C.c_double, _D, _INT, _D, _D, _D]
         L.orc_lvs_transport.argtypes = [C.c_int, C.c_double, _D, _INT, _D, _D, _D, _D, C.c_int, C.c_double,
                                         C.c_double, C.c_int, C.c_int, _D, C.c_double, C.c_int, _D, _D, _D]
+        L.orc_lvs_transport_geo.argtypes = L.orc_lvs_transport.argtypes + [C.c_void_p]
         L.orc_lvs_alphi_bc.argtypes = [C.c_int, C.c_double, _D]
         L.orc_lvs_band.argtypes = [C.c_int, C.c_double, _D, _INT]
         L.orc_lvs_reinit.argtypes = [C.c_int, C.c_double, _D, _INT, C.c_int]
@@ -164,8 +165,10 @@ def lvs_copy(st):
     return {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in st.items()}
 
 
-def lvs_transport(st, w, mflvs, *, iphs, denr, dtconst, first, m_step, vol_tot_iphs, mglobal, psi_cn, psi_zn):
-    """TRANSPORT + GRID_COUPLING(0) on a copy of st.  Returns (state, psi_cn, psi_zn, stats)."""
+def lvs_transport(st, w, mflvs, *, iphs, denr, dtconst, first, m_step, vol_tot_iphs, mglobal, psi_cn, psi_zn,
+                  geo=None):
+    """TRANSPORT + GRID_COUPLING(0) on a copy of st (geo: a stretched flow grid as col_geo
+    takes it).  Returns (state, psi_cn, psi_zn, stats)."""
     st = lvs_copy(st)
     n = st["n"]
     w = np.ascontiguousarray(w, dtype=np.float64)
@@ -175,9 +178,14 @@ def lvs_transport(st, w, mflvs, *, iphs, denr, dtconst, first, m_step, vol_tot_i
     pz = np.array(psi_zn, dtype=np.float64, copy=True)
     stats = np.zeros(4)
     vol = C.c_double(st["vol_tot_ori"])
-    rc = lib().orc_lvs_transport(n, st["length"], _p(st["phi"]), _pi(st["layer"]), _p(st["psif"]), _p(st["wo"]),
-                                 _p(w), _p(mf), int(iphs), float(denr), float(dtconst), int(first), int(m_step),
-                                 C.byref(vol), float(vol_tot_iphs), int(mglobal), _p(pc), _p(pz), _p(stats))
+    args = (n, st["length"], _p(st["phi"]), _pi(st["layer"]), _p(st["psif"]), _p(st["wo"]), _p(w), _p(mf),
+            int(iphs), float(denr), float(dtconst), int(first), int(m_step), C.byref(vol), float(vol_tot_iphs),
+            int(mglobal), _p(pc), _p(pz), _p(stats))
+    if geo is None:
+        rc = lib().orc_lvs_transport(*args)
+    else:
+        g = col_geo(geo)
+        rc = lib().orc_lvs_transport_geo(*args, C.byref(g))
     if rc == 2:
         raise OverflowError("band left the stored range k = -2..nf+4")
     assert rc == 0

@@ -178,3 +178,33 @@ def test_device_path_matches_host_path():
     back = dev.to(None)
     for k in ("phi", "layer", "psif", "wo", "vol_tot_ori", "psi_cn", "psi_zn"):
         assert np.array_equal(getattr(back, k), getattr(host, k)), k
+
+
+@pytest.mark.parametrize("iphs", [0, 1])
+def test_stretched_flow_grid(iphs):
+    """TRANSPORT + GRID_COUPLING(0) of columns on a wall-clustered flow grid (HYPTAN, gam 1.5):
+    VEL_INTP's stencil on the stretched faces and the coupling boxes from GEOM_COUPLING's
+    tables, host and device entries, bit for bit against the oracle on the same geometry."""
+    import torch
+    from lica_boiling1d_b200 import levelset
+    from lica_boiling1d_b200.column import ColumnGeometry
+    n = 96
+    geo = ColumnGeometry.tanh(n, 1.0, 1.5)
+    case = Case(n, [0.12, 0.3, 0.62], seed=21 + iphs, wscale=0.4, iphs=iphs, mf_amp=0.05)
+    host = case.batch()
+    dev = host.to("cuda")
+    for i, m in enumerate(range(1, 7)):
+        ws, mfs, vis = case.inputs()
+        prm = dict(denr=DENR, dtconst=1e-3, first=int(i == 0), m_step=m, mglobal=1)
+        st_h, sg_h = levelset.transport(host, ws, mfs, vis, iphs=iphs, geometry=geo, **prm)
+        st_d, sg_d = levelset.transport(dev, torch.from_numpy(ws).cuda(), torch.from_numpy(mfs).cuda(),
+                                        torch.from_numpy(vis).cuda(), iphs=iphs, geometry=geo, **prm)
+        torch.cuda.synchronize()
+        stats = []
+        for c, st in enumerate(case.states):
+            st2, pc, pz, s = O.lvs_transport(st, ws[c], mfs[c], iphs=iphs, vol_tot_iphs=vis[c], psi_cn=case.pcs[c],
+                                             psi_zn=case.pzs[c], geo=geo.arrays, **prm)
+            case.states[c], case.pcs[c], case.pzs[c] = st2, pc, pz
+            stats.append(s)
+        compare(case, host, sg_h, np.stack(stats), st_h, f"host step {m}")
+        compare(case, dev.to(None), sg_d.cpu().numpy(), np.stack(stats), st_d.cpu().numpy(), f"device step {m}")
