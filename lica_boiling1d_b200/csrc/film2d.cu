@@ -16,8 +16,8 @@
 //   (PASSIVE_SCALAR / TEMPASSIGN's role); TRANSPORT_RK3 with the reference's HJWENO in x and y
 //   (two_phase.f:1133-1495, 2477-2500); REINITIALIZATION's SSP-RK3 pseudo-time iterations with
 //   GODUNOV and Peng's smoothed sign (two_phase.f:2033-2474).
-// Surface tension is the continuum surface force -sigma kappa grad psi / rho_f with the
-// curvature of the refined level set (CAL_CUR / INTER_CUR's role, two_phase.f:3317-4432).
+// Surface tension is CAL_CUR's SURF CUR dpsi/dx / rho_f on the faces where psi jumps, with
+// CAL_CUR / CAL_CUR_INTEGRAL / INTER_CUR (two_phase.f:3317-4432) restated in 2-D below.
 // Simplifications: no interface recession term, explicit viscous terms.
 //
 // Every kernel is one thread per output cell, 32 x 8 thread blocks (coalesced rows), and
@@ -117,35 +117,131 @@ __global__ void k_props(const double* __restrict__ phi, double* __restrict__ psi
     tc[k] = c.tcm + c.tc_diff * ps;
 }
 
-// Curvature kappa = div(grad phi / |grad phi|) per flow cell (CAL_CUR's role in 2-D): central
-// differences on the refined grid (x periodic, y indices clamped) where |phi| < 2 h, the four
-// sub-cells averaged, limited to |kappa| <= 1/h.
-__device__ __forceinline__ double curv_refined(const double* __restrict__ phi, int I, int J, const Const& c) {
+// ---------------------------------------------------------------- CAL_CUR in 2-D
+// CAL_CUR(N_CUR = 4) (two_phase.f:2792, 3317-4432) on the refined grid, x periodic, y indices
+// clamped: (1) CURF_TMP, the curvature -(GXX GZ^2 + GZZ GX^2 - 2 GXZ GX GZ) / |grad phi|^3 by
+// central differences on band layers 1..N_CUR+1 (:3362-3397; the reference's y terms vanish
+// exactly for a field constant in y; |g|^3 = g2 sqrt(g2)); (2) CURF, CURF_TMP interpolated to
+// the foot of each cell of layers 1..N_CUR on the interface (:3405-3458, the trilinear form
+// with YD = 0); (3) per flow face where psi jumps, INTER_CUR's mean of CURF over the face box's
+// refined cells cut by the interface (0 < psi_f < 1, CURF /= 0), or over the box twice as wide
+// if it holds none (CAL_CUR_INTEGRAL, :3654-3795).  On the uniform 2x refinement the boxes
+// are whole refined cells.  A band layer m is |phi| < m hf.
+constexpr int kNCur = 4;
+
+__global__ void k_cur_tmp(const double* __restrict__ phi, double* __restrict__ kt, const Const c) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
+    if (I >= c.nxf || J >= c.nyf) return;
     const int nxf = c.nxf, nyf = c.nyf;
     const double* row = phi + (size_t)J * nxf;
     const double C = row[I];
-    if (!(fabs(C) < 2.0 * c.h)) return 0.0;
-    const int Ie = (I + 1 == nxf) ? 0 : I + 1, Iw = (I == 0) ? nxf - 1 : I - 1;
-    const double* up = phi + (size_t)(J + 1 < nyf ? J + 1 : nyf - 1) * nxf;
-    const double* dn = phi + (size_t)(J > 0 ? J - 1 : 0) * nxf;
-    const double E = row[Ie], W = row[Iw], N = up[I], S = dn[I];
-    const double fx = (E - W) * c.ih2f;
-    const double fy = (N - S) * c.ih2f;
-    const double fxx = (E - 2.0 * C + W) * c.ihfsq;
-    const double fyy = (N - 2.0 * C + S) * c.ihfsq;
-    const double fxy = ((up[Ie] - up[Iw]) - (dn[Ie] - dn[Iw])) * c.q4;
-    const double g2 = fx * fx + fy * fy;
-    if (!(g2 > 1e-12)) return 0.0;
-    const double num = (fxx * (fy * fy) - 2.0 * (fx * fy) * fxy) + fyy * (fx * fx);
-    return num / (g2 * sqrt(g2));
+    double out = 0.0;
+    if (fabs(C) < (kNCur + 1) * c.hf) {
+        const int Ie = (I + 1 == nxf) ? 0 : I + 1, Iw = (I == 0) ? nxf - 1 : I - 1;
+        const double* up = phi + (size_t)(J + 1 < nyf ? J + 1 : nyf - 1) * nxf;
+        const double* dn = phi + (size_t)(J > 0 ? J - 1 : 0) * nxf;
+        const double E = row[Ie], W = row[Iw], N = up[I], S = dn[I];
+        const double gx = 0.5 * (E - W) * c.ihf;
+        const double gz = 0.5 * (N - S) * c.ihf;
+        const double gxx = ((E - 2.0 * C) + W) * c.ihf * c.ihf;
+        const double gzz = ((N - 2.0 * C) + S) * c.ihf * c.ihf;
+        const double gxz = 0.25 * ((up[Ie] - up[Iw]) - (dn[Ie] - dn[Iw])) * c.ihf * c.ihf;
+        const double g2 = gx * gx + gz * gz;
+        if (g2 > 0.0) {
+            const double num = (gxx * (gz * gz) + gzz * (gx * gx)) - 2.0 * (gxz * gx * gz);
+            out = -num / (g2 * sqrt(g2));
+        }
+    }
+    kt[(size_t)J * nxf + I] = out;
 }
 
-__global__ void k_curv(const double* __restrict__ phi, double* __restrict__ kap, const Const c) {
+__global__ void k_cur_foot(const double* __restrict__ phi, const double* __restrict__ kt, double* __restrict__ cf,
+                           const Const c) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
+    if (I >= c.nxf || J >= c.nyf) return;
+    const int nxf = c.nxf, nyf = c.nyf;
+    const double C = phi[(size_t)J * nxf + I];
+    double out = 0.0;
+    if (fabs(C) < kNCur * c.hf) {
+        const int Ie = (I + 1 == nxf) ? 0 : I + 1, Iw = (I == 0) ? nxf - 1 : I - 1;
+        const int Jn = J + 1 < nyf ? J + 1 : nyf - 1, Js = J > 0 ? J - 1 : 0;
+        const double dpx = 0.5 * (phi[(size_t)J * nxf + Ie] - phi[(size_t)J * nxf + Iw]) * c.ihf;
+        const double dpz = 0.5 * (phi[(size_t)Jn * nxf + I] - phi[(size_t)Js * nxf + I]) * c.ihf;
+        const double g2 = dpx * dpx + dpz * dpz;
+        if (g2 > 0.0) {
+            const double amdpi = 1.0 / sqrt(g2);
+            const double dis = C * amdpi;
+            const double xp = (I + 0.5) * c.hf, zp = (J + 0.5) * c.hf;
+            const double xb = xp - dis * (dpx * amdpi), zb = zp - dis * (dpz * amdpi);
+            int i1, i2, j1, j2;
+            double xd, zd;
+            if (xb >= xp) {
+                xd = (xb - xp) * c.ihf;
+                i1 = I;
+                i2 = Ie;
+            } else {
+                xd = (xb - (xp - c.hf)) * c.ihf;
+                i1 = Iw;
+                i2 = I;
+            }
+            if (zb >= zp) {
+                zd = (zb - zp) * c.ihf;
+                j1 = J;
+                j2 = Jn;
+            } else {
+                zd = (zb - (zp - c.hf)) * c.ihf;
+                j1 = Js;
+                j2 = J;
+            }
+            const double c00 = kt[(size_t)j1 * nxf + i1] * (1.0 - xd) + kt[(size_t)j1 * nxf + i2] * xd;
+            const double c01 = kt[(size_t)j2 * nxf + i1] * (1.0 - xd) + kt[(size_t)j2 * nxf + i2] * xd;
+            out = c00 * (1.0 - zd) + c01 * zd;
+        }
+    }
+    cf[(size_t)J * nxf + I] = out;
+}
+
+// INTER_CUR over refined columns c0..c0+nc-1 (x periodic) and rows r0..r0+nr-1, column by
+// column; returns the cut-cell count (VOLF) and leaves the mean in cur when it is not 0.
+__device__ __forceinline__ double inter_cur(const double* __restrict__ phi, const double* __restrict__ cf, int c0,
+                                            int nc, int r0, int nr, const Const& c, double& cur) {
+    const int nxf = c.nxf;
+    double sum = 0.0, volf = 0.0;
+    for (int a = 0; a < nc; ++a) {
+        int II = c0 + a;
+        II = II < 0 ? II + nxf : (II >= nxf ? II - nxf : II);
+        for (int b = 0; b < nr; ++b) {
+            const size_t q = (size_t)(r0 + b) * nxf + II;
+            const double hh = heaviside(phi[q], c);
+            const double v = cf[q];
+            if (hh > 0.0 && hh < 1.0 && v != 0.0) {
+                sum = sum + v;
+                volf = volf + 1.0;
+            }
+        }
+    }
+    if (volf != 0.0) cur = sum / volf;
+    return volf;
+}
+
+// Face curvatures: cx on the face west of cell (i, j), cy on the face below it (row 0, the
+// wall: 0).
+__global__ void k_face_cur(const double* __restrict__ phi, const double* __restrict__ cf,
+                           const double* __restrict__ psi, double* __restrict__ cx, double* __restrict__ cy,
+                           const Const c) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= c.nx || j >= c.ny) return;
-    const double q = (curv_refined(phi, 2 * i, 2 * j, c) + curv_refined(phi, 2 * i + 1, 2 * j, c)) +
-                     (curv_refined(phi, 2 * i, 2 * j + 1, c) + curv_refined(phi, 2 * i + 1, 2 * j + 1, c));
-    kap[(size_t)j * c.nx + i] = fmin(fmax(0.25 * q, -c.ih), c.ih);
+    const int nx = c.nx;
+    const size_t k = (size_t)j * nx + i;
+    double vx = 0.0, vy = 0.0;
+    if ((psi[k] - psi[(size_t)j * nx + west(i, nx)]) != 0.0) {
+        if (inter_cur(phi, cf, 2 * i - 1, 2, 2 * j, 2, c, vx) == 0.0) inter_cur(phi, cf, 2 * i - 2, 4, 2 * j, 2, c, vx);
+    }
+    if (j >= 1 && (psi[k] - psi[k - nx]) != 0.0) {
+        if (inter_cur(phi, cf, 2 * i, 2, 2 * j - 1, 2, c, vy) == 0.0) inter_cur(phi, cf, 2 * i, 2, 2 * j - 2, 4, c, vy);
+    }
+    cx[k] = vx;
+    cy[k] = vy;
 }
 
 // Face coefficients beta = 1/rho: bx by harmonic mean (x periodic), by on rows 0..ny.
@@ -164,8 +260,8 @@ __global__ void k_beta(const double* __restrict__ den, double* __restrict__ bx, 
 // substep.
 __global__ void k_momentum(const double* __restrict__ u, const double* __restrict__ v,
                            const double* __restrict__ den, const double* __restrict__ vis,
-                           const double* __restrict__ psi, const double* __restrict__ kap,
-                           const double* __restrict__ p, const double* __restrict__ bx,
+                           const double* __restrict__ psi, const double* __restrict__ cx,
+                           const double* __restrict__ cy, const double* __restrict__ p, const double* __restrict__ bx,
                            const double* __restrict__ by, double* __restrict__ us, double* __restrict__ vs,
                            double* __restrict__ ru, double* __restrict__ rv, double dt, double gam, double ro,
                            double adt, const Const c) {
@@ -200,9 +296,8 @@ __global__ void k_momentum(const double* __restrict__ u, const double* __restric
         const double tys = mus * ((uc - usv) * ih + (vrow[i] - vrow[iw]) * ih);
         const double rho = 0.5 * (den[(size_t)j * nx + iw] + den[k]);
         const double visc = ((txe - txw) * ih + (tyn - tys) * ih) / rho;
-        // surface tension -sigma kappa grad psi on the face (continuum surface force)
-        const double kapf = 0.5 * (kap[(size_t)j * nx + iw] + kap[k]);
-        const double nu = visc - conv - (c.surf * kapf) * ((psi[k] - psi[(size_t)j * nx + iw]) * ih) / rho;
+        // surface tension SURF CUR dpsi/dx on the face (CAL_CUR's SUR_X, two_phase.f:3547-3556)
+        const double nu = visc - conv + (c.surf * cx[k]) * ((psi[k] - psi[(size_t)j * nx + iw]) * ih) / rho;
         us[k] = uc + dt * (gam * nu + ro * ru[k]) - adt * (bx[k] * ((p[k] - p[(size_t)j * nx + iw]) * ih));
         ru[k] = nu;
     }
@@ -228,9 +323,9 @@ __global__ void k_momentum(const double* __restrict__ u, const double* __restric
         const double rho = 0.5 * (dlo + dhi);
         const double visc = ((txe - txw) * ih + (tyn - tys) * ih) / rho;
         const size_t khi = (j + 1 < ny) ? k + nx : (size_t)(ny - 1) * nx + i;
-        const double kapf = 0.5 * (kap[k] + kap[khi]);
-        const double nv = visc - conv + c.gravity * (c.denp / rho - 1.0) -
-                          (c.surf * kapf) * ((psi[khi] - psi[k]) * ih) / rho;
+        const double cur = (j + 1 < ny) ? cy[k + nx] : 0.0;   // the face above row j (top face: 0)
+        const double nv = visc - conv + c.gravity * (c.denp / rho - 1.0) +
+                          (c.surf * cur) * ((psi[khi] - psi[k]) * ih) / rho;
         const size_t kf = (size_t)jf * nx + i;
         const double gp = (jf < ny) ? (p[kf] - p[k]) * ih : (0.0 - p[k]) * c.ih2;  // p = 0 on the top face
         vs[kf] = vc + dt * (gam * nv + ro * rv[k]) - adt * (by[kf] * gp);
@@ -468,9 +563,9 @@ struct lica_film2d {
     // flow-grid scratch
     double *psi = nullptr, *den = nullptr, *vis = nullptr, *densc = nullptr, *tc = nullptr, *bx = nullptr,
            *by = nullptr, *us = nullptr, *vs = nullptr, *ru = nullptr, *rv = nullptr, *rth = nullptr, *f = nullptr,
-           *mdot = nullptr, *th2 = nullptr, *dp = nullptr, *kap = nullptr;
-    // refined-grid scratch
-    double *rphi = nullptr, *ph[3] = {nullptr, nullptr, nullptr};
+           *mdot = nullptr, *th2 = nullptr, *dp = nullptr, *cx = nullptr, *cy = nullptr;
+    // refined-grid scratch (kt, cf: CAL_CUR's CURF_TMP and CURF)
+    double *rphi = nullptr, *ph[3] = {nullptr, nullptr, nullptr}, *kt = nullptr, *cf = nullptr;
     // optional learned initial guess of the pressure solves, and the training-pair capture
     lica_unet* guess = nullptr;
     double* capture = nullptr;
@@ -490,7 +585,7 @@ int dalloc(double** p, size_t n) {
 void free_all(lica_film2d* F) {
     if (F->mg) lica_mg_destroy(F->mg);
     double* ptrs[] = {F->psi, F->den, F->vis, F->densc, F->tc, F->bx, F->by, F->us, F->vs, F->ru, F->rv, F->rth, F->f,
-                      F->mdot, F->th2, F->dp, F->kap, F->rphi, F->ph[0], F->ph[1], F->ph[2]};
+                      F->mdot, F->th2, F->dp, F->cx, F->cy, F->rphi, F->ph[0], F->ph[1], F->ph[2], F->kt, F->cf};
     for (double* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -529,12 +624,14 @@ int lica_film2d_create(lica_film2d** out, int32_t nx, int32_t ny, const lica_fil
     }
     const size_t n = (size_t)nx * ny, nv = n + nx, nf = 4 * n;
     double** flow[] = {&F->psi, &F->den, &F->vis, &F->densc, &F->tc, &F->bx, &F->us, &F->ru, &F->rv, &F->rth,
-                       &F->f, &F->mdot, &F->th2, &F->dp, &F->kap};
+                       &F->f, &F->mdot, &F->th2, &F->dp, &F->cx, &F->cy};
     for (double** p : flow)
         if ((st = dalloc(p, n))) break;
     if (!st) st = dalloc(&F->by, nv);
     if (!st) st = dalloc(&F->vs, nv);
     if (!st) st = dalloc(&F->rphi, nf);
+    if (!st) st = dalloc(&F->kt, nf);
+    if (!st) st = dalloc(&F->cf, nf);
     for (int b = 0; b < 3 && !st; ++b) st = dalloc(&F->ph[b], nf);
     if (st) {
         free_all(F);
@@ -571,12 +668,14 @@ int lica_film2d_step_device(lica_film2d* F, double* u, double* v, double* p, dou
         const double adt = alpha * dt, iadt = 1.0 / (alpha * dt);
         k_props<<<gflow, blk, 0, s>>>(phc, F->psi, F->den, F->vis, F->densc, F->tc, c);
         k_beta<<<gflow, blk, 0, s>>>(F->den, F->bx, F->by, c);
-        k_curv<<<gflow, blk, 0, s>>>(phc, F->kap, c);
-        k_momentum<<<gflow, blk, 0, s>>>(u, v, F->den, F->vis, F->psi, F->kap, p, F->bx, F->by, F->us, F->vs, F->ru,
-                                         F->rv, dt, gam, ro, adt, c);
+        k_cur_tmp<<<gref, blk, 0, s>>>(phc, F->kt, c);
+        k_cur_foot<<<gref, blk, 0, s>>>(phc, F->kt, F->cf, c);
+        k_face_cur<<<gflow, blk, 0, s>>>(phc, F->cf, F->psi, F->cx, F->cy, c);
+        k_momentum<<<gflow, blk, 0, s>>>(u, v, F->den, F->vis, F->psi, F->cx, F->cy, p, F->bx, F->by, F->us, F->vs,
+                                         F->ru, F->rv, dt, gam, ro, adt, c);
         k_source_rhs<<<gflow, blk, 0, s>>>(thc, F->psi, F->tc, F->us, F->vs, F->f, F->mdot, iadt, c);
         LICA_CUDA_TRY(cudaGetLastError());
-        launches += 5;
+        launches += 7;
         // the pressure increment, from the learned guess (zero if it is no better) or zero
         local.guess_rel[k - 1] = 1.0;
         if (F->guess) {

@@ -79,7 +79,7 @@ double heaviside(double x, const D2& d) {
 }
 
 struct Props {
-    Vec psi, den, vis, densc, tc, bx, by, kap;
+    Vec psi, den, vis, densc, tc, bx, by, cx, cy;
 };
 
 void properties(const Vec& phi, const D2& d, Props& P) {
@@ -116,34 +116,126 @@ void properties(const Vec& phi, const D2& d, Props& P) {
     for (int i = 0; i < nx; ++i) P.by[(size_t)ny * nx + i] = 1.0 / P.den[(size_t)(ny - 1) * nx + i];
 }
 
-double curv_refined(const Vec& phi, int I, int J, const D2& d) {
+// CAL_CUR (two_phase.f:3317-4432) in 2-D, as film2d.py's curvature_refined,
+// curvature_interface and face_curvature state it: CURF_TMP on band layers 1..N_CUR+1,
+// CURF at the interface foot of layers 1..N_CUR, and per face INTER_CUR's mean over the
+// interface cells of the face's box (the box twice as wide where it holds none).
+constexpr int N_CUR = 4;
+
+void curvature_refined(const Vec& phi, const D2& d, Vec& kt) {
     const int nxf = d.nxf, nyf = d.nyf;
-    const double* row = &phi[(size_t)J * nxf];
-    const double* up = &phi[(size_t)std::min(J + 1, nyf - 1) * nxf];
-    const double* dn = &phi[(size_t)std::max(J - 1, 0) * nxf];
-    const int Ie = E_(I, nxf), Iw = W_(I, nxf);
-    const double C = row[I], E = row[Ie], W = row[Iw], N = up[I], S = dn[I];
-    const double fx = (E - W) * d.ih2f;
-    const double fy = (N - S) * d.ih2f;
-    const double fxx = (E - 2.0 * C + W) * d.ihfsq;
-    const double fyy = (N - 2.0 * C + S) * d.ihfsq;
-    const double fxy = ((up[Ie] - up[Iw]) - (dn[Ie] - dn[Iw])) * d.q4;
-    const double g2 = fx * fx + fy * fy;
-    const double num = (fxx * (fy * fy) - 2.0 * (fx * fy) * fxy) + fyy * (fx * fx);
-    return (std::fabs(C) < 2.0 * d.h && g2 > 1e-12) ? num / (g2 * std::sqrt(g2)) : 0.0;
+    kt.assign((size_t)nxf * nyf, 0.0);
+#pragma omp parallel for
+    for (int J = 0; J < nyf; ++J)
+        for (int I = 0; I < nxf; ++I) {
+            const double* row = &phi[(size_t)J * nxf];
+            const double* up = &phi[(size_t)std::min(J + 1, nyf - 1) * nxf];
+            const double* dn = &phi[(size_t)std::max(J - 1, 0) * nxf];
+            const int Ie = E_(I, nxf), Iw = W_(I, nxf);
+            const double C = row[I], E = row[Ie], W = row[Iw], N = up[I], S = dn[I];
+            if (!(std::fabs(C) < (N_CUR + 1) * d.hf)) continue;
+            const double gx = 0.5 * (E - W) * d.ihf;
+            const double gz = 0.5 * (N - S) * d.ihf;
+            const double gxx = ((E - 2.0 * C) + W) * d.ihf * d.ihf;
+            const double gzz = ((N - 2.0 * C) + S) * d.ihf * d.ihf;
+            const double gxz = 0.25 * ((up[Ie] - up[Iw]) - (dn[Ie] - dn[Iw])) * d.ihf * d.ihf;
+            const double g2 = gx * gx + gz * gz;
+            if (!(g2 > 0.0)) continue;
+            const double num = (gxx * (gz * gz) + gzz * (gx * gx)) - 2.0 * (gxz * gx * gz);
+            kt[(size_t)J * nxf + I] = -num / (g2 * std::sqrt(g2));
+        }
 }
 
-void curvature(const Vec& phi, const D2& d, Vec& kap) {
+void curvature_interface(const Vec& phi, const Vec& kt, const D2& d, Vec& cf) {
+    const int nxf = d.nxf, nyf = d.nyf;
+    cf.assign((size_t)nxf * nyf, 0.0);
+#pragma omp parallel for
+    for (int J = 0; J < nyf; ++J)
+        for (int I = 0; I < nxf; ++I) {
+            const int Jn = std::min(J + 1, nyf - 1), Js = std::max(J - 1, 0);
+            const int Ie = E_(I, nxf), Iw = W_(I, nxf);
+            const double C = phi[(size_t)J * nxf + I];
+            if (!(std::fabs(C) < N_CUR * d.hf)) continue;
+            const double dpx = 0.5 * (phi[(size_t)J * nxf + Ie] - phi[(size_t)J * nxf + Iw]) * d.ihf;
+            const double dpz = 0.5 * (phi[(size_t)Jn * nxf + I] - phi[(size_t)Js * nxf + I]) * d.ihf;
+            const double g2 = dpx * dpx + dpz * dpz;
+            if (!(g2 > 0.0)) continue;
+            const double amdpi = 1.0 / std::sqrt(g2);
+            const double dis = C * amdpi;
+            const double xp = (I + 0.5) * d.hf, zp = (J + 0.5) * d.hf;
+            const double xb = xp - dis * (dpx * amdpi), zb = zp - dis * (dpz * amdpi);
+            int i1, i2, j1, j2;
+            double xd, zd;
+            if (xb >= xp) {
+                xd = (xb - xp) * d.ihf;
+                i1 = I;
+                i2 = Ie;
+            } else {
+                xd = (xb - (xp - d.hf)) * d.ihf;
+                i1 = Iw;
+                i2 = I;
+            }
+            if (zb >= zp) {
+                zd = (zb - zp) * d.ihf;
+                j1 = J;
+                j2 = Jn;
+            } else {
+                zd = (zb - (zp - d.hf)) * d.ihf;
+                j1 = Js;
+                j2 = J;
+            }
+            const double c00 = kt[(size_t)j1 * nxf + i1] * (1.0 - xd) + kt[(size_t)j1 * nxf + i2] * xd;
+            const double c01 = kt[(size_t)j2 * nxf + i1] * (1.0 - xd) + kt[(size_t)j2 * nxf + i2] * xd;
+            cf[(size_t)J * nxf + I] = c00 * (1.0 - zd) + c01 * zd;
+        }
+}
+
+// INTER_CUR over refined columns c0..c0+nc-1 (x periodic) and rows r0..r0+nr-1, column by
+// column: the mean of CURF over the cells cut by the interface (0 < psi_f < 1, CURF /= 0).
+static bool inter_cur(const Vec& phi, const Vec& cf, int c0, int nc, int r0, int nr, const D2& d, double& cur) {
+    const int nxf = d.nxf;
+    double sum = 0.0, volf = 0.0;
+    for (int a = 0; a < nc; ++a) {
+        const int II = ((c0 + a) % nxf + nxf) % nxf;
+        for (int b = 0; b < nr; ++b) {
+            const size_t q = (size_t)(r0 + b) * nxf + II;
+            const double hh = heaviside(phi[q], d);
+            if (hh > 0.0 && hh < 1.0 && cf[q] != 0.0) {
+                sum = sum + cf[q];
+                volf = volf + 1.0;
+            }
+        }
+    }
+    if (volf != 0.0) cur = sum / volf;
+    return volf != 0.0;
+}
+
+void face_curvature(const Vec& phi, const Vec& cf, const D2& d, Props& P) {
     const int nx = d.nx, ny = d.ny;
-    kap.assign((size_t)nx * ny, 0.0);
+    P.cx.assign((size_t)nx * ny, 0.0);
+    P.cy.assign((size_t)nx * ny, 0.0);
 #pragma omp parallel for
     for (int j = 0; j < ny; ++j)
         for (int i = 0; i < nx; ++i) {
-            const double kc = 0.25 * ((curv_refined(phi, 2 * i, 2 * j, d) + curv_refined(phi, 2 * i + 1, 2 * j, d)) +
-                                      (curv_refined(phi, 2 * i, 2 * j + 1, d) +
-                                       curv_refined(phi, 2 * i + 1, 2 * j + 1, d)));
-            kap[(size_t)j * nx + i] = std::min(std::max(kc, -d.ih), d.ih);
+            const size_t k = (size_t)j * nx + i;
+            if ((P.psi[k] - P.psi[(size_t)j * nx + W_(i, nx)]) != 0.0) {
+                double cur = 0.0;
+                if (!inter_cur(phi, cf, 2 * i - 1, 2, 2 * j, 2, d, cur)) inter_cur(phi, cf, 2 * i - 2, 4, 2 * j, 2, d, cur);
+                P.cx[k] = cur;
+            }
+            if (j >= 1 && (P.psi[k] - P.psi[k - nx]) != 0.0) {
+                double cur = 0.0;
+                if (!inter_cur(phi, cf, 2 * i, 2, 2 * j - 1, 2, d, cur)) inter_cur(phi, cf, 2 * i, 2, 2 * j - 2, 4, d, cur);
+                P.cy[k] = cur;
+            }
         }
+}
+
+void curvature(const Vec& phi, const D2& d, Props& P) {
+    Vec kt, cf;
+    curvature_refined(phi, d, kt);
+    curvature_interface(phi, kt, d, cf);
+    face_curvature(phi, cf, d, P);
 }
 
 // volume source S and mdot (mass_source)
@@ -204,8 +296,7 @@ void momentum(const Vec& u, const Vec& v, const Props& P, const D2& d, Vec& nu, 
                 const double tys = mus * ((uc - us) * ih + (v[vrow + i] - v[vrow + iw]) * ih);
                 const double rho = 0.5 * (P.den[kw] + P.den[k]);
                 const double visc = ((txe - txw) * ih + (tyn - tys) * ih) / rho;
-                const double kf = 0.5 * (P.kap[kw] + P.kap[k]);
-                nu[k] = visc - conv - (d.surf * kf) * ((P.psi[k] - P.psi[kw]) * ih) / rho;
+                nu[k] = visc - conv + (d.surf * P.cx[k]) * ((P.psi[k] - P.psi[kw]) * ih) / rho;
             }
             {
                 // face j + 1
@@ -229,9 +320,9 @@ void momentum(const Vec& u, const Vec& v, const Props& P, const D2& d, Vec& nu, 
                 const double dlo = P.den[k], dhi = P.den[rn + i];
                 const double rho = 0.5 * (dlo + dhi);
                 const double visc = ((txe - txw) * ih + (tyn - tys) * ih) / rho;
-                const double kf = 0.5 * (P.kap[k] + P.kap[rn + i]);
-                nv[k] = visc - conv + d.gravity * (d.denp / rho - 1.0) -
-                        (d.surf * kf) * ((P.psi[rn + i] - P.psi[k]) * ih) / rho;
+                const double cf = (j + 1 < ny) ? P.cy[k + nx] : 0.0;   // the face above row j
+                nv[k] = visc - conv + d.gravity * (d.denp / rho - 1.0) +
+                        (d.surf * cf) * ((P.psi[rn + i] - P.psi[k]) * ih) / rho;
             }
         }
 }
@@ -373,7 +464,7 @@ int orc_film2d_step(int nx, int ny, const double* props, double rtol, int nreini
         const double adt = alpha * dt, iadt = 1.0 / (alpha * dt);
         properties(PH, d, P);
         mass_source(T, P, d, S, md);
-        curvature(PH, d, P.kap);
+        curvature(PH, d, P);
         momentum(U, V, P, d, nu, nvv);
 #pragma omp parallel for
         for (int j = 0; j < ny; ++j)

@@ -37,10 +37,11 @@ the reference's wall-normal z):
   * both on the band |phi| < 8 refined cells (BAND_GENERATION's role, two_phase.f:1622-2030):
     cells outside keep their value (the properties see phi only within one flow cell of the
     interface).
-  * surface tension: the continuum surface force -sigma kappa grad psi / rho_f on every face
-    (sigma = 1/We), kappa = div(grad phi / |grad phi|) from central differences of the refined
-    level set near the interface, averaged to the flow cells (the 2-D analogue of CAL_CUR /
-    CAL_CUR_INTEGRAL / INTER_CUR, two_phase.f:3317-4432).
+  * surface tension: CAL_CUR / CAL_CUR_INTEGRAL / INTER_CUR (two_phase.f:3317-4432) in 2-D:
+    the curvature of the refined level set on the band by central differences, carried to the
+    foot of each band cell on the interface (bilinear interpolation), averaged per flow face
+    over the interface cells of the face's box, and applied as SURF CUR dpsi/dx / rho_f on the
+    faces where psi jumps (SURF = 1/We).
 Documented simplifications: the interface recession term of the phase change is not applied
 (the interface moves with the one-fluid velocity, which carries the expansion flow of S),
 and the viscous terms are explicit.
@@ -222,32 +223,127 @@ def mass_source(th, psi, tc, D):
     return md * D.cvol, md
 
 
-def curvature(phi, D):
-    """Curvature kappa = div(grad phi / |grad phi|) per flow cell (CAL_CUR's role in 2-D):
-    second-order central differences on the refined grid (x periodic, y indices clamped),
-    computed where |phi| < 2 h (zero elsewhere), averaged over the four sub-cells and limited
-    to |kappa| <= 1/h."""
-    nj = phi.shape[0]
+N_CUR = 4   # CAL_CUR(4, ...) (two_phase.f:2792): kappa on band layers 1..N_CUR+1, CURF on 1..N_CUR
+
+
+def _nbrs(a):
+    """E, W (x periodic), N, S (y indices clamped) and the four corners of a refined array."""
+    nj = a.shape[0]
     idx = np.arange(nj)
-    up = phi[np.minimum(idx + 1, nj - 1)]
-    dn = phi[np.maximum(idx - 1, 0)]
-    E, W = np.roll(phi, -1, axis=1), np.roll(phi, 1, axis=1)
-    NE, NW = np.roll(up, -1, axis=1), np.roll(up, 1, axis=1)
-    SE, SW = np.roll(dn, -1, axis=1), np.roll(dn, 1, axis=1)
-    fx = (E - W) * D.ih2f
-    fy = (up - dn) * D.ih2f
-    fxx = (E - 2.0 * phi + W) * D.ihfsq
-    fyy = (up - 2.0 * phi + dn) * D.ihfsq
-    fxy = ((NE - NW) - (SE - SW)) * D.q4
-    g2 = fx * fx + fy * fy
-    num = (fxx * (fy * fy) - 2.0 * (fx * fy) * fxy) + fyy * (fx * fx)
+    up = a[np.minimum(idx + 1, nj - 1)]
+    dn = a[np.maximum(idx - 1, 0)]
+    E, W = np.roll(a, -1, axis=1), np.roll(a, 1, axis=1)
+    return E, W, up, dn, np.roll(up, -1, axis=1), np.roll(up, 1, axis=1), np.roll(dn, -1, axis=1), \
+        np.roll(dn, 1, axis=1)
+
+
+def curvature_refined(phi, D):
+    """CAL_CUR's CURF_TMP (two_phase.f:3362-3397) in 2-D: kappa = -(GXX GZ^2 + GZZ GX^2 -
+    2 GXZ GX GZ) / |grad phi|^3 from central differences on the refined grid, on the band
+    layers 1..N_CUR+1 (|phi| < (N_CUR+1) hf), 0 elsewhere and where grad phi vanishes.  The
+    reference's y terms are exactly zero for a field that does not vary in y; |g|^3 is
+    evaluated as g2 sqrt(g2)."""
+    E, W, N, S, NE, NW, SE, SW = _nbrs(phi)
+    gx = 0.5 * (E - W) * D.ihf
+    gz = 0.5 * (N - S) * D.ihf
+    gxx = ((E - 2.0 * phi) + W) * D.ihf * D.ihf
+    gzz = ((N - 2.0 * phi) + S) * D.ihf * D.ihf
+    gxz = 0.25 * ((NE - NW) - (SE - SW)) * D.ihf * D.ihf
+    g2 = gx * gx + gz * gz
+    num = (gxx * (gz * gz) + gzz * (gx * gx)) - 2.0 * (gxz * gx * gz)
+    ok = (np.abs(phi) < (N_CUR + 1) * D.hf) & (g2 > 0.0)
     with np.errstate(divide="ignore", invalid="ignore"):
-        k = np.where((np.abs(phi) < 2.0 * D.h) & (g2 > 1e-12), num / (g2 * np.sqrt(g2)), 0.0)
-    kc = 0.25 * ((k[0::2, 0::2] + k[0::2, 1::2]) + (k[1::2, 0::2] + k[1::2, 1::2]))
-    return np.minimum(np.maximum(kc, -D.ih), D.ih)
+        return np.where(ok, -num / (g2 * np.sqrt(g2)), 0.0)
 
 
-def momentum_u(u, v, den, vis, D, psi=None, kap=None):
+def curvature_interface(phi, kt, D):
+    """CAL_CUR's CURF (two_phase.f:3405-3458) in 2-D: kappa at the foot of each band cell
+    (layers 1..N_CUR) on the interface, x_base = x - phi n, interpolated bilinearly from
+    CURF_TMP (the reference's trilinear form with YD = 0); 0 off those layers."""
+    nj, ni = phi.shape
+    E, W, N, S = _nbrs(phi)[:4]
+    dpx = 0.5 * (E - W) * D.ihf
+    dpz = 0.5 * (N - S) * D.ihf
+    g2 = dpx * dpx + dpz * dpz
+    ok = (np.abs(phi) < N_CUR * D.hf) & (g2 > 0.0)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        amdpi = 1.0 / np.sqrt(g2)
+    dis = phi * amdpi
+    I = np.arange(ni)[None, :]
+    J = np.arange(nj)[:, None]
+    xp = (I + 0.5) * D.hf
+    zp = (J + 0.5) * D.hf
+    xb = xp - dis * (dpx * amdpi)
+    zb = zp - dis * (dpz * amdpi)
+    hx, hz = xb >= xp, zb >= zp
+    xd = np.where(hx, (xb - xp) * D.ihf, (xb - (xp - D.hf)) * D.ihf)
+    zd = np.where(hz, (zb - zp) * D.ihf, (zb - (zp - D.hf)) * D.ihf)
+    Ie, Iw = (I + 1) % ni, (I - 1) % ni
+    Jn, Js = np.minimum(J + 1, nj - 1), np.maximum(J - 1, 0)
+    i1 = np.where(hx, I, Iw)
+    i2 = np.where(hx, Ie, I)
+    j1 = np.where(hz, J, Js)
+    j2 = np.where(hz, Jn, J)
+    with np.errstate(invalid="ignore"):
+        c00 = kt[j1, i1] * (1.0 - xd) + kt[j1, i2] * xd
+        c01 = kt[j2, i1] * (1.0 - xd) + kt[j2, i2] * xd
+        out = c00 * (1.0 - zd) + c01 * zd
+    return np.where(ok, out, 0.0)
+
+
+def _box(val, cnt, rows, cols):
+    """INTER_CUR's sums over the refined cells rows x cols (lists of index arrays), column by
+    column and row by row within a column, as the reference's II / KK loops run."""
+    s = np.zeros(val[rows[0], cols[0]].shape)
+    v = np.zeros_like(s)
+    for c in cols:
+        for r in rows:
+            s = s + val[r, c]
+            v = v + cnt[r, c]
+    return s, v
+
+
+def face_curvature(phi, cf, psi, D):
+    """CAL_CUR's face loops with CAL_CUR_INTEGRAL / INTER_CUR (two_phase.f:3547-3590,
+    3654-4432) in 2-D: on every face where psi jumps, the mean of CURF over the refined cells
+    of the face's box (centre to centre across the face, face to face along it) that are cut
+    by the interface (0 < psi_f < 1, CURF /= 0); if none is, the box twice as wide across the
+    face; 0 where psi does not jump.  On the uniform 2x refinement the boxes are whole refined
+    cells, so every weight is 1.  Returns (cx on the u faces (ny, nx), cy on the v faces
+    below each row (ny, nx), row 0 the wall: 0)."""
+    ny, nx = psi.shape
+    nxf = 2 * nx
+    H = heaviside(phi, D)
+    cnt = ((H > 0.0) & (H < 1.0) & (cf != 0.0)).astype(np.float64)
+    val = np.where(cnt > 0.0, cf, 0.0)
+    i = np.arange(nx)[None, :]
+    j = np.arange(ny)[:, None]
+    # u faces: x box refined columns 2i-1..2i (fallback 2i-2..2i+1), rows 2j..2j+1
+    rows = [2 * j, 2 * j + 1]
+    s, v = _box(val, cnt, rows, [(2 * i - 1) % nxf, (2 * i) % nxf])
+    s2, v2 = _box(val, cnt, rows, [(2 * i + q) % nxf for q in (-2, -1, 0, 1)])
+    with np.errstate(divide="ignore", invalid="ignore"):
+        cur = np.where(v != 0.0, s / v, np.where(v2 != 0.0, s2 / v2, 0.0))
+    cx = np.where((psi - _w(psi)) != 0.0, cur, 0.0)
+    # v faces j = 1..ny-1: columns 2i..2i+1, rows 2j-1..2j (fallback 2j-2..2j+1)
+    jj = np.maximum(j, 1)
+    cols = [2 * i, 2 * i + 1]
+    s, v = _box(val, cnt, [2 * jj - 1, 2 * jj], cols)
+    s2, v2 = _box(val, cnt, [2 * jj + q for q in (-2, -1, 0, 1)], cols)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        cur = np.where(v != 0.0, s / v, np.where(v2 != 0.0, s2 / v2, 0.0))
+    cy = np.where((j >= 1) & ((psi - _rows_s(psi, psi[0])) != 0.0), cur, 0.0)
+    return cx, cy
+
+
+def curvature(phi, psi, D):
+    """CAL_CUR in 2-D: (cx, cy) face curvatures from the refined level set."""
+    kt = curvature_refined(phi, D)
+    cf = curvature_interface(phi, kt, D)
+    return face_curvature(phi, cf, psi, D)
+
+
+def momentum_u(u, v, den, vis, D, psi=None, cx=None):
     ih = D.ih
     ue, uw = _e(u), _w(u)
     un = _rows_n(u, u[-1])
@@ -269,14 +365,13 @@ def momentum_u(u, v, den, vis, D, psi=None, kap=None):
     tys = mus * ((u - us) * ih + (v[:-1] - vw[:-1]) * ih)
     rho = 0.5 * (_w(den) + den)
     visc = ((txe - txw) * ih + (tyn - tys) * ih) / rho
-    if kap is None:
+    if cx is None:
         return visc - conv
-    # surface tension -sigma kappa grad psi on the face (continuum surface force)
-    kf = 0.5 * (_w(kap) + kap)
-    return visc - conv - (D.surf * kf) * ((psi - _w(psi)) * ih) / rho
+    # surface tension SURF CUR dpsi/dx on the face (CAL_CUR's SUR_X, two_phase.f:3547-3556)
+    return visc - conv + (D.surf * cx) * ((psi - _w(psi)) * ih) / rho
 
 
-def momentum_v(u, v, den, vis, D, psi=None, kap=None):
+def momentum_v(u, v, den, vis, D, psi=None, cy=None):
     """Right-hand side on the faces j = 1..ny (returned as ny rows)."""
     ih = D.ih
     vc = v[1:]
@@ -302,11 +397,12 @@ def momentum_v(u, v, den, vis, D, psi=None, kap=None):
     dhi = _rows_n(den, den[-1])
     rho = 0.5 * (dlo + dhi)
     visc = ((txe - txw) * ih + (tyn - tys) * ih) / rho
-    if kap is None:
+    if cy is None:
         return visc - conv + D.gravity * (D.denp / rho - 1.0)
-    kf = 0.5 * (kap + _rows_n(kap, kap[-1]))
+    # the face above row j carries cy of row j + 1 (top face: no jump, 0)
+    cf = _rows_n(cy, 0.0)
     pshi = _rows_n(psi, psi[-1])
-    return visc - conv + D.gravity * (D.denp / rho - 1.0) - (D.surf * kf) * ((pshi - psi) * ih) / rho
+    return visc - conv + D.gravity * (D.denp / rho - 1.0) + (D.surf * cf) * ((pshi - psi) * ih) / rho
 
 
 def energy_rhs(th, u, v, densc, tc, D):
@@ -474,9 +570,9 @@ def step(state, dt, props, mg_solve, mg_levels=6):
         iadt = 1.0 / (alpha * dt)
         psi, den, vis, densc, tc, bx, by = properties(phi, D)
         S, md = mass_source(th, psi, tc, D)
-        kap = curvature(phi, D)
-        nu = momentum_u(u, v, den, vis, D, psi, kap)
-        nv = momentum_v(u, v, den, vis, D, psi, kap)
+        cx, cy = curvature(phi, psi, D)
+        nu = momentum_u(u, v, den, vis, D, psi, cx)
+        nv = momentum_v(u, v, den, vis, D, psi, cy)
         # predictor with the current pressure gradient (p = 0 on the top face)
         us = u + dt * (gam * nu + ro * ru) - adt * (bx * ((p - _w(p)) * D.ih))
         vs = np.zeros_like(v)

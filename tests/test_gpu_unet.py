@@ -180,11 +180,12 @@ def test_learned_guess_on_film_systems_falls_back_and_costs_no_iterations():
         it0, _, st0 = s.solve(p, sy["f"], sy["bx"], sy["by"], rtol=1e-10, max_iters=200)
         g, rg = ev.guess_checked(sy["rho"][None].contiguous(), sy["f"][None].contiguous(), sy["bx"][None].contiguous(),
                                  sy["by"][None].contiguous(), 1.0 / nx, 1.0 / nx)
-        p = g[0].contiguous()
+        fell_back = torch.count_nonzero(g).item() == 0
+        assert fell_back == bool(rg[0] >= 1.0)             # zero exactly when no better than zero
+        p = g[0].clone()                                   # the solve overwrites its start
         itg, relg, stg = s.solve(p, sy["f"], sy["bx"], sy["by"], rtol=1e-10, max_iters=200)
         assert st0 == 0 and stg == 0 and relg <= 1e-10
-        if rg[0] >= 1.0:
-            assert torch.count_nonzero(g).item() == 0      # the fallback: zero
+        if fell_back:
             assert itg == it0
         else:
             assert itg <= it0

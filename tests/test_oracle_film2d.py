@@ -113,23 +113,33 @@ def test_product_inputs_match_the_restatement():
 
 
 def test_curvature_of_a_circle():
-    """kappa = div(grad phi / |grad phi|) of phi = r - R is 1/r near the circle."""
+    """CAL_CUR in 2-D on phi = r - R (vapour inside): CURF_TMP = -div(grad phi / |grad phi|) =
+    -1/r on the band and 0 beyond it; CURF at the interface foot is -1/R within 2%;
+    the face curvatures are -1/R on every face where psi jumps and 0 elsewhere."""
     nx, ny = 64, 64
     D = F.Derived(nx, ny, F.default_props())
     hf = D.hf
     xf = (np.arange(2 * nx) + 0.5) * hf
     yf = (np.arange(2 * ny) + 0.5) * hf
     R = 0.25
-    phi = np.sqrt((xf[None, :] - 0.5) ** 2 + (yf[:, None] - 0.5) ** 2) - R
-    kap = F.curvature(phi, D)
+    r = np.sqrt((xf[None, :] - 0.5) ** 2 + (yf[:, None] - 0.5) ** 2)
+    phi = r - R
+    kt = F.curvature_refined(phi, D)
+    band = np.abs(phi) < 5 * hf
+    assert np.abs(kt[band] * r[band] + 1.0).max() < 1e-3
+    assert np.all(kt[~band] == 0.0)
+    cf = F.curvature_interface(phi, kt, D)
+    near = np.abs(phi) < 4 * hf
+    assert np.abs(cf[near] * R + 1.0).max() < 0.02
+    assert np.all(cf[~near] == 0.0)
     psi = F.properties(phi, D)[0]
-    band = (psi > 0.05) & (psi < 0.95)
-    assert band.sum() > 50
-    assert np.abs(kap[band] * R - 1.0).max() < 0.1
-    # zero beyond the curvature band (|phi| < 2 h on the refined centres)
-    xc = (np.arange(nx) + 0.5) * D.h
-    dist = np.abs(np.sqrt((xc[None, :] - 0.5) ** 2 + (xc[:, None] - 0.5) ** 2) - R)
-    assert np.abs(kap[dist > 3 * D.h]).max() == 0.0
+    cx, cy = F.curvature(phi, psi, D)
+    jx = (psi - np.roll(psi, 1, axis=1)) != 0.0
+    jy = np.zeros_like(jx)
+    jy[1:] = (psi[1:] - psi[:-1]) != 0.0
+    assert jx.sum() > 50 and jy.sum() > 50
+    assert np.abs(cx[jx] * R + 1.0).max() < 0.005 and np.abs(cy[jy] * R + 1.0).max() < 0.005
+    assert np.all(cx[~jx] == 0.0) and np.all(cy[~jy] == 0.0)
 
 
 def test_cpp_restatement_is_bit_identical_to_numpy():
