@@ -21,6 +21,10 @@
 //     and p.Ap; k_xupdate: x += alpha p and the true residual f - A x with its norm).
 //     Grid-wide sums use a deterministic last-block reduction, which also computes the
 //     CG scalars on the device, so the host never reads a scalar inside an iteration.
+//   * Optional (LICA_MG_CROSS_LEVEL=1 at create): the grid levels between level 0 and the
+//     single-CTA levels run as one cooperative launch per V-cycle leg (k_down_mid,
+//     k_up_mid) with grid barriers between levels; bit-identical, but slower on a B200 than
+//     one graph node per level, so it is off by default.
 //   * With use_graph the whole solve is one CUDA graph: set-up kernels followed by a
 //     conditional WHILE node whose body is one PCG iteration; the last block of
 //     k_xupdate sets the loop condition.
@@ -33,6 +37,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -67,6 +72,7 @@ struct State {
     int back;       // 1: stalled, the answer is the iterate before the last one (it was decremented)
     int kerr;       // 1: a bounded wait inside a kernel ran out (the solve ends with LICA_ERR_CUDA)
     unsigned cnt[4];
+    unsigned bar_count, bar_gen;  // grid barrier of the cross-level kernels
 };
 
 // ------------------------------------------------------------------------------------
@@ -164,7 +170,9 @@ struct RBGeom {
 };
 
 // Loads f, 1/d and the four weights of the thread's cells (zero outside the domain rows).
-template <typename T, class C>
+// COH: f was written earlier in the same launch (the cross-level kernels), so it is read
+// through L2 (ld.global.cg), never through the non-coherent read-only path.
+template <typename T, class C, bool COH = false>
 __device__ __forceinline__ void rb_load(RBCells<T, C::K>& cl, const RBGeom<C>& g, const T* __restrict__ f,
                                         const T* __restrict__ ax, const T* __restrict__ ay,
                                         const T* __restrict__ dinv, int nx, int ny, int gi0, int gj0) {
@@ -181,7 +189,7 @@ __device__ __forceinline__ void rb_load(RBCells<T, C::K>& cl, const RBGeom<C>& g
             T vf = T(0), vd = T(0), vw = T(0), ve = T(0), vs = T(0), vn = T(0);
             if (ok) {
                 const int o = j * nx;
-                vf = f[o + i];
+                vf = COH ? __ldcg(f + o + i) : f[o + i];
                 vd = dinv[o + i];
                 vw = ax[o + i];
                 ve = ax[o + ip];
@@ -415,6 +423,131 @@ __global__ void __launch_bounds__(RBCfg<NSW, TXX, TYY, R>::NTH, 2)
             st->beta = (st->it == 0) ? 0.0 : tot / st->rz;
             st->rz = tot;
         }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Cross-level kernels: the grid levels below level 0 (1 .. lcta-1) of one V-cycle leg in one
+// cooperative launch.  k_down_mid runs k_down's tile work level after level and k_up_mid
+// k_up's (LEVEL0 = false) from the coarsest grid level up to level 1, each block looping
+// over the tiles of a level, with a grid barrier between levels in place of a kernel
+// boundary.  Arrays written earlier in the launch (a level's restricted residual, the
+// coarser level's correction) are read through L2.  Same arithmetic as the per-level
+// kernels, so the results are identical.
+// ------------------------------------------------------------------------------------
+constexpr int RB_TILE_R = 4;  // rows per thread strip of the smoothing tiles
+
+struct MidLevel {
+    int nx, ny, big;  // big: 32 x 32 tiles (else 16 x 16)
+    const void *f, *ax, *ay, *di, *upre, *uc;
+    void *u, *fc, *up;
+};
+
+struct MidParams {
+    int l0, l1;  // levels l0 .. l1-1
+    State* st;
+    MidLevel lv[kMaxLevels];
+};
+
+constexpr unsigned kBarSpin = 1u << 21;  // bounded wait of a grid barrier (about 0.3 s)
+
+// Grid barrier over all blocks of a cooperative launch; a wait that runs out sets st->kerr
+// and lets the block go on (the solve then reports LICA_ERR_CUDA).
+__device__ __forceinline__ void grid_barrier(State* __restrict__ st) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vgen = &st->bar_gen;
+        const unsigned g0 = *vgen;
+        __threadfence();
+        const unsigned nb = gridDim.x * gridDim.y;
+        if (atomicAdd(&st->bar_count, 1u) == nb - 1u) {
+            atomicExch(&st->bar_count, 0u);
+            __threadfence();
+            atomicAdd(&st->bar_gen, 1u);
+        } else {
+            unsigned it = 0;
+            while (*vgen == g0) {
+                if (++it > kBarSpin) {
+                    atomicExch(&st->kerr, 1);
+                    break;
+                }
+                __nanosleep(100);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+template <typename T, int NSW, int TS>
+__device__ __forceinline__ void mid_down_level(const MidLevel& L, T* __restrict__ su) {
+    using C = RBCfg<NSW, TS, TS, RB_TILE_R>;
+    const int ntx = L.nx / TS, nt = ntx * (L.ny / TS);
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int bi = t % ntx, bj = t / ntx;
+        const RBGeom<C> g;
+        RBCells<T, C::K> cl;
+        for (int k = threadIdx.x; k < C::WORDS; k += blockDim.x) su[k] = T(0);
+        rb_load<T, C, true>(cl, g, (const T*)L.f, (const T*)L.ax, (const T*)L.ay, (const T*)L.di, L.nx, L.ny,
+                            bi * TS - C::H, bj * TS - C::H);
+        __syncthreads();
+        down_body<T, NSW, TS, TS, RB_TILE_R>(cl, g, su, (T*)L.u, (T*)L.fc, L.nx, bi * TS, bj * TS);
+        __syncthreads();  // su is reused by the next tile
+    }
+}
+
+template <typename T, int NSW, int TS>
+__device__ __forceinline__ void mid_up_level(const MidLevel& L, T* __restrict__ su) {
+    using C = RBCfg<NSW, TS, TS, RB_TILE_R>;
+    const int ntx = L.nx / TS, nt = ntx * (L.ny / TS), nx = L.nx, ncx = L.nx >> 1;
+    const T* upre = (const T*)L.upre;
+    const T* uc = (const T*)L.uc;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int bi = t % ntx, bj = t / ntx;
+        const int gi0 = bi * TS - C::H, gj0 = bj * TS - C::H;
+        const RBGeom<C> g;
+        RBCells<T, C::K> cl;
+        for (int k = threadIdx.x; k < C::WORDS; k += blockDim.x) su[k] = T(0);
+        rb_load<T, C>(cl, g, (const T*)L.f, (const T*)L.ax, (const T*)L.ay, (const T*)L.di, L.nx, L.ny, gi0, gj0);
+        T uv[2][C::K];
+        int i = gi0 + g.x;
+        if (i < 0) i += nx; else if (i >= nx) i -= nx;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+#pragma unroll
+            for (int k = 0; k < C::K; ++k) {
+                T v = T(0);
+                if (cl.valid & (1u << (c * C::K + k))) {
+                    const int j = gj0 + g.row(c, k);
+                    v = upre[j * nx + i];
+                    v += __ldcg(uc + (j >> 1) * ncx + (i >> 1));
+                }
+                uv[c][k] = v;
+            }
+        }
+        __syncthreads();  // zero fill done
+        up_body<T, NSW, TS, TS, RB_TILE_R, false>(cl, g, uv, su, (T*)L.up, L.nx, bi * TS, bj * TS);
+        __syncthreads();
+    }
+}
+
+template <typename T, int NSW>
+__global__ void __launch_bounds__(RBCfg<NSW, 32, 32, RB_TILE_R>::NTH, 2) k_down_mid(const __grid_constant__ MidParams P) {
+    __shared__ __align__(16) T su[RBCfg<NSW, 32, 32, RB_TILE_R>::WORDS];
+    for (int l = P.l0; l < P.l1; ++l) {
+        if (P.lv[l].big) mid_down_level<T, NSW, 32>(P.lv[l], su);
+        else mid_down_level<T, NSW, 16>(P.lv[l], su);
+        if (l + 1 < P.l1) grid_barrier(P.st);
+    }
+}
+
+template <typename T, int NSW>
+__global__ void __launch_bounds__(RBCfg<NSW, 32, 32, RB_TILE_R>::NTH, 2) k_up_mid(const __grid_constant__ MidParams P) {
+    __shared__ __align__(16) T su[RBCfg<NSW, 32, 32, RB_TILE_R>::WORDS];
+    for (int l = P.l1 - 1; l >= P.l0; --l) {
+        if (P.lv[l].big) mid_up_level<T, NSW, 32>(P.lv[l], su);
+        else mid_up_level<T, NSW, 16>(P.lv[l], su);
+        if (l > P.l0) grid_barrier(P.st);
     }
 }
 
@@ -1202,6 +1335,8 @@ __global__ void k_init_state(State* st, double tol, int max_it) {
     st->kerr = 0;
     st->sums[0] = st->sums[1] = 0.0;
     for (int k = 0; k < 4; ++k) st->cnt[k] = 0u;
+    st->bar_count = 0u;
+    st->bar_gen = 0u;
 }
 
 __global__ void k_zero(double* __restrict__ a, size_t n) {
@@ -1250,6 +1385,7 @@ struct lica_mg {
     double hx, hy;
     lica_mg_options o;
     int nouter = 0, lcta = 0, bottom = 0;
+    bool mid = false;  // levels 1 .. lcta-1 (two or more) run as the cross-level kernels
     std::vector<LevelBuf> lv;  // outer levels then inner levels
     size_t cta_smem = 0;
     CtaParams cp{};
@@ -1388,7 +1524,7 @@ const T* lvl_di(const LevelBuf& L) {
 // Smoothing tiles: 32 x 32 cells on levels with at least one tile per SM, 16 x 16 below
 // (more CTAs in flight where the level is small and each tile's latency is the cost);
 // strips of 4 rows per thread.
-constexpr int RB_R = 4;
+constexpr int RB_R = RB_TILE_R;
 constexpr int kSMs = 148;
 bool big_tiles(const LevelBuf& L) { return L.nx % 32 == 0 && L.ny % 32 == 0 && (L.nx / 32) * (L.ny / 32) >= kSMs; }
 
@@ -1457,6 +1593,74 @@ int launch_up(lica_mg* m, int l, cudaStream_t s) {
     return LICA_OK;
 }
 
+// The cross-level kernels for levels 1 .. lcta-1 (two or more of them), one cooperative
+// launch per leg; the grid is at most what the device holds at once, so the blocks meet at
+// every barrier.
+template <typename T>
+MidParams mid_params(lica_mg* m) {
+    MidParams P{};
+    P.l0 = 1;
+    P.l1 = m->lcta;
+    P.st = m->st;
+    for (int l = 1; l < m->lcta; ++l) {
+        const LevelBuf& L = m->lv[l];
+        const LevelBuf& C = m->lv[l + 1];
+        MidLevel& M = P.lv[l];
+        M.nx = L.nx;
+        M.ny = L.ny;
+        M.big = big_tiles(L) ? 1 : 0;
+        M.f = L.f;
+        M.ax = lvl_ax<T>(L);
+        M.ay = lvl_ay<T>(L);
+        M.di = lvl_di<T>(L);
+        M.u = L.u;
+        M.fc = C.f;
+        M.upre = L.u;
+        M.uc = (l + 1 == m->lcta) ? C.u : C.up;
+        M.up = L.up;
+    }
+    return P;
+}
+
+template <typename T, int NS>
+int launch_mid_ns(lica_mg* m, bool up, cudaStream_t s) {
+    const MidParams P = mid_params<T>(m);
+    int tiles = 0;
+    for (int l = P.l0; l < P.l1; ++l) {
+        const int ts = P.lv[l].big ? 32 : 16;
+        tiles = std::max(tiles, (P.lv[l].nx / ts) * (P.lv[l].ny / ts));
+    }
+    auto kern = up ? k_up_mid<T, NS> : k_down_mid<T, NS>;
+    const int nth = RBCfg<NS, 32, 32, RB_R>::NTH;
+    int occ = 0;
+    LICA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, nth, 0));
+    if (occ < 1) return LICA_ERR_CUDA;
+    const int grid = std::min(tiles, occ * m->nsm);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(nth);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    LICA_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, P));
+    lica_count_launches(1);
+    return LICA_OK;
+}
+
+template <typename T>
+int launch_mid(lica_mg* m, bool up, cudaStream_t s) {
+    ProfScope ps(m, up ? LICA_MG_UP : LICA_MG_DOWN, s);
+    switch (up ? m->o.nu2 : m->o.nu1) {
+        case 1: return launch_mid_ns<T, 1>(m, up, s);
+        case 2: return launch_mid_ns<T, 2>(m, up, s);
+        default: return launch_mid_ns<T, 3>(m, up, s);
+    }
+}
+
 template <typename T>
 int launch_cta(lica_mg* m, cudaStream_t s) {
     CtaParams P = m->cp;
@@ -1473,6 +1677,12 @@ int launch_cta(lica_mg* m, cudaStream_t s) {
 template <typename T>
 int vcycle(lica_mg* m, cudaStream_t s) {
     int st;
+    if (m->mid) {
+        if ((st = launch_down<T>(m, 0, s)) || (st = launch_mid<T>(m, false, s)) || (st = launch_cta<T>(m, s)) ||
+            (st = launch_mid<T>(m, true, s)) || (st = launch_up<T>(m, 0, s)))
+            return st;
+        return LICA_OK;
+    }
     for (int l = 0; l < m->lcta; ++l)
         if ((st = launch_down<T>(m, l, s))) return st;
     if ((st = launch_cta<T>(m, s))) return st;
@@ -1885,6 +2095,12 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
         if (m->lv[l].nx % 16 || m->lv[l].ny % 16) { delete m; return LICA_BAD_ARG; }
     }
     m->lcta = lcta;
+    {
+        // the cross-level kernels where two or more grid levels lie between level 0 and the
+        // single-CTA levels (LICA_MG_CROSS_LEVEL=0 keeps one launch per level)
+        const char* ev = std::getenv("LICA_MG_CROSS_LEVEL");
+        m->mid = lcta >= 3 && ev && ev[0] == '1';
+    }
     // shared-memory layout of the single-CTA kernel
     CtaParams& P = m->cp;
     std::memset(&P, 0, sizeof(P));
