@@ -242,6 +242,21 @@ def profile_batch(ncol, steps, threads):
                       "cells": int(n.sum()), "status": int(st.max())}), flush=True)
 
 
+def column_roofline(state_bytes, ms_per_step, kernel):
+    """HBM roofline of the fused column step: its algorithmic traffic is the column state read
+    and written once per step (every other array lives in shared memory or in a scratch
+    that stays in L2), timed by CUDA events over the persistent launch."""
+    alg = 2 * state_bytes
+    achieved = alg / (ms_per_step / 1e3) / 1e9
+    peak, src = peaks()
+    return {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": src, "traffic": None,
+            "alg_bytes_per_step": alg,
+            "note": "latency-bound, not bandwidth-bound: one CTA per column walks the step's phases in order "
+                    "(three Thomas sweeps per substep on one thread, band lists, the TEMP_EXTP iterations); "
+                    "the per-phase cycle profile is the lica_gpu_column_profile_device record"}
+
+
 def rk3_legs(dev, flush, steps_c1=C1["steps"], steps_c4=1000, warmup=3, rank=0, world=1, slowest=lambda x: x,
              film_steps=10, film_compare=False):
     import torch
@@ -291,6 +306,7 @@ def rk3_legs(dev, flush, steps_c1=C1["steps"], steps_c4=1000, warmup=3, rank=0, 
         hcol.steps(1, props)
     e2e_s = time.perf_counter() - t0
     bytes_state = sum(a.nbytes for a in pinned.values())
+    out["column_512"]["roofline"] = column_roofline(bytes_state, ms / steps_c1, "k_column_steps<256>")
     out["column_512"]["e2e"] = {"steps_per_s": ke / e2e_s, "h2d_bytes_per_step": bytes_state,
                                 "d2h_bytes_per_step": bytes_state,
                                 "path": "lica_gpu_column_steps (C ABI), host arrays, one step per call"}
@@ -319,7 +335,9 @@ def rk3_legs(dev, flush, steps_c1=C1["steps"], steps_c4=1000, warmup=3, rank=0, 
     fin = batch.to(None).arrays
     hist = shard.gather_histories([(lo + c, float(fin["stats"][c][5]), float(fin["scal"][c][4]))
                                    for c in range(len(n))], world)
+    batch_bytes = sum(int(a.numel()) * a.element_size() for a in batch.arrays.values())
     out["batch_4096"] = {
+        "roofline": column_roofline(batch_bytes, ms / steps_c4, f"k_column_steps<{th}>"),
         "workload": f"config 4: {C4_NCOL} independent 1-D boiling columns, uneven 128-2048 flow cells (seeded, "
                     f"{cells} in total), superheat 2-20 K, density ratio 100-1600, FP64 (the 1-D pressure solve is "
                     f"the exact Thomas sweep), {steps_c4} RK3 steps in one persistent launch per rank, longest first",

@@ -32,6 +32,7 @@ module lica_gpu
     integer(c_int32_t) :: ncoarse
     integer(c_int32_t) :: precision
     integer(c_int32_t) :: use_graph
+    integer(c_int32_t) :: smoother
   end type lica_mg_options
 
   type, bind(c) :: lica_mg_result

@@ -122,6 +122,11 @@ typedef struct {
     int32_t precision; /* 0: FP64 throughout; 1: mixed -- FP32 smoothing, restriction and
                           prolongation; FP64 residual, CG vectors and coarsest solve */
     int32_t use_graph; /* 1: the whole solve is one CUDA graph with a device-side loop */
+    int32_t smoother;  /* 0: red-black point Gauss-Seidel (temporal-blocked tiles, the
+                          single-CTA coarse kernel); 1: y-line zebra relaxation -- columns of
+                          one parity solved exactly along y (Thomas), for cells much finer
+                          in y than in x (stretched wall grids, lica_mg_stretched_system);
+                          FP64 only, every level as plain grid kernels */
 } lica_mg_options;
 
 typedef struct {

@@ -1344,6 +1344,134 @@ __global__ void k_zero(double* __restrict__ a, size_t n) {
         a[k] = 0.0;
 }
 
+// ------------------------------------------------------------------------------------
+// y-line zebra relaxation (lica_mg_options.smoother = 1, FP64): for strongly anisotropic
+// cells (wall-normal stretching), where point relaxation stops smoothing along x.  Every
+// level runs plain grid kernels in the oracle's order (oracle/mg2d.cpp, flag MG_YLINE):
+// columns of one parity are each solved exactly along y by the Thomas algorithm with the
+// x neighbours held, u(j-1) as - d u(j) + an u(j+1) = f - aw uw - ae ue (u = 0 past the
+// top face); the residual and its 2x2 restriction; piecewise-constant prolongation; the
+// bottom level by the dense elimination.  The pre-scaled weights AX, AY are the same
+// products the oracle forms, so a preconditioner application is bit-identical.
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_yline_half(double* __restrict__ u, const double* __restrict__ f,
+                                                    const double* __restrict__ ax, const double* __restrict__ ay,
+                                                    double* __restrict__ cp, double* __restrict__ dp, int nx, int ny,
+                                                    int parity) {
+    const int i = 2 * (int)(blockIdx.x * blockDim.x + threadIdx.x) + parity;
+    if (i >= nx) return;
+    const int ip = (i + 1 == nx) ? 0 : i + 1, im = (i == 0) ? nx - 1 : i - 1;
+    double prev_c = 0.0, prev_d = 0.0;
+    for (int j = 0; j < ny; ++j) {
+        const size_t k = (size_t)j * nx;
+        const double aw = ax[k + i], ae = ax[k + ip], as = ay[k + i], an = ay[k + nx + i];
+        double rhs = f[k + i];
+        rhs -= aw * u[k + im];
+        rhs -= ae * u[k + ip];
+        double d = aw;
+        d += ae;
+        d += as;
+        d += an;
+        const double diag = -d;
+        const double sup = (j < ny - 1) ? an : 0.0;
+        const double den = diag - as * prev_c;  // as = 0 on the bottom row
+        const double c = sup / den;
+        const double e = (rhs - as * prev_d) / den;
+        cp[k + i] = c;
+        dp[k + i] = e;
+        prev_c = c;
+        prev_d = e;
+    }
+    double x = prev_d;
+    u[(size_t)(ny - 1) * nx + i] = x;
+    for (int j = ny - 2; j >= 0; --j) {
+        const size_t k = (size_t)j * nx + i;
+        x = dp[k] - cp[k] * x;
+        u[k] = x;
+    }
+}
+
+// Residual r = f - (s - d u) of the four children of coarse cell (I, J) and their 2x2
+// average, fc = (r00 + r01) + (r10 + r11) times 1/4 in the oracle's order.
+__global__ void k_resid_restrict(const double* __restrict__ u, const double* __restrict__ f,
+                                 const double* __restrict__ ax, const double* __restrict__ ay, double* __restrict__ fc,
+                                 int nx, int ny) {
+    const int ncx = nx >> 1, ncy = ny >> 1;
+    const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
+    if (I >= ncx || J >= ncy) return;
+    double r[2][2];
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+            const int i = 2 * I + a, j = 2 * J + b;
+            const int ip = (i + 1 == nx) ? 0 : i + 1, im = (i == 0) ? nx - 1 : i - 1;
+            const size_t k = (size_t)j * nx;
+            const double aw = ax[k + i], ae = ax[k + ip], as = ay[k + i], an = ay[k + nx + i];
+            const double uw = u[k + im], ue = u[k + ip];
+            const double us = (j > 0) ? u[k - nx + i] : 0.0;
+            const double un = (j < ny - 1) ? u[k + nx + i] : 0.0;
+            double sm = aw * uw;
+            sm += ae * ue;
+            sm += as * us;
+            sm += an * un;
+            double d = aw;
+            d += ae;
+            d += as;
+            d += an;
+            r[b][a] = f[k + i] - (sm - d * u[k + i]);
+        }
+    }
+    fc[(size_t)J * ncx + I] = 0.25 * ((r[0][0] + r[0][1]) + (r[1][0] + r[1][1]));
+}
+
+// u += P uc, piecewise constant.
+__global__ void k_prolong_add(double* __restrict__ u, const double* __restrict__ uc, int nx, int ny) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= nx || j >= ny) return;
+    u[(size_t)j * nx + i] += uc[(size_t)(j >> 1) * (nx >> 1) + (i >> 1)];
+}
+
+// The bottom level's dense solve on row-major arrays (unknown row = j*nx + i): the
+// elimination factors of k_dense_factor applied to f in the oracle's order, then its back
+// substitution by thread 0 (the same arithmetic as s_dense).
+__global__ void __launch_bounds__(64) k_dense_solve(const double* __restrict__ lu, const double* __restrict__ f,
+                                                    double* __restrict__ u, int n) {
+    __shared__ double b[kMaxDense];
+    for (int k = threadIdx.x; k < n; k += blockDim.x) b[k] = f[k];
+    __syncthreads();
+    for (int k = 0; k + 1 < n; ++k) {
+        const double bk = b[k];
+        for (int i = k + 1 + threadIdx.x; i < n; i += blockDim.x) b[i] -= lu[i * n + k] * bk;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        for (int i = n - 1; i >= 0; --i) {
+            double sm = b[i];
+            for (int j = i + 1; j < n; ++j) sm -= lu[i * n + j] * b[j];
+            b[i] = sm / lu[i * n + i];
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < n; k += blockDim.x) u[k] = b[k];
+}
+
+// r.z of the level-0 preconditioner application and the CG beta (the part of k_up's
+// level-0 epilogue the y-line cycle needs).
+__global__ void __launch_bounds__(256) k_rz(const double* __restrict__ r, const double* __restrict__ z, size_t n,
+                                            State* __restrict__ st, double* __restrict__ partials) {
+    __shared__ double red[32];
+    double acc = 0.0;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        acc += r[k] * z[k];
+    const double b = block_sum(acc, red);
+    double tot;
+    if (grid_sum_last(b, partials, &st->cnt[0], &tot, red)) {
+        st->beta = (st->it == 0) ? 0.0 : tot / st->rz;
+        st->rz = tot;
+    }
+}
+
 // The oracle's mixed path takes r.z with the FP32 copy of r (the V-cycle input), so the
 // CG r.z partial of k_up<float,...,true> uses f (FP32) and z (FP32) -- the same values.
 
@@ -1386,6 +1514,8 @@ struct lica_mg {
     lica_mg_options o;
     int nouter = 0, lcta = 0, bottom = 0;
     bool mid = false;  // levels 1 .. lcta-1 (two or more) run as the cross-level kernels
+    bool yline = false;  // y-line zebra relaxation on every level (lica_mg_options.smoother = 1)
+    double *ycp = nullptr, *ydp = nullptr;  // the line solves' Thomas scratch (level-0 size)
     std::vector<LevelBuf> lv;  // outer levels then inner levels
     size_t cta_smem = 0;
     CtaParams cp{};
@@ -1691,7 +1821,101 @@ int vcycle(lica_mg* m, cudaStream_t s) {
     return LICA_OK;
 }
 
-int run_vcycle(lica_mg* m, cudaStream_t s) { return is_mixed(m) ? vcycle<float>(m, s) : vcycle<double>(m, s); }
+// The y-line V-cycle (FP64), z = M r on m->r / m->z; the oracle's vcycle_outer with
+// coarse_solve and vcycle_inner.
+int yl_smooth(lica_mg* m, int l, double* u, const double* f, int nsw, bool reverse, cudaStream_t s) {
+    const LevelBuf& L = m->lv[l];
+    const int cols = L.nx / 2;
+    for (int q = 0; q < nsw; ++q)
+        for (int c = 0; c < 2; ++c) {
+            const int parity = reverse ? 1 - c : c;
+            k_yline_half<<<(cols + 127) / 128, 128, 0, s>>>(u, f, L.ax64, L.ay64, m->ycp, m->ydp, L.nx, L.ny, parity);
+            LICA_CUDA_TRY(cudaGetLastError());
+            lica_count_launches(1);
+        }
+    return LICA_OK;
+}
+
+int yl_restrict(lica_mg* m, int l, const double* u, const double* f, cudaStream_t s) {
+    const LevelBuf& L = m->lv[l];
+    const dim3 blk(32, 8), grid((L.nx / 2 + 31) / 32, (L.ny / 2 + 7) / 8);
+    k_resid_restrict<<<grid, blk, 0, s>>>(u, f, L.ax64, L.ay64, (double*)m->lv[l + 1].f, L.nx, L.ny);
+    LICA_CUDA_TRY(cudaGetLastError());
+    LICA_CUDA_TRY(cudaMemsetAsync(m->lv[l + 1].u, 0, sizeof(double) * (size_t)m->lv[l + 1].nx * m->lv[l + 1].ny, s));
+    lica_count_launches(1);
+    return LICA_OK;
+}
+
+int yl_prolong(lica_mg* m, int l, double* u, cudaStream_t s) {
+    const LevelBuf& L = m->lv[l];
+    const dim3 blk(32, 8), grid((L.nx + 31) / 32, (L.ny + 7) / 8);
+    k_prolong_add<<<grid, blk, 0, s>>>(u, (const double*)m->lv[l + 1].u, L.nx, L.ny);
+    LICA_CUDA_TRY(cudaGetLastError());
+    lica_count_launches(1);
+    return LICA_OK;
+}
+
+int yl_dense(lica_mg* m, cudaStream_t s) {
+    const LevelBuf& B = m->lv[m->bottom];
+    k_dense_solve<<<1, 64, 0, s>>>(m->dense_lu, (const double*)B.f, (double*)B.u, B.nx * B.ny);
+    LICA_CUDA_TRY(cudaGetLastError());
+    lica_count_launches(1);
+    return LICA_OK;
+}
+
+int yl_inner(lica_mg* m, int l, cudaStream_t s) {
+    if (l == m->bottom) return yl_dense(m, s);
+    double* u = (double*)m->lv[l].u;
+    const double* f = (const double*)m->lv[l].f;
+    int st;
+    if ((st = yl_smooth(m, l, u, f, m->o.nu1, false, s)) || (st = yl_restrict(m, l, u, f, s)) ||
+        (st = yl_inner(m, l + 1, s)) || (st = yl_prolong(m, l, u, s)) || (st = yl_smooth(m, l, u, f, m->o.nu2, true, s)))
+        return st;
+    return LICA_OK;
+}
+
+int vcycle_yline(lica_mg* m, cudaStream_t s) {
+    const int lc = m->nouter - 1;
+    int st;
+    LICA_CUDA_TRY(cudaMemsetAsync(m->z, 0, sizeof(double) * (size_t)m->nx * m->ny, s));
+    {
+        ProfScope ps(m, LICA_MG_DOWN, s);
+        for (int l = 0; l < lc; ++l) {
+            double* u = l == 0 ? (double*)m->z : (double*)m->lv[l].u;
+            const double* f = l == 0 ? (const double*)m->r : (const double*)m->lv[l].f;
+            if ((st = yl_smooth(m, l, u, f, m->o.nu1, false, s)) || (st = yl_restrict(m, l, u, f, s))) return st;
+        }
+    }
+    {
+        ProfScope ps(m, LICA_MG_CTA, s);
+        if (lc == 0) return LICA_BAD_ARG;
+        if (lc == m->bottom) {
+            if ((st = yl_dense(m, s))) return st;
+        } else {
+            for (int c = 0; c < m->o.ncoarse; ++c)
+                if ((st = yl_inner(m, lc, s))) return st;
+        }
+    }
+    {
+        ProfScope ps(m, LICA_MG_UP, s);
+        for (int l = lc - 1; l >= 0; --l) {
+            double* u = l == 0 ? (double*)m->z : (double*)m->lv[l].u;
+            const double* f = l == 0 ? (const double*)m->r : (const double*)m->lv[l].f;
+            if ((st = yl_prolong(m, l, u, s)) || (st = yl_smooth(m, l, u, f, m->o.nu2, true, s))) return st;
+        }
+    }
+    const size_t n0 = (size_t)m->nx * m->ny;
+    const int nb = (int)std::min<size_t>(148, (n0 + 255) / 256);
+    k_rz<<<nb, 256, 0, s>>>((const double*)m->r, (const double*)m->z, n0, m->st, m->partials);
+    LICA_CUDA_TRY(cudaGetLastError());
+    lica_count_launches(1);
+    return LICA_OK;
+}
+
+int run_vcycle(lica_mg* m, cudaStream_t s) {
+    if (m->yline) return vcycle_yline(m, s);
+    return is_mixed(m) ? vcycle<float>(m, s) : vcycle<double>(m, s);
+}
 
 // Beta hierarchy for the caller's level-0 faces bx, by: FP64 faces coarsened level by
 // level, and every level's pre-scaled weights AX, AY; in the mixed path also the FP32
@@ -2020,7 +2244,8 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
     const lica_mg_options o = *opt;
     if (nx < TX || ny < TY || nx % TX || ny % TY || !(hx > 0) || !(hy > 0) || o.nlevels < 2 ||
         o.nlevels > 12 || o.nu1 < 1 || o.nu1 > 3 || o.nu2 < 1 || o.nu2 > 3 || o.ncoarse < 1 ||
-        (o.precision != 0 && o.precision != 1)) {
+        (o.precision != 0 && o.precision != 1) || (o.smoother != 0 && o.smoother != 1) ||
+        (o.smoother == 1 && o.precision != 0)) {
         lica_set_last_error("lica_mg_create", "unsupported sizes or options", __FILE__, __LINE__);
         return LICA_BAD_ARG;
     }
@@ -2099,7 +2324,8 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
         // the cross-level kernels where two or more grid levels lie between level 0 and the
         // single-CTA levels (LICA_MG_CROSS_LEVEL=0 keeps one launch per level)
         const char* ev = std::getenv("LICA_MG_CROSS_LEVEL");
-        m->mid = lcta >= 3 && ev && ev[0] == '1';
+        m->mid = lcta >= 3 && ev && ev[0] == '1' && o.smoother == 0;
+        m->yline = o.smoother == 1;
     }
     // shared-memory layout of the single-CTA kernel
     CtaParams& P = m->cp;
@@ -2137,10 +2363,14 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
     TRY_ALLOC(m->r, tsz * n0);
     TRY_ALLOC(m->zpre, tsz * n0);
     TRY_ALLOC(m->z, tsz * n0);
+    if (m->yline) {
+        TRY_ALLOC(m->ycp, sizeof(double) * n0);
+        TRY_ALLOC(m->ydp, sizeof(double) * n0);
+    }
     for (int l = 1; l <= m->bottom; ++l) {
         LevelBuf& L = m->lv[l];
         const size_t n = (size_t)L.nx * L.ny;
-        if (l <= lcta) {
+        if (l <= lcta || m->yline) {  // the y-line cycle keeps every level in global memory
             TRY_ALLOC(L.u, tsz * n);
             TRY_ALLOC(L.f, tsz * n);
         }
@@ -2291,6 +2521,8 @@ int lica_mg_destroy(lica_mg* m) {
     cudaFree(m->dense_lu);
     cudaFree(m->zpre);
     cudaFree(m->z);
+    cudaFree(m->ycp);
+    cudaFree(m->ydp);
     cudaFree(m->partials);
     cudaFree(m->st);
     if (m->st_host) cudaFreeHost(m->st_host);
@@ -2436,7 +2668,7 @@ int lica_mg_precond_device(lica_mg* m, double* z, const double* r, const double*
         lica_count_launches(1);
     } else {
         LICA_CUDA_TRY(cudaMemcpyAsync(m->r, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-        if ((st = vcycle<double>(m, s))) return st;
+        if ((st = run_vcycle(m, s))) return st;
         LICA_CUDA_TRY(cudaMemcpyAsync(z, m->z, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     }
     LICA_CUDA_TRY(cudaStreamSynchronize(s));

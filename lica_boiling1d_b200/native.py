@@ -14,7 +14,7 @@ _I64 = C.POINTER(C.c_int64)
 
 class MgOptions(C.Structure):
     _fields_ = [("nlevels", C.c_int32), ("nu1", C.c_int32), ("nu2", C.c_int32), ("ncoarse", C.c_int32),
-                ("precision", C.c_int32), ("use_graph", C.c_int32)]
+                ("precision", C.c_int32), ("use_graph", C.c_int32), ("smoother", C.c_int32)]
 
 
 class MgResult(C.Structure):

@@ -103,18 +103,22 @@ def stretched_system(yface, bx, by, f):
 
 
 PRECISION = {"fp64": 0, "mixed": 1}
+SMOOTHER = {"rb": 0, "yline": 1}   # red-black points; y-line zebra (stretched wall grids, FP64)
 
 
 class MultigridPoisson:
-    """PCG with a symmetric V(nu1,nu2) red-black multigrid preconditioner (C ABI lica_mg_*).
+    """PCG with a symmetric V(nu1,nu2) multigrid preconditioner (C ABI lica_mg_*), red-black
+    point smoothing or (smoother="yline") y-line zebra relaxation.
 
     Arrays: p, f of shape (ny, nx); bx (ny, nx) = beta on the face left of each cell
     (x periodic); by (ny+1, nx) = beta on the face below each row, row ny the top wall
     (p = 0 on that face), row 0 unused (Neumann bottom)."""
 
-    def __init__(self, nx, ny, hx, hy, *, nlevels=6, nu1=2, nu2=2, ncoarse=2, precision="fp64", use_graph=True):
+    def __init__(self, nx, ny, hx, hy, *, nlevels=6, nu1=2, nu2=2, ncoarse=2, precision="fp64", use_graph=True,
+                 smoother="rb"):
         self.nx, self.ny, self.hx, self.hy = nx, ny, hx, hy
-        self.options = native.MgOptions(nlevels, nu1, nu2, ncoarse, PRECISION[precision], int(use_graph))
+        self.options = native.MgOptions(nlevels, nu1, nu2, ncoarse, PRECISION[precision], int(use_graph),
+                                        SMOOTHER[smoother])
         h = C.c_void_p()
         native.check(native.lib().lica_mg_create(C.byref(h), nx, ny, hx, hy, C.byref(self.options)),
                      "lica_mg_create")
