@@ -1,6 +1,6 @@
 // Persistent, TMA-staged forms of the two PCG vector kernels on level 0 (k_cg_tma): the
 // same arithmetic as k_pupdate / k_xupdate, cell for cell, with the tiles streamed through a
-// two-stage shared-memory ring.  A CTA (one per SM, 512 threads) walks tiles t, t + grid,
+// CG_STAGES-deep shared-memory ring.  A CTA (one per SM, 512 threads) walks tiles t, t + grid,
 // ...; while it computes tile t the TMA copies of tile t + grid are in flight, so the
 // per-tile load latency of the one-tile-per-CTA kernels is hidden.
 //
@@ -32,6 +32,10 @@ constexpr int CG_X0 = 4;       // box column of tile column 0
 constexpr int CG_WW = 4;       // wrap strip width
 constexpr int CG_NT = 512;   // 32 rows x 16 column pairs of a tile
 constexpr int CG_RW = 34;      // ring array: columns -1 .. 32, rows -1 .. 32
+#ifndef LICA_CG_STAGES
+#define LICA_CG_STAGES 2
+#endif
+constexpr int CG_STAGES = LICA_CG_STAGES;   // tiles in flight + 1
 
 struct CgMaps {
     // by iteration parity: p_old / x read from [par], written to [par ^ 1]
@@ -76,7 +80,7 @@ struct CgLayout {
     using TB = typename std::conditional<XUP, double, TZ>::type;
     using S = CgStage<TB>;
     static constexpr int RING = S::al(CG_RW * CG_RW * 8);   // p_new / x_new on the tile and its ring
-    static constexpr int BYTES = 2 * S::BYTES + RING + 128;  // + room to align the base
+    static constexpr int BYTES = CG_STAGES * S::BYTES + RING + 128;  // + room to align the base
     // transaction bytes of one tile's copies (whole boxes, filled parts included)
     static constexpr uint32_t TX_MAIN =
         (uint32_t)(CG_BW * CG_BH * (3 * 8 + (int)sizeof(TB) + (XUP ? 8 : 0)));
@@ -122,37 +126,47 @@ __global__ void __launch_bounds__(CG_NT, 1) k_cg_tma(const __grid_constant__ CgA
     using S = typename Lay::S;
     extern __shared__ __align__(16) unsigned char cg_smem_raw[];
     unsigned char* sm = cg_smem_raw + ((128u - (tc::smem_u32(cg_smem_raw) & 127u)) & 127u);
-    unsigned char* stage[2] = {sm, sm + S::BYTES};
-    double* ring = reinterpret_cast<double*>(sm + 2 * S::BYTES);
-    __shared__ __align__(8) uint64_t bar[2];
+    double* ring = reinterpret_cast<double*>(sm + CG_STAGES * S::BYTES);
+    __shared__ __align__(8) uint64_t bar[CG_STAGES];
     __shared__ double red[32];
     const int ntiles = A.ntx * A.nty;
     const int par = A.st->it & 1;
     const double coef = XUP ? A.st->alpha : A.st->beta;
     if (threadIdx.x == 0) {
-        tc::mbar_init(&bar[0], 1);
-        tc::mbar_init(&bar[1], 1);
+        for (int q = 0; q < CG_STAGES; ++q) tc::mbar_init(&bar[q], 1);
         tc::fence_barrier_init();
     }
     __syncthreads();
-    if (threadIdx.x == 0 && (int)blockIdx.x < ntiles) cg_issue<TZ, XUP>(A, stage[0], &bar[0], blockIdx.x, par);
+    // the first CG_STAGES - 1 tiles in flight
+    if (threadIdx.x == 0)
+        for (int q = 0; q + 1 < CG_STAGES; ++q) {
+            const int t = (int)blockIdx.x + q * (int)gridDim.x;
+            if (t < ntiles) cg_issue<TZ, XUP>(A, sm + q * S::BYTES, &bar[q], t, par);
+        }
     double acc = 0.0;
     bool failed = false;
     int i = 0;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
-        const int s = i & 1;
-        // the next tile into the other stage (its last reader finished before the barrier
-        // that closed the previous iteration)
-        const bool next = tile + (int)gridDim.x < ntiles;
-        if (threadIdx.x == 0 && next) cg_issue<TZ, XUP>(A, stage[s ^ 1], &bar[s ^ 1], tile + gridDim.x, par);
-        const int ok = tc::mbar_wait(&bar[s], (uint32_t)((i >> 1) & 1)) ? 1 : 0;
+        const int s = i % CG_STAGES;
+        // tile i + CG_STAGES - 1 into the stage tile i - 1 used (its last reader finished
+        // before the barrier that closed the previous iteration)
+        {
+            const int t = tile + (CG_STAGES - 1) * (int)gridDim.x;
+            const int sn = (i + CG_STAGES - 1) % CG_STAGES;
+            if (threadIdx.x == 0 && t < ntiles) cg_issue<TZ, XUP>(A, sm + sn * S::BYTES, &bar[sn], t, par);
+        }
+        const int ok = tc::mbar_wait(&bar[s], (uint32_t)((i / CG_STAGES) & 1)) ? 1 : 0;
         if (!__syncthreads_and(ok)) {
-            // let the copies of the next tile land (bounded) before the CTA leaves
-            if (threadIdx.x == 0 && next) (void)tc::mbar_wait(&bar[s ^ 1], (uint32_t)(((i + 1) >> 1) & 1));
+            // let the copies still in flight land (bounded) before the CTA leaves
+            if (threadIdx.x == 0)
+                for (int q = 1; q < CG_STAGES; ++q) {
+                    const int t = tile + q * (int)gridDim.x;
+                    if (t < ntiles) (void)tc::mbar_wait(&bar[(i + q) % CG_STAGES], (uint32_t)(((i + q) / CG_STAGES) & 1));
+                }
             failed = true;
             break;
         }
-        unsigned char* sb = stage[s];
+        unsigned char* sb = sm + s * S::BYTES;
         const int tx = tile % A.ntx, ty = tile / A.ntx;
         // edge tiles: the wrapped column -1 (first tile column) or nx (last) into the boxes,
         // so that the passes below index the boxes alone
