@@ -10,9 +10,9 @@
 // columns at the far end of the row.  Rows off the domain are zero-filled by the TMA, as
 // the per-tile kernels' loads fill them.
 //
-// k_pupdate_tma: p_new = z + beta p_old on the tile and its ring, then p_new.(A p_new) on
-//   the tile; the last CTA sets alpha = rz / p.Ap.
-// k_xupdate_tma: x_new = x + alpha p on the tile and its ring, r = f - A x_new on the tile
+// k_pupdate_tma: p_new = z + beta p_old on the tile (and, as the stencil reads them, on its
+//   one-cell ring), then p_new.(A p_new) on the tile; the last CTA sets alpha = rz / p.Ap.
+// k_xupdate_tma: x_new = x + alpha p likewise, r = f - A x_new on the tile
 //   (stored as TR), ||r||^2; the last CTA runs xupdate_finish.
 // Every wait is bounded (tc::mbar_wait); one that runs out sets State::kerr.
 #pragma once
@@ -31,7 +31,6 @@ constexpr int CG_BH = 34;      // box height (rows gj0 .. gj0 + 33)
 constexpr int CG_X0 = 4;       // box column of tile column 0
 constexpr int CG_WW = 4;       // wrap strip width
 constexpr int CG_NT = 512;   // 32 rows x 16 column pairs of a tile
-constexpr int CG_RW = 34;      // ring array: columns -1 .. 32, rows -1 .. 32
 #ifndef LICA_CG_STAGES
 #define LICA_CG_STAGES 2
 #endif
@@ -54,7 +53,7 @@ struct CgArgs {
     int use_cond;
 };
 
-// One ring stage, boxes A, B, C, AX, AY and the wrap strips of A, B, AX.
+// One stage of the ring, boxes A, B, C, AX, AY and the wrap strips of A, B, AX.
 //   k_pupdate's: A = p_old, B = z (TB = the V-cycle's type), C unused.
 //   k_xupdate's: A = x, B = p (TB = double), C = f.
 template <typename TB>
@@ -79,8 +78,7 @@ template <typename TZ, bool XUP>
 struct CgLayout {
     using TB = typename std::conditional<XUP, double, TZ>::type;
     using S = CgStage<TB>;
-    static constexpr int RING = S::al(CG_RW * CG_RW * 8);   // p_new / x_new on the tile and its ring
-    static constexpr int BYTES = CG_STAGES * S::BYTES + RING + 128;  // + room to align the base
+    static constexpr int BYTES = CG_STAGES * S::BYTES + 128;  // + room to align the base
     // transaction bytes of one tile's copies (whole boxes, filled parts included)
     static constexpr uint32_t TX_MAIN =
         (uint32_t)(CG_BW * CG_BH * (3 * 8 + (int)sizeof(TB) + (XUP ? 8 : 0)));
@@ -126,7 +124,6 @@ __global__ void __launch_bounds__(CG_NT, 1) k_cg_tma(const __grid_constant__ CgA
     using S = typename Lay::S;
     extern __shared__ __align__(16) unsigned char cg_smem_raw[];
     unsigned char* sm = cg_smem_raw + ((128u - (tc::smem_u32(cg_smem_raw) & 127u)) & 127u);
-    double* ring = reinterpret_cast<double*>(sm + CG_STAGES * S::BYTES);
     __shared__ __align__(8) uint64_t bar[CG_STAGES];
     __shared__ double red[32];
     const int ntiles = A.ntx * A.nty;
@@ -187,41 +184,36 @@ __global__ void __launch_bounds__(CG_NT, 1) k_cg_tma(const __grid_constant__ CgA
             tc::fence_async_smem();
             __syncthreads();
         }
-        // the updated vector on the tile and its ring: box rows 0..33, columns 3..36
-        {
-            const double* av = reinterpret_cast<const double*>(sb + S::A);
-            const typename Lay::TB* bv = reinterpret_cast<const typename Lay::TB*>(sb + S::B);
-            for (int k = threadIdx.x; k < CG_RW * CG_RW; k += CG_NT) {
-                const int rr = k / CG_RW, rc = k - rr * CG_RW;
-                const int q = rr * CG_BW + rc + CG_X0 - 1;
-                double v;
-                if (XUP) v = av[q] + coef * double(bv[q]);
-                else v = double(bv[q]) + coef * av[q];
-                ring[k] = v;
-            }
-        }
-        __syncthreads();
         // the stencil on the tile: thread t owns cells 2 (t % 16) and 2 (t % 16) + 1 of row t / 16
         {
             const int ty_ = threadIdx.x >> 4, tx0 = (threadIdx.x & 15) * 2;
             const int br = ty_ + 1, bc = tx0 + CG_X0;
             const double* axb = reinterpret_cast<const double*>(sb + S::AX) + br * CG_BW + bc;
             const double* ayb = reinterpret_cast<const double*>(sb + S::AY) + br * CG_BW + bc;
-            const double* rg = ring + (ty_ + 1) * CG_RW + tx0 + 1;
             const size_t g = (size_t)(ty * CG_TS + ty_) * A.nx + tx * CG_TS + tx0;
+            // the updated vector (p_new or x_new) at a box cell, formed where the stencil reads
+            // it: each neighbour is recomputed rather than staged in a separate pass, which
+            // saves that pass and one CTA barrier per tile
+            const double* av = reinterpret_cast<const double*>(sb + S::A);
+            const typename Lay::TB* bv = reinterpret_cast<const typename Lay::TB*>(sb + S::B);
+            const int q0 = br * CG_BW + bc;
+            auto upd = [&](int e, int off) {   // off: 0 the cell, +-1 east / west, +-CG_BW north / south
+                const int q = q0 + e + off;
+                return XUP ? av[q] + coef * double(bv[q]) : double(bv[q]) + coef * av[q];
+            };
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
                 const double aw = axb[e], ae = axb[e + 1], as = ayb[e], an = ayb[e + CG_BW];
-                const double* c = rg + e;
-                double ss = aw * c[-1];
-                ss += ae * c[1];
-                ss += as * c[-CG_RW];
-                ss += an * c[CG_RW];
+                const double cw = upd(e, -1), ce = upd(e, 1), cs = upd(e, -CG_BW), cn = upd(e, CG_BW);
+                double ss = aw * cw;
+                ss += ae * ce;
+                ss += as * cs;
+                ss += an * cn;
                 double dd = aw;
                 dd += ae;
                 dd += as;
                 dd += an;
-                const double v = c[0];
+                const double v = upd(e, 0);
                 if (XUP) {
                     const double fv = reinterpret_cast<const double*>(sb + S::C)[br * CG_BW + bc + e];
                     const double r = fv - (ss - dd * v);
@@ -235,7 +227,7 @@ __global__ void __launch_bounds__(CG_NT, 1) k_cg_tma(const __grid_constant__ CgA
                 }
             }
         }
-        __syncthreads();   // the ring and this stage are free again
+        __syncthreads();   // this stage is free again
     }
     if (failed) {
         if (threadIdx.x == 0) atomicExch(&A.st->kerr, 1);
