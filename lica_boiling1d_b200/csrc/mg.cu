@@ -1537,6 +1537,8 @@ struct lica_mg {
     double* b_in[2] = {nullptr, nullptr};
     double* b_out[2] = {nullptr, nullptr};
     cudaStream_t b_up = nullptr, b_down = nullptr;
+    State* b_states = nullptr;  // pinned: each batched solve's final state
+    int b_states_cap = 0;
     cudaEvent_t b_ev_in[2] = {nullptr, nullptr}, b_ev_used[2] = {nullptr, nullptr};
     cudaEvent_t b_ev_solved[2] = {nullptr, nullptr}, b_ev_out[2] = {nullptr, nullptr};
     cudaStream_t cap_stream = nullptr;  // graphs are captured here, launched on the caller's stream
@@ -2194,21 +2196,29 @@ bool aligned16(const void* a, const void* b, const void* c, const void* d) {
     return true;
 }
 
+// Launch the solve's graph (built, or rebuilt for new arrays, tolerance or stream) on s.
+int graph_launch(lica_mg* m, double* x, const double* f, const double* bx, const double* by, double rtol, int max_it,
+                 cudaStream_t s) {
+    int st;
+    const bool same = m->gexec && m->gkey[0] == x && m->gkey[1] == f && m->gkey[2] == bx && m->gkey[3] == by &&
+                      m->gstream == s;
+    // rtol/max_it live in the graph's k_init_state node: rebuild when they change
+    if (!same || m->gtol != rtol || m->gmax != max_it) {
+        if ((st = build_graph(m, x, f, bx, by, rtol, max_it, s))) return st;
+        m->gtol = rtol;
+        m->gmax = max_it;
+    }
+    LICA_CUDA_TRY(cudaGraphLaunch(m->gexec, s));
+    return LICA_OK;
+}
+
 int solve_impl(lica_mg* m, double* x, const double* f, const double* bx, const double* by, double rtol, int max_it,
                lica_mg_result* res, cudaStream_t s) {
     if (!m || !x || !f || !bx || !by || !(rtol >= 0.0) || max_it < 0) return LICA_BAD_ARG;
     if (!aligned16(x, f, bx, by)) return LICA_BAD_ARG;
     int st;
     if (m->o.use_graph && !m->profile) {
-        const bool same = m->gexec && m->gkey[0] == x && m->gkey[1] == f && m->gkey[2] == bx && m->gkey[3] == by &&
-                          m->gstream == s;
-        // rtol/max_it live in the graph's k_init_state node: rebuild when they change
-        if (!same || m->gtol != rtol || m->gmax != max_it) {
-            if ((st = build_graph(m, x, f, bx, by, rtol, max_it, s))) return st;
-            m->gtol = rtol;
-            m->gmax = max_it;
-        }
-        LICA_CUDA_TRY(cudaGraphLaunch(m->gexec, s));
+        if ((st = graph_launch(m, x, f, bx, by, rtol, max_it, s))) return st;
         if ((st = read_state(m, s))) return st;
         lica_count_launches(m->setup_nodes + (int64_t)(m->st_host->it + m->st_host->back) * m->body_nodes);
     } else {
@@ -2526,6 +2536,7 @@ int lica_mg_destroy(lica_mg* m) {
     cudaFree(m->partials);
     cudaFree(m->st);
     if (m->st_host) cudaFreeHost(m->st_host);
+    if (m->b_states) cudaFreeHost(m->b_states);
     cudaFree(m->d_p);
     cudaFree(m->d_f);
     cudaFree(m->d_bx);
@@ -2602,6 +2613,17 @@ int lica_mg_solve_host_batch(lica_mg* m, int32_t count, double* const* p, const 
         }
     }
     cudaStream_t s = m->own_stream;
+    // With graphs the host never waits inside the loop: each solve's final state is copied to
+    // its own pinned slot and read after the last download.
+    const bool async = m->o.use_graph && !m->profile;
+    if (async && m->b_states_cap < count) {
+        if (m->b_states) cudaFreeHost(m->b_states);
+        m->b_states = nullptr;
+        m->b_states_cap = 0;
+        LICA_CUDA_TRY(cudaMallocHost((void**)&m->b_states, sizeof(State) * (size_t)count));
+        m->b_states_cap = count;
+    }
+    if (!(rtol >= 0.0) || max_iters < 0) return LICA_BAD_ARG;
     // upload of system k into input staging k % 2 once the solve of k - 2 has consumed it
     auto upload = [&](int32_t k) -> int {
         const int b = k & 1;
@@ -2627,9 +2649,14 @@ int lica_mg_solve_host_batch(lica_mg* m, int32_t count, double* const* p, const 
         LICA_CUDA_TRY(cudaMemcpyAsync(m->d_bx, in + 2 * n, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
         LICA_CUDA_TRY(cudaMemcpyAsync(m->d_by, in + 3 * n, sizeof(double) * nb, cudaMemcpyDeviceToDevice, s));
         LICA_CUDA_TRY(cudaEventRecord(m->b_ev_used[b], s));
-        st = solve_impl(m, m->d_p, m->d_f, m->d_bx, m->d_by, rtol, max_iters, &res[k], s);
-        if (st == LICA_ERR_CUDA || st == LICA_BAD_ARG) return st;
-        if (st != LICA_OK && worst == LICA_OK) worst = st;
+        if (async) {
+            if ((st = graph_launch(m, m->d_p, m->d_f, m->d_bx, m->d_by, rtol, max_iters, s))) return st;
+            LICA_CUDA_TRY(cudaMemcpyAsync(&m->b_states[k], m->st, sizeof(State), cudaMemcpyDeviceToHost, s));
+        } else {
+            st = solve_impl(m, m->d_p, m->d_f, m->d_bx, m->d_by, rtol, max_iters, &res[k], s);
+            if (st == LICA_ERR_CUDA || st == LICA_BAD_ARG) return st;
+            if (st != LICA_OK && worst == LICA_OK) worst = st;
+        }
         // the result leaves through output staging k % 2 (free once the download of k - 2 ended)
         LICA_CUDA_TRY(cudaStreamWaitEvent(s, m->b_ev_out[b], 0));
         LICA_CUDA_TRY(cudaMemcpyAsync(m->b_out[b], m->d_p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
@@ -2641,6 +2668,21 @@ int lica_mg_solve_host_batch(lica_mg* m, int32_t count, double* const* p, const 
     LICA_CUDA_TRY(cudaStreamSynchronize(m->b_down));
     LICA_CUDA_TRY(cudaStreamSynchronize(m->b_up));
     LICA_CUDA_TRY(cudaStreamSynchronize(s));
+    if (async) {
+        for (int32_t k = 0; k < count; ++k) {
+            const State& S = m->b_states[k];
+            if (S.kerr) {
+                lica_set_last_error("lica_mg_solve_host_batch", "a bounded wait inside a kernel ran out", __FILE__,
+                                    __LINE__);
+                return LICA_ERR_CUDA;
+            }
+            res[k].iterations = S.it;
+            res[k].status = S.status;
+            res[k].rel_residual = S.rel;
+            lica_count_launches(m->setup_nodes + (int64_t)(S.it + S.back) * m->body_nodes);
+            if (S.status != LICA_OK && worst == LICA_OK) worst = S.status;
+        }
+    }
     return worst;
 }
 
