@@ -317,13 +317,13 @@ def rk3_legs(dev, flush, steps_c1=C1["steps"], steps_c4=1000, warmup=3, rank=0, 
     n = n_all[lo:hi]
     batch = ColumnBatch.films(n, length[lo:hi], z0[lo:hi], bprops[lo:hi]).to(dev)
     from lica_boiling1d_b200 import autotune
-    th, trial = autotune.tune(batch, force=True)
-    batch.steps(warmup, threads=th)
+    (th, cap), trial = autotune.tune(batch, force=True)
+    batch.steps(warmup, threads=th, tri_cap=cap)
     torch.cuda.synchronize(dev)
     flush.fill_(5)
     l0 = native.launch_count()
     e0.record()
-    st = batch.steps(steps_c4, threads=th)
+    st = batch.steps(steps_c4, threads=th, tri_cap=cap)
     e1.record()
     torch.cuda.synchronize(dev)
     launches = native.launch_count() - l0
@@ -343,8 +343,9 @@ def rk3_legs(dev, flush, steps_c1=C1["steps"], steps_c4=1000, warmup=3, rank=0, 
                     f"the exact Thomas sweep), {steps_c4} RK3 steps in one persistent launch per rank, longest first",
         "steps_per_s": steps_c4 / (ms / 1e3), "ms_per_step": ms / steps_c4, "steps": steps_c4,
         "column_steps_per_s": C4_NCOL * steps_c4 / (ms / 1e3), "cell_updates_per_s": cells * steps_c4 / (ms / 1e3),
-        "threads": th, "autotune_ms_per_step": trial,
-        "autotune": "lica_boiling1d_b200.autotune: CTA width 64/128/256 timed on a copy of the batch, cached per GPU",
+        "threads": th, "tri_cap": cap, "autotune_ms_per_step": trial,
+        "autotune": "lica_boiling1d_b200.autotune: CTA width 64/128/256 x Thomas arrays in shared memory or "
+                    "scratch, timed on a copy of the batch, cached per GPU",
         "gpu_launches": launches,
         "ranks": world, "sharding": "contiguous column blocks balanced by cells, strong scaling of the fixed batch",
         "gathered_columns": len(hist)}

@@ -549,6 +549,19 @@ module lica_gpu
       type(c_ptr), value :: stream
     end function lica_gpu_column_batch_steps_device
 
+    integer(c_int) function lica_gpu_column_batch_steps_ex_device(batch, st, nsteps, threads, &
+        tri_cap, scratch, status, stream) bind(c, name="lica_gpu_column_batch_steps_ex_device")
+      import
+      type(c_ptr), value :: batch
+      type(lica_col_state), intent(in) :: st
+      integer(c_int32_t), value :: nsteps
+      integer(c_int32_t), value :: threads
+      integer(c_int32_t), value :: tri_cap
+      type(c_ptr), value :: scratch
+      type(c_ptr), value :: status
+      type(c_ptr), value :: stream
+    end function lica_gpu_column_batch_steps_ex_device
+
     integer(c_int) function lica_gpu_column_steps(ncol, n, length, props, st, nsteps, status) &
         bind(c, name="lica_gpu_column_steps")
       import

@@ -393,6 +393,12 @@ int lica_gpu_column_batch_destroy(lica_col_batch* batch);
 int lica_gpu_column_batch_layout(const lica_col_batch* batch, int64_t* offsets, int64_t* totals);
 int lica_gpu_column_batch_steps_device(const lica_col_batch* batch, const lica_col_state* st, int32_t nsteps,
                                        int32_t threads, void* scratch, int32_t* status, void* stream);
+/* The same with a limit on the column length whose Thomas arrays live in shared memory
+ * (tri_cap < 0: as large as the CTAs per SM allow, the default; 0: all in scratch; the arithmetic
+ * and results are the same either way) -- the launch autotuner's second axis. */
+int lica_gpu_column_batch_steps_ex_device(const lica_col_batch* batch, const lica_col_state* st, int32_t nsteps,
+                                          int32_t threads, int32_t tri_cap, void* scratch, int32_t* status,
+                                          void* stream);
 
 /* Same on host arrays (copies in, runs, copies out); returns the last non-OK column status. */
 int lica_gpu_column_steps(int32_t ncol, int32_t n, double length, const lica_col_props* props,

@@ -1,12 +1,14 @@
-"""Launch-shape autotuner of the batched column step (lica_gpu_column_batch_steps_device).
+"""Launch-shape autotuner of the batched column step (lica_gpu_column_batch_steps_ex_device).
 
-The step kernel runs one CTA per column, persistent over all the steps of a launch.  Its
-launch shape is the CTA width -- 64, 128 or 256 threads -- which also fixes how many
-columns share an SM (the 64-thread form is bounded for 5 CTAs per SM, the wider ones run
-one or two) and how long a column may be for its Thomas arrays to sit in shared memory
-(the kernel sizes that cap from the CTAs the registers allow per SM).  Which shape is
-fastest depends on the batch: many short columns favour narrow CTAs and more columns per
-SM, a few long ones wide CTAs that finish each column sooner.
+The step kernel runs one CTA per column, persistent over all the steps of a launch.  A
+launch shape has two axes:
+  * the CTA width -- 64, 128 or 256 threads -- which also fixes how many columns share an SM
+    (the 64-thread form is bounded for 5 CTAs per SM, the wider ones run one or two);
+  * the shared-memory cap of the Thomas arrays: as long a column as the CTAs per SM leave room
+    for (the default), or none (every column's arrays in the L2-resident scratch).  Results
+    are identical either way; the speed is not.
+Which shape is fastest depends on the batch: many short columns favour narrow CTAs and more
+columns per SM, a few long ones wide CTAs that finish each column sooner.
 
 ``tune(batch)`` times one warm-up step and ``trial_steps`` steps of each shape on a copy of
 the batch's device state (the batch itself does not advance), keeps the fastest, and
@@ -18,7 +20,21 @@ import json
 import os
 import threading
 
-SHAPES = (64, 128, 256)
+# (threads, tri_cap): tri_cap -1 = the largest the CTAs per SM allow, 0 = no shared arrays
+SHAPES = ((64, -1), (128, -1), (256, -1), (64, 0), (128, 0), (256, 0))
+
+
+def _name(shape):
+    return f"{shape[0]}/{'smem' if shape[1] < 0 else 'scratch'}"
+
+
+def _shape(entry):
+    """A cache entry's shape, or None if it is not one of SHAPES."""
+    try:
+        sh = (int(entry["threads"]), int(entry.get("tri_cap", -1)))
+    except (KeyError, TypeError, ValueError):
+        return None
+    return sh if sh in SHAPES else None
 _lock = threading.Lock()
 _memo = {}
 
@@ -63,8 +79,8 @@ def _store(entries):
 
 
 def tune(batch, trial_steps=2, force=False):
-    """The fastest CTA width for this batch on its GPU: (threads, {threads: ms per step} of
-    the trial, or None when the choice came from the cache)."""
+    """The fastest launch shape for this batch on its GPU: ((threads, tri_cap), {shape name:
+    ms per step} of the trial, or None when the choice came from the cache)."""
     import torch
     dev = batch.arrays["w"].device
     key = f"{_gpu_name(dev)}|{batch_key(batch)}"
@@ -73,25 +89,27 @@ def tune(batch, trial_steps=2, force=False):
             if key in _memo:
                 return _memo[key], None
             disk = _load()
-            if key in disk and int(disk[key]["threads"]) in SHAPES:
-                _memo[key] = int(disk[key]["threads"])
-                return _memo[key], None
+            sh = _shape(disk[key]) if key in disk else None
+            if sh is not None:
+                _memo[key] = sh
+                return sh, None
     times = {}
-    for th in SHAPES:
+    for th, cap in SHAPES:
         trial = batch.to(dev)
-        trial.steps(1, threads=th)
+        trial.steps(1, threads=th, tri_cap=cap)
         torch.cuda.synchronize(dev)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        trial.steps(trial_steps, threads=th)
+        trial.steps(trial_steps, threads=th, tri_cap=cap)
         b.record()
         torch.cuda.synchronize(dev)
-        times[th] = a.elapsed_time(b) / trial_steps
+        times[(th, cap)] = a.elapsed_time(b) / trial_steps
         del trial
     best = min(times, key=times.get)
+    named = {_name(k): v for k, v in times.items()}
     with _lock:
         _memo[key] = best
         disk = _load()
-        disk[key] = {"threads": best, "ms_per_step": {str(k): v for k, v in times.items()}}
+        disk[key] = {"threads": best[0], "tri_cap": best[1], "ms_per_step": named}
         _store(disk)
-    return best, times
+    return best, named

@@ -311,21 +311,22 @@ class ColumnBatch:
                 out[k] = torch.as_tensor(v if isinstance(v, np.ndarray) else v.cpu().numpy(), device=device).clone()
         return ColumnBatch(self.n, self.length, self.props, out, self._h)
 
-    def steps(self, nsteps, threads=0, stream=None, scratch=None):
+    def steps(self, nsteps, threads=0, stream=None, scratch=None, tri_cap=-1):
         """nsteps time steps of every column (device state).  threads: the CTA width (64,
-        128 or 256), or 0 for the autotuner's choice for this batch on this GPU (timed once
-        on a copy of the state, then cached; see autotune.py).  Returns the per-column
-        status."""
+        128 or 256), or 0 for the autotuner's launch shape for this batch on this GPU (timed
+        once on a copy of the state, then cached; see autotune.py); tri_cap: the longest
+        column whose Thomas arrays live in shared memory (-1: as the CTAs per SM allow, 0:
+        none).  Returns the per-column status."""
         import torch
         if threads == 0:
             from . import autotune
-            threads = autotune.tune(self)[0]
+            threads, tri_cap = autotune.tune(self)[0]
         dev = self.arrays["w"].device
         status = torch.zeros(self.ncol, dtype=torch.int32, device=dev)
         s = stream if stream is not None else torch.cuda.current_stream(dev)
         st = native.ColState(*[self.arrays[k].data_ptr() for k in native.COL_FIELDS])
-        native.check(native.lib().lica_gpu_column_batch_steps_device(
-            self._h.ptr, C.byref(st), int(nsteps), int(threads),
+        native.check(native.lib().lica_gpu_column_batch_steps_ex_device(
+            self._h.ptr, C.byref(st), int(nsteps), int(threads), int(tri_cap),
             C.c_void_p(scratch.data_ptr() if scratch is not None else None), C.c_void_p(status.data_ptr()),
             C.c_void_p(s.cuda_stream)), "column batch steps")
         return status

@@ -1762,7 +1762,7 @@ int column_ctas_by_registers() {
     return std::max(occ, 1);
 }
 
-int launch_columns(colk::Args& A, int nmax, int threads, void* stream) {
+int launch_columns(colk::Args& A, int nmax, int threads, void* stream, int cap_limit = -1) {
     const int nth = (threads == 64 || threads == 256) ? threads : colk::NT_DEFAULT;
     // Shared-memory tridiagonal arrays for columns up to tri_cap cells, sized so that the
     // CTAs the registers allow per SM still fit (longer columns keep them in scratch; the
@@ -1770,7 +1770,8 @@ int launch_columns(colk::Args& A, int nmax, int threads, void* stream) {
     const int ctas = nth == 64 ? column_ctas_by_registers<64>()
                                : (nth == 128 ? column_ctas_by_registers<128>() : column_ctas_by_registers<256>());
     const long budget = (long)(228 * 1024) / ctas - (long)sizeof(colk::Shared) - 2048;
-    const long cap = std::min<long>(nmax, budget / (5 * (long)sizeof(double)) - 2);
+    long cap = std::min<long>(nmax, budget / (5 * (long)sizeof(double)) - 2);
+    if (cap_limit >= 0) cap = std::min<long>(cap, cap_limit);   // a caller's (autotuner's) limit
     A.tri_cap = cap >= 64 ? (int)cap : 0;
     A.tri_smem = A.tri_cap > 0 ? 1 : 0;
     const size_t dyn = A.tri_smem ? 5 * ((size_t)A.tri_cap + 2) * sizeof(double) : 0;
@@ -2011,6 +2012,12 @@ int lica_gpu_column_batch_layout(const lica_col_batch* b, int64_t* offsets, int6
 
 int lica_gpu_column_batch_steps_device(const lica_col_batch* b, const lica_col_state* st, int32_t nsteps,
                                        int32_t threads, void* scratch, int32_t* status, void* stream) {
+    return lica_gpu_column_batch_steps_ex_device(b, st, nsteps, threads, -1, scratch, status, stream);
+}
+
+int lica_gpu_column_batch_steps_ex_device(const lica_col_batch* b, const lica_col_state* st, int32_t nsteps,
+                                          int32_t threads, int32_t tri_cap, void* scratch, int32_t* status,
+                                          void* stream) {
     if (!b || !state_ok(st) || nsteps < 0 || !status) return LICA_BAD_ARG;
     {
         // descriptors and launch order go to the device on first use (the host-side layout
@@ -2044,7 +2051,7 @@ int lica_gpu_column_batch_steps_device(const lica_col_batch* b, const lica_col_s
     }
     A.dscr = (double*)scr;
     A.iscr = (int*)((char*)scr + (size_t)b->tot[3] * sizeof(double));
-    return launch_columns(A, b->nmax, threads, stream);
+    return launch_columns(A, b->nmax, threads, stream, tri_cap);
 }
 
 }  // extern "C"

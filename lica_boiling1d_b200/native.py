@@ -126,6 +126,8 @@ SIGNATURES = {
     "lica_gpu_column_batch_layout": (C.c_int, [C.c_void_p, _I64, _I64]),
     "lica_gpu_column_batch_steps_device": (C.c_int, [C.c_void_p, C.POINTER(ColState), C.c_int32, C.c_int32,
                                                      C.c_void_p, C.c_void_p, C.c_void_p]),
+    "lica_gpu_column_batch_steps_ex_device": (C.c_int, [C.c_void_p, C.POINTER(ColState), C.c_int32, C.c_int32,
+                                                        C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "lica_gpu_column_steps": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.POINTER(ColProps), C.POINTER(ColState),
                                         C.c_int32, _I32]),
     "lica_gpu_column_init_geometry": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.POINTER(ColProps),

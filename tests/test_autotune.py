@@ -21,9 +21,11 @@ def test_batch_key_depends_on_the_shape_only():
 def test_cache_file_round_trip(tmp_path, monkeypatch):
     path = tmp_path / "tune.json"
     monkeypatch.setenv("LICA_TUNE_CACHE", str(path))
-    autotune._store({"GPU|ncol=1": {"threads": 64, "ms_per_step": {"64": 1.0}}})
+    autotune._store({"GPU|ncol=1": {"threads": 64, "tri_cap": 0, "ms_per_step": {"64/scratch": 1.0}}})
     assert json.loads(path.read_text())["GPU|ncol=1"]["threads"] == 64
-    assert autotune._load()["GPU|ncol=1"]["threads"] == 64
+    assert autotune._shape(autotune._load()["GPU|ncol=1"]) == (64, 0)
+    assert autotune._shape({"threads": 128}) == (128, -1)       # an entry written before the cap axis
+    assert autotune._shape({"threads": 96}) is None
     monkeypatch.setenv("LICA_TUNE_CACHE", str(tmp_path / "missing" / "x.json"))
     assert autotune._load() == {}
 
@@ -40,7 +42,8 @@ def test_tune_picks_a_shape_leaves_the_state_and_caches(tmp_path, monkeypatch):
     batch = ColumnBatch.films(n, length, z0, props).to("cuda")
     before = {k: v.clone() for k, v in batch.arrays.items()}
     th, times = autotune.tune(batch)
-    assert th in autotune.SHAPES and set(times) == set(autotune.SHAPES) and th == min(times, key=times.get)
+    assert th in autotune.SHAPES and set(times) == {autotune._name(x) for x in autotune.SHAPES}
+    assert times[autotune._name(th)] == min(times.values())
     for k, v in batch.arrays.items():
         assert torch.equal(v, before[k]), k          # the trial ran on a copy
     th2, times2 = autotune.tune(batch)
