@@ -44,6 +44,32 @@ def batch(rng, count, n):
     return [np.ascontiguousarray(np.stack([p[k] for p in ps])) for k in range(4)]
 
 
+def batch_device(rng, gen, count, n, *, bubbles_per_1024sq=64, rmin=8.0, rmax=48.0, rho_in=1000.0):
+    """count problems of problem()'s distribution built on the GPU (the numpy builder takes
+    about 0.2 s per 1024^2 problem): CUDA tensors rho, f, bx, by of shape (count, n, n) and
+    (count, n + 1, n).  rng draws the bubbles, gen (a CUDA torch.Generator) the RHS."""
+    import torch
+    dev = "cuda"
+    xs = torch.arange(n, device=dev, dtype=torch.float64) + 0.5
+    rho = torch.ones((count, n, n), device=dev, dtype=torch.float64)
+    for i in range(count):
+        nb = max(1, int(rng.poisson(bubbles_per_1024sq * n * n / 1024.0 ** 2)))
+        cx, cy, rr = rng.uniform(0.0, n, nb), rng.uniform(0.0, n, nb), rng.uniform(rmin, rmax, nb)
+        for k in range(nb):
+            dx = (xs - float(cx[k])).abs()
+            dx = torch.minimum(dx, n - dx)
+            dy = xs - float(cy[k])
+            rho[i][(dy[:, None] ** 2 + dx[None, :] ** 2) <= float(rr[k]) ** 2] = rho_in
+    f = torch.randn((count, n, n), generator=gen, device=dev, dtype=torch.float64)
+    f -= f.mean(dim=(1, 2), keepdim=True)
+    bx = 2.0 / (rho + torch.roll(rho, 1, dims=2))
+    by = torch.empty((count, n + 1, n), device=dev, dtype=torch.float64)
+    by[:, 1:n] = 2.0 / (rho[:, 1:] + rho[:, :-1])
+    by[:, 0] = 1.0 / rho[:, 0]
+    by[:, n] = 1.0 / rho[:, n - 1]
+    return rho, f.contiguous(), bx.contiguous(), by
+
+
 def train(net, steps, n, lr=1e-3, seed=0, log_every=100, log=print, lr_final=None, anorm=True):
     """Adam steps on fresh problems of n x n (net.n per step); returns the loss history.
     anorm: the loss is the relative A-norm error against the solver's solution of each
@@ -121,6 +147,95 @@ def train_film(net, steps, nx, ny, lr=1e-3, lr_final=1e-4, seed=0, pool_steps=64
     return hist
 
 
+def train_configs(pairs=20000, n2=1024, film=(512, 1536), images=4, lr=1e-3, lr_final=1e-4, seed=0, chunk=200,
+                  log=print, checkpoint=None):
+    """Config 5's training set: (density, RHS -> pressure) pairs from config-2 solves (n2 x n2,
+    the benchmark's bubble distribution built on the GPU, each problem solved to 1e-10 by the
+    multigrid) and
+    from config-3 solves (the 2-D film step's own three pressure systems per step at its full
+    size, captured as the film runs), half each, interleaved in chunks of `chunk` Adam steps.
+    One set of weights (the network is dimensionless); each grid shape keeps its own Adam
+    moments, and the weights move between the two at every switch (and to `checkpoint`, a
+    .npy path, if given).  Returns (params, loss history per config)."""
+    import torch
+    from . import film2d as G
+    from . import poisson
+    from .unet import LearnedGuess
+    rng = np.random.default_rng(seed)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    nx, ny = film
+    net2 = LearnedGuess(images, n2, n2, seed=seed + 1)
+    net3 = LearnedGuess(3, ny, nx, seed=seed + 1)
+    net3.set_params(net2.get_params())
+    h2 = 1.0 / n2
+    solver = poisson.MultigridPoisson(n2, n2, h2, h2, nlevels=max(2, int(np.log2(n2)) - 4), ncoarse=1)
+    P = G.default_props()
+    fst = G.to_device(G.initial_state(nx, ny, ny / 24.0, nx / 128.0, props=P))
+    fdt = G.stable_dt(nx, P)
+    fgpu = G.Film2D(nx, ny, P)
+    buf = torch.zeros(3 * (4 * nx * ny + (ny + 1) * nx), dtype=torch.float64, device="cuda")
+    steps2 = pairs // 2 // images
+    steps3 = pairs // 2 // 3
+    total = steps2 + steps3
+    hist = {"config2": [], "config3": []}
+    done2 = done3 = 0
+    cur = 2
+    t0 = time.time()
+    try:
+        fgpu.step(fst, fdt)     # the film's first step starts from the hydrostatic pressure
+        while done2 < steps2 or done3 < steps3:
+            if cur == 2 and done2 >= steps2:
+                cur = 3
+            if cur == 3 and done3 >= steps3:
+                cur = 2
+            net = net2 if cur == 2 else net3
+            for _ in range(chunk):
+                it = done2 + done3
+                lr_it = lr * (lr_final / lr) ** (it / max(1, total - 1))
+                if cur == 2:
+                    if done2 >= steps2:
+                        break
+                    rho, f, bx, by = batch_device(rng, gen, images, n2)
+                    ps = torch.zeros_like(f)
+                    for i in range(images):
+                        _, _, st = solver.solve(ps[i], f[i], bx[i], by[i], rtol=1e-10, max_iters=200)
+                        if st != 0:
+                            raise RuntimeError(f"solver status {st} on a config-2 training problem")
+                    hist["config2"].append(net.train_step(rho, f, bx, by, h2, h2, lr_it, p_star=ps))
+                    done2 += 1
+                else:
+                    if done3 >= steps3:
+                        break
+                    fgpu.capture(buf)
+                    fgpu.step(fst, fdt)
+                    fgpu.capture(None)
+                    sys3 = fgpu.unpack_capture(buf)
+                    rho, f, bx, by, dp = (torch.stack([q[k] for q in sys3]).contiguous()
+                                          for k in ("rho", "f", "bx", "by", "dp"))
+                    hist["config3"].append(net.train_step(rho, f, bx, by, 1.0 / nx, 1.0 / nx, lr_it, p_star=dp))
+                    done3 += 1
+            other = net3 if cur == 2 else net2
+            params = net.get_params()
+            other.set_params(params)
+            if checkpoint:
+                np.save(checkpoint, params)
+            if log:
+                l2 = np.mean(hist["config2"][-50:]) if hist["config2"] else 0.0
+                l3 = np.mean(hist["config3"][-50:]) if hist["config3"] else 0.0
+                log(f"pairs {images * done2 + 3 * done3:6d}  config-2 loss {l2:.4e}  config-3 loss {l3:.4e}  "
+                    f"({time.time() - t0:.1f} s)")
+            cur = 3 if cur == 2 else 2
+        params = (net2 if cur == 3 else net3).get_params()
+    finally:
+        fgpu.capture(None)
+        fgpu.close()
+        solver.close()
+        net2.close()
+        net3.close()
+    return params, hist
+
+
 def iterations(n, problems, guess_net=None, rtol=1e-10, nlevels=None, precision="fp64"):
     """PCG iterations (and final relative residuals) of each problem from x0 = 0, or from
     the network's guess with the zero fallback."""
@@ -165,8 +280,15 @@ def main():
     ap.add_argument("--film", action="store_true",
                     help="train on the 2-D film step's own pressure systems (writes the film weights)")
     ap.add_argument("--film-nx", type=int, default=256)
+    ap.add_argument("--configs", type=int, default=0, metavar="PAIRS",
+                    help="train on PAIRS pairs from config-2 (1024^2) and config-3 (512 x 1536 film) solves")
     a = ap.parse_args()
     from .unet import LearnedGuess
+    if a.configs:
+        params, _ = train_configs(a.configs, images=a.batch, lr=a.lr, lr_final=a.lr_final, seed=a.seed)
+        os.makedirs(os.path.dirname(a.out), exist_ok=True)
+        np.save(a.out, params)
+        return
     if a.film:
         nx, ny = a.film_nx, 3 * a.film_nx
         net = LearnedGuess(a.batch, ny, nx, seed=a.seed + 1)
