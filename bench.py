@@ -383,10 +383,10 @@ def film_leg(dev, flush, steps=10, warmup=2, compare=True):
     net = None
     from lica_boiling1d_b200 import train_guess
     arms = ["fp64", "mixed"]
-    if os.path.exists(train_guess.FILM_WEIGHTS):
+    if os.path.exists(train_guess.CONFIG_WEIGHTS):
         from lica_boiling1d_b200.unet import LearnedGuess
         net = LearnedGuess(1, ny, nx)
-        train_guess.load(net, train_guess.FILM_WEIGHTS)
+        train_guess.load(net, train_guess.CONFIG_WEIGHTS)
         arms.append("mixed_learned")
     for arm in arms:
         prec = "fp64" if arm == "fp64" else "mixed"
@@ -423,8 +423,9 @@ def film_leg(dev, flush, steps=10, warmup=2, compare=True):
         if arm == "mixed_learned":
             out[arm]["guess_rel_per_substep"] = grels[-1]
             out[arm]["mean_iterations_saved_vs_mixed"] = float(np.mean(out["mixed"]["_its"]) - np.mean(its))
-            out[arm]["note"] = ("mixed-precision MG-PCG started from the U-Net guess trained on the film's own "
-                                "(density, rhs -> increment) pairs; zero where the guess is no better")
+            out[arm]["note"] = ("mixed-precision MG-PCG started from the U-Net guess trained on 20,000 config-2 "
+                                "(1024^2) and config-3 (this film's own systems) pairs; zero where the guess is "
+                                "no better")
         out[arm]["_its"] = its
     if net is not None:
         net.close()
@@ -735,10 +736,10 @@ def learned_leg(args, dev, case, n, nlevels, f, bx, by, p, flush, stream, reps):
 
     from lica_boiling1d_b200 import poisson, train_guess
     from lica_boiling1d_b200.unet import LearnedGuess
-    if not os.path.exists(train_guess.WEIGHTS):
+    if not os.path.exists(train_guess.CONFIG_WEIGHTS):
         return {"unavailable": "no trained weights in the package"}
     net = LearnedGuess(1, n, n)
-    train_guess.load(net)
+    train_guess.load(net, train_guess.CONFIG_WEIGHTS)
     rho = torch.from_numpy(case.rho[None].copy()).to(dev)
     F, BX, BY = f[None], bx[None], by[None]
     x0 = torch.empty_like(F)
@@ -769,6 +770,14 @@ def learned_leg(args, dev, case, n, nlevels, f, bx, by, p, flush, stream, reps):
                     "note": "10 tcgen05 convolutions (BF16, FP32 accumulate) + pooling/upsampling/head"}
     _, rel0 = net.guess_checked(rho, F, BX, BY, case.hx, case.hy, out=x0)
     out["guess"]["rel_residual"] = float(rel0[0])
+    out["guess"]["weights"] = "config 5: 20,000 pairs from config-2 and config-3 solves (unet_guess_configs.npy)"
+    if os.path.exists(train_guess.WEIGHTS):
+        # the same network trained on 16,000 256^2 bubble problems only, for comparison
+        alt = LearnedGuess(1, n, n)
+        train_guess.load(alt, train_guess.WEIGHTS)
+        _, rel_alt = alt.guess_checked(rho, F, BX, BY, case.hx, case.hy, out=x0)
+        alt.close()
+        out["guess"]["rel_residual_bubble_only_weights"] = float(rel_alt[0])
     for prec in ("fp64", "mixed"):
         s = poisson.MultigridPoisson(n, n, case.hx, case.hy, nlevels=nlevels, ncoarse=args.ncoarse, precision=prec)
         for _ in range(3):

@@ -25,6 +25,9 @@ from .inputs import bubble_density, face_beta
 HERE = os.path.dirname(os.path.abspath(__file__))
 WEIGHTS = os.path.join(HERE, "weights", "unet_guess.npy")
 FILM_WEIGHTS = os.path.join(HERE, "weights", "unet_guess_film.npy")
+# config 5's training set: 20,000 pairs from config-2 (1024^2) and config-3 (512 x 1536 film)
+# solves (train_configs); the weights the benchmark's learned legs use
+CONFIG_WEIGHTS = os.path.join(HERE, "weights", "unet_guess_configs.npy")
 
 
 def problem(rng, n, ny=None, *, bubbles_per_1024sq=64, rmin=8.0, rmax=48.0):
