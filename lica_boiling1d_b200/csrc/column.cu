@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstring>
 #include <mutex>
 #include <vector>
 
@@ -2094,7 +2095,25 @@ int column_steps_host(int32_t ncol, int32_t n, double length, const lica_col_pro
         host_bytes = total;
     }
     char* base = host_buf;
-    for (int q = 0; q < nfld; ++q) LICA_CUDA_TRY(cudaMemcpy(base + off[q], f[q].h, f[q].bytes, cudaMemcpyHostToDevice));
+    // Small states (a few columns: the per-step drop-in use) go through one page-locked
+    // staging buffer, one copy each way instead of one per array; large ones copy directly.
+    static char* pin_buf = nullptr;
+    static size_t pin_bytes = 0;
+    const bool packed = total <= ((size_t)64 << 20);
+    if (packed && total > pin_bytes) {
+        if (pin_buf) cudaFreeHost(pin_buf);
+        pin_buf = nullptr;
+        pin_bytes = 0;
+        LICA_CUDA_TRY(cudaMallocHost((void**)&pin_buf, total));
+        pin_bytes = total;
+    }
+    if (packed) {
+        for (int q = 0; q < nfld; ++q) std::memcpy(pin_buf + off[q], f[q].h, f[q].bytes);
+        LICA_CUDA_TRY(cudaMemcpy(base, pin_buf, st_off, cudaMemcpyHostToDevice));
+    } else {
+        for (int q = 0; q < nfld; ++q)
+            LICA_CUDA_TRY(cudaMemcpy(base + off[q], f[q].h, f[q].bytes, cudaMemcpyHostToDevice));
+    }
     lica_col_state d;
     d.w = (double*)(base + off[0]);
     d.p = (double*)(base + off[1]);
@@ -2115,9 +2134,15 @@ int column_steps_host(int32_t ncol, int32_t n, double length, const lica_col_pro
     int rc = column_steps_device(ncol, n, length, props, &d, nsteps, 0, nullptr, dst, nullptr, geo);
     if (rc) return rc;
     LICA_CUDA_TRY(cudaDeviceSynchronize());
-    for (int q = 0; q < nfld; ++q)
-        LICA_CUDA_TRY(cudaMemcpy(f[q].h, base + off[q], f[q].bytes, cudaMemcpyDeviceToHost));
-    LICA_CUDA_TRY(cudaMemcpy(status, dst, 4 * nc, cudaMemcpyDeviceToHost));
+    if (packed) {
+        LICA_CUDA_TRY(cudaMemcpy(pin_buf, base, total, cudaMemcpyDeviceToHost));
+        for (int q = 0; q < nfld; ++q) std::memcpy(f[q].h, pin_buf + off[q], f[q].bytes);
+        std::memcpy(status, pin_buf + st_off, 4 * nc);
+    } else {
+        for (int q = 0; q < nfld; ++q)
+            LICA_CUDA_TRY(cudaMemcpy(f[q].h, base + off[q], f[q].bytes, cudaMemcpyDeviceToHost));
+        LICA_CUDA_TRY(cudaMemcpy(status, dst, 4 * nc, cudaMemcpyDeviceToHost));
+    }
     int worst = LICA_OK;
     for (size_t c = 0; c < nc; ++c)
         if (status[c] != LICA_OK) worst = status[c];
