@@ -53,3 +53,30 @@ def test_fortran_module_is_current_and_complete():
         args = [a.strip() for a in m.group(1).split(",") if a.strip()]
         assert args == [p for p, _ in params], name
     assert all(len(line) <= 100 for line in text.splitlines())
+
+
+def test_new_entry_points_refuse_bad_arguments_before_any_device_work():
+    """The geometry, y-line and batch-shape entry points check their arguments on the host
+    and return LICA_BAD_ARG (4) before touching a device, so these calls run without a GPU."""
+    import ctypes as C
+    L = native.lib()
+    bad = 4
+    st = native.ColState()
+    props = native.ColProps()
+    status = (C.c_int32 * 4)()
+    # a null geometry handle
+    assert L.lica_gpu_column_steps_geometry_device(None, 1, C.byref(props), C.byref(st), 1, 0, None,
+                                                   C.cast(status, C.c_void_p), None) == bad
+    assert L.lica_gpu_column_steps_geometry(None, 1, C.byref(props), C.byref(st), 1, status) == bad
+    prm = native.LvsParams(1, 1, 1, 1, 1000.0, 1e-3)
+    args = [None] * 12
+    assert L.lica_gpu_lvs_transport_geometry_device(None, 1, *args, C.byref(prm), None) == bad
+    # a geometry with null arrays, and a null output handle
+    g = native.ColGeometry()
+    h = C.c_void_p()
+    assert L.lica_gpu_column_geometry_create(C.byref(h), 64, 1.0, C.byref(g)) == bad and not h.value
+    assert L.lica_gpu_column_geometry_create(None, 64, 1.0, C.byref(g)) == bad
+    # y-line smoothing is FP64 only; unknown smoothers are refused
+    for prec, sm in ((1, 1), (0, 2)):
+        o = native.MgOptions(6, 2, 2, 1, prec, 1, sm)
+        assert L.lica_mg_create(C.byref(h), 1024, 1024, 1.0 / 1024, 1.0 / 1024, C.byref(o)) == bad
