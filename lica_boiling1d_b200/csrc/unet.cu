@@ -557,17 +557,29 @@ __global__ void k_apply_op(const double* __restrict__ u, const double* __restric
 }
 
 // r = f - A x0 (in place over ax), and per-image ||r||^2 (one block per image).
-__global__ void k_residual(const double* __restrict__ f, double* __restrict__ r, double* __restrict__ rr, int npix) {
+// r = f - (A x0) in place and ||r||^2 per image: kRmsParts blocks per image write partial
+// sums (k_part_sum adds them in a fixed order).
+__global__ void k_residual(const double* __restrict__ f, double* __restrict__ r, double* __restrict__ part,
+                           int npix) {
     __shared__ double red[32];
-    const size_t off = (size_t)blockIdx.x * npix;
+    const size_t off = (size_t)blockIdx.y * npix;
     double s = 0.0;
-    for (int k = threadIdx.x; k < npix; k += blockDim.x) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < npix; k += gridDim.x * blockDim.x) {
         const double v = f[off + k] - r[off + k];
         r[off + k] = v;
         s += v * v;
     }
     s = block_sum(s, red);
-    if (threadIdx.x == 0) rr[blockIdx.x] = s;
+    if (threadIdx.x == 0) part[blockIdx.y * kRmsParts + blockIdx.x] = s;
+}
+
+// out[image] = the sum of its kRmsParts partial sums, in index order (one block per image).
+__global__ void k_part_sum(const double* __restrict__ part, double* __restrict__ out) {
+    __shared__ double red[32];
+    double s = 0.0;
+    for (int k = threadIdx.x; k < kRmsParts; k += blockDim.x) s += part[blockIdx.x * kRmsParts + k];
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) out[blockIdx.x] = s;
 }
 
 // dL/dout = -2 (A r) sigma h^2 rho / (nimg ||f||^2), ||f||^2 = sigma^2 npix.
@@ -581,21 +593,23 @@ __global__ void k_gout(const double* __restrict__ ar, const double* __restrict__
 }
 
 // A-norm loss with the solver's solution p*: e = x0 - p* (into x0's buffer), per image
-// num = -e.(A e) (ae holds A e), den = -p*.f = p*.(-A p*); one block per image.
+// num = -e.(A e) (ae holds A e), den = -p*.f = p*.(-A p*), as kRmsParts partial sums per
+// image (k_part_sum adds them).
 __global__ void k_energy(const double* __restrict__ ae, const double* __restrict__ e, const double* __restrict__ ps,
-                         const double* __restrict__ f, double* __restrict__ num, double* __restrict__ den, int npix) {
+                         const double* __restrict__ f, double* __restrict__ part_num, double* __restrict__ part_den,
+                         int npix) {
     __shared__ double red[32];
-    const size_t off = (size_t)blockIdx.x * npix;
+    const size_t off = (size_t)blockIdx.y * npix;
     double a = 0.0, b = 0.0;
-    for (int k = threadIdx.x; k < npix; k += blockDim.x) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < npix; k += gridDim.x * blockDim.x) {
         a -= e[off + k] * ae[off + k];
         b -= ps[off + k] * f[off + k];
     }
     a = block_sum(a, red);
     b = block_sum(b, red);
     if (threadIdx.x == 0) {
-        num[blockIdx.x] = a;
-        den[blockIdx.x] = b;
+        part_num[blockIdx.y * kRmsParts + blockIdx.x] = a;
+        part_den[blockIdx.y * kRmsParts + blockIdx.x] = b;
     }
 }
 
@@ -667,6 +681,7 @@ struct lica_unet {
     double* ax = nullptr;   // A x0, then r, then A r
     double* rr = nullptr;   // per-image ||r||^2 (or the A-norm loss's numerator)
     double* den = nullptr;  // per-image A-norm of p*
+    double* part2 = nullptr;  // the A-norm loss's second set of partial sums (kRmsParts per image)
     // training buffers
     bool train_ready = false;
     float* gout = nullptr;
@@ -969,8 +984,8 @@ int lica_unet_create(lica_unet** out, int32_t n, int32_t h, int32_t w, uint64_t 
 int lica_unet_destroy(lica_unet* u) {
     if (!u) return LICA_OK;
     void* ptrs[] = {u->param, u->grad, u->adam_m, u->adam_v, u->x16, u->p1, u->p2, u->u2, u->u1, u->out32,
-                    u->sigma, u->rms_part, u->x0, u->ax, u->rr, u->den, u->gout, u->gy, u->gcat, u->dz, u->gsave[0], u->gsave[1],
-                    u->gsave[2], u->gpool, u->part, u->bpart, u->hpart, u->err};
+                    u->sigma, u->rms_part, u->x0, u->ax, u->rr, u->den, u->part2, u->gout, u->gy, u->gcat, u->dz,
+                    u->gsave[0], u->gsave[1], u->gsave[2], u->gpool, u->part, u->bpart, u->hpart, u->err};
     for (void* p : ptrs) cudaFree(p);
     for (int l = 0; l < kLayers; ++l) {
         cudaFree(u->wb[l]);
@@ -1025,9 +1040,10 @@ int lica_unet_guess_checked_device(lica_unet* u, const double* rho, const double
                      1.0 / (hy * hy))))
         return st;
     const int npix = u->h * u->w;
-    k_residual<<<u->n, 1024, 0, s>>>(f, u->ax, u->rr, npix);
+    k_residual<<<dim3(kRmsParts, u->n), kNT, 0, s>>>(f, u->ax, u->rms_part, npix);
+    k_part_sum<<<u->n, kNT, 0, s>>>(u->rms_part, u->rr);
     LICA_CUDA_TRY(cudaGetLastError());
-    lica_count_launches(1);
+    lica_count_launches(2);
     std::vector<double> rr(u->n), sg(u->n);
     LICA_CUDA_TRY(cudaMemcpyAsync(rr.data(), u->rr, sizeof(double) * u->n, cudaMemcpyDeviceToHost, s));
     LICA_CUDA_TRY(cudaMemcpyAsync(sg.data(), u->sigma, sizeof(double) * u->n, cudaMemcpyDeviceToHost, s));
@@ -1063,9 +1079,10 @@ int lica_unet_train_step_device(lica_unet* u, const double* rho, const double* f
     int st;
     if ((st = alloc_training(u))) return st;
     const size_t p0 = level_pixels(u, 0);
-    if (!u->x0) {
-        if ((st = dev_alloc(&u->x0, p0)) || (st = dev_alloc(&u->ax, p0)) || (st = dev_alloc(&u->den, u->n))) return st;
-    }
+    if ((!u->x0 && (st = dev_alloc(&u->x0, p0))) || (!u->ax && (st = dev_alloc(&u->ax, p0))) ||
+        (!u->den && (st = dev_alloc(&u->den, u->n))) ||
+        (!u->part2 && (st = dev_alloc(&u->part2, (size_t)u->n * kRmsParts))))
+        return st;
     const double hsq = hx * hy;
     const int npix = u->h * u->w;
     if ((st = forward(u, rho, f, hsq, u->x0, s))) return st;
@@ -1074,18 +1091,21 @@ int lica_unet_train_step_device(lica_unet* u, const double* rho, const double* f
         // e = x0 - p*, A e, loss = -e.(A e) / (-p*.f) per image, dL/dout
         if ((st = launch(p0, s, k_sub, u->x0, p_star, p0))) return st;
         if ((st = launch(p0, s, k_apply_op, (const double*)u->x0, bx, by, u->ax, u->n, u->h, u->w, cx, cy))) return st;
-        k_energy<<<u->n, 1024, 0, s>>>(u->ax, u->x0, p_star, f, u->rr, u->den, npix);
+        k_energy<<<dim3(kRmsParts, u->n), kNT, 0, s>>>(u->ax, u->x0, p_star, f, u->rms_part, u->part2, npix);
+        k_part_sum<<<u->n, kNT, 0, s>>>(u->rms_part, u->rr);
+        k_part_sum<<<u->n, kNT, 0, s>>>(u->part2, u->den);
         LICA_CUDA_TRY(cudaGetLastError());
-        lica_count_launches(1);
+        lica_count_launches(3);
         if ((st = launch(p0, s, k_gout_energy, (const double*)u->ax, (const double*)u->den, (const double*)u->sigma,
                          rho, hsq, u->gout, npix, u->n)))
             return st;
     } else {
         // r = f - A x0, ||r||^2; then A r into x0's buffer, and dL/dout
         if ((st = launch(p0, s, k_apply_op, (const double*)u->x0, bx, by, u->ax, u->n, u->h, u->w, cx, cy))) return st;
-        k_residual<<<u->n, 1024, 0, s>>>(f, u->ax, u->rr, npix);
+        k_residual<<<dim3(kRmsParts, u->n), kNT, 0, s>>>(f, u->ax, u->rms_part, npix);
+        k_part_sum<<<u->n, kNT, 0, s>>>(u->rms_part, u->rr);
         LICA_CUDA_TRY(cudaGetLastError());
-        lica_count_launches(1);
+        lica_count_launches(2);
         if ((st = launch(p0, s, k_apply_op, (const double*)u->ax, bx, by, u->x0, u->n, u->h, u->w, cx, cy))) return st;
         if ((st = launch(p0, s, k_gout, (const double*)u->x0, (const double*)u->sigma, rho, hsq, u->gout, npix, u->n)))
             return st;
