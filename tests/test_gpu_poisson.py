@@ -3,7 +3,7 @@
 Tolerances: the kernels follow the oracle's operation order without FMA contraction,
 so single applications (operator, preconditioner, tridiagonal solves, POISSON) must
 be bit-identical; solves differ only through the summation order of the CG dot
-products and must agree to 1e-10 relative L2, with the
+products and must agree to 1e-10 relative L2 (the pressure fields' tolerance), with the
 true residual at or below the requested tolerance.
 """
 import os
