@@ -2,8 +2,9 @@
 
 The step kernel runs one CTA per column, persistent over all the steps of a launch.  A
 launch shape has two axes:
-  * the CTA width -- 64, 128 or 256 threads -- which also fixes how many columns share an SM
-    (the 64-thread form is bounded for 5 CTAs per SM, the wider ones run one or two);
+  * the CTA width -- 32, 64, 128 or 256 threads -- which also fixes how many columns share an
+    SM (the 32- and 64-thread forms are bounded for 8 and 5 CTAs per SM, the wider ones run one
+    or two; a one-warp CTA runs TEMP_EXTP's two phases one after the other);
   * the shared-memory cap of the Thomas arrays: as long a column as the CTAs per SM leave room
     for (the default), or none (every column's arrays in the L2-resident scratch).  Results
     are identical either way; the speed is not.
@@ -21,7 +22,7 @@ import os
 import threading
 
 # (threads, tri_cap): tri_cap -1 = the largest the CTAs per SM allow, 0 = no shared arrays
-SHAPES = ((64, -1), (128, -1), (256, -1), (64, 0), (128, 0), (256, 0))
+SHAPES = ((32, -1), (64, -1), (128, -1), (256, -1), (32, 0), (64, 0), (128, 0), (256, 0))
 
 
 def _name(shape):

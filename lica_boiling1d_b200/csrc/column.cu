@@ -833,12 +833,15 @@ __device__ int temp_grad(const Geo& g, const Phys& ph, Col& c, Shared& sh, doubl
     __syncthreads();
     c.mark(PH_TEMPGRAD);
     {
-        // (2) TEMP_EXTP: the vapour phase on warp 0, the liquid phase on warp 1
+        // (2) TEMP_EXTP: the vapour phase on warp 0, the liquid phase on warp 1 (one after the
+        // other on warp 0 in a one-warp CTA)
         const int ka = sh.ibuf[1], kb = sh.ibuf[2], x0 = sh.ibuf[7];
-        if (warp < 2) {
+        const int nw = (int)(blockDim.x >> 5);
+        for (int phs = warp; phs < 2; phs += nw) {
             int it = 0;
-            if (kb >= ka) it = temp_extp(g, ph, sh, x0, ka - x0, kb - x0, warp, warp ? temp1 : temp0);
-            if (lane == 0) sh.ibuf[3 + warp * 2] = it;   // ibuf[3], ibuf[5]
+            if (kb >= ka) it = temp_extp(g, ph, sh, x0, ka - x0, kb - x0, phs, phs ? temp1 : temp0);
+            if (lane == 0) sh.ibuf[3 + phs * 2] = it;   // ibuf[3], ibuf[5]
+            __syncwarp();
         }
     }
     __syncthreads();
@@ -1319,7 +1322,7 @@ __device__ int column_step(const Geo& g, const Phys& ph, Col& c, Shared& sh, dou
 template <int NTH>
 // The 64-thread form is bounded for 5 CTAs per SM (about 200 registers): latency-bound
 // columns gain more from columns in flight than they lose to a few spilled registers.
-__global__ void __launch_bounds__(NTH, NTH == 64 ? 5 : 1) k_column_steps(const __grid_constant__ Args A) {
+__global__ void __launch_bounds__(NTH, NTH == 32 ? 8 : (NTH == 64 ? 5 : 1)) k_column_steps(const __grid_constant__ Args A) {
     __shared__ Shared sh;
     extern __shared__ double dsm[];   // 5 (n+2) doubles when A.tri_smem
     if ((int)blockIdx.x >= A.ncol) return;
@@ -1764,12 +1767,14 @@ int column_ctas_by_registers() {
 }
 
 int launch_columns(colk::Args& A, int nmax, int threads, void* stream, int cap_limit = -1) {
-    const int nth = (threads == 64 || threads == 256) ? threads : colk::NT_DEFAULT;
+    const int nth = (threads == 32 || threads == 64 || threads == 256) ? threads : colk::NT_DEFAULT;
     // Shared-memory tridiagonal arrays for columns up to tri_cap cells, sized so that the
     // CTAs the registers allow per SM still fit (longer columns keep them in scratch; the
     // arithmetic is the same either way).
-    const int ctas = nth == 64 ? column_ctas_by_registers<64>()
-                               : (nth == 128 ? column_ctas_by_registers<128>() : column_ctas_by_registers<256>());
+    const int ctas = nth == 32    ? column_ctas_by_registers<32>()
+                     : nth == 64  ? column_ctas_by_registers<64>()
+                     : nth == 128 ? column_ctas_by_registers<128>()
+                                  : column_ctas_by_registers<256>();
     const long budget = (long)(228 * 1024) / ctas - (long)sizeof(colk::Shared) - 2048;
     long cap = std::min<long>(nmax, budget / (5 * (long)sizeof(double)) - 2);
     if (cap_limit >= 0) cap = std::min<long>(cap, cap_limit);   // a caller's (autotuner's) limit
@@ -1778,12 +1783,14 @@ int launch_columns(colk::Args& A, int nmax, int threads, void* stream, int cap_l
     const size_t dyn = A.tri_smem ? 5 * ((size_t)A.tri_cap + 2) * sizeof(double) : 0;
     {
         static std::mutex mu;
-        static size_t set_bytes[3] = {0, 0, 0};
+        static size_t set_bytes[4] = {0, 0, 0, 0};
         std::lock_guard<std::mutex> lk(mu);
-        const int slot = nth == 64 ? 0 : (nth == 128 ? 1 : 2);
+        const int slot = nth == 64 ? 0 : (nth == 128 ? 1 : (nth == 256 ? 2 : 3));
         if (dyn > set_bytes[slot]) {
             cudaError_t e = cudaSuccess;
-            if (nth == 64)
+            if (nth == 32)
+                e = cudaFuncSetAttribute(colk::k_column_steps<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+            else if (nth == 64)
                 e = cudaFuncSetAttribute(colk::k_column_steps<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
             else if (nth == 128)
                 e = cudaFuncSetAttribute(colk::k_column_steps<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1795,7 +1802,8 @@ int launch_columns(colk::Args& A, int nmax, int threads, void* stream, int cap_l
             set_bytes[slot] = dyn;
         }
     }
-    if (nth == 64) colk::k_column_steps<64><<<A.ncol, 64, dyn, (cudaStream_t)stream>>>(A);
+    if (nth == 32) colk::k_column_steps<32><<<A.ncol, 32, dyn, (cudaStream_t)stream>>>(A);
+    else if (nth == 64) colk::k_column_steps<64><<<A.ncol, 64, dyn, (cudaStream_t)stream>>>(A);
     else if (nth == 128) colk::k_column_steps<128><<<A.ncol, 128, dyn, (cudaStream_t)stream>>>(A);
     else colk::k_column_steps<256><<<A.ncol, 256, dyn, (cudaStream_t)stream>>>(A);
     LICA_CUDA_TRY(cudaGetLastError());

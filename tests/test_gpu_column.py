@@ -116,7 +116,7 @@ def test_long_columns_with_tridiagonal_arrays_in_scratch():
     props = list(props) + [props[0], props[1]]
     dev = ColumnBatch.films(n, length, z0, props).to("cuda")
     refs = [O.col_init(int(n[c]), float(length[c]), float(z0[c]), props[c]) for c in range(len(n))]
-    other = dev.to("cuda")
+    start = dev.to("cuda")
     status = dev.steps(2, threads=64)
     torch.cuda.synchronize()
     assert int(status.abs().max()) == 0
@@ -126,12 +126,15 @@ def test_long_columns_with_tridiagonal_arrays_in_scratch():
         got = dev.column(c)
         for k, v in r.items():
             assert np.array_equal(got[k], v), (c, k)
-    # the autotuner's other axis: every column's arrays in scratch (tri_cap = 0), 128 threads
-    status = other.steps(2, threads=128, tri_cap=0)
-    torch.cuda.synchronize()
-    assert int(status.abs().max()) == 0
-    for k in dev.arrays:
-        assert torch.equal(dev.arrays[k], other.arrays[k]), k
+    # the autotuner's other shapes: every column's arrays in scratch (tri_cap = 0) at 128
+    # threads, and one-warp CTAs (TEMP_EXTP's two phases in turn on warp 0)
+    for th, cap in ((128, 0), (32, -1)):
+        other = start.to("cuda")
+        status = other.steps(2, threads=th, tri_cap=cap)
+        torch.cuda.synchronize()
+        assert int(status.abs().max()) == 0
+        for k in dev.arrays:
+            assert torch.equal(dev.arrays[k], other.arrays[k]), (th, k)
 
 
 @pytest.mark.parametrize("n,gam,z0s,steps", [(64, 1.0, [0.1], 40), (128, 2.0, [0.06, 0.25], 12)])
