@@ -376,22 +376,33 @@ __device__ void cal_continuity(const Geo& g, const Phys& ph, Col& c, double dtco
     __syncthreads();
 }
 
+// Arrays that are live only inside one routine share the slots of the Thomas arrays, which
+// are dead between the tridiagonal solves: CAL_DENVIS's face and centre values (inside
+// CAL_CONTINUITY, before the substep's first solve) take AK, BK, CK; TEMP_GRAD's two phase
+// temperatures take GK and GAM, and its PSI_TMP takes AK (after LHSPS, before LHSW).  Fewer
+// distinct arrays per column keep more of the columns in flight inside L2.
+__device__ __forceinline__ void share_scratch(Col& c) {
+    c.a[S_VZD] = c.a[S_AK];
+    c.a[S_VZV] = c.a[S_BK];
+    c.a[S_VCD] = c.a[S_CK];
+    c.a[S_TEMP0] = c.a[S_GK];
+    c.a[S_TEMP1] = c.a[S_GAM];
+    c.a[S_PSITMP] = c.a[S_AK];
+}
+
 // CAL_CONT_BC, 1d.f:2961-3003.
 __device__ void cal_cont_bc(const Geo& g, const Phys& ph, Col& c) {
     const int n = g.n;
-    double *dz = c.a[S_DENFZ], *dzi = c.a[S_DENFZI], *dc = c.a[S_DENFC];
-    const double *psi_z = c.a[S_PSIZ], *psi_c = c.a[S_PSIC];
+    // DENF_Z and DENF_C themselves are read by no routine of the step: only 1/DENF_Z is kept
+    double* dzi = c.a[S_DENFZI];
+    const double* psi_z = c.a[S_PSIZ];
     FOR_K(1, n) {
         const double d = ph.denm + ph.den_diff * psi_z[k];
-        dz[k] = d;
         dzi[k] = 1.0 / d;
-        dc[k] = ph.denm + ph.den_diff * psi_c[k];
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        dz[n + 1] = dz[n];
         dzi[n + 1] = dzi[n];
-        dz[0] = dz[1];
         dzi[0] = dzi[1];
     }
     __syncthreads();
@@ -1383,6 +1394,7 @@ __global__ void __launch_bounds__(NTH, NTH == 32 ? 8 : (NTH == 64 ? 5 : 1)) k_co
         c.a[S_GK] = dsm + 3 * sf;
         c.a[S_GAM] = dsm + 4 * sf;
     }
+    share_scratch(c);
     c.region = A.iscr + oi;
     c.prof = A.prof ? A.prof + (size_t)col * PH_COUNT : nullptr;
     c.t0 = clock64();
