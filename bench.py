@@ -14,7 +14,8 @@ superheat) and a batch of 4096 independent columns of uneven length (128-2048 ce
 density ratio 100-1600), whole RK3 steps in one persistent launch, beside the CPU
 restatement's time for the same steps; and the 2-D film-boiling step on 512 x 1536 (level
 set 1024 x 3072) with FP64 and mixed-precision pressure solves, its fields after one step
-compared with the FP64 CPU restatement.
+compared with the FP64 CPU restatement.  "bubble_tracking" times BUBBLE_TRACKING +
+BUBBLE_EIGENV of four level sets on a 256^3 grid (one launch) against the CPU restatement.
 
 Under torchrun each rank solves its own replica (the 2-D multigrid does not shard
 here); value = solves of all ranks / the slowest rank's time.  Rank 0 prints one JSON
@@ -356,6 +357,100 @@ def rk3_legs(dev, flush, steps_c1=C1["steps"], steps_c4=1000, warmup=3, rank=0, 
 
 # ------------------------------------------------------------------ 2-D film boiling
 FILM = dict(nx=512, ny=1536, y0=64.0, amp=4.0)
+
+
+BUB = dict(n=256, nlvs=4, reps=20)
+
+
+def bubble_fields(dev, n, nlvs):
+    """PSI_TMP of nlvs level sets on an n^3 unit-cube grid (two rotated ellipsoids each, edges
+    smeared over about a cell; 1 outside) and seeded velocity fields, built on the device."""
+    import torch
+    from lica_boiling1d_b200.bubbles import BubbleGrid
+    grid = BubbleGrid.uniform(n, n, n, 1.0, 1.0, 1.0)
+    x = torch.tensor(grid.xp, device=dev).view(1, 1, -1)
+    y = torch.tensor(grid.yp, device=dev).view(1, -1, 1)
+    z = torch.tensor(grid.zp, device=dev).view(-1, 1, 1)
+    rng = np.random.default_rng(11)
+    psi = torch.ones((nlvs,) + grid.field_shape, dtype=torch.float64, device=dev)
+    for q in range(nlvs):
+        for _ in range(2):
+            c = rng.uniform(0.25, 0.75, 3)
+            ax = rng.uniform(0.06, 0.16, 3)
+            rot = np.linalg.qr(rng.standard_normal((3, 3)))[0]
+            d = [x - c[0], y - c[1], z - c[2]]
+            r2 = sum(((d[0] * rot[0, k] + d[1] * rot[1, k] + d[2] * rot[2, k]) / ax[k]) ** 2 for k in range(3))
+            phi = (torch.sqrt(r2) - 1.0) * float(ax.min())
+            psi[q] = torch.minimum(psi[q], torch.clamp(0.5 + phi * (n / 1.5), 0.0, 1.0))
+    psi[:, [0, -1]] = 1.0
+    psi[:, :, [0, -1]] = 1.0
+    psi[:, :, :, [0, -1]] = 1.0
+    g = torch.Generator(device=dev).manual_seed(12)
+    uvw = [torch.randn(grid.field_shape, dtype=torch.float64, device=dev, generator=g) for _ in range(3)]
+    return grid, psi.contiguous(), uvw
+
+
+def bubble_leg(dev, flush, compare=True):
+    """BUBBLE_TRACKING + BUBBLE_EIGENV of four level sets on a 256^3 grid (one launch): level
+    sets per second, the HBM roofline of the one-pass kernel, and the records against the
+    oracle's two-sweep restatement, whose single-thread time is the CPU baseline."""
+    import torch
+
+    from lica_boiling1d_b200 import bubbles, native
+    n, nlvs, reps = BUB["n"], BUB["nlvs"], BUB["reps"]
+    grid, psi, (u, v, w) = bubble_fields(dev, n, nlvs)
+    tr = bubbles.BubbleTracker(grid, nlvs)
+    st = torch.cuda.current_stream(dev)
+    for _ in range(3):
+        raw = tr.track(psi, u, v, w, stream=st)
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    l0 = native.launch_count()
+    for k in range(reps):
+        flush.fill_(k & 0xFF)
+        ev[k][0].record(st)
+        raw = tr.track(psi, u, v, w, out=raw, stream=st)
+        ev[k][1].record(st)
+    torch.cuda.synchronize(dev)
+    launches = native.launch_count() - l0
+    ms = sum(a.elapsed_time(b) for a, b in ev) / reps
+    rec = bubbles.records(raw)
+    tr.close()
+    interior = psi[:, 1:-1, 1:-1, 1:-1]
+    gas = int((interior != 1.0).sum().item())
+    cells = n ** 3
+    alg = 8.0 * nlvs * cells + 24.0 * gas
+    peak, src = peaks()
+    achieved = alg / (ms / 1e3) / 1e9
+    out = {"workload": f"BUBBLE_TRACKING + BUBBLE_EIGENV of {nlvs} level sets (two rotated ellipsoidal bubbles "
+                       f"each) on a uniform {n}^3 grid, FP64, one launch; PSI_TMP fields "
+                       f"{nlvs * psi[0].numel() * 8 / 1e6:.0f} MB (> L2), 256 MiB flush between launches",
+           "level_sets_per_s": nlvs / (ms / 1e3), "ms_per_call": ms, "cells_per_s": nlvs * cells / (ms / 1e3),
+           "gas_cells": gas, "gpu_launches": launches,
+           "roofline": {"bound": "hbm", "kernel": "k_bubble", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "peak_source": src, "traffic": None,
+                        "alg_bytes_per_launch": alg,
+                        "note": "8 B of PSI_TMP per cell and level set, plus U, V, W (24 B) at each gas cell"}}
+    if compare:
+        from oracle import oracle
+        h = [a.cpu().numpy() for a in (psi, u, v, w)]
+        oracle.lib()
+        t0 = time.perf_counter()
+        ref = oracle.bubble_tracking(grid.as_dict(), *h)
+        cpu_s = time.perf_counter() - t0
+        rel = lambda a, b: float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))  # noqa: E731
+        out["vs_oracle"] = {"max_rel_diff_volume": rel(rec["vol"], ref["vol"]),
+                            "max_rel_diff_centroid_velocity": rel(rec["col"][:, :6], ref["col"][:, :6]),
+                            "max_rel_diff_eigenvalues": rel(np.sort(rec["ami"], axis=1), np.sort(ref["ami"], axis=1)),
+                            "max_rel_diff_aspect_ratio": rel(rec["col"][:, 6], ref["col"][:, 6]),
+                            "max_abs_diff_angles_deg": float(np.max(np.abs(rec["col"][:, 7:] - ref["col"][:, 7:]))),
+                            "note": "one-pass Welford/Chan moments on the GPU against the reference's two sweeps; "
+                                    "eigenvalues compared sorted (the diagonal position Jacobi leaves each in "
+                                    "depends on the rotation path)"}
+        out["cpu_baseline"] = {"value": nlvs / cpu_s, "unit": "level sets/s", "cores": 1, "kind": "port",
+                               "sample": f"the whole workload once ({nlvs} level sets, {n}^3), oracle C++ "
+                                         "restatement, one thread"}
+    return out
 
 
 def film_leg(dev, flush, steps=10, warmup=2, compare=True):
@@ -707,6 +802,9 @@ def run_ours(args):
                     "vcycles_saved": itm[-1] - lg["mixed"]["iterations"],
                     "note": "mixed-precision MG-PCG from the U-Net guess (guess + check + solve per step)"}
 
+    bubbles_leg = None
+    if rank == 0 and not args.skip_bubbles:
+        bubbles_leg = bubble_leg(dev, flush, compare=(world == 1 and not args.skip_cpu))
     err_headline = oracle_error(case, nlevels, p_last) if (rank == 0 and not args.skip_cpu) else None
     if rank == 0 and world == 1 and not args.skip_cpu and n == N:
         threads = os.cpu_count()
@@ -870,6 +968,7 @@ def finish(args, v):
             "rel_l2_error_vs_fp64_oracle": v.get("err_headline"),
             "roofline": v["roofline"], "cpu_baseline": v["cpu"], "e2e": v["e2e"], "gpu_launches": int(v["launches"]),
             "clocks": v["clk"], "variants": v["variants"], "rk3": v.get("rk3"),
+            "bubble_tracking": v.get("bubbles_leg"),
         }
         print(json.dumps(line), flush=True)
     v["solver"].close()
@@ -893,6 +992,7 @@ def main():
     ap.add_argument("--skip-rk3", action="store_true", help="skip the RK3 column legs")
     ap.add_argument("--skip-learned", action="store_true", help="skip the learned-guess legs")
     ap.add_argument("--skip-2048", action="store_true", help="skip the 2048x2048 solves")
+    ap.add_argument("--skip-bubbles", action="store_true", help="skip the 3-D bubble-statistics leg")
     ap.add_argument("--profile-guess", type=int, default=0,
                     help="only run this many U-Net guesses at 1024x1024 (profiling) and exit")
     ap.add_argument("--c1-steps", type=int, default=C1["steps"], help="timed steps of the 512-cell column")

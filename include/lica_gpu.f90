@@ -158,6 +158,32 @@ module lica_gpu
     real(c_double) :: guess_rel(3)
   end type lica_film2d_stats
 
+  type, bind(c) :: lica_bub_grid
+    integer(c_int32_t) :: n1m
+    integer(c_int32_t) :: n2m
+    integer(c_int32_t) :: n3m
+    integer(c_int32_t) :: ipx
+    integer(c_int32_t) :: ipy
+    integer(c_int32_t) :: ipz
+    real(c_double) :: zl
+    type(c_ptr) :: sdx
+    type(c_ptr) :: sdy
+    type(c_ptr) :: sdz
+    type(c_ptr) :: xp
+    type(c_ptr) :: yp
+    type(c_ptr) :: zp
+  end type lica_bub_grid
+
+  type, bind(c) :: lica_bub_record
+    real(c_double) :: time
+    integer(c_int64_t) :: llvs
+    real(c_double) :: col(9)
+    real(c_double) :: vel(3)
+    real(c_double) :: vol
+    real(c_double) :: ami(3)
+    integer(c_int64_t) :: iz_periodic
+  end type lica_bub_record
+
   interface
     type(c_ptr) function lica_last_error() bind(c, name="lica_last_error")
       import
@@ -985,5 +1011,50 @@ module lica_gpu
       type(c_ptr), value :: film
       type(c_ptr), value :: systems
     end function lica_film2d_capture_device
+
+    integer(c_int) function lica_gpu_bubble_grid_create(out, grid, max_lvs) &
+        bind(c, name="lica_gpu_bubble_grid_create")
+      import
+      type(c_ptr), intent(out) :: out
+      type(lica_bub_grid), intent(in) :: grid
+      integer(c_int32_t), value :: max_lvs
+    end function lica_gpu_bubble_grid_create
+
+    integer(c_int) function lica_gpu_bubble_grid_destroy(geo) &
+        bind(c, name="lica_gpu_bubble_grid_destroy")
+      import
+      type(c_ptr), value :: geo
+    end function lica_gpu_bubble_grid_destroy
+
+    integer(c_int) function lica_gpu_bubble_tracking_device(geo, nlvs, llvs0, psi_tmp, u, v, w, &
+        time, icacy, out, stream) bind(c, name="lica_gpu_bubble_tracking_device")
+      import
+      type(c_ptr), value :: geo
+      integer(c_int32_t), value :: nlvs
+      integer(c_int32_t), value :: llvs0
+      type(c_ptr), value :: psi_tmp
+      type(c_ptr), value :: u
+      type(c_ptr), value :: v
+      type(c_ptr), value :: w
+      real(c_double), value :: time
+      integer(c_int32_t), value :: icacy
+      type(c_ptr), value :: out
+      type(c_ptr), value :: stream
+    end function lica_gpu_bubble_tracking_device
+
+    integer(c_int) function lica_gpu_bubble_tracking(grid, nlvs, llvs0, psi_tmp, u, v, w, time, &
+        icacy, out) bind(c, name="lica_gpu_bubble_tracking")
+      import
+      type(lica_bub_grid), intent(in) :: grid
+      integer(c_int32_t), value :: nlvs
+      integer(c_int32_t), value :: llvs0
+      real(c_double), intent(in) :: psi_tmp(*)
+      real(c_double), intent(in) :: u(*)
+      real(c_double), intent(in) :: v(*)
+      real(c_double), intent(in) :: w(*)
+      real(c_double), value :: time
+      integer(c_int32_t), value :: icacy
+      type(lica_bub_record), intent(inout) :: out(*)
+    end function lica_gpu_bubble_tracking
   end interface
 end module lica_gpu

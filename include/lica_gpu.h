@@ -627,6 +627,64 @@ int lica_film2d_set_guess(lica_film2d* film, lica_unet* net);
  * turns it off. */
 int lica_film2d_capture_device(lica_film2d* film, double* systems);
 
+/* ------------------------------------------------------------------------------------
+ * Bubble statistics of several level sets on a 3-D grid: BUBBLE_TRACKING(LLVS, PSI_TMP,
+ * U, V, W) (two_phase.f:6321-6555) with BUBBLE_EIGENV (6558-6705) and Jacobi_bub
+ * (two_phase.f:19-97), for level sets llvs0 .. llvs0 + nlvs - 1 in one call.  Per level
+ * set: the gas volume VOL = sum (1 - PSI_TMP) SDX SDY SDZ over the cells with PSI_TMP != 1,
+ * the volume-weighted centroid and cell-centred velocity, the second moment of the gas
+ * volume about the centroid, its eigenvalues by cyclic Jacobi rotations (threshold 1e-12),
+ * the aspect ratio sqrt(largest / smallest) and the angles (degrees, folded into [0, 90])
+ * of the smallest eigenvalue's axis to x and to z.  With ipz = 1 and gas in the top cell
+ * plane K = N3M (IZ_PERIODIC), cells in the lower half (ZP <= ZL/2) count at ZP + ZL.
+ * The reference runs it in substep MSUB = 3 only; the caller decides when to call.
+ *
+ * Grid (Fortran index as offset, lower bound 0): sdx, xp n1m+2 doubles (SDX(0:N1),
+ * XP(0:N1)), likewise sdy, yp (n2m+2) and sdz, zp (n3m+2); cell I = 1..N1M uses SDX(I),
+ * XP(I).  ipx, ipy, ipz: periodic directions (IPV(N1M) = 1 when ipx, else N1).
+ * Fields U, V, W, PSI_TMP(0:N1, 0:N2, 0:N3), column-major: (i, j, k) at
+ * i + (n1m+2) (j + (n2m+2) k); psi_tmp holds nlvs such fields back to back.
+ * icacy 1: the record holds x, y, z and u, v, w; 2: r, theta, z and u_r, u_theta, w.
+ *
+ * The GPU computes each level set's moments in one pass over the fields (a weighted
+ * Welford update per gas cell, merged by Chan's rule in a fixed order), where the
+ * reference sums twice; the results agree to rounding.  An empty level set (VOL = 0)
+ * gives zero centroid, velocity and moments, ar = NaN (0/0) and angles 90 and 0, which
+ * is what the reference's formulas give from a zero moment. */
+typedef struct {
+    int32_t n1m, n2m, n3m;      /* cells per direction (N1M, N2M, N3M) */
+    int32_t ipx, ipy, ipz;      /* periodic directions (IPX, IPY, IPZ) */
+    double zl;                  /* ZL, the z period */
+    const double *sdx, *sdy, *sdz, *xp, *yp, *zp;
+} lica_bub_grid;
+
+typedef struct {
+    double time;
+    int64_t llvs;
+    double col[9];        /* the record of 0bub_tracking.dat after TIME and LLVS (FORMAT
+                             1ES15.7, 1I5, 9ES15.7; two_phase.f:6440-6443, 6539-6542) */
+    double vel[3];        /* VELVS(LLVS, 1:3) = UU, VV, WW (two_phase.f:6547-6549) */
+    double vol;           /* VOL */
+    double ami[3];        /* eigenvalues AMI(1,1), AMI(2,2), AMI(3,3) after Jacobi_bub */
+    int64_t iz_periodic;  /* IZ_PERIODIC */
+} lica_bub_record;
+
+/* A device copy of the grid with room for max_lvs (1..65535) level sets per call;
+ * LICA_BAD_ARG for a size below 1, a field of 2^31 or more doubles, or a cell width that
+ * is not positive. */
+typedef struct lica_bub_geo lica_bub_geo;
+int lica_gpu_bubble_grid_create(lica_bub_geo** out, const lica_bub_grid* grid, int32_t max_lvs);
+int lica_gpu_bubble_grid_destroy(lica_bub_geo* geo);
+/* Device arrays and a stream (enqueues and returns; one call at a time per geo); out is a
+ * device array of nlvs lica_bub_record. */
+int lica_gpu_bubble_tracking_device(lica_bub_geo* geo, int32_t nlvs, int32_t llvs0, const double* psi_tmp,
+                                    const double* u, const double* v, const double* w, double time, int32_t icacy,
+                                    void* out, void* stream);
+/* Host arrays (copies in, runs, copies out); out[nlvs]. */
+int lica_gpu_bubble_tracking(const lica_bub_grid* grid, int32_t nlvs, int32_t llvs0, const double* psi_tmp,
+                             const double* u, const double* v, const double* w, double time, int32_t icacy,
+                             lica_bub_record* out);
+
 #ifdef __cplusplus
 }
 #endif

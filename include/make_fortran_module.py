@@ -27,7 +27,8 @@ RESULT = {"int": "integer(c_int)", "int64_t": "integer(c_int64_t)", "size_t": "i
 # pointer arguments of host entry points that are one value, not an array
 SCALAR_OUT = {("lica_col_fld_dims", "n"), ("lica_mg_profile_read", "total_ms"), ("lica_mg_profile_read", "launches")}
 # struct pointer arguments that are arrays of structs
-STRUCT_ARRAYS = {("lica_gpu_column_batch_create", "props"), ("lica_mg_solve_host_batch", "res")}
+STRUCT_ARRAYS = {("lica_gpu_column_batch_create", "props"), ("lica_mg_solve_host_batch", "res"),
+                 ("lica_gpu_bubble_tracking", "out")}
 
 
 def strip_comments(txt):

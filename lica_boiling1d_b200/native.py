@@ -75,6 +75,11 @@ class Film2DStats(C.Structure):
                 ("guess_rel", C.c_double * 3)]
 
 
+class BubGrid(C.Structure):
+    _fields_ = [(k, C.c_int32) for k in ("n1m", "n2m", "n3m", "ipx", "ipy", "ipz")] + [("zl", C.c_double)] + \
+        [(k, C.c_void_p) for k in ("sdx", "sdy", "sdz", "xp", "yp", "zp")]
+
+
 # every symbol include/lica_gpu.h declares, with its ctypes signature
 SIGNATURES = {
     "lica_last_error": (C.c_char_p, []),
@@ -179,6 +184,12 @@ SIGNATURES = {
     "lica_film2d_capture_device": (C.c_int, [C.c_void_p, C.c_void_p]),
     "lica_film2d_step_device": (C.c_int, [C.c_void_p] * 6 + [C.c_double, C.POINTER(Film2DStats), C.c_void_p]),
     "lica_film2d_mdot_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "lica_gpu_bubble_grid_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(BubGrid), C.c_int32]),
+    "lica_gpu_bubble_grid_destroy": (C.c_int, [C.c_void_p]),
+    "lica_gpu_bubble_tracking_device": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32] + [C.c_void_p] * 4 +
+                                        [C.c_double, C.c_int32, C.c_void_p, C.c_void_p]),
+    "lica_gpu_bubble_tracking": (C.c_int, [C.POINTER(BubGrid), C.c_int32, C.c_int32] + [_D] * 4 +
+                                 [C.c_double, C.c_int32, C.c_void_p]),
 }
 
 STATUS = {0: "LICA_OK", 1: "LICA_NOT_CONVERGED", 2: "LICA_BAND_OVERFLOW", 3: "LICA_NAN", 4: "LICA_BAD_ARG",

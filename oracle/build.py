@@ -11,7 +11,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SOURCES = ["mg2d.cpp", "tridiag.cpp", "lvs1d.cpp", "column1d.cpp", "film2d.cpp"]
+SOURCES = ["mg2d.cpp", "tridiag.cpp", "lvs1d.cpp", "column1d.cpp", "film2d.cpp", "bubble3d.cpp"]
 
 
 def lib_path(native: bool = False) -> str:

@@ -50,6 +50,9 @@ def lib(native: bool = False):
         L.orc_col_temp_grad.argtypes = [C.c_int, C.c_double, _D, _INT, C.c_double, _D, _D, _D, _INT, _D, _D, _D,
                                         _INT, _D]
         L.orc_col_pressure_correction.argtypes = [C.c_int, C.c_double, _D, _INT, C.c_double, _D, _D, _D, _D]
+        L.orc_jacobi3.argtypes = [_D, _D, C.c_double]
+        L.orc_bubble_tracking.argtypes = [C.c_int] * 6 + [C.c_double] + [_D] * 6 + [C.c_int, C.c_int] + [_D] * 4 + \
+            [C.c_double, C.c_int, C.c_void_p]
         _LIBS[key] = L
     return _LIBS[key]
 
@@ -334,3 +337,34 @@ def col_step_geo(st, n, length, props, geo, native=False):
     pr, ip = _col_props(props)
     g = col_geo(geo)
     return lib(native).orc_col_step_geo(n, length, _p(pr), _pi(ip), *_col_args(st), _p(st["stats"]), C.byref(g))
+
+
+# one record of BUBBLE_TRACKING per level set (the layout of lica_bub_record)
+BUB_RECORD = np.dtype([("time", "f8"), ("llvs", "i8"), ("col", "f8", 9), ("vel", "f8", 3), ("vol", "f8"),
+                       ("ami", "f8", 3), ("iz_periodic", "i8")])
+
+
+def jacobi3(a, abserr=1e-12):
+    """Jacobi_bub on a symmetric 3x3 matrix: (a after the rotations, eigenvectors as columns)."""
+    a = np.array(a, dtype=np.float64, order="C", copy=True)
+    x = np.empty((3, 3))
+    lib().orc_jacobi3(_p(a), _p(x), abserr)
+    return a, x
+
+
+def bubble_tracking(grid, psi_tmp, u, v, w, *, time=0.0, icacy=1, llvs0=1):
+    """BUBBLE_TRACKING + BUBBLE_EIGENV for each field of psi_tmp (nlvs, n3m+2, n2m+2, n1m+2);
+    grid: dict with n1m, n2m, n3m, ipx, ipy, ipz, zl and sdx, sdy, sdz, xp, yp, zp (Fortran
+    index as offset).  Returns the records (BUB_RECORD)."""
+    psi = np.ascontiguousarray(psi_tmp, dtype=np.float64)
+    nlvs = psi.shape[0]
+    shape = (grid["n3m"] + 2, grid["n2m"] + 2, grid["n1m"] + 2)
+    assert psi.shape[1:] == shape
+    u, v, w = (np.ascontiguousarray(a, dtype=np.float64) for a in (u, v, w))
+    assert u.shape == v.shape == w.shape == shape
+    geo = [np.ascontiguousarray(grid[k], dtype=np.float64) for k in ("sdx", "sdy", "sdz", "xp", "yp", "zp")]
+    out = np.zeros(nlvs, dtype=BUB_RECORD)
+    lib().orc_bubble_tracking(grid["n1m"], grid["n2m"], grid["n3m"], grid["ipx"], grid["ipy"], grid["ipz"],
+                              grid["zl"], *[_p(a) for a in geo], nlvs, llvs0, _p(psi), _p(u), _p(v), _p(w),
+                              time, icacy, out.ctypes.data_as(C.c_void_p))
+    return out
