@@ -954,6 +954,27 @@ def profile_film(steps):
     gpu.close()
 
 
+def profile_bubbles(calls):
+    """A few bubble-statistics launches on the 256^3, four-level-set workload (for ncu);
+    prints the mean launch time."""
+    import torch
+
+    from lica_boiling1d_b200 import bubbles
+    dev = torch.device("cuda:0")
+    grid, psi, (u, v, w) = bubble_fields(dev, BUB["n"], BUB["nlvs"])
+    tr = bubbles.BubbleTracker(grid, BUB["nlvs"])
+    raw = tr.track(psi, u, v, w)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(calls):
+        raw = tr.track(psi, u, v, w, out=raw)
+    b.record()
+    torch.cuda.synchronize()
+    print(f"bubble statistics {BUB['n']}^3 x {BUB['nlvs']}: {a.elapsed_time(b) / calls:.4f} ms over {calls} calls")
+    tr.close()
+
+
 def finish(args, v):
     import torch.distributed as dist
     if v["rank"] == 0:
@@ -999,6 +1020,8 @@ def main():
     ap.add_argument("--c4-steps", type=int, default=1000, help="timed steps of the 4096-column batch")
     ap.add_argument("--film-steps", type=int, default=10, help="timed steps of the 2-D film (0: skip the leg)")
     ap.add_argument("--profile-film", type=int, default=0, help="run N 2-D film steps only (ncu launch lists)")
+    ap.add_argument("--profile-bubbles", type=int, default=0,
+                    help="run N bubble-statistics launches only (256^3, four level sets; for ncu)")
     ap.add_argument("--profile-batch", type=int, default=0,
                     help="only run NCOL columns of the uneven batch (profiling runs); see --c4-steps, --threads")
     ap.add_argument("--threads", type=int, default=64, help="column CTA width for --profile-batch")
@@ -1013,6 +1036,9 @@ def main():
         return
     if args.profile_guess:
         profile_guess(args.profile_guess)
+        return
+    if args.profile_bubbles:
+        profile_bubbles(args.profile_bubbles)
         return
     if args.profile_film:
         profile_film(args.profile_film)

@@ -275,17 +275,17 @@ __device__ void bub_finish(const BubArgs& A, const Mom& m, int l) {
     A.out[l] = r;
 }
 
-// One block row of gridDim.x blocks per level set (blockIdx.y).  The cell rows (J, K) are
-// dealt to the warps of the block row in turn; a warp takes kRowsInFlight of its rows at a
-// time and its lanes walk each row in 16-byte pairs of cells (the pair boundaries follow the
-// address, so a row may start or end with a ghost cell, which is skipped), one pair per row
-// in flight, so a lane keeps kRowsInFlight 16-byte loads outstanding whatever the row
-// length.  A gas cell's row constants are recomputed where it is met (gas cells are few).
-constexpr int kRowsInFlight = 8;
+// One block row of gridDim.x blocks per level set (blockIdx.y).  The level set's field is
+// read as one flat stream, ghost cells included, in 16-byte pairs aligned to the address:
+// thread t of the block row takes pairs t, t + T, t + 2T, ... (T threads in the row), sixteen
+// at a time, so a warp's loads are contiguous and a lane keeps sixteen 16-byte loads in flight.
+// Only a value other than 1 -- a gas cell, or a ghost cell the caller left unset -- is located
+// (two divisions) and, if it is inside the grid, entered; a lone element left at either end
+// of the stream is a corner ghost cell.
+constexpr int kPairsInFlight = 16;
 
-__device__ __forceinline__ void bub_cell(const BubArgs& A, Mom& m, int row, int i, double ps) {
+__device__ __forceinline__ void bub_cell(const BubArgs& A, Mom& m, int i, int j, int k, double ps) {
     const long long p1 = A.n1m + 2, p2 = (long long)(A.n2m + 2) * p1;
-    const int j = 1 + row % A.n2m, k = 1 + row / A.n2m;
     const long long base = j * p1 + k * p2, c = base + i;
     const double z = A.zp[k];
     const double s = (z <= 0.5 * A.zl) ? z + A.zl : z;
@@ -336,59 +336,50 @@ __device__ __forceinline__ void block_merge(Mom& m, double (*sh)[kMomN]) {
     }
 }
 
+constexpr size_t kBubSmem = (size_t)2 * kPairsInFlight * kBubThreads * sizeof(double);
+
 __global__ void __launch_bounds__(kBubThreads, 2) k_bubble(const __grid_constant__ BubArgs A) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int l = blockIdx.y;
-    const long long p1 = A.n1m + 2, p2 = (long long)(A.n2m + 2) * p1;
     const double* __restrict__ psi = A.psi + (long long)l * A.fsize;
     // elements e with (e + par) even start a 16-byte aligned pair (psi is 8-byte aligned)
     const int par = (int)((reinterpret_cast<uintptr_t>(psi) >> 3) & 1);
     Mom m;
     mom_zero(m);
-    const int nrows = A.n2m * A.n3m;
-    const int nw = gridDim.x * kBubWarps;
-    const int npairs = A.n1m / 2 + 1;  // pairs covering cells 1..n1m of any row
-    __shared__ double gv[2 * kRowsInFlight][kBubThreads];
-    for (int r0 = blockIdx.x * kBubWarps + warp; r0 < nrows; r0 += nw * kRowsInFlight) {
-        int e0[kRowsInFlight];  // the row's first pair (an offset below 2^31), -1 past the last row
-        unsigned odd = 0;       // bit q: that pair's first element is cell 0 (else cell 1)
+    const int p1 = A.n1m + 2, p2 = (A.n2m + 2) * p1;
+    const int npairs = (int)((A.fsize - par) >> 1);
+    const int T = gridDim.x * kBubThreads;
+    extern __shared__ double dyn[];  // kBubSmem: a pair batch's values while its gas cells are entered
+    double (*gv)[kBubThreads] = reinterpret_cast<double (*)[kBubThreads]>(dyn);
+    for (int p0 = blockIdx.x * kBubThreads + threadIdx.x; p0 < npairs; p0 += T * kPairsInFlight) {
+        double2 ps[kPairsInFlight];
 #pragma unroll
-        for (int q = 0; q < kRowsInFlight; ++q) {
-            const int row = r0 + q * nw;
-            const int b = (int)((1 + row % A.n2m) * p1 + (1 + row / A.n2m) * p2);
-            const int c0 = (b + 1 + par) & 1;
-            odd |= (unsigned)c0 << q;
-            e0[q] = (row < nrows) ? b + 1 - c0 : -1;
+        for (int q = 0; q < kPairsInFlight; ++q) {
+            const int p = p0 + q * T;
+            ps[q] = (p < npairs) ? __ldcs(reinterpret_cast<const double2*>(psi + par + 2 * p))
+                                 : make_double2(1.0, 1.0);
         }
-        for (int p = lane; p < npairs; p += 32) {
-            double2 ps[kRowsInFlight];
+        unsigned hit = 0;  // bit 2q (+1): the first (second) value of pair q is not 1
 #pragma unroll
-            for (int q = 0; q < kRowsInFlight; ++q)
-                ps[q] = (e0[q] >= 0) ? __ldcs(reinterpret_cast<const double2*>(psi + e0[q] + 2 * p))
-                                     : make_double2(1.0, 1.0);
-            // bit 2q (+1): the first (second) cell of row q's pair is a gas cell of the grid
-            unsigned gas = 0;
+        for (int q = 0; q < kPairsInFlight; ++q) {
+            if (ps[q].x != 1.0) hit |= 1u << (2 * q);
+            if (ps[q].y != 1.0) hit |= 2u << (2 * q);
+        }
+        if (hit) {
+            // park the values in shared memory, so that the loads' registers are free while
+            // the gas cells update the running state
 #pragma unroll
-            for (int q = 0; q < kRowsInFlight; ++q) {
-                const int i = 1 - (int)((odd >> q) & 1) + 2 * p;
-                if (ps[q].x != 1.0 && i >= 1 && i <= A.n1m) gas |= 1u << (2 * q);
-                if (ps[q].y != 1.0 && i + 1 <= A.n1m) gas |= 2u << (2 * q);
+            for (int q = 0; q < kPairsInFlight; ++q) {
+                gv[2 * q][threadIdx.x] = ps[q].x;
+                gv[2 * q + 1][threadIdx.x] = ps[q].y;
             }
-            if (gas) {
-                // park the pair values in shared memory, so that the loads' registers are free
-                // while the gas cells update the running state
-#pragma unroll
-                for (int q = 0; q < kRowsInFlight; ++q) {
-                    gv[2 * q][threadIdx.x] = ps[q].x;
-                    gv[2 * q + 1][threadIdx.x] = ps[q].y;
-                }
-                do {
-                    const int bit = __ffs(gas) - 1, q = bit >> 1;
-                    gas &= gas - 1;
-                    bub_cell(A, m, r0 + q * nw, 1 - (int)((odd >> q) & 1) + 2 * p + (bit & 1),
-                             gv[bit][threadIdx.x]);
-                } while (gas);
-            }
+            do {
+                const int bit = __ffs(hit) - 1;
+                hit &= hit - 1;
+                const int e = par + 2 * (p0 + (bit >> 1) * T) + (bit & 1);
+                const int k = e / p2, r = e - k * p2, j = r / p1, i = r - j * p1;
+                if (i >= 1 && i <= A.n1m && j >= 1 && j <= A.n2m && k >= 1 && k <= A.n3m)
+                    bub_cell(A, m, i, j, k, gv[bit][threadIdx.x]);
+            } while (hit);
         }
     }
     __shared__ double sh[kBubWarps][kMomN];
@@ -425,6 +416,7 @@ struct lica_bub_geo {
     int n1m, n2m, n3m, ipx, ipy, ipz;
     double zl;
     int max_lvs, nblk;
+    bool smem_set;       // k_bubble's dynamic shared-memory limit raised
     double* geom;        // sdx | sdy | sdz | xp | yp | zp, each direction's n+2 entries
     double* part;        // [max_lvs][nblk][kMomN]
     unsigned* counters;  // [max_lvs]
@@ -456,8 +448,9 @@ int lica_gpu_bubble_grid_create(lica_bub_geo** out, const lica_bub_grid* g, int3
     b->ipz = g->ipz != 0;
     b->zl = g->zl;
     b->max_lvs = max_lvs;
-    const long long rows = (long long)g->n2m * g->n3m;
-    b->nblk = (int)std::min<long long>((rows + kBubWarps - 1) / kBubWarps, kBubMaxBlocks);
+    const long long pairs = (long long)(g->n1m + 2) * (g->n2m + 2) * (g->n3m + 2) / 2;
+    b->nblk = (int)std::min<long long>((pairs + kBubThreads * kPairsInFlight - 1) / (kBubThreads * kPairsInFlight),
+                                       kBubMaxBlocks);
     const size_t ng = 2 * (size_t)(g->n1m + 2) + 2 * (size_t)(g->n2m + 2) + 2 * (size_t)(g->n3m + 2);
     double* host = new double[ng];
     size_t o = 0;
@@ -529,7 +522,11 @@ int lica_gpu_bubble_tracking_device(lica_bub_geo* b, int32_t nlvs, int32_t llvs0
     A.part = b->part;
     A.counters = b->counters;
     A.out = static_cast<lica_bub_record*>(out);
-    k_bubble<<<dim3(b->nblk, nlvs), kBubThreads, 0, (cudaStream_t)stream>>>(A);
+    if (!b->smem_set) {
+        LICA_CUDA_TRY(cudaFuncSetAttribute(k_bubble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBubSmem));
+        b->smem_set = true;
+    }
+    k_bubble<<<dim3(b->nblk, nlvs), kBubThreads, kBubSmem, (cudaStream_t)stream>>>(A);
     LICA_CUDA_TRY(cudaGetLastError());
     lica_count_launches(1);
     return LICA_OK;
