@@ -865,8 +865,11 @@ __device__ int temp_grad(const Geo& g, const Phys& ph, Col& c, Shared& sh, doubl
         __syncwarp();
         if (iters >= 0) {
             // (3) TF on layers 1..NN1 by TEMPASSIGN (chphase.f:372-463); tf0 in win.rk3, tf1
-            // in win.alphio (window-indexed, 0 elsewhere)
-            for (int i = cx.blo + lane; i <= cx.bhi; i += 32) {
+            // in win.alphio (window-indexed, 0 elsewhere).  TF_GRAD's central differences
+            // read one slot past the band on either side -- past the wall where the band is
+            // cut off there -- so those slots are zeroed too, not left to whatever the
+            // shared memory held.
+            for (int i = max(cx.blo - 1, 0) + lane; i <= min(cx.bhi + 1, lvs::WIN - 1); i += 32) {
                 const int k = cx.w0 + i, m = s->layer[i];
                 double v0 = 0.0, v1 = 0.0;
                 if (m >= 1 && m <= lvs::NN1) {
