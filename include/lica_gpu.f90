@@ -194,6 +194,13 @@ module lica_gpu
       import
     end function lica_kernel_launch_count
 
+    integer(c_int) function lica_debug_poison_shared(value, stream) &
+        bind(c, name="lica_debug_poison_shared")
+      import
+      real(c_double), value :: value
+      type(c_ptr), value :: stream
+    end function lica_debug_poison_shared
+
     integer(c_int) function lica_gpu_trdiag3(A, B, C, R, UU, l1, l2, ll1, ll2, ld) &
         bind(c, name="lica_gpu_trdiag3")
       import

@@ -47,6 +47,12 @@ const char* lica_last_error(void);
  * benchmark reads; graph replays count each kernel node). */
 int64_t lica_kernel_launch_count(void);
 
+/* Diagnostic (no counterpart in the reference): fills every SM's shared memory with value
+ * (launches on `stream` and returns).  The kernels here must never read shared memory they
+ * have not written; running them after this call with a NaN shows any that does, where
+ * ordinary runs can hide it behind whatever an earlier kernel left there. */
+int lica_debug_poison_shared(double value, void* stream);
+
 /* ------------------------------------------------------------------------------------
  * Tridiagonal solvers
  * ---------------------------------------------------------------------------------- */

@@ -84,6 +84,7 @@ class BubGrid(C.Structure):
 SIGNATURES = {
     "lica_last_error": (C.c_char_p, []),
     "lica_kernel_launch_count": (C.c_int64, []),
+    "lica_debug_poison_shared": (C.c_int, [C.c_double, C.c_void_p]),
     "lica_gpu_trdiag3": (C.c_int, [_D, _D, _D, _D, _D] + [C.c_int64] * 5),
     "lica_gpu_trdiag3p": (C.c_int, [_D, _D, _D, _D] + [C.c_int64] * 5),
     "lica_gpu_trdiag3_device": (C.c_int, [C.c_void_p] * 5 + [C.c_int64] * 5 + [C.c_void_p]),
@@ -233,3 +234,11 @@ def check(code, where, ok=(0,)):
 
 def launch_count() -> int:
     return int(lib().lica_kernel_launch_count())
+
+
+def poison_shared(value=float("nan"), stream=None):
+    """Fill every SM's shared memory with value and wait for it (diagnostic; see
+    lica_debug_poison_shared)."""
+    import torch
+    check(lib().lica_debug_poison_shared(float(value), stream), "lica_debug_poison_shared")
+    torch.cuda.synchronize()
