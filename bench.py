@@ -477,17 +477,19 @@ def film_leg(dev, flush, steps=10, warmup=2, compare=True):
     first = {}
     net = None
     from lica_boiling1d_b200 import train_guess
-    arms = ["fp64", "mixed"]
+    arms = ["fp64", "mixed", "fp64_warm", "mixed_warm"]
     if os.path.exists(train_guess.CONFIG_WEIGHTS):
         from lica_boiling1d_b200.unet import LearnedGuess
         net = LearnedGuess(1, ny, nx)
         train_guess.load(net, train_guess.CONFIG_WEIGHTS)
         arms.append("mixed_learned")
     for arm in arms:
-        prec = "fp64" if arm == "fp64" else "mixed"
+        prec = "fp64" if arm.startswith("fp64") else "mixed"
         gpu = G.Film2D(nx, ny, P, precision=prec)
         if arm == "mixed_learned":
             gpu.set_guess(net)
+        if arm.endswith("_warm"):
+            gpu.warm_start(True)
         state = G.to_device(st0)
         gpu.step(state, dt)
         torch.cuda.synchronize(dev)
@@ -521,6 +523,10 @@ def film_leg(dev, flush, steps=10, warmup=2, compare=True):
             out[arm]["note"] = ("mixed-precision MG-PCG started from the U-Net guess trained on 20,000 config-2 "
                                 "(1024^2) and config-3 (this film's own systems) pairs; zero where the guess is "
                                 "no better")
+        if arm.endswith("_warm"):
+            out[arm]["mean_iterations_saved_vs_cold"] = float(np.mean(out[prec]["_its"]) - np.mean(its))
+            out[arm]["note"] = ("each substep's solve starts from the increment the same substep solved in the "
+                                "previous step (lica_film2d_set_warm_start)")
         out[arm]["_its"] = its
     if net is not None:
         net.close()
@@ -529,6 +535,7 @@ def film_leg(dev, flush, steps=10, warmup=2, compare=True):
     out["ratio_mixed_learned_vs_fp64"] = (out["mixed_learned"]["steps_per_s"] / out["fp64"]["steps_per_s"]
                                           if "mixed_learned" in out else None)
     out["ratio_mixed_vs_fp64"] = out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"]
+    out["ratio_mixed_warm_vs_fp64"] = out["mixed_warm"]["steps_per_s"] / out["fp64"]["steps_per_s"]
     if compare:
         from oracle import film2d as F
         F.step_native(G.initial_state(64, 192, 8.0, 2.0, props=P), G.stable_dt(64, P), P, 3)  # load the library

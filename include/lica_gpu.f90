@@ -1012,6 +1012,13 @@ module lica_gpu
       type(c_ptr), value :: net
     end function lica_film2d_set_guess
 
+    integer(c_int) function lica_film2d_set_warm_start(film, on) &
+        bind(c, name="lica_film2d_set_warm_start")
+      import
+      type(c_ptr), value :: film
+      integer(c_int32_t), value :: on
+    end function lica_film2d_set_warm_start
+
     integer(c_int) function lica_film2d_capture_device(film, systems) &
         bind(c, name="lica_film2d_capture_device")
       import

@@ -569,6 +569,10 @@ struct lica_film2d {
     // optional learned initial guess of the pressure solves, and the training-pair capture
     lica_unet* guess = nullptr;
     double* capture = nullptr;
+    // optional warm start: each substep's increment kept for the same substep of the next step
+    bool warm = false;
+    bool have_prev[3] = {false, false, false};
+    double* dp_prev[3] = {nullptr, nullptr, nullptr};
 };
 
 namespace {
@@ -584,6 +588,10 @@ int dalloc(double** p, size_t n) {
 
 void free_all(lica_film2d* F) {
     if (F->mg) lica_mg_destroy(F->mg);
+    for (double*& d : F->dp_prev) {
+        cudaFree(d);
+        d = nullptr;
+    }
     double* ptrs[] = {F->psi, F->den, F->vis, F->densc, F->tc, F->bx, F->by, F->us, F->vs, F->ru, F->rv, F->rth, F->f,
                       F->mdot, F->th2, F->dp, F->cx, F->cy, F->rphi, F->ph[0], F->ph[1], F->ph[2], F->kt, F->cf};
     for (double* p : ptrs)
@@ -684,6 +692,8 @@ int lica_film2d_step_device(lica_film2d* F, double* u, double* v, double* p, dou
                                                           &rel0, s);
             if (gs != LICA_OK) return gs;
             local.guess_rel[k - 1] = rel0 < 1.0 ? rel0 : 1.0;
+        } else if (F->warm && F->have_prev[k - 1]) {
+            LICA_CUDA_TRY(cudaMemcpyAsync(F->dp, F->dp_prev[k - 1], n * sizeof(double), cudaMemcpyDeviceToDevice, s));
         } else {
             LICA_CUDA_TRY(cudaMemsetAsync(F->dp, 0, n * sizeof(double), s));
         }
@@ -694,6 +704,10 @@ int lica_film2d_step_device(lica_film2d* F, double* u, double* v, double* p, dou
         local.rel_residual[k - 1] = r.rel_residual;
         local.status[k - 1] = r.status;
         if (st != LICA_OK && st != LICA_NOT_CONVERGED && st != LICA_STALLED) return st;
+        if (F->warm) {
+            LICA_CUDA_TRY(cudaMemcpyAsync(F->dp_prev[k - 1], F->dp, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            F->have_prev[k - 1] = true;
+        }
         if (F->capture) {
             double* q = F->capture + (size_t)(k - 1) * (4 * n + (size_t)(F->ny + 1) * F->nx);
             const size_t nb = (size_t)(F->ny + 1) * F->nx;
@@ -747,6 +761,21 @@ int lica_film2d_step_device(lica_film2d* F, double* u, double* v, double* p, dou
 int lica_film2d_set_guess(lica_film2d* F, lica_unet* net) {
     if (!F) return LICA_BAD_ARG;
     F->guess = net;
+    return LICA_OK;
+}
+
+int lica_film2d_set_warm_start(lica_film2d* F, int32_t on) {
+    if (!F || (on != 0 && on != 1)) return LICA_BAD_ARG;
+    const size_t n = (size_t)F->nx * F->ny;
+    if (on) {
+        for (double*& d : F->dp_prev)
+            if (!d) {
+                const int rc = dalloc(&d, n);
+                if (rc != LICA_OK) return rc;
+            }
+    }
+    F->warm = on != 0;
+    for (bool& h : F->have_prev) h = false;
     return LICA_OK;
 }
 

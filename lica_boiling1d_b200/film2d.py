@@ -162,6 +162,11 @@ class Film2D:
         native.check(native.lib().lica_film2d_set_guess(self._h, net._h if net is not None else None),
                      "lica_film2d_set_guess")
 
+    def warm_start(self, on=True):
+        """Start each substep's pressure solve from the increment the same substep solved in
+        the previous step (zero in the first step); the kept increments are forgotten."""
+        native.check(native.lib().lica_film2d_set_warm_start(self._h, 1 if on else 0), "lica_film2d_set_warm_start")
+
     def capture(self, systems):
         """Record every step's three pressure systems into systems, a float64 CUDA tensor of
         3 * (4 nx ny + (ny + 1) nx) values (per substep: density, f, bx, by, dp); None: off."""

@@ -182,6 +182,7 @@ SIGNATURES = {
                                      C.c_int32]),
     "lica_film2d_destroy": (C.c_int, [C.c_void_p]),
     "lica_film2d_set_guess": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "lica_film2d_set_warm_start": (C.c_int, [C.c_void_p, C.c_int32]),
     "lica_film2d_capture_device": (C.c_int, [C.c_void_p, C.c_void_p]),
     "lica_film2d_step_device": (C.c_int, [C.c_void_p] * 6 + [C.c_double, C.POINTER(Film2DStats), C.c_void_p]),
     "lica_film2d_mdot_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

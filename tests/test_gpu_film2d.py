@@ -21,13 +21,15 @@ def _rel(a, b):
     return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
 
 
-def _run(nsteps, precision="fp64", nx=NX, ny=NY):
+def _run(nsteps, precision="fp64", nx=NX, ny=NY, warm=False):
     import torch
     from lica_boiling1d_b200 import film2d as G
     P = G.default_props()
     st0 = G.initial_state(nx, ny, y0_cells=8, amp_cells=2, props=P)
     dt = G.stable_dt(nx, P)
     gpu = G.Film2D(nx, ny, P, precision=precision)
+    if warm:
+        gpu.warm_start(True)
     dev = G.to_device(st0)
     infos = []
     for _ in range(nsteps):
@@ -61,6 +63,23 @@ def test_step_mixed_precision_pressure():
     assert infos[0]["status"] == [0, 0, 0] and max(infos[0]["rel"]) <= TOL
     errs = {k: _rel(got[k], ref[k]) for k in ref}
     assert all(e <= TOL for e in errs.values()), errs
+
+
+def test_warm_start_matches_oracle():
+    """Solves warm-started from the previous step's increment of the same substep stop at the
+    same 1e-10 residual, so after four steps every field meets the zero-start oracle's to 1e-9
+    (the solver paths differ, each within 1e-10), and from the second step on they take fewer
+    iterations in total than the solves from zero."""
+    got, ref, infos, rinfo, md = _run(4, warm=True)
+    cold = _run(4)[2]
+    for info in infos:
+        assert info["status"] == [0, 0, 0] and max(info["rel"]) <= TOL, info
+    errs = {k: _rel(got[k], ref[k]) for k in ref}
+    assert all(e <= 1e-9 for e in errs.values()), errs
+    assert infos[0]["iterations"] == cold[0]["iterations"]
+    warm_its = sum(sum(i["iterations"]) for i in infos[1:])
+    cold_its = sum(sum(i["iterations"]) for i in cold[1:])
+    assert warm_its < cold_its, (warm_its, cold_its)
 
 
 def test_bad_sizes_rejected():
