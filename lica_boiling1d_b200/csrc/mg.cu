@@ -1543,11 +1543,16 @@ struct lica_mg {
     cudaEvent_t b_ev_solved[2] = {nullptr, nullptr}, b_ev_out[2] = {nullptr, nullptr};
     cudaStream_t cap_stream = nullptr;  // graphs are captured here, launched on the caller's stream
     // graph cache
-    cudaGraphExec_t gexec = nullptr;
-    const void* gkey[4] = {nullptr, nullptr, nullptr, nullptr};
-    cudaStream_t gstream = nullptr;
-    double gtol = -1.0;
-    int gmax = -1;
+    // the solve's graph for the arrays, stream, tolerance and iteration cap of the last solve,
+    // and the one before it (a batch alternates between two staging buffers)
+    struct GraphSlot {
+        cudaGraphExec_t exec = nullptr;
+        const void* key[4] = {nullptr, nullptr, nullptr, nullptr};
+        cudaStream_t stream = nullptr;
+        double tol = -1.0;
+        int max = -1;
+    };
+    GraphSlot gcur, galt;
     int body_nodes = 0, setup_nodes = 0;
     // optional per-kernel-class timing (non-graph solves only)
     bool profile = false;
@@ -2117,9 +2122,9 @@ int build_graph(lica_mg* m, double* x, const double* f, const double* bx, const 
         bool p;
         ~Restore() { m->profile = p; }
     } restore{m, prof};
-    if (m->gexec) {
-        cudaGraphExecDestroy(m->gexec);
-        m->gexec = nullptr;
+    if (m->gcur.exec) {
+        cudaGraphExecDestroy(m->gcur.exec);
+        m->gcur = lica_mg::GraphSlot{};
     }
     cudaGraph_t g;
     LICA_CUDA_TRY(cudaGraphCreate(&g, 0));
@@ -2178,11 +2183,11 @@ int build_graph(lica_mg* m, double* x, const double* f, const double* bx, const 
     }
     // the captures counted as launches; undo that (replays are counted per run)
     lica_count_launches(-(int64_t)(m->setup_nodes + m->body_nodes));
-    e = cudaGraphInstantiate(&m->gexec, g, 0);
+    e = cudaGraphInstantiate(&m->gcur.exec, g, 0);
     cudaGraphDestroy(g);
     LICA_CUDA_TRY(e);
-    m->gkey[0] = x; m->gkey[1] = f; m->gkey[2] = bx; m->gkey[3] = by;
-    m->gstream = launch_stream;
+    m->gcur.key[0] = x; m->gcur.key[1] = f; m->gcur.key[2] = bx; m->gcur.key[3] = by;
+    m->gcur.stream = launch_stream;
     return LICA_OK;
 }
 
@@ -2200,15 +2205,21 @@ bool aligned16(const void* a, const void* b, const void* c, const void* d) {
 int graph_launch(lica_mg* m, double* x, const double* f, const double* bx, const double* by, double rtol, int max_it,
                  cudaStream_t s) {
     int st;
-    const bool same = m->gexec && m->gkey[0] == x && m->gkey[1] == f && m->gkey[2] == bx && m->gkey[3] == by &&
-                      m->gstream == s;
-    // rtol/max_it live in the graph's k_init_state node: rebuild when they change
-    if (!same || m->gtol != rtol || m->gmax != max_it) {
-        if ((st = build_graph(m, x, f, bx, by, rtol, max_it, s))) return st;
-        m->gtol = rtol;
-        m->gmax = max_it;
+    // rtol/max_it live in the graph's k_init_state node: a graph serves only its own
+    auto match = [&](const lica_mg::GraphSlot& g) {
+        return g.exec && g.key[0] == x && g.key[1] == f && g.key[2] == bx && g.key[3] == by && g.stream == s &&
+               g.tol == rtol && g.max == max_it;
+    };
+    if (!match(m->gcur)) {
+        // keep the current graph as the alternate; use the alternate if it fits, else build
+        std::swap(m->gcur, m->galt);
+        if (!match(m->gcur)) {
+            if ((st = build_graph(m, x, f, bx, by, rtol, max_it, s))) return st;
+            m->gcur.tol = rtol;
+            m->gcur.max = max_it;
+        }
     }
-    LICA_CUDA_TRY(cudaGraphLaunch(m->gexec, s));
+    LICA_CUDA_TRY(cudaGraphLaunch(m->gcur.exec, s));
     return LICA_OK;
 }
 
@@ -2501,7 +2512,8 @@ int lica_mg_create(lica_mg** out, int32_t nx, int32_t ny, double hx, double hy, 
 
 int lica_mg_destroy(lica_mg* m) {
     if (!m) return LICA_OK;
-    if (m->gexec) cudaGraphExecDestroy(m->gexec);
+    if (m->gcur.exec) cudaGraphExecDestroy(m->gcur.exec);
+    if (m->galt.exec) cudaGraphExecDestroy(m->galt.exec);
     for (auto& pe : m->prof_pending) {
         cudaEventDestroy(pe.second.first);
         cudaEventDestroy(pe.second.second);
@@ -2636,8 +2648,39 @@ int lica_mg_solve_host_batch(lica_mg* m, int32_t count, double* const* p, const 
         LICA_CUDA_TRY(cudaEventRecord(m->b_ev_in[b], m->b_up));
         return LICA_OK;
     };
-    int st = upload(0), worst = LICA_OK;
-    if (st) return st;
+    int st, worst = LICA_OK;
+    if (async) {
+        // Each system is solved where it was uploaded (its staging buffer holds p, f, bx, by;
+        // the solve's graph is cached for both buffers) and downloaded from there: no copies
+        // between buffers on the device, which would also push the solver's working set out
+        // of L2.  Upload k waits for the download of k - 2 from the same buffer, which follows
+        // its solve.
+        auto upload_in_place = [&](int32_t k) -> int {
+            const int b = k & 1;
+            double* in = m->b_in[b];
+            LICA_CUDA_TRY(cudaStreamWaitEvent(m->b_up, m->b_ev_out[b], 0));
+            LICA_CUDA_TRY(cudaMemcpyAsync(in, p[k], sizeof(double) * n, cudaMemcpyHostToDevice, m->b_up));
+            LICA_CUDA_TRY(cudaMemcpyAsync(in + n, f[k], sizeof(double) * n, cudaMemcpyHostToDevice, m->b_up));
+            LICA_CUDA_TRY(cudaMemcpyAsync(in + 2 * n, bx[k], sizeof(double) * n, cudaMemcpyHostToDevice, m->b_up));
+            LICA_CUDA_TRY(cudaMemcpyAsync(in + 3 * n, by[k], sizeof(double) * nb, cudaMemcpyHostToDevice, m->b_up));
+            LICA_CUDA_TRY(cudaEventRecord(m->b_ev_in[b], m->b_up));
+            return LICA_OK;
+        };
+        if ((st = upload_in_place(0))) return st;
+        for (int32_t k = 0; k < count; ++k) {
+            const int b = k & 1;
+            if (k + 1 < count && (st = upload_in_place(k + 1))) return st;
+            double* in = m->b_in[b];
+            LICA_CUDA_TRY(cudaStreamWaitEvent(s, m->b_ev_in[b], 0));
+            if ((st = graph_launch(m, in, in + n, in + 2 * n, in + 3 * n, rtol, max_iters, s))) return st;
+            LICA_CUDA_TRY(cudaMemcpyAsync(&m->b_states[k], m->st, sizeof(State), cudaMemcpyDeviceToHost, s));
+            LICA_CUDA_TRY(cudaEventRecord(m->b_ev_solved[b], s));
+            LICA_CUDA_TRY(cudaStreamWaitEvent(m->b_down, m->b_ev_solved[b], 0));
+            LICA_CUDA_TRY(cudaMemcpyAsync(p[k], in, sizeof(double) * n, cudaMemcpyDeviceToHost, m->b_down));
+            LICA_CUDA_TRY(cudaEventRecord(m->b_ev_out[b], m->b_down));
+        }
+    } else {
+    if ((st = upload(0))) return st;
     for (int32_t k = 0; k < count; ++k) {
         const int b = k & 1;
         // the next system's upload runs during this solve
@@ -2664,6 +2707,7 @@ int lica_mg_solve_host_batch(lica_mg* m, int32_t count, double* const* p, const 
         LICA_CUDA_TRY(cudaStreamWaitEvent(m->b_down, m->b_ev_solved[b], 0));
         LICA_CUDA_TRY(cudaMemcpyAsync(p[k], m->b_out[b], sizeof(double) * n, cudaMemcpyDeviceToHost, m->b_down));
         LICA_CUDA_TRY(cudaEventRecord(m->b_ev_out[b], m->b_down));
+    }
     }
     LICA_CUDA_TRY(cudaStreamSynchronize(m->b_down));
     LICA_CUDA_TRY(cudaStreamSynchronize(m->b_up));
