@@ -1781,8 +1781,23 @@ int column_ctas_by_registers() {
     return std::max(occ, 1);
 }
 
+// The CTA width when the caller leaves it open: 256 threads while the batch has at most one
+// column per SM (each column is a latency chain, and a wider CTA finishes its phases sooner),
+// 128 beyond that (more columns per SM).
+int default_width(int ncol) {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+                                                      cudaSuccess || sms < 1)
+            sms = 1;
+    }
+    return ncol <= sms ? 256 : colk::NT_DEFAULT;
+}
+
 int launch_columns(colk::Args& A, int nmax, int threads, void* stream, int cap_limit = -1) {
-    const int nth = (threads == 32 || threads == 64 || threads == 256) ? threads : colk::NT_DEFAULT;
+    const int nth = (threads == 32 || threads == 64 || threads == 128 || threads == 256) ? threads
+                                                                                          : default_width(A.ncol);
     // Shared-memory tridiagonal arrays for columns up to tri_cap cells, sized so that the
     // CTAs the registers allow per SM still fit (longer columns keep them in scratch; the
     // arithmetic is the same either way).
@@ -2118,6 +2133,11 @@ int column_steps_host(int32_t ncol, int32_t n, double length, const lica_col_pro
         host_bytes = total;
     }
     char* base = host_buf;
+    // copies and steps go on one stream of the library's, so the call waits once; a blocking
+    // stream, so it stays ordered after work a caller left on the legacy default stream that
+    // may use the same library scratch
+    static cudaStream_t host_stream = nullptr;
+    if (!host_stream) LICA_CUDA_TRY(cudaStreamCreateWithFlags(&host_stream, cudaStreamDefault));
     // Small states (a few columns: the per-step drop-in use) go through one page-locked
     // staging buffer, one copy each way instead of one per array; large ones copy directly.
     static char* pin_buf = nullptr;
@@ -2132,10 +2152,10 @@ int column_steps_host(int32_t ncol, int32_t n, double length, const lica_col_pro
     }
     if (packed) {
         for (int q = 0; q < nfld; ++q) std::memcpy(pin_buf + off[q], f[q].h, f[q].bytes);
-        LICA_CUDA_TRY(cudaMemcpy(base, pin_buf, st_off, cudaMemcpyHostToDevice));
+        LICA_CUDA_TRY(cudaMemcpyAsync(base, pin_buf, st_off, cudaMemcpyHostToDevice, host_stream));
     } else {
         for (int q = 0; q < nfld; ++q)
-            LICA_CUDA_TRY(cudaMemcpy(base + off[q], f[q].h, f[q].bytes, cudaMemcpyHostToDevice));
+            LICA_CUDA_TRY(cudaMemcpyAsync(base + off[q], f[q].h, f[q].bytes, cudaMemcpyHostToDevice, host_stream));
     }
     lica_col_state d;
     d.w = (double*)(base + off[0]);
@@ -2154,17 +2174,21 @@ int column_steps_host(int32_t ncol, int32_t n, double length, const lica_col_pro
     d.scal = (double*)(base + off[13]);
     d.stats = (double*)(base + off[14]);
     int32_t* dst = (int32_t*)(base + st_off);
-    int rc = column_steps_device(ncol, n, length, props, &d, nsteps, 0, nullptr, dst, nullptr, geo);
-    if (rc) return rc;
-    LICA_CUDA_TRY(cudaDeviceSynchronize());
+    int rc = column_steps_device(ncol, n, length, props, &d, nsteps, 0, nullptr, dst, host_stream, geo);
+    if (rc) {
+        cudaStreamSynchronize(host_stream);
+        return rc;
+    }
     if (packed) {
-        LICA_CUDA_TRY(cudaMemcpy(pin_buf, base, total, cudaMemcpyDeviceToHost));
+        LICA_CUDA_TRY(cudaMemcpyAsync(pin_buf, base, total, cudaMemcpyDeviceToHost, host_stream));
+        LICA_CUDA_TRY(cudaStreamSynchronize(host_stream));
         for (int q = 0; q < nfld; ++q) std::memcpy(f[q].h, pin_buf + off[q], f[q].bytes);
         std::memcpy(status, pin_buf + st_off, 4 * nc);
     } else {
         for (int q = 0; q < nfld; ++q)
-            LICA_CUDA_TRY(cudaMemcpy(f[q].h, base + off[q], f[q].bytes, cudaMemcpyDeviceToHost));
-        LICA_CUDA_TRY(cudaMemcpy(status, dst, 4 * nc, cudaMemcpyDeviceToHost));
+            LICA_CUDA_TRY(cudaMemcpyAsync(f[q].h, base + off[q], f[q].bytes, cudaMemcpyDeviceToHost, host_stream));
+        LICA_CUDA_TRY(cudaMemcpyAsync(status, dst, 4 * nc, cudaMemcpyDeviceToHost, host_stream));
+        LICA_CUDA_TRY(cudaStreamSynchronize(host_stream));
     }
     int worst = LICA_OK;
     for (size_t c = 0; c < nc; ++c)
