@@ -148,3 +148,11 @@ def format_records(recs):
     for r in recs:
         lines.append("%15.7E%5d" % (r["time"], r["llvs"]) + "".join("%15.7E" % c for c in r["col"]))
     return lines
+
+
+def append_records(path, recs):
+    """Append the records to a 0bub_tracking.dat file as BUBBLE_TRACKING does (OPEN with
+    POSITION='APPEND', one WRITE per level set; two_phase.f:6440-6443)."""
+    with open(path, "a") as fh:
+        for line in format_records(recs):
+            fh.write(line + "\n")

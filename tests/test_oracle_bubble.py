@@ -5,7 +5,7 @@ empty level set."""
 import numpy as np
 import pytest
 
-from lica_boiling1d_b200.bubbles import BubbleGrid, format_records
+from lica_boiling1d_b200.bubbles import BubbleGrid, append_records, format_records
 from oracle import oracle
 from tests import bubble_cases as bc
 
@@ -135,3 +135,16 @@ def test_format_records():
     line = format_records(rec)[0]
     assert len(line) == 15 + 5 + 9 * 15
     assert line.startswith("  1.5000000E+00    3  0.0000000E+00  5.0000000E-01")
+
+
+def test_append_records(tmp_path):
+    """Two calls append two lines each, in the reference's record format."""
+    grid, psi, (u, v, w) = bc.three_bubbles()
+    rec = _orc(grid, psi[:2], u, v, w, time=0.5, llvs0=1)
+    path = tmp_path / "0bub_tracking.dat"
+    append_records(path, rec)
+    append_records(path, rec)
+    lines = path.read_text().splitlines()
+    assert lines == format_records(rec) * 2
+    assert [int(x[15:20]) for x in lines] == [1, 2, 1, 2]
+    assert float(lines[0][20:35]) == pytest.approx(rec[0]["col"][0], rel=1e-7)
