@@ -51,7 +51,9 @@ def _close(gpu, ref):
 @pytest.mark.parametrize("icacy", [1, 2])
 def test_three_level_sets(icacy):
     grid, psi, (u, v, w) = bc.three_bubbles(seed=1)
-    grid.xp = grid.xp - 0.6
+    # the axis passes beside every bubble: a centroid on it (x = 0 up to rounding) would
+    # leave theta to the sign of a rounding error
+    grid.xp = grid.xp - 0.55
     grid.yp = grid.yp - 0.5
     got = bubbles.track(grid, psi, u, v, w, time=0.125, icacy=icacy, llvs0=2)
     _close(got, _orc(grid, psi, u, v, w, time=0.125, icacy=icacy, llvs0=2))
