@@ -382,7 +382,7 @@ __device__ __forceinline__ double up_body(const RBCells<T, RBCfg<NSW, TXX, TYY, 
 }
 
 template <typename T, int NSW, int TXX, int TYY, int R, bool LEVEL0>
-__global__ void __launch_bounds__(RBCfg<NSW, TXX, TYY, R>::NTH, 2)
+__global__ void __launch_bounds__(RBCfg<NSW, TXX, TYY, R>::NTH, std::is_same<T, float>::value ? 3 : 2)
     k_up(const T* __restrict__ u_pre, T* __restrict__ u_post, const T* __restrict__ uc, const T* __restrict__ f,
          const T* __restrict__ ax, const T* __restrict__ ay, const T* __restrict__ dinv, int nx, int ny,
          State* __restrict__ st, double* __restrict__ partials) {
