@@ -161,47 +161,47 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------ RK3 column legs
-C1 = dict(n=512, z0=0.1, denr=1000.0, visr=20.0, tcr=25.0, jakob=0.009, cflmax=0.3, steps=2000)
-C4_NCOL = 4096
+COLUMN512 = dict(n=512, z0=0.1, denr=1000.0, visr=20.0, tcr=25.0, jakob=0.009, cflmax=0.3, steps=2000)
+BATCH_NCOL = 4096
 
 
-def c1_props():
+def column512_props():
     from lica_boiling1d_b200.column import ColumnProps
-    return ColumnProps(denr=C1["denr"], visr=C1["visr"], tcr=C1["tcr"], jakob=C1["jakob"], cflmax=C1["cflmax"])
+    return ColumnProps(denr=COLUMN512["denr"], visr=COLUMN512["visr"], tcr=COLUMN512["tcr"], jakob=COLUMN512["jakob"], cflmax=COLUMN512["cflmax"])
 
 
-def c1_oracle(steps):
-    """Config 1 on the CPU restatement, one thread (as the reference's 1-D case runs): the
+def column512_oracle(steps):
+    """The 512-cell column on the CPU restatement, one thread (as the reference's 1-D case runs): the
     final state, the per-step interface history (TIME, place, VOL_TOT_IPHS, DT) and the
     seconds the steps took."""
     from oracle import oracle
-    props = c1_props()
-    st = oracle.col_init(C1["n"], 1.0, C1["z0"], props)
+    props = column512_props()
+    st = oracle.col_init(COLUMN512["n"], 1.0, COLUMN512["z0"], props)
     hist = np.zeros((steps, 4))
     t0 = time.perf_counter()
     for s in range(steps):
         tb = float(st["scal"][1])
-        if oracle.col_step(st, C1["n"], 1.0, props, native=True) != 0:
+        if oracle.col_step(st, COLUMN512["n"], 1.0, props, native=True) != 0:
             raise RuntimeError(f"oracle column step {s + 1} failed")
         hist[s] = oracle.col_history_record(st, tb, native=True)
     return st, hist, time.perf_counter() - t0
 
 
-def rk3_cpu(c1_steps=C1["steps"]):
-    """The CPU restatement's time for the same steps: the whole config-1 run of the 512-cell
+def rk3_cpu(col_steps_n=COLUMN512["steps"]):
+    """The CPU restatement's time for the same steps: the whole run of the 512-cell
     column (single thread), and a sample of the uneven batch run over all host cores
     (independent columns; the oracle releases the GIL).  Returns the figures and, apart,
-    the config-1 final state and history."""
+    the final state and history."""
     from concurrent.futures import ThreadPoolExecutor
 
     from lica_boiling1d_b200.column import uneven_batch
     from oracle import oracle
     oracle.lib(native=True)
-    c1_state, c1_hist, c1_s = c1_oracle(c1_steps)
-    c1 = c1_steps / c1_s
-    k = c1_steps
-    n, length, z0, bprops = uneven_batch(C4_NCOL, seed=0)
-    sample = list(range(0, C4_NCOL, max(1, C4_NCOL // 256)))
+    col_state, col_hist, col_s = column512_oracle(col_steps_n)
+    col_rate = col_steps_n / col_s
+    k = col_steps_n
+    n, length, z0, bprops = uneven_batch(BATCH_NCOL, seed=0)
+    sample = list(range(0, BATCH_NCOL, max(1, BATCH_NCOL // 256)))
     states = {c: oracle.col_init(int(n[c]), float(length[c]), float(z0[c]), bprops[c]) for c in sample}
     cores = os.cpu_count()
 
@@ -216,10 +216,10 @@ def rk3_cpu(c1_steps=C1["steps"]):
         dt = time.perf_counter() - t0
     cells = float(np.mean([n[c] for c in sample]))
     col_steps = done / dt
-    return {"c1_steps_per_s": c1, "c1_sample": f"all {k} steps of config 1 (512-cell column, CFL 0.3), one thread",
-            "batch_column_steps_per_s": col_steps, "batch_steps_per_s": col_steps / C4_NCOL,
+    return {"column_512_steps_per_s": col_rate, "column_512_sample": f"all {k} steps of the 512-cell column (CFL 0.3), one thread",
+            "batch_column_steps_per_s": col_steps, "batch_steps_per_s": col_steps / BATCH_NCOL,
             "batch_cell_updates_per_s": col_steps * cells, "cores": cores,
-            "batch_sample": f"{len(sample)} of the {C4_NCOL} columns x 2 steps on {cores} threads"}, (c1_state, c1_hist)
+            "batch_sample": f"{len(sample)} of the {BATCH_NCOL} columns x 2 steps on {cores} threads"}, (col_state, col_hist)
 
 
 def profile_batch(ncol, steps, threads):
@@ -258,7 +258,7 @@ def column_roofline(state_bytes, ms_per_step, kernel):
                     "the per-phase cycle profile is the lica_gpu_column_profile_device record"}
 
 
-def rk3_legs(dev, flush, steps_c1=C1["steps"], steps_c4=1000, warmup=3, rank=0, world=1, slowest=lambda x: x,
+def rk3_legs(dev, flush, steps_col=COLUMN512["steps"], steps_batch=1000, warmup=3, rank=0, world=1, slowest=lambda x: x,
              film_steps=10, film_compare=False):
     import torch
 
@@ -266,21 +266,21 @@ def rk3_legs(dev, flush, steps_c1=C1["steps"], steps_c4=1000, warmup=3, rank=0, 
     from lica_boiling1d_b200 import native, shard
     from lica_boiling1d_b200.column import ColumnBatch, Columns, uneven_batch
     out = {}
-    props = c1_props()
-    # C1: one column from its initial state, one persistent launch of steps_c1 steps that
+    props = column512_props()
+    # the 512-cell column: one column from its initial state, one persistent launch of steps_col steps that
     # records the interface history (warm-up on a separate copy)
-    col0 = Columns.film(C1["n"], 1.0, [C1["z0"]], props)
+    col0 = Columns.film(COLUMN512["n"], 1.0, [COLUMN512["z0"]], props)
     warm = col0.to(dev)
     warm.steps(warmup, props, threads=256)
     col = col0.to(dev)
-    hist = torch.zeros((1, steps_c1, 4), dtype=torch.float64, device=dev)
+    hist = torch.zeros((1, steps_col, 4), dtype=torch.float64, device=dev)
     torch.cuda.synchronize(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     flush.fill_(3)
     l0 = native.launch_count()
     colmod.history(hist)
     e0.record()
-    st = col.steps(steps_c1, props, threads=256)
+    st = col.steps(steps_col, props, threads=256)
     e1.record()
     torch.cuda.synchronize(dev)
     colmod.history(None)
@@ -289,17 +289,17 @@ def rk3_legs(dev, flush, steps_c1=C1["steps"], steps_c4=1000, warmup=3, rank=0, 
         raise RuntimeError(f"column step status {int(st.max())}")
     ms = e0.elapsed_time(e1)
     out["column_512"] = {
-        "workload": "config 1: 1-D boiling column, 512 uniform flow cells (1024 refined), film 0.1 L, density ratio "
+        "workload": "1-D boiling column, 512 uniform flow cells (1024 refined), film 0.1 L, density ratio "
                     "1000, viscosity ratio 20, conductivity ratio 25, Jakob 0.009 (10 K), RK3 at CFL 0.3, "
-                    f"{steps_c1} steps from the initial state in one persistent launch, FP64, 1-D POISSON exact",
-        "steps_per_s": steps_c1 / (ms / 1e3), "ms_per_step": ms / steps_c1, "steps": steps_c1, "threads": 256,
-        "cell_updates_per_s": C1["n"] * steps_c1 / (ms / 1e3), "gpu_launches": launches,
+                    f"{steps_col} steps from the initial state in one persistent launch, FP64, 1-D POISSON exact",
+        "steps_per_s": steps_col / (ms / 1e3), "ms_per_step": ms / steps_col, "steps": steps_col, "threads": 256,
+        "cell_updates_per_s": COLUMN512["n"] * steps_col / (ms / 1e3), "gpu_launches": launches,
         "interface_height": float(col.to(None).stats[0][5])}
-    out["_c1_gpu"] = (col.to(None), hist[0].cpu().numpy())
+    out["_column_gpu"] = (col.to(None), hist[0].cpu().numpy())
     # end to end: the host-array C-ABI entry, one step per call (state copied in and out)
     host = warm.to(None)
     pinned = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in host.arrays.items()}
-    hcol = Columns(C1["n"], 1.0, pinned)
+    hcol = Columns(COLUMN512["n"], 1.0, pinned)
     ke = 20
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
@@ -307,13 +307,13 @@ def rk3_legs(dev, flush, steps_c1=C1["steps"], steps_c4=1000, warmup=3, rank=0, 
         hcol.steps(1, props)
     e2e_s = time.perf_counter() - t0
     bytes_state = sum(a.nbytes for a in pinned.values())
-    out["column_512"]["roofline"] = column_roofline(bytes_state, ms / steps_c1, "k_column_steps<256>")
+    out["column_512"]["roofline"] = column_roofline(bytes_state, ms / steps_col, "k_column_steps<256>")
     out["column_512"]["e2e"] = {"steps_per_s": ke / e2e_s, "h2d_bytes_per_step": bytes_state,
                                 "d2h_bytes_per_step": bytes_state,
                                 "path": "lica_gpu_column_steps (C ABI), host arrays, one step per call"}
-    # C4: the uneven batch (over N ranks: contiguous blocks balanced by cells, no collective
+    # the 4096-column batch: the uneven batch (over N ranks: contiguous blocks balanced by cells, no collective
     # per step), CTA width picked by a short trial of each candidate
-    n_all, length, z0, bprops = uneven_batch(C4_NCOL, seed=0)
+    n_all, length, z0, bprops = uneven_batch(BATCH_NCOL, seed=0)
     lo, hi = shard.partition(n_all, world)[rank]
     n = n_all[lo:hi]
     batch = ColumnBatch.films(n, length[lo:hi], z0[lo:hi], bprops[lo:hi]).to(dev)
@@ -324,7 +324,7 @@ def rk3_legs(dev, flush, steps_c1=C1["steps"], steps_c4=1000, warmup=3, rank=0, 
     flush.fill_(5)
     l0 = native.launch_count()
     e0.record()
-    st = batch.steps(steps_c4, threads=th, tri_cap=cap)
+    st = batch.steps(steps_batch, threads=th, tri_cap=cap)
     e1.record()
     torch.cuda.synchronize(dev)
     launches = native.launch_count() - l0
@@ -338,12 +338,12 @@ def rk3_legs(dev, flush, steps_c1=C1["steps"], steps_c4=1000, warmup=3, rank=0, 
                                    for c in range(len(n))], world)
     batch_bytes = sum(int(a.numel()) * a.element_size() for a in batch.arrays.values())
     out["batch_4096"] = {
-        "roofline": column_roofline(batch_bytes, ms / steps_c4, f"k_column_steps<{th}>"),
-        "workload": f"config 4: {C4_NCOL} independent 1-D boiling columns, uneven 128-2048 flow cells (seeded, "
+        "roofline": column_roofline(batch_bytes, ms / steps_batch, f"k_column_steps<{th}>"),
+        "workload": f"{BATCH_NCOL} independent 1-D boiling columns, uneven 128-2048 flow cells (seeded, "
                     f"{cells} in total), superheat 2-20 K, density ratio 100-1600, FP64 (the 1-D pressure solve is "
-                    f"the exact Thomas sweep), {steps_c4} RK3 steps in one persistent launch per rank, longest first",
-        "steps_per_s": steps_c4 / (ms / 1e3), "ms_per_step": ms / steps_c4, "steps": steps_c4,
-        "column_steps_per_s": C4_NCOL * steps_c4 / (ms / 1e3), "cell_updates_per_s": cells * steps_c4 / (ms / 1e3),
+                    f"the exact Thomas sweep), {steps_batch} RK3 steps in one persistent launch per rank, longest first",
+        "steps_per_s": steps_batch / (ms / 1e3), "ms_per_step": ms / steps_batch, "steps": steps_batch,
+        "column_steps_per_s": BATCH_NCOL * steps_batch / (ms / 1e3), "cell_updates_per_s": cells * steps_batch / (ms / 1e3),
         "threads": th, "tri_cap": cap, "autotune_ms_per_step": trial,
         "autotune": "lica_boiling1d_b200.autotune: CTA width 64/128/256 x Thomas arrays in shared memory or "
                     "scratch, timed on a copy of the batch, cached per GPU",
@@ -478,10 +478,10 @@ def film_leg(dev, flush, steps=10, warmup=2, compare=True):
     net = None
     from lica_boiling1d_b200 import train_guess
     arms = ["fp64", "mixed", "fp64_warm", "mixed_warm"]
-    if os.path.exists(train_guess.CONFIG_WEIGHTS):
+    if os.path.exists(train_guess.SOLVER_PAIR_WEIGHTS):
         from lica_boiling1d_b200.unet import LearnedGuess
         net = LearnedGuess(1, ny, nx)
-        train_guess.load(net, train_guess.CONFIG_WEIGHTS)
+        train_guess.load(net, train_guess.SOLVER_PAIR_WEIGHTS)
         arms.append("mixed_learned")
     for arm in arms:
         prec = "fp64" if arm.startswith("fp64") else "mixed"
@@ -520,8 +520,8 @@ def film_leg(dev, flush, steps=10, warmup=2, compare=True):
         if arm == "mixed_learned":
             out[arm]["guess_rel_per_substep"] = grels[-1]
             out[arm]["mean_iterations_saved_vs_mixed"] = float(np.mean(out["mixed"]["_its"]) - np.mean(its))
-            out[arm]["note"] = ("mixed-precision MG-PCG started from the U-Net guess trained on 20,000 config-2 "
-                                "(1024^2) and config-3 (this film's own systems) pairs; zero where the guess is "
+            out[arm]["note"] = ("mixed-precision MG-PCG started from the U-Net guess trained on 20,000 "
+                                "1024^2 bubble-Poisson and 512 x 1536 film (this film's own systems) pairs; zero where the guess is "
                                 "no better")
         if arm.endswith("_warm"):
             out[arm]["mean_iterations_saved_vs_cold"] = float(np.mean(out[prec]["_its"]) - np.mean(its))
@@ -654,22 +654,22 @@ def run_ours(args):
     e2e, roofline, variants, cpu = None, None, {}, None
     rk3 = None
     if not args.skip_rk3:
-        rk3 = rk3_legs(dev, flush, steps_c1=args.c1_steps, steps_c4=args.c4_steps, rank=rank, world=world,
+        rk3 = rk3_legs(dev, flush, steps_col=args.column_steps, steps_batch=args.batch_steps, rank=rank, world=world,
                        slowest=slowest, film_steps=args.film_steps,
                        film_compare=(rank == 0 and world == 1 and not args.skip_cpu))
-        c1_gpu_state, c1_gpu_hist = rk3.pop("_c1_gpu")
+        col_gpu_state, col_gpu_hist = rk3.pop("_column_gpu")
         if rank == 0 and world == 1 and not args.skip_cpu:
-            rk3["cpu_baseline"], (c1_ref, c1_ref_hist) = rk3_cpu(args.c1_steps)
+            rk3["cpu_baseline"], (col_ref, col_ref_hist) = rk3_cpu(args.column_steps)
             rk3["cpu_baseline"]["kind"] = "port"
-            same = {k: bool(np.array_equal(c1_gpu_state.arrays[k][0], v)) for k, v in c1_ref.items()}
+            same = {k: bool(np.array_equal(col_gpu_state.arrays[k][0], v)) for k, v in col_ref.items()}
             rk3["column_512"]["vs_oracle"] = {
-                "history_steps_compared": int(c1_ref_hist.shape[0]),
-                "history_bit_identical": bool(np.array_equal(c1_gpu_hist, c1_ref_hist)),
-                "history_max_abs_diff": {name: float(np.abs(c1_gpu_hist[:, q] - c1_ref_hist[:, q]).max())
+                "history_steps_compared": int(col_ref_hist.shape[0]),
+                "history_bit_identical": bool(np.array_equal(col_gpu_hist, col_ref_hist)),
+                "history_max_abs_diff": {name: float(np.abs(col_gpu_hist[:, q] - col_ref_hist[:, q]).max())
                                          for q, name in enumerate(("time", "place", "vapour_volume", "dt"))},
                 "final_state_bit_identical": all(same.values()),
-                "final_interface_place": float(c1_ref_hist[-1, 1]),
-                "final_vapour_volume": float(c1_ref_hist[-1, 2]),
+                "final_interface_place": float(col_ref_hist[-1, 1]),
+                "final_vapour_volume": float(col_ref_hist[-1, 2]),
                 "note": "interface history = the reference's 0interface.dat (TIME, place) and VOL_TOT_IPHS per step"}
     if args.no_e2e:
         return finish(args, locals())
@@ -841,10 +841,10 @@ def learned_leg(args, dev, case, n, nlevels, f, bx, by, p, flush, stream, reps):
 
     from lica_boiling1d_b200 import poisson, train_guess
     from lica_boiling1d_b200.unet import LearnedGuess
-    if not os.path.exists(train_guess.CONFIG_WEIGHTS):
+    if not os.path.exists(train_guess.SOLVER_PAIR_WEIGHTS):
         return {"unavailable": "no trained weights in the package"}
     net = LearnedGuess(1, n, n)
-    train_guess.load(net, train_guess.CONFIG_WEIGHTS)
+    train_guess.load(net, train_guess.SOLVER_PAIR_WEIGHTS)
     rho = torch.from_numpy(case.rho[None].copy()).to(dev)
     F, BX, BY = f[None], bx[None], by[None]
     x0 = torch.empty_like(F)
@@ -875,7 +875,7 @@ def learned_leg(args, dev, case, n, nlevels, f, bx, by, p, flush, stream, reps):
                     "note": "10 tcgen05 convolutions (BF16, FP32 accumulate) + pooling/upsampling/head"}
     _, rel0 = net.guess_checked(rho, F, BX, BY, case.hx, case.hy, out=x0)
     out["guess"]["rel_residual"] = float(rel0[0])
-    out["guess"]["weights"] = "config 5: 20,000 pairs from config-2 and config-3 solves (unet_guess_configs.npy)"
+    out["guess"]["weights"] = "20,000 pairs from 1024^2 bubble-Poisson and 512 x 1536 film solves (unet_guess_solver_pairs.npy)"
     if os.path.exists(train_guess.WEIGHTS):
         # the same network trained on 16,000 256^2 bubble problems only, for comparison
         alt = LearnedGuess(1, n, n)
@@ -1023,14 +1023,14 @@ def main():
     ap.add_argument("--skip-bubbles", action="store_true", help="skip the 3-D bubble-statistics leg")
     ap.add_argument("--profile-guess", type=int, default=0,
                     help="only run this many U-Net guesses at 1024x1024 (profiling) and exit")
-    ap.add_argument("--c1-steps", type=int, default=C1["steps"], help="timed steps of the 512-cell column")
-    ap.add_argument("--c4-steps", type=int, default=1000, help="timed steps of the 4096-column batch")
+    ap.add_argument("--column-steps", type=int, default=COLUMN512["steps"], help="timed steps of the 512-cell column")
+    ap.add_argument("--batch-steps", type=int, default=1000, help="timed steps of the 4096-column batch")
     ap.add_argument("--film-steps", type=int, default=10, help="timed steps of the 2-D film (0: skip the leg)")
     ap.add_argument("--profile-film", type=int, default=0, help="run N 2-D film steps only (ncu launch lists)")
     ap.add_argument("--profile-bubbles", type=int, default=0,
                     help="run N bubble-statistics launches only (256^3, four level sets; for ncu)")
     ap.add_argument("--profile-batch", type=int, default=0,
-                    help="only run NCOL columns of the uneven batch (profiling runs); see --c4-steps, --threads")
+                    help="only run NCOL columns of the uneven batch (profiling runs); see --batch-steps, --threads")
     ap.add_argument("--threads", type=int, default=64, help="column CTA width for --profile-batch")
     ap.add_argument("--no-graph", action="store_true",
                     help="launch kernels one by one instead of one CUDA graph per solve (for ncu, which cannot "
@@ -1039,7 +1039,7 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     if args.profile_batch:
-        profile_batch(args.profile_batch, args.c4_steps, args.threads)
+        profile_batch(args.profile_batch, args.batch_steps, args.threads)
         return
     if args.profile_guess:
         profile_guess(args.profile_guess)

@@ -25,9 +25,9 @@ from .inputs import bubble_density, face_beta
 HERE = os.path.dirname(os.path.abspath(__file__))
 WEIGHTS = os.path.join(HERE, "weights", "unet_guess.npy")
 FILM_WEIGHTS = os.path.join(HERE, "weights", "unet_guess_film.npy")
-# config 5's training set: 20,000 pairs from config-2 (1024^2) and config-3 (512 x 1536 film)
-# solves (train_configs); the weights the benchmark's learned legs use
-CONFIG_WEIGHTS = os.path.join(HERE, "weights", "unet_guess_configs.npy")
+# 20,000 pairs from 1024^2 bubble-Poisson solves and 512 x 1536 film solves
+# (train_solver_pairs); the weights the benchmark's learned legs use
+SOLVER_PAIR_WEIGHTS = os.path.join(HERE, "weights", "unet_guess_solver_pairs.npy")
 
 
 def problem(rng, n, ny=None, *, bubbles_per_1024sq=64, rmin=8.0, rmax=48.0):
@@ -105,7 +105,7 @@ def train(net, steps, n, lr=1e-3, seed=0, log_every=100, log=print, lr_final=Non
 
 def film_pairs(nx, ny, steps, props=None, warm=2):
     """(rho, f, bx, by, dp) pressure systems of the 2-D film step's own solves: a film of nx x ny
-    (interface at ny/24 cells, amplitude nx/128 cells -- config 3's shape at any size) run for
+    (interface at ny/24 cells, amplitude nx/128 cells -- the 512 x 1536 film's shape at any size) run for
     warm + steps RK3 steps on the GPU; the three substeps' systems of each of the last steps,
     as CUDA tensors (a list of dicts)."""
     import torch
@@ -150,16 +150,16 @@ def train_film(net, steps, nx, ny, lr=1e-3, lr_final=1e-4, seed=0, pool_steps=64
     return hist
 
 
-def train_configs(pairs=20000, n2=1024, film=(512, 1536), images=4, lr=1e-3, lr_final=1e-4, seed=0, chunk=200,
-                  log=print, checkpoint=None):
-    """Config 5's training set: (density, RHS -> pressure) pairs from config-2 solves (n2 x n2,
+def train_solver_pairs(pairs=20000, n2=1024, film=(512, 1536), images=4, lr=1e-3, lr_final=1e-4, seed=0, chunk=200,
+                       log=print, checkpoint=None):
+    """The solver-pair training set: (density, RHS -> pressure) pairs from bubble-Poisson solves (n2 x n2,
     the benchmark's bubble distribution built on the GPU, each problem solved to 1e-10 by the
     multigrid) and
-    from config-3 solves (the 2-D film step's own three pressure systems per step at its full
+    from film solves (the 2-D film step's own three pressure systems per step at its full
     size, captured as the film runs), half each, interleaved in chunks of `chunk` Adam steps.
     One set of weights (the network is dimensionless); each grid shape keeps its own Adam
     moments, and the weights move between the two at every switch (and to `checkpoint`, a
-    .npy path, if given).  Returns (params, loss history per config)."""
+    .npy path, if given).  Returns (params, loss history per source)."""
     import torch
     from . import film2d as G
     from . import poisson
@@ -181,7 +181,7 @@ def train_configs(pairs=20000, n2=1024, film=(512, 1536), images=4, lr=1e-3, lr_
     steps2 = pairs // 2 // images
     steps3 = pairs // 2 // 3
     total = steps2 + steps3
-    hist = {"config2": [], "config3": []}
+    hist = {"bubbles": [], "film": []}
     done2 = done3 = 0
     cur = 2
     t0 = time.time()
@@ -204,8 +204,8 @@ def train_configs(pairs=20000, n2=1024, film=(512, 1536), images=4, lr=1e-3, lr_
                     for i in range(images):
                         _, _, st = solver.solve(ps[i], f[i], bx[i], by[i], rtol=1e-10, max_iters=200)
                         if st != 0:
-                            raise RuntimeError(f"solver status {st} on a config-2 training problem")
-                    hist["config2"].append(net.train_step(rho, f, bx, by, h2, h2, lr_it, p_star=ps))
+                            raise RuntimeError(f"solver status {st} on a bubble-Poisson training problem")
+                    hist["bubbles"].append(net.train_step(rho, f, bx, by, h2, h2, lr_it, p_star=ps))
                     done2 += 1
                 else:
                     if done3 >= steps3:
@@ -216,7 +216,7 @@ def train_configs(pairs=20000, n2=1024, film=(512, 1536), images=4, lr=1e-3, lr_
                     sys3 = fgpu.unpack_capture(buf)
                     rho, f, bx, by, dp = (torch.stack([q[k] for q in sys3]).contiguous()
                                           for k in ("rho", "f", "bx", "by", "dp"))
-                    hist["config3"].append(net.train_step(rho, f, bx, by, 1.0 / nx, 1.0 / nx, lr_it, p_star=dp))
+                    hist["film"].append(net.train_step(rho, f, bx, by, 1.0 / nx, 1.0 / nx, lr_it, p_star=dp))
                     done3 += 1
             other = net3 if cur == 2 else net2
             params = net.get_params()
@@ -224,9 +224,9 @@ def train_configs(pairs=20000, n2=1024, film=(512, 1536), images=4, lr=1e-3, lr_
             if checkpoint:
                 np.save(checkpoint, params)
             if log:
-                l2 = np.mean(hist["config2"][-50:]) if hist["config2"] else 0.0
-                l3 = np.mean(hist["config3"][-50:]) if hist["config3"] else 0.0
-                log(f"pairs {images * done2 + 3 * done3:6d}  config-2 loss {l2:.4e}  config-3 loss {l3:.4e}  "
+                l2 = np.mean(hist["bubbles"][-50:]) if hist["bubbles"] else 0.0
+                l3 = np.mean(hist["film"][-50:]) if hist["film"] else 0.0
+                log(f"pairs {images * done2 + 3 * done3:6d}  bubble loss {l2:.4e}  film loss {l3:.4e}  "
                     f"({time.time() - t0:.1f} s)")
             cur = 3 if cur == 2 else 2
         params = (net2 if cur == 3 else net3).get_params()
@@ -283,12 +283,12 @@ def main():
     ap.add_argument("--film", action="store_true",
                     help="train on the 2-D film step's own pressure systems (writes the film weights)")
     ap.add_argument("--film-nx", type=int, default=256)
-    ap.add_argument("--configs", type=int, default=0, metavar="PAIRS",
-                    help="train on PAIRS pairs from config-2 (1024^2) and config-3 (512 x 1536 film) solves")
+    ap.add_argument("--solver-pairs", type=int, default=0, metavar="PAIRS",
+                    help="train on PAIRS pairs from 1024^2 bubble-Poisson and 512 x 1536 film solves")
     a = ap.parse_args()
     from .unet import LearnedGuess
-    if a.configs:
-        params, _ = train_configs(a.configs, images=a.batch, lr=a.lr, lr_final=a.lr_final, seed=a.seed)
+    if a.solver_pairs:
+        params, _ = train_solver_pairs(a.solver_pairs, images=a.batch, lr=a.lr, lr_final=a.lr_final, seed=a.seed)
         os.makedirs(os.path.dirname(a.out), exist_ok=True)
         np.save(a.out, params)
         return

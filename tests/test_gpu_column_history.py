@@ -20,7 +20,7 @@ pytestmark = pytest.mark.gpu
 N, Z0, STEPS = 512, 0.1, 2000
 
 
-def c1_props():
+def column512_props():
     return ColumnProps(denr=1000.0, visr=20.0, tcr=25.0, jakob=0.009, cflmax=0.3)
 
 
@@ -36,7 +36,7 @@ def oracle_run(props, steps):
 
 def test_config1_history_2000_steps_bitwise():
     import torch
-    props = c1_props()
+    props = column512_props()
     ref, ref_hist = oracle_run(props, STEPS)
     cols = Columns.film(N, 1.0, [Z0], props).to("cuda")
     hist = torch.full((1, STEPS, 4), float("nan"), dtype=torch.float64, device="cuda")
@@ -64,7 +64,7 @@ def test_history_off_leaves_no_record_and_same_state():
     """The recorder changes nothing in the step: the same steps with and without it give
     the same state; with it off nothing is written."""
     import torch
-    props = c1_props()
+    props = column512_props()
     a = Columns.film(64, 1.0, [0.1], props).to("cuda")
     b = a.to("cuda")
     hist = torch.full((1, 8, 4), -1.0, dtype=torch.float64, device="cuda")

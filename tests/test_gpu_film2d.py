@@ -90,7 +90,7 @@ def test_bad_sizes_rejected():
 
 
 def test_config_size_step_matches_oracle():
-    """Config 3 at its own size, 512 x 1536 (level set 1024 x 3072), one FP64 step against the
+    """The film at its full size, 512 x 1536 (level set 1024 x 3072), one FP64 step against the
     C++ restatement (oracle/film2d.cpp, bit-identical to the numpy one).  The level set, the
     temperature and v meet 1e-10 relative L2.  The pressure solves of this size stop at FP64's
     attainable accuracy (LICA_STALLED near 3e-10: rounding the converged increment alone leaves

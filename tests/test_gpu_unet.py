@@ -194,17 +194,17 @@ def test_learned_guess_on_film_systems_falls_back_and_costs_no_iterations():
     ev.close()
 
 
-def test_config5_weights_on_held_out_config2_problems():
-    """The shipped config-5 weights (20,000 pairs from config-2 and config-3 solves,
-    train_guess.train_configs): on held-out 1024^2 problems of config 2's distribution the
-    guess's relative residual is below zero's (measured 0.35-0.36), and the PCG from it
-    reaches 1e-10 in no more iterations than from zero."""
+def test_solver_pair_weights_on_held_out_bubble_problems():
+    """The shipped solver-pair weights (20,000 pairs from 1024^2 bubble-Poisson and 512 x 1536
+    film solves, train_guess.train_solver_pairs): on held-out 1024^2 problems of the benchmark's
+    bubble distribution the guess's relative residual is below zero's (measured 0.35-0.36), and
+    the PCG from it reaches 1e-10 in no more iterations than from zero."""
     import torch
     from lica_boiling1d_b200 import train_guess as T
     from lica_boiling1d_b200.unet import LearnedGuess
     n = 1024
     net = LearnedGuess(1, n, n)
-    T.load(net, T.CONFIG_WEIGHTS)
+    T.load(net, T.SOLVER_PAIR_WEIGHTS)
     rng = np.random.default_rng(777)
     probs = [T.problem(rng, n) for _ in range(2)]
     rels = []
