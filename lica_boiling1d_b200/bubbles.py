@@ -156,3 +156,27 @@ def append_records(path, recs):
     with open(path, "a") as fh:
         for line in format_records(recs):
             fh.write(line + "\n")
+
+
+def contact_times(recs, vol_tot_ori, surf_j):
+    """CAL_TCON (two_phase.f:7304-7343) for every pair of the records' level sets: T_CON(L, LL)
+    = SURF_J * |VELVS(L) - VELVS(LL)|^2 * DCHAR with DCHAR = 0.5 (6 VOLS / 3.14159)^(1/3) and
+    VOLS = min(VOL_TOT_ORI(L), VOL_TOT_ORI(LL)) -- the reference's constants, in its order.
+    vol_tot_ori: the original volume of each record's level set.  Returns an nlvs x nlvs
+    array (zero on the diagonal)."""
+    vel = np.asarray(recs["vel"], dtype=np.float64)
+    vol = np.asarray(vol_tot_ori, dtype=np.float64)
+    nl = vel.shape[0]
+    if vol.shape != (nl,):
+        raise ValueError(f"vol_tot_ori must hold {nl} volumes")
+    out = np.zeros((nl, nl))
+    for a in range(nl):
+        for b in range(nl):
+            if a == b:
+                continue
+            vols = min(vol[b], vol[a])
+            dchar = 0.5 * ((6 * vols / 3.14159) ** (1.0 / 3.0))
+            d = vel[a] - vel[b]
+            urel = ((d[0] ** 2 + d[1] ** 2) + d[2] ** 2) ** 0.5
+            out[a, b] = surf_j * (urel ** 2) * dchar
+    return out

@@ -5,7 +5,7 @@ empty level set."""
 import numpy as np
 import pytest
 
-from lica_boiling1d_b200.bubbles import BubbleGrid, append_records, format_records
+from lica_boiling1d_b200.bubbles import BubbleGrid, append_records, contact_times, format_records
 from oracle import oracle
 from tests import bubble_cases as bc
 
@@ -148,3 +148,19 @@ def test_append_records(tmp_path):
     assert lines == format_records(rec) * 2
     assert [int(x[15:20]) for x in lines] == [1, 2, 1, 2]
     assert float(lines[0][20:35]) == pytest.approx(rec[0]["col"][0], rel=1e-7)
+
+
+def test_contact_times():
+    """CAL_TCON on three bubbles: symmetric, the smaller original volume sets the length, and a
+    known case: relative speed 5 (a velocity difference of (0, 3, -4)), volume pi/6 * 8 (a
+    sphere of diameter 2), SURF_J 0.5 -> 0.5 * 25 * 0.5 (8 pi / 3.14159)^(1/3)."""
+    rec = np.zeros(3, dtype=oracle.BUB_RECORD)
+    rec["vel"][0] = [1.0, 2.0, 0.0]
+    rec["vel"][1] = [1.0, -1.0, 4.0]
+    rec["vel"][2] = [1.0, 2.0, 0.0]
+    vol = np.array([np.pi / 6 * 8, np.pi / 6 * 27, 1.0])
+    t = contact_times(rec, vol, 0.5)
+    assert np.array_equal(t, t.T) and np.all(np.diag(t) == 0.0)
+    assert t[0, 1] == pytest.approx(0.5 * 25.0 * 0.5 * (8 * np.pi / 3.14159) ** (1 / 3), rel=1e-14)
+    assert t[0, 2] == 0.0  # same velocity
+    assert t[1, 2] == pytest.approx(0.5 * 25.0 * 0.5 * (6 / 3.14159) ** (1 / 3), rel=1e-14)
