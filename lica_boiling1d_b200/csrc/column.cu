@@ -1518,14 +1518,22 @@ colk::Phys make_phys(const lica_col_props* p) {
     return ph;
 }
 
+// Library-owned device buffers and streams are kept per device (ordinals 0..63), so a process
+// that drives several GPUs gets each one's own.
+constexpr int kMaxDevices = 64;
 struct ScratchCache {
     std::mutex mu;
     void* ptr = nullptr;
     size_t bytes = 0;
 };
-ScratchCache& scratch_cache() {
-    static ScratchCache s;
-    return s;
+int current_device() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) dev = 0;
+    return dev;
+}
+ScratchCache& scratch_cache(int dev) {
+    static ScratchCache s[kMaxDevices];
+    return s[dev];
 }
 
 // per-phase cycle profile target (device array of COLUMN_PHASES * ncol int64) or null
@@ -1812,11 +1820,17 @@ int launch_columns(colk::Args& A, int nmax, int threads, void* stream, int cap_l
     A.tri_smem = A.tri_cap > 0 ? 1 : 0;
     const size_t dyn = A.tri_smem ? 5 * ((size_t)A.tri_cap + 2) * sizeof(double) : 0;
     {
+        // the attribute is the current device's: kept per device
         static std::mutex mu;
-        static size_t set_bytes[4] = {0, 0, 0, 0};
+        static size_t set_bytes[kMaxDevices][4] = {};
         std::lock_guard<std::mutex> lk(mu);
+        const int dev = current_device();
+        if (dev >= kMaxDevices) {
+            lica_set_last_error("launch_columns", "device ordinal above 63", __FILE__, __LINE__);
+            return LICA_BAD_ARG;
+        }
         const int slot = nth == 64 ? 0 : (nth == 128 ? 1 : (nth == 256 ? 2 : 3));
-        if (dyn > set_bytes[slot]) {
+        if (dyn > set_bytes[dev][slot]) {
             cudaError_t e = cudaSuccess;
             if (nth == 32)
                 e = cudaFuncSetAttribute(colk::k_column_steps<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
@@ -1829,7 +1843,7 @@ int launch_columns(colk::Args& A, int nmax, int threads, void* stream, int cap_l
                 e = cudaFuncSetAttribute(colk::k_column_steps<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)dyn);
             LICA_CUDA_TRY(e);
-            set_bytes[slot] = dyn;
+            set_bytes[dev][slot] = dyn;
         }
     }
     if (nth == 32) colk::k_column_steps<32><<<A.ncol, 32, dyn, (cudaStream_t)stream>>>(A);
@@ -1842,7 +1856,12 @@ int launch_columns(colk::Args& A, int nmax, int threads, void* stream, int cap_l
 }
 
 int column_scratch(size_t need, void** out) {
-    ScratchCache& sc = scratch_cache();
+    const int dev = current_device();
+    if (dev >= kMaxDevices) {
+        lica_set_last_error("column scratch", "device ordinal above 63", __FILE__, __LINE__);
+        return LICA_BAD_ARG;
+    }
+    ScratchCache& sc = scratch_cache(dev);
     std::lock_guard<std::mutex> lk(sc.mu);
     if (need > sc.bytes) {
         if (sc.ptr) cudaFree(sc.ptr);
@@ -2120,26 +2139,34 @@ int column_steps_host(int32_t ncol, int32_t n, double length, const lica_col_pro
     }
     const size_t st_off = total;
     total += (4 * nc + 255) & ~(size_t)255;
-    // device copies in a grow-only buffer kept by the library (one host call at a time)
-    static std::mutex host_mu;
-    static char* host_buf = nullptr;
-    static size_t host_bytes = 0;
-    std::lock_guard<std::mutex> lk(host_mu);
-    if (total > host_bytes) {
-        if (host_buf) cudaFree(host_buf);
-        host_buf = nullptr;
-        host_bytes = 0;
-        LICA_CUDA_TRY(cudaMalloc(&host_buf, total));
-        host_bytes = total;
+    // device copies in a grow-only buffer kept by the library per device (one host call at a
+    // time)
+    const int dev = current_device();
+    if (dev >= kMaxDevices) {
+        lica_set_last_error("lica_gpu_column_steps", "device ordinal above 63", __FILE__, __LINE__);
+        return LICA_BAD_ARG;
     }
-    char* base = host_buf;
+    static std::mutex host_mu;
+    static char* host_buf[kMaxDevices] = {};
+    static size_t host_bytes[kMaxDevices] = {};
+    static cudaStream_t host_stream[kMaxDevices] = {};
+    std::lock_guard<std::mutex> lk(host_mu);
+    if (total > host_bytes[dev]) {
+        if (host_buf[dev]) cudaFree(host_buf[dev]);
+        host_buf[dev] = nullptr;
+        host_bytes[dev] = 0;
+        LICA_CUDA_TRY(cudaMalloc(&host_buf[dev], total));
+        host_bytes[dev] = total;
+    }
+    char* base = host_buf[dev];
     // copies and steps go on one stream of the library's, so the call waits once; a blocking
     // stream, so it stays ordered after work a caller left on the legacy default stream that
     // may use the same library scratch
-    static cudaStream_t host_stream = nullptr;
-    if (!host_stream) LICA_CUDA_TRY(cudaStreamCreateWithFlags(&host_stream, cudaStreamDefault));
+    if (!host_stream[dev]) LICA_CUDA_TRY(cudaStreamCreateWithFlags(&host_stream[dev], cudaStreamDefault));
+    cudaStream_t hs = host_stream[dev];
     // Small states (a few columns: the per-step drop-in use) go through one page-locked
-    // staging buffer, one copy each way instead of one per array; large ones copy directly.
+    // staging buffer (portable: pinned for every device), one copy each way instead of one
+    // per array; large ones copy directly.
     static char* pin_buf = nullptr;
     static size_t pin_bytes = 0;
     const bool packed = total <= ((size_t)64 << 20);
@@ -2147,15 +2174,15 @@ int column_steps_host(int32_t ncol, int32_t n, double length, const lica_col_pro
         if (pin_buf) cudaFreeHost(pin_buf);
         pin_buf = nullptr;
         pin_bytes = 0;
-        LICA_CUDA_TRY(cudaMallocHost((void**)&pin_buf, total));
+        LICA_CUDA_TRY(cudaHostAlloc((void**)&pin_buf, total, cudaHostAllocPortable));
         pin_bytes = total;
     }
     if (packed) {
         for (int q = 0; q < nfld; ++q) std::memcpy(pin_buf + off[q], f[q].h, f[q].bytes);
-        LICA_CUDA_TRY(cudaMemcpyAsync(base, pin_buf, st_off, cudaMemcpyHostToDevice, host_stream));
+        LICA_CUDA_TRY(cudaMemcpyAsync(base, pin_buf, st_off, cudaMemcpyHostToDevice, hs));
     } else {
         for (int q = 0; q < nfld; ++q)
-            LICA_CUDA_TRY(cudaMemcpyAsync(base + off[q], f[q].h, f[q].bytes, cudaMemcpyHostToDevice, host_stream));
+            LICA_CUDA_TRY(cudaMemcpyAsync(base + off[q], f[q].h, f[q].bytes, cudaMemcpyHostToDevice, hs));
     }
     lica_col_state d;
     d.w = (double*)(base + off[0]);
@@ -2174,21 +2201,21 @@ int column_steps_host(int32_t ncol, int32_t n, double length, const lica_col_pro
     d.scal = (double*)(base + off[13]);
     d.stats = (double*)(base + off[14]);
     int32_t* dst = (int32_t*)(base + st_off);
-    int rc = column_steps_device(ncol, n, length, props, &d, nsteps, 0, nullptr, dst, host_stream, geo);
+    int rc = column_steps_device(ncol, n, length, props, &d, nsteps, 0, nullptr, dst, hs, geo);
     if (rc) {
-        cudaStreamSynchronize(host_stream);
+        cudaStreamSynchronize(hs);
         return rc;
     }
     if (packed) {
-        LICA_CUDA_TRY(cudaMemcpyAsync(pin_buf, base, total, cudaMemcpyDeviceToHost, host_stream));
-        LICA_CUDA_TRY(cudaStreamSynchronize(host_stream));
+        LICA_CUDA_TRY(cudaMemcpyAsync(pin_buf, base, total, cudaMemcpyDeviceToHost, hs));
+        LICA_CUDA_TRY(cudaStreamSynchronize(hs));
         for (int q = 0; q < nfld; ++q) std::memcpy(f[q].h, pin_buf + off[q], f[q].bytes);
         std::memcpy(status, pin_buf + st_off, 4 * nc);
     } else {
         for (int q = 0; q < nfld; ++q)
-            LICA_CUDA_TRY(cudaMemcpyAsync(f[q].h, base + off[q], f[q].bytes, cudaMemcpyDeviceToHost, host_stream));
-        LICA_CUDA_TRY(cudaMemcpyAsync(status, dst, 4 * nc, cudaMemcpyDeviceToHost, host_stream));
-        LICA_CUDA_TRY(cudaStreamSynchronize(host_stream));
+            LICA_CUDA_TRY(cudaMemcpyAsync(f[q].h, base + off[q], f[q].bytes, cudaMemcpyDeviceToHost, hs));
+        LICA_CUDA_TRY(cudaMemcpyAsync(status, dst, 4 * nc, cudaMemcpyDeviceToHost, hs));
+        LICA_CUDA_TRY(cudaStreamSynchronize(hs));
     }
     int worst = LICA_OK;
     for (size_t c = 0; c < nc; ++c)
