@@ -1,8 +1,10 @@
-"""Sharding of independent 1-D column batches over ranks (one process per GPU).
+"""Sharding of independent work over ranks (one process per GPU).
 
 The columns of a batch never exchange data, so the ranks take contiguous blocks of the
 column list balanced by cells (a column step's work grows with its cells), step their
-block with no collective, and gather the per-column histories once at the end.
+block with no collective, and gather the per-column histories once at the end.  The bubble
+statistics of several level sets shard the same way: each rank tracks a contiguous block of
+the level sets (equal work: every level set reads one field) and the records are gathered.
 """
 import numpy as np
 
@@ -35,3 +37,14 @@ def gather_histories(local, world, group=None):
     parts = [None] * world
     dist.all_gather_object(parts, list(local), group=group)
     return [rec for part in parts for rec in part]
+
+
+def gather_records(local, world, group=None):
+    """The ranks' structured-array records (e.g. bubbles.RECORD) concatenated in rank order,
+    on every rank (one all_gather)."""
+    if world == 1:
+        return np.asarray(local)
+    import torch.distributed as dist
+    parts = [None] * world
+    dist.all_gather_object(parts, np.asarray(local), group=group)
+    return np.concatenate(parts)

@@ -1,6 +1,7 @@
-"""Column-batch sharding over ranks on the CPU: the balanced partition, and a world-size-2
-gloo run (each rank steps its block of an uneven batch with the oracle, no per-step
-collective, one gather at the end) that must reproduce the single-process run exactly."""
+"""Sharding over ranks on the CPU: the balanced partition; a world-size-2 gloo run in which
+each rank steps its block of an uneven column batch with the oracle (no per-step collective,
+one gather at the end) and must reproduce the single-process run exactly; and the same for
+the bubble statistics of several level sets, each rank taking a block of the level sets."""
 import os
 import socket
 
@@ -71,3 +72,39 @@ def test_sharded_batch_matches_single_process():
     n, length, z0, props = case
     ref = _records(0, len(n), n, length, z0, props, steps)
     assert got == ref
+
+
+def _bubble_worker(rank, world, port, queue):
+    import torch.distributed as dist
+    from oracle import oracle as O
+    from tests import bubble_cases as bc
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    grid, psi, (u, v, w) = bc.three_bubbles(n1=24, n2=20, n3=28)
+    lo, hi = shard.partition(np.ones(len(psi)), world)[rank]
+    local = O.bubble_tracking(grid.as_dict(), psi[lo:hi], u, v, w, time=0.5, llvs0=1 + lo)
+    recs = shard.gather_records(local, world)
+    if rank == 0:
+        queue.put(recs.tobytes())
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_sharded_bubble_statistics_match_single_process():
+    import torch.multiprocessing as mp
+    from oracle import oracle as O
+    from tests import bubble_cases as bc
+    ctx = mp.get_context("spawn")
+    queue = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_bubble_worker, args=(r, 2, port, queue)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = queue.get(timeout=240)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    grid, psi, (u, v, w) = bc.three_bubbles(n1=24, n2=20, n3=28)
+    ref = O.bubble_tracking(grid.as_dict(), psi, u, v, w, time=0.5, llvs0=1)
+    assert got == ref.tobytes()
