@@ -164,3 +164,24 @@ def test_contact_times():
     assert t[0, 1] == pytest.approx(0.5 * 25.0 * 0.5 * (8 * np.pi / 3.14159) ** (1 / 3), rel=1e-14)
     assert t[0, 2] == 0.0  # same velocity
     assert t[1, 2] == pytest.approx(0.5 * 25.0 * 0.5 * (6 / 3.14159) ** (1 / 3), rel=1e-14)
+
+
+def test_host_api_rejects_bad_shapes():
+    """The bubble API checks shapes before it reaches the GPU."""
+    from lica_boiling1d_b200 import bubbles
+    grid = BubbleGrid.uniform(8, 6, 4, 1.0, 1.0, 1.0)
+    fs = grid.field_shape
+    good = np.ones(fs)
+    with pytest.raises(ValueError):
+        bubbles.track(grid, np.ones((2,) + fs[:-1] + (fs[-1] + 1,)), good, good, good)
+    with pytest.raises(ValueError):
+        bubbles.track(grid, np.ones((1,) + fs), good, good, np.ones(fs[::-1]))
+    with pytest.raises(ValueError):
+        bubbles.track(grid, np.ones(fs), good, good, good)  # no level-set axis
+    bad = BubbleGrid.uniform(8, 6, 4, 1.0, 1.0, 1.0)
+    bad.sdy = np.ones(3)
+    with pytest.raises(ValueError):
+        bad._c()
+    rec = np.zeros(2, dtype=bubbles.RECORD)
+    with pytest.raises(ValueError):
+        bubbles.contact_times(rec, [1.0], 0.1)
