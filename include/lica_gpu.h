@@ -359,7 +359,7 @@ int lica_col_fld_read(const char* path, int32_t n, double length, const lica_col
 size_t lica_gpu_column_scratch_bytes(int32_t ncol, int32_t n);
 
 /* nsteps time steps of every column; device arrays.  threads: CTA width per column, 32,
- * 64, 128 or 256 (0: 256 for up to one column per SM, else 128); wider CTAs finish one
+ * 64, 128 or 256 (0: 256 for up to one column per SM, else 64); wider CTAs finish one
  * column sooner, narrower ones keep more columns per SM; every width gives the same bits.  scratch: NULL (the library keeps
  * one) or lica_gpu_column_scratch_bytes() of device memory.  status[ncol] (device) gets
  * LICA_OK, LICA_NOT_CONVERGED (TEMP_EXTP did not converge), LICA_BAND_OVERFLOW or

@@ -39,7 +39,7 @@ struct Phys {
     int iphs, mglobal;
 };
 
-constexpr int NT_DEFAULT = 128;  // threads per column CTA unless the caller picks 64 or 256
+constexpr int NT_DEFAULT = 128;  // threads per column CTA of the single-routine kernel
 constexpr int NFLOW = 30;        // flow-sized scratch arrays per column
 constexpr int XR = 132;          // TEMP_EXTP extension range held in shared memory (+halo)
 
@@ -1791,7 +1791,8 @@ int column_ctas_by_registers() {
 
 // The CTA width when the caller leaves it open: 256 threads while the batch has at most one
 // column per SM (each column is a latency chain, and a wider CTA finishes its phases sooner),
-// 128 beyond that (more columns per SM).
+// 64 beyond that (five columns per SM; on the 4096-column batch 64 threads take 25.6-25.8 ms
+// a step, 128 threads 38.7).
 int default_width(int ncol) {
     static int sms = 0;
     if (!sms) {
@@ -1800,7 +1801,7 @@ int default_width(int ncol) {
                                                       cudaSuccess || sms < 1)
             sms = 1;
     }
-    return ncol <= sms ? 256 : colk::NT_DEFAULT;
+    return ncol <= sms ? 256 : 64;
 }
 
 int launch_columns(colk::Args& A, int nmax, int threads, void* stream, int cap_limit = -1) {
