@@ -5,7 +5,10 @@
  *   - the 2-D multigrid (lica_mg_create / lica_mg_solve_host) on a bubble-like coefficient
  *     field: the residual the host computes from the header's operator must meet 1e-10;
  *   - whole RK3 steps of a column (lica_gpu_column_init / lica_gpu_column_steps), then the
- *     per-routine drop-ins REINITIALIZATION and GRID_COUPLING on the stepped state.
+ *     per-routine drop-ins REINITIALIZATION and GRID_COUPLING on the stepped state;
+ *   - BUBBLE_TRACKING (lica_gpu_bubble_tracking) of a 3 x 2 x 4-cell gas block with uniform
+ *     velocity in an 8^3 box: volume, centroid, velocity, second moments (n^2 - 1) h^2 / 12
+ *     per axis, aspect ratio sqrt(5) and the smallest axis along y.
  * Usage: host_gpu.  Prints "ok" and exits 0, or names the failed check. */
 #include <math.h>
 #include <stdio.h>
@@ -166,8 +169,51 @@ static int check_column(void) {
     return 0;
 }
 
+#define BN 8
+#define BIDX(i, j, k) ((i) + (BN + 2) * ((j) + (BN + 2) * (k)))
+
+static int check_bubbles(void) {
+    static double psi[(BN + 2) * (BN + 2) * (BN + 2)], u[(BN + 2) * (BN + 2) * (BN + 2)],
+        v[(BN + 2) * (BN + 2) * (BN + 2)], w[(BN + 2) * (BN + 2) * (BN + 2)];
+    double sd[BN + 2], xp[BN + 2];
+    const double h = 1.0 / BN;
+    for (int i = 0; i < BN + 2; ++i) {
+        sd[i] = h;
+        xp[i] = (i - 0.5) * h;
+    }
+    for (int q = 0; q < (BN + 2) * (BN + 2) * (BN + 2); ++q) {
+        psi[q] = 1.0;
+        u[q] = 1.0;
+        v[q] = 2.0;
+        w[q] = 3.0;
+    }
+    for (int k = 2; k <= 5; ++k)
+        for (int j = 3; j <= 4; ++j)
+            for (int i = 2; i <= 4; ++i) psi[BIDX(i, j, k)] = 0.0;
+    lica_bub_grid g = {BN, BN, BN, 1, 1, 0, 1.0, sd, sd, sd, xp, xp, xp};
+    lica_bub_record r;
+    if (lica_gpu_bubble_tracking(&g, 1, 7, psi, u, v, w, 0.25, 1, &r) != LICA_OK)
+        return fail("lica_gpu_bubble_tracking");
+    const double h2 = h * h, ev[3] = {8.0 / 12.0 * h2, 3.0 / 12.0 * h2, 15.0 / 12.0 * h2};
+    if (r.llvs != 7 || r.time != 0.25 || r.iz_periodic != 0) return fail("bubble record header");
+    if (fabs(r.vol - 24.0 * h * h2) > 1e-15) return fail("bubble volume");
+    if (fabs(r.col[0] - 2.5 * h) > 1e-14 || fabs(r.col[1] - 3.0 * h) > 1e-14 || fabs(r.col[2] - 3.0 * h) > 1e-14)
+        return fail("bubble centroid");
+    if (fabs(r.col[3] - 1.0) > 1e-13 || fabs(r.col[4] - 2.0) > 1e-13 || fabs(r.col[5] - 3.0) > 1e-13)
+        return fail("bubble velocity");
+    for (int a = 0; a < 3; ++a) {
+        int found = 0;
+        for (int b = 0; b < 3; ++b)
+            if (fabs(r.ami[b] - ev[a]) <= 1e-12 * ev[a]) found = 1;
+        if (!found) return fail("bubble second moments");
+    }
+    if (fabs(r.col[6] - sqrt(5.0)) > 1e-12) return fail("bubble aspect ratio");
+    if (fabs(r.col[7] - 90.0) > 1e-9 || fabs(r.col[8] - 90.0) > 1e-9) return fail("bubble angles");
+    return 0;
+}
+
 int main(void) {
-    if (check_poisson() || check_multigrid() || check_column()) return 1;
+    if (check_poisson() || check_multigrid() || check_column() || check_bubbles()) return 1;
     printf("ok\n");
     return 0;
 }

@@ -28,8 +28,9 @@ def test_compiled_host_drives_restart_and_grid_entry_points(tmp_path):
 @pytest.mark.gpu
 @pytest.mark.skipif(shutil.which("gcc") is None, reason="needs gcc")
 def test_compiled_host_drives_gpu_entry_points(tmp_path):
-    """tests/abi/host_gpu.c: POISSON, the 2-D multigrid solve, whole column steps and the
-    single-routine drop-ins, called from C with host arrays through the header alone."""
+    """tests/abi/host_gpu.c: POISSON, the 2-D multigrid solve, whole column steps, the
+    single-routine drop-ins and the bubble statistics, called from C with host arrays through
+    the header alone."""
     lib = build.build()
     exe = str(tmp_path / "host_gpu")
     libdir = os.path.dirname(lib)
